@@ -1,0 +1,55 @@
+"""ctypes binding of libqcm_b200.so (the C-ABI declared in include/qcm_b200.h).
+
+The library is built in-tree (qcmaquis_b200/libqcm_b200.so).  Importing this
+module fails loudly if it is missing: there is no Python or CPU fallback for
+the device path.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libqcm_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(f"qcmaquis_b200: native library missing at {LIB_PATH}; "
+                      "build it with `make -C qcmaquis_b200/csrc` (or __graft_entry__.build())")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+c_int, c_double, c_size_t, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_void_p
+c_uint32, c_uint64 = ctypes.c_uint32, ctypes.c_uint64
+P = ctypes.POINTER
+
+
+class QcmError(RuntimeError):
+    pass
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc != 0:
+        msg = lib.qcm_last_error().decode()
+        raise QcmError(f"{what}: status {rc}: {msg}")
+
+
+def _sig(name, restype, *argtypes):
+    f = getattr(lib, name)
+    f.restype = restype
+    f.argtypes = list(argtypes)
+    return f
+
+
+_sig("qcm_last_error", ctypes.c_char_p)
+_sig("qcm_version", ctypes.c_char_p)
+_sig("qcm_mpo_build_qc", c_int, c_int, P(c_double), P(c_double), c_double, P(c_void_p))
+_sig("qcm_mpo_make_twosite", c_int, c_void_p, P(c_void_p))
+_sig("qcm_mpo_length", c_int, c_void_p)
+_sig("qcm_mpo_serialize", c_int, c_void_p, c_void_p, c_size_t, P(c_size_t))
+_sig("qcm_mpo_deserialize", c_int, c_void_p, c_size_t, P(c_void_p))
+_sig("qcm_mpo_free", None, c_void_p)
+
+
+def dptr(a):
+    """double* of a C-contiguous float64 numpy array."""
+    return a.ctypes.data_as(P(c_double))

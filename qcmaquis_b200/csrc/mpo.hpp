@@ -1,0 +1,61 @@
+// MPO tensors for the two-site DMRG path (host side).
+//
+// Mirrors the parts of framework/dmrg/mp_tensors/mpotensor.h the contraction
+// schedule uses: row_dim/col_dim, row(b1) iteration in increasing b2
+// (std::set row_index), column(b2) iteration in increasing b1 (CSC col_tags),
+// at(b1,b2) -> list of (operator, scale) (term_descriptor), and the bond
+// Hermitian-conjugate map (mpotensor_detail.h:141-186).
+//
+// Site operators use the reference's W(in, out) convention (a block
+// (left_charge = phys_in, right_charge = phys_out) holds <out|O|in>, see
+// site_hamil_tasks.hpp:109-110 and op_iterate.hpp:54-66); entries are stored
+// as flat (in_state, out_state, value) over the physical Index's state order.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "symm.hpp"
+
+namespace qcm {
+
+struct SparseOp {
+    std::vector<uint32_t> in, out;
+    std::vector<double> val;
+};
+
+struct MPOTensor {
+    uint32_t rows = 1, cols = 1;
+    // entries sorted by (b1, b2); several consecutive entries may share (b1, b2)
+    std::vector<uint32_t> b1, b2, op;
+    std::vector<double> scale;
+    std::shared_ptr<std::vector<SparseOp>> ops;
+    Index phys;
+    // Hermitian pairs on the left and right bond: herm[b] = partner or -1
+    std::vector<int32_t> herm_left, phase_left, herm_right, phase_right;
+
+    // derived lookup structures
+    std::vector<uint32_t> row_ptr;   // CSR over entries (entries already row sorted)
+    std::vector<uint32_t> col_ptr, col_ent;  // CSC: entries of column b2, increasing b1
+    void finalize();
+};
+
+struct MPO {
+    std::vector<MPOTensor> t;
+    bool twosite = false;
+};
+
+// Builds the exact QC Hamiltonian MPO (TwoU1) from integrals h (L x L) and
+// V (L^4, chemist notation (pq|rs)).  The core energy is not part of the MPO.
+MPO build_qc_mpo(int L, const double* h, const double* V, double cutoff);
+
+// Two-site MPO: W_ts[p](b1,b3) = sum_b2 kron(W[p](b1,b2), W[p+1](b2,b3))
+// (mp_tensors/ts_ops.hpp:97-168).
+MPO make_twosite_mpo(const MPO& m);
+
+std::vector<uint8_t> serialize_mpo(const MPO& m);
+MPO deserialize_mpo(const uint8_t* p, std::size_t n);
+
+}  // namespace qcm
