@@ -1,0 +1,170 @@
+// ORACLE -- TEST INFRASTRUCTURE ONLY.  extern "C" entry points used by tests/, smoke()
+// and bench.py (cpu_baseline / --impl reference) through ctypes.
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "dmrg.hpp"
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+using namespace orc;
+
+namespace {
+thread_local std::string g_err;
+int fail(const std::string& m) { g_err = m; return -1; }
+void* dup_blob(const std::vector<uint8_t>& b, std::size_t* len) {
+    void* p = std::malloc(b.size() ? b.size() : 1);
+    std::memcpy(p, b.data(), b.size());
+    *len = b.size();
+    return p;
+}
+struct W {
+    std::vector<uint8_t> b;
+    template <class T> void put(T v) { const uint8_t* p = reinterpret_cast<const uint8_t*>(&v); b.insert(b.end(), p, p + sizeof(T)); }
+};
+}  // namespace
+
+struct orc_dmrg { DMRG* d; };
+
+extern "C" {
+
+const char* orc_last_error(void) { return g_err.c_str(); }
+
+int orc_init(const char* blas_path, int nthreads) {
+    std::string err;
+    if (!blas_init(blas_path, err)) return fail("blas_init: " + err);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    return 0;
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_free(void* p) { std::free(p); }
+
+int orc_dmrg_create(const void* blob, size_t n, int nup, int ndown, size_t Mmax, size_t init_bd, double cutoff, double tol,
+                    int maxiter, double ecore, orc_dmrg** out) {
+    try {
+        bool ts = false;
+        auto mpo = load_mpo_blob(static_cast<const uint8_t*>(blob), n, ts);
+        if (ts) return fail("orc_dmrg_create: expected a single-site MPO");
+        DMRGParams p;
+        p.Mmax = Mmax; p.init_bond_dimension = init_bd; p.cutoff = cutoff; p.jcd_tol = tol; p.jcd_maxiter = maxiter; p.ecore = ecore;
+        *out = new orc_dmrg{new DMRG(std::move(mpo), nup, ndown, p)};
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
+void orc_dmrg_free(orc_dmrg* h) { if (h) { delete h->d; delete h; } }
+
+int orc_dmrg_set_mmax(orc_dmrg* h, size_t Mmax) { h->d->p.Mmax = Mmax; return 0; }
+
+// energies/tw/tf/bond: arrays of 2L-2.  If stop_step >= 0, the frozen site problem of
+// that step is returned in *snap (free with orc_free) and the sweep stops there.
+int orc_dmrg_sweep(orc_dmrg* h, int sweep, double* energies, double* tw, double* tf, uint64_t* bond, int stop_step,
+                   void** snap, size_t* snap_len) {
+    try {
+        std::vector<double> E;
+        std::vector<TruncationResults> T;
+        std::vector<uint8_t> sb;
+        h->d->sweep(sweep, E, T, stop_step, &sb);
+        if (stop_step >= 0 && snap) { *snap = dup_blob(sb, snap_len); return 0; }
+        for (std::size_t i = 0; i < E.size(); ++i) {
+            if (energies) energies[i] = E[i];
+            if (tw) tw[i] = T[i].truncated_weight;
+            if (tf) tf[i] = T[i].truncated_fraction;
+            if (bond) bond[i] = T[i].bond_dimension;
+        }
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
+// [hpsi_count, hpsi_time, hpsi_flops, jd_time, schedule_time, trunc_time, boundary_time]
+int orc_dmrg_stats(orc_dmrg* h, double* out) {
+    DMRG& d = *h->d;
+    out[0] = double(d.hpsi_count); out[1] = d.hpsi_time; out[2] = double(d.hpsi_flops);
+    out[3] = d.jd_time; out[4] = d.schedule_time; out[5] = d.trunc_time; out[6] = d.boundary_time;
+    return 0;
+}
+
+// H_eff x for a frozen site problem; x, y are the twin blocks concatenated in block order.
+int orc_heff_apply(const void* snap, size_t n, const void* mpo_blob, size_t mn, int site1, const double* x, double* y,
+                   size_t len, int repeat, double* flops, double* seconds) {
+    try {
+        bool ts = false;
+        auto mpo = load_mpo_blob(static_cast<const uint8_t*>(mpo_blob), mn, ts);
+        MPOTensor W = ts ? mpo[site1] : make_twosite_mpo(mpo[site1], mpo[site1 + 1]);
+        MPSTensor twin;
+        Boundary Lb, Rb;
+        load_site_problem(static_cast<const uint8_t*>(snap), n, twin, Lb, Rb);
+        auto sched = create_contraction_schedule(twin, Lb, Rb, W);
+        std::vector<const double*> xv(twin.left.size(), nullptr);
+        std::vector<double*> yv(twin.left.size(), nullptr);
+        std::size_t off = 0;
+        for (std::size_t k = 0; k < twin.data.n_blocks(); ++k) {
+            std::size_t lb = twin.left.position(twin.data.lc[k]);
+            xv[lb] = x + off;
+            yv[lb] = y + off;
+            off += twin.data.b[k].d.size();
+        }
+        if (off != len) return fail("orc_heff_apply: vector length mismatch");
+        auto t0 = std::chrono::steady_clock::now();
+        for (int r = 0; r < std::max(1, repeat); ++r) {
+            std::fill(y, y + len, 0.0);
+            super_hamil_mv(*sched, Lb, Rb, xv, yv);
+        }
+        auto t1 = std::chrono::steady_clock::now();
+        if (flops) *flops = double(sched->total_flops);
+        if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count() / std::max(1, repeat);
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
+// Flat export of the schedule (bookkeeping parity).  Layout ("QSCH" v1):
+// u32 nblocks; per block: u32 ntj, ntj x (u32 mps_offset, ci, ci_eff, lb_ket);
+//   u32 ncoh; per cohort: u32 lb, rb, ls, rs, ci, ci_eff, nSrows, stripe, nunits;
+//   per unit: u32 offset, ms, nlines, nalpha; nlines x (u32 b1, u32 count); nalpha x (f64 alpha, u32 ti, u32 col)
+int orc_schedule_export(const void* snap, size_t n, const void* mpo_blob, size_t mn, int site1, void** out, size_t* len,
+                        double* flops) {
+    try {
+        bool ts = false;
+        auto mpo = load_mpo_blob(static_cast<const uint8_t*>(mpo_blob), mn, ts);
+        MPOTensor Wt = ts ? mpo[site1] : make_twosite_mpo(mpo[site1], mpo[site1 + 1]);
+        MPSTensor twin;
+        Boundary Lb, Rb;
+        load_site_problem(static_cast<const uint8_t*>(snap), n, twin, Lb, Rb);
+        auto s = create_contraction_schedule(twin, Lb, Rb, Wt);
+        W w;
+        w.put<uint32_t>(0x48435351u);
+        w.put<uint32_t>(uint32_t(s->blocks.size()));
+        for (auto& b : s->blocks) {
+            w.put<uint32_t>(uint32_t(b.t_schedule.size()));
+            for (auto& j : b.t_schedule) { w.put(j.mps_offset); w.put(j.ci); w.put(j.ci_eff); w.put(j.lb_ket); }
+            w.put<uint32_t>(uint32_t(b.data.size()));
+            for (auto& c : b.data) {
+                w.put(c.lb); w.put(c.rb); w.put(c.ls); w.put(c.rs); w.put(c.ci); w.put(c.ci_eff); w.put(c.nSrows); w.put(c.stripe);
+                w.put<uint32_t>(uint32_t(c.suv.size()));
+                for (auto& u : c.suv) {
+                    w.put(u.offset); w.put(u.ms); w.put<uint32_t>(uint32_t(u.b1.size())); w.put<uint32_t>(uint32_t(u.alpha.size()));
+                    for (std::size_t l = 0; l < u.b1.size(); ++l) { w.put(u.b1[l]); w.put(u.b2s[l]); }
+                    for (std::size_t a = 0; a < u.alpha.size(); ++a) { w.put(u.alpha[a]); w.put(u.tidx[2 * a]); w.put(u.tidx[2 * a + 1]); }
+                }
+            }
+        }
+        if (flops) *flops = double(s->total_flops);
+        *out = dup_blob(w.b, len);
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
+}  // extern "C"

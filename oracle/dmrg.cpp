@@ -1,0 +1,592 @@
+// ORACLE -- TEST INFRASTRUCTURE ONLY.  Two-site tensors, truncation, JD and the sweep,
+// restated from mp_tensors/{twositetensor.hpp,ts_ops.hpp,mpstensor.hpp,mps.hpp,
+// mps_initializers.h,mps_sectors.h}, block_matrix/block_matrix_algorithms.h,
+// ietl/jacobi.h and optimize/{ts_optimize.hpp,optimize.h}.
+#include "dmrg.hpp"
+
+#include <chrono>
+#include <cstring>
+
+namespace orc {
+
+namespace {
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+Mat matmul(const Mat& A, const Mat& B) {
+    Mat C(A.r, B.c);
+    dgemm('N', 'N', int(A.r), int(B.c), int(A.c), 1.0, A.d.data(), int(std::max<std::size_t>(A.r, 1)), B.d.data(),
+          int(std::max<std::size_t>(B.r, 1)), 0.0, C.d.data(), int(std::max<std::size_t>(C.r, 1)));
+    return C;
+}
+// block_matrix gemm (block_matrix_algorithms.h:64-90) for charge-diagonal operands
+BlockMatrix bm_gemm(const BlockMatrix& A, const BlockMatrix& B) {
+    BlockMatrix C;
+    for (std::size_t k = 0; k < A.n_blocks(); ++k) {
+        std::size_t j = B.find_left(A.rc[k]);
+        if (j == B.n_blocks()) continue;
+        C.insert(A.lc[k], B.rc[j], matmul(A.b[k], B.b[j]));
+    }
+    return C;
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// two-site MPO (ts_ops.hpp:97-168).  An entry with several operators takes all of
+// them (the reference's single-summand branch reads operator 0 only; its MPOs
+// carry one operator per entry).
+MPOTensor make_twosite_mpo(const MPOTensor& W1, const MPOTensor& W2) {
+    MPOTensor T;
+    T.rows = W1.rows;
+    T.cols = W2.cols;
+    T.phys = W1.phys * W2.phys;
+    T.herm_left = W1.herm_left; T.phase_left = W1.phase_left;
+    T.herm_right = W2.herm_right; T.phase_right = W2.phase_right;
+    ProductBasis pb(W1.phys, W2.phys);
+    // sub-index of (s1, ss1) x (s2, ss2) inside the fused sector: pb + ss1*d2 + ss2 (alps_detail.hpp op_kron)
+    auto sector_sub = [&](std::size_t s1, unsigned ss1, std::size_t s2, unsigned ss2, std::size_t& sec, unsigned& sub) {
+        Q c = W1.phys[s1].first + W2.phys[s2].first;
+        sec = T.phys.position(c);
+        sub = unsigned(pb(W1.phys[s1].first, W2.phys[s2].first) + ss1 * W2.phys[s2].second + ss2);
+    };
+    auto kron_into = [&](const SiteOp& a, const SiteOp& b, double f, std::map<std::tuple<std::size_t, std::size_t, unsigned, unsigned>, double>& acc) {
+        for (auto& ba : a.blocks)
+            for (auto& bb : b.blocks)
+                for (std::size_t i = 0; i < ba.coeff.size(); ++i)
+                    for (std::size_t j = 0; j < bb.coeff.size(); ++j) {
+                        std::size_t si, so;
+                        unsigned ui, uo;
+                        sector_sub(ba.in_sec, ba.ss1[i], bb.in_sec, bb.ss1[j], si, ui);
+                        sector_sub(ba.out_sec, ba.ss2[i], bb.out_sec, bb.ss2[j], so, uo);
+                        acc[{si, so, ui, uo}] += f * ba.coeff[i] * bb.coeff[j];
+                    }
+    };
+    for (unsigned b1 = 0; b1 < W1.rows; ++b1) {
+        std::map<unsigned, std::vector<unsigned>> summands;  // b3 -> b2 list
+        for (unsigned b2 : W1.row_b2[b1])
+            for (unsigned b3 : W2.row_b2[b2]) summands[b3].push_back(b2);
+        for (auto& kv : summands) {
+            unsigned b3 = kv.first;
+            std::map<std::tuple<std::size_t, std::size_t, unsigned, unsigned>, double> acc;
+            double scale = 1.0;
+            const auto& e1s = W1.at.at({b1, kv.second[0]});
+            const auto& e2s = W2.at.at({kv.second[0], b3});
+            if (kv.second.size() == 1 && e1s.size() == 1 && e2s.size() == 1) {
+                kron_into(W1.ops[W1.op[e1s[0]]], W2.ops[W2.op[e2s[0]]], 1.0, acc);
+                scale = W1.scale[e1s[0]] * W2.scale[e2s[0]];
+            } else {
+                for (unsigned b2 : kv.second)
+                    for (unsigned e1 : W1.at.at({b1, b2}))
+                        for (unsigned e2 : W2.at.at({b2, b3}))
+                            kron_into(W1.ops[W1.op[e1]], W2.ops[W2.op[e2]], W1.scale[e1] * W2.scale[e2], acc);
+            }
+            SiteOp op;
+            for (auto& a : acc) {
+                if (a.second == 0.0) continue;
+                std::size_t si = std::get<0>(a.first), so = std::get<1>(a.first);
+                std::size_t bi = 0;
+                while (bi < op.blocks.size() && !(op.blocks[bi].in_sec == si && op.blocks[bi].out_sec == so)) ++bi;
+                if (bi == op.blocks.size()) op.blocks.push_back(OpBlock{si, so, {}, {}, {}});
+                op.blocks[bi].ss1.push_back(std::get<2>(a.first));
+                op.blocks[bi].ss2.push_back(std::get<3>(a.first));
+                op.blocks[bi].coeff.push_back(a.second);
+            }
+            if (op.blocks.empty()) continue;
+            unsigned e = unsigned(T.b1.size());
+            T.b1.push_back(b1); T.b2.push_back(b3); T.op.push_back(unsigned(T.ops.size())); T.scale.push_back(scale);
+            T.ops.push_back(std::move(op));
+            T.at[{b1, b3}].push_back(e);
+        }
+    }
+    T.row_b2.resize(T.rows);
+    T.col_b1.resize(T.cols);
+    for (auto& kv : T.at) { T.row_b2[kv.first.first].push_back(kv.first.second); T.col_b1[kv.first.second].push_back(kv.first.first); }
+    for (auto& v : T.row_b2) std::sort(v.begin(), v.end());
+    for (auto& v : T.col_b1) std::sort(v.begin(), v.end());
+    return T;
+}
+
+// ---------------------------------------------------------------------------
+// two-site tensor (twositetensor.hpp:29-199, ts_reshape.h)
+TwoSite::TwoSite(MPSTensor a, MPSTensor b) {
+    phys1 = a.phys; phys2 = b.phys; phys = phys1 * phys2; left = a.left; right = b.right;
+    a.make_left_paired();
+    b.make_right_paired();
+    both = bm_gemm(a.data, b.data);
+}
+
+MPSTensor TwoSite::make_mps() const {
+    ProductBasis in_left(phys1, left), in_right(phys2, right, true), out_right(phys, right, true), ppb(phys1, phys2);
+    MPSTensor t;
+    t.phys = phys; t.left = left; t.right = right; t.pairing = RightPaired;
+    for (std::size_t k = 0; k < both.n_blocks(); ++k) {
+        Q c = both.lc[k];
+        const Mat& in = both.b[k];
+        for (std::size_t s1 = 0; s1 < phys1.size(); ++s1) {
+            Q p1 = phys1[s1].first;
+            std::size_t l = left.position(c + (-p1));
+            if (l == left.size()) continue;
+            for (std::size_t s2 = 0; s2 < phys2.size(); ++s2) {
+                Q p2 = phys2[s2].first;
+                std::size_t r = right.position(c + p2);
+                if (r == right.size()) continue;
+                Q lc = left[l].first, rc = right[r].first, sc = p1 + p2;
+                std::size_t ob = t.data.find(lc, lc);
+                if (ob == t.data.n_blocks()) ob = t.data.insert(lc, lc, Mat(left[l].second, out_right.size(lc)));
+                Mat& out = t.data.b[ob];
+                std::size_t ldim = left[l].second, rdim = right[r].second, sd1 = phys1[s1].second, sd2 = phys2[s2].second;
+                std::size_t ilo = in_left(p1, lc), iro = in_right(p2, rc), oro = out_right(sc, rc), opo = ppb(p1, p2);
+                for (std::size_t ss1 = 0; ss1 < sd1; ++ss1)
+                    for (std::size_t ss2 = 0; ss2 < sd2; ++ss2) {
+                        std::size_t so = opo + ss1 * sd2 + ss2;
+                        for (std::size_t rr = 0; rr < rdim; ++rr)
+                            for (std::size_t ll = 0; ll < ldim; ++ll)
+                                out(ll, oro + so * rdim + rr) = in(ilo + ss1 * ldim + ll, iro + ss2 * rdim + rr);
+                    }
+            }
+        }
+    }
+    return t;
+}
+
+void TwoSite::set_from_mps(const MPSTensor& tw) {
+    ProductBasis in_left(phys1, left), in_right(phys2, right, true), out_right(phys, right, true), ppb(phys1, phys2);
+    for (auto& m : both.b) std::fill(m.d.begin(), m.d.end(), 0.0);
+    for (std::size_t k = 0; k < tw.data.n_blocks(); ++k) {
+        Q lc = tw.data.lc[k];
+        std::size_t l = left.position(lc);
+        const Mat& src = tw.data.b[k];
+        for (std::size_t s1 = 0; s1 < phys1.size(); ++s1)
+            for (std::size_t s2 = 0; s2 < phys2.size(); ++s2) {
+                Q p1 = phys1[s1].first, p2 = phys2[s2].first;
+                Q rc = lc + p1 + p2;
+                std::size_t r = right.position(rc);
+                if (r == right.size()) continue;
+                Q c = lc + p1;
+                std::size_t bb = both.find(c, c);
+                if (bb == both.n_blocks()) continue;
+                Mat& dst = both.b[bb];
+                std::size_t ldim = left[l].second, rdim = right[r].second, sd1 = phys1[s1].second, sd2 = phys2[s2].second;
+                std::size_t ilo = in_left(p1, lc), iro = in_right(p2, rc), oro = out_right(p1 + p2, rc), opo = ppb(p1, p2);
+                for (std::size_t ss1 = 0; ss1 < sd1; ++ss1)
+                    for (std::size_t ss2 = 0; ss2 < sd2; ++ss2) {
+                        std::size_t so = opo + ss1 * sd2 + ss2;
+                        for (std::size_t rr = 0; rr < rdim; ++rr)
+                            for (std::size_t ll = 0; ll < ldim; ++ll)
+                                dst(ilo + ss1 * ldim + ll, iro + ss2 * rdim + rr) = src(ll, oro + so * rdim + rr);
+                    }
+            }
+    }
+}
+
+TruncationResults svd_truncate(const BlockMatrix& M, BlockMatrix& U, BlockMatrix& V, std::vector<std::vector<double>>& S,
+                               double cutoff, std::size_t Mmax) {
+    std::size_t nb = M.n_blocks();
+    U = BlockMatrix(); V = BlockMatrix();
+    std::vector<Mat> Ub(nb), Vb(nb);
+    S.assign(nb, {});
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < int(nb); ++k) dgesvd_thin(M.b[k], Ub[k], S[k], Vb[k]);
+    // estimate_truncation (block_matrix_algorithms.h:136-183)
+    std::vector<double> all;
+    for (auto& s : S) all.insert(all.end(), s.begin(), s.end());
+    std::sort(all.begin(), all.end());
+    std::reverse(all.begin(), all.end());
+    TruncationResults tr;
+    double evalscut = cutoff * all[0];
+    if (all.size() > Mmax) evalscut = std::max(evalscut, all[Mmax]);
+    tr.smallest_ev = evalscut / all[0];
+    double tf = 0, tw = 0, sum = 0, sum2 = 0;
+    auto it = std::find_if(all.begin(), all.end(), [&](double x) { return x < evalscut; });
+    for (; it != all.end(); ++it) { tf += *it; tw += (*it) * (*it); }
+    for (double x : all) { sum += x; sum2 += x * x; }
+    tr.truncated_fraction = tf / sum;
+    tr.truncated_weight = tw / sum2;
+    for (std::size_t k = 0; k < nb; ++k) {
+        std::size_t keep = std::find_if(S[k].begin(), S[k].end(), [&](double x) { return x < evalscut; }) - S[k].begin();
+        if (keep == 0) continue;
+        Mat u(Ub[k].r, keep), v(keep, Vb[k].c);
+        for (std::size_t j = 0; j < keep; ++j)
+            for (std::size_t i = 0; i < Ub[k].r; ++i) u(i, j) = Ub[k](i, j);
+        for (std::size_t j = 0; j < Vb[k].c; ++j)
+            for (std::size_t i = 0; i < keep; ++i) v(i, j) = Vb[k](i, j);
+        S[k].resize(keep);
+        U.insert(M.lc[k], M.rc[k], std::move(u));
+        V.insert(M.lc[k], M.rc[k], std::move(v));
+        tr.bond_dimension += keep;
+    }
+    std::vector<std::vector<double>> Sk;
+    for (std::size_t k = 0; k < nb; ++k) if (!S[k].empty()) Sk.push_back(S[k]);
+    S = Sk;
+    return tr;
+}
+
+void TwoSite::split_l2r(std::size_t Mmax, double cutoff, MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const {
+    BlockMatrix U, V;
+    std::vector<std::vector<double>> S;
+    tr = svd_truncate(both, U, V, S, cutoff, Mmax);
+    m1 = MPSTensor();
+    m1.phys = phys1; m1.left = left; m1.right = U.right_basis(); m1.pairing = LeftPaired; m1.data = U;
+    for (std::size_t k = 0; k < V.n_blocks(); ++k)
+        for (std::size_t j = 0; j < V.b[k].c; ++j)
+            for (std::size_t i = 0; i < V.b[k].r; ++i) V.b[k](i, j) *= S[k][i];
+    m2 = MPSTensor();
+    m2.phys = phys2; m2.left = V.left_basis(); m2.right = right; m2.pairing = RightPaired; m2.data = V;
+}
+
+void TwoSite::split_r2l(std::size_t Mmax, double cutoff, MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const {
+    BlockMatrix U, V;
+    std::vector<std::vector<double>> S;
+    tr = svd_truncate(both, U, V, S, cutoff, Mmax);
+    m2 = MPSTensor();
+    m2.phys = phys2; m2.left = V.left_basis(); m2.right = right; m2.pairing = RightPaired; m2.data = V;
+    for (std::size_t k = 0; k < U.n_blocks(); ++k)
+        for (std::size_t j = 0; j < U.b[k].c; ++j)
+            for (std::size_t i = 0; i < U.b[k].r; ++i) U.b[k](i, j) *= S[k][j];
+    m1 = MPSTensor();
+    m1.phys = phys1; m1.left = left; m1.right = U.right_basis(); m1.pairing = LeftPaired; m1.data = U;
+}
+
+BlockMatrix normalize_left(MPSTensor& t) {
+    t.make_left_paired();
+    BlockMatrix Qm, R;
+    for (std::size_t k = 0; k < t.data.n_blocks(); ++k) {
+        Mat q, r;
+        qr(t.data.b[k], q, r);
+        Qm.insert(t.data.lc[k], t.data.rc[k], std::move(q));
+        R.insert(t.data.rc[k], t.data.rc[k], std::move(r));
+    }
+    t.data = Qm;
+    t.right = Qm.right_basis();
+    return R;
+}
+
+BlockMatrix normalize_right(MPSTensor& t) {
+    t.make_right_paired();
+    BlockMatrix Lm, Qm;
+    for (std::size_t k = 0; k < t.data.n_blocks(); ++k) {
+        Mat l, q;
+        lq(t.data.b[k], l, q);
+        Lm.insert(t.data.lc[k], t.data.lc[k], std::move(l));
+        Qm.insert(t.data.lc[k], t.data.rc[k], std::move(q));
+    }
+    t.data = Qm;
+    t.left = Qm.left_basis();
+    return Lm;
+}
+
+void multiply_from_left(MPSTensor& t, const BlockMatrix& N) {
+    t.make_right_paired();
+    t.data = bm_gemm(N, t.data);
+    t.left = t.data.left_basis();
+}
+
+void multiply_from_right(MPSTensor& t, const BlockMatrix& N) {
+    t.make_left_paired();
+    t.data = bm_gemm(t.data, N);
+    t.right = t.data.right_basis();
+}
+
+// ---------------------------------------------------------------------------
+// Jacobi-Davidson (ietl/jacobi.h:386-474; jcd_gmres_solver with max_iter 0 at :141-157)
+double jacobi_davidson(const std::function<void(const std::vector<double>&, std::vector<double>&)>& mult,
+                       const std::vector<double>& x0, double tol, int maxiter, std::vector<double>& out, int& iters) {
+    const std::size_t n = x0.size();
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+        double s = 0; for (std::size_t i = 0; i < n; ++i) s += a[i] * b[i]; return s; };
+    auto nrm = [&](const std::vector<double>& a) { return std::sqrt(dot(a, a)); };
+    std::vector<std::vector<double>> V(maxiter), VA(maxiter);
+    std::vector<double> M(std::size_t(maxiter) * maxiter, 0.0);
+    V[0] = x0;
+    int it = 0;
+    double theta = 0;
+    std::vector<double> s, u(n), uA(n);
+    while (true) {
+        std::vector<double>& t = V[it];
+        double tau = nrm(t);
+        for (int i = 1; i <= it; ++i) { double d = dot(V[i - 1], t); for (std::size_t k = 0; k < n; ++k) t[k] -= d * V[i - 1][k]; }
+        if (nrm(t) < 0.25 * tau)
+            for (int i = 1; i <= it; ++i) { double d = dot(V[i - 1], t); for (std::size_t k = 0; k < n; ++k) t[k] -= d * V[i - 1][k]; }
+        double tn = nrm(t);
+        for (auto& x : t) x /= tn;
+        VA[it].assign(n, 0.0);
+        mult(t, VA[it]);
+        for (int i = 1; i <= it + 1; ++i) M[(i - 1) + std::size_t(it) * maxiter] = dot(V[i - 1], VA[it]);
+        dsyevx_lowest(M.data(), maxiter, it + 1, tol, theta, s);
+        for (std::size_t k = 0; k < n; ++k) { u[k] = V[0][k] * s[0]; uA[k] = VA[0][k] * s[0]; }
+        for (int j = 1; j <= it; ++j)
+            for (std::size_t k = 0; k < n; ++k) { u[k] += V[j][k] * s[j]; uA[k] += VA[j][k] * s[j]; }
+        std::vector<double>& r = uA;
+        for (std::size_t k = 0; k < n; ++k) r[k] -= theta * u[k];
+        ++it;
+        double rn = nrm(r);
+        if (rn <= tol * std::fabs(theta) || rn < tol || it >= maxiter) { out = u; iters = it; return theta; }
+        double dru = dot(r, u), duu = dot(u, u);
+        V[it].assign(n, 0.0);
+        for (std::size_t k = 0; k < n; ++k) V[it][k] = -r[k] + dru / duu * u[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// MPS initialisation: allowed_sectors (mps_sectors.h:52-140) + const_mps_init
+// (mps_initializers.h:84-100) + MPS::normalize_left (mps.hpp:129-136)
+namespace {
+std::vector<Index> allowed_sectors(int L, const Index& phys, Q right_end, std::size_t Mmax) {
+    Index physc = phys;
+    physc.sort();
+    Q maxc = physc.v.front().first, minc = physc.v.back().first;
+    if (minc > maxc) std::swap(maxc, minc);
+    Q maxt, mint;
+    for (int i = 0; i < L; ++i) { maxt = maxt + maxc; mint = mint + minc; }
+    std::vector<Index> la(L + 1), ra(L + 1), allowed(L + 1);
+    la[0].insert(Q(0, 0), 1);
+    ra[L].insert(right_end, 1);
+    Q cmaxi = maxt, cmini = mint;
+    for (int i = 1; i <= L; ++i) {
+        la[i] = phys * la[i - 1];
+        cmaxi = cmaxi + (-maxc);
+        cmini = cmini + (-minc);
+        Index keep;
+        for (auto& e : la[i].v) {
+            if ((e.first + cmaxi) < right_end) continue;
+            if ((e.first + cmini) > right_end) continue;
+            keep.v.push_back({e.first, std::min(Mmax, e.second)});
+        }
+        la[i] = keep;
+    }
+    cmaxi = maxt; cmini = mint;
+    for (int i = L - 1; i >= 0; --i) {
+        ra[i] = adjoin(phys) * ra[i + 1];
+        cmaxi = cmaxi + (-maxc);
+        cmini = cmini + (-minc);
+        Index keep;
+        for (auto& e : ra[i].v) {
+            if ((e.first + (-cmaxi)) > Q(0, 0)) continue;
+            if ((e.first + (-cmini)) < Q(0, 0)) continue;
+            keep.v.push_back({e.first, std::min(Mmax, e.second)});
+        }
+        ra[i] = keep;
+    }
+    for (int i = 0; i <= L; ++i) {
+        Index a = la[i], b = ra[i];
+        common_subset(a, b);
+        for (auto& e : a.v) e.second = std::min(Mmax, std::min(la[i].size_of_block(e.first), ra[i].size_of_block(e.first)));
+        allowed[i] = a;
+    }
+    return allowed;
+}
+
+// MPSTensor(sd, ld, rd, fillrand=false, val) (mpstensor.hpp:40-71)
+MPSTensor const_tensor(const Index& sd, const Index& ld, const Index& rd, double val) {
+    MPSTensor t;
+    t.phys = sd;
+    Index lb = sd * ld, rb = rd;
+    common_subset(lb, rb);
+    t.right = rb;
+    Index possible = adjoin(sd) * t.right, ltemp = ld;
+    common_subset(ltemp, possible);
+    t.left = ltemp;
+    lb.sort(); rb.sort(); t.left.sort(); t.right.sort();
+    t.pairing = LeftPaired;
+    for (std::size_t k = 0; k < lb.size(); ++k) t.data.insert(lb[k].first, rb[k].first, Mat(lb[k].second, rb[k].second, val));
+    return t;
+}
+}  // namespace
+
+DMRG::DMRG(std::vector<MPOTensor> mpo_single, int nup, int ndown, const DMRGParams& prm) : mpo(std::move(mpo_single)), p(prm) {
+    L = int(mpo.size());
+    for (int i = 0; i + 1 < L; ++i) ts_mpo.push_back(make_twosite_mpo(mpo[i], mpo[i + 1]));
+    Index phys = mpo[0].phys;
+    std::vector<Index> allowed = allowed_sectors(L, phys, Q(nup, ndown), p.init_bond_dimension);
+    mps.resize(L);
+    for (int i = 0; i < L; ++i) {
+        mps[i] = const_tensor(phys, allowed[i], allowed[i + 1], 1.0);
+        mps[i].scale(1.0 / mps[i].norm());
+    }
+    // MPS::normalize_left: canonize(L-1) then normalise the last site
+    for (int i = 0; i < L - 1; ++i) {
+        BlockMatrix t = normalize_left(mps[i]);
+        multiply_from_left(mps[i + 1], t);
+        mps[i + 1].scale(1.0 / mps[i + 1].norm());
+    }
+    normalize_left(mps[L - 1]);
+    // optimizer_base: mps.canonize(0)
+    for (int i = L - 1; i > 0; --i) {
+        BlockMatrix t = normalize_right(mps[i]);
+        multiply_from_right(mps[i - 1], t);
+        mps[i - 1].scale(1.0 / mps[i - 1].norm());
+    }
+    // init_left_right (optimize.h:158-195)
+    left_.resize(L + 1);
+    right_.resize(L + 1);
+    left_[0] = trivial_boundary(mps[0].left, mpo[0].rows);
+    right_[L] = trivial_boundary(mps[L - 1].right, mpo[L - 1].cols);
+    for (int i = L - 1; i >= 0; --i) right_[i] = overlap_mpo_right_step(mps[i], mps[i], right_[i + 1], mpo[i], true);
+}
+
+void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc, int stop_step,
+                 std::vector<uint8_t>* snap) {
+    (void)sweep_no;
+    energies.clear();
+    trunc.clear();
+    for (int _site = 0; _site < 2 * L - 2; ++_site) {
+        int lr, site1, site2;
+        int site = (_site < L - 1) ? _site : 2 * L - 2 - _site;
+        if (_site < L - 1) { lr = 1; site1 = site; site2 = site + 1; }
+        else { lr = -1; site1 = site - 1; site2 = site; }
+        TwoSite tst(mps[site1], mps[site2]);
+        MPSTensor twin = tst.make_mps();
+        if (stop_step == _site && snap) {
+            *snap = save_site_problem(twin, left_[site1], right_[site2 + 1]);
+            return;
+        }
+        // solve_site_problem (solver_interface.hpp:30-77)
+        double t0 = now_s();
+        auto sched = create_contraction_schedule(twin, left_[site1], right_[site2 + 1], ts_mpo[site1]);
+        double t1 = now_s();
+        schedule_time += t1 - t0;
+        std::vector<std::size_t> off;
+        std::size_t tot = 0;
+        for (auto& b : twin.data.b) { off.push_back(tot); tot += b.d.size(); }
+        std::vector<double> x0(tot);
+        for (std::size_t k = 0; k < twin.data.n_blocks(); ++k) std::copy(twin.data.b[k].d.begin(), twin.data.b[k].d.end(), x0.begin() + off[k]);
+        auto mult = [&](const std::vector<double>& x, std::vector<double>& y) {
+            double h0 = now_s();
+            std::vector<const double*> xv(twin.left.size(), nullptr);
+            std::vector<double*> yv(twin.left.size(), nullptr);
+            std::fill(y.begin(), y.end(), 0.0);
+            for (std::size_t lb = 0; lb < twin.left.size(); ++lb) {
+                std::size_t k = twin.data.find(twin.left[lb].first, twin.left[lb].first);
+                if (k == twin.data.n_blocks()) continue;
+                xv[lb] = x.data() + off[k];
+                yv[lb] = y.data() + off[k];
+            }
+            super_hamil_mv(*sched, left_[site1], right_[site2 + 1], xv, yv);
+            hpsi_time += now_s() - h0;
+            hpsi_count++;
+            hpsi_flops += sched->total_flops;
+        };
+        std::vector<double> xo;
+        int iters = 0;
+        double E = jacobi_davidson(mult, x0, p.jcd_tol, p.jcd_maxiter, xo, iters);
+        jd_time += now_s() - t1;
+        for (std::size_t k = 0; k < twin.data.n_blocks(); ++k)
+            std::copy(xo.begin() + off[k], xo.begin() + off[k] + twin.data.b[k].d.size(), twin.data.b[k].d.begin());
+        tst.set_from_mps(twin);
+        energies.push_back(E + p.ecore);
+        TruncationResults tr;
+        double t2 = now_s();
+        if (lr == 1) {
+            tst.split_l2r(p.Mmax, p.cutoff, mps[site1], mps[site2], tr);
+            BlockMatrix t = normalize_left(mps[site2]);
+            if (site2 < L - 1) multiply_from_left(mps[site2 + 1], t);
+            double t3 = now_s();
+            trunc_time += t3 - t2;
+            left_[site2] = overlap_mpo_left_step(mps[site1], mps[site1], left_[site1], mpo[site1], true);
+            boundary_time += now_s() - t3;
+        } else {
+            tst.split_r2l(p.Mmax, p.cutoff, mps[site1], mps[site2], tr);
+            BlockMatrix t = normalize_right(mps[site1]);
+            if (site1 > 0) multiply_from_right(mps[site1 - 1], t);
+            double t3 = now_s();
+            trunc_time += t3 - t2;
+            right_[site2] = overlap_mpo_right_step(mps[site2], mps[site2], right_[site2 + 1], mpo[site2], true);
+            boundary_time += now_s() - t3;
+        }
+        trunc.push_back(tr);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// "QSPB" v1 site-problem blob
+namespace {
+struct W {
+    std::vector<uint8_t> b;
+    template <class T> void put(T v) { const uint8_t* p = reinterpret_cast<const uint8_t*>(&v); b.insert(b.end(), p, p + sizeof(T)); }
+    void idx(const Index& i) { put<uint32_t>(uint32_t(i.size())); for (auto& e : i.v) { put<int32_t>(e.first.n[0]); put<int32_t>(e.first.n[1]); put<uint32_t>(uint32_t(e.second)); } }
+    void bnd(const Boundary& B) {
+        const BoundaryIndex& x = B.index;
+        idx(x.bra); idx(x.ket);
+        uint32_t aux = x.n_cohorts() ? uint32_t(x.offsets[0].size()) : 0;
+        put<uint32_t>(x.n_cohorts()); put<uint32_t>(aux);
+        for (unsigned ci = 0; ci < x.n_cohorts(); ++ci) {
+            uint32_t lb = 0, rb = 0;
+            for (std::size_t i = 0; i < x.lbrb.size(); ++i)
+                for (std::size_t j = 0; j < x.lbrb[i].size(); ++j) if (x.lbrb[i][j] == ci) { lb = uint32_t(i); rb = uint32_t(j); }
+            put<uint32_t>(lb); put<uint32_t>(rb); put<uint8_t>(uint8_t(x.tr_[ci]));
+            put<uint32_t>(uint32_t(x.lsz[ci])); put<uint32_t>(uint32_t(x.rsz[ci])); put<uint32_t>(x.nb[ci]);
+            for (uint32_t b = 0; b < aux; ++b) put<int64_t>(x.offsets[ci][b]);
+            for (uint32_t b = 0; b < aux; ++b) put<double>(x.cscale[ci][b]);
+            put<uint64_t>(B.data[ci].size());
+            for (double v : B.data[ci]) put<double>(v);
+        }
+    }
+};
+struct R {
+    const uint8_t* p; std::size_t n, k = 0;
+    template <class T> T get() { if (k + sizeof(T) > n) throw std::runtime_error("site problem blob truncated"); T v; std::memcpy(&v, p + k, sizeof(T)); k += sizeof(T); return v; }
+    Index idx() { Index i; uint32_t m = get<uint32_t>(); for (uint32_t s = 0; s < m; ++s) { int a = get<int32_t>(), b = get<int32_t>(); uint32_t z = get<uint32_t>(); i.v.push_back({Q(a, b), z}); } return i; }
+    Boundary bnd() {
+        Boundary B;
+        Index bra = idx(), ket = idx();
+        B.index = BoundaryIndex(bra, ket);
+        uint32_t nc = get<uint32_t>(), aux = get<uint32_t>();
+        B.data.resize(nc);
+        for (uint32_t ci = 0; ci < nc; ++ci) {
+            uint32_t lb = get<uint32_t>(), rb = get<uint32_t>();
+            uint8_t tr = get<uint8_t>();
+            uint32_t ls = get<uint32_t>(), rs = get<uint32_t>(), nb = get<uint32_t>();
+            std::vector<long> off(aux);
+            std::vector<double> cs(aux);
+            for (auto& o : off) o = long(get<int64_t>());
+            for (auto& c : cs) c = get<double>();
+            B.index.lbrb[lb][rb] = ci;
+            B.index.offsets.push_back(off); B.index.cscale.push_back(cs);
+            B.index.trans.push_back(std::vector<char>(aux, 0)); B.index.tr_.push_back(char(tr));
+            B.index.lsz.push_back(ls); B.index.rsz.push_back(rs); B.index.nb.push_back(nb);
+            uint64_t nd = get<uint64_t>();
+            B.data[ci].resize(nd);
+            for (auto& v : B.data[ci]) v = get<double>();
+        }
+        return B;
+    }
+};
+}  // namespace
+
+std::vector<uint8_t> save_site_problem(const MPSTensor& twin0, const Boundary& L, const Boundary& Rb) {
+    MPSTensor twin = twin0;
+    twin.make_right_paired();
+    W w;
+    w.put<uint32_t>(0x42505351u);  // "QSPB"
+    w.put<uint32_t>(1);
+    w.idx(twin.phys); w.idx(twin.left); w.idx(twin.right);
+    w.put<uint32_t>(uint32_t(twin.data.n_blocks()));
+    for (std::size_t k = 0; k < twin.data.n_blocks(); ++k) {
+        w.put<int32_t>(twin.data.lc[k].n[0]); w.put<int32_t>(twin.data.lc[k].n[1]);
+        w.put<uint32_t>(uint32_t(twin.data.b[k].r)); w.put<uint32_t>(uint32_t(twin.data.b[k].c));
+        for (double v : twin.data.b[k].d) w.put<double>(v);
+    }
+    w.bnd(L);
+    w.bnd(Rb);
+    return w.b;
+}
+
+void load_site_problem(const uint8_t* p, std::size_t n, MPSTensor& twin, Boundary& Lb, Boundary& Rb) {
+    R r{p, n};
+    if (r.get<uint32_t>() != 0x42505351u || r.get<uint32_t>() != 1) throw std::runtime_error("bad site problem blob");
+    twin = MPSTensor();
+    twin.phys = r.idx(); twin.left = r.idx(); twin.right = r.idx();
+    twin.pairing = RightPaired;
+    uint32_t nb = r.get<uint32_t>();
+    for (uint32_t k = 0; k < nb; ++k) {
+        int a = r.get<int32_t>(), b = r.get<int32_t>();
+        uint32_t rows = r.get<uint32_t>(), cols = r.get<uint32_t>();
+        Mat m(rows, cols);
+        for (auto& v : m.d) v = r.get<double>();
+        twin.data.insert(Q(a, b), Q(a, b), std::move(m));
+    }
+    Lb = r.bnd();
+    Rb = r.bnd();
+}
+
+}  // namespace orc

@@ -1,0 +1,75 @@
+// ORACLE -- TEST INFRASTRUCTURE ONLY.  DMRG layer of the CPU restatement.
+#pragma once
+
+#include <functional>
+
+#include "engine.hpp"
+
+namespace orc {
+
+// block_matrix/block_matrix_algorithms.h:48-63
+struct TruncationResults {
+    std::size_t bond_dimension = 0;
+    double truncated_weight = 0, truncated_fraction = 0, smallest_ev = 0;
+};
+
+// two-site MPO (mp_tensors/ts_ops.hpp:97-168)
+MPOTensor make_twosite_mpo(const MPOTensor& W1, const MPOTensor& W2);
+
+// two-site tensor (mp_tensors/twositetensor.hpp)
+struct TwoSite {
+    Index phys1, phys2, phys, left, right;
+    BlockMatrix both;  // both-paired: rows phys1 x left, cols phys2 x right
+    TwoSite(MPSTensor a, MPSTensor b);
+    MPSTensor make_mps() const;                      // reshape_both_to_right
+    void set_from_mps(const MPSTensor& twin);        // reshape_right_to_both
+    void split_l2r(std::size_t Mmax, double cutoff, MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const;
+    void split_r2l(std::size_t Mmax, double cutoff, MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const;
+};
+
+// per-block SVD + estimate_truncation (block_matrix_algorithms.h:136-240)
+TruncationResults svd_truncate(const BlockMatrix& M, BlockMatrix& U, BlockMatrix& V, std::vector<std::vector<double>>& S,
+                               double cutoff, std::size_t Mmax);
+
+// MPSTensor normalisation (mpstensor.hpp:242-352)
+BlockMatrix normalize_left(MPSTensor& t);
+BlockMatrix normalize_right(MPSTensor& t);
+void multiply_from_left(MPSTensor& t, const BlockMatrix& N);
+void multiply_from_right(MPSTensor& t, const BlockMatrix& N);
+
+// Jacobi-Davidson for the lowest eigenpair (ietl/jacobi.h:386-474, gmres = 0)
+double jacobi_davidson(const std::function<void(const std::vector<double>&, std::vector<double>&)>& mult,
+                       const std::vector<double>& x0, double tol, int maxiter, std::vector<double>& out, int& iters);
+
+struct DMRGParams {
+    std::size_t Mmax = 64;
+    std::size_t init_bond_dimension = 64;
+    double cutoff = 1e-16;
+    double jcd_tol = 1e-10;
+    int jcd_maxiter = 8;
+    double ecore = 0.0;
+};
+
+struct DMRG {
+    int L;
+    std::vector<MPOTensor> mpo, ts_mpo;
+    std::vector<MPSTensor> mps;
+    std::vector<Boundary> left_, right_;
+    DMRGParams p;
+    std::size_t hpsi_count = 0;
+    double hpsi_time = 0, jd_time = 0, schedule_time = 0, trunc_time = 0, boundary_time = 0;
+    std::size_t hpsi_flops = 0;
+
+    DMRG(std::vector<MPOTensor> mpo_single, int nup, int ndown, const DMRGParams& prm);
+    // one full two-site sweep (ts_optimize.hpp:114-362); energies per step.
+    // If stop_step >= 0 the sweep stops before solving that step and the
+    // frozen site problem is written to *snap.
+    void sweep(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc, int stop_step = -1,
+               std::vector<uint8_t>* snap = nullptr);
+};
+
+// frozen site problem ("QSPB" v1): twin MPS (right-paired) + L + R boundaries
+std::vector<uint8_t> save_site_problem(const MPSTensor& twin, const Boundary& L, const Boundary& R);
+void load_site_problem(const uint8_t* p, std::size_t n, MPSTensor& twin, Boundary& L, Boundary& R);
+
+}  // namespace orc

@@ -1,0 +1,140 @@
+"""ctypes binding of the oracle (CPU restatement of the reference path).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+cpu_baseline / --impl reference legs of bench.py, never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+
+P = ctypes.POINTER
+c_int, c_double, c_size_t, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_size_t, ctypes.c_void_p
+
+
+def build() -> None:
+    subprocess.run(["make", "-C", _HERE], check=True, stdout=subprocess.DEVNULL)
+
+
+def openblas_path() -> str:
+    import scipy
+    libs = glob.glob(os.path.join(os.path.dirname(scipy.__file__) + ".libs", "libscipy_openblas*.so"))
+    if not libs:
+        raise RuntimeError("scipy-bundled OpenBLAS not found")
+    return libs[0]
+
+
+_lib = None
+
+
+def lib(nthreads: int = 0):
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_init.argtypes = [ctypes.c_char_p, c_int]
+        L.orc_max_threads.restype = c_int
+        L.orc_free.argtypes = [c_void_p]
+        L.orc_dmrg_create.argtypes = [c_void_p, c_size_t, c_int, c_int, c_size_t, c_size_t, c_double, c_double, c_int,
+                                      c_double, P(c_void_p)]
+        L.orc_dmrg_free.argtypes = [c_void_p]
+        L.orc_dmrg_set_mmax.argtypes = [c_void_p, c_size_t]
+        L.orc_dmrg_sweep.argtypes = [c_void_p, c_int, P(c_double), P(c_double), P(c_double), P(ctypes.c_uint64), c_int,
+                                     P(c_void_p), P(c_size_t)]
+        L.orc_dmrg_stats.argtypes = [c_void_p, P(c_double)]
+        L.orc_heff_apply.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), P(c_double), c_size_t,
+                                     c_int, P(c_double), P(c_double)]
+        L.orc_schedule_export.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_void_p), P(c_size_t),
+                                          P(c_double)]
+        _check(L, L.orc_init(openblas_path().encode(), nthreads))
+        _lib = L
+    return _lib
+
+
+def _check(L, rc):
+    if rc != 0:
+        raise RuntimeError("oracle: " + L.orc_last_error().decode())
+
+
+def _dp(a):
+    return a.ctypes.data_as(P(c_double))
+
+
+class OracleDMRG:
+    """Two-site DMRG on the CPU restatement (ts_optimize semantics)."""
+
+    def __init__(self, mpo_blob: bytes, L: int, nup: int, ndown: int, M: int, init_bond_dimension: int | None = None,
+                 cutoff: float = 1e-16, tol: float = 1e-10, maxiter: int = 8, ecore: float = 0.0):
+        self.lib = lib()
+        self.L = L
+        self._blob = ctypes.create_string_buffer(mpo_blob, len(mpo_blob))
+        h = c_void_p()
+        _check(self.lib, self.lib.orc_dmrg_create(self._blob, len(mpo_blob), nup, ndown, M,
+                                                  init_bond_dimension or M, cutoff, tol, maxiter, ecore,
+                                                  ctypes.byref(h)))
+        self.h = h
+
+    def sweep(self, sweep: int = 0):
+        n = 2 * self.L - 2
+        E, tw, tf = np.zeros(n), np.zeros(n), np.zeros(n)
+        bd = np.zeros(n, dtype=np.uint64)
+        _check(self.lib, self.lib.orc_dmrg_sweep(self.h, sweep, _dp(E), _dp(tw), _dp(tf),
+                                                 bd.ctypes.data_as(P(ctypes.c_uint64)), -1, None, None))
+        return E, tw, tf, bd
+
+    def snapshot(self, sweep: int, step: int) -> bytes:
+        """Run the sweep up to `step` and return the frozen site problem of that step."""
+        p, n = c_void_p(), c_size_t()
+        _check(self.lib, self.lib.orc_dmrg_sweep(self.h, sweep, None, None, None, None, step, ctypes.byref(p),
+                                                 ctypes.byref(n)))
+        b = ctypes.string_at(p, n.value)
+        self.lib.orc_free(p)
+        return b
+
+    def set_mmax(self, M: int):
+        self.lib.orc_dmrg_set_mmax(self.h, M)
+
+    def stats(self):
+        out = np.zeros(7)
+        self.lib.orc_dmrg_stats(self.h, _dp(out))
+        keys = ["hpsi_count", "hpsi_time", "hpsi_flops", "jd_time", "schedule_time", "trunc_time", "boundary_time"]
+        return dict(zip(keys, out.tolist()))
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            self.lib.orc_dmrg_free(self.h)
+            self.h = c_void_p()
+
+
+def heff_apply(snap: bytes, mpo_blob: bytes, site1: int, x: np.ndarray, repeat: int = 1):
+    """Oracle H_eff x on a frozen site problem; returns (y, flops_per_apply, seconds_per_apply)."""
+    L = lib()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.zeros_like(x)
+    fl, sec = c_double(), c_double()
+    sb = ctypes.create_string_buffer(snap, len(snap))
+    mb = ctypes.create_string_buffer(mpo_blob, len(mpo_blob))
+    _check(L, L.orc_heff_apply(sb, len(snap), mb, len(mpo_blob), site1, _dp(x), _dp(y), x.size, repeat,
+                               ctypes.byref(fl), ctypes.byref(sec)))
+    return y, fl.value, sec.value
+
+
+def schedule_export(snap: bytes, mpo_blob: bytes, site1: int):
+    L = lib()
+    p, n, fl = c_void_p(), c_size_t(), c_double()
+    sb = ctypes.create_string_buffer(snap, len(snap))
+    mb = ctypes.create_string_buffer(mpo_blob, len(mpo_blob))
+    _check(L, L.orc_schedule_export(sb, len(snap), mb, len(mpo_blob), site1, ctypes.byref(p), ctypes.byref(n),
+                                    ctypes.byref(fl)))
+    b = ctypes.string_at(p, n.value)
+    L.orc_free(p)
+    return b, fl.value
