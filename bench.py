@@ -1,0 +1,280 @@
+#!/usr/bin/env python
+"""Benchmark of the two-site DMRG effective-Hamiltonian hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--L 16] [--M 256] [--seed 0]
+
+A step is one H_eff . psi (the Davidson callback, super_hamil_mv) on a frozen
+two-site problem: the middle bond of a seeded synthetic ab-initio Hamiltonian
+(TwoU1, Sz = 0, N = L electrons) after one full two-site sweep at bond
+dimension M.  The frozen problem (twin MPS, left/right boundaries, two-site
+MPO) is produced on the host by the oracle sweep, then moved to HBM; only the
+H_eff apply is timed.
+
+`value` = reference work count (ScheduleNew::total_flops, solver/tasks.cpp:
+388-398, 777-796) x steps / device time (CUDA events, L2 flushed between
+steps), summed over ranks / max over ranks.  `e2e` is the same metric through
+qcm_heff_apply with pinned host buffers (H2D of psi and D2H of H.psi inside
+the timed region).  The path does not shard across GPUs here (one B200 per
+solve): N > 1 runs N independent replicas.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--L", type=int, default=16)
+    ap.add_argument("--M", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(a):
+    return (f"two-site H_eff.psi, synthetic ab-initio L={a.L} N={a.L} TwoU1 Sz=0 seed {a.seed}, "
+            f"M={a.M}, middle bond after one sweep")
+
+
+def frozen_problem(a):
+    from qcmaquis_b200.fcidump import synthetic_integrals
+    from qcmaquis_b200.mpo import MPO
+    from oracle.oracle import OracleDMRG
+    h, V, e = synthetic_integrals(a.L, a.seed)
+    m = MPO.qc(h, V)
+    blob = m.blob()
+    d = OracleDMRG(blob, a.L, a.L // 2, a.L // 2, a.M, init_bond_dimension=5)
+    d.sweep(0)
+    step = a.L // 2 - 1
+    snap = d.snapshot(1, step)
+    return m, blob, snap, step
+
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev):
+        self.dev = dev
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1])); mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if a.impl == "b200" else "gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return world, rank, local, pg
+
+
+def cpu_baseline(snap, blob, site, x, flops, budget_s=15.0):
+    from oracle.oracle import heff_apply, lib as olib
+    olib()
+    y, _, sec = heff_apply(snap, blob, site, x, repeat=1)
+    reps = max(1, min(50, int(budget_s / max(sec, 1e-3))))
+    _, _, sec = heff_apply(snap, blob, site, x, repeat=reps)
+    return {"value": flops / sec / 1e9, "unit": "GFLOP/s", "cores": olib().orc_max_threads(), "kind": "port",
+            "sample": f"{reps} H_eff.psi applies of the same frozen problem (oracle, OpenMP over ket sectors, "
+                      f"OpenBLAS dgemm), {sec * 1e3:.1f} ms each"}
+
+
+def run_reference(a, world, rank, pg):
+    if rank != 0:
+        return
+    from qcmaquis_b200.heff import parse_site_problem, twin_vector
+    from oracle.oracle import heff_apply, lib as olib
+    m, blob, snap, site = frozen_problem(a)
+    x = twin_vector(parse_site_problem(snap))
+    for _ in range(a.warmup):
+        _, flops, _ = heff_apply(snap, blob, site, x, repeat=1)
+    t0 = time.perf_counter()
+    _, flops, sec = heff_apply(snap, blob, site, x, repeat=a.steps)
+    wall = time.perf_counter() - t0
+    val = flops / sec / 1e9
+    cores = olib().orc_max_threads()
+    line = {"impl": "reference", "metric": "H_eff.psi GFLOP/s (FP64)", "value": val, "unit": "GFLOP/s",
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": sec * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "seed": a.seed},
+            "cpu_baseline": {"value": val, "unit": "GFLOP/s", "cores": cores, "kind": "port",
+                             "sample": f"{a.steps} H_eff.psi applies ({wall:.1f} s) with all host threads"},
+            "e2e": {"value": val, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(a, world, rank, local, pg):
+    import torch
+    from qcmaquis_b200 import heff
+    torch.cuda.set_device(local)
+    m, blob, snap, site = frozen_problem(a)
+    ts = m.twosite()
+    p = heff.parse_site_problem(snap)
+    ctx = heff.Context(local)
+    plan = heff.plan_from_problem(ctx, p, ts, site)
+    info = plan.info
+    x_host = heff.twin_vector(p)
+    n = plan.n
+    dev = torch.device("cuda", local)
+    xd = torch.from_numpy(x_host).to(dev)
+    yd = torch.empty_like(xd)
+    flush = torch.empty(int(256 * 2**20 // 4), dtype=torch.float32, device=dev)  # 256 MiB > L2 (126 MB)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    dmma_peak, dfma_peak = heff.probe_fp64_peaks()
+    torch.cuda.synchronize()
+    # warm-up (plan stream; the context stream is separate from torch's)
+    for _ in range(a.warmup):
+        plan.apply_device(xd.data_ptr(), yd.data_ptr())
+    ctx.synchronize()
+    prof = [plan.profile(xd.data_ptr(), yd.data_ptr()) for _ in range(3)]
+    # timed region: per-step CUDA events on the plan's stream via qcm_heff_profile
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    times, phases = [], []
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ms = plan.profile(xd.data_ptr(), yd.data_ptr())
+        times.append(ms[3])
+        phases.append(ms[:3])
+    torch.cuda.synchronize()
+    ck = clocks.stop()
+    total_ms = float(sum(times))
+    if pg is not None:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+        pg.barrier()
+    value = info["flops"] * a.steps * world / (total_ms * 1e-3) / 1e9
+    # e2e through the C-ABI with pinned host buffers
+    xh = torch.from_numpy(x_host).pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    import ctypes
+    from qcmaquis_b200._lib import lib, check, P, c_double
+    xp = ctypes.cast(xh.data_ptr(), P(c_double))
+    yp = ctypes.cast(yh.data_ptr(), P(c_double))
+    for _ in range(2):
+        check(lib.qcm_heff_apply(plan.h, xp, yp), "qcm_heff_apply")
+    e2e_t = []
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        check(lib.qcm_heff_apply(plan.h, xp, yp), "qcm_heff_apply")
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = float(sum(e2e_t))
+    if pg is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_val = info["flops"] * a.steps * world / e2e_s / 1e9
+    # correctness guard on the timed problem: device result vs the oracle
+    from oracle.oracle import heff_apply
+    y_ref, _, _ = heff_apply(snap, blob, site, x_host)
+    rel = float(np.abs(yh.numpy() - y_ref).max() / np.abs(y_ref).max())
+    # roofline of the dominant kernel
+    ph = np.mean(np.array(phases), axis=0)
+    names = ["k_tgemm", "k_gather", "k_lsgemm"]
+    dom = int(np.argmax(ph))
+    if dom == 1:
+        bytes_ = 8.0 * (info["g_reads"] + info["g_elems"])
+        ach = bytes_ / (ph[1] * 1e-3) / 1e9
+        roof = {"kernel": names[1], "bound": "hbm", "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                "frac": ach / hbm_peak, "traffic": None,
+                "algorithmic": "8 B x (T elements read per alpha + S elements written)",
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)"}
+    else:
+        fl = info["flops_t"] if dom == 0 else info["flops_ls"]
+        ach = fl / (ph[dom] * 1e-3) / 1e12
+        roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": dmma_peak, "unit": "TFLOP/s",
+                "frac": ach / dmma_peak, "traffic": None,
+                "algorithmic": "reference flop count of the phase (2 m n k)",
+                "peak_source": "FP64 DMMA probe qcm_probe_fp64_peaks (of measured)"}
+    roof["phase_ms"] = {k: float(v) for k, v in zip(names, ph)}
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(snap, blob, site, x_host, info["flops"])
+    if rank == 0:
+        line = {"metric": "H_eff.psi GFLOP/s (FP64 plain form)", "value": value, "unit": "GFLOP/s", "n_gpus": world,
+                "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "seed": a.seed, "vec_len": n,
+                           "flops_per_step": info["flops"], "l2": "flushed between steps (256 MiB write)",
+                           "parallelism": f"replicas x{world}"},
+                "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+                "gpu_launches": 3 * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
+                "fp64_peaks_tflops": {"dmma": dmma_peak, "dfma": dfma_peak},
+                "max_rel_err_vs_oracle": rel}
+        print(json.dumps(line), flush=True)
+    del plan
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+def main():
+    a = parse()
+    world, rank, local, pg = dist_setup(a)
+    if a.impl == "reference":
+        run_reference(a, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    run_b200(a, world, rank, local, pg)
+
+
+if __name__ == "__main__":
+    main()

@@ -57,6 +57,107 @@ int qcm_mpo_serialize(const qcm_mpo* m, void* buf, size_t cap, size_t* len);
 int qcm_mpo_deserialize(const void* buf, size_t len, qcm_mpo** out);
 void qcm_mpo_free(qcm_mpo* m);
 
+/* ------------------------------------------------------------------------ */
+/* Context, resident boundaries, H_eff plan                                   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct qcm_ctx qcm_ctx;
+typedef struct qcm_boundary qcm_boundary;
+typedef struct qcm_heff qcm_heff;
+
+/* One charge sector of an Index: TwoU1 charge (a, b) = (N_up, N_down) and size.
+ * Sector lists are in strictly descending lexicographic charge order, as the
+ * reference's sorted Index (block_matrix/indexing_stable.hpp:97-300). */
+typedef struct {
+    int32_t a, b;
+    uint32_t size;
+} qcm_sector;
+
+/* Boundary (environment) tensor: the reference's Boundary + BoundaryIndex
+ * (mp_tensors/boundary.h:76-406).  Cohort ci couples bra sector cohort_bra[ci]
+ * and ket sector cohort_ket[ci]; it holds n_blocks[ci] column-major blocks of
+ * size(bra) x size(ket); offsets[ci*aux_dim + b] is the element offset of MPO
+ * index b inside the cohort (-1 = absent), cscale the conjugate scale, tr[ci]
+ * = 1 if the cohort is stored as its Hermitian partner's transpose.
+ * n_blocks may be NULL (then counted from offsets; 0 for tr cohorts).
+ * data + data_offset[ci] holds the cohort's values (host memory). */
+typedef struct {
+    uint32_t n_bra, n_ket;
+    const qcm_sector* bra;
+    const qcm_sector* ket;
+    uint32_t n_cohorts, aux_dim;
+    const uint32_t* cohort_bra;
+    const uint32_t* cohort_ket;
+    const uint8_t* tr;
+    const uint32_t* n_blocks;
+    const int64_t* offsets;
+    const double* cscale;
+    const uint64_t* data_offset;
+    const double* data;
+} qcm_boundary_desc;
+
+/* Indices of the right-paired two-site tensor (twin MPS, twositetensor.hpp:131-150). */
+typedef struct {
+    uint32_t n_phys, n_left, n_right;
+    const qcm_sector* phys;
+    const qcm_sector* left;
+    const qcm_sector* right;
+} qcm_mps_desc;
+
+typedef struct {
+    uint64_t vec_len, t_len, s_len;
+    uint64_t n_tjobs, n_ttiles, n_gtasks, n_alpha, n_segs, n_outs, n_otiles;
+    double flops, flops_t, flops_ls, flops_s; /* ScheduleNew::total_flops per H.psi (solver/tasks.cpp:388-398, 777-796) */
+    uint64_t g_elems, g_reads;                /* S elements written / T elements read by the gather */
+    uint64_t l_len, r_len;                    /* boundary elements resident in HBM */
+} qcm_heff_info;
+
+#define QCM_PLAN_BOOKKEEPING 1 /* keep the (cohort, unit, line, alpha) list for parity checks */
+#define QCM_PLAN_HOST_ONLY 2   /* build the schedule on the host only (ctx may be NULL; no apply) */
+
+/* Context on one CUDA device with its own stream.  Replaces accelerator::gpu
+ * setup (solver/accelerator.cpp:52-330); QCM_ERR_NODEV without a GPU. */
+int qcm_ctx_create(int device, qcm_ctx** out);
+void qcm_ctx_destroy(qcm_ctx* ctx);
+int qcm_ctx_synchronize(qcm_ctx* ctx);
+
+/* Copy a boundary into HBM (resident).  Replaces storage::gpu::broadcast::fetch
+ * of Boundary cohorts (utils/storage.h:441-519, 594-615). */
+int qcm_boundary_upload(qcm_ctx* ctx, const qcm_boundary_desc* desc, qcm_boundary** out);
+/* Index-only boundary (no device data) for host-only schedule construction. */
+int qcm_boundary_index_create(const qcm_boundary_desc* desc, qcm_boundary** out);
+void qcm_boundary_free(qcm_boundary* b);
+
+/* Build the flattened contraction schedule of H_eff for the two-site tensor
+ * `twin` between L and R with two-site MPO tensor ts_mpo[site] and stage it in
+ * HBM.  Replaces create_contraction_schedule + ScheduleNew::stage_gpu
+ * (contractions/create_schedule/site_hamil_schedule.hpp:42-93,
+ * solver/tasks.cpp:918-977). */
+int qcm_heff_plan_create(qcm_ctx* ctx, const qcm_boundary* L, const qcm_boundary* R, const qcm_mpo* ts_mpo, int site,
+                         const qcm_mps_desc* twin, int flags, qcm_heff** out);
+int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info);
+
+/* y = H_eff x.  x, y: host buffers of vec_len doubles, the twin's right-paired
+ * blocks (ls x stripe, column-major) concatenated in left-sector order;
+ * synchronous.  Replaces ietl::mult -> super_hamil_mv
+ * (solver/ietl_interface_dv.h:112-118, solver/super_hamil_mv.hpp:100-155). */
+int qcm_heff_apply(qcm_heff* h, const double* x, double* y);
+/* Same with device pointers, enqueued on the context stream (asynchronous). */
+int qcm_heff_apply_device(qcm_heff* h, const double* x_dev, double* y_dev);
+
+/* Bookkeeping rows (parity checks; plan built with QCM_PLAN_BOOKKEEPING):
+ * ints[10*i..] = (lb_in, lb_out, ci, ci_eff, unit_offset, ms, b1_row,
+ * mps_offset, ci_right, column), alpha[i].  Call with ints == NULL for *n. */
+int qcm_heff_bookkeeping(const qcm_heff* h, uint32_t* ints, double* alpha, uint64_t cap, uint64_t* n);
+/* One device apply with CUDA events between the phases, synchronous:
+ * ms[0] T-GEMM, ms[1] S gather, ms[2] L.S GEMM, ms[3] whole H.psi. */
+int qcm_heff_profile(qcm_heff* h, const double* x_dev, double* y_dev, float* ms);
+void qcm_heff_free(qcm_heff* h);
+
+/* FP64 throughput probes on the current device (TFLOP/s): DMMA (mma.sync
+ * m8n8k4 .f64) and DFMA loops.  Roofline denominators of the FP64 form. */
+int qcm_probe_fp64_peaks(double* dmma_tflops, double* dfma_tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,8 @@
 #include "dmrg.hpp"
 
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 namespace orc {
@@ -164,7 +166,8 @@ void TwoSite::set_from_mps(const MPSTensor& tw) {
                 if (r == right.size()) continue;
                 Q c = lc + p1;
                 std::size_t bb = both.find(c, c);
-                if (bb == both.n_blocks()) continue;
+                if (bb == both.n_blocks())  // ts_reshape.h: the both-paired block is created when missing
+                    bb = both.insert(c, c, Mat(in_left.size(c), in_right.size(c)));
                 Mat& dst = both.b[bb];
                 std::size_t ldim = left[l].second, rdim = right[r].second, sd1 = phys1[s1].second, sd2 = phys2[s2].second;
                 std::size_t ilo = in_left(p1, lc), iro = in_right(p2, rc), oro = out_right(p1 + p2, rc), opo = ppb(p1, p2);
@@ -204,7 +207,7 @@ TruncationResults svd_truncate(const BlockMatrix& M, BlockMatrix& U, BlockMatrix
     tr.truncated_weight = tw / sum2;
     for (std::size_t k = 0; k < nb; ++k) {
         std::size_t keep = std::find_if(S[k].begin(), S[k].end(), [&](double x) { return x < evalscut; }) - S[k].begin();
-        if (keep == 0) continue;
+        if (keep == 0) { S[k].clear(); continue; }
         Mat u(Ub[k].r, keep), v(keep, Vb[k].c);
         for (std::size_t j = 0; j < keep; ++j)
             for (std::size_t i = 0; i < Ub[k].r; ++i) u(i, j) = Ub[k](i, j);
@@ -473,13 +476,21 @@ void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<Trunca
         for (std::size_t k = 0; k < twin.data.n_blocks(); ++k)
             std::copy(xo.begin() + off[k], xo.begin() + off[k] + twin.data.b[k].d.size(), twin.data.b[k].d.begin());
         tst.set_from_mps(twin);
+        static const bool dbg = std::getenv("ORC_DEBUG") != nullptr;
+        if (dbg) {
+            double nt = 0; for (auto& b : twin.data.b) for (double v : b.d) nt += v * v;
+            std::fprintf(stderr, "step %d: |twin|^2=%.12f |both|^2=%.12f\n", _site, nt, tst.both.norm2());
+        }
         energies.push_back(E + p.ecore);
         TruncationResults tr;
         double t2 = now_s();
         if (lr == 1) {
             tst.split_l2r(p.Mmax, p.cutoff, mps[site1], mps[site2], tr);
+            if (dbg) std::fprintf(stderr, "   split: |U|^2=%.12f |SV|^2=%.12f tw=%.3e\n", mps[site1].data.norm2(), mps[site2].data.norm2(), tr.truncated_weight);
             BlockMatrix t = normalize_left(mps[site2]);
+            if (dbg) std::fprintf(stderr, "   qr: |Q|^2=%.12f |R|^2=%.12f\n", mps[site2].data.norm2(), t.norm2());
             if (site2 < L - 1) multiply_from_left(mps[site2 + 1], t);
+            if (dbg && site2 < L - 1) std::fprintf(stderr, "   next: |RB|^2=%.12f\n", mps[site2 + 1].data.norm2());
             double t3 = now_s();
             trunc_time += t3 - t2;
             left_[site2] = overlap_mpo_left_step(mps[site1], mps[site1], left_[site1], mpo[site1], true);

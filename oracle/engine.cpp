@@ -101,6 +101,21 @@ std::vector<double> Cohort::create_s_r(const TList& T) const {
     return ret;
 }
 
+std::vector<double> Cohort::contract_buf(const std::vector<const double*>& left, const TList& T) const {
+    std::vector<double> sloc = create_s_r(T);
+    int M = int(rs), N = int(stripe), K = int(nSrows * ls);
+    const double* luse = left[ci_eff];
+    std::vector<double> lbuf;
+    if (ci != ci_eff) {
+        lbuf.resize(std::size_t(M) * K);
+        tr_tile_v(ls, rs, nSrows, left[ci_eff], lbuf.data());
+        luse = lbuf.data();
+    }
+    std::vector<double> buf(std::size_t(M) * N);
+    dgemm('N', 'N', M, N, K, 1.0, luse, M, sloc.data(), K, 0.0, buf.data(), M);
+    return buf;
+}
+
 void Cohort::contract(const std::vector<const double*>& left, const TList& T, double* out, std::mutex& mu) const {
     std::vector<double> sloc = create_s_r(T);
     int M = int(rs), N = int(stripe), K = int(nSrows * ls);
@@ -474,15 +489,29 @@ std::unique_ptr<Schedule> create_contraction_schedule(MPSTensor& initial, const 
 
 void super_hamil_mv(const Schedule& sched, const Boundary& left, const Boundary& right,
                     const std::vector<const double*>& x, const std::vector<double*>& y) {
+    // Cohort products are formed in parallel over ket blocks as in super_hamil_mv.hpp:121-132,
+    // then added to each output block in a fixed (lb_in, cohort) order, so the result does
+    // not depend on the thread count (the reference's mutex-ordered axpy does).
     std::vector<const double*> lv = boundary_view(left), rv = boundary_view(right);
-    std::vector<std::mutex> mutexes(sched.blocks.size());
+    const std::size_t nb = sched.blocks.size();
+    std::vector<std::vector<std::vector<double>>> part(nb);
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int b = 0; b < int(sched.blocks.size()); ++b) {
+    for (int b = 0; b < int(nb); ++b) {
         const MPSBlock& blk = sched.blocks[b];
         if (blk.data.empty()) continue;
         TList T = blk.create_T(rv, x);
-        for (const Cohort& c : blk.data) c.contract(lv, T, y[c.rb], mutexes[c.rb]);
+        part[b].resize(blk.data.size());
+        for (std::size_t c = 0; c < blk.data.size(); ++c) part[b][c] = blk.data[c].contract_buf(lv, T);
     }
+    std::vector<std::vector<std::pair<std::size_t, std::size_t>>> by_out(nb);
+    for (std::size_t b = 0; b < nb; ++b)
+        for (std::size_t c = 0; c < sched.blocks[b].data.size(); ++c) by_out[sched.blocks[b].data[c].rb].push_back({b, c});
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int o = 0; o < int(nb); ++o)
+        for (auto& bc : by_out[o]) {
+            const std::vector<double>& buf = part[bc.first][bc.second];
+            daxpy(buf.size(), 1.0, buf.data(), y[o]);
+        }
 }
 
 Boundary overlap_mpo_left_step(const MPSTensor& bra_in, const MPSTensor& ket_in, const Boundary& left, const MPOTensor& mpo,

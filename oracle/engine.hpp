@@ -49,6 +49,7 @@ struct Cohort {
     std::vector<double> create_s(const TList& T) const;    // tasks.cpp:425-454
     std::vector<double> create_s_r(const TList& T) const;  // tasks.cpp:466-494
     void contract(const std::vector<const double*>& left, const TList& T, double* out, std::mutex& mu) const;  // :286-313
+    std::vector<double> contract_buf(const std::vector<const double*>& left, const TList& T) const;     // same, no accumulation
     void prop_l(const double* bra, const TList& T, double* new_left) const;   // :198-209
     void prop_r(const double* bra, const TList& T, double* new_right) const;  // :243-260
     void lbtm(const TList& T, double* out, double alpha) const;               // :346-362

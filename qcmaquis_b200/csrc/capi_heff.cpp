@@ -1,0 +1,234 @@
+// C-ABI: context, resident boundaries and the H_eff plan / apply (the H.psi callback).
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../../include/qcm_b200.h"
+#include "capi_util.hpp"
+#include "device.hpp"
+#include "heff.hpp"
+
+namespace qcm {
+const MPO& mpo_of(const qcm_mpo* m);
+}
+
+struct qcm_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+};
+
+struct qcm_boundary {
+    qcm_ctx* ctx;
+    qcm::DevBoundary b;
+};
+
+struct qcm_heff {
+    qcm_ctx* ctx;
+    std::unique_ptr<qcm::HeffPlan> p;
+};
+
+namespace {
+qcm::Index to_index(uint32_t n, const qcm_sector* s) {
+    qcm::Index r;
+    for (uint32_t i = 0; i < n; ++i) r.d.push_back({qcm::Charge(s[i].a, s[i].b), s[i].size});
+    for (std::size_t i = 1; i < r.d.size(); ++i)
+        if (!(r.d[i - 1].first > r.d[i].first)) throw std::runtime_error("sector list must be in strictly descending charge order");
+    return r;
+}
+}  // namespace
+
+extern "C" {
+
+int qcm_ctx_create(int device, qcm_ctx** out) {
+    QCM_TRY
+    if (!out) return qcm::fail(QCM_ERR_ARG, "qcm_ctx_create: out is NULL");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return qcm::fail(QCM_ERR_NODEV, "no CUDA device (no CPU fallback)");
+    if (device < 0 || device >= n) return qcm::fail(QCM_ERR_ARG, "qcm_ctx_create: bad device index");
+    QCM_CUDA(cudaSetDevice(device));
+    auto* c = new qcm_ctx;
+    c->device = device;
+    QCM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    *out = c;
+    return QCM_OK;
+    QCM_CATCH
+}
+
+void qcm_ctx_destroy(qcm_ctx* c) {
+    if (!c) return;
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int qcm_ctx_synchronize(qcm_ctx* c) {
+    QCM_TRY
+    QCM_CUDA(cudaStreamSynchronize(c->stream));
+    return QCM_OK;
+    QCM_CATCH
+}
+
+}  // extern "C"
+
+namespace {
+int boundary_make(qcm_ctx* ctx, const qcm_boundary_desc* d, qcm_boundary** out) {
+    QCM_TRY
+    if (!d || !out) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_upload: NULL argument");
+    if (ctx) QCM_CUDA(cudaSetDevice(ctx->device));
+    auto b = std::make_unique<qcm_boundary>();
+    b->ctx = ctx;
+    qcm::BoundaryIndexH& x = b->b.idx;
+    x.bra = to_index(d->n_bra, d->bra);
+    x.ket = to_index(d->n_ket, d->ket);
+    x.aux = d->aux_dim;
+    const uint32_t nc = d->n_cohorts;
+    x.cbra.assign(d->cohort_bra, d->cohort_bra + nc);
+    x.cket.assign(d->cohort_ket, d->cohort_ket + nc);
+    x.tr.assign(d->tr, d->tr + nc);
+    x.offsets.assign(d->offsets, d->offsets + std::size_t(nc) * d->aux_dim);
+    x.cscale.assign(d->cscale, d->cscale + std::size_t(nc) * d->aux_dim);
+    x.lsz.resize(nc); x.rsz.resize(nc); x.nb.resize(nc);
+    for (uint32_t ci = 0; ci < nc; ++ci) {
+        if (x.cbra[ci] >= x.bra.size() || x.cket[ci] >= x.ket.size())
+            return qcm::fail(QCM_ERR_ARG, "qcm_boundary_upload: cohort sector out of range");
+        x.lsz[ci] = uint32_t(x.bra[x.cbra[ci]].second);
+        x.rsz[ci] = uint32_t(x.ket[x.cket[ci]].second);
+        if (d->n_blocks) x.nb[ci] = d->n_blocks[ci];
+        else {
+            uint32_t n = 0;
+            for (uint32_t k = 0; k < d->aux_dim; ++k) n += x.offsets[std::size_t(ci) * d->aux_dim + k] > -1;
+            x.nb[ci] = x.tr[ci] ? 0 : n;
+        }
+    }
+    x.finish();
+    if (!ctx) {
+        *out = b.release();
+        return QCM_OK;
+    }
+    b->b.data.alloc(x.total ? x.total : 1);
+    QCM_CUDA(cudaMemsetAsync(b->b.data.get(), 0, (x.total ? x.total : 1) * sizeof(double), ctx->stream));
+    if (d->data) {
+        for (uint32_t ci = 0; ci < nc; ++ci) {
+            uint64_t n = x.cohort_size(ci);
+            if (n)
+                QCM_CUDA(cudaMemcpyAsync(b->b.data.get() + x.data_off[ci], d->data + d->data_offset[ci], n * sizeof(double),
+                                         cudaMemcpyHostToDevice, ctx->stream));
+        }
+    }
+    QCM_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = b.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+}  // namespace
+
+extern "C" {
+
+int qcm_boundary_upload(qcm_ctx* ctx, const qcm_boundary_desc* d, qcm_boundary** out) {
+    if (!ctx) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_upload: ctx is NULL");
+    return boundary_make(ctx, d, out);
+}
+
+int qcm_boundary_index_create(const qcm_boundary_desc* d, qcm_boundary** out) { return boundary_make(nullptr, d, out); }
+
+void qcm_boundary_free(qcm_boundary* b) { delete b; }
+
+int qcm_heff_plan_create(qcm_ctx* ctx, const qcm_boundary* L, const qcm_boundary* R, const qcm_mpo* ts_mpo, int site,
+                         const qcm_mps_desc* twin, int flags, qcm_heff** out) {
+    QCM_TRY
+    const bool host_only = (flags & QCM_PLAN_HOST_ONLY) != 0;
+    if ((!ctx && !host_only) || !L || !R || !ts_mpo || !twin || !out)
+        return qcm::fail(QCM_ERR_ARG, "qcm_heff_plan_create: NULL argument");
+    if (!host_only && (!L->ctx || !R->ctx)) return qcm::fail(QCM_ERR_ARG, "qcm_heff_plan_create: boundaries are not resident");
+    const qcm::MPO& m = qcm::mpo_of(ts_mpo);
+    if (!m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_heff_plan_create: expected a two-site MPO");
+    if (site < 0 || std::size_t(site) >= m.t.size()) return qcm::fail(QCM_ERR_ARG, "qcm_heff_plan_create: site out of range");
+    if (!host_only) QCM_CUDA(cudaSetDevice(ctx->device));
+    auto h = std::make_unique<qcm_heff>();
+    h->ctx = ctx;
+    h->p = qcm::build_heff_plan(L->b, R->b, m.t[site], to_index(twin->n_phys, twin->phys), to_index(twin->n_left, twin->left),
+                                to_index(twin->n_right, twin->right), (flags & QCM_PLAN_BOOKKEEPING) != 0);
+    if (!host_only) {
+        h->p->stream = ctx->stream;
+        qcm::upload_plan(*h->p);
+    }
+    *out = h.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info) {
+    if (!h || !info) return qcm::fail(QCM_ERR_ARG, "qcm_heff_get_info: NULL argument");
+    const qcm::HeffPlan& p = *h->p;
+    info->vec_len = p.x_len;
+    info->t_len = p.t_len;
+    info->s_len = p.s_len;
+    info->n_tjobs = p.tjobs.size();
+    info->n_ttiles = p.ttiles.size();
+    info->n_gtasks = p.gtasks.size();
+    info->n_alpha = p.alpha.size();
+    info->n_segs = p.segs.size();
+    info->n_outs = p.outs.size();
+    info->n_otiles = p.otiles.size();
+    info->flops = p.flops;
+    info->flops_t = p.flops_t;
+    info->flops_ls = p.flops_ls;
+    info->flops_s = p.flops_s;
+    info->g_elems = p.g_elems;
+    info->g_reads = p.g_reads;
+    info->l_len = p.L ? p.L->idx.total : 0;
+    info->r_len = p.R ? p.R->idx.total : 0;
+    return QCM_OK;
+}
+
+int qcm_heff_apply_device(qcm_heff* h, const double* x_dev, double* y_dev) {
+    QCM_TRY
+    if (!h || !x_dev || !y_dev) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device: NULL argument");
+    if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device: host-only plan");
+    qcm::heff_apply_device(*h->p, x_dev, y_dev);
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_heff_apply(qcm_heff* h, const double* x, double* y) {
+    QCM_TRY
+    if (!h || !x || !y) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply: NULL argument");
+    if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply: host-only plan");
+    qcm::HeffPlan& p = *h->p;
+    if (p.d_x.size() < p.x_len) { p.d_x.alloc(p.x_len); p.d_y.alloc(p.x_len); }
+    QCM_CUDA(cudaMemcpyAsync(p.d_x.get(), x, p.x_len * sizeof(double), cudaMemcpyHostToDevice, p.stream));
+    qcm::heff_apply_device(p, p.d_x.get(), p.d_y.get());
+    QCM_CUDA(cudaMemcpyAsync(y, p.d_y.get(), p.x_len * sizeof(double), cudaMemcpyDeviceToHost, p.stream));
+    QCM_CUDA(cudaStreamSynchronize(p.stream));
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_heff_bookkeeping(const qcm_heff* h, uint32_t* ints, double* alpha, uint64_t cap, uint64_t* n) {
+    if (!h || !n) return qcm::fail(QCM_ERR_ARG, "qcm_heff_bookkeeping: NULL argument");
+    const qcm::HeffPlan& p = *h->p;
+    *n = p.bk_alpha.size();
+    if (ints && alpha) {
+        if (cap < *n) return qcm::fail(QCM_ERR_ARG, "qcm_heff_bookkeeping: buffer too small");
+        std::memcpy(ints, p.bk_int.data(), p.bk_int.size() * sizeof(uint32_t));
+        std::memcpy(alpha, p.bk_alpha.data(), p.bk_alpha.size() * sizeof(double));
+    }
+    return QCM_OK;
+}
+
+int qcm_heff_profile(qcm_heff* h, const double* x_dev, double* y_dev, float* ms) {
+    QCM_TRY
+    if (!h || !h->ctx || !x_dev || !y_dev || !ms) return qcm::fail(QCM_ERR_ARG, "qcm_heff_profile: bad argument");
+    cudaEvent_t ev[4];
+    for (auto& e : ev) QCM_CUDA(cudaEventCreate(&e));
+    qcm::heff_apply_device(*h->p, x_dev, y_dev, ev);
+    QCM_CUDA(cudaEventSynchronize(ev[3]));
+    for (int i = 0; i < 3; ++i) QCM_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+    QCM_CUDA(cudaEventElapsedTime(&ms[3], ev[0], ev[3]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    return QCM_OK;
+    QCM_CATCH
+}
+
+void qcm_heff_free(qcm_heff* h) { delete h; }
+
+}  // extern "C"
