@@ -106,10 +106,13 @@ typedef struct {
 
 typedef struct {
     uint64_t vec_len, t_len, s_len;
-    uint64_t n_tjobs, n_ttiles, n_gtasks, n_alpha, n_segs, n_outs, n_otiles;
+    uint64_t n_tjobs, n_ttiles, n_gtasks /* S-build units */, n_alpha, n_segs, n_outs, n_otiles;
     double flops, flops_t, flops_ls, flops_s; /* ScheduleNew::total_flops per H.psi (solver/tasks.cpp:388-398, 777-796) */
     uint64_t g_elems, g_reads;                /* S elements written / T elements read by the gather */
     uint64_t l_len, r_len;                    /* boundary elements resident in HBM */
+    uint64_t n_kitems;                        /* split-K items of the L.S GEMM */
+    double flops_sdense;                      /* tensor-core work of the S build (dense unit GEMMs) */
+    uint64_t launches;                        /* own kernels launched per apply */
 } qcm_heff_info;
 
 #define QCM_PLAN_BOOKKEEPING 1 /* keep the (cohort, unit, line, alpha) list for parity checks */

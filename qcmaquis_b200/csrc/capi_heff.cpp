@@ -163,18 +163,21 @@ int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info) {
     info->t_len = p.t_len;
     info->s_len = p.s_len;
     info->n_tjobs = p.tjobs.size();
-    info->n_ttiles = p.ttiles.size();
-    info->n_gtasks = p.gtasks.size();
-    info->n_alpha = p.alpha.size();
+    info->n_ttiles = p.ttiles[0].size() + p.ttiles[1].size() + p.ttiles[2].size();
+    info->n_gtasks = p.units.size();
+    info->n_alpha = p.went.size();
     info->n_segs = p.segs.size();
     info->n_outs = p.outs.size();
-    info->n_otiles = p.otiles.size();
+    info->n_otiles = p.otiles[0].size() + p.otiles[1].size() + p.otiles[2].size();
+    info->n_kitems = p.kitems[0].size() + p.kitems[1].size() + p.kitems[2].size();
+    info->launches = uint64_t(qcm::heff_launches_per_apply(p));
     info->flops = p.flops;
     info->flops_t = p.flops_t;
     info->flops_ls = p.flops_ls;
     info->flops_s = p.flops_s;
     info->g_elems = p.g_elems;
     info->g_reads = p.g_reads;
+    info->flops_sdense = p.flops_sdense;
     info->l_len = p.L ? p.L->idx.total : 0;
     info->r_len = p.R ? p.R->idx.total : 0;
     return QCM_OK;

@@ -64,9 +64,20 @@ struct TJobD {        // T[c_off] (M x N) = psi[a_off] (M x K, lda) * Rop (K x N
     uint64_t a_off, b_off, c_off;
     uint32_t M, K, N, lda, brs, tr;  // Rop(k, n) = R[b_off + (n/brs)*K*brs + (tr ? n%brs + k*brs : k + (n%brs)*K)]
 };
-struct GTaskD {       // S[s_off + r + c*ldS] (r < rows, c < cols) = sum_a alpha[a] * T[toff[a] + r + c*rows]
-    uint64_t s_off;
-    uint32_t ldS, rows, cols, a_start, a_count, pad;
+struct UnitD {        // S rows of one cohort unit: S_u (lines x elements) = W_u (lines x slices) * slices
+    uint64_t s_off;   // S offset of (row 0, first column of the unit) in the cohort's S (ld = ldS)
+    uint32_t ldS;     // nS * ls_in of the cohort
+    uint32_t ls;      // rows of a slice = ls_in; element e of a slice is (r, c) = (e % ls, e / ls)
+    uint32_t ne;      // elements per slice = ls_in * ms
+    uint32_t nl;      // lines (L block rows with coefficients)
+    uint32_t line0;   // first entry in line_b1[]
+    uint32_t nk;      // distinct T slices referenced
+    uint32_t slice0;  // first entry in slice_off[]
+    uint32_t sptr0;   // first of nk + 1 entry pointers in sptr[]
+};
+struct WEntD {        // coefficient alpha at (line, slice) of a unit; entries sorted by slice
+    uint32_t line, k;
+    double a;
 };
 struct SegD {         // K segment of an output block: L cohort (M x nS*ls_in, maybe tile-transposed) times S (ldS = nS*ls_in)
     uint64_t l_off, s_off;
@@ -77,6 +88,18 @@ struct OutD {
     uint32_t M, N, seg_start, seg_count;
 };
 struct TileD { uint32_t item, m0, n0, pad; };
+struct KItemD {       // split-K work item of the L.S GEMM: output tile, one segment, K range
+    uint32_t tile, seg, k0, k1;
+};
+struct OTileD {       // output tile of the L.S GEMM and its contiguous range of split-K partials
+    uint32_t out, m0, n0, part0, nparts, pad0, pad1, pad2;
+};
+
+// DMMA tile shapes (rows x cols of the CTA tile); the class is chosen per job from its row count
+enum { SHAPE_16 = 0, SHAPE_32 = 1, SHAPE_64 = 2, N_SHAPES = 3 };
+inline int shape_for_rows(uint32_t M) { return M <= 16 ? SHAPE_16 : (M <= 32 ? SHAPE_32 : SHAPE_64); }
+inline uint32_t shape_bm(int s) { return s == SHAPE_16 ? 16 : (s == SHAPE_32 ? 32 : 64); }
+inline uint32_t shape_bn(int s) { return s == SHAPE_64 ? 64 : 128; }
 
 struct HeffPlan {
     Index phys, left, right;
@@ -85,32 +108,43 @@ struct HeffPlan {
     uint64_t x_len = 0;
 
     std::vector<TJobD> tjobs;
-    std::vector<TileD> ttiles;
+    std::vector<TileD> ttiles[N_SHAPES];
     uint64_t t_len = 0;
 
-    std::vector<GTaskD> gtasks;
-    std::vector<double> alpha;
-    std::vector<uint64_t> aoff;
+    std::vector<UnitD> units;
+    std::vector<TileD> utiles[N_SHAPES];   // (unit, line tile m0, element tile n0)
+    std::vector<uint32_t> line_b1, sptr;
+    std::vector<uint64_t> slice_off;
+    std::vector<WEntD> went;
     uint64_t s_len = 0;
 
     std::vector<SegD> segs;
     std::vector<OutD> outs;
-    std::vector<TileD> otiles;
+    std::vector<OTileD> otiles[N_SHAPES];
+    std::vector<KItemD> kitems[N_SHAPES];
+    uint64_t p_len = 0;  // split-K partial tiles (doubles)
 
     // reference work count ScheduleNew::total_flops (tasks.cpp:388-398, 777-796)
     double flops = 0, flops_t = 0, flops_ls = 0, flops_s = 0;
-    // gather volume: S elements written, T elements read (one per alpha per element)
+    // S build volume: S elements written, T elements read (one per alpha per element),
+    // dense tensor-core work of the unit GEMMs (2 * lines * slices * elements)
     uint64_t g_elems = 0, g_reads = 0;
+    double flops_sdense = 0;
     // bookkeeping export rows: (lb_in, lb_out, ci, ci_eff, unit offset, ms, b1, mps_offset, ci_right, col) + alpha
     std::vector<uint32_t> bk_int;
     std::vector<double> bk_alpha;
 
     // device copies
     DBuf<TJobD> d_tjobs;
-    DBuf<TileD> d_ttiles, d_otiles;
-    DBuf<GTaskD> d_gtasks;
-    DBuf<double> d_alpha;
-    DBuf<uint64_t> d_aoff;
+    DBuf<TileD> d_ttiles[N_SHAPES];
+    DBuf<OTileD> d_otiles[N_SHAPES];
+    DBuf<KItemD> d_kitems[N_SHAPES];
+    DBuf<double> d_P;
+    DBuf<UnitD> d_units;
+    DBuf<TileD> d_utiles[N_SHAPES];
+    DBuf<uint32_t> d_line_b1, d_sptr;
+    DBuf<uint64_t> d_slice_off;
+    DBuf<WEntD> d_went;
     DBuf<SegD> d_segs;
     DBuf<OutD> d_outs;
     DBuf<double> d_T, d_S;
@@ -133,5 +167,6 @@ void upload_plan(HeffPlan& p);
 // ev (optional, 4 events) is recorded before the T-GEMM, after it, after the S
 // gather and after the L.S GEMM.
 void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev = nullptr);
+int heff_launches_per_apply(const HeffPlan& p);
 
 }  // namespace qcm

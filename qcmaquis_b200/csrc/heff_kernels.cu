@@ -1,16 +1,21 @@
 // FP64 H_eff kernels for sm_100a.
 //
-// tcgen05.mma has no f64 kind, so the plain (FP64) form runs its sector GEMMs on
-// the double-precision tensor path: mma.sync.aligned.m8n8k4 .f64 (DMMA).
-// One CTA = 64 x 64 output tile, 4 warps each owning a 32 x 32 warp tile
-// (4 x 4 DMMA fragments), K staged through shared memory 16 deep.
+// tcgen05.mma has no f64 kind, so the plain (FP64) form runs every contraction
+// on the double-precision tensor path, mma.sync.aligned.m8n8k4 .f64 (DMMA).  A
+// CTA of 4 warps owns a BM x BN tile (16x128, 32x128 or 64x64, picked from the
+// row count so short sectors do not waste rows).  K is staged 16 deep through a
+// two-stage cp.async pipeline (the operands are gathered through per-column /
+// per-row base tables, so bulk tensor copies do not apply).
 //
-//   k_tgemm : T[ti] = psi_slab * R[ci_eff] (per-block transposed when the R
-//             cohort is stored as its Hermitian partner)      (tasks.cpp:707-752)
-//   k_gather: S = sum alpha * T slices                        (gpu_dgemm_ddot.cu:282-359)
-//   k_lsgemm: y[lb_out] = sum over cohorts L[ci_eff] * S, one K loop over all
-//             cohorts of the output block -> deterministic, no atomics
-//                                                             (tasks.cpp:315-344 + atomic_add)
+//   k_tgemm   : T[ti] = psi_slab * R[ci_eff] (per-block transposed when the R
+//               cohort is stored as its Hermitian partner)         (tasks.cpp:707-752)
+//   k_sgemm   : S rows of a cohort unit = W_u (lines x slices, the sparse MPO
+//               coefficients densified tile by tile in shared memory) * T slices.
+//               Replaces the alpha-weighted gather (gpu_dgemm_ddot.cu:282-359,
+//               tasks.cpp:466-494) by a tensor-core GEMM.
+//   k_lspart  : split-K partial tiles of y[lb_out] = sum_cohorts L[ci_eff] * S
+//   k_lsreduce: partials of each output tile summed in a fixed order -> y
+//               (deterministic; replaces cublasDgemm + atomic_add, tasks.cpp:315-344)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -20,7 +25,7 @@
 namespace qcm {
 namespace {
 
-constexpr int BM = 64, BN = 64, BK = 16, PAD = 4, NTHR = 128;
+constexpr int BK = 16, PAD = 4, NTHR = 128;
 
 __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -28,188 +33,308 @@ __device__ __forceinline__ void dmma(double (&c)[2], double a, double b) {
                  : "d"(a), "d"(b));
 }
 
-// Shared-memory tile pair and the warp-level DMMA product over one BK chunk.
-struct Tiles {
-    double A[BK][BM + PAD];
-    double B[BK][BN + PAD];
+// 8-byte asynchronous global->shared copy; a false predicate writes zeros (src-size 0)
+__device__ __forceinline__ void cp8(double* smem, const double* gmem, bool pred) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(pred ? 8 : 0));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// CTA tile = WM x WN warps, each warp FM x FN DMMA fragments of 8 x 8.
+template <int WM_, int WN_, int FM_, int FN_>
+struct Shape {
+    static constexpr int WM = WM_, WN = WN_, FM = FM_, FN = FN_;
+    static constexpr int BM = WM * FM * 8, BN = WN * FN * 8;
+    static constexpr int A_PER = BM * BK / NTHR, B_PER = BN * BK / NTHR;
+    static_assert(WM * WN * 32 == NTHR, "4 warps per CTA");
+};
+using Sh16 = Shape<1, 4, 2, 4>;  // 16 x 128
+using Sh32 = Shape<1, 4, 4, 4>;  // 32 x 128
+using Sh64 = Shape<2, 2, 4, 4>;  // 64 x 64
+
+template <class S>
+struct Stage {
+    double A[BK][S::BM + PAD];
+    double B[BK][S::BN + PAD];
 };
 
-__device__ __forceinline__ void mma_chunk(const Tiles& t, double (&acc)[4][4][2], int wm, int wn, int lane) {
+template <class S>
+struct Acc {
+    double c[S::FM][S::FN][2];
+    __device__ void zero() {
+#pragma unroll
+        for (int i = 0; i < S::FM; ++i)
+#pragma unroll
+            for (int j = 0; j < S::FN; ++j) c[i][j][0] = c[i][j][1] = 0.0;
+    }
+};
+
+template <class S>
+__device__ __forceinline__ void mma_stage(const double (*A)[S::BM + PAD], const double (*B)[S::BN + PAD], Acc<S>& acc,
+                                          int warp, int lane) {
     const int r = lane >> 2, q = lane & 3;
+    const int wm = warp % S::WM, wn = warp / S::WM;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
-        double a[4], b[4];
+        double a[S::FM], b[S::FN];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = t.A[kk + q][wm * 32 + i * 8 + r];
+        for (int i = 0; i < S::FM; ++i) a[i] = A[kk + q][wm * S::FM * 8 + i * 8 + r];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = t.B[kk + q][wn * 32 + j * 8 + r];
+        for (int j = 0; j < S::FN; ++j) b[j] = B[kk + q][wn * S::FN * 8 + j * 8 + r];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < S::FM; ++i)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) dmma(acc[i][j], a[i], b[j]);
+            for (int j = 0; j < S::FN; ++j) dmma(acc.c[i][j], a[i], b[j]);
     }
 }
 
-__device__ __forceinline__ void store_tile(double* __restrict__ C, uint64_t c_off, uint32_t ldc, uint32_t M, uint32_t N,
-                                           uint32_t m0, uint32_t n0, const double (&acc)[4][4][2], int wm, int wn,
-                                           int lane) {
+// Visit every accumulator element: f(m, n, value) with tile-local (m, n).
+template <class S, class F>
+__device__ __forceinline__ void for_acc(const Acc<S>& acc, int warp, int lane, F f) {
     const int r = lane >> 2, q = lane & 3;
+    const int wm = warp % S::WM, wn = warp / S::WM;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < S::FM; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < S::FN; ++j)
 #pragma unroll
-            for (int c = 0; c < 2; ++c) {
-                uint32_t m = m0 + wm * 32 + i * 8 + r;
-                uint32_t n = n0 + wn * 32 + j * 8 + q * 2 + c;
-                if (m < M && n < N) C[c_off + m + uint64_t(n) * ldc] = acc[i][j][c];
-            }
+            for (int c = 0; c < 2; ++c) f(wm * S::FM * 8 + i * 8 + r, wn * S::FN * 8 + j * 8 + q * 2 + c, acc.c[i][j][c]);
 }
 
-// T-GEMM: one CTA per (job, 64x64 tile)
+// ---------------------------------------------------------------------------
+// T-GEMM: one CTA per (job, tile)
+template <class S>
 __global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, const TileD* __restrict__ tiles,
                                                 const double* __restrict__ x, const double* __restrict__ R,
                                                 double* __restrict__ T) {
-    __shared__ Tiles t;
-    __shared__ uint64_t colbase[BN];
+    __shared__ Stage<S> st[2];
+    __shared__ uint64_t colbase[S::BN];
     const TileD tile = tiles[blockIdx.x];
     const TJobD J = jobs[tile.item];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 1, wn = warp >> 1;
-    if (tid < BN) {
-        uint32_t n = tile.n0 + tid;
-        uint64_t cb = 0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int c = tid; c < S::BN; c += NTHR) {
+        uint32_t n = tile.n0 + c;
+        uint64_t cb = J.b_off;
         if (n < J.N) {
             uint32_t b = n / J.brs, j = n - b * J.brs;
             cb = J.b_off + uint64_t(b) * J.K * J.brs + (J.tr ? uint64_t(j) : uint64_t(j) * J.K);
         }
-        colbase[tid] = cb;
+        colbase[c] = cb;
     }
-    const uint64_t kstride = J.tr ? J.brs : 1;
-    double acc[4][4][2];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     __syncthreads();
-    for (uint32_t k0 = 0; k0 < J.K; k0 += BK) {
+    const uint64_t kstride = J.tr ? J.brs : 1;
+    auto issue = [&](int sidx, uint32_t k0) {
+        Stage<S>& s = st[sidx];
 #pragma unroll
-        for (int rr = 0; rr < (BM * BK) / NTHR; ++rr) {
+        for (int rr = 0; rr < S::A_PER; ++rr) {
             int e = tid + rr * NTHR;
-            int m = e & (BM - 1), k = e >> 6;
+            int m = e % S::BM, k = e / S::BM;
             uint32_t gm = tile.m0 + m, gk = k0 + k;
-            t.A[k][m] = (gm < J.M && gk < J.K) ? x[J.a_off + gm + uint64_t(gk) * J.lda] : 0.0;
+            bool ok = gm < J.M && gk < J.K;
+            cp8(&s.A[k][m], ok ? x + J.a_off + gm + uint64_t(gk) * J.lda : x, ok);
         }
         if (!J.tr) {
 #pragma unroll
-            for (int rr = 0; rr < (BN * BK) / NTHR; ++rr) {
+            for (int rr = 0; rr < S::B_PER; ++rr) {
                 int e = tid + rr * NTHR;
-                int k = e & (BK - 1), n = e >> 4;
+                int k = e % BK, n = e / BK;
                 uint32_t gn = tile.n0 + n, gk = k0 + k;
-                t.B[k][n] = (gn < J.N && gk < J.K) ? R[colbase[n] + gk] : 0.0;
+                bool ok = gn < J.N && gk < J.K;
+                cp8(&s.B[k][n], ok ? R + colbase[n] + gk : R, ok);
             }
         } else {
 #pragma unroll
-            for (int rr = 0; rr < (BN * BK) / NTHR; ++rr) {
+            for (int rr = 0; rr < S::B_PER; ++rr) {
                 int e = tid + rr * NTHR;
-                int n = e & (BN - 1), k = e >> 6;
+                int n = e % S::BN, k = e / S::BN;
                 uint32_t gn = tile.n0 + n, gk = k0 + k;
-                t.B[k][n] = (gn < J.N && gk < J.K) ? R[colbase[n] + uint64_t(gk) * kstride] : 0.0;
+                bool ok = gn < J.N && gk < J.K;
+                cp8(&s.B[k][n], ok ? R + colbase[n] + uint64_t(gk) * kstride : R, ok);
             }
         }
+        cp_commit();
+    };
+    Acc<S> acc;
+    acc.zero();
+    const uint32_t nk = (J.K + BK - 1) / BK;
+    issue(0, 0);
+    for (uint32_t kc = 0; kc < nk; ++kc) {
+        cp_wait_all();
         __syncthreads();
-        mma_chunk(t, acc, wm, wn, lane);
-        __syncthreads();
+        if (kc + 1 < nk) issue((kc + 1) & 1, (kc + 1) * BK);
+        mma_stage<S>(st[kc & 1].A, st[kc & 1].B, acc, warp, lane);
     }
-    store_tile(T, J.c_off, J.M, J.M, J.N, tile.m0, tile.n0, acc, wm, wn, lane);
+    for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
+        uint32_t gm = tile.m0 + m, gn = tile.n0 + n;
+        if (gm < J.M && gn < J.N) T[J.c_off + gm + uint64_t(gn) * J.M] = v;
+    });
 }
 
-// S gather: one CTA per (cohort, unit, L block row) line
-__global__ void __launch_bounds__(256) k_gather(const GTaskD* __restrict__ tasks, const double* __restrict__ alpha,
-                                                const uint64_t* __restrict__ aoff, const double* __restrict__ T,
-                                                double* __restrict__ S) {
-    __shared__ double sa[64];
-    __shared__ uint64_t so[64];
-    const GTaskD g = tasks[blockIdx.x];
-    const uint32_t n = g.rows * g.cols;
-    for (uint32_t a0 = 0; a0 < g.a_count; a0 += 64) {
-        uint32_t na = min(64u, g.a_count - a0);
-        __syncthreads();
-        if (threadIdx.x < na) {
-            sa[threadIdx.x] = alpha[g.a_start + a0 + threadIdx.x];
-            so[threadIdx.x] = aoff[g.a_start + a0 + threadIdx.x];
-        }
-        __syncthreads();
-        for (uint32_t e = threadIdx.x; e < n; e += blockDim.x) {
-            uint32_t c = e / g.rows, r = e - c * g.rows;
-            uint64_t rel = r + uint64_t(c) * g.rows;
-            double s = 0.0;
-            for (uint32_t a = 0; a < na; ++a) s = fma(sa[a], T[so[a] + rel], s);
-            double* dst = &S[g.s_off + r + uint64_t(c) * g.ldS];
-            *dst = (a0 == 0) ? s : *dst + s;
-        }
-    }
-}
-
-// L.S GEMM: one CTA per (output block, 64x64 tile); K runs over every cohort segment
-__global__ void __launch_bounds__(NTHR) k_lsgemm(const OutD* __restrict__ outs, const SegD* __restrict__ segs,
-                                                 const TileD* __restrict__ tiles, const double* __restrict__ Lb,
-                                                 const double* __restrict__ S, double* __restrict__ y) {
-    __shared__ Tiles t;
-    __shared__ uint64_t kbase[BK];
+// ---------------------------------------------------------------------------
+// S build: one CTA per (unit, line tile, element tile)
+template <class S>
+__global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units, const TileD* __restrict__ tiles,
+                                                const uint32_t* __restrict__ line_b1, const uint64_t* __restrict__ slice_off,
+                                                const uint32_t* __restrict__ sptr, const WEntD* __restrict__ went,
+                                                const double* __restrict__ T, double* __restrict__ Sm) {
+    __shared__ double Bs[2][BK][S::BN + PAD];
+    __shared__ double As[BK][S::BM + PAD];
+    __shared__ uint64_t soff[2][BK];
     const TileD tile = tiles[blockIdx.x];
-    const OutD O = outs[tile.item];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 1, wn = warp >> 1;
-    double acc[4][4][2];
+    const UnitD U = units[tile.item];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t nk = (U.nk + BK - 1) / BK;
+    auto issue = [&](int sidx, uint32_t k0) {
+        if (tid < BK) soff[sidx][tid] = (k0 + tid < U.nk) ? slice_off[U.slice0 + k0 + tid] : 0;
+        __syncthreads();
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    const uint32_t M = O.M;
-    for (uint32_t sgi = 0; sgi < O.seg_count; ++sgi) {
-        const SegD sg = segs[O.seg_start + sgi];
-        const uint32_t Kc = sg.nS * sg.ls_in;
-        const uint64_t blk = uint64_t(M) * sg.ls_in;
-        for (uint32_t k0 = 0; k0 < Kc; k0 += BK) {
-            if (tid < BK) {
-                uint32_t kk = k0 + tid;
-                uint64_t kb = 0;
-                if (kk < Kc) {
-                    uint32_t b = kk / sg.ls_in, j = kk - b * sg.ls_in;
-                    kb = sg.l_off + b * blk + (sg.tr ? uint64_t(j) : uint64_t(j) * M);
-                }
-                kbase[tid] = kb;
-            }
-            __syncthreads();
-            if (!sg.tr) {
-#pragma unroll
-                for (int rr = 0; rr < (BM * BK) / NTHR; ++rr) {
-                    int e = tid + rr * NTHR;
-                    int m = e & (BM - 1), k = e >> 6;
-                    uint32_t gm = tile.m0 + m, gk = k0 + k;
-                    t.A[k][m] = (gm < M && gk < Kc) ? Lb[kbase[k] + gm] : 0.0;
-                }
-            } else {
-#pragma unroll
-                for (int rr = 0; rr < (BM * BK) / NTHR; ++rr) {
-                    int e = tid + rr * NTHR;
-                    int k = e & (BK - 1), m = e >> 4;
-                    uint32_t gm = tile.m0 + m, gk = k0 + k;
-                    t.A[k][m] = (gm < M && gk < Kc) ? Lb[kbase[k] + uint64_t(gm) * sg.ls_in] : 0.0;
-                }
-            }
-#pragma unroll
-            for (int rr = 0; rr < (BN * BK) / NTHR; ++rr) {
-                int e = tid + rr * NTHR;
-                int k = e & (BK - 1), n = e >> 4;
-                uint32_t gn = tile.n0 + n, gk = k0 + k;
-                t.B[k][n] = (gn < O.N && gk < Kc) ? S[sg.s_off + gk + uint64_t(gn) * Kc] : 0.0;
-            }
-            __syncthreads();
-            mma_chunk(t, acc, wm, wn, lane);
-            __syncthreads();
+        for (int rr = 0; rr < S::B_PER; ++rr) {
+            int e = tid + rr * NTHR;
+            int n = e % S::BN, k = e / S::BN;
+            uint32_t gn = tile.n0 + n, gk = k0 + k;
+            bool ok = gn < U.ne && gk < U.nk;
+            cp8(&Bs[sidx][k][n], ok ? T + soff[sidx][k] + gn : T, ok);
         }
+        cp_commit();
+    };
+    Acc<S> acc;
+    acc.zero();
+    issue(0, 0);
+    for (uint32_t kc = 0; kc < nk; ++kc) {
+        const uint32_t k0 = kc * BK;
+        // densify the coefficient tile W_u[m0 .. m0+BM, k0 .. k0+BK]
+        for (int e = tid; e < BK * (S::BM + PAD); e += NTHR) (&As[0][0])[e] = 0.0;
+        __syncthreads();
+        const uint32_t e0 = sptr[U.sptr0 + k0], e1 = sptr[U.sptr0 + min(k0 + BK, U.nk)];
+        for (uint32_t e = e0 + tid; e < e1; e += NTHR) {
+            const WEntD w = went[e];
+            if (w.line >= tile.m0 && w.line < tile.m0 + S::BM) As[w.k - k0][w.line - tile.m0] = w.a;
+        }
+        cp_wait_all();
+        __syncthreads();
+        if (kc + 1 < nk) issue((kc + 1) & 1, k0 + BK);
+        mma_stage<S>(As, Bs[kc & 1], acc, warp, lane);
+        __syncthreads();
     }
-    store_tile(y, O.y_off, M, M, O.N, tile.m0, tile.n0, acc, wm, wn, lane);
+    for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
+        uint32_t gl = tile.m0 + m, gn = tile.n0 + n;
+        if (gl < U.nl && gn < U.ne) {
+            uint32_t b1 = line_b1[U.line0 + gl];
+            uint32_t c = gn / U.ls, r = gn - c * U.ls;
+            Sm[U.s_off + uint64_t(b1) * U.ls + r + uint64_t(c) * U.ldS] = v;
+        }
+    });
+}
+
+// ---------------------------------------------------------------------------
+// L.S GEMM, split-K: item = (output tile, segment, K range) -> partial tile P[item]
+template <class S>
+__global__ void __launch_bounds__(NTHR) k_lspart(const KItemD* __restrict__ items, const OTileD* __restrict__ otiles,
+                                                 const OutD* __restrict__ outs, const SegD* __restrict__ segs,
+                                                 const double* __restrict__ Lb, const double* __restrict__ Sm,
+                                                 double* __restrict__ P) {
+    __shared__ Stage<S> st[2];
+    __shared__ uint64_t kbase[2][BK];
+    const KItemD it = items[blockIdx.x];
+    const OTileD ot = otiles[it.tile];
+    const OutD O = outs[ot.out];
+    const SegD sg = segs[it.seg];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t M = O.M, Kc = sg.nS * sg.ls_in;
+    const uint64_t blk = uint64_t(M) * sg.ls_in;
+    auto issue = [&](int sidx, uint32_t k0) {
+        if (tid < BK) {
+            uint32_t kk = k0 + tid;
+            uint64_t kb = sg.l_off;
+            if (kk < it.k1) {
+                uint32_t b = kk / sg.ls_in, j = kk - b * sg.ls_in;
+                kb = sg.l_off + b * blk + (sg.tr ? uint64_t(j) : uint64_t(j) * M);
+            }
+            kbase[sidx][tid] = kb;
+        }
+        __syncthreads();
+        Stage<S>& s = st[sidx];
+        if (!sg.tr) {
+#pragma unroll
+            for (int rr = 0; rr < S::A_PER; ++rr) {
+                int e = tid + rr * NTHR;
+                int m = e % S::BM, k = e / S::BM;
+                uint32_t gm = ot.m0 + m, gk = k0 + k;
+                bool ok = gm < M && gk < it.k1;
+                cp8(&s.A[k][m], ok ? Lb + kbase[sidx][k] + gm : Lb, ok);
+            }
+        } else {
+#pragma unroll
+            for (int rr = 0; rr < S::A_PER; ++rr) {
+                int e = tid + rr * NTHR;
+                int k = e % BK, m = e / BK;
+                uint32_t gm = ot.m0 + m, gk = k0 + k;
+                bool ok = gm < M && gk < it.k1;
+                cp8(&s.A[k][m], ok ? Lb + kbase[sidx][k] + uint64_t(gm) * sg.ls_in : Lb, ok);
+            }
+        }
+#pragma unroll
+        for (int rr = 0; rr < S::B_PER; ++rr) {
+            int e = tid + rr * NTHR;
+            int k = e % BK, n = e / BK;
+            uint32_t gn = ot.n0 + n, gk = k0 + k;
+            bool ok = gn < O.N && gk < it.k1;
+            cp8(&s.B[k][n], ok ? Sm + sg.s_off + gk + uint64_t(gn) * Kc : Sm, ok);
+        }
+        cp_commit();
+    };
+    Acc<S> acc;
+    acc.zero();
+    const uint32_t nk = (it.k1 - it.k0 + BK - 1) / BK;
+    issue(0, it.k0);
+    for (uint32_t kc = 0; kc < nk; ++kc) {
+        cp_wait_all();
+        __syncthreads();
+        if (kc + 1 < nk) issue((kc + 1) & 1, it.k0 + (kc + 1) * BK);
+        mma_stage<S>(st[kc & 1].A, st[kc & 1].B, acc, warp, lane);
+    }
+    double* Pt = P + uint64_t(blockIdx.x) * S::BM * S::BN;
+    for_acc<S>(acc, warp, lane, [&](int m, int n, double v) { Pt[m + n * S::BM] = v; });
+}
+
+// Sum the partial tiles of each output tile in item order and write y.
+template <class S>
+__global__ void __launch_bounds__(256) k_lsreduce(const OTileD* __restrict__ otiles, const OutD* __restrict__ outs,
+                                                  const double* __restrict__ P, double* __restrict__ y) {
+    const OTileD ot = otiles[blockIdx.x];
+    const OutD O = outs[ot.out];
+    for (int e = threadIdx.x; e < S::BM * S::BN; e += blockDim.x) {
+        const int m = e % S::BM, n = e / S::BM;
+        const uint32_t gm = ot.m0 + m, gn = ot.n0 + n;
+        if (gm >= O.M || gn >= O.N) continue;
+        double s = 0.0;
+        for (uint32_t p = 0; p < ot.nparts; ++p) s += P[uint64_t(ot.part0 + p) * S::BM * S::BN + e];
+        y[O.y_off + gm + uint64_t(gn) * O.M] = s;
+    }
+}
+
+template <class S>
+void launch_t(HeffPlan& p, int sh, const double* x, cudaStream_t s) {
+    if (!p.ttiles[sh].empty())
+        k_tgemm<S><<<unsigned(p.ttiles[sh].size()), NTHR, 0, s>>>(p.d_tjobs.get(), p.d_ttiles[sh].get(), x,
+                                                                  p.R->data.get(), p.d_T.get());
+}
+
+template <class S>
+void launch_s(HeffPlan& p, int sh, cudaStream_t s) {
+    if (!p.utiles[sh].empty())
+        k_sgemm<S><<<unsigned(p.utiles[sh].size()), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get(), p.d_line_b1.get(),
+                                                                  p.d_slice_off.get(), p.d_sptr.get(), p.d_went.get(),
+                                                                  p.d_T.get(), p.d_S.get());
+}
+
+template <class S>
+void launch_ls(HeffPlan& p, int sh, double* y, cudaStream_t s) {
+    if (p.kitems[sh].empty()) return;
+    k_lspart<S><<<unsigned(p.kitems[sh].size()), NTHR, 0, s>>>(p.d_kitems[sh].get(), p.d_otiles[sh].get(), p.d_outs.get(),
+                                                               p.d_segs.get(), p.L->data.get(), p.d_S.get(), p.d_P.get());
+    k_lsreduce<S><<<unsigned(p.otiles[sh].size()), 256, 0, s>>>(p.d_otiles[sh].get(), p.d_outs.get(), p.d_P.get(), y);
 }
 
 }  // namespace
@@ -218,31 +343,51 @@ void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev)
     cudaStream_t s = p.stream;
     if (ev) QCM_CUDA(cudaEventRecord(ev[0], s));
     QCM_CUDA(cudaMemsetAsync(y, 0, p.x_len * sizeof(double), s));
-    if (!p.ttiles.empty())
-        k_tgemm<<<unsigned(p.ttiles.size()), NTHR, 0, s>>>(p.d_tjobs.get(), p.d_ttiles.get(), x, p.R->data.get(), p.d_T.get());
+    launch_t<Sh16>(p, SHAPE_16, x, s);
+    launch_t<Sh32>(p, SHAPE_32, x, s);
+    launch_t<Sh64>(p, SHAPE_64, x, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[1], s));
-    if (p.s_len) QCM_CUDA(cudaMemsetAsync(p.d_S.get(), 0, p.s_len * sizeof(double), s));
-    if (!p.gtasks.empty())
-        k_gather<<<unsigned(p.gtasks.size()), 256, 0, s>>>(p.d_gtasks.get(), p.d_alpha.get(), p.d_aoff.get(), p.d_T.get(), p.d_S.get());
+    if (p.s_len) QCM_CUDA(cudaMemsetAsync(p.d_S.get(), 0, p.s_len * sizeof(double), s));  // rows without lines stay 0
+    launch_s<Sh16>(p, SHAPE_16, s);
+    launch_s<Sh32>(p, SHAPE_32, s);
+    launch_s<Sh64>(p, SHAPE_64, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
-    if (!p.otiles.empty())
-        k_lsgemm<<<unsigned(p.otiles.size()), NTHR, 0, s>>>(p.d_outs.get(), p.d_segs.get(), p.d_otiles.get(), p.L->data.get(), p.d_S.get(), y);
+    launch_ls<Sh16>(p, SHAPE_16, y, s);
+    launch_ls<Sh32>(p, SHAPE_32, y, s);
+    launch_ls<Sh64>(p, SHAPE_64, y, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[3], s));
     QCM_CUDA(cudaGetLastError());
+}
+
+int heff_launches_per_apply(const HeffPlan& p) {
+    int n = 0;
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        n += !p.ttiles[sh].empty();
+        n += !p.utiles[sh].empty();
+        n += p.kitems[sh].empty() ? 0 : 2;
+    }
+    return n;
 }
 
 void upload_plan(HeffPlan& p) {
     cudaStream_t s = p.stream;
     p.d_tjobs.upload(p.tjobs, s);
-    p.d_ttiles.upload(p.ttiles, s);
-    p.d_gtasks.upload(p.gtasks, s);
-    p.d_alpha.upload(p.alpha, s);
-    p.d_aoff.upload(p.aoff, s);
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        p.d_ttiles[sh].upload(p.ttiles[sh], s);
+        p.d_utiles[sh].upload(p.utiles[sh], s);
+        p.d_otiles[sh].upload(p.otiles[sh], s);
+        p.d_kitems[sh].upload(p.kitems[sh], s);
+    }
+    p.d_units.upload(p.units, s);
+    p.d_line_b1.upload(p.line_b1, s);
+    p.d_slice_off.upload(p.slice_off, s);
+    p.d_sptr.upload(p.sptr, s);
+    p.d_went.upload(p.went, s);
     p.d_segs.upload(p.segs, s);
     p.d_outs.upload(p.outs, s);
-    p.d_otiles.upload(p.otiles, s);
     p.d_T.alloc(p.t_len);
     p.d_S.alloc(p.s_len);
+    p.d_P.alloc(p.p_len);
     QCM_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -36,12 +36,13 @@ HeffPlan::~HeffPlan() {
 }
 
 namespace {
-constexpr uint32_t TILE_M = 64, TILE_N = 64;
-
-void add_tiles(std::vector<TileD>& tiles, uint32_t item, uint32_t M, uint32_t N) {
-    for (uint32_t n0 = 0; n0 < N; n0 += TILE_N)
-        for (uint32_t m0 = 0; m0 < M; m0 += TILE_M) tiles.push_back(TileD{item, m0, n0, 0});
+void add_tiles(std::vector<TileD>* tiles, uint32_t item, uint32_t M, uint32_t N) {
+    int sh = shape_for_rows(M);
+    uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
+    for (uint32_t n0 = 0; n0 < N; n0 += bn)
+        for (uint32_t m0 = 0; m0 < M; m0 += bm) tiles[sh].push_back(TileD{item, m0, n0, 0});
 }
+constexpr uint32_t KCHUNK = 512;  // K rows per split-K item of the L.S GEMM
 }  // namespace
 
 std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
@@ -183,18 +184,22 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             uint64_t s_off = p->s_len;
             p->s_len += (uint64_t(K_c) * stripe + 31) / 32 * 32;
             for (auto& u : units) {
+                // unit GEMM data: lines (b1 rows with coefficients), distinct T slices, entries by slice
+                std::vector<uint32_t> lines;
+                std::unordered_map<uint64_t, uint32_t> kidx;  // T offset -> slice index
+                std::vector<uint64_t> slices;
+                std::vector<std::vector<std::pair<uint32_t, double>>> by_slice;
                 std::size_t nu = 0;
                 for (uint32_t b = 0; b < nS; ++b) {
                     auto& ln = u.lines[b];
                     if (ln.empty()) continue;
+                    uint32_t li = uint32_t(lines.size());
+                    lines.push_back(b);
                     nu += ln.size();
-                    GTaskD g{};
-                    g.s_off = s_off + uint64_t(b) * ls_in + uint64_t(u.offset) * K_c;
-                    g.ldS = K_c; g.rows = ls_in; g.cols = u.ms;
-                    g.a_start = uint32_t(p->alpha.size()); g.a_count = uint32_t(ln.size());
                     for (std::size_t k = 0; k < ln.size(); ++k) {
-                        p->alpha.push_back(ln[k].first);
-                        p->aoff.push_back(ln[k].second);
+                        auto ins = kidx.emplace(ln[k].second, uint32_t(slices.size()));
+                        if (ins.second) { slices.push_back(ln[k].second); by_slice.emplace_back(); }
+                        by_slice[ins.first->second].push_back({li, ln[k].first});
                         if (bookkeeping) {
                             const auto& bk = u.bk[b];
                             uint32_t row[10] = {lb_in, lb_out, ci, ci_eff, u.offset, u.ms, b, bk[3 * k], bk[3 * k + 1], bk[3 * k + 2]};
@@ -202,13 +207,30 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                             p->bk_alpha.push_back(ln[k].first);
                         }
                     }
-                    if (ls_in && u.ms) {
-                        p->gtasks.push_back(g);
-                        p->g_elems += uint64_t(ls_in) * u.ms;
-                        p->g_reads += uint64_t(ls_in) * u.ms * ln.size();
-                    }
                 }
                 p->flops_s += 2.0 * ls_in * u.ms * double(nu);
+                if (lines.empty() || ls_in == 0 || u.ms == 0) continue;
+                UnitD ud{};
+                ud.s_off = s_off + uint64_t(u.offset) * K_c;
+                ud.ldS = K_c; ud.ls = ls_in; ud.ne = ls_in * u.ms;
+                ud.nl = uint32_t(lines.size()); ud.line0 = uint32_t(p->line_b1.size());
+                ud.nk = uint32_t(slices.size()); ud.slice0 = uint32_t(p->slice_off.size());
+                ud.sptr0 = uint32_t(p->sptr.size());
+                p->line_b1.insert(p->line_b1.end(), lines.begin(), lines.end());
+                p->slice_off.insert(p->slice_off.end(), slices.begin(), slices.end());
+                for (uint32_t k = 0; k < ud.nk; ++k) {
+                    p->sptr.push_back(uint32_t(p->went.size()));
+                    for (auto& e : by_slice[k]) p->went.push_back(WEntD{e.first, k, e.second});
+                }
+                p->sptr.push_back(uint32_t(p->went.size()));
+                int sh = shape_for_rows(ud.nl);
+                uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
+                for (uint32_t n0 = 0; n0 < ud.ne; n0 += bn)
+                    for (uint32_t m0 = 0; m0 < ud.nl; m0 += bm) p->utiles[sh].push_back(TileD{uint32_t(p->units.size()), m0, n0, 0});
+                p->units.push_back(ud);
+                p->g_elems += uint64_t(ls_in) * u.ms * ud.nl;
+                p->g_reads += uint64_t(ls_in) * u.ms * nu;
+                p->flops_sdense += 2.0 * ud.nl * ud.nk * double(ud.ne);
             }
             p->flops_ls += 2.0 * ls_out * ls_in * double(nS) * stripe;
             SegD sg{};
@@ -231,10 +253,29 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             o.seg_start = uint32_t(p->segs.size());
             o.seg_count = uint32_t(per_out[lb_out].size());
             p->segs.insert(p->segs.end(), per_out[lb_out].begin(), per_out[lb_out].end());
-            if (o.M && o.N) add_tiles(p->otiles, uint32_t(p->outs.size()), o.M, o.N);
+            if (o.M && o.N) {
+                int sh = shape_for_rows(o.M);
+                uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
+                for (uint32_t n0 = 0; n0 < o.N; n0 += bn)
+                    for (uint32_t m0 = 0; m0 < o.M; m0 += bm) {
+                        OTileD t{};
+                        t.out = uint32_t(p->outs.size()); t.m0 = m0; t.n0 = n0;
+                        t.part0 = uint32_t(p->kitems[sh].size());
+                        for (uint32_t sg = o.seg_start; sg < o.seg_start + o.seg_count; ++sg) {
+                            uint32_t Kc = p->segs[sg].nS * p->segs[sg].ls_in;
+                            for (uint32_t k0 = 0; k0 < Kc; k0 += KCHUNK)
+                                p->kitems[sh].push_back(KItemD{uint32_t(p->otiles[sh].size()), sg, k0, std::min(Kc, k0 + KCHUNK)});
+                        }
+                        t.nparts = uint32_t(p->kitems[sh].size()) - t.part0;
+                        p->otiles[sh].push_back(t);
+                    }
+            }
             p->outs.push_back(o);
         }
     }
+    uint64_t pl = 0;
+    for (int sh = 0; sh < N_SHAPES; ++sh) pl = std::max<uint64_t>(pl, uint64_t(p->kitems[sh].size()) * shape_bm(sh) * shape_bn(sh));
+    p->p_len = pl;
     p->flops = p->flops_t + p->flops_ls + p->flops_s;
     return p;
 }
