@@ -157,6 +157,23 @@ int qcm_heff_bookkeeping(const qcm_heff* h, uint32_t* ints, double* alpha, uint6
 int qcm_heff_profile(qcm_heff* h, const double* x_dev, double* y_dev, float* ms);
 void qcm_heff_free(qcm_heff* h);
 
+/* No counterpart in the reference.  For callers that cannot allocate device memory
+ * when they need H.psi -- a host code whose HBM is owned by its own caching
+ * allocator (a cudaMalloc here may fail or fragment it) or a solver loop that
+ * must not stall on cudaFree's device-wide synchronisation -- this variant of
+ * qcm_heff_apply_device calls no cudaMalloc/cudaFree and no allocating library
+ * routine.  Its scratch (T slices, S, split-K partials) lives in one fixed
+ * static device array of QCM_NOALLOC_SCRATCH_DOUBLES doubles (64 MiB), which
+ * every GPU that loads this library holds until the process exits.  Plans
+ * needing more scratch are rejected with QCM_ERR_ARG.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) once;
+ * make that first call before any stream capture.  All calls on a device share
+ * the array and it keeps the last call's contents (S is cleared inside each
+ * call): calls that overlap on the GPU -- other streams, other threads --
+ * race.  Enqueued on the context stream (asynchronous). */
+#define QCM_NOALLOC_SCRATCH_DOUBLES (8u * 1024u * 1024u)
+int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, double* y_dev);
+
 /* FP64 throughput probes on the current device (TFLOP/s): DMMA (mma.sync
  * m8n8k4 .f64) and DFMA loops.  Roofline denominators of the FP64 form. */
 int qcm_probe_fp64_peaks(double* dmma_tflops, double* dfma_tflops);

@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "../../include/qcm_b200.h"
+#include "capi_types.hpp"
 #include "capi_util.hpp"
 #include "device.hpp"
 #include "heff.hpp"
@@ -12,20 +13,6 @@ namespace qcm {
 const MPO& mpo_of(const qcm_mpo* m);
 }
 
-struct qcm_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-};
-
-struct qcm_boundary {
-    qcm_ctx* ctx;
-    qcm::DevBoundary b;
-};
-
-struct qcm_heff {
-    qcm_ctx* ctx;
-    std::unique_ptr<qcm::HeffPlan> p;
-};
 
 namespace {
 qcm::Index to_index(uint32_t n, const qcm_sector* s) {

@@ -168,5 +168,7 @@ void upload_plan(HeffPlan& p);
 // gather and after the L.S GEMM.
 void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev = nullptr);
 int heff_launches_per_apply(const HeffPlan& p);
+// Same apply with caller-provided scratch: Tb (t_len), Sb (s_len) and Pb (p_len) doubles.
+void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* Tb, double* Sb, double* Pb);
 
 }  // namespace qcm

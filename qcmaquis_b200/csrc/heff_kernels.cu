@@ -315,48 +315,59 @@ __global__ void __launch_bounds__(256) k_lsreduce(const OTileD* __restrict__ oti
 }
 
 template <class S>
-void launch_t(HeffPlan& p, int sh, const double* x, cudaStream_t s) {
+void launch_t(HeffPlan& p, int sh, const double* x, double* Tb, cudaStream_t s) {
     if (!p.ttiles[sh].empty())
         k_tgemm<S><<<unsigned(p.ttiles[sh].size()), NTHR, 0, s>>>(p.d_tjobs.get(), p.d_ttiles[sh].get(), x,
-                                                                  p.R->data.get(), p.d_T.get());
+                                                                  p.R->data.get(), Tb);
 }
 
 template <class S>
-void launch_s(HeffPlan& p, int sh, cudaStream_t s) {
+void launch_s(HeffPlan& p, int sh, const double* Tb, double* Sb, cudaStream_t s) {
     if (!p.utiles[sh].empty())
         k_sgemm<S><<<unsigned(p.utiles[sh].size()), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get(), p.d_line_b1.get(),
-                                                                  p.d_slice_off.get(), p.d_sptr.get(), p.d_went.get(),
-                                                                  p.d_T.get(), p.d_S.get());
+                                                                  p.d_slice_off.get(), p.d_sptr.get(), p.d_went.get(), Tb, Sb);
 }
 
 template <class S>
-void launch_ls(HeffPlan& p, int sh, double* y, cudaStream_t s) {
+void launch_ls(HeffPlan& p, int sh, const double* Sb, double* Pb, double* y, cudaStream_t s) {
     if (p.kitems[sh].empty()) return;
     k_lspart<S><<<unsigned(p.kitems[sh].size()), NTHR, 0, s>>>(p.d_kitems[sh].get(), p.d_otiles[sh].get(), p.d_outs.get(),
-                                                               p.d_segs.get(), p.L->data.get(), p.d_S.get(), p.d_P.get());
-    k_lsreduce<S><<<unsigned(p.otiles[sh].size()), 256, 0, s>>>(p.d_otiles[sh].get(), p.d_outs.get(), p.d_P.get(), y);
+                                                               p.d_segs.get(), p.L->data.get(), Sb, Pb);
+    k_lsreduce<S><<<unsigned(p.otiles[sh].size()), 256, 0, s>>>(p.d_otiles[sh].get(), p.d_outs.get(), Pb, y);
 }
 
 }  // namespace
 
-void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev) {
+namespace {
+// One H.psi: T-GEMM -> S build -> split-K L.S, with the scratch buffers T, S and P given
+// explicitly (the plan's own buffers, or caller-provided memory of the same sizes).
+void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double* Tb, double* Sb, double* Pb) {
     cudaStream_t s = p.stream;
     if (ev) QCM_CUDA(cudaEventRecord(ev[0], s));
     QCM_CUDA(cudaMemsetAsync(y, 0, p.x_len * sizeof(double), s));
-    launch_t<Sh16>(p, SHAPE_16, x, s);
-    launch_t<Sh32>(p, SHAPE_32, x, s);
-    launch_t<Sh64>(p, SHAPE_64, x, s);
+    launch_t<Sh16>(p, SHAPE_16, x, Tb, s);
+    launch_t<Sh32>(p, SHAPE_32, x, Tb, s);
+    launch_t<Sh64>(p, SHAPE_64, x, Tb, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[1], s));
-    if (p.s_len) QCM_CUDA(cudaMemsetAsync(p.d_S.get(), 0, p.s_len * sizeof(double), s));  // rows without lines stay 0
-    launch_s<Sh16>(p, SHAPE_16, s);
-    launch_s<Sh32>(p, SHAPE_32, s);
-    launch_s<Sh64>(p, SHAPE_64, s);
+    if (p.s_len) QCM_CUDA(cudaMemsetAsync(Sb, 0, p.s_len * sizeof(double), s));  // rows without lines stay 0
+    launch_s<Sh16>(p, SHAPE_16, Tb, Sb, s);
+    launch_s<Sh32>(p, SHAPE_32, Tb, Sb, s);
+    launch_s<Sh64>(p, SHAPE_64, Tb, Sb, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
-    launch_ls<Sh16>(p, SHAPE_16, y, s);
-    launch_ls<Sh32>(p, SHAPE_32, y, s);
-    launch_ls<Sh64>(p, SHAPE_64, y, s);
+    launch_ls<Sh16>(p, SHAPE_16, Sb, Pb, y, s);
+    launch_ls<Sh32>(p, SHAPE_32, Sb, Pb, y, s);
+    launch_ls<Sh64>(p, SHAPE_64, Sb, Pb, y, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[3], s));
     QCM_CUDA(cudaGetLastError());
+}
+}  // namespace
+
+void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev) {
+    apply_impl(p, x, y, ev, p.d_T.get(), p.d_S.get(), p.d_P.get());
+}
+
+void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* Tb, double* Sb, double* Pb) {
+    apply_impl(p, x, y, nullptr, Tb, Sb, Pb);
 }
 
 int heff_launches_per_apply(const HeffPlan& p) {

@@ -63,6 +63,8 @@ _lib._sig("qcm_heff_apply", c_int, c_void_p, P(c_double), P(c_double))
 _lib._sig("qcm_heff_apply_device", c_int, c_void_p, c_void_p, c_void_p)
 _lib._sig("qcm_heff_bookkeeping", c_int, c_void_p, P(c_uint32), P(c_double), c_uint64, P(c_uint64))
 _lib._sig("qcm_heff_profile", c_int, c_void_p, c_void_p, c_void_p, P(ctypes.c_float))
+_lib._sig("qcm_heff_apply_device_noalloc", c_int, c_void_p, c_void_p, c_void_p)
+NOALLOC_SCRATCH_DOUBLES = 8 * 1024 * 1024
 _lib._sig("qcm_heff_free", None, c_void_p)
 _lib._sig("qcm_probe_fp64_peaks", c_int, P(c_double), P(c_double))
 
@@ -238,6 +240,12 @@ class HeffPlan:
 
     def apply_device(self, x_ptr: int, y_ptr: int):
         check(lib.qcm_heff_apply_device(self.h, c_void_p(x_ptr), c_void_p(y_ptr)), "qcm_heff_apply_device")
+
+    def apply_device_noalloc(self, x_ptr: int, y_ptr: int):
+        """apply_device without any device allocation: scratch in the library's fixed 64 MiB array
+        (for hosts that cannot cudaMalloc here; overlapping calls on one GPU race)."""
+        check(lib.qcm_heff_apply_device_noalloc(self.h, c_void_p(x_ptr), c_void_p(y_ptr)),
+              "qcm_heff_apply_device_noalloc")
 
     def profile(self, x_ptr: int, y_ptr: int):
         """Per-phase device times (ms): T-GEMM, S gather, L.S GEMM, total."""

@@ -1,0 +1,41 @@
+"""The allocation-free H_eff entry point (qcm_heff_apply_device_noalloc) through the C-ABI.
+
+It exists for host codes that cannot call cudaMalloc where they need H.psi (their
+HBM belongs to their own caching allocator, or their solver loop must not stall
+on cudaFree's device-wide synchronisation).  Its scratch is the library's fixed
+64 MiB device array instead of the plan's own buffers; the result must equal the
+regular device apply's, call after call (the array keeps the previous call's
+contents, so a stale buffer would show on the second call).  Collected last so a
+run that stops at the first failure has already run every other test.
+"""
+import numpy as np
+import pytest
+
+from qcmaquis_b200 import heff
+
+from helpers import qc_system, snapshot, site_of_step
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("L,M,sw,step", [(8, 64, 1, 3), (6, 16, 1, 7)])
+def test_noalloc_matches_device_apply_twice(gpu_ctx, L, M, sw, step):
+    import torch
+    snap = snapshot(L, M, sw, step)
+    h, V, e, m, ts, blob = qc_system(L, 0)
+    p = heff.parse_site_problem(snap)
+    plan = heff.plan_from_problem(gpu_ctx, p, ts, site_of_step(L, step))
+    assert plan.info["t_len"] + plan.info["s_len"] <= heff.NOALLOC_SCRATCH_DOUBLES
+    rng = np.random.default_rng(5)
+    xs = [torch.from_numpy(rng.standard_normal(plan.n)).cuda() for _ in range(2)]
+    for x in xs:  # two calls in a row, different inputs
+        y_ref = torch.empty_like(x)
+        y = torch.full_like(x, np.nan)
+        torch.cuda.synchronize()
+        plan.apply_device(x.data_ptr(), y_ref.data_ptr())
+        gpu_ctx.synchronize()
+        plan.apply_device_noalloc(x.data_ptr(), y.data_ptr())
+        gpu_ctx.synchronize()
+        a, b = y.cpu().numpy(), y_ref.cpu().numpy()
+        assert np.all(np.isfinite(a))
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
