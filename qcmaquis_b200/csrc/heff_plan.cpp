@@ -8,8 +8,14 @@
 //           * L.conjugate_scale(ci, b1),
 //   T slice = (ket offset + ss1 * rs_in, ci_right), column right_offset / rs_in,
 //   S row block = position of b1 in the L cohort, column = unit offset.
-// The result is laid out as device work lists instead of per-sector objects.
+// The result is laid out as device work lists.  Every lookup the inner loop
+// needs (sector offsets, cohort indices, T jobs) is a flat table built once per
+// plan, and the ket sectors are processed in parallel (OpenMP) and merged in
+// sector order, so the plan does not depend on the thread count.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <stdexcept>
 
@@ -36,13 +42,39 @@ HeffPlan::~HeffPlan() {
 }
 
 namespace {
+
+constexpr uint32_t NONE = 0xffffffffu;
+constexpr uint32_t KCHUNK = 512;  // K rows per split-K item of the L.S GEMM
+
 void add_tiles(std::vector<TileD>* tiles, uint32_t item, uint32_t M, uint32_t N) {
     int sh = shape_for_rows(M);
     uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
     for (uint32_t n0 = 0; n0 < N; n0 += bn)
         for (uint32_t m0 = 0; m0 < M; m0 += bm) tiles[sh].push_back(TileD{item, m0, n0, 0});
 }
-constexpr uint32_t KCHUNK = 512;  // K rows per split-K item of the L.S GEMM
+
+struct RSec { uint32_t rb, rs, off; };  // right sector of (left sector, phys sector), column offset
+
+// Everything one ket sector (lb_in) contributes; offsets relative to the part.
+struct Part {
+    std::vector<TJobD> tjobs;
+    std::vector<uint32_t> tjob_mps;  // mps column offset of each job (bookkeeping)
+    uint64_t t_len = 0;
+    std::vector<UnitD> units;
+    std::vector<uint32_t> line_b1, sptr;
+    std::vector<uint64_t> slice_off;
+    std::vector<WEntD> went;
+    uint64_t s_len = 0;
+    std::vector<std::pair<uint32_t, SegD>> segs;
+    double flops_t = 0, flops_s = 0, flops_ls = 0, flops_sdense = 0;
+    uint64_t g_elems = 0, g_reads = 0;
+    std::vector<uint32_t> bk_int;
+    std::vector<double> bk_alpha;
+};
+
+struct Em { uint32_t line, slice; double a; uint32_t mps, cir, col; };
+struct U { uint32_t st, offset, ms, rb_out; std::vector<Em> em; std::vector<uint32_t> lines; };
+
 }  // namespace
 
 std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
@@ -57,222 +89,297 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     p->L = &Lb; p->R = &Rb;
     ProductBasis rpb(phys, right, true);
     StateMap sm(phys);
+    const uint32_t nl = uint32_t(left.size()), nr = uint32_t(right.size()), nps = uint32_t(phys.size());
+    const uint32_t nst = uint32_t(sm.nstates());
 
     // vector layout: right-paired blocks in left-index order
-    p->x_off.resize(left.size());
-    p->x_cols.resize(left.size());
-    for (std::size_t lb = 0; lb < left.size(); ++lb) {
+    p->x_off.resize(nl);
+    p->x_cols.resize(nl);
+    for (uint32_t lb = 0; lb < nl; ++lb) {
         p->x_off[lb] = p->x_len;
         p->x_cols[lb] = uint32_t(rpb.size(left[lb].first));
         p->x_len += left[lb].second * p->x_cols[lb];
     }
 
-    // operators of the MPO tensor grouped per (op, output sector): (in state, out state, value)
-    struct OE { uint32_t in, out; double v; };
-    std::vector<std::vector<std::vector<OE>>> op_by_out(W.ops->size(), std::vector<std::vector<OE>>(phys.size()));
-    for (std::size_t o = 0; o < W.ops->size(); ++o) {
+    // ---- flat lookup tables ----
+    std::vector<RSec> rsec(std::size_t(nl) * nps, RSec{NONE, 0, 0});
+    for (uint32_t lb = 0; lb < nl; ++lb)
+        for (uint32_t s = 0; s < nps; ++s) {
+            Charge rc = left[lb].first + phys[s].first;
+            std::size_t rb = right.position(rc);
+            if (rb < nr) rsec[std::size_t(lb) * nps + s] = RSec{uint32_t(rb), uint32_t(right[rb].second), uint32_t(rpb(phys[s].first, rc))};
+        }
+    // R cohort of (ket right sector, bra right sector), and its storage partner
+    std::vector<uint32_t> Rci(std::size_t(nr) * nr, NONE), Rcie(std::size_t(nr) * nr, NONE);
+    for (uint32_t a = 0; a < nr; ++a)
+        for (uint32_t b = 0; b < nr; ++b) {
+            uint32_t ci = R.cohort_index(right[a].first, right[b].first);
+            if (ci == R.n_cohorts()) continue;
+            uint32_t ce = R.tr[ci] ? R.cohort_index(right[b].first, right[a].first) : ci;
+            if (ce == R.n_cohorts()) throw std::runtime_error("heff plan: transposed cohort without partner");
+            Rci[std::size_t(a) * nr + b] = ci;
+            Rcie[std::size_t(a) * nr + b] = ce;
+        }
+    // op entries, CSR per operator: (input state, output state, value)
+    const std::size_t nops = W.ops->size();
+    std::vector<uint32_t> optr(nops + 1, 0), oin, oout;
+    std::vector<double> oval;
+    for (std::size_t o = 0; o < nops; ++o) {
         const SparseOp& s = (*W.ops)[o];
-        for (std::size_t e = 0; e < s.val.size(); ++e)
-            op_by_out[o][sm.sector[s.out[e]]].push_back(OE{s.in[e], s.out[e], s.val[e]});
+        optr[o] = uint32_t(oin.size());
+        for (std::size_t e = 0; e < s.val.size(); ++e) { oin.push_back(s.in[e]); oout.push_back(s.out[e]); oval.push_back(s.val[e]); }
     }
+    optr[nops] = uint32_t(oin.size());
 
-    std::vector<std::pair<uint32_t, SegD>> seg_tmp;
-    for (uint32_t lb_in = 0; lb_in < left.size(); ++lb_in) {
-        Charge lc_in = left[lb_in].first;
-        uint32_t ls_in = uint32_t(left[lb_in].second);
-        // ---- T jobs ----
-        std::unordered_map<uint64_t, uint32_t> tmap;  // (mps col offset, ci_right) -> job
-        for (uint32_t s = 0; s < phys.size(); ++s) {
-            Charge rc_ket = lc_in + phys[s].first;
-            std::size_t rbk = right.position(rc_ket);
-            if (rbk == right.size()) continue;
-            uint32_t rs_ket = uint32_t(right[rbk].second);
-            uint32_t ket_off = uint32_t(rpb(phys[s].first, rc_ket));
-            for (std::size_t rb_bra = 0; rb_bra < right.size(); ++rb_bra) {
-                Charge rc_bra = right[rb_bra].first;
-                uint32_t ci = R.cohort_index(rc_ket, rc_bra);
-                if (ci == R.n_cohorts()) continue;
-                uint32_t ci_eff = R.tr[ci] ? R.cohort_index(rc_bra, rc_ket) : ci;
-                if (ci_eff == R.n_cohorts()) throw std::runtime_error("heff plan: transposed cohort without partner");
-                for (uint32_t ss = 0; ss < phys[s].second; ++ss) {
-                    uint32_t mps_off = ket_off + ss * rs_ket;
-                    TJobD j{};
-                    j.a_off = p->x_off[lb_in] + uint64_t(mps_off) * ls_in;
-                    j.b_off = Rb.idx.data_off[ci_eff];
-                    j.c_off = p->t_len;
-                    j.M = ls_in; j.K = rs_ket; j.brs = R.rsz[ci]; j.N = R.nb[ci_eff] * j.brs; j.lda = ls_in;
-                    j.tr = (ci != ci_eff) ? 1 : 0;
-                    p->flops_t += 2.0 * ls_in * double(R.cohort_size(ci_eff));
-                    if (tmap.emplace((uint64_t(mps_off) << 32) | ci, uint32_t(p->tjobs.size())).second) {
-                        p->t_len += (uint64_t(j.M) * j.N + 31) / 32 * 32;
-                        if (j.M && j.N) add_tiles(p->ttiles, uint32_t(p->tjobs.size()), j.M, j.N);
-                        p->tjobs.push_back(j);
-                    }
-                }
+    std::vector<Part> parts(nl);
+    const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
+    auto tnow = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    const double t_a = tnow();
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int lbi = 0; lbi < int(nl); ++lbi) {
+        const uint32_t lb_in = uint32_t(lbi);
+        Part& P = parts[lb_in];
+        const uint32_t ls_in = uint32_t(left[lb_in].second);
+        // ---- T jobs: one per (input state, bra right sector) ----
+        std::vector<uint32_t> tj(std::size_t(nst) * nr, NONE);
+        for (uint32_t st = 0; st < nst; ++st) {
+            const uint32_t s = uint32_t(sm.sector[st]), ss = uint32_t(sm.sub[st]);
+            const RSec& ri = rsec[std::size_t(lb_in) * nps + s];
+            if (ri.rb == NONE) continue;
+            for (uint32_t rbb = 0; rbb < nr; ++rbb) {
+                uint32_t ci = Rci[std::size_t(ri.rb) * nr + rbb];
+                if (ci == NONE) continue;
+                uint32_t ce = Rcie[std::size_t(ri.rb) * nr + rbb];
+                TJobD j{};
+                uint32_t mps_off = ri.off + ss * ri.rs;
+                j.a_off = p->x_off[lb_in] + uint64_t(mps_off) * ls_in;
+                j.b_off = R.data_off[ce];
+                j.c_off = P.t_len;
+                j.M = ls_in; j.K = ri.rs; j.brs = R.rsz[ci]; j.N = R.nb[ce] * j.brs; j.lda = ls_in;
+                j.tr = (ci != ce) ? 1 : 0;
+                P.flops_t += 2.0 * ls_in * double(R.cohort_size(ce));
+                tj[std::size_t(st) * nr + rbb] = uint32_t(P.tjobs.size());
+                P.t_len += (uint64_t(j.M) * j.N + 31) / 32 * 32;
+                P.tjobs.push_back(j);
+                P.tjob_mps.push_back(mps_off);
             }
         }
-        // ---- cohorts ----
-        for (uint32_t lb_out = 0; lb_out < left.size(); ++lb_out) {
-            Charge lc_out = left[lb_out].first;
-            uint32_t ls_out = uint32_t(left[lb_out].second);
-            uint32_t ci = L.cohort_index(lc_out, lc_in);
+        // slice numbering: slot of (job, b2 position); cleared after each unit
+        std::vector<uint32_t> job_pos0(P.tjobs.size() + 1, 0);
+        for (std::size_t k = 0; k < P.tjobs.size(); ++k)
+            job_pos0[k + 1] = job_pos0[k] + (P.tjobs[k].brs ? P.tjobs[k].N / P.tjobs[k].brs : 0);
+        std::vector<uint32_t> slot(job_pos0.back() + 1, NONE);
+
+        for (uint32_t lb_out = 0; lb_out < nl; ++lb_out) {
+            uint32_t ci = L.cohort_index(left[lb_out].first, left[lb_in].first);
             if (ci == L.n_cohorts()) continue;
-            uint32_t ci_eff = L.tr[ci] ? L.cohort_index(lc_in, lc_out) : ci;
-            if (ci_eff == L.n_cohorts()) throw std::runtime_error("heff plan: transposed cohort without partner");
-            uint32_t nS = L.nb[ci_eff];
-            struct Unit { uint32_t offset, ms; std::vector<std::vector<std::pair<double, uint64_t>>> lines; std::vector<std::vector<uint32_t>> bk; };
-            std::vector<Unit> units;
-            std::vector<int> unit_of_state(sm.nstates(), -1);
+            uint32_t ce = L.tr[ci] ? L.cohort_index(left[lb_in].first, left[lb_out].first) : ci;
+            if (ce == L.n_cohorts()) throw std::runtime_error("heff plan: transposed cohort without partner");
+            const uint32_t ls_out = uint32_t(left[lb_out].second);
+            const uint32_t nS = L.nb[ce];
+            const uint32_t K_c = nS * ls_in;
+            // units = output states whose right sector exists
+            std::vector<U> units;
             uint32_t stripe = 0;
-            for (uint32_t s = 0; s < phys.size(); ++s) {
-                Charge rc_out = lc_out + phys[s].first;
-                std::size_t rbo = right.position(rc_out);
-                if (rbo == right.size()) continue;
-                uint32_t rs_out = uint32_t(right[rbo].second);
-                uint32_t out_off = uint32_t(rpb(phys[s].first, rc_out));
-                for (uint32_t ss2 = 0; ss2 < phys[s].second; ++ss2) {
-                    unit_of_state[sm.first[s] + ss2] = int(units.size());
-                    Unit u;
-                    u.offset = out_off + ss2 * rs_out;
-                    u.ms = rs_out;
-                    u.lines.resize(nS);
-                    if (bookkeeping) u.bk.resize(nS);
-                    units.push_back(std::move(u));
-                    stripe += rs_out;
-                }
+            for (uint32_t st = 0; st < nst; ++st) {
+                const RSec& ro = rsec[std::size_t(lb_out) * nps + sm.sector[st]];
+                if (ro.rb == NONE) continue;
+                units.push_back(U{st, ro.off + uint32_t(sm.sub[st]) * ro.rs, ro.rs, ro.rb, {}, {}});
+                stripe += ro.rs;
             }
             if (stripe != p->x_cols[lb_out]) throw std::runtime_error("heff plan: cohort stripe differs from the block width");
+            // per (input state, unit): R cohort, T job and slice geometry
+            std::vector<int> unit_of(nst, -1);
+            for (std::size_t k = 0; k < units.size(); ++k) unit_of[units[k].st] = int(k);
+            const std::size_t nu = units.size();
+            std::vector<uint32_t> cir_t(std::size_t(nst) * nu, NONE), job_t(std::size_t(nst) * nu, NONE), rsin_t(nst, 0);
+            for (uint32_t sti = 0; sti < nst; ++sti) {
+                const RSec& ri = rsec[std::size_t(lb_in) * nps + sm.sector[sti]];
+                if (ri.rb == NONE) continue;
+                rsin_t[sti] = ri.rs;
+                for (std::size_t k = 0; k < nu; ++k) {
+                    cir_t[sti * nu + k] = Rci[std::size_t(ri.rb) * nr + units[k].rb_out];
+                    job_t[sti * nu + k] = tj[std::size_t(sti) * nr + units[k].rb_out];
+                }
+            }
+            const int64_t* Roff = R.offsets.data();
+            const double* Rcs = R.cscale.data();
+            const std::size_t Raux = R.aux;
             std::size_t n_alpha = 0;
             for (uint32_t b1 = 0; b1 < W.rows; ++b1) {
                 if (!L.has_block(ci, b1)) continue;
-                uint32_t left_idx = uint32_t(L.offset(ci, b1) / (int64_t(ls_in) * ls_out));
-                double lscale = L.conj_scale(ci, b1);
+                const uint32_t bpos = uint32_t(L.offset(ci, b1) / (int64_t(ls_in) * ls_out));
+                const double lsc = L.conj_scale(ci, b1);
                 for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
-                    uint32_t b2 = W.b2[e];
-                    const auto& by_out = op_by_out[W.op[e]];
-                    for (uint32_t s = 0; s < phys.size(); ++s) {
-                        Charge rc_out = lc_out + phys[s].first;
-                        if (!right.has(rc_out)) continue;
-                        for (const OE& oe : by_out[s]) {
-                            Charge phys_in = phys[sm.sector[oe.in]].first;
-                            Charge rc_in = lc_in + phys_in;
-                            uint32_t ci_r = R.cohort_index(rc_in, rc_out);
-                            if (!R.has_block(ci_r, b2)) continue;
-                            std::size_t rbi = right.position(rc_in);
-                            if (rbi == right.size()) continue;
-                            uint32_t rs_in = uint32_t(right[rbi].second);
-                            uint32_t in_off = uint32_t(rpb(phys_in, rc_in));
-                            uint32_t mps_off = in_off + uint32_t(sm.sub[oe.in]) * rs_in;
-                            auto it = tmap.find((uint64_t(mps_off) << 32) | ci_r);
-                            if (it == tmap.end()) continue;
-                            uint32_t col = uint32_t(R.offset(ci_r, b2) / rs_in);
-                            double a = oe.v * R.conj_scale(ci_r, b2) * W.scale[e] * lscale;
-                            const TJobD& tj = p->tjobs[it->second];
-                            int u = unit_of_state[oe.out];
-                            units[u].lines[left_idx].push_back({a, tj.c_off + uint64_t(col) * ls_in});
-                            if (bookkeeping) {
-                                auto& bk = units[u].bk[left_idx];
-                                bk.push_back(mps_off); bk.push_back(ci_r); bk.push_back(col);
-                            }
-                            ++n_alpha;
-                        }
+                    const uint32_t b2 = W.b2[e], op = W.op[e];
+                    const double wsc = W.scale[e] * lsc;
+                    for (uint32_t k = optr[op]; k < optr[op + 1]; ++k) {
+                        const int u = unit_of[oout[k]];
+                        if (u < 0) continue;
+                        const uint32_t sti = oin[k];
+                        const uint32_t cir = cir_t[sti * nu + u];
+                        if (cir == NONE) continue;
+                        const int64_t roff = Roff[cir * Raux + b2];
+                        if (roff < 0) continue;
+                        const uint32_t job = job_t[sti * nu + u];
+                        if (job == NONE) continue;
+                        U& un = units[u];
+                        const uint32_t col = uint32_t(roff / rsin_t[sti]);
+                        if (un.lines.empty() || un.lines.back() != bpos) un.lines.push_back(bpos);
+                        un.em.push_back(Em{uint32_t(un.lines.size() - 1), job_pos0[job] + col / un.ms,
+                                           oval[k] * Rcs[cir * Raux + b2] * wsc, P.tjob_mps[job], cir, col});
+                        ++n_alpha;
                     }
                 }
             }
             if (n_alpha == 0) continue;
-            uint32_t K_c = nS * ls_in;
-            uint64_t s_off = p->s_len;
-            p->s_len += (uint64_t(K_c) * stripe + 31) / 32 * 32;
-            for (auto& u : units) {
-                // unit GEMM data: lines (b1 rows with coefficients), distinct T slices, entries by slice
-                std::vector<uint32_t> lines;
-                std::unordered_map<uint64_t, uint32_t> kidx;  // T offset -> slice index
-                std::vector<uint64_t> slices;
-                std::vector<std::vector<std::pair<uint32_t, double>>> by_slice;
-                std::size_t nu = 0;
-                for (uint32_t b = 0; b < nS; ++b) {
-                    auto& ln = u.lines[b];
-                    if (ln.empty()) continue;
-                    uint32_t li = uint32_t(lines.size());
-                    lines.push_back(b);
-                    nu += ln.size();
-                    for (std::size_t k = 0; k < ln.size(); ++k) {
-                        auto ins = kidx.emplace(ln[k].second, uint32_t(slices.size()));
-                        if (ins.second) { slices.push_back(ln[k].second); by_slice.emplace_back(); }
-                        by_slice[ins.first->second].push_back({li, ln[k].first});
-                        if (bookkeeping) {
-                            const auto& bk = u.bk[b];
-                            uint32_t row[10] = {lb_in, lb_out, ci, ci_eff, u.offset, u.ms, b, bk[3 * k], bk[3 * k + 1], bk[3 * k + 2]};
-                            p->bk_int.insert(p->bk_int.end(), row, row + 10);
-                            p->bk_alpha.push_back(ln[k].first);
-                        }
-                    }
+            const uint64_t s_off = P.s_len;
+            P.s_len += (uint64_t(K_c) * stripe + 31) / 32 * 32;
+            for (U& u : units) {
+                P.flops_s += 2.0 * ls_in * u.ms * double(u.em.size());
+                if (u.em.empty()) continue;
+                // number the unit's slices in first-use order
+                std::vector<uint32_t> slices;
+                for (Em& m : u.em) {
+                    uint32_t& sl = slot[m.slice];
+                    if (sl == NONE) { sl = uint32_t(slices.size()); slices.push_back(m.slice); }
                 }
-                p->flops_s += 2.0 * ls_in * u.ms * double(nu);
-                if (lines.empty() || ls_in == 0 || u.ms == 0) continue;
                 UnitD ud{};
                 ud.s_off = s_off + uint64_t(u.offset) * K_c;
                 ud.ldS = K_c; ud.ls = ls_in; ud.ne = ls_in * u.ms;
-                ud.nl = uint32_t(lines.size()); ud.line0 = uint32_t(p->line_b1.size());
-                ud.nk = uint32_t(slices.size()); ud.slice0 = uint32_t(p->slice_off.size());
-                ud.sptr0 = uint32_t(p->sptr.size());
-                p->line_b1.insert(p->line_b1.end(), lines.begin(), lines.end());
-                p->slice_off.insert(p->slice_off.end(), slices.begin(), slices.end());
-                for (uint32_t k = 0; k < ud.nk; ++k) {
-                    p->sptr.push_back(uint32_t(p->went.size()));
-                    for (auto& e : by_slice[k]) p->went.push_back(WEntD{e.first, k, e.second});
+                ud.nl = uint32_t(u.lines.size()); ud.line0 = uint32_t(P.line_b1.size());
+                ud.nk = uint32_t(slices.size()); ud.slice0 = uint32_t(P.slice_off.size());
+                ud.sptr0 = uint32_t(P.sptr.size());
+                P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
+                for (uint32_t gp : slices) {
+                    // slot -> (job, b2 position) -> T offset of the slice
+                    uint32_t job = uint32_t(std::upper_bound(job_pos0.begin(), job_pos0.end(), gp) - job_pos0.begin()) - 1;
+                    uint32_t pos = gp - job_pos0[job];
+                    P.slice_off.push_back(P.tjobs[job].c_off + uint64_t(pos) * u.ms * ls_in);
                 }
-                p->sptr.push_back(uint32_t(p->went.size()));
-                int sh = shape_for_rows(ud.nl);
-                uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
-                for (uint32_t n0 = 0; n0 < ud.ne; n0 += bn)
-                    for (uint32_t m0 = 0; m0 < ud.nl; m0 += bm) p->utiles[sh].push_back(TileD{uint32_t(p->units.size()), m0, n0, 0});
-                p->units.push_back(ud);
-                p->g_elems += uint64_t(ls_in) * u.ms * ud.nl;
-                p->g_reads += uint64_t(ls_in) * u.ms * nu;
-                p->flops_sdense += 2.0 * ud.nl * ud.nk * double(ud.ne);
-            }
-            p->flops_ls += 2.0 * ls_out * ls_in * double(nS) * stripe;
-            SegD sg{};
-            sg.l_off = Lb.idx.data_off[ci_eff];
-            sg.s_off = s_off;
-            sg.ls_in = ls_in; sg.nS = nS; sg.tr = (ci != ci_eff) ? 1 : 0;
-            seg_tmp.push_back({lb_out, sg});
-        }
-    }
-    // group segments per output block; inside a block they stay in lb_in order
-    {
-        std::vector<std::vector<SegD>> per_out(left.size());
-        for (std::size_t i = 0; i < seg_tmp.size(); ++i) per_out[seg_tmp[i].first].push_back(seg_tmp[i].second);
-        for (uint32_t lb_out = 0; lb_out < left.size(); ++lb_out) {
-            if (per_out[lb_out].empty()) continue;
-            OutD o{};
-            o.y_off = p->x_off[lb_out];
-            o.M = uint32_t(left[lb_out].second);
-            o.N = p->x_cols[lb_out];
-            o.seg_start = uint32_t(p->segs.size());
-            o.seg_count = uint32_t(per_out[lb_out].size());
-            p->segs.insert(p->segs.end(), per_out[lb_out].begin(), per_out[lb_out].end());
-            if (o.M && o.N) {
-                int sh = shape_for_rows(o.M);
-                uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
-                for (uint32_t n0 = 0; n0 < o.N; n0 += bn)
-                    for (uint32_t m0 = 0; m0 < o.M; m0 += bm) {
-                        OTileD t{};
-                        t.out = uint32_t(p->outs.size()); t.m0 = m0; t.n0 = n0;
-                        t.part0 = uint32_t(p->kitems[sh].size());
-                        for (uint32_t sg = o.seg_start; sg < o.seg_start + o.seg_count; ++sg) {
-                            uint32_t Kc = p->segs[sg].nS * p->segs[sg].ls_in;
-                            for (uint32_t k0 = 0; k0 < Kc; k0 += KCHUNK)
-                                p->kitems[sh].push_back(KItemD{uint32_t(p->otiles[sh].size()), sg, k0, std::min(Kc, k0 + KCHUNK)});
-                        }
-                        t.nparts = uint32_t(p->kitems[sh].size()) - t.part0;
-                        p->otiles[sh].push_back(t);
+                // entries sorted by slice (counting sort)
+                std::vector<uint32_t> cnt(ud.nk + 1, 0);
+                for (Em& m : u.em) cnt[slot[m.slice] + 1]++;
+                for (uint32_t k = 0; k < ud.nk; ++k) cnt[k + 1] += cnt[k];
+                const uint32_t w0 = uint32_t(P.went.size());
+                for (uint32_t k = 0; k <= ud.nk; ++k) P.sptr.push_back(w0 + cnt[k]);
+                P.went.resize(w0 + u.em.size());
+                std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
+                for (Em& m : u.em) {
+                    uint32_t k = slot[m.slice];
+                    P.went[w0 + fill[k]++] = WEntD{m.line, k, m.a};
+                }
+                if (bookkeeping)
+                    for (Em& m : u.em) {
+                        uint32_t row[10] = {lb_in, lb_out, ci, ce, u.offset, u.ms, u.lines[m.line], m.mps, m.cir, m.col};
+                        P.bk_int.insert(P.bk_int.end(), row, row + 10);
+                        P.bk_alpha.push_back(m.a);
                     }
+                for (uint32_t gp : slices) slot[gp] = NONE;
+                P.units.push_back(ud);
+                P.g_elems += uint64_t(ud.ne) * ud.nl;
+                P.g_reads += uint64_t(ud.ne) * u.em.size();
+                P.flops_sdense += 2.0 * ud.nl * ud.nk * double(ud.ne);
             }
-            p->outs.push_back(o);
+            P.flops_ls += 2.0 * ls_out * ls_in * double(nS) * stripe;
+            SegD sg{};
+            sg.l_off = L.data_off[ce];
+            sg.s_off = s_off;
+            sg.ls_in = ls_in; sg.nS = nS; sg.tr = (ci != ce) ? 1 : 0;
+            P.segs.push_back({lb_out, sg});
         }
     }
+
+    const double t_b = tnow();
+    // ---- merge the parts in ket-sector order: prefix offsets, one allocation, parallel copy ----
+    struct Base { uint64_t t, s; uint32_t job, unit, line, slice, sptr, went; std::size_t bk; };
+    std::vector<Base> base(nl + 1);
+    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (uint32_t i = 0; i < nl; ++i) {
+        const Part& P = parts[i];
+        base[i + 1] = Base{base[i].t + P.t_len, base[i].s + P.s_len, base[i].job + uint32_t(P.tjobs.size()),
+                           base[i].unit + uint32_t(P.units.size()), base[i].line + uint32_t(P.line_b1.size()),
+                           base[i].slice + uint32_t(P.slice_off.size()), base[i].sptr + uint32_t(P.sptr.size()),
+                           base[i].went + uint32_t(P.went.size()), base[i].bk + P.bk_alpha.size()};
+    }
+    const Base& tot = base[nl];
+    p->tjobs.resize(tot.job);
+    p->units.resize(tot.unit);
+    p->line_b1.resize(tot.line);
+    p->slice_off.resize(tot.slice);
+    p->sptr.resize(tot.sptr);
+    p->went.resize(tot.went);
+    if (bookkeeping) { p->bk_int.resize(tot.bk * 10); p->bk_alpha.resize(tot.bk); }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int ii = 0; ii < int(nl); ++ii) {
+        Part& P = parts[ii];
+        const Base& B = base[ii];
+        for (std::size_t k = 0; k < P.tjobs.size(); ++k) { TJobD j = P.tjobs[k]; j.c_off += B.t; p->tjobs[B.job + k] = j; }
+        for (std::size_t k = 0; k < P.units.size(); ++k) {
+            UnitD u = P.units[k];
+            u.s_off += B.s; u.line0 += B.line; u.slice0 += B.slice; u.sptr0 += B.sptr;
+            p->units[B.unit + k] = u;
+        }
+        std::copy(P.line_b1.begin(), P.line_b1.end(), p->line_b1.begin() + B.line);
+        for (std::size_t k = 0; k < P.slice_off.size(); ++k) p->slice_off[B.slice + k] = P.slice_off[k] + B.t;
+        for (std::size_t k = 0; k < P.sptr.size(); ++k) p->sptr[B.sptr + k] = P.sptr[k] + B.went;
+        std::copy(P.went.begin(), P.went.end(), p->went.begin() + B.went);
+        if (bookkeeping) {
+            std::copy(P.bk_int.begin(), P.bk_int.end(), p->bk_int.begin() + B.bk * 10);
+            std::copy(P.bk_alpha.begin(), P.bk_alpha.end(), p->bk_alpha.begin() + B.bk);
+        }
+        for (auto& sg : P.segs) sg.second.s_off += B.s;
+        P.tjobs = {}; P.tjob_mps = {}; P.units = {}; P.line_b1 = {}; P.slice_off = {}; P.sptr = {}; P.went = {};
+        P.bk_int = {}; P.bk_alpha = {};
+    }
+    p->t_len = tot.t;
+    p->s_len = tot.s;
+    std::vector<std::vector<SegD>> per_out(nl);
+    for (uint32_t i = 0; i < nl; ++i) {
+        const Part& P = parts[i];
+        for (auto& sg : P.segs) per_out[sg.first].push_back(sg.second);
+        p->flops_t += P.flops_t; p->flops_s += P.flops_s; p->flops_ls += P.flops_ls; p->flops_sdense += P.flops_sdense;
+        p->g_elems += P.g_elems; p->g_reads += P.g_reads;
+    }
+    for (uint32_t j = 0; j < p->tjobs.size(); ++j)
+        if (p->tjobs[j].M && p->tjobs[j].N) add_tiles(p->ttiles, j, p->tjobs[j].M, p->tjobs[j].N);
+    for (uint32_t k = 0; k < p->units.size(); ++k) {
+        const UnitD& u = p->units[k];
+        int sh = shape_for_rows(u.nl);
+        uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
+        for (uint32_t n0 = 0; n0 < u.ne; n0 += bn)
+            for (uint32_t m0 = 0; m0 < u.nl; m0 += bm) p->utiles[sh].push_back(TileD{k, m0, n0, 0});
+    }
+    // output blocks, their segments (lb_in order) and split-K items
+    for (uint32_t lb_out = 0; lb_out < nl; ++lb_out) {
+        if (per_out[lb_out].empty()) continue;
+        OutD o{};
+        o.y_off = p->x_off[lb_out];
+        o.M = uint32_t(left[lb_out].second);
+        o.N = p->x_cols[lb_out];
+        o.seg_start = uint32_t(p->segs.size());
+        o.seg_count = uint32_t(per_out[lb_out].size());
+        p->segs.insert(p->segs.end(), per_out[lb_out].begin(), per_out[lb_out].end());
+        if (o.M && o.N) {
+            int sh = shape_for_rows(o.M);
+            uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
+            for (uint32_t n0 = 0; n0 < o.N; n0 += bn)
+                for (uint32_t m0 = 0; m0 < o.M; m0 += bm) {
+                    OTileD t{};
+                    t.out = uint32_t(p->outs.size()); t.m0 = m0; t.n0 = n0;
+                    t.part0 = uint32_t(p->kitems[sh].size());
+                    for (uint32_t sg = o.seg_start; sg < o.seg_start + o.seg_count; ++sg) {
+                        uint32_t Kc = p->segs[sg].nS * p->segs[sg].ls_in;
+                        for (uint32_t k0 = 0; k0 < Kc; k0 += KCHUNK)
+                            p->kitems[sh].push_back(KItemD{uint32_t(p->otiles[sh].size()), sg, k0, std::min(Kc, k0 + KCHUNK)});
+                    }
+                    t.nparts = uint32_t(p->kitems[sh].size()) - t.part0;
+                    p->otiles[sh].push_back(t);
+                }
+        }
+        p->outs.push_back(o);
+    }
+    if (tdbg) std::fprintf(stderr, "plan: tables+parts %.3f s, merge %.3f s\n", t_b - t_a, tnow() - t_b);
     uint64_t pl = 0;
     for (int sh = 0; sh < N_SHAPES; ++sh) pl = std::max<uint64_t>(pl, uint64_t(p->kitems[sh].size()) * shape_bm(sh) * shape_bn(sh));
     p->p_len = pl;
