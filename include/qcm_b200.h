@@ -174,6 +174,77 @@ void qcm_heff_free(qcm_heff* h);
 #define QCM_NOALLOC_SCRATCH_DOUBLES (8u * 1024u * 1024u)
 int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, double* y_dev);
 
+/* ------------------------------------------------------------------------ */
+/* Eigensolver, boundary propagation and the two-site sweep                   */
+/* ------------------------------------------------------------------------ */
+
+/* Lowest eigenpair of H_eff by Jacobi-Davidson (no GMRES inner solve), start
+ * vector x0, eigenvector to out (host buffers of vec_len doubles, the
+ * qcm_heff_apply layout); search space and updates in HBM.  Replaces
+ * solve<double>(out, initial, SH, ortho = {}, jcd_gmres = 0, tol, maxiter)
+ * (solver/solver.cpp:14-28 -> solve_ietl_jcd, ietl_jacobi_davidson.h:35-76,
+ * ietl/jacobi.h:386-474).  Returns the eigenvalue in *eval (no core energy). */
+int qcm_jd_solve(qcm_heff* h, const double* x0, double tol, int maxiter, double* out, double* eval, int* iters);
+
+/* New environment from one MPS site tensor, given right-paired (its blocks
+ * ls x stripe, column-major, concatenated in left-sector order, as for
+ * qcm_heff_apply), with bra = ket.  mpo: single-site MPO, tensor `site`.
+ * symmetric != 0 applies the Hermitian complement (complement_transpose).
+ * Replace contraction::Engine::overlap_mpo_left_step / overlap_mpo_right_step
+ * (contractions/engine.hpp:54-71, boundary_ops/move_boundary.hpp:147-404). */
+int qcm_boundary_step_left(qcm_ctx* ctx, const qcm_boundary* L, const qcm_mpo* mpo, int site, const qcm_mps_desc* mps,
+                           const double* data_rp, int symmetric, qcm_boundary** out);
+int qcm_boundary_step_right(qcm_ctx* ctx, const qcm_boundary* R, const qcm_mpo* mpo, int site, const qcm_mps_desc* mps,
+                            const double* data_rp, int symmetric, qcm_boundary** out);
+
+typedef struct {
+    uint32_t n_bra, n_ket, n_cohorts, aux_dim;
+    uint64_t total;    /* doubles in the device buffer (cohorts start on 32-element boundaries) */
+    uint32_t resident; /* 1 if the boundary holds device data */
+} qcm_boundary_info;
+int qcm_boundary_get_info(const qcm_boundary* b, qcm_boundary_info* info);
+/* Copy the index and data of a boundary to host arrays sized from
+ * qcm_boundary_get_info (n_cohorts, n_cohorts * aux_dim, total); any pointer
+ * may be NULL.  Same fields as qcm_boundary_desc. */
+int qcm_boundary_download(const qcm_boundary* b, qcm_sector* bra, qcm_sector* ket, uint32_t* cohort_bra,
+                          uint32_t* cohort_ket, uint8_t* tr, uint32_t* n_blocks, int64_t* offsets, double* cscale,
+                          uint64_t* data_offset, double* data);
+
+/* Two-site ground-state DMRG with the whole step on the device (H_eff plan,
+ * JD, SVD truncation, QR/LQ canonisation, boundary step).  Replaces
+ * ts_optimize<Matrix, SymmGroup, Storage> (optimize/ts_optimize.hpp:62-362)
+ * with init_state = const (mp_tensors/mps_initializers.h:84-100). */
+typedef struct qcm_dmrg qcm_dmrg;
+typedef struct {
+    uint64_t max_bond_dimension;  /* max_bond_dimension */
+    uint64_t init_bond_dimension; /* init_bond_dimension */
+    double truncation_cutoff;     /* truncation_final */
+    double jcd_tol;               /* ietl_jcd_tol */
+    int32_t jcd_maxiter;          /* ietl_jcd_maxiter (1..64) */
+    double ecore;                 /* added to the reported energies */
+} qcm_dmrg_params;
+/* block_matrix_algorithms.h:48-63 */
+typedef struct {
+    uint64_t bond_dimension;
+    double truncated_weight, truncated_fraction, smallest_ev;
+} qcm_trunc_result;
+typedef struct {
+    uint64_t hpsi_count;
+    double hpsi_flops; /* reference flop count (ScheduleNew::total_flops) summed over the applies */
+    double plan_s, jd_s, trunc_s, boundary_s, total_s; /* wall time per phase, summed over sweeps */
+} qcm_dmrg_stats;
+
+/* mpo: single-site QC MPO; nup/ndown: u1_total_charge1/2.  Builds the const
+ * MPS, canonises it to site 0 and the right boundaries. */
+int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const qcm_dmrg_params* params, qcm_dmrg** out);
+int qcm_dmrg_length(const qcm_dmrg* d);
+/* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL). */
+int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);
+int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* stats);
+/* Current bond dimensions (right basis size of sites 0 .. L-2). */
+int qcm_dmrg_bond_dimensions(const qcm_dmrg* d, uint64_t* dims);
+void qcm_dmrg_free(qcm_dmrg* d);
+
 /* FP64 throughput probes on the current device (TFLOP/s): DMMA (mma.sync
  * m8n8k4 .f64) and DFMA loops.  Roofline denominators of the FP64 form. */
 int qcm_probe_fp64_peaks(double* dmma_tflops, double* dfma_tflops);

@@ -89,6 +89,34 @@ int orc_dmrg_sweep(orc_dmrg* h, int sweep, double* energies, double* tw, double*
     } catch (const std::exception& e) { return fail(e.what()); }
 }
 
+// Boundary step case from the current state (call after a sweep stopped at a step of the
+// left-to-right half): side 0 = overlap_mpo_left_step(mps[site], left_[site]),
+// side 1 = overlap_mpo_right_step(mps[site], right_[site + 1]); free with orc_free.
+int orc_dmrg_boundary_export(orc_dmrg* h, int side, int site, void** out, size_t* len) {
+    try {
+        DMRG& d = *h->d;
+        if (site < 0 || site >= d.L) return fail("orc_dmrg_boundary_export: site out of range");
+        auto same = [](const Index& a, const Index& b) {
+            if (a.size() != b.size()) return false;
+            for (std::size_t i = 0; i < a.size(); ++i)
+                if (!(a[i].first == b[i].first) || a[i].second != b[i].second) return false;
+            return true;
+        };
+        if (side == 0) {
+            const Boundary& in = d.left_[site];
+            if (!same(in.index.bra, d.mps[site].left)) return fail("orc_dmrg_boundary_export: left boundary does not match the site");
+            Boundary res = overlap_mpo_left_step(d.mps[site], d.mps[site], in, d.mpo[site], true);
+            *out = dup_blob(save_boundary_step(0, site, d.mps[site], in, res), len);
+        } else {
+            const Boundary& in = d.right_[site + 1];
+            if (!same(in.index.bra, d.mps[site].right)) return fail("orc_dmrg_boundary_export: right boundary does not match the site");
+            Boundary res = overlap_mpo_right_step(d.mps[site], d.mps[site], in, d.mpo[site], true);
+            *out = dup_blob(save_boundary_step(1, site, d.mps[site], in, res), len);
+        }
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
 // [hpsi_count, hpsi_time, hpsi_flops, jd_time, schedule_time, trunc_time, boundary_time]
 int orc_dmrg_stats(orc_dmrg* h, double* out) {
     DMRG& d = *h->d;

@@ -582,6 +582,26 @@ std::vector<uint8_t> save_site_problem(const MPSTensor& twin0, const Boundary& L
     return w.b;
 }
 
+std::vector<uint8_t> save_boundary_step(int side, int site, const MPSTensor& m0, const Boundary& in, const Boundary& out) {
+    MPSTensor m = m0;
+    m.make_right_paired();
+    W w;
+    w.put<uint32_t>(0x50534251u);  // "QBSP"
+    w.put<uint32_t>(1);
+    w.put<uint32_t>(uint32_t(side));
+    w.put<uint32_t>(uint32_t(site));
+    w.idx(m.phys); w.idx(m.left); w.idx(m.right);
+    w.put<uint32_t>(uint32_t(m.data.n_blocks()));
+    for (std::size_t k = 0; k < m.data.n_blocks(); ++k) {
+        w.put<int32_t>(m.data.lc[k].n[0]); w.put<int32_t>(m.data.lc[k].n[1]);
+        w.put<uint32_t>(uint32_t(m.data.b[k].r)); w.put<uint32_t>(uint32_t(m.data.b[k].c));
+        for (double v : m.data.b[k].d) w.put<double>(v);
+    }
+    w.bnd(in);
+    w.bnd(out);
+    return w.b;
+}
+
 void load_site_problem(const uint8_t* p, std::size_t n, MPSTensor& twin, Boundary& Lb, Boundary& Rb) {
     R r{p, n};
     if (r.get<uint32_t>() != 0x42505351u || r.get<uint32_t>() != 1) throw std::runtime_error("bad site problem blob");

@@ -51,6 +51,7 @@ def lib(nthreads: int = 0):
         L.orc_dmrg_sweep.argtypes = [c_void_p, c_int, P(c_double), P(c_double), P(c_double), P(ctypes.c_uint64), c_int,
                                      P(c_void_p), P(c_size_t)]
         L.orc_dmrg_stats.argtypes = [c_void_p, P(c_double)]
+        L.orc_dmrg_boundary_export.argtypes = [c_void_p, c_int, c_int, P(c_void_p), P(c_size_t)]
         L.orc_heff_apply.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), P(c_double), c_size_t,
                                      c_int, P(c_double), P(c_double)]
         L.orc_schedule_export.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_void_p), P(c_size_t),
@@ -96,6 +97,15 @@ class OracleDMRG:
         p, n = c_void_p(), c_size_t()
         _check(self.lib, self.lib.orc_dmrg_sweep(self.h, sweep, None, None, None, None, step, ctypes.byref(p),
                                                  ctypes.byref(n)))
+        b = ctypes.string_at(p, n.value)
+        self.lib.orc_free(p)
+        return b
+
+    def boundary_export(self, side: int, site: int) -> bytes:
+        """Boundary step case ("QBSP" v1) from the current state: side 0 = left step of
+        mps[site] from left_[site], side 1 = right step of mps[site] from right_[site + 1]."""
+        p, n = c_void_p(), c_size_t()
+        _check(self.lib, self.lib.orc_dmrg_boundary_export(self.h, side, site, ctypes.byref(p), ctypes.byref(n)))
         b = ctypes.string_at(p, n.value)
         self.lib.orc_free(p)
         return b

@@ -1,0 +1,222 @@
+// C-ABI: Jacobi-Davidson solve, boundary steps, boundary download and the two-site sweep.
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "../../include/qcm_b200.h"
+#include "capi_types.hpp"
+#include "capi_util.hpp"
+#include "dmrg_dev.hpp"
+
+namespace qcm {
+const MPO& mpo_of(const qcm_mpo* m);
+}
+
+struct qcm_dmrg {
+    qcm_ctx* ctx = nullptr;
+    std::unique_ptr<qcm::DevDMRG> e;
+};
+
+namespace {
+
+qcm::Index to_index(uint32_t n, const qcm_sector* s) {
+    qcm::Index r;
+    for (uint32_t i = 0; i < n; ++i) r.d.push_back({qcm::Charge(s[i].a, s[i].b), s[i].size});
+    for (std::size_t i = 1; i < r.d.size(); ++i)
+        if (!(r.d[i - 1].first > r.d[i].first)) throw std::runtime_error("sector list must be in strictly descending charge order");
+    return r;
+}
+
+// right-paired MPS tensor from packed host blocks (left-sector order, ls x stripe each)
+qcm::DMPS upload_mps(qcm::Ctx& c, const qcm_mps_desc* d, const double* data) {
+    qcm::DMPS t;
+    t.phys = to_index(d->n_phys, d->phys);
+    t.left = to_index(d->n_left, d->left);
+    t.right = to_index(d->n_right, d->right);
+    t.right_paired = true;
+    t.b = qcm::layout_right_paired(t.phys, t.left, t.right);
+    t.b.allocate(c.s, true);
+    uint64_t h = 0;
+    for (std::size_t k = 0; k < t.b.n(); ++k) {
+        const uint64_t n = t.b.elems(k);
+        QCM_CUDA(cudaMemcpyAsync(t.b.d.get() + t.b.off[k], data + h, n * sizeof(double), cudaMemcpyHostToDevice, c.s));
+        h += n;
+    }
+    return t;
+}
+
+int boundary_step(qcm_ctx* ctx, const qcm_boundary* B, const qcm_mpo* mpo, int site, const qcm_mps_desc* mps,
+                  const double* data_rp, int symmetric, bool left, qcm_boundary** out) {
+    QCM_TRY
+    if (!ctx || !B || !mpo || !mps || !data_rp || !out) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_step: NULL argument");
+    if (!B->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_step: boundary is not resident");
+    const qcm::MPO& m = qcm::mpo_of(mpo);
+    if (m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_step: expected a single-site MPO");
+    if (site < 0 || std::size_t(site) >= m.t.size()) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_step: site out of range");
+    const qcm::MPOTensor& W = m.t[site];
+    if ((left ? W.rows : W.cols) != B->b.idx.aux)
+        return qcm::fail(QCM_ERR_ARG, "qcm_boundary_step: MPO bond dimension does not match the boundary");
+    QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::Ctx c;
+    c.s = ctx->stream;
+    qcm::DMPS ket = upload_mps(c, mps, data_rp);
+    auto res = std::make_unique<qcm_boundary>();
+    res->ctx = ctx;
+    std::unique_ptr<qcm::DevBoundary> nb;
+    if (left) {
+        qcm::DMPS bra = qcm::right_paired_copy(c, ket);
+        qcm::make_left_paired(c, bra);
+        nb = qcm::boundary_step_left(c, B->b, ket, bra, W, symmetric != 0);
+    } else {
+        nb = qcm::boundary_step_right(c, B->b, ket, W, symmetric != 0);
+    }
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    res->b.idx = std::move(nb->idx);
+    res->b.data = std::move(nb->data);
+    *out = res.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+
+void fill_sectors(const qcm::Index& x, qcm_sector* out) {
+    for (std::size_t i = 0; i < x.size(); ++i)
+        out[i] = qcm_sector{x[i].first.a, x[i].first.b, uint32_t(x[i].second)};
+}
+
+}  // namespace
+
+extern "C" {
+
+int qcm_jd_solve(qcm_heff* h, const double* x0, double tol, int maxiter, double* out, double* eval, int* iters) {
+    QCM_TRY
+    if (!h || !x0 || !out || !eval) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: NULL argument");
+    if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: host-only plan");
+    if (maxiter < 1 || maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: maxiter must be in 1..64");
+    qcm::HeffPlan& p = *h->p;
+    qcm::Ctx c;
+    c.s = p.stream;
+    qcm::DBuf<double> x(p.x_len ? p.x_len : 1);
+    QCM_CUDA(cudaMemcpyAsync(x.get(), x0, p.x_len * sizeof(double), cudaMemcpyHostToDevice, c.s));
+    int it = 0;
+    *eval = qcm::jacobi_davidson(c, p, x.get(), tol, maxiter, it);
+    QCM_CUDA(cudaMemcpyAsync(out, x.get(), p.x_len * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    if (iters) *iters = it;
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_boundary_step_left(qcm_ctx* ctx, const qcm_boundary* L, const qcm_mpo* mpo, int site, const qcm_mps_desc* mps,
+                           const double* data_rp, int symmetric, qcm_boundary** out) {
+    return boundary_step(ctx, L, mpo, site, mps, data_rp, symmetric, true, out);
+}
+
+int qcm_boundary_step_right(qcm_ctx* ctx, const qcm_boundary* R, const qcm_mpo* mpo, int site, const qcm_mps_desc* mps,
+                            const double* data_rp, int symmetric, qcm_boundary** out) {
+    return boundary_step(ctx, R, mpo, site, mps, data_rp, symmetric, false, out);
+}
+
+int qcm_boundary_get_info(const qcm_boundary* b, qcm_boundary_info* info) {
+    if (!b || !info) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_get_info: NULL argument");
+    const qcm::BoundaryIndexH& x = b->b.idx;
+    info->n_bra = uint32_t(x.bra.size());
+    info->n_ket = uint32_t(x.ket.size());
+    info->n_cohorts = x.n_cohorts();
+    info->aux_dim = x.aux;
+    info->total = x.total;
+    info->resident = b->ctx ? 1 : 0;
+    return QCM_OK;
+}
+
+int qcm_boundary_download(const qcm_boundary* b, qcm_sector* bra, qcm_sector* ket, uint32_t* cohort_bra,
+                          uint32_t* cohort_ket, uint8_t* tr, uint32_t* n_blocks, int64_t* offsets, double* cscale,
+                          uint64_t* data_offset, double* data) {
+    QCM_TRY
+    if (!b) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_download: NULL boundary");
+    const qcm::BoundaryIndexH& x = b->b.idx;
+    const std::size_t nc = x.n_cohorts(), na = std::size_t(nc) * x.aux;
+    if (bra) fill_sectors(x.bra, bra);
+    if (ket) fill_sectors(x.ket, ket);
+    if (cohort_bra) std::memcpy(cohort_bra, x.cbra.data(), nc * sizeof(uint32_t));
+    if (cohort_ket) std::memcpy(cohort_ket, x.cket.data(), nc * sizeof(uint32_t));
+    if (tr) std::memcpy(tr, x.tr.data(), nc);
+    if (n_blocks) std::memcpy(n_blocks, x.nb.data(), nc * sizeof(uint32_t));
+    if (offsets) std::memcpy(offsets, x.offsets.data(), na * sizeof(int64_t));
+    if (cscale) std::memcpy(cscale, x.cscale.data(), na * sizeof(double));
+    if (data_offset) std::memcpy(data_offset, x.data_off.data(), nc * sizeof(uint64_t));
+    if (data) {
+        if (!b->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_download: boundary is not resident");
+        QCM_CUDA(cudaSetDevice(b->ctx->device));
+        if (x.total)
+            QCM_CUDA(cudaMemcpyAsync(data, b->b.data.get(), x.total * sizeof(double), cudaMemcpyDeviceToHost, b->ctx->stream));
+        QCM_CUDA(cudaStreamSynchronize(b->ctx->stream));
+    }
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const qcm_dmrg_params* prm, qcm_dmrg** out) {
+    QCM_TRY
+    if (!ctx || !mpo || !prm || !out) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: NULL argument");
+    const qcm::MPO& m = qcm::mpo_of(mpo);
+    if (m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: expected a single-site MPO");
+    if (prm->jcd_maxiter < 1 || prm->jcd_maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: jcd_maxiter must be in 1..64");
+    if (prm->max_bond_dimension < 1 || prm->init_bond_dimension < 1)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: bond dimensions must be positive");
+    QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::DMRGParams p;
+    p.Mmax = prm->max_bond_dimension;
+    p.init_bond_dimension = prm->init_bond_dimension;
+    p.cutoff = prm->truncation_cutoff;
+    p.jcd_tol = prm->jcd_tol;
+    p.jcd_maxiter = prm->jcd_maxiter;
+    p.ecore = prm->ecore;
+    qcm::MPO ts = qcm::make_twosite_mpo(m);
+    auto d = std::make_unique<qcm_dmrg>();
+    d->ctx = ctx;
+    d->e = std::make_unique<qcm::DevDMRG>(m.t, ts.t, nup, ndown, p, ctx->stream);
+    *out = d.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_length(const qcm_dmrg* d) { return d ? d->e->L : -1; }
+
+int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc) {
+    QCM_TRY
+    if (!d || !energies) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_sweep: NULL argument");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    std::vector<double> E;
+    std::vector<qcm::TruncResults> T;
+    d->e->sweep(E, T);
+    std::memcpy(energies, E.data(), E.size() * sizeof(double));
+    if (trunc)
+        for (std::size_t i = 0; i < T.size(); ++i)
+            trunc[i] = qcm_trunc_result{T[i].bond_dimension, T[i].truncated_weight, T[i].truncated_fraction, T[i].smallest_ev};
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* s) {
+    if (!d || !s) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_get_stats: NULL argument");
+    const qcm::DMRGStats& t = d->e->st;
+    s->hpsi_count = t.hpsi_count;
+    s->hpsi_flops = t.hpsi_flops;
+    s->plan_s = t.plan_s;
+    s->jd_s = t.jd_s;
+    s->trunc_s = t.trunc_s;
+    s->boundary_s = t.boundary_s;
+    s->total_s = t.total_s;
+    return QCM_OK;
+}
+
+int qcm_dmrg_bond_dimensions(const qcm_dmrg* d, uint64_t* dims) {
+    if (!d || !dims) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_bond_dimensions: NULL argument");
+    const qcm::DevDMRG& e = *d->e;
+    for (int i = 0; i + 1 < e.L; ++i) dims[i] = e.mps[i].right.sum_of_sizes();
+    return QCM_OK;
+}
+
+void qcm_dmrg_free(qcm_dmrg* d) { delete d; }
+
+}  // extern "C"

@@ -1,0 +1,417 @@
+// MPS tensors, two-site tensors and their factorizations on the device.
+//
+// Reshapes (mp_tensors/reshapes.h, mpstensor.hpp:211-240) are sub-block copies
+// between the left-paired ((phys x left) x right) and right-paired
+// (left x (phys x right)) forms; the two-site tensor (twositetensor.hpp:29-199,
+// ts_reshape.h) is the block product of a left-paired and a right-paired site
+// tensor, re-blocked over the fused physical index.  Truncation follows
+// svd_truncate / estimate_truncation (block_matrix_algorithms.h:136-240) with
+// the per-block SVDs on the device and the global cut on the host.
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+#include "dmrg_dev.hpp"
+
+namespace qcm {
+
+namespace {
+
+std::size_t find_block(const DBlocks& b, Charge c) {
+    for (std::size_t k = 0; k < b.n(); ++k) if (b.lc[k] == c) return k;
+    return b.n();
+}
+
+DMPS reshaped_left(Ctx& c, const DMPS& t) {
+    DMPS o;
+    o.phys = t.phys; o.left = t.left; o.right = t.right; o.right_paired = false;
+    o.b = layout_left_paired(t.phys, t.left, t.right);
+    o.b.allocate(c.s, true);
+    ProductBasis out_left(t.phys, t.left), in_right(t.phys, t.right, true);
+    std::vector<CopyJob> jobs;
+    for (std::size_t k = 0; k < o.b.n(); ++k) {
+        const Charge rc = o.b.rc[k];
+        const uint32_t rdim = o.b.cols[k];
+        for (std::size_t s = 0; s < t.phys.size(); ++s) {
+            const Charge p = t.phys[s].first, lc = rc - p;
+            const std::size_t lb = t.left.position(lc);
+            if (lb == t.left.size()) continue;
+            const std::size_t ks = find_block(t.b, lc);
+            if (ks == t.b.n()) continue;
+            const uint32_t ldim = uint32_t(t.left[lb].second);
+            if (t.b.rows[ks] != ldim) throw std::runtime_error("reshape: block rows differ from the left index");
+            const uint64_t ol = out_left(p, lc), ir = in_right(p, rc);
+            for (uint32_t ss = 0; ss < t.phys[s].second; ++ss)
+                jobs.push_back(CopyJob{t.b.off[ks] + (ir + uint64_t(ss) * rdim) * ldim, o.b.off[k] + ol + uint64_t(ss) * ldim,
+                                       ldim, rdim, ldim, o.b.rows[k], 0, 0});
+        }
+    }
+    batched_copy(jobs, t.b.d.get(), t.b.total, o.b.d.get(), o.b.total, c.cjobs, c.s);
+    return o;
+}
+
+DMPS reshaped_right(Ctx& c, const DMPS& t) {
+    DMPS o;
+    o.phys = t.phys; o.left = t.left; o.right = t.right; o.right_paired = true;
+    o.b = layout_right_paired(t.phys, t.left, t.right);
+    o.b.allocate(c.s, true);
+    ProductBasis in_left(t.phys, t.left), out_right(t.phys, t.right, true);
+    std::vector<CopyJob> jobs;
+    for (std::size_t k = 0; k < o.b.n(); ++k) {
+        const Charge lc = o.b.lc[k];
+        const uint32_t ldim = o.b.rows[k];
+        for (std::size_t s = 0; s < t.phys.size(); ++s) {
+            const Charge p = t.phys[s].first, rc = lc + p;
+            const std::size_t rb = t.right.position(rc);
+            if (rb == t.right.size()) continue;
+            const std::size_t ks = find_block(t.b, rc);
+            if (ks == t.b.n()) continue;
+            const uint32_t rdim = uint32_t(t.right[rb].second);
+            if (t.b.cols[ks] != rdim) throw std::runtime_error("reshape: block columns differ from the right index");
+            const uint64_t il = in_left(p, lc), orr = out_right(p, rc);
+            for (uint32_t ss = 0; ss < t.phys[s].second; ++ss)
+                jobs.push_back(CopyJob{t.b.off[ks] + il + uint64_t(ss) * ldim, o.b.off[k] + (orr + uint64_t(ss) * rdim) * ldim,
+                                       ldim, rdim, t.b.rows[ks], ldim, 0, 0});
+        }
+    }
+    batched_copy(jobs, t.b.d.get(), t.b.total, o.b.d.get(), o.b.total, c.cjobs, c.s);
+    return o;
+}
+
+Index sorted_basis(const std::vector<std::pair<Charge, std::size_t>>& v) {
+    Index r;
+    r.d = v;
+    r.sort();
+    return r;
+}
+
+}  // namespace
+
+DBlocks layout_right_paired(const Index& phys, const Index& left, const Index& right, bool packed) {
+    ProductBasis pb(phys, right, true);
+    DBlocks b;
+    for (std::size_t lb = 0; lb < left.size(); ++lb) {
+        const Charge c = left[lb].first;
+        const std::size_t n = pb.size(c);
+        if (n == 0 || left[lb].second == 0) continue;
+        b.add(c, c, uint32_t(left[lb].second), uint32_t(n), packed);
+    }
+    return b;
+}
+
+DBlocks layout_left_paired(const Index& phys, const Index& left, const Index& right) {
+    ProductBasis pb(phys, left);
+    DBlocks b;
+    for (std::size_t rb = 0; rb < right.size(); ++rb) {
+        const Charge c = right[rb].first;
+        const std::size_t n = pb.size(c);
+        if (n == 0 || right[rb].second == 0) continue;
+        b.add(c, c, uint32_t(n), uint32_t(right[rb].second));
+    }
+    return b;
+}
+
+void make_left_paired(Ctx& c, DMPS& t) {
+    if (!t.right_paired) return;
+    t = reshaped_left(c, t);
+}
+
+void make_right_paired(Ctx& c, DMPS& t) {
+    if (t.right_paired) return;
+    t = reshaped_right(c, t);
+}
+
+DMPS right_paired_copy(Ctx& c, const DMPS& t) {
+    if (!t.right_paired) return reshaped_right(c, t);
+    DMPS o;
+    o.phys = t.phys; o.left = t.left; o.right = t.right; o.right_paired = true;
+    o.b.lc = t.b.lc; o.b.rc = t.b.rc; o.b.rows = t.b.rows; o.b.cols = t.b.cols; o.b.off = t.b.off; o.b.total = t.b.total;
+    o.b.allocate(c.s, false);
+    QCM_CUDA(cudaMemcpyAsync(o.b.d.get(), t.b.d.get(), std::max<uint64_t>(t.b.total, 1) * sizeof(double),
+                             cudaMemcpyDeviceToDevice, c.s));
+    return o;
+}
+
+double norm2(Ctx& c, const DBlocks& b) {
+    if (!b.total) return 0.0;
+    Ctx::ensure(c.scal, 64);
+    dev_dots(b.d.get(), 0, 1, b.d.get(), b.total, c.scal.get(), c.s);
+    double r = 0;
+    QCM_CUDA(cudaMemcpyAsync(&r, c.scal.get(), sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    return r;
+}
+
+void scale(Ctx& c, DBlocks& b, double f) {
+    if (b.total) dev_axpby(f, b.d.get(), 0.0, b.d.get(), b.total, c.s);
+}
+
+DBlocks normalize_left(Ctx& c, DMPS& t) {
+    make_left_paired(c, t);
+    DBlocks Q, R;
+    for (std::size_t k = 0; k < t.b.n(); ++k) {
+        const uint32_t m = t.b.rows[k], n = t.b.cols[k], kk = std::min(m, n);
+        Q.add(t.b.lc[k], t.b.rc[k], m, kk);
+        R.add(t.b.rc[k], t.b.rc[k], kk, n);
+    }
+    Q.allocate(c.s, true);
+    R.allocate(c.s, true);
+    for (std::size_t k = 0; k < t.b.n(); ++k)
+        qr_thin(*c.sv, c.s, t.b.d.get() + t.b.off[k], int(t.b.rows[k]), int(t.b.cols[k]), Q.d.get() + Q.off[k],
+                R.d.get() + R.off[k]);
+    c.sv->check(c.s);
+    t.b = std::move(Q);
+    t.right = t.b.right_basis();
+    return R;
+}
+
+DBlocks normalize_right(Ctx& c, DMPS& t) {
+    make_right_paired(c, t);
+    DBlocks Lm, Q;
+    for (std::size_t k = 0; k < t.b.n(); ++k) {
+        const uint32_t m = t.b.rows[k], n = t.b.cols[k], kk = std::min(m, n);
+        Lm.add(t.b.lc[k], t.b.lc[k], m, kk);
+        Q.add(t.b.lc[k], t.b.rc[k], kk, n);
+    }
+    Lm.allocate(c.s, true);
+    Q.allocate(c.s, true);
+    for (std::size_t k = 0; k < t.b.n(); ++k)
+        lq_thin(*c.sv, c.s, t.b.d.get() + t.b.off[k], int(t.b.rows[k]), int(t.b.cols[k]), Lm.d.get() + Lm.off[k],
+                Q.d.get() + Q.off[k]);
+    c.sv->check(c.s);
+    t.b = std::move(Q);
+    t.left = t.b.left_basis();
+    return Lm;
+}
+
+void multiply_from_left(Ctx& c, DMPS& t, const DBlocks& N) {
+    make_right_paired(c, t);
+    DBlocks o;
+    std::vector<GemmJob> jobs;
+    for (std::size_t j = 0; j < N.n(); ++j) {
+        const std::size_t ks = find_block(t.b, N.rc[j]);
+        if (ks == t.b.n()) continue;
+        if (t.b.rows[ks] != N.cols[j]) throw std::runtime_error("multiply_from_left: inner dimensions differ");
+        o.add(N.lc[j], t.b.rc[ks], N.rows[j], t.b.cols[ks]);
+        GemmJob g{};
+        g.a_off = N.off[j]; g.lda = N.rows[j];
+        g.b_off = t.b.off[ks]; g.ldb = t.b.rows[ks];
+        g.c_off = o.off.back(); g.ldc = N.rows[j];
+        g.M = N.rows[j]; g.N = t.b.cols[ks]; g.K = N.cols[j]; g.alpha = 1.0; g.beta = 0.0;
+        jobs.push_back(g);
+    }
+    o.allocate(c.s, true);
+    batched_gemm(jobs, N.d.get(), N.total, t.b.d.get(), t.b.total, o.d.get(), o.total, c.gjobs, c.gtiles, c.s);
+    t.b = std::move(o);
+    t.left = t.b.left_basis();
+}
+
+void multiply_from_right(Ctx& c, DMPS& t, const DBlocks& N) {
+    make_left_paired(c, t);
+    DBlocks o;
+    std::vector<GemmJob> jobs;
+    for (std::size_t k = 0; k < t.b.n(); ++k) {
+        const std::size_t j = find_block(N, t.b.rc[k]);
+        if (j == N.n()) continue;
+        if (N.rows[j] != t.b.cols[k]) throw std::runtime_error("multiply_from_right: inner dimensions differ");
+        o.add(t.b.lc[k], N.rc[j], t.b.rows[k], N.cols[j]);
+        GemmJob g{};
+        g.a_off = t.b.off[k]; g.lda = t.b.rows[k];
+        g.b_off = N.off[j]; g.ldb = N.rows[j];
+        g.c_off = o.off.back(); g.ldc = t.b.rows[k];
+        g.M = t.b.rows[k]; g.N = N.cols[j]; g.K = t.b.cols[k]; g.alpha = 1.0; g.beta = 0.0;
+        jobs.push_back(g);
+    }
+    o.allocate(c.s, true);
+    batched_gemm(jobs, t.b.d.get(), t.b.total, N.d.get(), N.total, o.d.get(), o.total, c.gjobs, c.gtiles, c.s);
+    t.b = std::move(o);
+    t.right = t.b.right_basis();
+}
+
+// ---------------------------------------------------------------------------
+// two-site tensor
+void DTwoSite::build(Ctx& c, const DMPS& a, const DMPS& b) {
+    if (a.right_paired || !b.right_paired) throw std::runtime_error("two-site tensor: expects left-paired a, right-paired b");
+    phys1 = a.phys; phys2 = b.phys; phys = index_product(phys1, phys2); left = a.left; right = b.right;
+    ProductBasis in_left(phys1, left), in_right(phys2, right, true), out_right(phys, right, true), ppb(phys1, phys2);
+    // both-paired layout: every middle charge with rows and columns (ts_reshape.h creates the
+    // blocks the product leaves out when reshaping back)
+    both = DBlocks();
+    prod.clear();
+    std::vector<GemmJob> jobs;
+    Index mids = index_product(phys1, left);
+    for (std::size_t i = 0; i < mids.size(); ++i) {
+        const Charge m = mids[i].first;
+        const std::size_t rows = in_left.size(m), cols = in_right.size(m);
+        if (!rows || !cols) continue;
+        both.add(m, m, uint32_t(rows), uint32_t(cols));
+        const std::size_t ka = find_block(a.b, m), kb = find_block(b.b, m);
+        const bool pr = ka < a.b.n() && kb < b.b.n();
+        prod.push_back(pr ? 1 : 0);
+        if (!pr) continue;
+        if (a.b.rows[ka] != rows || b.b.cols[kb] != cols || a.b.cols[ka] != b.b.rows[kb])
+            throw std::runtime_error("two-site tensor: block shapes differ from the product bases");
+        GemmJob g{};
+        g.a_off = a.b.off[ka]; g.lda = a.b.rows[ka];
+        g.b_off = b.b.off[kb]; g.ldb = b.b.rows[kb];
+        g.c_off = both.off.back(); g.ldc = uint32_t(rows);
+        g.M = uint32_t(rows); g.N = uint32_t(cols); g.K = a.b.cols[ka]; g.alpha = 1.0; g.beta = 0.0;
+        jobs.push_back(g);
+    }
+    both.allocate(c.s, true);
+    batched_gemm(jobs, a.b.d.get(), a.b.total, b.b.d.get(), b.b.total, both.d.get(), both.total, c.gjobs, c.gtiles, c.s);
+
+    // twin (make_mps): right-paired blocks for the left charges the product blocks reach
+    std::vector<uint8_t> need(left.size(), 0);
+    for (std::size_t k = 0; k < both.n(); ++k) {
+        if (!prod[k]) continue;
+        for (std::size_t s1 = 0; s1 < phys1.size(); ++s1) {
+            const std::size_t l = left.position(both.lc[k] - phys1[s1].first);
+            if (l == left.size()) continue;
+            for (std::size_t s2 = 0; s2 < phys2.size(); ++s2)
+                if (right.has(both.lc[k] + phys2[s2].first)) need[l] = 1;
+        }
+    }
+    twin = DMPS();
+    twin.phys = phys; twin.right = right; twin.right_paired = true;
+    for (std::size_t l = 0; l < left.size(); ++l)
+        if (need[l] && out_right.size(left[l].first)) twin.left.d.push_back(left[l]);
+    twin.b = layout_right_paired(phys, twin.left, right, true);
+    twin.b.allocate(c.s, true);
+    std::vector<CopyJob> cj;
+    for (std::size_t k = 0; k < both.n(); ++k) {
+        if (!prod[k]) continue;
+        const Charge m = both.lc[k];
+        for (std::size_t s1 = 0; s1 < phys1.size(); ++s1) {
+            const Charge p1 = phys1[s1].first, lc = m - p1;
+            const std::size_t l = left.position(lc);
+            if (l == left.size()) continue;
+            const std::size_t kt = find_block(twin.b, lc);
+            for (std::size_t s2 = 0; s2 < phys2.size(); ++s2) {
+                const Charge p2 = phys2[s2].first, rc = m + p2;
+                const std::size_t r = right.position(rc);
+                if (r == right.size()) continue;
+                const uint32_t ldim = uint32_t(left[l].second), rdim = uint32_t(right[r].second);
+                const uint32_t sd1 = uint32_t(phys1[s1].second), sd2 = uint32_t(phys2[s2].second);
+                const uint64_t ilo = in_left(p1, lc), iro = in_right(p2, rc), oro = out_right(p1 + p2, rc), opo = ppb(p1, p2);
+                for (uint32_t ss1 = 0; ss1 < sd1; ++ss1)
+                    for (uint32_t ss2 = 0; ss2 < sd2; ++ss2) {
+                        const uint64_t so = opo + uint64_t(ss1) * sd2 + ss2;
+                        cj.push_back(CopyJob{both.off[k] + ilo + uint64_t(ss1) * ldim + (iro + uint64_t(ss2) * rdim) * both.rows[k],
+                                             twin.b.off[kt] + (oro + so * rdim) * ldim, ldim, rdim, both.rows[k], ldim, 0, 0});
+                    }
+            }
+        }
+    }
+    batched_copy(cj, both.d.get(), both.total, twin.b.d.get(), twin.b.total, c.cjobs, c.s);
+}
+
+void DTwoSite::twin_to_both(Ctx& c) {
+    ProductBasis in_left(phys1, left), in_right(phys2, right, true), out_right(phys, right, true), ppb(phys1, phys2);
+    if (both.total) QCM_CUDA(cudaMemsetAsync(both.d.get(), 0, both.total * sizeof(double), c.s));
+    std::vector<CopyJob> cj;
+    for (std::size_t kt = 0; kt < twin.b.n(); ++kt) {
+        const Charge lc = twin.b.lc[kt];
+        const std::size_t l = left.position(lc);
+        for (std::size_t s1 = 0; s1 < phys1.size(); ++s1)
+            for (std::size_t s2 = 0; s2 < phys2.size(); ++s2) {
+                const Charge p1 = phys1[s1].first, p2 = phys2[s2].first, rc = lc + p1 + p2;
+                const std::size_t r = right.position(rc);
+                if (r == right.size()) continue;
+                const std::size_t k = find_block(both, lc + p1);
+                if (k == both.n()) throw std::runtime_error("two-site tensor: missing both-paired block");
+                const uint32_t ldim = uint32_t(left[l].second), rdim = uint32_t(right[r].second);
+                const uint32_t sd1 = uint32_t(phys1[s1].second), sd2 = uint32_t(phys2[s2].second);
+                const uint64_t ilo = in_left(p1, lc), iro = in_right(p2, rc), oro = out_right(p1 + p2, rc), opo = ppb(p1, p2);
+                for (uint32_t ss1 = 0; ss1 < sd1; ++ss1)
+                    for (uint32_t ss2 = 0; ss2 < sd2; ++ss2) {
+                        const uint64_t so = opo + uint64_t(ss1) * sd2 + ss2;
+                        cj.push_back(CopyJob{twin.b.off[kt] + (oro + so * rdim) * ldim,
+                                             both.off[k] + ilo + uint64_t(ss1) * ldim + (iro + uint64_t(ss2) * rdim) * both.rows[k],
+                                             ldim, rdim, ldim, both.rows[k], 0, 0});
+                    }
+            }
+    }
+    batched_copy(cj, twin.b.d.get(), twin.b.total, both.d.get(), both.total, c.cjobs, c.s);
+}
+
+TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMPS& m1, DMPS& m2) {
+    const std::size_t nb = both.n();
+    std::vector<uint64_t> uo(nb), so(nb), vo(nb);
+    std::vector<uint32_t> kk(nb);
+    uint64_t ul = 0, sl = 0, vl = 0;
+    for (std::size_t k = 0; k < nb; ++k) {
+        kk[k] = std::min(both.rows[k], both.cols[k]);
+        uo[k] = ul; ul += (uint64_t(both.rows[k]) * kk[k] + 31) / 32 * 32;
+        so[k] = sl; sl += kk[k];
+        vo[k] = vl; vl += (uint64_t(both.cols[k]) * kk[k] + 31) / 32 * 32;
+    }
+    DBuf<double> U(std::max<uint64_t>(ul, 1)), S(std::max<uint64_t>(sl, 1)), V(std::max<uint64_t>(vl, 1));
+    for (std::size_t k = 0; k < nb; ++k)
+        svd_thin(*c.sv, c.s, both.d.get() + both.off[k], int(both.rows[k]), int(both.cols[k]), U.get() + uo[k], S.get() + so[k],
+                 V.get() + vo[k]);
+    c.sv->check(c.s);
+    std::vector<double> hs(sl);
+    if (sl) QCM_CUDA(cudaMemcpyAsync(hs.data(), S.get(), sl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+
+    // estimate_truncation (block_matrix_algorithms.h:136-183)
+    std::vector<double> all(hs);
+    std::sort(all.begin(), all.end(), std::greater<double>());
+    TruncResults tr;
+    if (all.empty() || all[0] == 0.0) throw std::runtime_error("truncation: two-site tensor is zero");
+    double evalscut = cutoff * all[0];
+    if (all.size() > Mmax) evalscut = std::max(evalscut, all[Mmax]);
+    tr.smallest_ev = evalscut / all[0];
+    double tf = 0, tw = 0, sum = 0, sum2 = 0;
+    for (double x : all) {
+        sum += x; sum2 += x * x;
+        if (x < evalscut) { tf += x; tw += x * x; }
+    }
+    tr.truncated_fraction = tf / sum;
+    tr.truncated_weight = tw / sum2;
+    std::vector<uint32_t> keep(nb, 0);
+    for (std::size_t k = 0; k < nb; ++k) {
+        uint32_t n = 0;
+        while (n < kk[k] && !(hs[so[k] + n] < evalscut)) ++n;
+        keep[k] = n;
+        tr.bond_dimension += n;
+    }
+
+    // U[:, :keep] and V^T[:keep, :], with S multiplied into V^T (l2r) or U (r2l)
+    m1 = DMPS(); m2 = DMPS();
+    m1.phys = phys1; m1.left = left; m1.right_paired = false;
+    m2.phys = phys2; m2.right = right; m2.right_paired = true;
+    std::vector<std::pair<Charge, std::size_t>> mid;
+    for (std::size_t k = 0; k < nb; ++k) {
+        if (!keep[k]) continue;
+        mid.push_back({both.lc[k], keep[k]});
+        m1.b.add(both.lc[k], both.lc[k], both.rows[k], keep[k]);
+        m2.b.add(both.lc[k], both.lc[k], keep[k], both.cols[k]);
+    }
+    m1.right = sorted_basis(mid);
+    m2.left = m1.right;
+    m1.b.allocate(c.s, true);
+    m2.b.allocate(c.s, true);
+    std::vector<CopyJob> ju, jv;
+    std::size_t i = 0;
+    for (std::size_t k = 0; k < nb; ++k) {
+        if (!keep[k]) continue;
+        ju.push_back(CopyJob{uo[k], m1.b.off[i], both.rows[k], keep[k], both.rows[k], both.rows[k], 0, 0});
+        jv.push_back(CopyJob{vo[k], m2.b.off[i], both.cols[k], keep[k], both.cols[k], keep[k], 1, 0});
+        ++i;
+    }
+    batched_copy(ju, U.get(), ul, m1.b.d.get(), m1.b.total, c.cjobs, c.s);
+    batched_copy(jv, V.get(), vl, m2.b.d.get(), m2.b.total, c.cjobs, c.s);
+    i = 0;
+    for (std::size_t k = 0; k < nb; ++k) {
+        if (!keep[k]) continue;
+        if (l2r) dev_scale_rows(m2.b.d.get() + m2.b.off[i], keep[k], both.cols[k], keep[k], S.get() + so[k], c.s);
+        else dev_scale_cols(m1.b.d.get() + m1.b.off[i], both.rows[k], keep[k], both.rows[k], S.get() + so[k], c.s);
+        ++i;
+    }
+    QCM_CUDA(cudaStreamSynchronize(c.s));  // U, S, V are released on return
+    return tr;
+}
+
+}  // namespace qcm

@@ -1,0 +1,172 @@
+// Device-resident MPS tensors, boundary steps and the two-site sweep on one B200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "dev_ops.hpp"
+#include "device.hpp"
+#include "heff.hpp"
+#include "linalg.hpp"
+#include "mpo.hpp"
+#include "symm.hpp"
+
+namespace qcm {
+
+// Block matrix in HBM: block k has charges (lc[k], rc[k]), rows x cols, column-major at off[k].
+struct DBlocks {
+    std::vector<Charge> lc, rc;
+    std::vector<uint32_t> rows, cols;
+    std::vector<uint64_t> off;
+    uint64_t total = 0;
+    DBuf<double> d;
+    std::size_t n() const { return lc.size(); }
+    std::size_t find_l(Charge c) const {
+        for (std::size_t k = 0; k < lc.size(); ++k) if (lc[k] == c) return k;
+        return lc.size();
+    }
+    std::size_t find_r(Charge c) const {
+        for (std::size_t k = 0; k < rc.size(); ++k) if (rc[k] == c) return k;
+        return rc.size();
+    }
+    // blocks start on 32-element boundaries unless packed (the H_eff vector layout is packed)
+    void add(Charge l, Charge r, uint32_t nr, uint32_t nc, bool packed = false) {
+        lc.push_back(l); rc.push_back(r); rows.push_back(nr); cols.push_back(nc);
+        off.push_back(total);
+        total += packed ? uint64_t(nr) * nc : (uint64_t(nr) * nc + 31) / 32 * 32;
+    }
+    uint64_t elems(std::size_t k) const { return uint64_t(rows[k]) * cols[k]; }
+    void allocate(cudaStream_t s, bool zero) {
+        d.alloc(total ? total : 1);
+        if (zero) QCM_CUDA(cudaMemsetAsync(d.get(), 0, (total ? total : 1) * sizeof(double), s));
+    }
+    Index left_basis() const { Index r; for (std::size_t k = 0; k < n(); ++k) r.d.push_back({lc[k], rows[k]}); return r; }
+    Index right_basis() const { Index r; for (std::size_t k = 0; k < n(); ++k) r.d.push_back({rc[k], cols[k]}); return r; }
+};
+
+// MPSTensor (mp_tensors/mpstensor.h): blocks keyed by the left charge when
+// right-paired (ls x stripe, columns ProductBasis(phys, right, -p + r)) and by
+// the right charge when left-paired (rows ProductBasis(phys, left), rs columns).
+struct DMPS {
+    Index phys, left, right;
+    bool right_paired = false;
+    DBlocks b;
+};
+
+// Work lists of the unit S-GEMM (shared by H_eff and the boundary steps)
+struct SBuild {
+    std::vector<UnitD> units;
+    std::vector<TileD> utiles[N_SHAPES];
+    std::vector<uint32_t> line_b1, sptr;
+    std::vector<uint64_t> slice_off;
+    std::vector<WEntD> went;
+    DBuf<UnitD> d_units;
+    DBuf<TileD> d_utiles[N_SHAPES];
+    DBuf<uint32_t> d_line_b1, d_sptr;
+    DBuf<uint64_t> d_slice_off;
+    DBuf<WEntD> d_went;
+    struct E { uint32_t line; uint64_t slice; double a; };
+    // lines[i] = output line position of local line i; entries reference local lines
+    void add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint32_t col_stride, uint32_t ne,
+                  const std::vector<uint32_t>& lines, const std::vector<E>& ents);
+    void upload(cudaStream_t s);
+    // throws unless every unit's S writes and T slice reads lie inside [0, s_len) and [0, t_len)
+    void validate(uint64_t t_len, uint64_t s_len) const;
+};
+
+// Engine context: stream, cuSOLVER handle and scratch buffers reused across steps.
+struct Ctx {
+    cudaStream_t s = nullptr;
+    std::unique_ptr<Solver> sv;
+    DBuf<double> T, S, work, tmp, jd, scal, coef;
+    DBuf<GemmJob> gjobs;
+    DBuf<uint32_t> gtiles;
+    DBuf<CopyJob> cjobs;
+    DBuf<TJobD> tjobs;
+    DBuf<TileD> ttiles[N_SHAPES];
+    DBuf<int> info;
+    static void ensure(DBuf<double>& b, uint64_t n) { if (b.size() < n) b.alloc(n); }
+};
+
+// ---- MPS tensors on the device (mp_tensors/mpstensor.hpp, reshapes.h) ----
+DBlocks layout_right_paired(const Index& phys, const Index& left, const Index& right, bool packed = false);
+DBlocks layout_left_paired(const Index& phys, const Index& left, const Index& right);
+void make_left_paired(Ctx& c, DMPS& t);
+void make_right_paired(Ctx& c, DMPS& t);
+DMPS right_paired_copy(Ctx& c, const DMPS& t);
+double norm2(Ctx& c, const DBlocks& b);
+void scale(Ctx& c, DBlocks& b, double f);
+// normalize_left/right (mpstensor.hpp:242-300): QR / LQ per block; returns R / L as a block matrix
+DBlocks normalize_left(Ctx& c, DMPS& t);
+DBlocks normalize_right(Ctx& c, DMPS& t);
+void multiply_from_left(Ctx& c, DMPS& t, const DBlocks& N);   // t = N * t (right-paired)
+void multiply_from_right(Ctx& c, DMPS& t, const DBlocks& N);  // t = t * N (left-paired)
+
+// block_matrix_algorithms.h:48-63
+struct TruncResults {
+    uint64_t bond_dimension = 0;
+    double truncated_weight = 0, truncated_fraction = 0, smallest_ev = 0;
+};
+
+// TwoSiteTensor (mp_tensors/twositetensor.hpp:29-199, ts_reshape.h)
+struct DTwoSite {
+    Index phys1, phys2, phys, left, right;
+    DBlocks both;               // rows ProductBasis(phys1, left), cols ProductBasis(phys2, right, -p + r), per middle charge
+    std::vector<uint8_t> prod;  // block is a product block of a * b (the rest are created by the back-reshape)
+    DMPS twin;                  // right-paired over phys1 x phys2, packed (H_eff vector layout)
+    void build(Ctx& c, const DMPS& a_lp, const DMPS& b_rp);
+    void twin_to_both(Ctx& c);  // reshape_right_to_both
+    // split_mps_l2r / split_mps_r2l with svd_truncate (block_matrix_algorithms.h:136-240)
+    TruncResults split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMPS& m1, DMPS& m2);
+};
+
+// Jacobi-Davidson for the lowest eigenpair (ietl/jacobi.h:386-474 with gmres 0):
+// x (device, plan vector layout) holds the start vector and receives the eigenvector.
+double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters);
+
+// Boundary steps (contractions/boundary_ops/move_boundary.hpp:147-404): new left boundary
+// from L[site] and mps[site]; new right boundary from R[site+1] and mps[site].
+std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& L, const DMPS& ket_rp, const DMPS& bra_lp,
+                                                const MPOTensor& W, bool symmetric);
+std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& R, const DMPS& ket, const MPOTensor& W,
+                                                 bool symmetric);
+
+// trivial boundary: one cohort per sector, aux_dim blocks of ones (boundary.h / optimize.h:158-195)
+std::unique_ptr<DevBoundary> trivial_boundary(const Index& idx, uint32_t aux_dim, cudaStream_t s);
+
+// complement_transpose of a boundary index (boundary.h:150-179; abelian conjugate correction 1)
+void complement_transpose(BoundaryIndexH& x, const std::vector<int32_t>& herm, const std::vector<int32_t>& phase, bool forward);
+
+// Two-site DMRG sweep on the device (optimize/ts_optimize.hpp:114-362, optimize.h:134-233).
+struct DMRGParams {
+    uint64_t Mmax = 64;
+    uint64_t init_bond_dimension = 64;
+    double cutoff = 1e-16;
+    double jcd_tol = 1e-10;
+    int jcd_maxiter = 8;
+    double ecore = 0.0;
+};
+
+struct DMRGStats {
+    uint64_t hpsi_count = 0;
+    double hpsi_flops = 0, hpsi_ms = 0;  // reference flop count and device time of the H.psi applies
+    double plan_s = 0, jd_s = 0, trunc_s = 0, boundary_s = 0, total_s = 0;
+};
+
+struct DevDMRG {
+    int L = 0;
+    std::vector<MPOTensor> mpo, ts_mpo;
+    std::vector<DMPS> mps;
+    std::vector<std::unique_ptr<DevBoundary>> left_, right_;
+    DMRGParams p;
+    DMRGStats st;
+    Ctx c;
+    DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, int nup, int ndown,
+            const DMRGParams& prm, cudaStream_t s);
+    void sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc);
+};
+
+}  // namespace qcm

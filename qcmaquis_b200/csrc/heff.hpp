@@ -65,15 +65,16 @@ struct TJobD {        // T[c_off] (M x N) = psi[a_off] (M x K, lda) * Rop (K x N
     uint32_t M, K, N, lda, brs, tr;  // Rop(k, n) = R[b_off + (n/brs)*K*brs + (tr ? n%brs + k*brs : k + (n%brs)*K)]
 };
 struct UnitD {        // S rows of one cohort unit: S_u (lines x elements) = W_u (lines x slices) * slices
-    uint64_t s_off;   // S offset of (row 0, first column of the unit) in the cohort's S (ld = ldS)
-    uint32_t ldS;     // nS * ls_in of the cohort
-    uint32_t ls;      // rows of a slice = ls_in; element e of a slice is (r, c) = (e % ls, e / ls)
-    uint32_t ne;      // elements per slice = ls_in * ms
-    uint32_t nl;      // lines (L block rows with coefficients)
-    uint32_t line0;   // first entry in line_b1[]
-    uint32_t nk;      // distinct T slices referenced
-    uint32_t slice0;  // first entry in slice_off[]
-    uint32_t sptr0;   // first of nk + 1 entry pointers in sptr[]
+    uint64_t s_off;        // S offset of (line 0, element 0) of the unit
+    uint64_t line_stride;  // S offset step per line
+    uint32_t erows;        // element e of a slice is (r, c) = (e % erows, e / erows) ...
+    uint32_t col_stride;   // ... and lands at s_off + line*line_stride + r + c*col_stride
+    uint32_t ne;           // elements per slice
+    uint32_t nl;           // lines (boundary blocks with coefficients)
+    uint32_t line0;        // first entry in line_b1[]
+    uint32_t nk;           // distinct T slices referenced
+    uint32_t slice0;       // first entry in slice_off[]
+    uint32_t sptr0;        // first of nk + 1 entry pointers in sptr[]
 };
 struct WEntD {        // coefficient alpha at (line, slice) of a unit; entries sorted by slice
     uint32_t line, k;
@@ -168,6 +169,12 @@ void upload_plan(HeffPlan& p);
 // gather and after the L.S GEMM.
 void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev = nullptr);
 int heff_launches_per_apply(const HeffPlan& p);
+// Grouped T-GEMM and unit S-GEMM launches over prepared work lists (three tile shapes each).
+void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const double* x,
+               const double* R, double* T, cudaStream_t s);
+void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const uint32_t* line_b1,
+               const uint64_t* slice_off, const uint32_t* sptr, const WEntD* went, const double* T, double* S,
+               cudaStream_t s);
 // Same apply with caller-provided scratch: Tb (t_len), Sb (s_len) and Pb (p_len) doubles.
 void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* Tb, double* Sb, double* Pb);
 

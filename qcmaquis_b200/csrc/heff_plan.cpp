@@ -246,7 +246,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 }
                 UnitD ud{};
                 ud.s_off = s_off + uint64_t(u.offset) * K_c;
-                ud.ldS = K_c; ud.ls = ls_in; ud.ne = ls_in * u.ms;
+                ud.line_stride = ls_in; ud.erows = ls_in; ud.col_stride = K_c; ud.ne = ls_in * u.ms;
                 ud.nl = uint32_t(u.lines.size()); ud.line0 = uint32_t(P.line_b1.size());
                 ud.nk = uint32_t(slices.size()); ud.slice0 = uint32_t(P.slice_off.size());
                 ud.sptr0 = uint32_t(P.sptr.size());

@@ -1,0 +1,195 @@
+// Dense per-block factorizations on the device (see linalg.hpp).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+#include <string>
+
+#include "linalg.hpp"
+
+#define QCM_SOLVER(call)                                                                                   \
+    do {                                                                                                   \
+        cusolverStatus_t st_ = (call);                                                                     \
+        if (st_ != CUSOLVER_STATUS_SUCCESS)                                                                \
+            throw qcm::cuda_error(std::string(#call) + ": cuSOLVER status " + std::to_string(int(st_)));   \
+    } while (0)
+
+namespace qcm {
+namespace {
+
+constexpr uint32_t INFO_CAP = 4096;
+
+// 32 x 32 tiled transpose: dst(j, i) = src(i, j), src m x n (ld lds), dst n x m (ld ldd)
+__global__ void k_transpose(const double* __restrict__ src, uint32_t m, uint32_t n, uint32_t lds, double* __restrict__ dst,
+                            uint32_t ldd) {
+    __shared__ double t[32][33];
+    const uint32_t i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
+    for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+        uint32_t i = i0 + threadIdx.x, j = j0 + r;
+        if (i < m && j < n) t[r][threadIdx.x] = src[i + uint64_t(j) * lds];
+    }
+    __syncthreads();
+    for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
+        uint32_t j = j0 + threadIdx.x, i = i0 + r;
+        if (i < m && j < n) dst[j + uint64_t(i) * ldd] = t[threadIdx.x][r];
+    }
+}
+
+// mode 0: dst(i, j) = i <= j ? src(i, j) : 0   (R factor)
+// mode 1: dst(i, j) = j <= i ? src(j, i) : 0   (L factor = transposed R factor)
+__global__ void k_tri(const double* __restrict__ src, uint32_t lds, double* __restrict__ dst, uint32_t ldd, uint32_t rows,
+                      uint32_t cols, int mode) {
+    const uint64_t n = uint64_t(rows) * cols;
+    for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < n; e += uint64_t(gridDim.x) * blockDim.x) {
+        uint32_t j = uint32_t(e / rows), i = uint32_t(e - uint64_t(j) * rows);
+        double v = 0.0;
+        if (mode == 0) { if (i <= j) v = src[i + uint64_t(j) * lds]; }
+        else { if (j <= i) v = src[j + uint64_t(i) * lds]; }
+        dst[i + uint64_t(j) * ldd] = v;
+    }
+}
+
+void transpose(const double* src, uint32_t m, uint32_t n, uint32_t lds, double* dst, uint32_t ldd, cudaStream_t s) {
+    if (!m || !n) return;
+    dim3 g((m + 31) / 32, (n + 31) / 32), b(32, 8);
+    k_transpose<<<g, b, 0, s>>>(src, m, n, lds, dst, ldd);
+    QCM_CUDA(cudaGetLastError());
+}
+
+void tri(const double* src, uint32_t lds, double* dst, uint32_t ldd, uint32_t rows, uint32_t cols, int mode, cudaStream_t s) {
+    if (!rows || !cols) return;
+    uint64_t n = uint64_t(rows) * cols;
+    unsigned g = unsigned(std::min<uint64_t>((n + 255) / 256, 148 * 8));
+    k_tri<<<g, 256, 0, s>>>(src, lds, dst, ldd, rows, cols, mode);
+    QCM_CUDA(cudaGetLastError());
+}
+
+void ensure(DBuf<double>& b, std::size_t n) { if (b.size() < n) b.alloc(std::max<std::size_t>(n, 1)); }
+
+int* next_info(Solver& sv, cudaStream_t s) {
+    if (sv.n_info >= INFO_CAP) sv.check(s);
+    return sv.info.get() + sv.n_info++;
+}
+
+}  // namespace
+
+Solver::Solver() {
+    QCM_SOLVER(cusolverDnCreate(&h));
+    QCM_SOLVER(cusolverDnCreateGesvdjInfo(&svdp));
+    QCM_SOLVER(cusolverDnXgesvdjSetMaxSweeps(svdp, 100));
+    QCM_SOLVER(cusolverDnXgesvdjSetSortEig(svdp, 1));
+    info.alloc(INFO_CAP);
+    tau.alloc(1024);
+}
+
+Solver::~Solver() {
+    if (svdp) cusolverDnDestroyGesvdjInfo(svdp);
+    if (h) cusolverDnDestroy(h);
+}
+
+void Solver::bind(cudaStream_t s) { QCM_SOLVER(cusolverDnSetStream(h, s)); }
+
+void Solver::check(cudaStream_t s) {
+    if (!n_info) return;
+    std::vector<int> hi(n_info);
+    QCM_CUDA(cudaMemcpyAsync(hi.data(), info.get(), n_info * sizeof(int), cudaMemcpyDeviceToHost, s));
+    QCM_CUDA(cudaStreamSynchronize(s));
+    n_info = 0;
+    for (int v : hi)
+        if (v != 0) throw std::runtime_error("device factorization failed (info " + std::to_string(v) + ")");
+}
+
+void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* U, double* S, double* V) {
+    if (m == 0 || n == 0) return;
+    sv.bind(s);
+    ensure(sv.a, std::size_t(m) * n);
+    QCM_CUDA(cudaMemcpyAsync(sv.a.get(), A, std::size_t(m) * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    int lwork = 0;
+    QCM_SOLVER(cusolverDnDgesvdj_bufferSize(sv.h, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, sv.a.get(), m, S, U, m, V, n, &lwork,
+                                            sv.svdp));
+    ensure(sv.work, std::size_t(lwork));
+    QCM_SOLVER(cusolverDnDgesvdj(sv.h, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, sv.a.get(), m, S, U, m, V, n, sv.work.get(), lwork,
+                                 next_info(sv, s), sv.svdp));
+}
+
+namespace {
+// Householder QR of a (m x n, ld m) in place; leaves R in the upper triangle and Q's reflectors below
+void geqrf_orgqr(Solver& sv, cudaStream_t s, int m, int n, double* Rout, uint32_t ldr, int rmode, uint32_t rrows,
+                 uint32_t rcols) {
+    const int k = std::min(m, n);
+    ensure(sv.tau, std::size_t(k));
+    int lw1 = 0, lw2 = 0;
+    QCM_SOLVER(cusolverDnDgeqrf_bufferSize(sv.h, m, n, sv.a.get(), m, &lw1));
+    QCM_SOLVER(cusolverDnDorgqr_bufferSize(sv.h, m, k, k, sv.a.get(), m, sv.tau.get(), &lw2));
+    ensure(sv.work, std::size_t(std::max(lw1, lw2)));
+    QCM_SOLVER(cusolverDnDgeqrf(sv.h, m, n, sv.a.get(), m, sv.tau.get(), sv.work.get(), std::max(lw1, lw2), next_info(sv, s)));
+    tri(sv.a.get(), uint32_t(m), Rout, ldr, rrows, rcols, rmode, s);
+    QCM_SOLVER(cusolverDnDorgqr(sv.h, m, k, k, sv.a.get(), m, sv.tau.get(), sv.work.get(), std::max(lw1, lw2),
+                                next_info(sv, s)));
+}
+}  // namespace
+
+void qr_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* Q, double* R) {
+    if (m == 0 || n == 0) return;
+    sv.bind(s);
+    const int k = std::min(m, n);
+    ensure(sv.a, std::size_t(m) * n);
+    QCM_CUDA(cudaMemcpyAsync(sv.a.get(), A, std::size_t(m) * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    geqrf_orgqr(sv, s, m, n, R, uint32_t(k), 0, uint32_t(k), uint32_t(n));
+    QCM_CUDA(cudaMemcpyAsync(Q, sv.a.get(), std::size_t(m) * k * sizeof(double), cudaMemcpyDeviceToDevice, s));
+}
+
+void lq_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* L, double* Q) {
+    if (m == 0 || n == 0) return;
+    sv.bind(s);
+    const int k = std::min(m, n);
+    ensure(sv.a, std::size_t(m) * n);
+    transpose(A, uint32_t(m), uint32_t(n), uint32_t(m), sv.a.get(), uint32_t(n), s);  // a = A^T (n x m)
+    geqrf_orgqr(sv, s, n, m, L, uint32_t(m), 1, uint32_t(m), uint32_t(k));             // L = R'^T (m x k)
+    transpose(sv.a.get(), uint32_t(n), uint32_t(k), uint32_t(n), Q, uint32_t(k), s);   // Q = Q'^T (k x n)
+}
+
+void sym_lowest_eigenpair(const double* M, int ldm, int n, double& w, std::vector<double>& z) {
+    std::vector<double> A(std::size_t(n) * n), V(std::size_t(n) * n, 0.0);
+    for (int j = 0; j < n; ++j)
+        for (int i = 0; i <= j; ++i) A[i + std::size_t(j) * n] = A[j + std::size_t(i) * n] = M[i + std::size_t(j) * ldm];
+    for (int i = 0; i < n; ++i) V[i + std::size_t(i) * n] = 1.0;
+    auto a = [&](int i, int j) -> double& { return A[i + std::size_t(j) * n]; };
+    // cyclic Jacobi (Golub & Van Loan, Algorithm 8.5.3) until the off-diagonal part is negligible
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        double off = 0.0, tot = 0.0;
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) { tot += a(i, j) * a(i, j); if (i != j) off += a(i, j) * a(i, j); }
+        if (off <= 1e-32 * tot || off == 0.0) break;
+        for (int p = 0; p < n - 1; ++p)
+            for (int q = p + 1; q < n; ++q) {
+                double apq = a(p, q);
+                if (apq == 0.0) continue;
+                double tau = (a(q, q) - a(p, p)) / (2.0 * apq);
+                double t = (tau >= 0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+                double c = 1.0 / std::sqrt(1.0 + t * t), s = t * c;
+                for (int k = 0; k < n; ++k) {  // A <- A J
+                    double akp = a(k, p), akq = a(k, q);
+                    a(k, p) = c * akp - s * akq;
+                    a(k, q) = s * akp + c * akq;
+                }
+                for (int k = 0; k < n; ++k) {  // A <- J^T A
+                    double apk = a(p, k), aqk = a(q, k);
+                    a(p, k) = c * apk - s * aqk;
+                    a(q, k) = s * apk + c * aqk;
+                }
+                for (int k = 0; k < n; ++k) {  // V <- V J
+                    double vkp = V[k + std::size_t(p) * n], vkq = V[k + std::size_t(q) * n];
+                    V[k + std::size_t(p) * n] = c * vkp - s * vkq;
+                    V[k + std::size_t(q) * n] = s * vkp + c * vkq;
+                }
+            }
+    }
+    int best = 0;
+    for (int i = 1; i < n; ++i) if (a(i, i) < a(best, best)) best = i;
+    w = a(best, best);
+    z.assign(V.begin() + std::size_t(best) * n, V.begin() + std::size_t(best + 1) * n);
+}
+
+}  // namespace qcm

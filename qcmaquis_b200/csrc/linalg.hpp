@@ -1,0 +1,48 @@
+// Dense per-block factorizations on the device, used by the truncation and
+// canonisation steps of the sweep:
+//   thin SVD   (framework/alps/matrix/algorithms.hpp:243-257, gesvd 'S','S')
+//   thin QR    (algorithms.hpp:260-291, geqrf + orgqr)
+//   thin LQ    (algorithms.hpp:293-325, gelqf + orglq; here QR of the transpose,
+//               which applies the same Householder reflectors)
+// plus the Rayleigh-Ritz eigenproblem of the Jacobi-Davidson solver (host, <= 64 x 64).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "device.hpp"
+
+namespace qcm {
+
+struct Solver {
+    cusolverDnHandle_t h = nullptr;
+    gesvdjInfo_t svdp = nullptr;
+    DBuf<double> work, a, b, tau;
+    DBuf<int> info;  // one status word per factorization since the last check
+    uint32_t n_info = 0;
+    Solver();
+    ~Solver();
+    Solver(const Solver&) = delete;
+    Solver& operator=(const Solver&) = delete;
+    void bind(cudaStream_t s);
+    // throws if any factorization since the last call reported a failure (synchronizes s)
+    void check(cudaStream_t s);
+};
+
+// A (m x n, lda = m) is read only.  k = min(m, n).
+// U (m x k, ld m), S (k, descending), V (n x k, ld n): A = U diag(S) V^T
+void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* U, double* S, double* V);
+// Q (m x k, ld m), R (k x n, ld k, upper trapezoidal): A = Q R
+void qr_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* Q, double* R);
+// L (m x k, ld m, lower trapezoidal), Q (k x n, ld k): A = L Q
+void lq_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* L, double* Q);
+
+// Lowest eigenpair of the symmetric n x n matrix held in the upper triangle of
+// M (column-major, leading dimension ldm); cyclic Jacobi rotations, FP64.
+// Replaces the dsyevx(range='I', il=iu=1) call of ietl/jacobi.h:476-516.
+void sym_lowest_eigenpair(const double* M, int ldm, int n, double& w, std::vector<double>& z);
+
+}  // namespace qcm

@@ -1,0 +1,282 @@
+// Jacobi-Davidson eigensolver and the two-site DMRG sweep on the device.
+//
+// JD (ietl/jacobi.h:386-474, jcd_gmres_solver with max_iter 0 at :141-157): the
+// search space, its H images and every vector update live in HBM; only the
+// Rayleigh-Ritz matrix (<= maxiter^2 numbers), its eigenvector and three norms
+// per iteration cross to the host.  Dot products use a fixed-order reduction,
+// so a solve is reproducible run to run.
+//
+// Sweep (optimize/ts_optimize.hpp:114-362): per step, two-site tensor -> H_eff
+// plan -> JD -> SVD truncation -> QR/LQ re-gauge -> boundary step, all on one
+// stream.  Initialisation: const MPS over allowed_sectors (mps_sectors.h:52-140,
+// mps_initializers.h:84-100), MPS::normalize_left (mps.hpp:129-136),
+// canonize(0) and the right boundaries (optimize.h:158-195).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <stdexcept>
+
+#include "dmrg_dev.hpp"
+
+namespace qcm {
+
+namespace {
+double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+void download(Ctx& c, const double* d, double* h, std::size_t n) {
+    QCM_CUDA(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+}
+}  // namespace
+
+double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters) {
+    if (maxiter < 1 || maxiter > 64) throw std::runtime_error("jacobi_davidson: maxiter must be in 1..64");
+    const uint64_t n = p.x_len, ld = (n + 31) / 32 * 32;
+    // V[0..maxiter), VA[0..maxiter), u, r
+    Ctx::ensure(c.jd, (2 * uint64_t(maxiter) + 2) * ld);
+    Ctx::ensure(c.scal, 256);
+    Ctx::ensure(c.coef, 64);
+    double* V = c.jd.get();
+    double* VA = V + uint64_t(maxiter) * ld;
+    double* u = VA + uint64_t(maxiter) * ld;
+    double* r = u + ld;
+    double* sc = c.scal.get();
+    auto Vi = [&](int i) { return V + uint64_t(i) * ld; };
+    auto VAi = [&](int i) { return VA + uint64_t(i) * ld; };
+    QCM_CUDA(cudaMemcpyAsync(Vi(0), x, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
+    std::vector<double> M(std::size_t(maxiter) * maxiter, 0.0), s;
+    int it = 0;
+    double theta = 0.0;
+    while (true) {
+        double* t = Vi(it);
+        // modified Gram-Schmidt against V[0..it), repeated once if the norm dropped below 1/4
+        auto mgs = [&]() {
+            for (int i = 0; i < it; ++i) {
+                dev_dots(Vi(i), 0, 1, t, n, sc + 2 + i, c.s);
+                dev_axpy_dscalar(sc + 2 + i, -1.0, Vi(i), t, n, c.s);
+            }
+            dev_dots(t, 0, 1, t, n, sc + 1, c.s);
+        };
+        dev_dots(t, 0, 1, t, n, sc, c.s);
+        mgs();
+        double h2[2];
+        download(c, sc, h2, 2);
+        double tau = std::sqrt(h2[0]), tn = std::sqrt(h2[1]);
+        if (tn < 0.25 * tau) {
+            mgs();
+            download(c, sc + 1, h2, 1);
+            tn = std::sqrt(h2[0]);
+        }
+        dev_axpby(1.0 / tn, t, 0.0, t, n, c.s);
+        heff_apply_device(p, t, VAi(it));
+        // column it of the projected matrix: <V_i, A V_it>
+        dev_dots(V, ld, uint32_t(it + 1), VAi(it), n, sc + 80, c.s);
+        std::vector<double> col(it + 1);
+        download(c, sc + 80, col.data(), col.size());
+        for (int i = 0; i <= it; ++i) M[i + std::size_t(it) * maxiter] = col[i];
+        sym_lowest_eigenpair(M.data(), maxiter, it + 1, theta, s);
+        QCM_CUDA(cudaMemcpyAsync(c.coef.get(), s.data(), s.size() * sizeof(double), cudaMemcpyHostToDevice, c.s));
+        dev_lincomb(V, ld, uint32_t(it + 1), c.coef.get(), n, u, false, c.s);
+        // r = A u - theta u
+        dev_lincomb(VA, ld, uint32_t(it + 1), c.coef.get(), n, r, false, c.s);
+        dev_axpby(-theta, u, 1.0, r, n, c.s);
+        dev_dots(r, 0, 1, r, n, sc + 160, c.s);
+        dev_dots(r, 0, 1, u, n, sc + 161, c.s);
+        dev_dots(u, 0, 1, u, n, sc + 162, c.s);
+        double h3[3];
+        download(c, sc + 160, h3, 3);
+        ++it;
+        const double rn = std::sqrt(h3[0]);
+        if (rn <= tol * std::fabs(theta) || rn < tol || it >= maxiter) {
+            QCM_CUDA(cudaMemcpyAsync(x, u, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
+            iters = it;
+            return theta;
+        }
+        // correction t = -r + (r.u)/(u.u) u
+        dev_axpby(-1.0, r, 0.0, Vi(it), n, c.s);
+        dev_axpby(h3[1] / h3[2], u, 1.0, Vi(it), n, c.s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+std::unique_ptr<DevBoundary> trivial_boundary(const Index& idx, uint32_t aux_dim, cudaStream_t s) {
+    auto B = std::make_unique<DevBoundary>();
+    BoundaryIndexH& x = B->idx;
+    x.bra = idx; x.ket = idx; x.aux = aux_dim;
+    for (uint32_t i = 0; i < idx.size(); ++i) {
+        const uint32_t ls = uint32_t(idx[i].second);
+        x.cbra.push_back(i); x.cket.push_back(i); x.lsz.push_back(ls); x.rsz.push_back(ls);
+        x.nb.push_back(aux_dim); x.tr.push_back(0);
+        for (uint32_t b = 0; b < aux_dim; ++b) { x.offsets.push_back(int64_t(b) * ls * ls); x.cscale.push_back(1.0); }
+    }
+    x.finish();
+    B->data.alloc(x.total ? x.total : 1);
+    dev_fill(B->data.get(), x.total ? x.total : 1, 1.0, s);
+    return B;
+}
+
+namespace {
+// allowed_sectors (mps_sectors.h:52-140)
+std::vector<Index> allowed_sectors(int L, const Index& phys, Charge right_end, std::size_t Mmax) {
+    Index physc = phys;
+    physc.sort();
+    Charge maxc = physc.d.front().first, minc = physc.d.back().first;
+    if (minc > maxc) std::swap(maxc, minc);
+    Charge maxt, mint;
+    for (int i = 0; i < L; ++i) { maxt = maxt + maxc; mint = mint + minc; }
+    std::vector<Index> la(L + 1), ra(L + 1), allowed(L + 1);
+    la[0].d.push_back({Charge(0, 0), 1});
+    ra[L].d.push_back({right_end, 1});
+    Charge cmaxi = maxt, cmini = mint;
+    for (int i = 1; i <= L; ++i) {
+        la[i] = index_product(phys, la[i - 1]);
+        cmaxi = cmaxi - maxc;
+        cmini = cmini - minc;
+        Index keep;
+        for (auto& e : la[i].d) {
+            if ((e.first + cmaxi) < right_end) continue;
+            if ((e.first + cmini) > right_end) continue;
+            keep.d.push_back({e.first, std::min(Mmax, e.second)});
+        }
+        la[i] = keep;
+    }
+    cmaxi = maxt; cmini = mint;
+    for (int i = L - 1; i >= 0; --i) {
+        ra[i] = index_product(adjoin(phys), ra[i + 1]);
+        cmaxi = cmaxi - maxc;
+        cmini = cmini - minc;
+        Index keep;
+        for (auto& e : ra[i].d) {
+            if ((e.first - cmaxi) > Charge(0, 0)) continue;
+            if ((e.first - cmini) < Charge(0, 0)) continue;
+            keep.d.push_back({e.first, std::min(Mmax, e.second)});
+        }
+        ra[i] = keep;
+    }
+    for (int i = 0; i <= L; ++i) {
+        Index a = la[i], b = ra[i];
+        common_subset(a, b);
+        for (auto& e : a.d) e.second = std::min(Mmax, std::min(la[i].size_of(e.first), ra[i].size_of(e.first)));
+        allowed[i] = a;
+    }
+    return allowed;
+}
+
+// MPSTensor(sd, ld, rd, fillrand = false, val) (mpstensor.hpp:40-71), left-paired blocks of `val`
+DMPS const_tensor(Ctx& c, const Index& sd, const Index& ld, const Index& rd, double val) {
+    DMPS t;
+    t.phys = sd;
+    Index lb = index_product(sd, ld), rb = rd;
+    common_subset(lb, rb);
+    t.right = rb;
+    Index possible = index_product(adjoin(sd), t.right), ltemp = ld;
+    common_subset(ltemp, possible);
+    t.left = ltemp;
+    lb.sort(); rb.sort(); t.left.sort(); t.right.sort();
+    t.right_paired = false;
+    t.b = layout_left_paired(t.phys, t.left, t.right);
+    for (std::size_t k = 0; k < t.b.n(); ++k)
+        if (t.b.rows[k] != lb.size_of(t.b.rc[k])) throw std::runtime_error("const MPS: left basis reduced by the right basis");
+    t.b.allocate(c.s, true);
+    for (std::size_t k = 0; k < t.b.n(); ++k) dev_fill(t.b.d.get() + t.b.off[k], t.b.elems(k), val, c.s);
+    return t;
+}
+}  // namespace
+
+DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, int nup, int ndown,
+                 const DMRGParams& prm, cudaStream_t s)
+    : mpo(single), ts_mpo(twosite), p(prm) {
+    c.s = s;
+    c.sv = std::make_unique<Solver>();
+    L = int(mpo.size());
+    if (L < 2 || int(ts_mpo.size()) != L - 1) throw std::runtime_error("DMRG: need L >= 2 site tensors and L - 1 two-site tensors");
+    const Index& phys = mpo[0].phys;
+    std::vector<Index> allowed = allowed_sectors(L, phys, Charge(nup, ndown), p.init_bond_dimension);
+    mps.resize(L);
+    for (int i = 0; i < L; ++i) {
+        mps[i] = const_tensor(c, phys, allowed[i], allowed[i + 1], 1.0);
+        scale(c, mps[i].b, 1.0 / std::sqrt(norm2(c, mps[i].b)));
+    }
+    for (int i = 0; i < L - 1; ++i) {
+        DBlocks t = normalize_left(c, mps[i]);
+        multiply_from_left(c, mps[i + 1], t);
+        scale(c, mps[i + 1].b, 1.0 / std::sqrt(norm2(c, mps[i + 1].b)));
+    }
+    normalize_left(c, mps[L - 1]);
+    for (int i = L - 1; i > 0; --i) {
+        DBlocks t = normalize_right(c, mps[i]);
+        multiply_from_right(c, mps[i - 1], t);
+        scale(c, mps[i - 1].b, 1.0 / std::sqrt(norm2(c, mps[i - 1].b)));
+    }
+    left_.resize(L + 1);
+    right_.resize(L + 1);
+    left_[0] = trivial_boundary(mps[0].left, mpo[0].rows, c.s);
+    right_[L] = trivial_boundary(mps[L - 1].right, mpo[L - 1].cols, c.s);
+    for (int i = L - 1; i >= 0; --i) {
+        make_right_paired(c, mps[i]);
+        right_[i] = boundary_step_right(c, *right_[i + 1], mps[i], mpo[i], true);
+    }
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+}
+
+void DevDMRG::sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc) {
+    energies.clear();
+    trunc.clear();
+    const double t_start = now_s();
+    for (int _site = 0; _site < 2 * L - 2; ++_site) {
+        int lr, site1, site2;
+        const int site = (_site < L - 1) ? _site : 2 * L - 2 - _site;
+        if (_site < L - 1) { lr = 1; site1 = site; site2 = site + 1; }
+        else { lr = -1; site1 = site - 1; site2 = site; }
+        const double t0 = now_s();
+        make_left_paired(c, mps[site1]);
+        make_right_paired(c, mps[site2]);
+        DTwoSite tst;
+        tst.build(c, mps[site1], mps[site2]);
+        auto plan = build_heff_plan(*left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, false);
+        plan->stream = c.s;
+        upload_plan(*plan);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        const double t1 = now_s();
+        st.plan_s += t1 - t0;
+        int iters = 0;
+        const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        const double t2 = now_s();
+        st.jd_s += t2 - t1;
+        st.hpsi_count += uint64_t(iters);
+        st.hpsi_flops += double(iters) * plan->flops;
+        plan.reset();
+        tst.twin_to_both(c);
+        energies.push_back(E + p.ecore);
+        TruncResults tr;
+        if (lr == 1) {
+            tr = tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+            DBlocks t = normalize_left(c, mps[site2]);
+            if (site2 < L - 1) multiply_from_left(c, mps[site2 + 1], t);
+            QCM_CUDA(cudaStreamSynchronize(c.s));
+            const double t3 = now_s();
+            st.trunc_s += t3 - t2;
+            DMPS ket = right_paired_copy(c, mps[site1]);
+            left_[site2] = boundary_step_left(c, *left_[site1], ket, mps[site1], mpo[site1], true);
+            QCM_CUDA(cudaStreamSynchronize(c.s));
+            st.boundary_s += now_s() - t3;
+        } else {
+            tr = tst.split(c, false, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+            DBlocks t = normalize_right(c, mps[site1]);
+            if (site1 > 0) multiply_from_right(c, mps[site1 - 1], t);
+            QCM_CUDA(cudaStreamSynchronize(c.s));
+            const double t3 = now_s();
+            st.trunc_s += t3 - t2;
+            right_[site2] = boundary_step_right(c, *right_[site2 + 1], mps[site2], mpo[site2], true);
+            QCM_CUDA(cudaStreamSynchronize(c.s));
+            st.boundary_s += now_s() - t3;
+        }
+        trunc.push_back(tr);
+    }
+    st.total_s += now_s() - t_start;
+}
+
+}  // namespace qcm

@@ -1,0 +1,108 @@
+"""Two-site DMRG on the device: Jacobi-Davidson solve, boundary steps and the sweep.
+
+Reference interface mirrored here:
+    solve<double>(out, initial, SH, ortho, jcd_gmres, jcd_tol, jcd_max_iter)   (solver/solver.cpp:14-28)
+    contraction::Engine::overlap_mpo_left_step / overlap_mpo_right_step       (contractions/engine.hpp:54-71)
+    ts_optimize::sweep                                                         (optimize/ts_optimize.hpp:114-362)
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import lib, check, P, c_int, c_void_p, c_uint64, c_double
+from .heff import Boundary, MPSDesc, _sectors
+
+
+class DMRGParams(ctypes.Structure):
+    _fields_ = [("max_bond_dimension", c_uint64), ("init_bond_dimension", c_uint64), ("truncation_cutoff", c_double),
+                ("jcd_tol", c_double), ("jcd_maxiter", ctypes.c_int32), ("ecore", c_double)]
+
+
+class TruncResult(ctypes.Structure):
+    _fields_ = [("bond_dimension", c_uint64), ("truncated_weight", c_double), ("truncated_fraction", c_double),
+                ("smallest_ev", c_double)]
+
+
+class DMRGStats(ctypes.Structure):
+    _fields_ = [("hpsi_count", c_uint64), ("hpsi_flops", c_double), ("plan_s", c_double), ("jd_s", c_double),
+                ("trunc_s", c_double), ("boundary_s", c_double), ("total_s", c_double)]
+
+
+_lib._sig("qcm_jd_solve", c_int, c_void_p, P(c_double), c_double, c_int, P(c_double), P(c_double), P(c_int))
+_lib._sig("qcm_boundary_step_left", c_int, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), P(c_double), c_int,
+          P(c_void_p))
+_lib._sig("qcm_boundary_step_right", c_int, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), P(c_double), c_int,
+          P(c_void_p))
+_lib._sig("qcm_dmrg_create", c_int, c_void_p, c_void_p, c_int, c_int, P(DMRGParams), P(c_void_p))
+_lib._sig("qcm_dmrg_length", c_int, c_void_p)
+_lib._sig("qcm_dmrg_sweep", c_int, c_void_p, P(c_double), P(TruncResult))
+_lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
+_lib._sig("qcm_dmrg_bond_dimensions", c_int, c_void_p, P(c_uint64))
+_lib._sig("qcm_dmrg_free", None, c_void_p)
+
+
+def jd_solve(plan, x0: np.ndarray, tol: float = 1e-10, maxiter: int = 8):
+    """Lowest eigenpair of a plan's H_eff from start vector x0: (eigenvalue, eigenvector, iterations)."""
+    x0 = np.ascontiguousarray(x0, dtype=np.float64)
+    assert x0.size == plan.n
+    out = np.empty_like(x0)
+    ev, it = c_double(), c_int()
+    check(lib.qcm_jd_solve(plan.h, _lib.dptr(x0), tol, maxiter, _lib.dptr(out), ctypes.byref(ev), ctypes.byref(it)),
+          "qcm_jd_solve")
+    return ev.value, out, it.value
+
+
+def boundary_step(ctx, B: Boundary, mpo, site: int, phys, left, right, data_rp: np.ndarray, side: str,
+                  symmetric: bool = True) -> Boundary:
+    """New boundary from site tensor `site` (right-paired blocks concatenated in left-sector order)
+    and the previous boundary B: side "left" (L[site] -> L[site+1]) or "right" (R[site+1] -> R[site])."""
+    ps, ls, rs = _sectors(phys), _sectors(left), _sectors(right)
+    d = MPSDesc()
+    d.n_phys, d.n_left, d.n_right = len(phys), len(left), len(right)
+    d.phys, d.left, d.right = ps, ls, rs
+    data_rp = np.ascontiguousarray(data_rp, dtype=np.float64)
+    h = c_void_p()
+    fn = lib.qcm_boundary_step_left if side == "left" else lib.qcm_boundary_step_right
+    check(fn(ctx.h, B.h, mpo.handle, site, ctypes.byref(d), _lib.dptr(data_rp), 1 if symmetric else 0, ctypes.byref(h)),
+          "qcm_boundary_step_" + side)
+    return Boundary.from_handle(ctx, h)
+
+
+class DMRG:
+    """Two-site ground-state DMRG (TwoU1, init_state = const) with every step on the device."""
+
+    def __init__(self, ctx, mpo, nup: int, ndown: int, max_bond_dimension: int, init_bond_dimension: int | None = None,
+                 truncation_cutoff: float = 1e-16, jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0):
+        self.ctx, self.mpo = ctx, mpo
+        p = DMRGParams(max_bond_dimension, init_bond_dimension or max_bond_dimension, truncation_cutoff, jcd_tol,
+                       jcd_maxiter, ecore)
+        h = c_void_p()
+        check(lib.qcm_dmrg_create(ctx.h, mpo.handle, nup, ndown, ctypes.byref(p), ctypes.byref(h)), "qcm_dmrg_create")
+        self.h = h
+        self.L = lib.qcm_dmrg_length(h)
+
+    def sweep(self):
+        """One sweep: (energies[2L-2], list of truncation dicts)."""
+        n = 2 * self.L - 2
+        E = np.zeros(n)
+        tr = (TruncResult * n)()
+        check(lib.qcm_dmrg_sweep(self.h, _lib.dptr(E), tr), "qcm_dmrg_sweep")
+        return E, [{f: getattr(t, f) for f, _ in TruncResult._fields_} for t in tr]
+
+    def stats(self) -> dict:
+        s = DMRGStats()
+        check(lib.qcm_dmrg_get_stats(self.h, ctypes.byref(s)), "qcm_dmrg_get_stats")
+        return {f: getattr(s, f) for f, _ in DMRGStats._fields_}
+
+    def bond_dimensions(self) -> np.ndarray:
+        d = np.zeros(self.L - 1, dtype=np.uint64)
+        check(lib.qcm_dmrg_bond_dimensions(self.h, d.ctypes.data_as(P(c_uint64))), "qcm_dmrg_bond_dimensions")
+        return d
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib.qcm_dmrg_free(self.h)
+            self.h = c_void_p()

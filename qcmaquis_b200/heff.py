@@ -51,12 +51,20 @@ class HeffInfo(ctypes.Structure):
                 ("l_len", c_uint64), ("r_len", c_uint64), ("n_kitems", c_uint64), ("flops_sdense", c_double), ("launches", c_uint64)]
 
 
+class BoundaryInfo(ctypes.Structure):
+    _fields_ = [("n_bra", c_uint32), ("n_ket", c_uint32), ("n_cohorts", c_uint32), ("aux_dim", c_uint32),
+                ("total", c_uint64), ("resident", c_uint32)]
+
+
 _lib._sig("qcm_ctx_create", c_int, c_int, P(c_void_p))
 _lib._sig("qcm_ctx_destroy", None, c_void_p)
 _lib._sig("qcm_ctx_synchronize", c_int, c_void_p)
 _lib._sig("qcm_boundary_upload", c_int, c_void_p, P(BoundaryDesc), P(c_void_p))
 _lib._sig("qcm_boundary_index_create", c_int, P(BoundaryDesc), P(c_void_p))
 _lib._sig("qcm_boundary_free", None, c_void_p)
+_lib._sig("qcm_boundary_get_info", c_int, c_void_p, P(BoundaryInfo))
+_lib._sig("qcm_boundary_download", c_int, c_void_p, P(Sector), P(Sector), P(c_uint32), P(c_uint32), P(ctypes.c_uint8),
+          P(c_uint32), P(ctypes.c_int64), P(c_double), P(c_uint64), P(c_double))
 _lib._sig("qcm_heff_plan_create", c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), c_int, P(c_void_p))
 _lib._sig("qcm_heff_get_info", c_int, c_void_p, P(HeffInfo))
 _lib._sig("qcm_heff_apply", c_int, c_void_p, P(c_double), P(c_double))
@@ -89,40 +97,49 @@ def _sectors(lst):
     return arr
 
 
-def parse_site_problem(blob: bytes):
-    off = 0
+class _Reader:
+    """Little-endian reader of the QSPB / QBSP blobs."""
 
-    def get(fmt):
-        nonlocal off
-        v = struct.unpack_from("<" + fmt, blob, off)
-        off += struct.calcsize("<" + fmt)
+    def __init__(self, blob: bytes):
+        self.blob, self.off = blob, 0
+
+    def get(self, fmt):
+        v = struct.unpack_from("<" + fmt, self.blob, self.off)
+        self.off += struct.calcsize("<" + fmt)
         return v
 
-    def idx():
-        (n,) = get("I")
-        return [get("iiI") for _ in range(n)]
+    def idx(self):
+        (n,) = self.get("I")
+        return [self.get("iiI") for _ in range(n)]
 
-    def arr(dtype, n):
-        nonlocal off
-        a = np.frombuffer(blob, dtype=dtype, count=n, offset=off).copy()
-        off += np.dtype(dtype).itemsize * n
+    def arr(self, dtype, n):
+        a = np.frombuffer(self.blob, dtype=dtype, count=n, offset=self.off).copy()
+        self.off += np.dtype(dtype).itemsize * n
         return a
 
-    def bnd():
-        bra, ket = idx(), idx()
-        nc, aux = get("II")
+    def blocks(self):
+        (nb,) = self.get("I")
+        out = []
+        for _ in range(nb):
+            a, b, r, c = self.get("iiII")
+            out.append(((a, b), self.arr("<f8", r * c).reshape(c, r).T))
+        return out
+
+    def bnd(self):
+        bra, ket = self.idx(), self.idx()
+        nc, aux = self.get("II")
         cb, ck, tr, ls, rs, nb = [], [], [], [], [], []
         offs, cs, data, doff = [], [], [], []
         pos = 0
         for _ in range(nc):
-            b0, k0 = get("II")
-            (t,) = get("B")
-            l, r, n = get("III")
+            b0, k0 = self.get("II")
+            (t,) = self.get("B")
+            l, r, n = self.get("III")
             cb.append(b0); ck.append(k0); tr.append(t); ls.append(l); rs.append(r); nb.append(n)
-            offs.append(arr("<i8", aux))
-            cs.append(arr("<f8", aux))
-            (nd,) = get("Q")
-            data.append(arr("<f8", nd))
+            offs.append(self.arr("<i8", aux))
+            cs.append(self.arr("<f8", aux))
+            (nd,) = self.get("Q")
+            data.append(self.arr("<f8", nd))
             doff.append(pos)
             pos += nd
         return dict(bra=bra, ket=ket, aux=aux, cohort_bra=np.array(cb, np.uint32), cohort_ket=np.array(ck, np.uint32),
@@ -133,17 +150,30 @@ def parse_site_problem(blob: bytes):
                     data=np.concatenate(data) if data else np.zeros(0),
                     data_offset=np.array(doff, np.uint64))
 
-    magic, ver = get("II")
+
+def parse_site_problem(blob: bytes):
+    r = _Reader(blob)
+    magic, ver = r.get("II")
     assert magic == 0x42505351 and ver == 1, "not a QSPB v1 site problem"
-    phys, left, right = idx(), idx(), idx()
-    (nb,) = get("I")
-    blocks = []
-    for _ in range(nb):
-        a, b, r, c = get("iiII")
-        blocks.append(((a, b), arr("<f8", r * c).reshape(c, r).T))
-    L = bnd()
-    R = bnd()
+    phys, left, right = r.idx(), r.idx(), r.idx()
+    blocks = r.blocks()
+    L = r.bnd()
+    R = r.bnd()
     return dict(phys=phys, left=left, right=right, blocks=blocks, L=L, R=R)
+
+
+def parse_boundary_step(blob: bytes):
+    """"QBSP" v1: u32 side (0 left, 1 right), u32 site; Index phys, left, right; the site
+    tensor's right-paired blocks (as in QSPB); input boundary; output boundary."""
+    r = _Reader(blob)
+    magic, ver = r.get("II")
+    assert magic == 0x50534251 and ver == 1, "not a QBSP v1 boundary step"
+    side, site = r.get("II")
+    phys, left, right = r.idx(), r.idx(), r.idx()
+    blocks = r.blocks()
+    bin_ = r.bnd()
+    bout = r.bnd()
+    return dict(side=side, site=site, phys=phys, left=left, right=right, blocks=blocks, B_in=bin_, B_out=bout)
 
 
 def twin_vector(problem) -> np.ndarray:
@@ -204,6 +234,42 @@ class Boundary:
             check(lib.qcm_boundary_upload(ctx.h, ctypes.byref(d), ctypes.byref(h)), "qcm_boundary_upload")
         self.h = h
         self._keep = None
+
+    @classmethod
+    def from_handle(cls, ctx, h):
+        b = cls.__new__(cls)
+        b.ctx, b.h, b._keep = ctx, h, None
+        return b
+
+    def info(self) -> dict:
+        i = BoundaryInfo()
+        check(lib.qcm_boundary_get_info(self.h, ctypes.byref(i)), "qcm_boundary_get_info")
+        return {f: getattr(i, f) for f, _ in BoundaryInfo._fields_}
+
+    def download(self) -> dict:
+        """Index and data as a dict with the fields of the boundary description (data_offset per cohort)."""
+        i = self.info()
+        nc, aux, nb_, nk_ = i["n_cohorts"], i["aux_dim"], i["n_bra"], i["n_ket"]
+        bra, ket = (Sector * max(1, nb_))(), (Sector * max(1, nk_))()
+        out = dict(cohort_bra=np.zeros(max(nc, 1), np.uint32), cohort_ket=np.zeros(max(nc, 1), np.uint32),
+                   tr=np.zeros(max(nc, 1), np.uint8), n_blocks=np.zeros(max(nc, 1), np.uint32),
+                   offsets=np.zeros(max(nc * aux, 1), np.int64), cscale=np.zeros(max(nc * aux, 1)),
+                   data_offset=np.zeros(max(nc, 1), np.uint64), data=np.zeros(max(i["total"], 1)))
+        check(lib.qcm_boundary_download(self.h, bra, ket, out["cohort_bra"].ctypes.data_as(P(c_uint32)),
+                                        out["cohort_ket"].ctypes.data_as(P(c_uint32)),
+                                        out["tr"].ctypes.data_as(P(ctypes.c_uint8)),
+                                        out["n_blocks"].ctypes.data_as(P(c_uint32)),
+                                        out["offsets"].ctypes.data_as(P(ctypes.c_int64)), _lib.dptr(out["cscale"]),
+                                        out["data_offset"].ctypes.data_as(P(c_uint64)),
+                                        _lib.dptr(out["data"]) if i["resident"] else None), "qcm_boundary_download")
+        for k in ("cohort_bra", "cohort_ket", "tr", "n_blocks", "data_offset"):
+            out[k] = out[k][:nc]
+        out["offsets"], out["cscale"] = out["offsets"][:nc * aux], out["cscale"][:nc * aux]
+        out["data"] = out["data"][:i["total"]]
+        out["bra"] = [(s.a, s.b, s.size) for s in bra[:nb_]]
+        out["ket"] = [(s.a, s.b, s.size) for s in ket[:nk_]]
+        out["aux"] = aux
+        return out
 
     def __del__(self):
         if getattr(self, "h", None) is not None and self.h.value:

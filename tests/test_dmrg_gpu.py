@@ -1,0 +1,122 @@
+"""Device boundary steps, Jacobi-Davidson and full sweeps against the oracle.
+
+Boundary steps: same site tensor and input boundary as the oracle's
+overlap_mpo_left/right_step (QBSP cases), every cohort block compared.
+JD: the oracle's frozen site problem, eigenvalue vs the oracle's step energy.
+Sweeps: per-step energies of whole two-site sweeps (gauge independent) within
+1e-10 Eh, bond dimensions and truncated weights per step.
+"""
+import numpy as np
+import pytest
+
+from helpers import qc_system, snapshot, site_of_step
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-10
+
+
+def _cohorts(b):
+    """{(bra charge, ket charge): (n_blocks, rows, cols, {b: block})} of a boundary dict."""
+    out = {}
+    aux = b["aux"]
+    for ci in range(len(b["cohort_bra"])):
+        bra = b["bra"][int(b["cohort_bra"][ci])]
+        ket = b["ket"][int(b["cohort_ket"][ci])]
+        r, c = bra[2], ket[2]
+        offs = b["offsets"][ci * aux:(ci + 1) * aux]
+        base = int(b["data_offset"][ci])
+        blocks = {}
+        for k in range(aux):
+            o = int(offs[k])
+            if o < 0 or b["tr"][ci]:
+                continue
+            blocks[k] = b["data"][base + o: base + o + r * c].reshape(c, r).T
+        out[(bra[:2], ket[:2])] = (int(b["n_blocks"][ci]), int(b["tr"][ci]), blocks,
+                                   tuple(b["cscale"][ci * aux:(ci + 1) * aux]))
+    return out
+
+
+def _step_case(L, M, sweeps_before, step, side, seed=0):
+    from oracle.oracle import OracleDMRG
+    from qcmaquis_b200.heff import parse_boundary_step
+    h, V, e, m, ts, blob = qc_system(L, seed)
+    d = OracleDMRG(blob, L, L // 2, L // 2, M)
+    for s in range(sweeps_before):
+        d.sweep(s)
+    d.snapshot(sweeps_before, step)  # stops before solving `step`
+    site1 = site_of_step(L, step)
+    site = site1 if side == 0 else site1 + 1
+    return m, parse_boundary_step(d.boundary_export(side, site))
+
+
+@pytest.mark.parametrize("L,M,sw,step,side", [(6, 16, 0, 2, 0), (6, 16, 1, 3, 1), (8, 32, 1, 3, 0), (8, 32, 1, 4, 1)])
+def test_boundary_step_matches_oracle(gpu_ctx, L, M, sw, step, side):
+    from qcmaquis_b200.dmrg import boundary_step
+    from qcmaquis_b200.heff import Boundary
+    m, case = _step_case(L, M, sw, step, side)
+    data_rp = np.concatenate([blk.T.ravel() for (_, blk) in case["blocks"]])
+    B = Boundary(gpu_ctx, case["B_in"])
+    out = boundary_step(gpu_ctx, B, m, case["site"], case["phys"], case["left"], case["right"], data_rp,
+                        "left" if side == 0 else "right")
+    got, ref = _cohorts(out.download()), _cohorts(case["B_out"])
+    assert set(got) == set(ref)
+    scale = max(np.abs(case["B_out"]["data"]).max(), 1.0)
+    for key, (nb, tr, blocks, cs) in ref.items():
+        gnb, gtr, gblocks, gcs = got[key]
+        assert (gnb, gtr) == (nb, tr), key
+        assert set(gblocks) == set(blocks), key
+        assert np.allclose(gcs, cs), key
+        for k, blk in blocks.items():
+            assert np.abs(gblocks[k] - blk).max() <= 1e-12 * scale, (key, k)
+
+
+@pytest.mark.parametrize("L,M,sw,step", [(6, 16, 1, 2), (8, 32, 1, 9)])
+def test_jd_matches_oracle_step_energy(gpu_ctx, L, M, sw, step):
+    from oracle.oracle import OracleDMRG
+    from qcmaquis_b200.dmrg import jd_solve
+    from qcmaquis_b200.heff import parse_site_problem, plan_from_problem, twin_vector
+    h, V, e, m, ts, blob = qc_system(L)
+    prob = parse_site_problem(snapshot(L, M, sw, step))
+    plan = plan_from_problem(gpu_ctx, prob, ts, site_of_step(L, step))
+    ev, vec, it = jd_solve(plan, twin_vector(prob), 1e-10, 8)
+    d = OracleDMRG(blob, L, L // 2, L // 2, M)
+    for s in range(sw):
+        d.sweep(s)
+    E_ref = d.sweep(sw)[0][step]
+    assert abs(ev - E_ref) < E_TOL
+    # the returned vector is a normalised eigenvector estimate with Rayleigh quotient ev
+    hv = plan.apply(vec)
+    assert abs(np.dot(vec, vec) - 1.0) < 1e-12
+    assert abs(np.dot(vec, hv) - ev) < 1e-9
+
+
+@pytest.mark.parametrize("L,M,sweeps", [(6, 16, 2), (8, 32, 2)])
+def test_sweep_energies_match_oracle(gpu_ctx, L, M, sweeps):
+    from oracle.oracle import OracleDMRG
+    from qcmaquis_b200.dmrg import DMRG
+    h, V, e, m, ts, blob = qc_system(L)
+    ref = OracleDMRG(blob, L, L // 2, L // 2, M)
+    dev = DMRG(gpu_ctx, m, L // 2, L // 2, M)
+    for s in range(sweeps):
+        E_ref, tw_ref, tf_ref, bd_ref = ref.sweep(s)
+        E, tr = dev.sweep()
+        assert np.abs(E - E_ref).max() < E_TOL, (s, E - E_ref)
+        bd = np.array([t["bond_dimension"] for t in tr])
+        assert np.array_equal(bd, bd_ref.astype(np.int64)), (s, bd, bd_ref)
+        tw = np.array([t["truncated_weight"] for t in tr])
+        assert np.allclose(tw, tw_ref, rtol=1e-6, atol=1e-14), (s, tw, tw_ref)
+
+
+def test_config1_sweeps_match_golden(gpu_ctx):
+    """L=8, N=8, M=64, 4 sweeps: per-sweep minimum energy vs the committed oracle golden values."""
+    import json
+    import os
+    from qcmaquis_b200.dmrg import DMRG
+    golden = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))
+    h, V, e, m, ts, blob = qc_system(8)
+    dev = DMRG(gpu_ctx, m, 4, 4, 64)
+    mins = [float(dev.sweep()[0].min()) for _ in range(4)]
+    ref = golden["config1_oracle_sweep_energies"]
+    assert np.abs(np.array(mins) - np.array(ref)).max() < E_TOL, (mins, ref)
+    assert abs(mins[-1] - golden["config1_fci"]) < 1e-8

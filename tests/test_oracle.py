@@ -72,3 +72,24 @@ def test_heff_linearity_and_symmetry():
     yab, _, _ = heff_apply(snap, blob, site_of_step(L, 2), 2.0 * a - 3.0 * b)
     assert np.abs(yab - (2 * ya - 3 * yb)).max() < 1e-11 * np.abs(yab).max()
     assert abs(a @ yb - b @ ya) < 1e-11 * np.abs(ya).max() * np.sqrt(n)
+
+
+def test_boundary_step_export_parses():
+    """QBSP cases: the site tensor's sectors match the input boundary and the output index."""
+    from oracle.oracle import OracleDMRG
+    from qcmaquis_b200.heff import parse_boundary_step
+    from tests.helpers import qc_system
+    h, V, e, m, ts, blob = qc_system(6)
+    d = OracleDMRG(blob, 6, 3, 3, 16)
+    d.sweep(0)
+    d.snapshot(1, 2)
+    for side, site in ((0, 2), (1, 3)):
+        c = parse_boundary_step(d.boundary_export(side, site))
+        assert (c["side"], c["site"]) == (side, site)
+        edge = c["left"] if side == 0 else c["right"]
+        new = c["right"] if side == 0 else c["left"]
+        assert c["B_in"]["bra"] == edge and c["B_out"]["bra"] == new
+        assert len(c["blocks"]) == len(c["left"])
+        for (ch, blk), sec in zip(c["blocks"], c["left"]):
+            assert ch == tuple(sec[:2]) and blk.shape[0] == sec[2]
+        assert np.isfinite(c["B_out"]["data"]).all() and np.abs(c["B_out"]["data"]).max() > 0
