@@ -237,6 +237,11 @@ typedef struct {
 /* mpo: single-site QC MPO; nup/ndown: u1_total_charge1/2.  Builds the const
  * MPS, canonises it to site 0 and the right boundaries. */
 int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const qcm_dmrg_params* params, qcm_dmrg** out);
+/* Same with a given MPS (restart): sites[i] / data[i] describe site tensor i
+ * right-paired, as for qcm_boundary_step_*; sites 1 .. L-1 right-normalised
+ * (the state canonize(0) leaves).  The right boundaries are built on the device. */
+int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* params, const qcm_mps_desc* sites,
+                             const double* const* data, qcm_dmrg** out);
 int qcm_dmrg_length(const qcm_dmrg* d);
 /* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL). */
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);

@@ -117,6 +117,16 @@ int orc_dmrg_boundary_export(orc_dmrg* h, int side, int site, void** out, size_t
     } catch (const std::exception& e) { return fail(e.what()); }
 }
 
+// Current site tensor `site` ("QMPS" v1, right-paired); free with orc_free.
+int orc_dmrg_mps_export(orc_dmrg* h, int site, void** out, size_t* len) {
+    try {
+        DMRG& d = *h->d;
+        if (site < 0 || site >= d.L) return fail("orc_dmrg_mps_export: site out of range");
+        *out = dup_blob(save_mps_tensor(d.mps[site]), len);
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
 // [hpsi_count, hpsi_time, hpsi_flops, jd_time, schedule_time, trunc_time, boundary_time]
 int orc_dmrg_stats(orc_dmrg* h, double* out) {
     DMRG& d = *h->d;

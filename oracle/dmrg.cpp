@@ -582,6 +582,22 @@ std::vector<uint8_t> save_site_problem(const MPSTensor& twin0, const Boundary& L
     return w.b;
 }
 
+std::vector<uint8_t> save_mps_tensor(const MPSTensor& m0) {
+    MPSTensor m = m0;
+    m.make_right_paired();
+    W w;
+    w.put<uint32_t>(0x53504D51u);  // "QMPS"
+    w.put<uint32_t>(1);
+    w.idx(m.phys); w.idx(m.left); w.idx(m.right);
+    w.put<uint32_t>(uint32_t(m.data.n_blocks()));
+    for (std::size_t k = 0; k < m.data.n_blocks(); ++k) {
+        w.put<int32_t>(m.data.lc[k].n[0]); w.put<int32_t>(m.data.lc[k].n[1]);
+        w.put<uint32_t>(uint32_t(m.data.b[k].r)); w.put<uint32_t>(uint32_t(m.data.b[k].c));
+        for (double v : m.data.b[k].d) w.put<double>(v);
+    }
+    return w.b;
+}
+
 std::vector<uint8_t> save_boundary_step(int side, int site, const MPSTensor& m0, const Boundary& in, const Boundary& out) {
     MPSTensor m = m0;
     m.make_right_paired();

@@ -72,6 +72,9 @@ struct DMRG {
 std::vector<uint8_t> save_site_problem(const MPSTensor& twin, const Boundary& L, const Boundary& R);
 void load_site_problem(const uint8_t* p, std::size_t n, MPSTensor& twin, Boundary& L, Boundary& R);
 
+// one site tensor ("QMPS" v1): Index phys, left, right; right-paired blocks as in QSPB
+std::vector<uint8_t> save_mps_tensor(const MPSTensor& m);
+
 // boundary step case ("QBSP" v1): side (0 left, 1 right), site; the site tensor (right-paired,
 // same block layout as QSPB); the input boundary; the oracle's output boundary
 std::vector<uint8_t> save_boundary_step(int side, int site, const MPSTensor& m, const Boundary& in, const Boundary& out);

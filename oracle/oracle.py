@@ -52,6 +52,7 @@ def lib(nthreads: int = 0):
                                      P(c_void_p), P(c_size_t)]
         L.orc_dmrg_stats.argtypes = [c_void_p, P(c_double)]
         L.orc_dmrg_boundary_export.argtypes = [c_void_p, c_int, c_int, P(c_void_p), P(c_size_t)]
+        L.orc_dmrg_mps_export.argtypes = [c_void_p, c_int, P(c_void_p), P(c_size_t)]
         L.orc_heff_apply.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), P(c_double), c_size_t,
                                      c_int, P(c_double), P(c_double)]
         L.orc_schedule_export.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_void_p), P(c_size_t),
@@ -106,6 +107,14 @@ class OracleDMRG:
         mps[site] from left_[site], side 1 = right step of mps[site] from right_[site + 1]."""
         p, n = c_void_p(), c_size_t()
         _check(self.lib, self.lib.orc_dmrg_boundary_export(self.h, side, site, ctypes.byref(p), ctypes.byref(n)))
+        b = ctypes.string_at(p, n.value)
+        self.lib.orc_free(p)
+        return b
+
+    def mps_export(self, site: int) -> bytes:
+        """Current site tensor ("QMPS" v1, right-paired blocks)."""
+        p, n = c_void_p(), c_size_t()
+        _check(self.lib, self.lib.orc_dmrg_mps_export(self.h, site, ctypes.byref(p), ctypes.byref(n)))
         b = ctypes.string_at(p, n.value)
         self.lib.orc_free(p)
         return b

@@ -12,7 +12,13 @@
 //   L_new = bra^T * S                      -> batched GEMM, one job per cohort
 // Cohort offsets follow Cohort::finalize (tasks.cpp:506-526): MPO indices with
 // coefficients get consecutive block positions in index order.
+//
+// The schedule is built per ket sector in parallel (OpenMP) from flat lookup
+// tables and merged in sector order, so the result does not depend on the
+// thread count.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
 #include <unordered_map>
@@ -24,12 +30,106 @@ namespace qcm {
 namespace {
 constexpr uint32_t NONE = 0xffffffffu;
 
+// QCM_STEP_TIMING=1 prints host schedule time and device time of every boundary step
+double step_now() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+void step_report(const char* side, double t0, double t1, cudaStream_t s) {
+    static const bool on = std::getenv("QCM_STEP_TIMING") != nullptr;
+    if (!on) return;
+    QCM_CUDA(cudaStreamSynchronize(s));
+    std::fprintf(stderr, "[bstep %s] schedule %.4f s, device %.4f s\n", side, t1 - t0, step_now() - t1);
+}
+
 void add_tiles(std::vector<TileD>* tiles, uint32_t item, uint32_t M, uint32_t N) {
     int sh = shape_for_rows(M);
     uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
     for (uint32_t n0 = 0; n0 < N; n0 += bn)
         for (uint32_t m0 = 0; m0 < M; m0 += bm) tiles[sh].push_back(TileD{item, m0, n0, 0});
 }
+
+// sparse operator entries of an MPO tensor, CSR per operator
+struct OpCSR {
+    std::vector<uint32_t> ptr, in, out;
+    std::vector<double> val;
+    explicit OpCSR(const MPOTensor& W) {
+        const std::size_t n = W.ops->size();
+        ptr.assign(n + 1, 0);
+        for (std::size_t o = 0; o < n; ++o) {
+            const SparseOp& s = (*W.ops)[o];
+            ptr[o] = uint32_t(in.size());
+            in.insert(in.end(), s.in.begin(), s.in.end());
+            out.insert(out.end(), s.out.begin(), s.out.end());
+            val.insert(val.end(), s.val.begin(), s.val.end());
+        }
+        ptr[n] = uint32_t(in.size());
+    }
+};
+
+// cohort of (sector a, sector b) by positions, and its storage partner
+void cohort_tables(const BoundaryIndexH& B, const Index& ia, const Index& ib, std::vector<uint32_t>& ci_t,
+                   std::vector<uint32_t>& ce_t) {
+    const std::size_t na = ia.size(), nb = ib.size();
+    ci_t.assign(na * nb, NONE);
+    ce_t.assign(na * nb, NONE);
+    for (std::size_t a = 0; a < na; ++a)
+        for (std::size_t b = 0; b < nb; ++b) {
+            uint32_t ci = B.cohort_index(ia[a].first, ib[b].first);
+            if (ci == B.n_cohorts()) continue;
+            uint32_t ce = B.tr[ci] ? B.cohort_index(ib[b].first, ia[a].first) : ci;
+            if (ce == B.n_cohorts()) throw std::runtime_error("boundary step: transposed cohort without partner");
+            ci_t[a * nb + b] = ci;
+            ce_t[a * nb + b] = ce;
+        }
+}
+
+// One ket sector's share of a boundary step; all offsets relative to the part.
+struct BPart {
+    std::vector<TJobD> tjobs;      // right step: grouped T-GEMM jobs
+    std::vector<GemmJob> tgemm;    // left step: T_b jobs (batched GEMM)
+    uint64_t t_len = 0;
+    SBuild sb;
+    uint64_t s_len = 0;
+    struct Coh { uint32_t bra, ket, nS; uint64_t s_off; std::vector<int64_t> offs; };
+    std::vector<Coh> coh;
+};
+
+struct Ent { uint32_t line_key; uint64_t slice; double a; };
+
+// Units of one cohort -> SBuild (lines = finalize positions)
+void emit_units(BPart& P, const std::vector<uint32_t>& pos, uint64_t s_off, const std::vector<uint64_t>& unit_off,
+                uint64_t line_stride, const std::vector<uint32_t>& erows, uint32_t col_stride,
+                const std::vector<uint32_t>& ne, std::vector<std::vector<Ent>>& em) {
+    for (std::size_t u = 0; u < em.size(); ++u) {
+        if (em[u].empty()) continue;
+        std::vector<uint32_t> lines;
+        std::vector<SBuild::E> ents;
+        ents.reserve(em[u].size());
+        for (const Ent& x : em[u]) {
+            const uint32_t p = pos[x.line_key];
+            if (lines.empty() || lines.back() != p) lines.push_back(p);
+            ents.push_back(SBuild::E{uint32_t(lines.size() - 1), x.slice, x.a});
+        }
+        P.sb.add_unit(s_off + unit_off[u], line_stride, erows[u], col_stride, ne[u], lines, ents);
+    }
+}
+
+// Appends src (offsets relative to its part) to dst with T / S bases.
+void append_sbuild(SBuild& dst, const SBuild& src, uint64_t t_base, uint64_t s_base) {
+    const uint32_t u0 = uint32_t(dst.units.size()), l0 = uint32_t(dst.line_b1.size()), k0 = uint32_t(dst.slice_off.size());
+    const uint32_t p0 = uint32_t(dst.sptr.size()), w0 = uint32_t(dst.went.size());
+    for (UnitD u : src.units) {
+        u.s_off += s_base; u.line0 += l0; u.slice0 += k0; u.sptr0 += p0;
+        dst.units.push_back(u);
+    }
+    dst.line_b1.insert(dst.line_b1.end(), src.line_b1.begin(), src.line_b1.end());
+    for (uint64_t o : src.slice_off) dst.slice_off.push_back(o + t_base);
+    for (uint32_t p : src.sptr) dst.sptr.push_back(p + w0);
+    dst.went.insert(dst.went.end(), src.went.begin(), src.went.end());
+    for (int k = 0; k < N_SHAPES; ++k)
+        for (TileD t : src.utiles[k]) { t.item += u0; dst.utiles[k].push_back(t); }
+}
+
 }  // namespace
 
 void SBuild::add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint32_t col_stride, uint32_t ne,
@@ -49,14 +149,9 @@ void SBuild::add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint
     u.nk = uint32_t(slices.size()); u.slice0 = uint32_t(slice_off.size()); u.sptr0 = uint32_t(sptr.size());
     line_b1.insert(line_b1.end(), lines.begin(), lines.end());
     slice_off.insert(slice_off.end(), slices.begin(), slices.end());
-    std::vector<uint32_t> cnt(u.nk + 1, 0);
-    for (uint32_t k : ek) cnt[k + 1]++;
-    for (uint32_t k = 0; k < u.nk; ++k) cnt[k + 1] += cnt[k];
-    const uint32_t w0 = uint32_t(went.size());
-    for (uint32_t k = 0; k <= u.nk; ++k) sptr.push_back(w0 + cnt[k]);
-    went.resize(w0 + ents.size());
-    std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
-    for (std::size_t i = 0; i < ents.size(); ++i) went[w0 + fill[ek[i]]++] = WEntD{ents[i].line, ek[i], ents[i].a};
+    std::vector<WEntD> es(ents.size());
+    for (std::size_t i = 0; i < ents.size(); ++i) es[i] = WEntD{ents[i].line, ek[i], ents[i].a};
+    pack_unit_entries(std::move(es), u.nk, went, sptr);
     int sh = shape_for_rows(u.nl);
     uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
     for (uint32_t n0 = 0; n0 < u.ne; n0 += bn)
@@ -89,24 +184,26 @@ void SBuild::upload(cudaStream_t s) {
 }
 
 void complement_transpose(BoundaryIndexH& x, const std::vector<int32_t>& herm, const std::vector<int32_t>& phase, bool forward) {
-    // rebuild the (bra, ket) -> cohort map, add transposed partners, fill Hermitian blocks
+    // add transposed partners of every cohort and fill Hermitian blocks (boundary.h:150-179)
     const uint32_t n0 = x.n_cohorts();
-    auto lookup = [&](uint32_t a, uint32_t b) -> uint32_t {
-        for (uint32_t ci = 0; ci < x.n_cohorts(); ++ci) if (x.cbra[ci] == a && x.cket[ci] == b) return ci;
-        return NONE;
-    };
+    std::unordered_map<uint64_t, uint32_t> where;
+    for (uint32_t ci = 0; ci < n0; ++ci) where[(uint64_t(x.cbra[ci]) << 32) | x.cket[ci]] = ci;
     for (uint32_t ciA = 0; ciA < n0; ++ciA) {
         Charge lb = x.bra[x.cbra[ciA]].first, rb = x.ket[x.cket[ciA]].first;
         std::size_t pb = x.bra.position(rb), pk = x.ket.position(lb);
         if (pb >= x.bra.size() || pk >= x.ket.size()) continue;
-        uint32_t ciB = lookup(uint32_t(pb), uint32_t(pk));
-        if (ciB == NONE) {
+        auto it = where.find((uint64_t(pb) << 32) | pk);
+        uint32_t ciB;
+        if (it == where.end()) {
             ciB = x.n_cohorts();
+            where[(uint64_t(pb) << 32) | pk] = ciB;
             x.cbra.push_back(uint32_t(pb)); x.cket.push_back(uint32_t(pk));
             x.lsz.push_back(uint32_t(x.bra[pb].second)); x.rsz.push_back(uint32_t(x.ket[pk].second));
             x.nb.push_back(0); x.tr.push_back(1);
             x.offsets.resize(x.offsets.size() + x.aux, -1);
             x.cscale.resize(x.cscale.size() + x.aux, 1.0);
+        } else {
+            ciB = it->second;
         }
         for (uint32_t b = 0; b < x.aux; ++b) {
             // Hermitian::skip(b, ket charge, bra charge): l < r and b has a partner
@@ -145,144 +242,168 @@ std::unique_ptr<DevBoundary> finish_boundary(BoundaryIndexH& idx, cudaStream_t s
 std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold, const DMPS& ket, const MPOTensor& W,
                                                  bool symmetric) {
     if (!ket.right_paired) throw std::runtime_error("boundary_step_right: ket must be right-paired");
+    const double tb0 = step_now();
     const BoundaryIndexH& R = Rold.idx;
     const Index& phys = ket.phys;
     const Index& left = ket.left;
     const Index& right = ket.right;
+    if (W.cols != R.aux) throw std::runtime_error("boundary_step_right: MPO column dimension differs from the boundary");
     ProductBasis rpb(phys, right, true);
     StateMap sm(phys);
-    const uint32_t nl = uint32_t(left.size()), nst = uint32_t(sm.nstates());
+    const uint32_t nl = uint32_t(left.size()), nr = uint32_t(right.size()), nps = uint32_t(phys.size());
+    const uint32_t nst = uint32_t(sm.nstates());
     // block offsets of the (right-paired) ket per left sector
     std::vector<uint64_t> koff(nl, 0);
     std::vector<uint32_t> kcols(nl, 0);
-    std::vector<bool> kok(nl, false);
+    std::vector<uint8_t> kok(nl, 0);
     for (uint32_t lb = 0; lb < nl; ++lb) {
         std::size_t k = ket.b.find_l(left[lb].first);
-        if (k < ket.b.n()) { koff[lb] = ket.b.off[k]; kcols[lb] = ket.b.cols[k]; kok[lb] = true; }
+        if (k < ket.b.n()) { koff[lb] = ket.b.off[k]; kcols[lb] = ket.b.cols[k]; kok[lb] = 1; }
     }
-    std::vector<TJobD> tjobs;
-    std::vector<TileD> ttiles[N_SHAPES];
-    uint64_t t_len = 0;
-    SBuild sb;
-    uint64_t s_len = 0;
-    std::vector<GemmJob> prop;
-    BoundaryIndexH nidx;
-    nidx.bra = left; nidx.ket = left; nidx.aux = W.rows;
-    struct Pending { uint64_t s_off; uint32_t lb_ket, lb_bra, nS; std::vector<int64_t> offs; };
-    std::vector<Pending> pend;
-    for (uint32_t lb_ket = 0; lb_ket < nl; ++lb_ket) {
+    // right sector, its size and column offset for (left sector, phys sector)
+    struct RSec { uint32_t rb, rs, off; };
+    std::vector<RSec> rsec(std::size_t(nl) * nps, RSec{NONE, 0, 0});
+    for (uint32_t lb = 0; lb < nl; ++lb)
+        for (uint32_t s = 0; s < nps; ++s) {
+            const Charge rc = left[lb].first + phys[s].first;
+            const std::size_t rb = right.position(rc);
+            if (rb < nr) rsec[std::size_t(lb) * nps + s] = RSec{uint32_t(rb), uint32_t(right[rb].second), uint32_t(rpb(phys[s].first, rc))};
+        }
+    std::vector<uint32_t> Rci, Rce;
+    cohort_tables(R, right, right, Rci, Rce);
+    const OpCSR oc(W);
+
+    std::vector<BPart> parts(nl);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int lbi = 0; lbi < int(nl); ++lbi) {
+        const uint32_t lb_ket = uint32_t(lbi);
         if (!kok[lb_ket]) continue;
+        BPart& P = parts[lb_ket];
         const Charge lc_ket = left[lb_ket].first;
         const uint32_t ls_ket = uint32_t(left[lb_ket].second);
-        // T jobs (rshtm_t_tasks): (mps offset, ci) -> job
-        std::unordered_map<uint64_t, uint32_t> tmap;
-        for (uint32_t s = 0; s < phys.size(); ++s) {
-            Charge rc_ket = lc_ket + phys[s].first;
-            std::size_t rbk = right.position(rc_ket);
-            if (rbk == right.size()) continue;
-            uint32_t rs_ket = uint32_t(right[rbk].second), koff_s = uint32_t(rpb(phys[s].first, rc_ket));
-            for (std::size_t rbb = 0; rbb < right.size(); ++rbb) {
-                uint32_t ci = R.cohort_index(rc_ket, right[rbb].first);
-                if (ci == R.n_cohorts()) continue;
-                uint32_t ce = R.tr[ci] ? R.cohort_index(right[rbb].first, rc_ket) : ci;
-                for (uint32_t ss = 0; ss < phys[s].second; ++ss) {
-                    uint32_t mo = koff_s + ss * rs_ket;
-                    TJobD j{};
-                    j.a_off = koff[lb_ket] + uint64_t(mo) * ls_ket;
-                    j.b_off = Rold.idx.data_off[ce];
-                    j.c_off = t_len;
-                    j.M = ls_ket; j.K = rs_ket; j.brs = R.rsz[ci]; j.N = R.nb[ce] * j.brs; j.lda = ls_ket;
-                    j.tr = ci != ce;
-                    tmap.emplace((uint64_t(mo) << 32) | ci, uint32_t(tjobs.size()));
-                    t_len += (uint64_t(j.M) * j.N + 31) / 32 * 32;
-                    if (j.M && j.N) add_tiles(ttiles, uint32_t(tjobs.size()), j.M, j.N);
-                    tjobs.push_back(j);
-                }
+        // T jobs (rshtm_t_tasks): one per (input state, bra right sector)
+        std::vector<uint32_t> tj(std::size_t(nst) * nr, NONE);
+        for (uint32_t st = 0; st < nst; ++st) {
+            const RSec& ri = rsec[std::size_t(lb_ket) * nps + sm.sector[st]];
+            if (ri.rb == NONE) continue;
+            for (uint32_t rbb = 0; rbb < nr; ++rbb) {
+                const uint32_t ci = Rci[std::size_t(ri.rb) * nr + rbb];
+                if (ci == NONE) continue;
+                const uint32_t ce = Rce[std::size_t(ri.rb) * nr + rbb];
+                TJobD j{};
+                j.a_off = koff[lb_ket] + uint64_t(ri.off + uint32_t(sm.sub[st]) * ri.rs) * ls_ket;
+                j.b_off = R.data_off[ce];
+                j.c_off = P.t_len;
+                j.M = ls_ket; j.K = ri.rs; j.brs = R.rsz[ci]; j.N = R.nb[ce] * j.brs; j.lda = ls_ket;
+                j.tr = ci != ce;
+                tj[std::size_t(st) * nr + rbb] = uint32_t(P.tjobs.size());
+                P.t_len += (uint64_t(j.M) * j.N + 31) / 32 * 32;
+                P.tjobs.push_back(j);
             }
         }
         // cohorts (rshtm_tasks)
+        std::vector<int> unit_of(nst, -1);
+        std::vector<uint32_t> line_count(W.rows, 0), pos(W.rows, NONE);
         for (uint32_t lb_bra = 0; lb_bra < nl; ++lb_bra) {
             const Charge lc_bra = left[lb_bra].first;
-            if (std::abs(lc_ket.particles() - lc_bra.particles()) > 2) continue;
-            if (!kok[lb_bra]) continue;
+            if (std::abs(lc_ket.particles() - lc_bra.particles()) > 2 || !kok[lb_bra]) continue;
             const uint32_t ls_bra = uint32_t(left[lb_bra].second);
-            struct U { uint32_t st, offset, ms; std::vector<std::pair<uint32_t, SBuild::E>> em; };
-            std::vector<U> units;
-            std::vector<int> unit_of(nst, -1);
-            uint32_t stripe = 0;
+            // units: output states whose right sector exists
+            std::vector<uint32_t> ust, urbb, uer, une;
+            std::vector<uint64_t> uoff;
+            std::fill(unit_of.begin(), unit_of.end(), -1);
             for (uint32_t st = 0; st < nst; ++st) {
-                Charge rc_bra = lc_bra + phys[sm.sector[st]].first;
-                std::size_t rbb = right.position(rc_bra);
-                if (rbb == right.size()) continue;
-                uint32_t rs = uint32_t(right[rbb].second);
-                unit_of[st] = int(units.size());
-                units.push_back(U{st, uint32_t(rpb(phys[sm.sector[st]].first, rc_bra)) + uint32_t(sm.sub[st]) * rs, rs, {}});
-                stripe += rs;
+                const RSec& ro = rsec[std::size_t(lb_bra) * nps + sm.sector[st]];
+                if (ro.rb == NONE) continue;
+                unit_of[st] = int(ust.size());
+                ust.push_back(st); urbb.push_back(ro.rb);
+                uoff.push_back(uint64_t(ro.off + uint32_t(sm.sub[st]) * ro.rs));
+                uer.push_back(ls_ket); une.push_back(ls_ket * ro.rs);
             }
-            std::vector<uint32_t> line_count(W.rows, 0);
+            std::vector<std::vector<Ent>> em(ust.size());
+            std::fill(line_count.begin(), line_count.end(), 0);
             for (uint32_t b1 = 0; b1 < W.rows; ++b1) {
                 if (symmetric && lc_ket < lc_bra && W.herm_left[b1] >= 0) continue;
                 for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
-                    const uint32_t b2 = W.b2[e];
-                    const SparseOp& op = (*W.ops)[W.op[e]];
-                    for (std::size_t k = 0; k < op.val.size(); ++k) {
-                        int u = unit_of[op.out[k]];
+                    const uint32_t b2 = W.b2[e], o = W.op[e];
+                    for (uint32_t k = oc.ptr[o]; k < oc.ptr[o + 1]; ++k) {
+                        const int u = unit_of[oc.out[k]];
                         if (u < 0) continue;
-                        const uint32_t sti = op.in[k];
-                        Charge rc_ket = lc_ket + phys[sm.sector[sti]].first;
-                        Charge rc_bra = lc_bra + phys[sm.sector[units[u].st]].first;
-                        uint32_t ci = R.cohort_index(rc_ket, rc_bra);
-                        if (!R.has_block(ci, b2)) continue;
-                        std::size_t rbk = right.position(rc_ket);
-                        if (rbk == right.size()) continue;
-                        uint32_t rs_ket = uint32_t(right[rbk].second);
-                        uint32_t mo = uint32_t(rpb(phys[sm.sector[sti]].first, rc_ket)) + uint32_t(sm.sub[sti]) * rs_ket;
-                        auto it = tmap.find((uint64_t(mo) << 32) | ci);
-                        if (it == tmap.end()) continue;
-                        uint32_t col = uint32_t(R.offset(ci, b2) / rs_ket);
-                        double a = op.val[k] * R.conj_scale(ci, b2) * W.scale[e];
-                        units[u].em.push_back({b1, SBuild::E{0, tjobs[it->second].c_off + uint64_t(col) * ls_ket, a}});
+                        const uint32_t sti = oc.in[k];
+                        const RSec& ri = rsec[std::size_t(lb_ket) * nps + sm.sector[sti]];
+                        if (ri.rb == NONE) continue;
+                        const uint32_t ci = Rci[std::size_t(ri.rb) * nr + urbb[u]];
+                        if (ci == NONE || !R.has_block(ci, b2)) continue;
+                        const uint32_t job = tj[std::size_t(sti) * nr + urbb[u]];
+                        if (job == NONE) continue;
+                        const uint64_t col = uint64_t(R.offset(ci, b2)) / ri.rs;
+                        const double a = oc.val[k] * R.conj_scale(ci, b2) * W.scale[e];
+                        em[u].push_back(Ent{b1, P.tjobs[job].c_off + col * ls_ket, a});
                         line_count[b1]++;
                     }
                 }
             }
             // finalize: MPO rows with coefficients get consecutive positions
-            std::vector<uint32_t> pos(W.rows, NONE);
             uint32_t nS = 0;
-            for (uint32_t b1 = 0; b1 < W.rows; ++b1) if (line_count[b1]) pos[b1] = nS++;
+            for (uint32_t b1 = 0; b1 < W.rows; ++b1) pos[b1] = line_count[b1] ? nS++ : NONE;
             if (nS == 0) continue;
             const uint32_t K_c = nS * ls_ket;
-            const uint64_t s_off = s_len;
-            s_len += (uint64_t(K_c) * stripe + 31) / 32 * 32;
-            for (U& u : units) {
-                if (u.em.empty()) continue;
-                std::vector<uint32_t> lines;
-                std::vector<SBuild::E> ents;
-                for (auto& pe : u.em) {
-                    uint32_t p = pos[pe.first];
-                    if (lines.empty() || lines.back() != p) lines.push_back(p);
-                    SBuild::E e = pe.second;
-                    e.line = uint32_t(lines.size() - 1);
-                    ents.push_back(e);
-                }
-                sb.add_unit(s_off + uint64_t(u.offset) * K_c, ls_ket, ls_ket, K_c, ls_ket * u.ms, lines, ents);
-            }
-            Pending pd{s_off, lb_ket, lb_bra, nS, std::vector<int64_t>(W.rows, -1)};
+            const uint64_t s_off = P.s_len;
+            P.s_len += (uint64_t(K_c) * kcols[lb_bra] + 31) / 32 * 32;
+            for (auto& x : uoff) x *= K_c;
+            emit_units(P, pos, s_off, uoff, ls_ket, uer, K_c, une, em);
+            BPart::Coh ch{lb_ket, lb_bra, nS, s_off, std::vector<int64_t>(W.rows, -1)};
             for (uint32_t b1 = 0; b1 < W.rows; ++b1)
-                if (pos[b1] != NONE) pd.offs[b1] = int64_t(pos[b1]) * ls_ket * ls_bra;
-            pend.push_back(std::move(pd));
+                if (pos[b1] != NONE) ch.offs[b1] = int64_t(pos[b1]) * ls_ket * ls_bra;
+            P.coh.push_back(std::move(ch));
         }
     }
-    // new boundary index (BoundaryIndex(ket_left_i, bra_left_i), add_cohort(lb_ket, rb))
-    for (auto& pd : pend) {
-        nidx.cbra.push_back(pd.lb_ket); nidx.cket.push_back(pd.lb_bra);
-        nidx.lsz.push_back(uint32_t(left[pd.lb_ket].second)); nidx.rsz.push_back(uint32_t(left[pd.lb_bra].second));
-        nidx.nb.push_back(pd.nS); nidx.tr.push_back(0);
-        nidx.offsets.insert(nidx.offsets.end(), pd.offs.begin(), pd.offs.end());
-        nidx.cscale.insert(nidx.cscale.end(), W.rows, 1.0);
+
+    // merge in ket-sector order; new index (BoundaryIndex(ket_left_i, bra_left_i))
+    std::vector<TJobD> tjobs;
+    std::vector<TileD> ttiles[N_SHAPES];
+    SBuild sb;
+    uint64_t t_len = 0, s_len = 0;
+    BoundaryIndexH nidx;
+    nidx.bra = left; nidx.ket = left; nidx.aux = W.rows;
+    struct Pend { uint32_t ci_new; uint32_t lb_ket, lb_bra, nS; uint64_t s_off; };
+    std::vector<Pend> pend;
+    for (uint32_t lb = 0; lb < nl; ++lb) {
+        BPart& P = parts[lb];
+        for (TJobD j : P.tjobs) {
+            j.c_off += t_len;
+            if (j.M && j.N) add_tiles(ttiles, uint32_t(tjobs.size()), j.M, j.N);
+            tjobs.push_back(j);
+        }
+        append_sbuild(sb, P.sb, t_len, s_len);
+        for (auto& ch : P.coh) {
+            pend.push_back(Pend{nidx.n_cohorts(), ch.bra, ch.ket, ch.nS, ch.s_off + s_len});
+            nidx.cbra.push_back(ch.bra); nidx.cket.push_back(ch.ket);
+            nidx.lsz.push_back(uint32_t(left[ch.bra].second)); nidx.rsz.push_back(uint32_t(left[ch.ket].second));
+            nidx.nb.push_back(ch.nS); nidx.tr.push_back(0);
+            nidx.offsets.insert(nidx.offsets.end(), ch.offs.begin(), ch.offs.end());
+            nidx.cscale.insert(nidx.cscale.end(), W.rows, 1.0);
+        }
+        t_len += P.t_len;
+        s_len += P.s_len;
+        P = BPart();
     }
-    complement_transpose(nidx, W.herm_left, W.phase_left, false);
+    if (symmetric) complement_transpose(nidx, W.herm_left, W.phase_left, false);
     auto Rn = finish_boundary(nidx, c.s);
+    // prop_r: new_R[b] (ls_ket x ls_bra) = S_b * bra^T
+    std::vector<GemmJob> prop;
+    for (const Pend& pd : pend) {
+        const uint32_t ls = uint32_t(left[pd.lb_ket].second), lsb = uint32_t(left[pd.lb_bra].second);
+        for (uint32_t b = 0; b < pd.nS; ++b) {
+            GemmJob g{};
+            g.a_off = pd.s_off + uint64_t(b) * ls; g.lda = pd.nS * ls;
+            g.b_off = koff[pd.lb_bra]; g.ldb = lsb; g.tb = 1;
+            g.c_off = Rn->idx.data_off[pd.ci_new] + uint64_t(b) * ls * lsb; g.ldc = ls;
+            g.M = ls; g.N = lsb; g.K = kcols[pd.lb_bra]; g.alpha = 1.0; g.beta = 0.0;
+            prop.push_back(g);
+        }
+    }
+    const double tb1 = step_now();
     // execute
     Ctx::ensure(c.T, t_len ? t_len : 1);
     Ctx::ensure(c.S, s_len ? s_len : 1);
@@ -295,23 +416,9 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
     if (s_len) QCM_CUDA(cudaMemsetAsync(c.S.get(), 0, s_len * sizeof(double), c.s));
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_sptr.get(),
               sb.d_went.get(), c.T.get(), c.S.get(), c.s);
-    // prop_r: new_R[b] (ls_ket x ls_bra) = S_b * bra^T
-    for (std::size_t i = 0; i < pend.size(); ++i) {
-        const Pending& pd = pend[i];
-        const uint32_t ls = uint32_t(left[pd.lb_ket].second), lsb = uint32_t(left[pd.lb_bra].second);
-        const uint32_t ci = Rn->idx.cohort_index(left[pd.lb_ket].first, left[pd.lb_bra].first);
-        const uint32_t stripe = kcols[pd.lb_bra];
-        for (uint32_t b = 0; b < pd.nS; ++b) {
-            GemmJob g{};
-            g.a_off = pd.s_off + uint64_t(b) * ls; g.lda = pd.nS * ls;
-            g.b_off = koff[pd.lb_bra]; g.ldb = lsb; g.tb = 1;
-            g.c_off = Rn->idx.data_off[ci] + uint64_t(b) * ls * lsb; g.ldc = ls;
-            g.M = ls; g.N = lsb; g.K = stripe; g.alpha = 1.0; g.beta = 0.0;
-            prop.push_back(g);
-        }
-    }
     // A = S scratch, B = ket data, C = new boundary: three different base pointers
     batched_gemm(prop, c.S.get(), s_len, ket.b.d.get(), ket.b.total, Rn->data.get(), Rn->idx.total, c.gjobs, c.gtiles, c.s);
+    step_report("right", tb0, tb1, c.s);
     return Rn;
 }
 
@@ -319,142 +426,170 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
 std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold, const DMPS& ket, const DMPS& bra,
                                                 const MPOTensor& W, bool symmetric) {
     if (!ket.right_paired || bra.right_paired) throw std::runtime_error("boundary_step_left: ket right-paired, bra left-paired");
+    const double tb0 = step_now();
     const BoundaryIndexH& L = Lold.idx;
     const Index& phys = ket.phys;
     const Index& left = ket.left;
     const Index& right = ket.right;
+    if (W.rows != L.aux) throw std::runtime_error("boundary_step_left: MPO row dimension differs from the boundary");
     ProductBasis kpb(phys, right, true);  // ket right-paired columns
     ProductBasis bpb(phys, left);         // bra left-paired rows
     StateMap sm(phys);
-    const uint32_t nl = uint32_t(left.size()), nr = uint32_t(right.size()), nst = uint32_t(sm.nstates());
+    const uint32_t nl = uint32_t(left.size()), nr = uint32_t(right.size()), nps = uint32_t(phys.size());
+    const uint32_t nst = uint32_t(sm.nstates());
     std::vector<uint64_t> koff(nl, 0), boff(nr, 0);
-    std::vector<bool> kok(nl, false), bok(nr, false);
+    std::vector<uint8_t> kok(nl, 0), bok(nr, 0);
     std::vector<uint32_t> brows(nr, 0);
     for (uint32_t lb = 0; lb < nl; ++lb) {
         std::size_t k = ket.b.find_l(left[lb].first);
-        if (k < ket.b.n()) { koff[lb] = ket.b.off[k]; kok[lb] = true; }
+        if (k < ket.b.n()) { koff[lb] = ket.b.off[k]; kok[lb] = 1; }
     }
     for (uint32_t rb = 0; rb < nr; ++rb) {
         std::size_t k = bra.b.find_r(right[rb].first);
-        if (k < bra.b.n()) { boff[rb] = bra.b.off[k]; brows[rb] = bra.b.rows[k]; bok[rb] = true; }
+        if (k < bra.b.n()) { boff[rb] = bra.b.off[k]; brows[rb] = bra.b.rows[k]; bok[rb] = 1; }
     }
-    std::vector<GemmJob> tj_gemm, prop;
-    uint64_t t_len = 0, s_len = 0;
-    SBuild sb;
-    BoundaryIndexH nidx;
-    nidx.bra = right; nidx.ket = right; nidx.aux = W.cols;
-    for (uint32_t rb_ket = 0; rb_ket < nr; ++rb_ket) {
+    // left sector, its size, ket column offset (right-paired) and bra row offset (left-paired)
+    // of (right sector, phys sector)
+    struct LSec { uint32_t lb, ls, koff, boff; };
+    std::vector<LSec> lsec(std::size_t(nr) * nps, LSec{NONE, 0, 0, 0});
+    for (uint32_t rb = 0; rb < nr; ++rb)
+        for (uint32_t s = 0; s < nps; ++s) {
+            const Charge lc = right[rb].first - phys[s].first;
+            const std::size_t lb = left.position(lc);
+            if (lb < nl)
+                lsec[std::size_t(rb) * nps + s] = LSec{uint32_t(lb), uint32_t(left[lb].second),
+                                                       uint32_t(kpb(phys[s].first, right[rb].first)), uint32_t(bpb(phys[s].first, lc))};
+        }
+    std::vector<uint32_t> Lci, Lce;
+    cohort_tables(L, left, left, Lci, Lce);
+    const OpCSR oc(W);
+
+    std::vector<BPart> parts(nr);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int rbi = 0; rbi < int(nr); ++rbi) {
+        const uint32_t rb_ket = uint32_t(rbi);
+        BPart& P = parts[rb_ket];
         const Charge rc_ket = right[rb_ket].first;
         const uint32_t rs_ket = uint32_t(right[rb_ket].second);
-        // T jobs (lshtm_t_tasks): T[ti] = nb blocks of ls_bra x rs_ket
-        std::unordered_map<uint64_t, uint64_t> tmap;  // (mps offset, ci) -> T offset
-        for (uint32_t s = 0; s < phys.size(); ++s) {
-            Charge lc_ket = rc_ket + (-phys[s].first);
-            std::size_t lbk = left.position(lc_ket);
-            if (lbk == left.size() || !kok[lbk]) continue;
-            const uint32_t ls_ket = uint32_t(left[lbk].second);
-            const uint32_t ko = uint32_t(kpb(phys[s].first, rc_ket));
+        // T jobs (lshtm_t_tasks): per (input state, bra left sector), nb GEMMs of ls_bra x rs_ket
+        std::vector<uint32_t> tj(std::size_t(nst) * nl, NONE);
+        std::vector<uint64_t> tj_off;
+        for (uint32_t st = 0; st < nst; ++st) {
+            const LSec& li = lsec[std::size_t(rb_ket) * nps + sm.sector[st]];
+            if (li.lb == NONE || !kok[li.lb]) continue;
+            const uint32_t ls_ket = li.ls, mo = li.koff + uint32_t(sm.sub[st]) * rs_ket;
             for (uint32_t lb_bra = 0; lb_bra < nl; ++lb_bra) {
-                uint32_t ci = L.cohort_index(left[lb_bra].first, lc_ket);
-                if (ci == L.n_cohorts()) continue;
-                uint32_t ce = L.tr[ci] ? L.cohort_index(lc_ket, left[lb_bra].first) : ci;
+                const uint32_t ci = Lci[std::size_t(lb_bra) * nl + li.lb];
+                if (ci == NONE) continue;
+                const uint32_t ce = Lce[std::size_t(lb_bra) * nl + li.lb];
                 const uint32_t ls_bra = uint32_t(left[lb_bra].second), nb = L.nb[ce];
-                for (uint32_t ss = 0; ss < phys[s].second; ++ss) {
-                    const uint32_t mo = ko + ss * rs_ket;
-                    const uint64_t c_off = t_len;
-                    tmap.emplace((uint64_t(mo) << 32) | ci, c_off);
-                    t_len += (uint64_t(ls_bra) * rs_ket * nb + 31) / 32 * 32;
-                    for (uint32_t b = 0; b < nb; ++b) {
-                        GemmJob g{};
-                        g.a_off = Lold.idx.data_off[ce] + uint64_t(b) * ls_bra * ls_ket;
-                        g.ta = (ci != ce); g.lda = g.ta ? ls_ket : ls_bra;
-                        g.b_off = koff[lbk] + uint64_t(mo) * ls_ket; g.ldb = ls_ket;
-                        g.c_off = c_off + uint64_t(b) * ls_bra * rs_ket; g.ldc = ls_bra;
-                        g.M = ls_bra; g.N = rs_ket; g.K = ls_ket; g.alpha = 1.0; g.beta = 0.0;
-                        tj_gemm.push_back(g);
-                    }
+                const uint64_t c_off = P.t_len;
+                tj[std::size_t(st) * nl + lb_bra] = uint32_t(tj_off.size());
+                tj_off.push_back(c_off);
+                P.t_len += (uint64_t(ls_bra) * rs_ket * nb + 31) / 32 * 32;
+                for (uint32_t b = 0; b < nb; ++b) {
+                    GemmJob g{};
+                    g.a_off = L.data_off[ce] + uint64_t(b) * ls_bra * ls_ket;
+                    g.ta = (ci != ce); g.lda = g.ta ? ls_ket : ls_bra;
+                    g.b_off = koff[li.lb] + uint64_t(mo) * ls_ket; g.ldb = ls_ket;
+                    g.c_off = c_off + uint64_t(b) * ls_bra * rs_ket; g.ldc = ls_bra;
+                    g.M = ls_bra; g.N = rs_ket; g.K = ls_ket; g.alpha = 1.0; g.beta = 0.0;
+                    P.tgemm.push_back(g);
                 }
             }
         }
         // cohorts (lshtm_tasks)
+        std::vector<int> unit_of(nst, -1);
+        std::vector<uint32_t> line_count(W.cols, 0), pos(W.cols, NONE);
         for (uint32_t rb_bra = 0; rb_bra < nr; ++rb_bra) {
             const Charge rc_bra = right[rb_bra].first;
             if (std::abs(rc_bra.particles() - rc_ket.particles()) > 2 || !bok[rb_bra]) continue;
             const uint32_t rs_bra = uint32_t(right[rb_bra].second), stripe = brows[rb_bra];
-            struct U { uint32_t st, offset, ms; Charge lc_bra; std::vector<std::pair<uint32_t, SBuild::E>> em; };
-            std::vector<U> units;
-            std::vector<int> unit_of(nst, -1);
+            std::vector<uint32_t> ust, ulb, uer, une;
+            std::vector<uint64_t> uoff;
+            std::fill(unit_of.begin(), unit_of.end(), -1);
             for (uint32_t st = 0; st < nst; ++st) {
-                Charge lc_bra = rc_bra + (-phys[sm.sector[st]].first);
-                std::size_t lbb = left.position(lc_bra);
-                if (lbb == left.size()) continue;
-                uint32_t ls_bra = uint32_t(left[lbb].second);
-                unit_of[st] = int(units.size());
-                units.push_back(U{st, uint32_t(bpb(phys[sm.sector[st]].first, lc_bra)) + uint32_t(sm.sub[st]) * ls_bra, ls_bra, lc_bra, {}});
+                const LSec& lo = lsec[std::size_t(rb_bra) * nps + sm.sector[st]];
+                if (lo.lb == NONE) continue;
+                unit_of[st] = int(ust.size());
+                ust.push_back(st); ulb.push_back(lo.lb);
+                uoff.push_back(uint64_t(lo.boff + uint32_t(sm.sub[st]) * lo.ls));
+                uer.push_back(lo.ls); une.push_back(lo.ls * rs_ket);
             }
-            std::vector<uint32_t> line_count(W.cols, 0);
+            std::vector<std::vector<Ent>> em(ust.size());
+            std::fill(line_count.begin(), line_count.end(), 0);
             for (uint32_t b2 = 0; b2 < W.cols; ++b2) {
                 if (symmetric && rc_bra < rc_ket && W.herm_right[b2] >= 0) continue;
                 for (uint32_t q = W.col_ptr[b2]; q < W.col_ptr[b2 + 1]; ++q) {
-                    const uint32_t e = W.col_ent[q], b1 = W.b1[e];
-                    const SparseOp& op = (*W.ops)[W.op[e]];
-                    for (std::size_t k = 0; k < op.val.size(); ++k) {
-                        int u = unit_of[op.out[k]];
+                    const uint32_t e = W.col_ent[q], b1 = W.b1[e], o = W.op[e];
+                    for (uint32_t k = oc.ptr[o]; k < oc.ptr[o + 1]; ++k) {
+                        const int u = unit_of[oc.out[k]];
                         if (u < 0) continue;
-                        const uint32_t sti = op.in[k];
-                        Charge lc_ket = rc_ket + (-phys[sm.sector[sti]].first);
-                        std::size_t lbk = left.position(lc_ket);
-                        if (lbk == left.size() || !kok[lbk]) continue;
-                        uint32_t ci = L.cohort_index(units[u].lc_bra, lc_ket);
-                        if (!L.has_block(ci, b1)) continue;
-                        const uint32_t ls_ket = uint32_t(left[lbk].second);
-                        const uint32_t mo = uint32_t(kpb(phys[sm.sector[sti]].first, rc_ket)) + uint32_t(sm.sub[sti]) * rs_ket;
-                        auto it = tmap.find((uint64_t(mo) << 32) | ci);
-                        if (it == tmap.end()) continue;
-                        const uint32_t col = uint32_t(L.offset(ci, b1) / ls_ket);
-                        const double a = op.val[k] * L.conj_scale(ci, b1) * W.scale[e];
-                        units[u].em.push_back({b2, SBuild::E{0, it->second + uint64_t(col) * rs_ket, a}});
+                        const uint32_t sti = oc.in[k];
+                        const LSec& li = lsec[std::size_t(rb_ket) * nps + sm.sector[sti]];
+                        if (li.lb == NONE || !kok[li.lb]) continue;
+                        const uint32_t ci = Lci[std::size_t(ulb[u]) * nl + li.lb];
+                        if (ci == NONE || !L.has_block(ci, b1)) continue;
+                        const uint32_t job = tj[std::size_t(sti) * nl + ulb[u]];
+                        if (job == NONE) continue;
+                        const uint64_t col = uint64_t(L.offset(ci, b1)) / li.ls;
+                        const double a = oc.val[k] * L.conj_scale(ci, b1) * W.scale[e];
+                        em[u].push_back(Ent{b2, tj_off[job] + col * rs_ket, a});
                         line_count[b2]++;
                     }
                 }
             }
-            std::vector<uint32_t> pos(W.cols, NONE);
             uint32_t nS = 0;
-            for (uint32_t b2 = 0; b2 < W.cols; ++b2) if (line_count[b2]) pos[b2] = nS++;
+            for (uint32_t b2 = 0; b2 < W.cols; ++b2) pos[b2] = line_count[b2] ? nS++ : NONE;
             if (nS == 0) continue;
-            const uint64_t s_off = s_len;
-            s_len += (uint64_t(stripe) * nS * rs_ket + 31) / 32 * 32;
-            for (U& u : units) {
-                if (u.em.empty()) continue;
-                std::vector<uint32_t> lines;
-                std::vector<SBuild::E> ents;
-                for (auto& pe : u.em) {
-                    uint32_t p = pos[pe.first];
-                    if (lines.empty() || lines.back() != p) lines.push_back(p);
-                    SBuild::E e = pe.second;
-                    e.line = uint32_t(lines.size() - 1);
-                    ents.push_back(e);
-                }
-                sb.add_unit(s_off + u.offset, uint64_t(rs_ket) * stripe, u.ms, stripe, u.ms * rs_ket, lines, ents);
-            }
-            // new cohort (rb_bra, rb_ket): nS blocks rs_bra x rs_ket
-            nidx.cbra.push_back(rb_bra); nidx.cket.push_back(rb_ket);
-            nidx.lsz.push_back(rs_bra); nidx.rsz.push_back(rs_ket);
-            nidx.nb.push_back(nS); nidx.tr.push_back(0);
+            const uint64_t s_off = P.s_len;
+            P.s_len += (uint64_t(stripe) * nS * rs_ket + 31) / 32 * 32;
+            emit_units(P, pos, s_off, uoff, uint64_t(rs_ket) * stripe, uer, stripe, une, em);
+            BPart::Coh ch{rb_bra, rb_ket, nS, s_off, std::vector<int64_t>(W.cols, -1)};
             for (uint32_t b2 = 0; b2 < W.cols; ++b2)
-                nidx.offsets.push_back(pos[b2] == NONE ? -1 : int64_t(pos[b2]) * rs_bra * rs_ket);
-            nidx.cscale.insert(nidx.cscale.end(), W.cols, 1.0);
-            GemmJob g{};
-            g.a_off = boff[rb_bra]; g.ta = 1; g.lda = stripe;
-            g.b_off = s_off; g.ldb = stripe;
-            g.c_off = uint64_t(nidx.n_cohorts() - 1);  // cohort index, resolved after the index is final
-            g.M = rs_bra; g.N = nS * rs_ket; g.K = stripe; g.alpha = 1.0; g.beta = 0.0;
-            prop.push_back(g);
+                if (pos[b2] != NONE) ch.offs[b2] = int64_t(pos[b2]) * rs_bra * rs_ket;
+            P.coh.push_back(std::move(ch));
         }
+    }
+
+    // merge in ket-sector order; new index (BoundaryIndex(bra_right_i, ket_right_i))
+    std::vector<GemmJob> tj_gemm;
+    SBuild sb;
+    uint64_t t_len = 0, s_len = 0;
+    BoundaryIndexH nidx;
+    nidx.bra = right; nidx.ket = right; nidx.aux = W.cols;
+    struct Pend { uint32_t ci_new, rb_bra, nS; uint64_t s_off; uint32_t rs_ket; };
+    std::vector<Pend> pend;
+    for (uint32_t rb = 0; rb < nr; ++rb) {
+        BPart& P = parts[rb];
+        for (GemmJob g : P.tgemm) { g.c_off += t_len; tj_gemm.push_back(g); }
+        append_sbuild(sb, P.sb, t_len, s_len);
+        for (auto& ch : P.coh) {
+            pend.push_back(Pend{nidx.n_cohorts(), ch.bra, ch.nS, ch.s_off + s_len, uint32_t(right[ch.ket].second)});
+            nidx.cbra.push_back(ch.bra); nidx.cket.push_back(ch.ket);
+            nidx.lsz.push_back(uint32_t(right[ch.bra].second)); nidx.rsz.push_back(uint32_t(right[ch.ket].second));
+            nidx.nb.push_back(ch.nS); nidx.tr.push_back(0);
+            nidx.offsets.insert(nidx.offsets.end(), ch.offs.begin(), ch.offs.end());
+            nidx.cscale.insert(nidx.cscale.end(), W.cols, 1.0);
+        }
+        t_len += P.t_len;
+        s_len += P.s_len;
+        P = BPart();
     }
     if (symmetric) complement_transpose(nidx, W.herm_right, W.phase_right, true);
     auto Ln = finish_boundary(nidx, c.s);
-    for (auto& g : prop) { g.ldc = uint32_t(g.M); g.c_off = Ln->idx.data_off[g.c_off]; }
+    // prop_l: L_new (rs_bra x nS*rs_ket) = bra^T * S
+    std::vector<GemmJob> prop;
+    for (const Pend& pd : pend) {
+        GemmJob g{};
+        g.a_off = boff[pd.rb_bra]; g.ta = 1; g.lda = brows[pd.rb_bra];
+        g.b_off = pd.s_off; g.ldb = brows[pd.rb_bra];
+        g.c_off = Ln->idx.data_off[pd.ci_new]; g.ldc = uint32_t(right[pd.rb_bra].second);
+        g.M = uint32_t(right[pd.rb_bra].second); g.N = pd.nS * pd.rs_ket; g.K = brows[pd.rb_bra];
+        g.alpha = 1.0; g.beta = 0.0;
+        prop.push_back(g);
+    }
+    const double tb1 = step_now();
     Ctx::ensure(c.T, t_len ? t_len : 1);
     Ctx::ensure(c.S, s_len ? s_len : 1);
     batched_gemm(tj_gemm, Lold.data.get(), Lold.idx.total, ket.b.d.get(), ket.b.total, c.T.get(), t_len, c.gjobs, c.gtiles, c.s);
@@ -464,6 +599,7 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_sptr.get(),
               sb.d_went.get(), c.T.get(), c.S.get(), c.s);
     batched_gemm(prop, bra.b.d.get(), bra.b.total, c.S.get(), s_len, Ln->data.get(), Ln->idx.total, c.gjobs, c.gtiles, c.s);
+    step_report("left", tb0, tb1, c.s);
     return Ln;
 }
 

@@ -180,6 +180,37 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     QCM_CATCH
 }
 
+int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* prm, const qcm_mps_desc* sites,
+                             const double* const* data, qcm_dmrg** out) {
+    QCM_TRY
+    if (!ctx || !mpo || !prm || !sites || !data || !out) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: NULL argument");
+    const qcm::MPO& m = qcm::mpo_of(mpo);
+    if (m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: expected a single-site MPO");
+    if (prm->jcd_maxiter < 1 || prm->jcd_maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: jcd_maxiter must be in 1..64");
+    QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::DMRGParams p;
+    p.Mmax = prm->max_bond_dimension;
+    p.init_bond_dimension = prm->init_bond_dimension;
+    p.cutoff = prm->truncation_cutoff;
+    p.jcd_tol = prm->jcd_tol;
+    p.jcd_maxiter = prm->jcd_maxiter;
+    p.ecore = prm->ecore;
+    qcm::Ctx tmp;
+    tmp.s = ctx->stream;
+    std::vector<qcm::DMPS> ms;
+    for (std::size_t i = 0; i < m.t.size(); ++i) {
+        if (!data[i]) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: NULL site data");
+        ms.push_back(upload_mps(tmp, &sites[i], data[i]));
+    }
+    qcm::MPO ts = qcm::make_twosite_mpo(m);
+    auto d = std::make_unique<qcm_dmrg>();
+    d->ctx = ctx;
+    d->e = std::make_unique<qcm::DevDMRG>(m.t, ts.t, std::move(ms), p, ctx->stream);
+    *out = d.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_dmrg_length(const qcm_dmrg* d) { return d ? d->e->L : -1; }
 
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc) {

@@ -164,9 +164,16 @@ struct DevDMRG {
     DMRGParams p;
     DMRGStats st;
     Ctx c;
+    // const MPS over the allowed sectors of (nup, ndown), canonised to site 0
     DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, int nup, int ndown,
             const DMRGParams& prm, cudaStream_t s);
+    // given MPS (right-normalised on sites 1 .. L-1, as after canonize(0))
+    DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, std::vector<DMPS> sites,
+            const DMRGParams& prm, cudaStream_t s);
     void sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc);
+
+  private:
+    void init_boundaries();
 };
 
 }  // namespace qcm

@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <memory>
 #include <unordered_map>
@@ -95,6 +96,25 @@ struct KItemD {       // split-K work item of the L.S GEMM: output tile, one seg
 struct OTileD {       // output tile of the L.S GEMM and its contiguous range of split-K partials
     uint32_t out, m0, n0, part0, nparts, pad0, pad1, pad2;
 };
+
+// Appends one unit's coefficient entries (line, slice k, alpha) to went, sorted by
+// (slice, line), with entries that share (line, slice) summed in their input order --
+// several MPO terms may couple the same boundary block, input state and output state,
+// and the densified coefficient tile holds their sum -- and the unit's nk + 1 slice
+// pointers to sptr.
+inline void pack_unit_entries(std::vector<WEntD> ents, uint32_t nk, std::vector<WEntD>& went, std::vector<uint32_t>& sptr) {
+    std::stable_sort(ents.begin(), ents.end(),
+                     [](const WEntD& x, const WEntD& y) { return x.k < y.k || (x.k == y.k && x.line < y.line); });
+    const uint32_t w0 = uint32_t(went.size());
+    uint32_t k = 0;
+    sptr.push_back(w0);
+    for (std::size_t i = 0; i < ents.size(); ++i) {
+        while (k < ents[i].k) { sptr.push_back(uint32_t(went.size())); ++k; }
+        if (went.size() > w0 && went.back().k == ents[i].k && went.back().line == ents[i].line) went.back().a += ents[i].a;
+        else went.push_back(ents[i]);
+    }
+    while (k < nk) { sptr.push_back(uint32_t(went.size())); ++k; }
+}
 
 // DMMA tile shapes (rows x cols of the CTA tile); the class is chosen per job from its row count
 enum { SHAPE_16 = 0, SHAPE_32 = 1, SHAPE_64 = 2, N_SHAPES = 3 };

@@ -257,18 +257,11 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     uint32_t pos = gp - job_pos0[job];
                     P.slice_off.push_back(P.tjobs[job].c_off + uint64_t(pos) * u.ms * ls_in);
                 }
-                // entries sorted by slice (counting sort)
-                std::vector<uint32_t> cnt(ud.nk + 1, 0);
-                for (Em& m : u.em) cnt[slot[m.slice] + 1]++;
-                for (uint32_t k = 0; k < ud.nk; ++k) cnt[k + 1] += cnt[k];
-                const uint32_t w0 = uint32_t(P.went.size());
-                for (uint32_t k = 0; k <= ud.nk; ++k) P.sptr.push_back(w0 + cnt[k]);
-                P.went.resize(w0 + u.em.size());
-                std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
-                for (Em& m : u.em) {
-                    uint32_t k = slot[m.slice];
-                    P.went[w0 + fill[k]++] = WEntD{m.line, k, m.a};
-                }
+                // entries sorted by slice, duplicates of (line, slice) summed
+                std::vector<WEntD> ents;
+                ents.reserve(u.em.size());
+                for (Em& m : u.em) ents.push_back(WEntD{m.line, slot[m.slice], m.a});
+                pack_unit_entries(std::move(ents), ud.nk, P.went, P.sptr);
                 if (bookkeeping)
                     for (Em& m : u.em) {
                         uint32_t row[10] = {lb_in, lb_out, ci, ce, u.offset, u.ms, u.lines[m.line], m.mps, m.cir, m.col};

@@ -210,6 +210,23 @@ DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTens
         multiply_from_right(c, mps[i - 1], t);
         scale(c, mps[i - 1].b, 1.0 / std::sqrt(norm2(c, mps[i - 1].b)));
     }
+    init_boundaries();
+}
+
+DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, std::vector<DMPS> sites,
+                 const DMRGParams& prm, cudaStream_t s)
+    : mpo(single), ts_mpo(twosite), mps(std::move(sites)), p(prm) {
+    c.s = s;
+    c.sv = std::make_unique<Solver>();
+    L = int(mpo.size());
+    if (L < 2 || int(ts_mpo.size()) != L - 1 || int(mps.size()) != L)
+        throw std::runtime_error("DMRG: need L site tensors, L MPO tensors and L - 1 two-site tensors");
+    for (int i = 0; i + 1 < L; ++i)
+        if (!(mps[i].right == mps[i + 1].left)) throw std::runtime_error("DMRG: site tensors do not share their bond indices");
+    init_boundaries();
+}
+
+void DevDMRG::init_boundaries() {
     left_.resize(L + 1);
     right_.resize(L + 1);
     left_[0] = trivial_boundary(mps[0].left, mpo[0].rows, c.s);

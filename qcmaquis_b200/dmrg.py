@@ -37,6 +37,8 @@ _lib._sig("qcm_boundary_step_left", c_int, c_void_p, c_void_p, c_void_p, c_int, 
 _lib._sig("qcm_boundary_step_right", c_int, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), P(c_double), c_int,
           P(c_void_p))
 _lib._sig("qcm_dmrg_create", c_int, c_void_p, c_void_p, c_int, c_int, P(DMRGParams), P(c_void_p))
+_lib._sig("qcm_dmrg_create_from_mps", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)),
+          P(c_void_p))
 _lib._sig("qcm_dmrg_length", c_int, c_void_p)
 _lib._sig("qcm_dmrg_sweep", c_int, c_void_p, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
@@ -83,6 +85,32 @@ class DMRG:
         check(lib.qcm_dmrg_create(ctx.h, mpo.handle, nup, ndown, ctypes.byref(p), ctypes.byref(h)), "qcm_dmrg_create")
         self.h = h
         self.L = lib.qcm_dmrg_length(h)
+
+    @classmethod
+    def from_mps(cls, ctx, mpo, sites, max_bond_dimension: int, truncation_cutoff: float = 1e-16,
+                 jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0):
+        """Restart from a given MPS: sites = [dict(phys, left, right, blocks)] with right-paired blocks
+        (one per left sector, in sector order), sites 1 .. L-1 right-normalised."""
+        self = cls.__new__(cls)
+        self.ctx, self.mpo = ctx, mpo
+        p = DMRGParams(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore)
+        descs = (MPSDesc * len(sites))()
+        keep, ptrs = [], (P(c_double) * len(sites))()
+        for i, st in enumerate(sites):
+            if [tuple(b[0]) for b in st["blocks"]] != [tuple(x[:2]) for x in st["left"]]:
+                raise ValueError(f"site {i}: expected one right-paired block per left sector, in sector order")
+            ps, ls, rs = _sectors(st["phys"]), _sectors(st["left"]), _sectors(st["right"])
+            data = np.ascontiguousarray(np.concatenate([blk.T.ravel() for (_, blk) in st["blocks"]]))
+            keep += [ps, ls, rs, data]
+            descs[i].n_phys, descs[i].n_left, descs[i].n_right = len(st["phys"]), len(st["left"]), len(st["right"])
+            descs[i].phys, descs[i].left, descs[i].right = ps, ls, rs
+            ptrs[i] = _lib.dptr(data)
+        h = c_void_p()
+        check(lib.qcm_dmrg_create_from_mps(ctx.h, mpo.handle, ctypes.byref(p), descs, ptrs, ctypes.byref(h)),
+              "qcm_dmrg_create_from_mps")
+        self.h = h
+        self.L = lib.qcm_dmrg_length(h)
+        return self
 
     def sweep(self):
         """One sweep: (energies[2L-2], list of truncation dicts)."""

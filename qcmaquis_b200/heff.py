@@ -162,6 +162,15 @@ def parse_site_problem(blob: bytes):
     return dict(phys=phys, left=left, right=right, blocks=blocks, L=L, R=R)
 
 
+def parse_mps_tensor(blob: bytes):
+    """"QMPS" v1: Index phys, left, right; right-paired blocks (ls x stripe) in left-sector order."""
+    r = _Reader(blob)
+    magic, ver = r.get("II")
+    assert magic == 0x53504D51 and ver == 1, "not a QMPS v1 site tensor"
+    phys, left, right = r.idx(), r.idx(), r.idx()
+    return dict(phys=phys, left=left, right=right, blocks=r.blocks())
+
+
 def parse_boundary_step(blob: bytes):
     """"QBSP" v1: u32 side (0 left, 1 right), u32 site; Index phys, left, right; the site
     tensor's right-paired blocks (as in QSPB); input boundary; output boundary."""

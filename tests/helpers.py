@@ -62,3 +62,79 @@ def parse_schedule_export(sch: bytes):
                         rows.append((lb, rb, ci, cie, uo, ms, b1, tj[a[1]][0], tj[a[1]][1], a[2], a[0]))
                     k += cnt
     return rows
+
+
+# ---------------------------------------------------------------------------
+# dense restatement of one boundary step (independent of the block bookkeeping)
+
+def _offsets(idx):
+    o, t = [], 0
+    for (_, _, s) in idx:
+        o.append(t)
+        t += s
+    return o, t
+
+
+def dense_site_tensor(phys, left, right, blocks):
+    """A[state, l, r] from right-paired blocks (columns ordered by ProductBasis(phys, right, -p + r))."""
+    lo, ln = _offsets(left)
+    ro, rn = _offsets(right)
+    so, sn = _offsets(phys)
+    rpos = {(a, b): i for i, (a, b, _) in enumerate(right)}
+    lpos = {(a, b): i for i, (a, b, _) in enumerate(left)}
+    A = np.zeros((sn, ln, rn))
+    for (ch, blk) in blocks:
+        lb = lpos[ch]
+        col = 0
+        for s, (pa, pb, d) in enumerate(phys):
+            rc = (ch[0] + pa, ch[1] + pb)
+            if rc not in rpos:
+                continue
+            rb = rpos[rc]
+            rs = right[rb][2]
+            for ss in range(d):
+                A[so[s] + ss, lo[lb]:lo[lb] + left[lb][2], ro[rb]:ro[rb] + rs] = blk[:, col:col + rs]
+                col += rs
+        assert col == blk.shape[1]
+    return A
+
+
+def dense_boundary(b):
+    """B[aux, bra, ket] of a boundary dict (cohort blocks bra size x ket size)."""
+    bo, bn = _offsets(b["bra"])
+    ko, kn = _offsets(b["ket"])
+    aux = b["aux"]
+    B = np.zeros((aux, bn, kn))
+    for ci in range(len(b["cohort_bra"])):
+        if b["tr"][ci]:
+            assert (b["offsets"][ci * aux:(ci + 1) * aux] < 0).all()
+            continue
+        i, j = int(b["cohort_bra"][ci]), int(b["cohort_ket"][ci])
+        r, c = b["bra"][i][2], b["ket"][j][2]
+        base = int(b["data_offset"][ci])
+        for k in range(aux):
+            o = int(b["offsets"][ci * aux + k])
+            if o >= 0:
+                B[k, bo[i]:bo[i] + r, ko[j]:ko[j] + c] = b["data"][base + o: base + o + r * c].reshape(c, r).T
+    return B
+
+
+def dense_mpo_tensor(t):
+    """W[b1, b2, out, in] of one MPO tensor dict (mpo.parse_blob)."""
+    n = sum(s[2] for s in t["phys"])
+    W = np.zeros((t["rows"], t["cols"], n, n))
+    for e in range(len(t["b1"])):
+        op = t["ops"][int(t["op"][e])]
+        W[int(t["b1"][e]), int(t["b2"][e]), op["out"], op["inp"]] += t["scale"][e] * op["val"]
+    return W
+
+
+def dense_boundary_step(case, mpo_tensor):
+    """New boundary of a QBSP case, dense: left  L'[b2, r', r] = A[s', l', r'] L[b1, l', l] W[b1, b2, s', s] A[s, l, r];
+    right R'[b1, l, l'] = A[s, l, r] W[b1, b2, s', s] R[b2, r, r'] A[s', l', r']."""
+    A = dense_site_tensor(case["phys"], case["left"], case["right"], case["blocks"])
+    B = dense_boundary(case["B_in"])
+    W = dense_mpo_tensor(mpo_tensor)
+    if case["side"] == 0:
+        return np.einsum("pak,xac,xypq,qcl->ykl", A, B, W, A, optimize=True)
+    return np.einsum("qak,xypq,ykl,pbl->xab", A, W, B, A, optimize=True)
