@@ -2,21 +2,26 @@
 """Benchmark of the two-site DMRG effective-Hamiltonian hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--L 16] [--M 256] [--seed 0]
+                    [--L 24] [--M 512] [--init-bd 64] [--sweeps 2] [--seed 0]
 
-A step is one H_eff . psi (the Davidson callback, super_hamil_mv) on a frozen
-two-site problem: the middle bond of a seeded synthetic ab-initio Hamiltonian
-(TwoU1, Sz = 0, N = L electrons) after one full two-site sweep at bond
-dimension M.  The frozen problem (twin MPS, left/right boundaries, two-site
-MPO) is produced on the host by the oracle sweep, then moved to HBM; only the
-H_eff apply is timed.
+Workload: the seeded synthetic ab-initio Hamiltonian of the precision-form
+configuration (L = 24 orbitals, N = 24 electrons, TwoU1 Sz = 0, M = 512; FP64
+plain form).  Setup (untimed): the device engine runs `--sweeps` full two-site
+sweeps from the const initial state (each timed on its own and reported under
+"sweep"), then continues the next sweep up to the middle bond (step L/2 - 1)
+and freezes that site problem.
 
-`value` = reference work count (ScheduleNew::total_flops, solver/tasks.cpp:
-388-398, 777-796) x steps / device time (CUDA events, L2 flushed between
-steps), summed over ranks / max over ranks.  `e2e` is the same metric through
-qcm_heff_apply with pinned host buffers (H2D of psi and D2H of H.psi inside
-the timed region).  The path does not shard across GPUs here (one B200 per
-solve): N > 1 runs N independent replicas.
+A step is one H_eff . psi (the Davidson callback, super_hamil_mv) on that
+frozen problem.  `value` = reference work count (ScheduleNew::total_flops,
+solver/tasks.cpp:388-398, 777-796) x steps / device time (CUDA events on the
+plan stream, L2 flushed between steps), summed over ranks / max over ranks.
+`e2e` is the same metric through qcm_heff_apply with pinned host buffers (H2D
+of psi and D2H of H.psi inside the timed region).  The path does not shard
+across GPUs here (one B200 per solve): N > 1 runs N independent replicas.
+
+The reference arm (--impl reference) times the CPU restatement of the same
+H.psi (the oracle: OpenMP over ket sectors, OpenBLAS dgemm) on the same frozen
+problem, exported by the device engine as a "QSPB" blob.
 """
 from __future__ import annotations
 
@@ -40,30 +45,50 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--L", type=int, default=16)
-    ap.add_argument("--M", type=int, default=256)
+    ap.add_argument("--L", type=int, default=24)
+    ap.add_argument("--M", type=int, default=512)
+    ap.add_argument("--init-bd", type=int, default=64)
+    ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
 
 def workload_name(a):
-    return (f"two-site H_eff.psi, synthetic ab-initio L={a.L} N={a.L} TwoU1 Sz=0 seed {a.seed}, "
-            f"M={a.M}, middle bond after one sweep")
+    return (f"two-site H_eff.psi, synthetic ab-initio L={a.L} N={a.L} TwoU1 Sz=0 seed {a.seed}, M={a.M} "
+            f"(init_bond_dimension {a.init_bd}), middle bond after {a.sweeps} sweeps")
 
 
-def frozen_problem(a):
+def frozen_problem(a, device: int, export: bool):
+    """Device sweeps, then the middle-bond site problem: (ctx, dmrg, plan, x, mpo_blob, snap, site, sweep_info)."""
     from qcmaquis_b200.fcidump import synthetic_integrals
     from qcmaquis_b200.mpo import MPO
-    from oracle.oracle import OracleDMRG
+    from qcmaquis_b200.heff import Context
+    from qcmaquis_b200.dmrg import DMRG
     h, V, e = synthetic_integrals(a.L, a.seed)
     m = MPO.qc(h, V)
-    blob = m.blob()
-    d = OracleDMRG(blob, a.L, a.L // 2, a.L // 2, a.M, init_bond_dimension=5)
-    d.sweep(0)
-    step = a.L // 2 - 1
-    snap = d.snapshot(1, step)
-    return m, blob, snap, step
+    ctx = Context(device)
+    t0 = time.perf_counter()
+    d = DMRG(ctx, m, a.L // 2, a.L // 2, a.M, a.init_bd)
+    t_init = time.perf_counter() - t0
+    sweeps = []
+    for s in range(a.sweeps):
+        st0 = d.stats()
+        t0 = time.perf_counter()
+        E, tr = d.sweep()
+        dt = time.perf_counter() - t0
+        st1 = d.stats()
+        sweeps.append({"sweep": s, "seconds": dt, "energy_min": float(E.min()),
+                       "max_bond_dimension": int(max(t["bond_dimension"] for t in tr)),
+                       "hpsi": int(st1["hpsi_count"] - st0["hpsi_count"]),
+                       "hpsi_gflop": (st1["hpsi_flops"] - st0["hpsi_flops"]) / 1e9,
+                       "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}})
+    site = a.L // 2 - 1
+    d.run(site)
+    plan, x = d.pending_plan()
+    snap = d.pending_export() if export else None
+    info = {"init_s": t_init, "sweeps": sweeps, "site": site}
+    return ctx, d, plan, x, m.blob(), snap, site, info
 
 
 class Clocks:
@@ -118,7 +143,7 @@ def dist_setup(a):
     return world, rank, local, pg
 
 
-def cpu_baseline(snap, blob, site, x, flops, budget_s=15.0):
+def cpu_baseline(snap, blob, site, x, flops, budget_s=20.0):
     from oracle.oracle import heff_apply, lib as olib
     olib()
     y, _, sec = heff_apply(snap, blob, site, x, repeat=1)
@@ -132,24 +157,27 @@ def cpu_baseline(snap, blob, site, x, flops, budget_s=15.0):
 def run_reference(a, world, rank, pg):
     if rank != 0:
         return
-    from qcmaquis_b200.heff import parse_site_problem, twin_vector
     from oracle.oracle import heff_apply, lib as olib
-    m, blob, snap, site = frozen_problem(a)
-    x = twin_vector(parse_site_problem(snap))
+    ctx, d, plan, x, blob, snap, site, sinfo = frozen_problem(a, 0, export=True)
+    flops = plan.info["flops"]
+    del plan, d
     for _ in range(a.warmup):
-        _, flops, _ = heff_apply(snap, blob, site, x, repeat=1)
+        heff_apply(snap, blob, site, x, repeat=1)
     t0 = time.perf_counter()
-    _, flops, sec = heff_apply(snap, blob, site, x, repeat=a.steps)
+    _, flops_o, sec = heff_apply(snap, blob, site, x, repeat=a.steps)
     wall = time.perf_counter() - t0
-    val = flops / sec / 1e9
+    val = flops_o / sec / 1e9
     cores = olib().orc_max_threads()
-    line = {"impl": "reference", "metric": "H_eff.psi GFLOP/s (FP64)", "value": val, "unit": "GFLOP/s",
+    line = {"impl": "reference", "metric": "H_eff.psi GFLOP/s (FP64 plain form)", "value": val, "unit": "GFLOP/s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "seed": a.seed},
+            "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "init_bond_dimension": a.init_bd,
+                       "seed": a.seed, "flops_per_step": flops_o},
             "cpu_baseline": {"value": val, "unit": "GFLOP/s", "cores": cores, "kind": "port",
                              "sample": f"{a.steps} H_eff.psi applies ({wall:.1f} s) with all host threads"},
-            "e2e": {"value": val, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": val, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "frozen problem produced by the device engine (untimed) and exported as a QSPB blob"}
+    assert abs(flops_o - flops) <= 1e-9 * flops, "oracle and device work counts differ"
     print(json.dumps(line), flush=True)
 
 
@@ -157,13 +185,9 @@ def run_b200(a, world, rank, local, pg):
     import torch
     from qcmaquis_b200 import heff
     torch.cuda.set_device(local)
-    m, blob, snap, site = frozen_problem(a)
-    ts = m.twosite()
-    p = heff.parse_site_problem(snap)
-    ctx = heff.Context(local)
-    plan = heff.plan_from_problem(ctx, p, ts, site)
+    want_cpu = rank == 0 and world == 1 and not a.no_cpu_baseline
+    ctx, d, plan, x_host, blob, snap, site, sinfo = frozen_problem(a, local, export=want_cpu)
     info = plan.info
-    x_host = heff.twin_vector(p)
     n = plan.n
     dev = torch.device("cuda", local)
     xd = torch.from_numpy(x_host).to(dev)
@@ -223,9 +247,11 @@ def run_b200(a, world, rank, local, pg):
         e2e_s = float(t.item())
     e2e_val = info["flops"] * a.steps * world / e2e_s / 1e9
     # correctness guard on the timed problem: device result vs the oracle
-    from oracle.oracle import heff_apply
-    y_ref, _, _ = heff_apply(snap, blob, site, x_host)
-    rel = float(np.abs(yh.numpy() - y_ref).max() / np.abs(y_ref).max())
+    rel = None
+    if snap is not None:
+        from oracle.oracle import heff_apply
+        y_ref, _, _ = heff_apply(snap, blob, site, x_host)
+        rel = float(np.abs(yh.numpy() - y_ref).max() / np.abs(y_ref).max())
     # roofline of the dominant kernel (phase): reference flop count of the phase / its device time
     ph = np.mean(np.array(phases), axis=0)
     names = ["k_tgemm", "k_sgemm", "k_lspart+k_lsreduce"]
@@ -240,21 +266,22 @@ def run_b200(a, world, rank, local, pg):
         roof["executed_dense_tflops"] = info["flops_sdense"] / (ph[1] * 1e-3) / 1e12
     roof["phase_ms"] = {k: float(v) for k, v in zip(names, ph)}
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    if want_cpu:
         cpu = cpu_baseline(snap, blob, site, x_host, info["flops"])
     if rank == 0:
         line = {"metric": "H_eff.psi GFLOP/s (FP64 plain form)", "value": value, "unit": "GFLOP/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "seed": a.seed, "vec_len": n,
-                           "flops_per_step": info["flops"], "l2": "flushed between steps (256 MiB write)",
-                           "parallelism": f"replicas x{world}"},
+                "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "init_bond_dimension": a.init_bd,
+                           "seed": a.seed, "vec_len": n, "flops_per_step": info["flops"],
+                           "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+                "sweep": sinfo,
                 "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
                 "gpu_launches": int(info["launches"]) * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
                 "fp64_peaks_tflops": {"dmma": dmma_peak, "dfma": dfma_peak},
                 "max_rel_err_vs_oracle": rel}
         print(json.dumps(line), flush=True)
-    del plan
+    del plan, d
     if pg is not None:
         pg.destroy_process_group()
 

@@ -243,9 +243,26 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
 int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* params, const qcm_mps_desc* sites,
                              const double* const* data, qcm_dmrg** out);
 int qcm_dmrg_length(const qcm_dmrg* d);
-/* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL). */
+/* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL); only
+ * between sweeps (see qcm_dmrg_run). */
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);
 int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* stats);
+/* Run the current sweep up to (not including) step stop_step (2L - 2 completes
+ * it); energies / trunc receive one entry per step run (may be NULL), *n_steps
+ * their count. */
+int qcm_dmrg_run(qcm_dmrg* d, int stop_step, double* energies, qcm_trunc_result* trunc, int* n_steps);
+/* Step index (0 .. 2L-3) the current sweep continues with. */
+int qcm_dmrg_next_step(const qcm_dmrg* d);
+/* H_eff plan of the pending step (its boundaries are the sweep's own: the plan
+ * is valid until the sweep continues) and, if twin != NULL, its start vector
+ * (vec_len doubles, cap = buffer length).  Replaces the snapshot of the site
+ * problem that ts_optimize hands to solve_site_problem (ts_optimize.hpp:185-240). */
+int qcm_dmrg_pending_plan(qcm_dmrg* d, double* twin, uint64_t cap, qcm_heff** out);
+/* Start vector of the pending step (*n = vec_len; twin may be NULL to query). */
+int qcm_dmrg_pending_twin(qcm_dmrg* d, double* twin, uint64_t cap, uint64_t* n);
+/* The pending step's frozen site problem as a "QSPB" v1 blob (twin + L + R, the
+ * interchange format read by the test oracle).  Call with buf == NULL for *len. */
+int qcm_dmrg_pending_export(qcm_dmrg* d, void* buf, size_t cap, size_t* len);
 /* Current bond dimensions (right basis size of sites 0 .. L-2). */
 int qcm_dmrg_bond_dimensions(const qcm_dmrg* d, uint64_t* dims);
 void qcm_dmrg_free(qcm_dmrg* d);

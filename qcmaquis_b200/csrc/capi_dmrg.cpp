@@ -78,6 +78,34 @@ int boundary_step(qcm_ctx* ctx, const qcm_boundary* B, const qcm_mpo* mpo, int s
     QCM_CATCH
 }
 
+// "QSPB" v1 site-problem blob writer (the frozen-problem interchange format)
+struct Blob {
+    std::vector<uint8_t> b;
+    template <class T> void put(T v) { const uint8_t* p = reinterpret_cast<const uint8_t*>(&v); b.insert(b.end(), p, p + sizeof(T)); }
+    void idx(const qcm::Index& i) {
+        put<uint32_t>(uint32_t(i.size()));
+        for (auto& e : i.d) { put<int32_t>(e.first.a); put<int32_t>(e.first.b); put<uint32_t>(uint32_t(e.second)); }
+    }
+    void bnd(const qcm::DevBoundary& B, cudaStream_t s) {
+        const qcm::BoundaryIndexH& x = B.idx;
+        std::vector<double> h(x.total);
+        if (x.total) QCM_CUDA(cudaMemcpyAsync(h.data(), B.data.get(), x.total * sizeof(double), cudaMemcpyDeviceToHost, s));
+        QCM_CUDA(cudaStreamSynchronize(s));
+        idx(x.bra); idx(x.ket);
+        put<uint32_t>(x.n_cohorts()); put<uint32_t>(x.aux);
+        for (uint32_t ci = 0; ci < x.n_cohorts(); ++ci) {
+            put<uint32_t>(x.cbra[ci]); put<uint32_t>(x.cket[ci]); put<uint8_t>(x.tr[ci]);
+            put<uint32_t>(x.lsz[ci]); put<uint32_t>(x.rsz[ci]); put<uint32_t>(x.nb[ci]);
+            for (uint32_t b = 0; b < x.aux; ++b) put<int64_t>(x.offsets[std::size_t(ci) * x.aux + b]);
+            for (uint32_t b = 0; b < x.aux; ++b) put<double>(x.cscale[std::size_t(ci) * x.aux + b]);
+            const uint64_t n = x.cohort_size(ci);
+            put<uint64_t>(n);
+            const uint8_t* p = reinterpret_cast<const uint8_t*>(h.data() + x.data_off[ci]);
+            b.insert(b.end(), p, p + n * sizeof(double));
+        }
+    }
+};
+
 void fill_sectors(const qcm::Index& x, qcm_sector* out) {
     for (std::size_t i = 0; i < x.size(); ++i)
         out[i] = qcm_sector{x[i].first.a, x[i].first.b, uint32_t(x[i].second)};
@@ -213,9 +241,94 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
 
 int qcm_dmrg_length(const qcm_dmrg* d) { return d ? d->e->L : -1; }
 
+int qcm_dmrg_run(qcm_dmrg* d, int stop_step, double* energies, qcm_trunc_result* trunc, int* n_steps) {
+    QCM_TRY
+    if (!d) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_run: NULL argument");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    std::vector<double> E;
+    std::vector<qcm::TruncResults> T;
+    d->e->run_until(stop_step, E, T);
+    if (energies) std::memcpy(energies, E.data(), E.size() * sizeof(double));
+    if (trunc)
+        for (std::size_t i = 0; i < T.size(); ++i)
+            trunc[i] = qcm_trunc_result{T[i].bond_dimension, T[i].truncated_weight, T[i].truncated_fraction, T[i].smallest_ev};
+    if (n_steps) *n_steps = int(E.size());
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_next_step(const qcm_dmrg* d) { return d ? d->e->next_step : -1; }
+
+int qcm_dmrg_pending_plan(qcm_dmrg* d, double* twin, uint64_t cap, qcm_heff** out) {
+    QCM_TRY
+    if (!d || !out) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_plan: NULL argument");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    std::vector<double> x;
+    auto h = std::make_unique<qcm_heff>();
+    h->ctx = d->ctx;
+    h->p = d->e->pending_plan(twin ? &x : nullptr, nullptr, nullptr, nullptr);
+    h->p->stream = d->ctx->stream;
+    qcm::upload_plan(*h->p);
+    if (twin) {
+        if (cap < x.size()) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_plan: twin buffer too small");
+        std::memcpy(twin, x.data(), x.size() * sizeof(double));
+    }
+    *out = h.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_pending_twin(qcm_dmrg* d, double* twin, uint64_t cap, uint64_t* n) {
+    QCM_TRY
+    if (!d || !n) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_twin: NULL argument");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    std::vector<double> x;
+    d->e->pending_twin(x);
+    *n = x.size();
+    if (twin) {
+        if (cap < x.size()) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_twin: buffer too small");
+        std::memcpy(twin, x.data(), x.size() * sizeof(double));
+    }
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_pending_export(qcm_dmrg* d, void* buf, size_t cap, size_t* len) {
+    QCM_TRY
+    if (!d || !len) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_export: NULL argument");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::DevDMRG& e = *d->e;
+    std::vector<double> x;
+    qcm::Index phys, left, right;
+    auto plan = e.pending_plan(&x, &phys, &left, &right);
+    int lr, site1, site2;
+    e.step_sites(e.next_step, lr, site1, site2);
+    Blob w;
+    w.put<uint32_t>(0x42505351u);  // "QSPB"
+    w.put<uint32_t>(1);
+    w.idx(phys); w.idx(left); w.idx(right);
+    w.put<uint32_t>(uint32_t(left.size()));
+    for (std::size_t lb = 0; lb < left.size(); ++lb) {
+        w.put<int32_t>(left[lb].first.a); w.put<int32_t>(left[lb].first.b);
+        w.put<uint32_t>(uint32_t(left[lb].second)); w.put<uint32_t>(plan->x_cols[lb]);
+        const uint8_t* p = reinterpret_cast<const uint8_t*>(x.data() + plan->x_off[lb]);
+        w.b.insert(w.b.end(), p, p + uint64_t(left[lb].second) * plan->x_cols[lb] * sizeof(double));
+    }
+    w.bnd(*e.left_[site1], e.c.s);
+    w.bnd(*e.right_[site2 + 1], e.c.s);
+    *len = w.b.size();
+    if (buf) {
+        if (cap < w.b.size()) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_export: buffer too small");
+        std::memcpy(buf, w.b.data(), w.b.size());
+    }
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc) {
     QCM_TRY
     if (!d || !energies) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_sweep: NULL argument");
+    if (d->e->next_step != 0) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_sweep: a sweep is in progress (finish it with qcm_dmrg_run)");
     QCM_CUDA(cudaSetDevice(d->ctx->device));
     std::vector<double> E;
     std::vector<qcm::TruncResults> T;

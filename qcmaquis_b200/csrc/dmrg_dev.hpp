@@ -170,10 +170,20 @@ struct DevDMRG {
     // given MPS (right-normalised on sites 1 .. L-1, as after canonize(0))
     DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, std::vector<DMPS> sites,
             const DMRGParams& prm, cudaStream_t s);
+    int next_step = 0;  // step index (0 .. 2L-3) the sweep continues with
     void sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc);
+    // run the current sweep up to (not including) step `stop`; appends energies / truncations
+    void run_until(int stop, std::vector<double>& energies, std::vector<TruncResults>& trunc);
+    // H_eff plan of the pending step (boundaries and MPS of this object; valid until the sweep continues),
+    // the twin vector on the host, and the twin's indices
+    std::unique_ptr<HeffPlan> pending_plan(std::vector<double>* twin, Index* phys, Index* left, Index* right);
+    // start vector of the pending step (right-paired twin, H_eff vector layout)
+    void pending_twin(std::vector<double>& twin);
+    void step_sites(int step, int& lr, int& site1, int& site2) const;
 
   private:
     void init_boundaries();
+    void step(int step, double& energy, TruncResults& tr);
 };
 
 }  // namespace qcm

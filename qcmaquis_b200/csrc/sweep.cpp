@@ -238,62 +238,113 @@ void DevDMRG::init_boundaries() {
     QCM_CUDA(cudaStreamSynchronize(c.s));
 }
 
+void DevDMRG::step_sites(int _site, int& lr, int& site1, int& site2) const {
+    const int site = (_site < L - 1) ? _site : 2 * L - 2 - _site;
+    if (_site < L - 1) { lr = 1; site1 = site; site2 = site + 1; }
+    else { lr = -1; site1 = site - 1; site2 = site; }
+}
+
+void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
+    int lr, site1, site2;
+    step_sites(_site, lr, site1, site2);
+    const double t0 = now_s();
+    make_left_paired(c, mps[site1]);
+    make_right_paired(c, mps[site2]);
+    DTwoSite tst;
+    tst.build(c, mps[site1], mps[site2]);
+    auto plan = build_heff_plan(*left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, false);
+    plan->stream = c.s;
+    upload_plan(*plan);
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    const double t1 = now_s();
+    st.plan_s += t1 - t0;
+    int iters = 0;
+    const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters);
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    const double t2 = now_s();
+    st.jd_s += t2 - t1;
+    st.hpsi_count += uint64_t(iters);
+    st.hpsi_flops += double(iters) * plan->flops;
+    plan.reset();
+    tst.twin_to_both(c);
+    energy = E + p.ecore;
+    if (lr == 1) {
+        tr = tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+        DBlocks t = normalize_left(c, mps[site2]);
+        if (site2 < L - 1) multiply_from_left(c, mps[site2 + 1], t);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        const double t3 = now_s();
+        st.trunc_s += t3 - t2;
+        DMPS ket = right_paired_copy(c, mps[site1]);
+        left_[site2] = boundary_step_left(c, *left_[site1], ket, mps[site1], mpo[site1], true);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        st.boundary_s += now_s() - t3;
+    } else {
+        tr = tst.split(c, false, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+        DBlocks t = normalize_right(c, mps[site1]);
+        if (site1 > 0) multiply_from_right(c, mps[site1 - 1], t);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        const double t3 = now_s();
+        st.trunc_s += t3 - t2;
+        right_[site2] = boundary_step_right(c, *right_[site2 + 1], mps[site2], mpo[site2], true);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        st.boundary_s += now_s() - t3;
+    }
+}
+
+void DevDMRG::run_until(int stop, std::vector<double>& energies, std::vector<TruncResults>& trunc) {
+    if (stop < next_step || stop > 2 * L - 2) throw std::runtime_error("DMRG: stop step outside the current sweep");
+    const double t_start = now_s();
+    for (; next_step < stop; ++next_step) {
+        double E = 0;
+        TruncResults tr;
+        step(next_step, E, tr);
+        energies.push_back(E);
+        trunc.push_back(tr);
+    }
+    if (next_step == 2 * L - 2) next_step = 0;
+    st.total_s += now_s() - t_start;
+}
+
 void DevDMRG::sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc) {
     energies.clear();
     trunc.clear();
-    const double t_start = now_s();
-    for (int _site = 0; _site < 2 * L - 2; ++_site) {
-        int lr, site1, site2;
-        const int site = (_site < L - 1) ? _site : 2 * L - 2 - _site;
-        if (_site < L - 1) { lr = 1; site1 = site; site2 = site + 1; }
-        else { lr = -1; site1 = site - 1; site2 = site; }
-        const double t0 = now_s();
-        make_left_paired(c, mps[site1]);
-        make_right_paired(c, mps[site2]);
-        DTwoSite tst;
-        tst.build(c, mps[site1], mps[site2]);
-        auto plan = build_heff_plan(*left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, false);
-        plan->stream = c.s;
-        upload_plan(*plan);
-        QCM_CUDA(cudaStreamSynchronize(c.s));
-        const double t1 = now_s();
-        st.plan_s += t1 - t0;
-        int iters = 0;
-        const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters);
-        QCM_CUDA(cudaStreamSynchronize(c.s));
-        const double t2 = now_s();
-        st.jd_s += t2 - t1;
-        st.hpsi_count += uint64_t(iters);
-        st.hpsi_flops += double(iters) * plan->flops;
-        plan.reset();
-        tst.twin_to_both(c);
-        energies.push_back(E + p.ecore);
-        TruncResults tr;
-        if (lr == 1) {
-            tr = tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
-            DBlocks t = normalize_left(c, mps[site2]);
-            if (site2 < L - 1) multiply_from_left(c, mps[site2 + 1], t);
-            QCM_CUDA(cudaStreamSynchronize(c.s));
-            const double t3 = now_s();
-            st.trunc_s += t3 - t2;
-            DMPS ket = right_paired_copy(c, mps[site1]);
-            left_[site2] = boundary_step_left(c, *left_[site1], ket, mps[site1], mpo[site1], true);
-            QCM_CUDA(cudaStreamSynchronize(c.s));
-            st.boundary_s += now_s() - t3;
-        } else {
-            tr = tst.split(c, false, p.Mmax, p.cutoff, mps[site1], mps[site2]);
-            DBlocks t = normalize_right(c, mps[site1]);
-            if (site1 > 0) multiply_from_right(c, mps[site1 - 1], t);
-            QCM_CUDA(cudaStreamSynchronize(c.s));
-            const double t3 = now_s();
-            st.trunc_s += t3 - t2;
-            right_[site2] = boundary_step_right(c, *right_[site2 + 1], mps[site2], mpo[site2], true);
-            QCM_CUDA(cudaStreamSynchronize(c.s));
-            st.boundary_s += now_s() - t3;
-        }
-        trunc.push_back(tr);
+    run_until(2 * L - 2, energies, trunc);
+}
+
+void DevDMRG::pending_twin(std::vector<double>& twin) {
+    int lr, site1, site2;
+    step_sites(next_step, lr, site1, site2);
+    make_left_paired(c, mps[site1]);
+    make_right_paired(c, mps[site2]);
+    DTwoSite tst;
+    tst.build(c, mps[site1], mps[site2]);
+    twin.resize(tst.twin.b.total);
+    if (!twin.empty())
+        QCM_CUDA(cudaMemcpyAsync(twin.data(), tst.twin.b.d.get(), twin.size() * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+}
+
+std::unique_ptr<HeffPlan> DevDMRG::pending_plan(std::vector<double>* twin, Index* phys_out, Index* left_out,
+                                                Index* right_out) {
+    int lr, site1, site2;
+    step_sites(next_step, lr, site1, site2);
+    make_left_paired(c, mps[site1]);
+    make_right_paired(c, mps[site2]);
+    DTwoSite tst;
+    tst.build(c, mps[site1], mps[site2]);
+    auto plan = build_heff_plan(*left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, false);
+    plan->stream = c.s;
+    if (twin) {
+        twin->resize(plan->x_len);
+        if (plan->x_len != tst.twin.b.total) throw std::runtime_error("DMRG: twin layout differs from the plan");
+        QCM_CUDA(cudaMemcpyAsync(twin->data(), tst.twin.b.d.get(), plan->x_len * sizeof(double), cudaMemcpyDeviceToHost, c.s));
     }
-    st.total_s += now_s() - t_start;
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    if (phys_out) *phys_out = tst.phys;
+    if (left_out) *left_out = tst.twin.left;
+    if (right_out) *right_out = tst.right;
+    return plan;
 }
 
 }  // namespace qcm

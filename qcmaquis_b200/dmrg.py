@@ -13,7 +13,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import lib, check, P, c_int, c_void_p, c_uint64, c_double
-from .heff import Boundary, MPSDesc, _sectors
+from .heff import Boundary, HeffPlan, MPSDesc, _sectors
 
 
 class DMRGParams(ctypes.Structure):
@@ -40,6 +40,11 @@ _lib._sig("qcm_dmrg_create", c_int, c_void_p, c_void_p, c_int, c_int, P(DMRGPara
 _lib._sig("qcm_dmrg_create_from_mps", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)),
           P(c_void_p))
 _lib._sig("qcm_dmrg_length", c_int, c_void_p)
+_lib._sig("qcm_dmrg_run", c_int, c_void_p, c_int, P(c_double), P(TruncResult), P(c_int))
+_lib._sig("qcm_dmrg_next_step", c_int, c_void_p)
+_lib._sig("qcm_dmrg_pending_plan", c_int, c_void_p, P(c_double), c_uint64, P(c_void_p))
+_lib._sig("qcm_dmrg_pending_twin", c_int, c_void_p, P(c_double), c_uint64, P(c_uint64))
+_lib._sig("qcm_dmrg_pending_export", c_int, c_void_p, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
 _lib._sig("qcm_dmrg_sweep", c_int, c_void_p, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
 _lib._sig("qcm_dmrg_bond_dimensions", c_int, c_void_p, P(c_uint64))
@@ -119,6 +124,39 @@ class DMRG:
         tr = (TruncResult * n)()
         check(lib.qcm_dmrg_sweep(self.h, _lib.dptr(E), tr), "qcm_dmrg_sweep")
         return E, [{f: getattr(t, f) for f, _ in TruncResult._fields_} for t in tr]
+
+    def run(self, stop_step: int):
+        """Run the current sweep up to (not including) step stop_step: (energies, truncation dicts)."""
+        n = 2 * self.L - 2
+        E = np.zeros(n)
+        tr = (TruncResult * n)()
+        k = c_int()
+        check(lib.qcm_dmrg_run(self.h, stop_step, _lib.dptr(E), tr, ctypes.byref(k)), "qcm_dmrg_run")
+        return E[:k.value], [{f: getattr(t, f) for f, _ in TruncResult._fields_} for t in tr[:k.value]]
+
+    @property
+    def next_step(self) -> int:
+        return lib.qcm_dmrg_next_step(self.h)
+
+    def pending_plan(self):
+        """(H_eff plan, start vector) of the pending step; the plan is valid until the sweep continues."""
+        h = c_void_p()
+        check(lib.qcm_dmrg_pending_plan(self.h, None, 0, ctypes.byref(h)), "qcm_dmrg_pending_plan")
+        plan = HeffPlan.from_handle(self.ctx, h, owner=self)
+        n = c_uint64()
+        check(lib.qcm_dmrg_pending_twin(self.h, None, 0, ctypes.byref(n)), "qcm_dmrg_pending_twin")
+        x = np.zeros(n.value)
+        check(lib.qcm_dmrg_pending_twin(self.h, _lib.dptr(x), x.size, ctypes.byref(n)), "qcm_dmrg_pending_twin")
+        assert x.size == plan.n
+        return plan, x
+
+    def pending_export(self) -> bytes:
+        """The pending step's frozen site problem ("QSPB" v1)."""
+        n = ctypes.c_size_t()
+        check(lib.qcm_dmrg_pending_export(self.h, None, 0, ctypes.byref(n)), "qcm_dmrg_pending_export")
+        buf = ctypes.create_string_buffer(n.value)
+        check(lib.qcm_dmrg_pending_export(self.h, buf, n.value, ctypes.byref(n)), "qcm_dmrg_pending_export")
+        return buf.raw
 
     def stats(self) -> dict:
         s = DMRGStats()

@@ -306,6 +306,18 @@ class HeffPlan:
         self.info = {f: getattr(info, f) for f, _ in HeffInfo._fields_}
         self.n = int(info.vec_len)
 
+    @classmethod
+    def from_handle(cls, ctx, h, owner=None):
+        """Wrap a plan handle made by the library (owner keeps its boundaries alive)."""
+        self = cls.__new__(cls)
+        self.ctx, self.L, self.R, self.mpo, self.owner = ctx, None, None, None, owner
+        self.h = h
+        info = HeffInfo()
+        check(lib.qcm_heff_get_info(h, ctypes.byref(info)), "qcm_heff_get_info")
+        self.info = {f: getattr(info, f) for f, _ in HeffInfo._fields_}
+        self.n = int(info.vec_len)
+        return self
+
     def apply(self, x: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)
         assert x.size == self.n

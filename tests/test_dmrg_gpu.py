@@ -129,3 +129,26 @@ def test_config1_sweeps_match_golden(gpu_ctx):
     d = np.abs(np.array(mins) - np.array(ref))
     assert d[0] < 1e-4 and d[1] < 1e-7 and d[2:].max() < E_TOL, (mins, ref)
     assert abs(mins[-1] - golden["config1_fci"]) < 1e-8
+
+
+def test_pending_problem_export_matches_oracle(gpu_ctx):
+    """Partial sweep, then the pending step's plan and its QSPB export: device H.psi vs the oracle's
+    on the exported problem, and the exported twin equals the plan's start vector."""
+    from oracle.oracle import heff_apply
+    from qcmaquis_b200.dmrg import DMRG
+    from qcmaquis_b200.heff import parse_site_problem, twin_vector
+    h, V, e, m, ts, blob = qc_system(8)
+    dev = DMRG(gpu_ctx, m, 4, 4, 32)
+    dev.sweep()
+    E, tr = dev.run(3)
+    assert len(E) == 3 and dev.next_step == 3
+    plan, x = dev.pending_plan()
+    snap = dev.pending_export()
+    prob = parse_site_problem(snap)
+    assert np.array_equal(twin_vector(prob), x)
+    y = plan.apply(x)
+    y_ref, _, _ = heff_apply(snap, blob, 3, x)
+    assert np.abs(y - y_ref).max() <= 1e-12 * np.abs(y_ref).max()
+    del plan
+    E2, _ = dev.run(2 * 8 - 2)
+    assert len(E2) == 2 * 8 - 2 - 3 and dev.next_step == 0
