@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 
 #include "dmrg_dev.hpp"
@@ -247,12 +249,23 @@ void DevDMRG::step_sites(int _site, int& lr, int& site1, int& site2) const {
 void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     int lr, site1, site2;
     step_sites(_site, lr, site1, site2);
+    // QCM_SWEEP_TIMING=1 prints the wall time of each phase of every step
+    static const bool timing = std::getenv("QCM_SWEEP_TIMING") != nullptr;
+    double tt[8];
+    auto mark = [&](int i) {
+        if (!timing) return;
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        tt[i] = now_s();
+    };
     const double t0 = now_s();
+    tt[0] = t0;
     make_left_paired(c, mps[site1]);
     make_right_paired(c, mps[site2]);
     DTwoSite tst;
     tst.build(c, mps[site1], mps[site2]);
+    mark(1);
     auto plan = build_heff_plan(*left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, false);
+    mark(2);
     plan->stream = c.s;
     upload_plan(*plan);
     QCM_CUDA(cudaStreamSynchronize(c.s));
@@ -267,13 +280,17 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     st.hpsi_flops += double(iters) * plan->flops;
     plan.reset();
     tst.twin_to_both(c);
+    mark(3);
     energy = E + p.ecore;
+    double t3_last = 0;
     if (lr == 1) {
         tr = tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+        mark(4);
         DBlocks t = normalize_left(c, mps[site2]);
         if (site2 < L - 1) multiply_from_left(c, mps[site2 + 1], t);
         QCM_CUDA(cudaStreamSynchronize(c.s));
         const double t3 = now_s();
+        t3_last = t3;
         st.trunc_s += t3 - t2;
         DMPS ket = right_paired_copy(c, mps[site1]);
         left_[site2] = boundary_step_left(c, *left_[site1], ket, mps[site1], mpo[site1], true);
@@ -281,14 +298,23 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         st.boundary_s += now_s() - t3;
     } else {
         tr = tst.split(c, false, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+        mark(4);
         DBlocks t = normalize_right(c, mps[site1]);
         if (site1 > 0) multiply_from_right(c, mps[site1 - 1], t);
         QCM_CUDA(cudaStreamSynchronize(c.s));
         const double t3 = now_s();
+        t3_last = t3;
         st.trunc_s += t3 - t2;
         right_[site2] = boundary_step_right(c, *right_[site2 + 1], mps[site2], mpo[site2], true);
         QCM_CUDA(cudaStreamSynchronize(c.s));
         st.boundary_s += now_s() - t3;
+    }
+    if (timing) {
+        const double tend = now_s();
+        std::fprintf(stderr,
+                     "[step %d] twosite %.4f plan %.4f upload %.4f jd %.4f (%d) t2b %.4f svd %.4f qr %.4f bstep %.4f total %.4f\n",
+                     _site, tt[1] - tt[0], tt[2] - tt[1], t1 - tt[2], t2 - t1, iters, tt[3] - t2, tt[4] - tt[3],
+                     t3_last - tt[4], tend - t3_last, tend - tt[0]);
     }
 }
 

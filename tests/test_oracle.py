@@ -93,3 +93,23 @@ def test_boundary_step_export_parses():
         for (ch, blk), sec in zip(c["blocks"], c["left"]):
             assert ch == tuple(sec[:2]) and blk.shape[0] == sec[2]
         assert np.isfinite(c["B_out"]["data"]).all() and np.abs(c["B_out"]["data"]).max() > 0
+
+
+@pytest.mark.parametrize("sw,step,side", [(0, 2, 0), (1, 3, 1)])
+def test_oracle_boundary_step_matches_dense_contraction(sw, step, side):
+    """The oracle's overlap_mpo_left/right_step equals a dense einsum of site tensor, boundary and MPO."""
+    from qcmaquis_b200.heff import parse_boundary_step
+    from qcmaquis_b200.mpo import parse_blob
+    from helpers import dense_boundary, dense_boundary_step
+    L, M = 6, 16
+    h, V, e, m, ts, blob = qc_system(L)
+    d = OracleDMRG(blob, L, 3, 3, M)
+    for s in range(sw):
+        d.sweep(s)
+    d.snapshot(sw, step)
+    site1 = site_of_step(L, step)
+    site = site1 if side == 0 else site1 + 1
+    case = parse_boundary_step(d.boundary_export(side, site))
+    ref = dense_boundary_step(case, parse_blob(blob)[site])
+    got = dense_boundary(case["B_out"])
+    assert np.abs(ref - got).max() <= 1e-13 * np.abs(ref).max()
