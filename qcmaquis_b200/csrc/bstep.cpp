@@ -4,10 +4,10 @@
 // Right step (rshtm_t_tasks / rshtm_tasks, right_tasks.hpp:39-167; prop_r, tasks.cpp:243-284):
 //   T = ket_slab * R_old[ci_eff]          -> grouped T-GEMM (same kernel as H_eff)
 //   S = sum alpha * T slices               -> unit S-GEMM (same kernel as H_eff)
-//   R_new[b] = S_b * bra^T                 -> batched GEMM, one job per MPO row block
+//   R_new[b] = S_b * bra^T                 -> batched GEMM, one row-blocked job per cohort
 // Left step (lshtm_t_tasks / lshtm_tasks, left_tasks.hpp:38-172; create_T_left,
 // create_s, prop_l, tasks.cpp:198-241, 425-454, 545-601):
-//   T_b = L_old[ci_eff]_b(^T) * ket_slab   -> batched GEMM, one job per (T job, MPO block)
+//   T_b = L_old[ci_eff]_b(^T) * ket_slab   -> batched GEMM, one row-blocked job per T job
 //   S (stripe x nS*rs_ket) = sum alpha * T slices  -> unit S-GEMM with the left layout
 //   L_new = bra^T * S                      -> batched GEMM, one job per cohort
 // Cohort offsets follow Cohort::finalize (tasks.cpp:506-526): MPO indices with
@@ -34,11 +34,12 @@ constexpr uint32_t NONE = 0xffffffffu;
 double step_now() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
-void step_report(const char* side, double t0, double t1, cudaStream_t s) {
+void step_report(const char* side, double t0, double tp, double t1, cudaStream_t s) {
     static const bool on = std::getenv("QCM_STEP_TIMING") != nullptr;
     if (!on) return;
     QCM_CUDA(cudaStreamSynchronize(s));
-    std::fprintf(stderr, "[bstep %s] schedule %.4f s, device %.4f s\n", side, t1 - t0, step_now() - t1);
+    std::fprintf(stderr, "[bstep %s] schedule %.4f s (parts %.4f, merge %.4f), device %.4f s\n", side, t1 - t0, tp - t0,
+                 t1 - tp, step_now() - t1);
 }
 
 void add_tiles(std::vector<TileD>* tiles, uint32_t item, uint32_t M, uint32_t N) {
@@ -359,6 +360,7 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
         }
     }
 
+    const double tbp = step_now();
     // merge in ket-sector order; new index (BoundaryIndex(ket_left_i, bra_left_i))
     std::vector<TJobD> tjobs;
     std::vector<TileD> ttiles[N_SHAPES];
@@ -390,18 +392,17 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
     }
     if (symmetric) complement_transpose(nidx, W.herm_left, W.phase_left, false);
     auto Rn = finish_boundary(nidx, c.s);
-    // prop_r: new_R[b] (ls_ket x ls_bra) = S_b * bra^T
+    // prop_r: new_R[b] (ls_ket x ls_bra) = S_b * bra^T for all b of a cohort in one job
+    // (rows b-major in S; C row blocks = the cohort's MPO-index blocks)
     std::vector<GemmJob> prop;
     for (const Pend& pd : pend) {
         const uint32_t ls = uint32_t(left[pd.lb_ket].second), lsb = uint32_t(left[pd.lb_bra].second);
-        for (uint32_t b = 0; b < pd.nS; ++b) {
-            GemmJob g{};
-            g.a_off = pd.s_off + uint64_t(b) * ls; g.lda = pd.nS * ls;
-            g.b_off = koff[pd.lb_bra]; g.ldb = lsb; g.tb = 1;
-            g.c_off = Rn->idx.data_off[pd.ci_new] + uint64_t(b) * ls * lsb; g.ldc = ls;
-            g.M = ls; g.N = lsb; g.K = kcols[pd.lb_bra]; g.alpha = 1.0; g.beta = 0.0;
-            prop.push_back(g);
-        }
+        GemmJob g{};
+        g.a_off = pd.s_off; g.lda = pd.nS * ls;
+        g.b_off = koff[pd.lb_bra]; g.ldb = lsb; g.tb = 1;
+        g.c_off = Rn->idx.data_off[pd.ci_new]; g.ldc = ls; g.crb = ls; g.c_bs = uint64_t(ls) * lsb;
+        g.M = pd.nS * ls; g.N = lsb; g.K = kcols[pd.lb_bra]; g.alpha = 1.0; g.beta = 0.0;
+        prop.push_back(g);
     }
     const double tb1 = step_now();
     // execute
@@ -418,7 +419,7 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
               sb.d_went.get(), c.T.get(), c.S.get(), c.s);
     // A = S scratch, B = ket data, C = new boundary: three different base pointers
     batched_gemm(prop, c.S.get(), s_len, ket.b.d.get(), ket.b.total, Rn->data.get(), Rn->idx.total, c.gjobs, c.gtiles, c.s);
-    step_report("right", tb0, tb1, c.s);
+    step_report("right", tb0, tbp, tb1, c.s);
     return Rn;
 }
 
@@ -487,15 +488,15 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
                 tj[std::size_t(st) * nl + lb_bra] = uint32_t(tj_off.size());
                 tj_off.push_back(c_off);
                 P.t_len += (uint64_t(ls_bra) * rs_ket * nb + 31) / 32 * 32;
-                for (uint32_t b = 0; b < nb; ++b) {
-                    GemmJob g{};
-                    g.a_off = L.data_off[ce] + uint64_t(b) * ls_bra * ls_ket;
-                    g.ta = (ci != ce); g.lda = g.ta ? ls_ket : ls_bra;
-                    g.b_off = koff[li.lb] + uint64_t(mo) * ls_ket; g.ldb = ls_ket;
-                    g.c_off = c_off + uint64_t(b) * ls_bra * rs_ket; g.ldc = ls_bra;
-                    g.M = ls_bra; g.N = rs_ket; g.K = ls_ket; g.alpha = 1.0; g.beta = 0.0;
-                    P.tgemm.push_back(g);
-                }
+                if (nb == 0) continue;
+                // all nb blocks of the cohort in one job: A and C row blocks = MPO-index blocks
+                GemmJob g{};
+                g.a_off = L.data_off[ce]; g.arb = ls_bra; g.a_bs = uint64_t(ls_bra) * ls_ket;
+                g.ta = (ci != ce); g.lda = g.ta ? ls_ket : ls_bra;
+                g.b_off = koff[li.lb] + uint64_t(mo) * ls_ket; g.ldb = ls_ket;
+                g.c_off = c_off; g.crb = ls_bra; g.c_bs = uint64_t(ls_bra) * rs_ket; g.ldc = ls_bra;
+                g.M = nb * ls_bra; g.N = rs_ket; g.K = ls_ket; g.alpha = 1.0; g.beta = 0.0;
+                P.tgemm.push_back(g);
             }
         }
         // cohorts (lshtm_tasks)
@@ -552,6 +553,7 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
         }
     }
 
+    const double tbp = step_now();
     // merge in ket-sector order; new index (BoundaryIndex(bra_right_i, ket_right_i))
     std::vector<GemmJob> tj_gemm;
     SBuild sb;
@@ -599,7 +601,7 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_sptr.get(),
               sb.d_went.get(), c.T.get(), c.S.get(), c.s);
     batched_gemm(prop, bra.b.d.get(), bra.b.total, c.S.get(), s_len, Ln->data.get(), Ln->idx.total, c.gjobs, c.gtiles, c.s);
-    step_report("left", tb0, tb1, c.s);
+    step_report("left", tb0, tbp, tb1, c.s);
     return Ln;
 }
 

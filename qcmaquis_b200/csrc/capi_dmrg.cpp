@@ -57,6 +57,7 @@ int boundary_step(qcm_ctx* ctx, const qcm_boundary* B, const qcm_mpo* mpo, int s
     if ((left ? W.rows : W.cols) != B->b.idx.aux)
         return qcm::fail(QCM_ERR_ARG, "qcm_boundary_step: MPO bond dimension does not match the boundary");
     QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::AllocStream scope(ctx->stream);
     qcm::Ctx c;
     c.s = ctx->stream;
     qcm::DMPS ket = upload_mps(c, mps, data_rp);
@@ -121,6 +122,7 @@ int qcm_jd_solve(qcm_heff* h, const double* x0, double tol, int maxiter, double*
     if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: host-only plan");
     if (maxiter < 1 || maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: maxiter must be in 1..64");
     qcm::HeffPlan& p = *h->p;
+    qcm::AllocStream scope(p.stream);
     qcm::Ctx c;
     c.s = p.stream;
     qcm::DBuf<double> x(p.x_len ? p.x_len : 1);
@@ -175,6 +177,7 @@ int qcm_boundary_download(const qcm_boundary* b, qcm_sector* bra, qcm_sector* ke
     if (data) {
         if (!b->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_download: boundary is not resident");
         QCM_CUDA(cudaSetDevice(b->ctx->device));
+        qcm::AllocStream scope(b->ctx->stream);
         if (x.total)
             QCM_CUDA(cudaMemcpyAsync(data, b->b.data.get(), x.total * sizeof(double), cudaMemcpyDeviceToHost, b->ctx->stream));
         QCM_CUDA(cudaStreamSynchronize(b->ctx->stream));
@@ -192,6 +195,7 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     if (prm->max_bond_dimension < 1 || prm->init_bond_dimension < 1)
         return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: bond dimensions must be positive");
     QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::AllocStream scope(ctx->stream);
     qcm::DMRGParams p;
     p.Mmax = prm->max_bond_dimension;
     p.init_bond_dimension = prm->init_bond_dimension;
@@ -216,6 +220,7 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     if (m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: expected a single-site MPO");
     if (prm->jcd_maxiter < 1 || prm->jcd_maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: jcd_maxiter must be in 1..64");
     QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::AllocStream scope(ctx->stream);
     qcm::DMRGParams p;
     p.Mmax = prm->max_bond_dimension;
     p.init_bond_dimension = prm->init_bond_dimension;
@@ -245,6 +250,7 @@ int qcm_dmrg_run(qcm_dmrg* d, int stop_step, double* energies, qcm_trunc_result*
     QCM_TRY
     if (!d) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_run: NULL argument");
     QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
     std::vector<double> E;
     std::vector<qcm::TruncResults> T;
     d->e->run_until(stop_step, E, T);
@@ -263,6 +269,7 @@ int qcm_dmrg_pending_plan(qcm_dmrg* d, double* twin, uint64_t cap, qcm_heff** ou
     QCM_TRY
     if (!d || !out) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_plan: NULL argument");
     QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
     std::vector<double> x;
     auto h = std::make_unique<qcm_heff>();
     h->ctx = d->ctx;
@@ -282,6 +289,7 @@ int qcm_dmrg_pending_twin(qcm_dmrg* d, double* twin, uint64_t cap, uint64_t* n) 
     QCM_TRY
     if (!d || !n) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_twin: NULL argument");
     QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
     std::vector<double> x;
     d->e->pending_twin(x);
     *n = x.size();
@@ -297,6 +305,7 @@ int qcm_dmrg_pending_export(qcm_dmrg* d, void* buf, size_t cap, size_t* len) {
     QCM_TRY
     if (!d || !len) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_export: NULL argument");
     QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
     qcm::DevDMRG& e = *d->e;
     std::vector<double> x;
     qcm::Index phys, left, right;
@@ -330,6 +339,7 @@ int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc) {
     if (!d || !energies) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_sweep: NULL argument");
     if (d->e->next_step != 0) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_sweep: a sweep is in progress (finish it with qcm_dmrg_run)");
     QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
     std::vector<double> E;
     std::vector<qcm::TruncResults> T;
     d->e->sweep(E, T);

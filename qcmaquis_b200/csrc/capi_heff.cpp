@@ -36,6 +36,7 @@ int qcm_ctx_create(int device, qcm_ctx** out) {
     auto* c = new qcm_ctx;
     c->device = device;
     QCM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    qcm::register_stream(c->stream);
     *out = c;
     return QCM_OK;
     QCM_CATCH
@@ -43,7 +44,11 @@ int qcm_ctx_create(int device, qcm_ctx** out) {
 
 void qcm_ctx_destroy(qcm_ctx* c) {
     if (!c) return;
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+        qcm::retire_stream(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
     delete c;
 }
 
@@ -61,6 +66,7 @@ int boundary_make(qcm_ctx* ctx, const qcm_boundary_desc* d, qcm_boundary** out) 
     QCM_TRY
     if (!d || !out) return qcm::fail(QCM_ERR_ARG, "qcm_boundary_upload: NULL argument");
     if (ctx) QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::AllocStream scope(ctx ? ctx->stream : nullptr);
     auto b = std::make_unique<qcm_boundary>();
     b->ctx = ctx;
     qcm::BoundaryIndexH& x = b->b.idx;
@@ -130,6 +136,7 @@ int qcm_heff_plan_create(qcm_ctx* ctx, const qcm_boundary* L, const qcm_boundary
     if (!m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_heff_plan_create: expected a two-site MPO");
     if (site < 0 || std::size_t(site) >= m.t.size()) return qcm::fail(QCM_ERR_ARG, "qcm_heff_plan_create: site out of range");
     if (!host_only) QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::AllocStream scope(host_only ? nullptr : ctx->stream);
     auto h = std::make_unique<qcm_heff>();
     h->ctx = ctx;
     h->p = qcm::build_heff_plan(L->b, R->b, m.t[site], to_index(twin->n_phys, twin->phys), to_index(twin->n_left, twin->left),
@@ -184,6 +191,7 @@ int qcm_heff_apply(qcm_heff* h, const double* x, double* y) {
     if (!h || !x || !y) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply: NULL argument");
     if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply: host-only plan");
     qcm::HeffPlan& p = *h->p;
+    qcm::AllocStream scope(p.stream);
     if (p.d_x.size() < p.x_len) { p.d_x.alloc(p.x_len); p.d_y.alloc(p.x_len); }
     QCM_CUDA(cudaMemcpyAsync(p.d_x.get(), x, p.x_len * sizeof(double), cudaMemcpyHostToDevice, p.stream));
     qcm::heff_apply_device(p, p.d_x.get(), p.d_y.get());

@@ -32,7 +32,9 @@ __global__ void __launch_bounds__(NTHR) k_bgemm(const GemmJob* __restrict__ jobs
             if (!J.ta) { m = e % S::BM; k = e / S::BM; } else { k = e % BK; m = e / BK; }
             uint32_t gm = tile.m0 + m, gk = k0 + k;
             bool ok = gm < J.M && gk < J.K;
-            const double* src = J.ta ? A + J.a_off + gk + uint64_t(gm) * J.lda : A + J.a_off + gm + uint64_t(gk) * J.lda;
+            uint64_t base = J.a_off;
+            if (J.arb) { const uint32_t blk = gm / J.arb; base += uint64_t(blk) * J.a_bs; gm -= blk * J.arb; }
+            const double* src = J.ta ? A + base + gk + uint64_t(gm) * J.lda : A + base + gm + uint64_t(gk) * J.lda;
             cp8(&s.A[k][m], ok ? src : A, ok);
         }
 #pragma unroll
@@ -60,7 +62,9 @@ __global__ void __launch_bounds__(NTHR) k_bgemm(const GemmJob* __restrict__ jobs
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
         uint32_t gm = tile.m0 + m, gn = tile.n0 + n;
         if (gm < J.M && gn < J.N) {
-            double* c = C + J.c_off + gm + uint64_t(gn) * J.ldc;
+            uint64_t base = J.c_off;
+            if (J.crb) { const uint32_t blk = gm / J.crb; base += uint64_t(blk) * J.c_bs; gm -= blk * J.crb; }
+            double* c = C + base + gm + uint64_t(gn) * J.ldc;
             *c = (J.beta == 0.0) ? J.alpha * v : J.alpha * v + J.beta * *c;
         }
     });
@@ -147,11 +151,17 @@ void batched_gemm(const std::vector<GemmJob>& jobs, const double* A, uint64_t a_
                   double* C, uint64_t c_len, DBuf<GemmJob>& jobbuf, DBuf<uint32_t>& tilebuf, cudaStream_t s) {
     if (jobs.empty()) return;
     for (const GemmJob& j : jobs) {
-        if (j.ta) check_extent(j.a_off, j.K, j.M, j.lda, a_len, "gemm A");
-        else check_extent(j.a_off, j.M, j.K, j.lda, a_len, "gemm A");
+        if (!j.M || !j.N) continue;
+        const uint32_t arb = j.arb ? j.arb : j.M, crb = j.crb ? j.crb : j.M;
+        if (j.M % arb || j.M % crb) throw std::runtime_error("gemm: rows are not a whole number of row blocks");
+        const uint64_t alast = j.a_off + uint64_t(j.M / arb - 1) * j.a_bs, clast = j.c_off + uint64_t(j.M / crb - 1) * j.c_bs;
+        for (uint64_t ao : {j.a_off, alast}) {
+            if (j.ta) check_extent(ao, j.K, arb, j.lda, a_len, "gemm A");
+            else check_extent(ao, arb, j.K, j.lda, a_len, "gemm A");
+        }
         if (j.tb) check_extent(j.b_off, j.N, j.K, j.ldb, b_len, "gemm B");
         else check_extent(j.b_off, j.K, j.N, j.ldb, b_len, "gemm B");
-        check_extent(j.c_off, j.M, j.N, j.ldc, c_len, "gemm C");
+        for (uint64_t co : {j.c_off, clast}) check_extent(co, crb, j.N, j.ldc, c_len, "gemm C");
     }
     std::vector<GTile> tiles;
     for (uint32_t j = 0; j < jobs.size(); ++j)

@@ -14,11 +14,16 @@ namespace qcm {
 
 // C[c_off] (M x N, ldc) = alpha * op(A)[a_off] * op(B)[b_off] + beta * C
 // op(A) = A (lda, column-major) or A^T; same for B.
+// Row-blocked operands (arb / crb > 0): rows m of op(A) / C come in blocks of arb / crb rows,
+// block j starting at a_off + j*a_bs / c_off + j*c_bs (a stack of matrices with their own
+// layout, as a boundary's MPO-index blocks are stored); M must be a multiple of the block.
 struct GemmJob {
     uint64_t a_off, b_off, c_off;
     uint32_t M, N, K, lda, ldb, ldc;
     uint32_t ta, tb;
     double alpha, beta;
+    uint32_t arb = 0, crb = 0;
+    uint64_t a_bs = 0, c_bs = 0;
 };
 
 // dst[dst_off + i + j*dst_ld] = src[src_off + i + j*src_ld] (i < rows, j < cols);

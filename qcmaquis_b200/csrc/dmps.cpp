@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
+#include <string>
 
 #include "dmrg_dev.hpp"
 
@@ -347,9 +348,31 @@ TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMP
         vo[k] = vl; vl += (uint64_t(both.cols[k]) * kk[k] + 31) / 32 * 32;
     }
     DBuf<double> U(std::max<uint64_t>(ul, 1)), S(std::max<uint64_t>(sl, 1)), V(std::max<uint64_t>(vl, 1));
-    for (std::size_t k = 0; k < nb; ++k)
-        svd_thin(*c.sv, c.s, both.d.get() + both.off[k], int(both.rows[k]), int(both.cols[k]), U.get() + uo[k], S.get() + so[k],
-                 V.get() + vo[k]);
+    // independent block SVDs on the solver's side lanes, largest first, round robin
+    std::vector<std::size_t> order(nb);
+    for (std::size_t k = 0; k < nb; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](std::size_t x, std::size_t y) { return both.elems(x) > both.elems(y); });
+    int* info = c.sv->reserve_info(uint32_t(nb), c.s);
+    c.sv->fork(c.s);
+    // cuSOLVER's Jacobi SVD returns only when its block is done, so each lane gets its own host thread
+    std::string err;
+#pragma omp parallel for num_threads(Solver::LANES) schedule(static, 1)
+    for (int lane = 0; lane < Solver::LANES; ++lane) {
+        try {
+            QCM_CUDA(cudaSetDevice(c.device));
+            for (std::size_t i = std::size_t(lane); i < nb; i += Solver::LANES) {
+                const std::size_t k = order[i];
+                svd_thin_lane(*c.sv, lane, both.d.get() + both.off[k], int(both.rows[k]), int(both.cols[k]), U.get() + uo[k],
+                              S.get() + so[k], V.get() + vo[k], info + k);
+            }
+        } catch (const std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
+    c.sv->join(c.s);
     c.sv->check(c.s);
     std::vector<double> hs(sl);
     if (sl) QCM_CUDA(cudaMemcpyAsync(hs.data(), S.get(), sl * sizeof(double), cudaMemcpyDeviceToHost, c.s));

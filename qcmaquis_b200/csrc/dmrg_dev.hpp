@@ -80,6 +80,7 @@ struct SBuild {
 // Engine context: stream, cuSOLVER handle and scratch buffers reused across steps.
 struct Ctx {
     cudaStream_t s = nullptr;
+    int device = 0;
     std::unique_ptr<Solver> sv;
     DBuf<double> T, S, work, tmp, jd, scal, coef;
     DBuf<GemmJob> gjobs;

@@ -128,15 +128,15 @@ struct HeffPlan {
     std::vector<uint32_t> x_cols;
     uint64_t x_len = 0;
 
-    std::vector<TJobD> tjobs;
+    hvec<TJobD> tjobs;
     std::vector<TileD> ttiles[N_SHAPES];
     uint64_t t_len = 0;
 
-    std::vector<UnitD> units;
+    hvec<UnitD> units;
     std::vector<TileD> utiles[N_SHAPES];   // (unit, line tile m0, element tile n0)
-    std::vector<uint32_t> line_b1, sptr;
-    std::vector<uint64_t> slice_off;
-    std::vector<WEntD> went;
+    hvec<uint32_t> line_b1, sptr;
+    hvec<uint64_t> slice_off;
+    hvec<WEntD> went;
     uint64_t s_len = 0;
 
     std::vector<SegD> segs;

@@ -81,11 +81,56 @@ Solver::Solver() {
     QCM_SOLVER(cusolverDnXgesvdjSetSortEig(svdp, 1));
     info.alloc(INFO_CAP);
     tau.alloc(1024);
+    QCM_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+    for (Lane& L : lane) {
+        QCM_CUDA(cudaStreamCreateWithFlags(&L.s, cudaStreamNonBlocking));
+        register_stream(L.s);
+        QCM_CUDA(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
+        QCM_SOLVER(cusolverDnCreate(&L.h));
+        QCM_SOLVER(cusolverDnSetStream(L.h, L.s));
+        QCM_SOLVER(cusolverDnCreateGesvdjInfo(&L.svdp));
+        QCM_SOLVER(cusolverDnXgesvdjSetMaxSweeps(L.svdp, 100));
+        QCM_SOLVER(cusolverDnXgesvdjSetSortEig(L.svdp, 1));
+    }
 }
 
 Solver::~Solver() {
+    for (Lane& L : lane) {
+        if (L.s) cudaStreamSynchronize(L.s);
+        L.a.reset();
+        L.work.reset();
+        if (L.s) {
+            cudaStreamSynchronize(L.s);
+            retire_stream(L.s);
+        }
+        if (L.svdp) cusolverDnDestroyGesvdjInfo(L.svdp);
+        if (L.h) cusolverDnDestroy(L.h);
+        if (L.done) cudaEventDestroy(L.done);
+        if (L.s) cudaStreamDestroy(L.s);
+    }
+    if (fork_ev) cudaEventDestroy(fork_ev);
     if (svdp) cusolverDnDestroyGesvdjInfo(svdp);
     if (h) cusolverDnDestroy(h);
+}
+
+void Solver::fork(cudaStream_t s) {
+    QCM_CUDA(cudaEventRecord(fork_ev, s));
+    for (Lane& L : lane) QCM_CUDA(cudaStreamWaitEvent(L.s, fork_ev, 0));
+}
+
+int* Solver::reserve_info(uint32_t n, cudaStream_t s) {
+    if (n > INFO_CAP) throw std::runtime_error("too many factorizations in one batch");
+    if (n_info + n > INFO_CAP) check(s);
+    int* p = info.get() + n_info;
+    n_info += n;
+    return p;
+}
+
+void Solver::join(cudaStream_t s) {
+    for (Lane& L : lane) {
+        QCM_CUDA(cudaEventRecord(L.done, L.s));
+        QCM_CUDA(cudaStreamWaitEvent(s, L.done, 0));
+    }
 }
 
 void Solver::bind(cudaStream_t s) { QCM_SOLVER(cusolverDnSetStream(h, s)); }
@@ -111,6 +156,20 @@ void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double*
     ensure(sv.work, std::size_t(lwork));
     QCM_SOLVER(cusolverDnDgesvdj(sv.h, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, sv.a.get(), m, S, U, m, V, n, sv.work.get(), lwork,
                                  next_info(sv, s), sv.svdp));
+}
+
+void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, double* S, double* V, int* info) {
+    if (m == 0 || n == 0) return;
+    Solver::Lane& L = sv.lane[l];
+    AllocStream scope(L.s);  // a lane's buffers are ordered on the lane's stream
+    if (L.a.size() < std::size_t(m) * n) L.a.alloc(std::size_t(m) * n);
+    QCM_CUDA(cudaMemcpyAsync(L.a.get(), A, std::size_t(m) * n * sizeof(double), cudaMemcpyDeviceToDevice, L.s));
+    int lwork = 0;
+    QCM_SOLVER(cusolverDnDgesvdj_bufferSize(L.h, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, L.a.get(), m, S, U, m, V, n, &lwork,
+                                            L.svdp));
+    if (L.work.size() < std::size_t(lwork)) L.work.alloc(std::size_t(lwork));
+    QCM_SOLVER(cusolverDnDgesvdj(L.h, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, L.a.get(), m, S, U, m, V, n, L.work.get(), lwork,
+                                 info, L.svdp));
 }
 
 namespace {

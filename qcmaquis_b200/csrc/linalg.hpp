@@ -23,6 +23,17 @@ struct Solver {
     DBuf<double> work, a, b, tau;
     DBuf<int> info;  // one status word per factorization since the last check
     uint32_t n_info = 0;
+    // side streams for independent per-block factorizations (fork from / join to a stream)
+    static constexpr int LANES = 8;
+    struct Lane {
+        cudaStream_t s = nullptr;
+        cusolverDnHandle_t h = nullptr;
+        gesvdjInfo_t svdp = nullptr;
+        DBuf<double> a, work;
+        cudaEvent_t done = nullptr;
+    };
+    Lane lane[LANES];
+    cudaEvent_t fork_ev = nullptr;
     Solver();
     ~Solver();
     Solver(const Solver&) = delete;
@@ -30,11 +41,19 @@ struct Solver {
     void bind(cudaStream_t s);
     // throws if any factorization since the last call reported a failure (synchronizes s)
     void check(cudaStream_t s);
+    // lanes start after the work queued on s so far; s continues after all lanes' work
+    void fork(cudaStream_t s);
+    void join(cudaStream_t s);
+    // n consecutive status words for factorizations issued from several host threads
+    int* reserve_info(uint32_t n, cudaStream_t s);
 };
 
 // A (m x n, lda = m) is read only.  k = min(m, n).
 // U (m x k, ld m), S (k, descending), V (n x k, ld n): A = U diag(S) V^T
 void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* U, double* S, double* V);
+// the same on side lane `l` (between fork and join), status to *info; lanes may be driven
+// from different host threads (one thread per lane: the Jacobi SVD blocks its caller)
+void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, double* S, double* V, int* info);
 // Q (m x k, ld m), R (k x n, ld k, upper trapezoidal): A = Q R
 void qr_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* Q, double* R);
 // L (m x k, ld m, lower trapezoidal), Q (k x n, ld k): A = L Q
