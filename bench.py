@@ -276,6 +276,7 @@ def run_b200(a, world, rank, local, pg):
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "init_bond_dimension": a.init_bd,
                            "seed": a.seed, "vec_len": n, "flops_per_step": info["flops"],
+                           "coefficient_block_doubles": info["w_len"], "s_len": info["s_len"], "t_len": info["t_len"],
                            "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
                 "sweep": sinfo,
                 "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},

@@ -113,6 +113,7 @@ typedef struct {
     uint64_t n_kitems;                        /* split-K items of the L.S GEMM */
     double flops_sdense;                      /* tensor-core work of the S build (dense unit GEMMs) */
     uint64_t launches;                        /* own kernels launched per apply */
+    uint64_t w_len;                           /* doubles of the dense coefficient blocks of the S build */
 } qcm_heff_info;
 
 #define QCM_PLAN_BOOKKEEPING 1 /* keep the (cohort, unit, line, alpha) list for parity checks */

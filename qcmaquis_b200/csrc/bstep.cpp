@@ -119,16 +119,20 @@ void emit_units(BPart& P, const std::vector<uint32_t>& pos, uint64_t s_off, cons
 void append_sbuild(SBuild& dst, const SBuild& src, uint64_t t_base, uint64_t s_base) {
     const uint32_t u0 = uint32_t(dst.units.size()), l0 = uint32_t(dst.line_b1.size()), k0 = uint32_t(dst.slice_off.size());
     const uint32_t p0 = uint32_t(dst.sptr.size()), w0 = uint32_t(dst.went.size());
+    const uint64_t wb = dst.w_len;
     for (UnitD u : src.units) {
-        u.s_off += s_base; u.line0 += l0; u.slice0 += k0; u.sptr0 += p0;
+        u.s_off += s_base; u.line0 += l0; u.slice0 += k0; u.sptr0 += p0; u.w_off += wb;
         dst.units.push_back(u);
     }
+    dst.w_len += src.w_len;
+    const uint32_t kb = uint32_t(dst.klist.size());
+    dst.klist.insert(dst.klist.end(), src.klist.begin(), src.klist.end());
     dst.line_b1.insert(dst.line_b1.end(), src.line_b1.begin(), src.line_b1.end());
     for (uint64_t o : src.slice_off) dst.slice_off.push_back(o + t_base);
     for (uint32_t p : src.sptr) dst.sptr.push_back(p + w0);
     dst.went.insert(dst.went.end(), src.went.begin(), src.went.end());
     for (int k = 0; k < N_SHAPES; ++k)
-        for (TileD t : src.utiles[k]) { t.item += u0; dst.utiles[k].push_back(t); }
+        for (TileD t : src.utiles[k]) { t.item += u0; t.pad += kb; dst.utiles[k].push_back(t); }
 }
 
 }  // namespace
@@ -148,21 +152,22 @@ void SBuild::add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint
     u.s_off = s_off; u.line_stride = line_stride; u.erows = erows; u.col_stride = col_stride; u.ne = ne;
     u.nl = uint32_t(lines.size()); u.line0 = uint32_t(line_b1.size());
     u.nk = uint32_t(slices.size()); u.slice0 = uint32_t(slice_off.size()); u.sptr0 = uint32_t(sptr.size());
+    u.w_off = w_len;
+    w_len += uint64_t(u.nl) * u.nk;
     line_b1.insert(line_b1.end(), lines.begin(), lines.end());
     slice_off.insert(slice_off.end(), slices.begin(), slices.end());
     std::vector<WEntD> es(ents.size());
     for (std::size_t i = 0; i < ents.size(); ++i) es[i] = WEntD{ents[i].line, ek[i], ents[i].a};
     pack_unit_entries(std::move(es), u.nk, went, sptr);
-    int sh = shape_for_rows(u.nl);
-    uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
-    for (uint32_t n0 = 0; n0 < u.ne; n0 += bn)
-        for (uint32_t m0 = 0; m0 < u.nl; m0 += bm) utiles[sh].push_back(TileD{uint32_t(units.size()), m0, n0, 0});
+    const uint32_t e0 = sptr[u.sptr0], e1 = sptr[u.sptr0 + u.nk];
+    add_unit_tiles(u, uint32_t(units.size()), went.data() + e0, e1 - e0, utiles, klist);
     units.push_back(u);
 }
 
 void SBuild::validate(uint64_t t_len, uint64_t s_len) const {
     for (const UnitD& u : units) {
         if (!u.ne || !u.nl) continue;
+        if (u.w_off + uint64_t(u.nl) * u.nk > w_len) throw std::runtime_error("device work list out of bounds: coefficient block");
         if (u.erows == 0 || u.ne % u.erows) throw std::runtime_error("S unit: element count is not a whole number of columns");
         uint32_t maxline = 0;
         for (uint32_t l = 0; l < u.nl; ++l) maxline = std::max(maxline, line_b1[u.line0 + l]);
@@ -173,6 +178,14 @@ void SBuild::validate(uint64_t t_len, uint64_t s_len) const {
         for (uint32_t w = sptr[u.sptr0]; w < sptr[u.sptr0 + u.nk]; ++w)
             if (went[w].line >= u.nl || went[w].k >= u.nk) throw std::runtime_error("S unit: coefficient index out of range");
     }
+    for (int sh = 0; sh < N_SHAPES; ++sh)
+        for (const TileD& t : utiles[sh]) {
+            if (t.item >= units.size() || std::size_t(t.pad) >= klist.size() || std::size_t(t.pad) + 1 + klist[t.pad] > klist.size())
+                throw std::runtime_error("S tile outside its work lists");
+            const UnitD& u = units[t.item];
+            for (uint32_t i = 0; i < klist[t.pad]; ++i)
+                if (uint32_t(klist[t.pad + 1 + i]) * 16 >= u.nk) throw std::runtime_error("S tile: k-step out of range");
+        }
 }
 
 void SBuild::upload(cudaStream_t s) {
@@ -182,6 +195,7 @@ void SBuild::upload(cudaStream_t s) {
     d_sptr.upload(sptr, s);
     d_slice_off.upload(slice_off, s);
     d_went.upload(went, s);
+    d_klist.upload(klist, s);
 }
 
 void complement_transpose(BoundaryIndexH& x, const std::vector<int32_t>& herm, const std::vector<int32_t>& phase, bool forward) {
@@ -415,8 +429,10 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
     sb.upload(c.s);
     run_tgemm(c.tjobs.get(), c.ttiles, ttiles, ket.b.d.get(), Rold.data.get(), c.T.get(), c.s);
     if (s_len) QCM_CUDA(cudaMemsetAsync(c.S.get(), 0, s_len * sizeof(double), c.s));
-    run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_sptr.get(),
-              sb.d_went.get(), c.T.get(), c.S.get(), c.s);
+    Ctx::ensure(c.W, sb.w_len ? sb.w_len : 1);
+    fill_coefficients(sb.d_units.get(), uint32_t(sb.units.size()), sb.d_sptr.get(), sb.d_went.get(), c.W.get(), sb.w_len, c.s);
+    run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
+              c.T.get(), c.S.get(), c.s);
     // A = S scratch, B = ket data, C = new boundary: three different base pointers
     batched_gemm(prop, c.S.get(), s_len, ket.b.d.get(), ket.b.total, Rn->data.get(), Rn->idx.total, c.gjobs, c.gtiles, c.s);
     step_report("right", tb0, tbp, tb1, c.s);
@@ -598,8 +614,10 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
     sb.validate(t_len, s_len);
     sb.upload(c.s);
     if (s_len) QCM_CUDA(cudaMemsetAsync(c.S.get(), 0, s_len * sizeof(double), c.s));
-    run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_sptr.get(),
-              sb.d_went.get(), c.T.get(), c.S.get(), c.s);
+    Ctx::ensure(c.W, sb.w_len ? sb.w_len : 1);
+    fill_coefficients(sb.d_units.get(), uint32_t(sb.units.size()), sb.d_sptr.get(), sb.d_went.get(), c.W.get(), sb.w_len, c.s);
+    run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
+              c.T.get(), c.S.get(), c.s);
     batched_gemm(prop, bra.b.d.get(), bra.b.total, c.S.get(), s_len, Ln->data.get(), Ln->idx.total, c.gjobs, c.gtiles, c.s);
     step_report("left", tb0, tbp, tb1, c.s);
     return Ln;

@@ -36,6 +36,7 @@ struct Shape {
 using Sh16 = Shape<1, 4, 2, 4>;  // 16 x 128
 using Sh32 = Shape<1, 4, 4, 4>;  // 32 x 128
 using Sh64 = Shape<2, 2, 4, 4>;  // 64 x 64
+using Sh128 = Shape<4, 1, 4, 4>; // 128 x 32
 
 template <class S>
 struct Stage {

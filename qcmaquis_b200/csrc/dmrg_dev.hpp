@@ -63,7 +63,10 @@ struct SBuild {
     std::vector<uint32_t> line_b1, sptr;
     std::vector<uint64_t> slice_off;
     std::vector<WEntD> went;
+    uint64_t w_len = 0;  // dense coefficient blocks (doubles)
+    std::vector<uint16_t> klist;  // non-empty k-steps per S-GEMM m-tile
     DBuf<UnitD> d_units;
+    DBuf<uint16_t> d_klist;
     DBuf<TileD> d_utiles[N_SHAPES];
     DBuf<uint32_t> d_line_b1, d_sptr;
     DBuf<uint64_t> d_slice_off;
@@ -82,7 +85,7 @@ struct Ctx {
     cudaStream_t s = nullptr;
     int device = 0;
     std::unique_ptr<Solver> sv;
-    DBuf<double> T, S, work, tmp, jd, scal, coef;
+    DBuf<double> T, S, W, work, tmp, jd, scal, coef;
     DBuf<GemmJob> gjobs;
     DBuf<uint32_t> gtiles;
     DBuf<CopyJob> cjobs;

@@ -76,6 +76,7 @@ struct UnitD {        // S rows of one cohort unit: S_u (lines x elements) = W_u
     uint32_t nk;           // distinct T slices referenced
     uint32_t slice0;       // first entry in slice_off[]
     uint32_t sptr0;        // first of nk + 1 entry pointers in sptr[]
+    uint64_t w_off;        // dense coefficient block W_u (nl x nk, column-major) in the W buffer
 };
 struct WEntD {        // coefficient alpha at (line, slice) of a unit; entries sorted by slice
     uint32_t line, k;
@@ -116,11 +117,19 @@ inline void pack_unit_entries(std::vector<WEntD> ents, uint32_t nk, std::vector<
     while (k < nk) { sptr.push_back(uint32_t(went.size())); ++k; }
 }
 
-// DMMA tile shapes (rows x cols of the CTA tile); the class is chosen per job from its row count
-enum { SHAPE_16 = 0, SHAPE_32 = 1, SHAPE_64 = 2, N_SHAPES = 3 };
+// DMMA tile shapes (rows x cols of the CTA tile).  GEMM jobs pick the class from their row
+// count (16 x 128, 32 x 128, 64 x 64); S-build units also use 128 x 32 (see add_unit_tiles).
+enum { SHAPE_16 = 0, SHAPE_32 = 1, SHAPE_64 = 2, SHAPE_128 = 3, N_SHAPES = 4 };
 inline int shape_for_rows(uint32_t M) { return M <= 16 ? SHAPE_16 : (M <= 32 ? SHAPE_32 : SHAPE_64); }
-inline uint32_t shape_bm(int s) { return s == SHAPE_16 ? 16 : (s == SHAPE_32 ? 32 : 64); }
-inline uint32_t shape_bn(int s) { return s == SHAPE_64 ? 64 : 128; }
+inline uint32_t shape_bm(int s) { return s == SHAPE_16 ? 16 : (s == SHAPE_32 ? 32 : (s == SHAPE_64 ? 64 : 128)); }
+inline uint32_t shape_bn(int s) { return s == SHAPE_64 ? 64 : (s == SHAPE_128 ? 32 : 128); }
+
+// S-GEMM tiles of one unit.  ents[0..n) are the unit's coefficient entries.  The tile shape
+// is the one with the least tensor work counting only the (BM lines x 16 slices) coefficient
+// blocks that hold an entry; every m-tile's non-empty k-steps go to klist as (count, steps...)
+// and its tiles carry that list's offset in TileD::pad.
+void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_t n, std::vector<TileD>* utiles,
+                    std::vector<uint16_t>& klist);
 
 struct HeffPlan {
     Index phys, left, right;
@@ -138,6 +147,8 @@ struct HeffPlan {
     hvec<uint64_t> slice_off;
     hvec<WEntD> went;
     uint64_t s_len = 0;
+    uint64_t w_len = 0;  // dense coefficient blocks of all units (doubles)
+    std::vector<uint16_t> klist;  // non-empty k-steps per S-GEMM m-tile
 
     std::vector<SegD> segs;
     std::vector<OutD> outs;
@@ -166,6 +177,8 @@ struct HeffPlan {
     DBuf<uint32_t> d_line_b1, d_sptr;
     DBuf<uint64_t> d_slice_off;
     DBuf<WEntD> d_went;
+    DBuf<double> d_W;
+    DBuf<uint16_t> d_klist;
     DBuf<SegD> d_segs;
     DBuf<OutD> d_outs;
     DBuf<double> d_T, d_S;
@@ -193,8 +206,11 @@ int heff_launches_per_apply(const HeffPlan& p);
 void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const double* x,
                const double* R, double* T, cudaStream_t s);
 void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const uint32_t* line_b1,
-               const uint64_t* slice_off, const uint32_t* sptr, const WEntD* went, const double* T, double* S,
+               const uint64_t* slice_off, const uint16_t* klist, const double* W, const double* T, double* S,
                cudaStream_t s);
+// Scatters every unit's coefficient entries into its dense block of W (w_len doubles, zeroed first).
+void fill_coefficients(const UnitD* units, uint32_t n_units, const uint32_t* sptr, const WEntD* went, double* W,
+                       uint64_t w_len, cudaStream_t s);
 // Same apply with caller-provided scratch: Tb (t_len), Sb (s_len) and Pb (p_len) doubles.
 void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* Tb, double* Sb, double* Pb);
 

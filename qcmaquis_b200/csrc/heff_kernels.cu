@@ -9,8 +9,9 @@
 //
 //   k_tgemm   : T[ti] = psi_slab * R[ci_eff] (per-block transposed when the R
 //               cohort is stored as its Hermitian partner)         (tasks.cpp:707-752)
-//   k_sgemm   : S rows of a cohort unit = W_u (lines x slices, the sparse MPO
-//               coefficients densified tile by tile in shared memory) * T slices.
+//   k_sgemm   : S rows of a cohort unit = W_u (lines x slices, the unit's MPO
+//               coefficients as a dense block, scattered once per plan by
+//               k_wfill) * T slices.
 //               Replaces the alpha-weighted gather (gpu_dgemm_ddot.cu:282-359,
 //               tasks.cpp:466-494) by a tensor-core GEMM.
 //   k_lspart  : split-K partial tiles of y[lb_out] = sum_cohorts L[ci_eff] * S
@@ -19,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <stdexcept>
 
 #include "dmma.cuh"
 #include "heff.hpp"
@@ -102,46 +104,46 @@ __global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, 
 template <class S>
 __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units, const TileD* __restrict__ tiles,
                                                 const uint32_t* __restrict__ line_b1, const uint64_t* __restrict__ slice_off,
-                                                const uint32_t* __restrict__ sptr, const WEntD* __restrict__ went,
+                                                const uint16_t* __restrict__ klist, const double* __restrict__ W,
                                                 const double* __restrict__ T, double* __restrict__ Sm) {
-    __shared__ double Bs[2][BK][S::BN + PAD];
-    __shared__ double As[BK][S::BM + PAD];
-    __shared__ uint64_t soff[2][BK];
+    __shared__ Stage<S> st[2];
     const TileD tile = tiles[blockIdx.x];
     const UnitD U = units[tile.item];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t nk = (U.nk + BK - 1) / BK;
+    // only the k-steps whose coefficient block (this tile's lines x 16 slices) holds an entry
+    const uint16_t* ks = klist + tile.pad;
+    const uint32_t nsteps = ks[0];
+    const double* Wu = W + U.w_off;
     auto issue = [&](int sidx, uint32_t k0) {
-        if (tid < BK) soff[sidx][tid] = (k0 + tid < U.nk) ? slice_off[U.slice0 + k0 + tid] : 0;
-        __syncthreads();
+        Stage<S>& s = st[sidx];
+        // A = W_u (lines x slices, column-major, ld nl)
+#pragma unroll
+        for (int rr = 0; rr < S::A_PER; ++rr) {
+            int e = tid + rr * NTHR;
+            int m = e % S::BM, k = e / S::BM;
+            uint32_t gm = tile.m0 + m, gk = k0 + k;
+            bool ok = gm < U.nl && gk < U.nk;
+            cp8(&s.A[k][m], ok ? Wu + gm + uint64_t(gk) * U.nl : W, ok);
+        }
+        // B row k = T slice k (ne contiguous elements)
 #pragma unroll
         for (int rr = 0; rr < S::B_PER; ++rr) {
             int e = tid + rr * NTHR;
             int n = e % S::BN, k = e / S::BN;
             uint32_t gn = tile.n0 + n, gk = k0 + k;
             bool ok = gn < U.ne && gk < U.nk;
-            cp8(&Bs[sidx][k][n], ok ? T + soff[sidx][k] + gn : T, ok);
+            cp8(&s.B[k][n], ok ? T + __ldg(slice_off + U.slice0 + gk) + gn : T, ok);
         }
         cp_commit();
     };
     Acc<S> acc;
     acc.zero();
-    issue(0, 0);
-    for (uint32_t kc = 0; kc < nk; ++kc) {
-        const uint32_t k0 = kc * BK;
-        // densify the coefficient tile W_u[m0 .. m0+BM, k0 .. k0+BK]
-        for (int e = tid; e < BK * (S::BM + PAD); e += NTHR) (&As[0][0])[e] = 0.0;
-        __syncthreads();
-        const uint32_t e0 = sptr[U.sptr0 + k0], e1 = sptr[U.sptr0 + min(k0 + BK, U.nk)];
-        for (uint32_t e = e0 + tid; e < e1; e += NTHR) {
-            const WEntD w = went[e];
-            if (w.line >= tile.m0 && w.line < tile.m0 + S::BM) As[w.k - k0][w.line - tile.m0] = w.a;
-        }
+    if (nsteps) issue(0, uint32_t(ks[1]) * BK);
+    for (uint32_t i = 0; i < nsteps; ++i) {
         cp_wait_all();
         __syncthreads();
-        if (kc + 1 < nk) issue((kc + 1) & 1, k0 + BK);
-        mma_stage<S>(As, Bs[kc & 1], acc, warp, lane);
-        __syncthreads();
+        if (i + 1 < nsteps) issue((i + 1) & 1, uint32_t(ks[2 + i]) * BK);
+        mma_stage<S>(st[i & 1].A, st[i & 1].B, acc, warp, lane);
     }
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
         uint32_t gl = tile.m0 + m, gn = tile.n0 + n;
@@ -151,6 +153,17 @@ __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units,
             Sm[U.s_off + uint64_t(b1) * U.line_stride + r + uint64_t(c) * U.col_stride] = v;
         }
     });
+}
+
+// One CTA per unit: its coefficient entries into the dense block W_u (duplicates were merged on the host)
+__global__ void k_wfill(const UnitD* __restrict__ units, const uint32_t* __restrict__ sptr, const WEntD* __restrict__ went,
+                        double* __restrict__ W) {
+    const UnitD U = units[blockIdx.x];
+    const uint32_t e0 = sptr[U.sptr0], e1 = sptr[U.sptr0 + U.nk];
+    for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+        const WEntD w = went[e];
+        W[U.w_off + w.line + uint64_t(w.k) * U.nl] = w.a;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -251,7 +264,7 @@ template <class S>
 void launch_s(HeffPlan& p, int sh, const double* Tb, double* Sb, cudaStream_t s) {
     if (!p.utiles[sh].empty())
         k_sgemm<S><<<unsigned(p.utiles[sh].size()), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get(), p.d_line_b1.get(),
-                                                                  p.d_slice_off.get(), p.d_sptr.get(), p.d_went.get(), Tb, Sb);
+                                                                  p.d_slice_off.get(), p.d_klist.get(), p.d_W.get(), Tb, Sb);
 }
 
 template <class S>
@@ -279,6 +292,7 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
     launch_s<Sh16>(p, SHAPE_16, Tb, Sb, s);
     launch_s<Sh32>(p, SHAPE_32, Tb, Sb, s);
     launch_s<Sh64>(p, SHAPE_64, Tb, Sb, s);
+    launch_s<Sh128>(p, SHAPE_128, Tb, Sb, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
     launch_ls<Sh16>(p, SHAPE_16, Sb, Pb, y, s);
     launch_ls<Sh32>(p, SHAPE_32, Sb, Pb, y, s);
@@ -308,14 +322,23 @@ void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<T
 }
 
 void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const uint32_t* line_b1,
-               const uint64_t* slice_off, const uint32_t* sptr, const WEntD* went, const double* T, double* S,
+               const uint64_t* slice_off, const uint16_t* klist, const double* W, const double* T, double* S,
                cudaStream_t s) {
     if (!htiles[SHAPE_16].empty())
-        k_sgemm<Sh16><<<unsigned(htiles[SHAPE_16].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_16].get(), line_b1, slice_off, sptr, went, T, S);
+        k_sgemm<Sh16><<<unsigned(htiles[SHAPE_16].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_16].get(), line_b1, slice_off, klist, W, T, S);
     if (!htiles[SHAPE_32].empty())
-        k_sgemm<Sh32><<<unsigned(htiles[SHAPE_32].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_32].get(), line_b1, slice_off, sptr, went, T, S);
+        k_sgemm<Sh32><<<unsigned(htiles[SHAPE_32].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_32].get(), line_b1, slice_off, klist, W, T, S);
     if (!htiles[SHAPE_64].empty())
-        k_sgemm<Sh64><<<unsigned(htiles[SHAPE_64].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_64].get(), line_b1, slice_off, sptr, went, T, S);
+        k_sgemm<Sh64><<<unsigned(htiles[SHAPE_64].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_64].get(), line_b1, slice_off, klist, W, T, S);
+    if (!htiles[SHAPE_128].empty())
+        k_sgemm<Sh128><<<unsigned(htiles[SHAPE_128].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_128].get(), line_b1, slice_off, klist, W, T, S);
+    QCM_CUDA(cudaGetLastError());
+}
+
+void fill_coefficients(const UnitD* units, uint32_t n_units, const uint32_t* sptr, const WEntD* went, double* W,
+                       uint64_t w_len, cudaStream_t s) {
+    if (w_len) QCM_CUDA(cudaMemsetAsync(W, 0, w_len * sizeof(double), s));
+    if (n_units) k_wfill<<<n_units, 128, 0, s>>>(units, sptr, went, W);
     QCM_CUDA(cudaGetLastError());
 }
 
@@ -331,6 +354,17 @@ int heff_launches_per_apply(const HeffPlan& p) {
 
 void upload_plan(HeffPlan& p) {
     cudaStream_t s = p.stream;
+    for (const UnitD& u : p.units)
+        if (u.w_off + uint64_t(u.nl) * u.nk > p.w_len || (u.nk && u.slice0 + u.nk > p.slice_off.size()))
+            throw std::runtime_error("heff plan: unit outside its work lists");
+    for (int sh = 0; sh < N_SHAPES; ++sh)
+        for (const TileD& t : p.utiles[sh]) {
+            if (t.item >= p.units.size() || std::size_t(t.pad) >= p.klist.size() ||
+                std::size_t(t.pad) + 1 + p.klist[t.pad] > p.klist.size())
+                throw std::runtime_error("heff plan: S tile outside its work lists");
+            for (uint32_t i = 0; i < p.klist[t.pad]; ++i)
+                if (uint32_t(p.klist[t.pad + 1 + i]) * BK >= p.units[t.item].nk) throw std::runtime_error("heff plan: S tile k-step out of range");
+        }
     p.d_tjobs.upload(p.tjobs, s);
     for (int sh = 0; sh < N_SHAPES; ++sh) {
         p.d_ttiles[sh].upload(p.ttiles[sh], s);
@@ -343,11 +377,15 @@ void upload_plan(HeffPlan& p) {
     p.d_slice_off.upload(p.slice_off, s);
     p.d_sptr.upload(p.sptr, s);
     p.d_went.upload(p.went, s);
+    p.d_klist.upload(p.klist, s);
     p.d_segs.upload(p.segs, s);
     p.d_outs.upload(p.outs, s);
     p.d_T.alloc(p.t_len);
     p.d_S.alloc(p.s_len);
     p.d_P.alloc(p.p_len);
+    // dense coefficient blocks, built once per plan and reused by every apply
+    p.d_W.alloc(p.w_len ? p.w_len : 1);
+    fill_coefficients(p.d_units.get(), uint32_t(p.units.size()), p.d_sptr.get(), p.d_went.get(), p.d_W.get(), p.w_len, s);
     QCM_CUDA(cudaStreamSynchronize(s));
 }
 

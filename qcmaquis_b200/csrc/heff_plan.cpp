@@ -64,7 +64,7 @@ struct Part {
     std::vector<uint32_t> line_b1, sptr;
     std::vector<uint64_t> slice_off;
     std::vector<WEntD> went;
-    uint64_t s_len = 0;
+    uint64_t s_len = 0, w_len = 0;
     std::vector<std::pair<uint32_t, SegD>> segs;
     double flops_t = 0, flops_s = 0, flops_ls = 0, flops_sdense = 0;
     uint64_t g_elems = 0, g_reads = 0;
@@ -76,6 +76,41 @@ struct Em { uint32_t line, slice; double a; uint32_t mps, cir, col; };
 struct U { uint32_t st, offset, ms, rb_out; std::vector<Em> em; std::vector<uint32_t> lines; };
 
 }  // namespace
+
+void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_t n, std::vector<TileD>* utiles,
+                    std::vector<uint16_t>& klist) {
+    if (!u.nl || !u.ne || !u.nk || !n) return;
+    constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK)
+    const uint32_t nks = (u.nk + KS - 1) / KS;
+    // candidate shapes and a relative cost per tensor flop (the 16-row shape runs 2 x 4 fragments per warp)
+    static const int cand[4] = {SHAPE_16, SHAPE_32, SHAPE_64, SHAPE_128};
+    static const double eff[4] = {1.3, 1.0, 1.0, 1.05};
+    int best = -1;
+    double best_cost = 0;
+    std::vector<uint8_t> occ, best_occ;
+    for (int ci = 0; ci < 4; ++ci) {
+        const uint32_t bm = shape_bm(cand[ci]), bn = shape_bn(cand[ci]);
+        const uint32_t nmt = (u.nl + bm - 1) / bm, nnt = (u.ne + bn - 1) / bn;
+        occ.assign(std::size_t(nmt) * nks, 0);
+        for (std::size_t i = 0; i < n; ++i) occ[std::size_t(ents[i].line / bm) * nks + ents[i].k / KS] = 1;
+        std::size_t on = 0;
+        for (uint8_t o : occ) on += o;
+        const double cost = eff[ci] * double(on) * bm * KS * double(nnt) * bn;
+        if (best < 0 || cost < best_cost) { best = ci; best_cost = cost; best_occ.swap(occ); }
+    }
+    const int sh = cand[best];
+    const uint32_t bm = shape_bm(sh), bn = shape_bn(sh), nmt = (u.nl + bm - 1) / bm;
+    for (uint32_t mt = 0; mt < nmt; ++mt) {
+        const uint32_t off = uint32_t(klist.size());
+        klist.push_back(0);
+        uint16_t cnt = 0;
+        for (uint32_t ks = 0; ks < nks; ++ks)
+            if (best_occ[std::size_t(mt) * nks + ks]) { klist.push_back(uint16_t(ks)); ++cnt; }
+        klist[off] = cnt;
+        if (!cnt) continue;
+        for (uint32_t n0 = 0; n0 < u.ne; n0 += bn) utiles[sh].push_back(TileD{item, mt * bm, n0, off});
+    }
+}
 
 std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
                                           const Index& phys, const Index& left, const Index& right, bool bookkeeping) {
@@ -250,6 +285,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 ud.nl = uint32_t(u.lines.size()); ud.line0 = uint32_t(P.line_b1.size());
                 ud.nk = uint32_t(slices.size()); ud.slice0 = uint32_t(P.slice_off.size());
                 ud.sptr0 = uint32_t(P.sptr.size());
+                ud.w_off = P.w_len;
+                P.w_len += uint64_t(ud.nl) * ud.nk;
                 P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
                 for (uint32_t gp : slices) {
                     // slot -> (job, b2 position) -> T offset of the slice
@@ -285,12 +322,12 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
 
     const double t_b = tnow();
     // ---- merge the parts in ket-sector order: prefix offsets, one allocation, parallel copy ----
-    struct Base { uint64_t t, s; uint32_t job, unit, line, slice, sptr, went; std::size_t bk; };
+    struct Base { uint64_t t, s, w; uint32_t job, unit, line, slice, sptr, went; std::size_t bk; };
     std::vector<Base> base(nl + 1);
-    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0, 0};
+    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (uint32_t i = 0; i < nl; ++i) {
         const Part& P = parts[i];
-        base[i + 1] = Base{base[i].t + P.t_len, base[i].s + P.s_len, base[i].job + uint32_t(P.tjobs.size()),
+        base[i + 1] = Base{base[i].t + P.t_len, base[i].s + P.s_len, base[i].w + P.w_len, base[i].job + uint32_t(P.tjobs.size()),
                            base[i].unit + uint32_t(P.units.size()), base[i].line + uint32_t(P.line_b1.size()),
                            base[i].slice + uint32_t(P.slice_off.size()), base[i].sptr + uint32_t(P.sptr.size()),
                            base[i].went + uint32_t(P.went.size()), base[i].bk + P.bk_alpha.size()};
@@ -310,7 +347,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         for (std::size_t k = 0; k < P.tjobs.size(); ++k) { TJobD j = P.tjobs[k]; j.c_off += B.t; p->tjobs[B.job + k] = j; }
         for (std::size_t k = 0; k < P.units.size(); ++k) {
             UnitD u = P.units[k];
-            u.s_off += B.s; u.line0 += B.line; u.slice0 += B.slice; u.sptr0 += B.sptr;
+            u.s_off += B.s; u.line0 += B.line; u.slice0 += B.slice; u.sptr0 += B.sptr; u.w_off += B.w;
             p->units[B.unit + k] = u;
         }
         std::copy(P.line_b1.begin(), P.line_b1.end(), p->line_b1.begin() + B.line);
@@ -327,6 +364,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     }
     p->t_len = tot.t;
     p->s_len = tot.s;
+    p->w_len = tot.w;
     std::vector<std::vector<SegD>> per_out(nl);
     for (uint32_t i = 0; i < nl; ++i) {
         const Part& P = parts[i];
@@ -336,12 +374,23 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     }
     for (uint32_t j = 0; j < p->tjobs.size(); ++j)
         if (p->tjobs[j].M && p->tjobs[j].N) add_tiles(p->ttiles, j, p->tjobs[j].M, p->tjobs[j].N);
-    for (uint32_t k = 0; k < p->units.size(); ++k) {
-        const UnitD& u = p->units[k];
-        int sh = shape_for_rows(u.nl);
-        uint32_t bm = shape_bm(sh), bn = shape_bn(sh);
-        for (uint32_t n0 = 0; n0 < u.ne; n0 += bn)
-            for (uint32_t m0 = 0; m0 < u.nl; m0 += bm) p->utiles[sh].push_back(TileD{k, m0, n0, 0});
+    {
+        // S-GEMM tiles and their non-empty k-steps, per unit in parallel, then concatenated in unit order
+        const std::size_t nu = p->units.size();
+        struct UT { std::vector<TileD> t[N_SHAPES]; std::vector<uint16_t> kl; };
+        std::vector<UT> ut(nu);
+#pragma omp parallel for schedule(dynamic, 16)
+        for (long long kk = 0; kk < (long long)nu; ++kk) {
+            const UnitD& u = p->units[kk];
+            const uint32_t e0 = p->sptr[u.sptr0], e1 = p->sptr[u.sptr0 + u.nk];
+            add_unit_tiles(u, uint32_t(kk), p->went.data() + e0, e1 - e0, ut[kk].t, ut[kk].kl);
+        }
+        for (std::size_t k = 0; k < nu; ++k) {
+            const uint32_t kb = uint32_t(p->klist.size());
+            for (int sh = 0; sh < N_SHAPES; ++sh)
+                for (TileD t : ut[k].t[sh]) { t.pad += kb; p->utiles[sh].push_back(t); }
+            p->klist.insert(p->klist.end(), ut[k].kl.begin(), ut[k].kl.end());
+        }
     }
     // output blocks, their segments (lb_in order) and split-K items
     for (uint32_t lb_out = 0; lb_out < nl; ++lb_out) {
@@ -372,7 +421,45 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         }
         p->outs.push_back(o);
     }
-    if (tdbg) std::fprintf(stderr, "plan: tables+parts %.3f s, merge %.3f s\n", t_b - t_a, tnow() - t_b);
+    if (tdbg) {
+        std::fprintf(stderr, "plan: tables+parts %.3f s, merge %.3f s\n", t_b - t_a, tnow() - t_b);
+        // S-build unit shapes: useful (nalpha), dense (nl*nk) and tile-padded work
+        double w_alpha = 0, w_dense = 0, w_pad = 0;
+        uint64_t hist_nl[8] = {0}, hist_nk[8] = {0};
+        double fl_nl[8] = {0}, fl_nk[8] = {0};
+        auto bin = [](uint32_t v) { int b = 0; while (b < 7 && v > (4u << b)) ++b; return b; };  // <=4,8,...,256,>256
+        for (const UnitD& u : p->units) {
+            const uint32_t na = p->sptr[u.sptr0 + u.nk] - p->sptr[u.sptr0];
+            const int sh = shape_for_rows(u.nl);
+            const double bm = shape_bm(sh), bn = shape_bn(sh);
+            w_alpha += 2.0 * na * u.ne;
+            w_dense += 2.0 * u.nl * double(u.nk) * u.ne;
+            w_pad += 2.0 * std::ceil(u.nl / bm) * bm * std::ceil(u.nk / 16.0) * 16.0 * std::ceil(u.ne / bn) * bn;
+            hist_nl[bin(u.nl)]++; hist_nk[bin(u.nk)]++;
+            fl_nl[bin(u.nl)] += 2.0 * u.nl * double(u.nk) * u.ne;
+            fl_nk[bin(u.nk)] += 2.0 * u.nl * double(u.nk) * u.ne;
+        }
+        std::fprintf(stderr, "plan: %zu units, S work alpha %.3e dense %.3e padded %.3e flop\n", p->units.size(), w_alpha, w_dense, w_pad);
+        // k-step occupancy of the coefficient tiles: work if all-zero (BM x 16) blocks were skipped
+        for (int bmq : {16, 32, 64, 128}) {
+            double w_skip = 0, w_full = 0;
+            for (const UnitD& u : p->units) {
+                const uint32_t nmt = (u.nl + bmq - 1) / bmq, nks = (u.nk + 15) / 16;
+                std::vector<uint8_t> occ(std::size_t(nmt) * nks, 0);
+                for (uint32_t w = p->sptr[u.sptr0]; w < p->sptr[u.sptr0 + u.nk]; ++w)
+                    occ[std::size_t(p->went[w].line / bmq) * nks + p->went[w].k / 16] = 1;
+                std::size_t on = 0;
+                for (uint8_t o : occ) on += o;
+                w_skip += 2.0 * on * bmq * 16.0 * u.ne;
+                w_full += 2.0 * nmt * bmq * nks * 16.0 * u.ne;
+            }
+            std::fprintf(stderr, "  BM %3d: padded (lines, slices) work %.3e, nonzero-block work %.3e (%.2f)\n", bmq, w_full, w_skip,
+                         w_skip / w_full);
+        }
+        for (int b = 0; b < 8; ++b)
+            std::fprintf(stderr, "  bin <=%u: nl units %llu (dense flop %.2e) | nk units %llu (dense flop %.2e)\n", 4u << b,
+                         (unsigned long long)hist_nl[b], fl_nl[b], (unsigned long long)hist_nk[b], fl_nk[b]);
+    }
     uint64_t pl = 0;
     for (int sh = 0; sh < N_SHAPES; ++sh) pl = std::max<uint64_t>(pl, uint64_t(p->kitems[sh].size()) * shape_bm(sh) * shape_bn(sh));
     p->p_len = pl;
