@@ -115,24 +115,50 @@ void emit_units(BPart& P, const std::vector<uint32_t>& pos, uint64_t s_off, cons
     }
 }
 
-// Appends src (offsets relative to its part) to dst with T / S bases.
-void append_sbuild(SBuild& dst, const SBuild& src, uint64_t t_base, uint64_t s_base) {
-    const uint32_t u0 = uint32_t(dst.units.size()), l0 = uint32_t(dst.line_b1.size()), k0 = uint32_t(dst.slice_off.size());
-    const uint32_t p0 = uint32_t(dst.sptr.size()), w0 = uint32_t(dst.went.size());
-    const uint64_t wb = dst.w_len;
-    for (UnitD u : src.units) {
-        u.s_off += s_base; u.line0 += l0; u.slice0 += k0; u.sptr0 += p0; u.w_off += wb;
-        dst.units.push_back(u);
+// Concatenates the parts' S-build lists in part order (offsets relative to each part), with
+// the parts' T / S buffer bases; the copies run in parallel over parts.
+template <class Part>
+void merge_sbuilds(std::vector<Part>& parts, SBuild& dst, const std::vector<uint64_t>& t_base,
+                   const std::vector<uint64_t>& s_base) {
+    const std::size_t np = parts.size();
+    struct B { std::size_t unit, line, slice, sptr, went, kl; uint64_t w; std::size_t tile[N_SHAPES]; };
+    std::vector<B> base(np + 1);
+    base[0] = B{};
+    for (std::size_t i = 0; i < np; ++i) {
+        const SBuild& x = parts[i].sb;
+        B b = base[i];
+        b.unit += x.units.size(); b.line += x.line_b1.size(); b.slice += x.slice_off.size(); b.sptr += x.sptr.size();
+        b.went += x.went.size(); b.kl += x.klist.size(); b.w += x.w_len;
+        for (int k = 0; k < N_SHAPES; ++k) b.tile[k] += x.utiles[k].size();
+        base[i + 1] = b;
     }
-    dst.w_len += src.w_len;
-    const uint32_t kb = uint32_t(dst.klist.size());
-    dst.klist.insert(dst.klist.end(), src.klist.begin(), src.klist.end());
-    dst.line_b1.insert(dst.line_b1.end(), src.line_b1.begin(), src.line_b1.end());
-    for (uint64_t o : src.slice_off) dst.slice_off.push_back(o + t_base);
-    for (uint32_t p : src.sptr) dst.sptr.push_back(p + w0);
-    dst.went.insert(dst.went.end(), src.went.begin(), src.went.end());
-    for (int k = 0; k < N_SHAPES; ++k)
-        for (TileD t : src.utiles[k]) { t.item += u0; t.pad += kb; dst.utiles[k].push_back(t); }
+    const B& tot = base[np];
+    dst.units.resize(tot.unit); dst.line_b1.resize(tot.line); dst.slice_off.resize(tot.slice); dst.sptr.resize(tot.sptr);
+    dst.went.resize(tot.went); dst.klist.resize(tot.kl); dst.w_len = tot.w;
+    for (int k = 0; k < N_SHAPES; ++k) dst.utiles[k].resize(tot.tile[k]);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long long ii = 0; ii < (long long)np; ++ii) {
+        SBuild& x = parts[ii].sb;
+        const B& b = base[ii];
+        for (std::size_t k = 0; k < x.units.size(); ++k) {
+            UnitD u = x.units[k];
+            u.s_off += s_base[ii]; u.line0 += uint32_t(b.line); u.slice0 += uint32_t(b.slice); u.sptr0 += uint32_t(b.sptr);
+            u.w_off += b.w;
+            dst.units[b.unit + k] = u;
+        }
+        std::copy(x.line_b1.begin(), x.line_b1.end(), dst.line_b1.begin() + b.line);
+        for (std::size_t k = 0; k < x.slice_off.size(); ++k) dst.slice_off[b.slice + k] = x.slice_off[k] + t_base[ii];
+        for (std::size_t k = 0; k < x.sptr.size(); ++k) dst.sptr[b.sptr + k] = x.sptr[k] + uint32_t(b.went);
+        std::copy(x.went.begin(), x.went.end(), dst.went.begin() + b.went);
+        std::copy(x.klist.begin(), x.klist.end(), dst.klist.begin() + b.kl);
+        for (int sh = 0; sh < N_SHAPES; ++sh)
+            for (std::size_t k = 0; k < x.utiles[sh].size(); ++k) {
+                TileD t = x.utiles[sh][k];
+                t.item += uint32_t(b.unit); t.pad += uint32_t(b.kl);
+                dst.utiles[sh][b.tile[sh] + k] = t;
+            }
+        x = SBuild();
+    }
 }
 
 }  // namespace
@@ -140,13 +166,19 @@ void append_sbuild(SBuild& dst, const SBuild& src, uint64_t t_base, uint64_t s_b
 void SBuild::add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint32_t col_stride, uint32_t ne,
                       const std::vector<uint32_t>& lines, const std::vector<E>& ents) {
     if (ents.empty() || ne == 0) return;
-    std::unordered_map<uint64_t, uint32_t> kid;
+    // slices numbered in first-use order (open-addressing table keyed by the T offset)
+    std::size_t cap = 16;
+    while (cap < 2 * ents.size()) cap <<= 1;
+    std::vector<uint64_t> key(cap, ~uint64_t(0));
+    std::vector<uint32_t> val(cap);
     std::vector<uint64_t> slices;
     std::vector<uint32_t> ek(ents.size());
     for (std::size_t i = 0; i < ents.size(); ++i) {
-        auto ins = kid.emplace(ents[i].slice, uint32_t(slices.size()));
-        if (ins.second) slices.push_back(ents[i].slice);
-        ek[i] = ins.first->second;
+        const uint64_t sl = ents[i].slice;
+        std::size_t h = std::size_t((sl * 0x9E3779B97F4A7C15ull) >> 17) & (cap - 1);
+        while (key[h] != ~uint64_t(0) && key[h] != sl) h = (h + 1) & (cap - 1);
+        if (key[h] == ~uint64_t(0)) { key[h] = sl; val[h] = uint32_t(slices.size()); slices.push_back(sl); }
+        ek[i] = val[h];
     }
     UnitD u{};
     u.s_off = s_off; u.line_stride = line_stride; u.erows = erows; u.col_stride = col_stride; u.ne = ne;
@@ -384,6 +416,12 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
     nidx.bra = left; nidx.ket = left; nidx.aux = W.rows;
     struct Pend { uint32_t ci_new; uint32_t lb_ket, lb_bra, nS; uint64_t s_off; };
     std::vector<Pend> pend;
+    std::vector<uint64_t> tb(nl), sbase(nl);
+    {
+        uint64_t t = 0, sx = 0;
+        for (uint32_t lb = 0; lb < nl; ++lb) { tb[lb] = t; sbase[lb] = sx; t += parts[lb].t_len; sx += parts[lb].s_len; }
+    }
+    merge_sbuilds(parts, sb, tb, sbase);
     for (uint32_t lb = 0; lb < nl; ++lb) {
         BPart& P = parts[lb];
         for (TJobD j : P.tjobs) {
@@ -391,7 +429,6 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
             if (j.M && j.N) add_tiles(ttiles, uint32_t(tjobs.size()), j.M, j.N);
             tjobs.push_back(j);
         }
-        append_sbuild(sb, P.sb, t_len, s_len);
         for (auto& ch : P.coh) {
             pend.push_back(Pend{nidx.n_cohorts(), ch.bra, ch.ket, ch.nS, ch.s_off + s_len});
             nidx.cbra.push_back(ch.bra); nidx.cket.push_back(ch.ket);
@@ -578,10 +615,15 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
     nidx.bra = right; nidx.ket = right; nidx.aux = W.cols;
     struct Pend { uint32_t ci_new, rb_bra, nS; uint64_t s_off; uint32_t rs_ket; };
     std::vector<Pend> pend;
+    std::vector<uint64_t> tb(nr), sbase(nr);
+    {
+        uint64_t t = 0, sx = 0;
+        for (uint32_t rb = 0; rb < nr; ++rb) { tb[rb] = t; sbase[rb] = sx; t += parts[rb].t_len; sx += parts[rb].s_len; }
+    }
+    merge_sbuilds(parts, sb, tb, sbase);
     for (uint32_t rb = 0; rb < nr; ++rb) {
         BPart& P = parts[rb];
         for (GemmJob g : P.tgemm) { g.c_off += t_len; tj_gemm.push_back(g); }
-        append_sbuild(sb, P.sb, t_len, s_len);
         for (auto& ch : P.coh) {
             pend.push_back(Pend{nidx.n_cohorts(), ch.bra, ch.nS, ch.s_off + s_len, uint32_t(right[ch.ket].second)});
             nidx.cbra.push_back(ch.bra); nidx.cket.push_back(ch.ket);

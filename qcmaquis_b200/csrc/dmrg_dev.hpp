@@ -58,11 +58,11 @@ struct DMPS {
 
 // Work lists of the unit S-GEMM (shared by H_eff and the boundary steps)
 struct SBuild {
-    std::vector<UnitD> units;
+    hvec<UnitD> units;
     std::vector<TileD> utiles[N_SHAPES];
-    std::vector<uint32_t> line_b1, sptr;
-    std::vector<uint64_t> slice_off;
-    std::vector<WEntD> went;
+    hvec<uint32_t> line_b1, sptr;
+    hvec<uint64_t> slice_off;
+    hvec<WEntD> went;
     uint64_t w_len = 0;  // dense coefficient blocks (doubles)
     std::vector<uint16_t> klist;  // non-empty k-steps per S-GEMM m-tile
     DBuf<UnitD> d_units;

@@ -103,18 +103,32 @@ struct OTileD {       // output tile of the L.S GEMM and its contiguous range of
 // several MPO terms may couple the same boundary block, input state and output state,
 // and the densified coefficient tile holds their sum -- and the unit's nk + 1 slice
 // pointers to sptr.
-inline void pack_unit_entries(std::vector<WEntD> ents, uint32_t nk, std::vector<WEntD>& went, std::vector<uint32_t>& sptr) {
-    std::stable_sort(ents.begin(), ents.end(),
-                     [](const WEntD& x, const WEntD& y) { return x.k < y.k || (x.k == y.k && x.line < y.line); });
-    const uint32_t w0 = uint32_t(went.size());
-    uint32_t k = 0;
-    sptr.push_back(w0);
-    for (std::size_t i = 0; i < ents.size(); ++i) {
-        while (k < ents[i].k) { sptr.push_back(uint32_t(went.size())); ++k; }
-        if (went.size() > w0 && went.back().k == ents[i].k && went.back().line == ents[i].line) went.back().a += ents[i].a;
-        else went.push_back(ents[i]);
+template <class WV, class PV>
+inline void pack_unit_entries(std::vector<WEntD> ents, uint32_t nk, WV& went, PV& sptr) {
+    // counting sort by slice; entries arrive in line order, so each slice's lines stay ascending
+    std::vector<uint32_t> cnt(std::size_t(nk) + 1, 0);
+    for (const WEntD& e : ents) cnt[e.k + 1]++;
+    for (uint32_t k = 0; k < nk; ++k) cnt[k + 1] += cnt[k];
+    std::vector<WEntD> sorted(ents.size());
+    {
+        std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
+        for (const WEntD& e : ents) sorted[fill[e.k]++] = e;
     }
-    while (k < nk) { sptr.push_back(uint32_t(went.size())); ++k; }
+    for (uint32_t k = 0; k < nk; ++k)  // a slice's lines need not arrive sorted when lines repeat out of order
+        if (!std::is_sorted(sorted.begin() + cnt[k], sorted.begin() + cnt[k + 1],
+                            [](const WEntD& x, const WEntD& y) { return x.line < y.line; }))
+            std::stable_sort(sorted.begin() + cnt[k], sorted.begin() + cnt[k + 1],
+                             [](const WEntD& x, const WEntD& y) { return x.line < y.line; });
+    const uint32_t w0 = uint32_t(went.size());
+    sptr.push_back(w0);
+    for (uint32_t k = 0; k < nk; ++k) {
+        for (uint32_t i = cnt[k]; i < cnt[k + 1]; ++i) {
+            const WEntD& e = sorted[i];
+            if (went.size() > w0 && went.back().k == e.k && went.back().line == e.line) went.back().a += e.a;
+            else went.push_back(e);
+        }
+        sptr.push_back(uint32_t(went.size()));
+    }
 }
 
 // DMMA tile shapes (rows x cols of the CTA tile).  GEMM jobs pick the class from their row

@@ -82,6 +82,16 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_
     if (!u.nl || !u.ne || !u.nk || !n) return;
     constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK)
     const uint32_t nks = (u.nk + KS - 1) / KS;
+    // occupancy of (16 lines x 16 slices) coefficient blocks; coarser line tiles OR rows together
+    const uint32_t n16 = (u.nl + 15) / 16;
+    std::vector<uint8_t> occ16(std::size_t(n16) * nks, 0);
+    for (std::size_t i = 0; i < n; ++i) occ16[std::size_t(ents[i].line / 16) * nks + ents[i].k / KS] = 1;
+    auto occ_at = [&](uint32_t bm, std::vector<uint8_t>& occ) {
+        const uint32_t f = bm / 16, nmt = (u.nl + bm - 1) / bm;
+        occ.assign(std::size_t(nmt) * nks, 0);
+        for (uint32_t r = 0; r < n16; ++r)
+            for (uint32_t ks = 0; ks < nks; ++ks) occ[std::size_t(r / f) * nks + ks] |= occ16[std::size_t(r) * nks + ks];
+    };
     // candidate shapes and a relative cost per tensor flop (the 16-row shape runs 2 x 4 fragments per warp)
     static const int cand[4] = {SHAPE_16, SHAPE_32, SHAPE_64, SHAPE_128};
     static const double eff[4] = {1.3, 1.0, 1.0, 1.05};
@@ -90,9 +100,8 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_
     std::vector<uint8_t> occ, best_occ;
     for (int ci = 0; ci < 4; ++ci) {
         const uint32_t bm = shape_bm(cand[ci]), bn = shape_bn(cand[ci]);
-        const uint32_t nmt = (u.nl + bm - 1) / bm, nnt = (u.ne + bn - 1) / bn;
-        occ.assign(std::size_t(nmt) * nks, 0);
-        for (std::size_t i = 0; i < n; ++i) occ[std::size_t(ents[i].line / bm) * nks + ents[i].k / KS] = 1;
+        const uint32_t nnt = (u.ne + bn - 1) / bn;
+        occ_at(bm, occ);
         std::size_t on = 0;
         for (uint8_t o : occ) on += o;
         const double cost = eff[ci] * double(on) * bm * KS * double(nnt) * bn;
@@ -439,7 +448,9 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             fl_nl[bin(u.nl)] += 2.0 * u.nl * double(u.nk) * u.ne;
             fl_nk[bin(u.nk)] += 2.0 * u.nl * double(u.nk) * u.ne;
         }
-        std::fprintf(stderr, "plan: %zu units, S work alpha %.3e dense %.3e padded %.3e flop\n", p->units.size(), w_alpha, w_dense, w_pad);
+        std::fprintf(stderr, "plan: %zu units, %zu coefficients, %zu S tiles, S work alpha %.3e dense %.3e padded %.3e flop\n",
+                     p->units.size(), p->went.size(), p->utiles[0].size() + p->utiles[1].size() + p->utiles[2].size() + p->utiles[3].size(),
+                     w_alpha, w_dense, w_pad);
         // k-step occupancy of the coefficient tiles: work if all-zero (BM x 16) blocks were skipped
         for (int bmq : {16, 32, 64, 128}) {
             double w_skip = 0, w_full = 0;
