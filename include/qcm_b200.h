@@ -223,6 +223,9 @@ typedef struct {
     double jcd_tol;               /* ietl_jcd_tol */
     int32_t jcd_maxiter;          /* ietl_jcd_maxiter (1..64) */
     double ecore;                 /* added to the reported energies */
+    int32_t twosite_truncation;   /* 0: svd, 1: heev on the reduced density matrix with noise alpha */
+    double alpha_initial, alpha_main, alpha_final; /* noise of sweeps < ngrowsweeps, < + nmainsweeps, later */
+    int32_t ngrowsweeps, nmainsweeps;
 } qcm_dmrg_params;
 /* block_matrix_algorithms.h:48-63 */
 typedef struct {

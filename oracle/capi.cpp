@@ -69,6 +69,14 @@ void orc_dmrg_free(orc_dmrg* h) { if (h) { delete h->d; delete h; } }
 
 int orc_dmrg_set_mmax(orc_dmrg* h, size_t Mmax) { h->d->p.Mmax = Mmax; return 0; }
 
+// twosite_truncation = heev with alpha_initial / alpha_main / alpha_final over ngrowsweeps / nmainsweeps
+int orc_dmrg_set_heev(orc_dmrg* h, int heev, double a_init, double a_main, double a_final, int ngrow, int nmain) {
+    DMRGParams& p = h->d->p;
+    p.heev = heev != 0; p.alpha_initial = a_init; p.alpha_main = a_main; p.alpha_final = a_final;
+    p.ngrowsweeps = ngrow; p.nmainsweeps = nmain;
+    return 0;
+}
+
 // energies/tw/tf/bond: arrays of 2L-2.  If stop_step >= 0, the frozen site problem of
 // that step is returned in *snap (free with orc_free) and the sweep stops there.
 int orc_dmrg_sweep(orc_dmrg* h, int sweep, double* energies, double* tw, double* tf, uint64_t* bond, int stop_step,

@@ -276,12 +276,15 @@ typedef void (*dorgqr_t)(const int*, const int*, const int*, double*, const int*
 typedef void (*dsyevx_t)(const char*, const char*, const char*, const int*, double*, const int*, const double*,
                          const double*, const int*, const int*, const double*, int*, double*, double*, const int*,
                          double*, const int*, int*, int*, int*);
+typedef void (*dsyevd_t)(const char*, const char*, const int*, double*, const int*, double*, double*, const int*, int*,
+                         const int*, int*);
 typedef void (*setthreads_t)(int);
 dgemm_t p_dgemm = nullptr;
 dgesvd_t p_dgesvd = nullptr;
 dgeqrf_t p_dgeqrf = nullptr, p_dgelqf = nullptr;
 dorgqr_t p_dorgqr = nullptr, p_dorglq = nullptr;
 dsyevx_t p_dsyevx = nullptr;
+dsyevd_t p_dsyevd = nullptr;
 }  // namespace
 
 bool blas_init(const char* path, std::string& err) {
@@ -297,8 +300,9 @@ bool blas_init(const char* path, std::string& err) {
     p_dorgqr = (dorgqr_t)dlsym(h, "scipy_dorgqr_");
     p_dorglq = (dorgqr_t)dlsym(h, "scipy_dorglq_");
     p_dsyevx = (dsyevx_t)dlsym(h, "scipy_dsyevx_");
+    p_dsyevd = (dsyevd_t)dlsym(h, "scipy_dsyevd_");
     auto st = (setthreads_t)dlsym(h, "scipy_openblas_set_num_threads");
-    if (!p_dgemm || !p_dgesvd || !p_dgeqrf || !p_dgelqf || !p_dorgqr || !p_dorglq || !p_dsyevx) {
+    if (!p_dgemm || !p_dgesvd || !p_dgeqrf || !p_dgelqf || !p_dorgqr || !p_dorglq || !p_dsyevx || !p_dsyevd) {
         err = "missing LAPACK symbol";
         p_dgemm = nullptr;
         return false;
@@ -402,6 +406,29 @@ void dsyevx_lowest(const double* M, int ldm, int dim, double abstol, double& w, 
     if (info != 0) throw std::runtime_error("oracle dsyevx failed");
     w = wv[0];
     z.assign(zv.begin(), zv.begin() + dim);
+}
+
+void heev_desc(const Mat& M0, Mat& evecs, std::vector<double>& evals) {
+    const int n = int(M0.r);
+    evals.assign(n, 0.0);
+    evecs = Mat(n, n);
+    if (n == 0) return;
+    Mat A = M0;
+    char jobz = 'V', uplo = 'L';
+    int lwork = -1, liwork = -1, info = 0, iwq = 0;
+    double wq = 0;
+    std::vector<double> w(n);
+    p_dsyevd(&jobz, &uplo, &n, A.d.data(), &n, w.data(), &wq, &lwork, &iwq, &liwork, &info);
+    lwork = std::max(1, int(wq));
+    liwork = std::max(1, iwq);
+    std::vector<double> work(lwork);
+    std::vector<int> iwork(liwork);
+    p_dsyevd(&jobz, &uplo, &n, A.d.data(), &n, w.data(), work.data(), &lwork, iwork.data(), &liwork, &info);
+    if (info != 0) throw std::runtime_error("oracle dsyevd failed");
+    for (int c = 0; c < n; ++c) {
+        evals[c] = w[n - 1 - c];
+        for (int i = 0; i < n; ++i) evecs(i, c) = A(i, n - 1 - c);
+    }
 }
 
 }  // namespace orc

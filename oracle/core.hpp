@@ -190,5 +190,7 @@ void qr(const Mat& A, Mat& Q, Mat& R);
 void lq(const Mat& A, Mat& L, Mat& Qm);
 // lowest eigenpair of the leading dim x dim upper triangle of M (ld = ldm), dsyevx range 'I'
 void dsyevx_lowest(const double* M, int ldm, int dim, double abstol, double& w, std::vector<double>& z);
+// alps/matrix/algorithms.hpp:374-396 (heevd 'V', then reversed to descending order)
+void heev_desc(const Mat& M, Mat& evecs, std::vector<double>& evals);
 
 }  // namespace orc

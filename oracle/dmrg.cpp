@@ -182,17 +182,10 @@ void TwoSite::set_from_mps(const MPSTensor& tw) {
     }
 }
 
-TruncationResults svd_truncate(const BlockMatrix& M, BlockMatrix& U, BlockMatrix& V, std::vector<std::vector<double>>& S,
-                               double cutoff, std::size_t Mmax) {
-    std::size_t nb = M.n_blocks();
-    U = BlockMatrix(); V = BlockMatrix();
-    std::vector<Mat> Ub(nb), Vb(nb);
-    S.assign(nb, {});
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int k = 0; k < int(nb); ++k) dgesvd_thin(M.b[k], Ub[k], S[k], Vb[k]);
-    // estimate_truncation (block_matrix_algorithms.h:136-183)
+TruncationResults estimate_truncation(const std::vector<std::vector<double>>& vals, std::size_t Mmax, double cutoff,
+                                      std::vector<std::size_t>& keeps) {
     std::vector<double> all;
-    for (auto& s : S) all.insert(all.end(), s.begin(), s.end());
+    for (auto& s : vals) all.insert(all.end(), s.begin(), s.end());
     std::sort(all.begin(), all.end());
     std::reverse(all.begin(), all.end());
     TruncationResults tr;
@@ -205,8 +198,49 @@ TruncationResults svd_truncate(const BlockMatrix& M, BlockMatrix& U, BlockMatrix
     for (double x : all) { sum += x; sum2 += x * x; }
     tr.truncated_fraction = tf / sum;
     tr.truncated_weight = tw / sum2;
+    keeps.assign(vals.size(), 0);
+    for (std::size_t k = 0; k < vals.size(); ++k)
+        keeps[k] = std::size_t(std::find_if(vals[k].begin(), vals[k].end(), [&](double x) { return x < evalscut; }) - vals[k].begin());
+    return tr;
+}
+
+TruncationResults heev_truncate(const BlockMatrix& dm, BlockMatrix& U, double cutoff, std::size_t Mmax) {
+    const std::size_t nb = dm.n_blocks();
+    std::vector<Mat> ev(nb);
+    std::vector<std::vector<double>> w(nb), wsq(nb);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < int(nb); ++k) heev_desc(dm.b[k], ev[k], w[k]);
     for (std::size_t k = 0; k < nb; ++k) {
-        std::size_t keep = std::find_if(S[k].begin(), S[k].end(), [&](double x) { return x < evalscut; }) - S[k].begin();
+        wsq[k] = w[k];
+        for (double& x : wsq[k]) if (x > 0.0) x = std::sqrt(x);
+    }
+    std::vector<std::size_t> keeps;
+    TruncationResults tr = estimate_truncation(wsq, Mmax, cutoff, keeps);
+    U = BlockMatrix();
+    for (std::size_t k = 0; k < nb; ++k) {
+        if (keeps[k] == 0) continue;
+        Mat u(ev[k].r, keeps[k]);
+        for (std::size_t j = 0; j < keeps[k]; ++j)
+            for (std::size_t i = 0; i < ev[k].r; ++i) u(i, j) = ev[k](i, j);
+        U.insert(dm.lc[k], dm.rc[k], std::move(u));
+        tr.bond_dimension += keeps[k];
+    }
+    tr.truncated_weight = tr.truncated_fraction;  // heev_truncate reports the fraction in both fields
+    return tr;
+}
+
+TruncationResults svd_truncate(const BlockMatrix& M, BlockMatrix& U, BlockMatrix& V, std::vector<std::vector<double>>& S,
+                               double cutoff, std::size_t Mmax) {
+    std::size_t nb = M.n_blocks();
+    U = BlockMatrix(); V = BlockMatrix();
+    std::vector<Mat> Ub(nb), Vb(nb);
+    S.assign(nb, {});
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < int(nb); ++k) dgesvd_thin(M.b[k], Ub[k], S[k], Vb[k]);
+    std::vector<std::size_t> keeps;
+    TruncationResults tr = estimate_truncation(S, Mmax, cutoff, keeps);
+    for (std::size_t k = 0; k < nb; ++k) {
+        const std::size_t keep = keeps[k];
         if (keep == 0) { S[k].clear(); continue; }
         Mat u(Ub[k].r, keep), v(keep, Vb[k].c);
         for (std::size_t j = 0; j < keep; ++j)
@@ -248,6 +282,74 @@ void TwoSite::split_r2l(std::size_t Mmax, double cutoff, MPSTensor& m1, MPSTenso
             for (std::size_t i = 0; i < U.b[k].r; ++i) U.b[k](i, j) *= S[k][j];
     m1 = MPSTensor();
     m1.phys = phys1; m1.left = left; m1.right = U.right_basis(); m1.pairing = LeftPaired; m1.data = U;
+}
+
+void TwoSite::predict_split_l2r(std::size_t Mmax, double cutoff, double alpha, const Boundary& lb, const MPOTensor& mpo,
+                                MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const {
+    if (alpha == 0.0) { split_l2r(Mmax, cutoff, m1, m2, tr); return; }
+    // the both-paired data as a left-paired tensor over (phys1, left) x (adjoin(phys2) * right)
+    MPSTensor tmp;
+    tmp.phys = phys1; tmp.left = left; tmp.right = adjoin(phys2) * right; tmp.pairing = LeftPaired; tmp.data = both;
+    BlockMatrix dm;
+    for (std::size_t k = 0; k < both.n_blocks(); ++k) {
+        const Mat& b = both.b[k];
+        Mat d(b.r, b.r);
+        dgemm('N', 'T', int(b.r), int(b.r), int(b.c), 1.0, b.d.data(), int(std::max<std::size_t>(b.r, 1)), b.d.data(),
+              int(std::max<std::size_t>(b.r, 1)), 0.0, d.d.data(), int(std::max<std::size_t>(b.r, 1)));
+        dm.insert(both.lc[k], both.lc[k], std::move(d));
+    }
+    alpha_dm_direct(tmp, lb, mpo, dm, alpha);
+    BlockMatrix U;
+    tr = heev_truncate(dm, U, cutoff, Mmax);
+    m1 = MPSTensor();
+    m1.phys = phys1; m1.left = left; m1.right = U.right_basis(); m1.pairing = LeftPaired; m1.data = U;
+    BlockMatrix V;  // U^T both
+    for (std::size_t k = 0; k < U.n_blocks(); ++k) {
+        const std::size_t j = both.find(U.lc[k], U.lc[k]);
+        const Mat& u = U.b[k];
+        const Mat& b = both.b[j];
+        Mat v(u.c, b.c);
+        dgemm('T', 'N', int(u.c), int(b.c), int(u.r), 1.0, u.d.data(), int(u.r), b.d.data(), int(b.r), 0.0, v.d.data(), int(u.c));
+        V.insert(U.lc[k], U.lc[k], std::move(v));
+    }
+    m2 = MPSTensor();
+    m2.phys = phys2; m2.left = V.left_basis(); m2.right = right; m2.pairing = RightPaired; m2.data = V;
+}
+
+void TwoSite::predict_split_r2l(std::size_t Mmax, double cutoff, double alpha, const Boundary& rb, const MPOTensor& mpo,
+                                MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const {
+    if (alpha == 0.0) { split_r2l(Mmax, cutoff, m1, m2, tr); return; }
+    // the both-paired data as a right-paired tensor over (phys1 * left) x (phys2, right)
+    MPSTensor tmp;
+    tmp.phys = phys2; tmp.left = phys1 * left; tmp.right = right; tmp.pairing = RightPaired; tmp.data = both;
+    BlockMatrix dm;
+    for (std::size_t k = 0; k < both.n_blocks(); ++k) {
+        const Mat& b = both.b[k];
+        Mat d(b.c, b.c);
+        dgemm('T', 'N', int(b.c), int(b.c), int(b.r), 1.0, b.d.data(), int(std::max<std::size_t>(b.r, 1)), b.d.data(),
+              int(std::max<std::size_t>(b.r, 1)), 0.0, d.d.data(), int(std::max<std::size_t>(b.c, 1)));
+        dm.insert(both.lc[k], both.lc[k], std::move(d));
+    }
+    alpha_dm_direct_right(tmp, rb, mpo, dm, alpha);
+    BlockMatrix U;
+    tr = heev_truncate(dm, U, cutoff, Mmax);
+    BlockMatrix Ut, V;  // U^T (right-paired site 2) and both U (left-paired site 1)
+    for (std::size_t k = 0; k < U.n_blocks(); ++k) {
+        const Mat& u = U.b[k];
+        Mat t(u.c, u.r);
+        for (std::size_t j = 0; j < u.c; ++j)
+            for (std::size_t i = 0; i < u.r; ++i) t(j, i) = u(i, j);
+        Ut.insert(U.lc[k], U.lc[k], std::move(t));
+        const std::size_t jb = both.find(U.lc[k], U.lc[k]);
+        const Mat& b = both.b[jb];
+        Mat v(b.r, u.c);
+        dgemm('N', 'N', int(b.r), int(u.c), int(b.c), 1.0, b.d.data(), int(b.r), u.d.data(), int(u.r), 0.0, v.d.data(), int(b.r));
+        V.insert(U.lc[k], U.lc[k], std::move(v));
+    }
+    m2 = MPSTensor();
+    m2.phys = phys2; m2.left = Ut.left_basis(); m2.right = right; m2.pairing = RightPaired; m2.data = Ut;
+    m1 = MPSTensor();
+    m1.phys = phys1; m1.left = left; m1.right = V.right_basis(); m1.pairing = LeftPaired; m1.data = V;
 }
 
 BlockMatrix normalize_left(MPSTensor& t) {
@@ -429,7 +531,6 @@ DMRG::DMRG(std::vector<MPOTensor> mpo_single, int nup, int ndown, const DMRGPara
 
 void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc, int stop_step,
                  std::vector<uint8_t>* snap) {
-    (void)sweep_no;
     energies.clear();
     trunc.clear();
     for (int _site = 0; _site < 2 * L - 2; ++_site) {
@@ -484,8 +585,12 @@ void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<Trunca
         energies.push_back(E + p.ecore);
         TruncationResults tr;
         double t2 = now_s();
+        // alpha of this sweep (ts_optimize.hpp:275-282)
+        const double alpha = sweep_no < p.ngrowsweeps ? p.alpha_initial
+                             : (sweep_no < p.ngrowsweeps + p.nmainsweeps ? p.alpha_main : p.alpha_final);
         if (lr == 1) {
-            tst.split_l2r(p.Mmax, p.cutoff, mps[site1], mps[site2], tr);
+            if (p.heev) tst.predict_split_l2r(p.Mmax, p.cutoff, alpha, left_[site1], mpo[site1], mps[site1], mps[site2], tr);
+            else tst.split_l2r(p.Mmax, p.cutoff, mps[site1], mps[site2], tr);
             if (dbg) std::fprintf(stderr, "   split: |U|^2=%.12f |SV|^2=%.12f tw=%.3e\n", mps[site1].data.norm2(), mps[site2].data.norm2(), tr.truncated_weight);
             BlockMatrix t = normalize_left(mps[site2]);
             if (dbg) std::fprintf(stderr, "   qr: |Q|^2=%.12f |R|^2=%.12f\n", mps[site2].data.norm2(), t.norm2());
@@ -496,7 +601,8 @@ void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<Trunca
             left_[site2] = overlap_mpo_left_step(mps[site1], mps[site1], left_[site1], mpo[site1], true);
             boundary_time += now_s() - t3;
         } else {
-            tst.split_r2l(p.Mmax, p.cutoff, mps[site1], mps[site2], tr);
+            if (p.heev) tst.predict_split_r2l(p.Mmax, p.cutoff, alpha, right_[site2 + 1], mpo[site2], mps[site1], mps[site2], tr);
+            else tst.split_r2l(p.Mmax, p.cutoff, mps[site1], mps[site2], tr);
             BlockMatrix t = normalize_right(mps[site1]);
             if (site1 > 0) multiply_from_right(mps[site1 - 1], t);
             double t3 = now_s();

@@ -25,7 +25,20 @@ struct TwoSite {
     void set_from_mps(const MPSTensor& twin);        // reshape_right_to_both
     void split_l2r(std::size_t Mmax, double cutoff, MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const;
     void split_r2l(std::size_t Mmax, double cutoff, MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const;
+    // predict_split_l2r / _r2l (contractions/boundary_ops/prediction.hpp:152-236): the reduced
+    // density matrix plus alpha times the boundary noise term, truncated by heev_truncate;
+    // alpha = 0 falls back to the SVD split
+    void predict_split_l2r(std::size_t Mmax, double cutoff, double alpha, const Boundary& left, const MPOTensor& mpo,
+                           MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const;
+    void predict_split_r2l(std::size_t Mmax, double cutoff, double alpha, const Boundary& right, const MPOTensor& mpo,
+                           MPSTensor& m1, MPSTensor& m2, TruncationResults& tr) const;
 };
+
+// estimate_truncation (block_matrix_algorithms.h:136-183) on per-block descending values
+TruncationResults estimate_truncation(const std::vector<std::vector<double>>& vals, std::size_t Mmax, double cutoff,
+                                      std::vector<std::size_t>& keeps);
+// heev_truncate (block_matrix_algorithms.h:299-355): U = kept eigenvectors (descending), weight = fraction
+TruncationResults heev_truncate(const BlockMatrix& dm, BlockMatrix& U, double cutoff, std::size_t Mmax);
 
 // per-block SVD + estimate_truncation (block_matrix_algorithms.h:136-240)
 TruncationResults svd_truncate(const BlockMatrix& M, BlockMatrix& U, BlockMatrix& V, std::vector<std::vector<double>>& S,
@@ -48,6 +61,10 @@ struct DMRGParams {
     double jcd_tol = 1e-10;
     int jcd_maxiter = 8;
     double ecore = 0.0;
+    // twosite_truncation = heev and its noise (ts_optimize.hpp:275-296)
+    bool heev = false;
+    double alpha_initial = 1e-2, alpha_main = 1e-4, alpha_final = 1e-8;
+    int ngrowsweeps = 0, nmainsweeps = 0;
 };
 
 struct DMRG {

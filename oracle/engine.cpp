@@ -608,4 +608,94 @@ Boundary overlap_mpo_right_step(const MPSTensor& bra_in, const MPSTensor& ket_in
     return ret;
 }
 
+// move_boundary.hpp:37-89: schedule of the left step with bra = ket and no Hermitian
+// skip, then lbtm of every cohort into the dm block of its bra right sector
+void alpha_dm_direct(const MPSTensor& ket_in, const Boundary& left, const MPOTensor& mpo, BlockMatrix& dm, double alpha) {
+    MPSTensor ket = ket_in;
+    ket.make_right_paired();
+    const Index& physical_i = ket.phys;
+    const Index& left_i = ket.left;
+    Index right_i = ket.right, out_left_i = physical_i * left_i;
+    common_subset(out_left_i, right_i);
+    ProductBasis left_pb(physical_i, left_i);
+    ProductBasis right_pb(physical_i, right_i, true);
+    MPSTensor view = ket;  // lshtm_tasks reads the indices from the tensors
+    view.right = right_i;
+    Schedule tasks;
+    tasks.lr_ket_sizes = right_i.sizes();
+    tasks.blocks.resize(right_i.size());
+    for (unsigned rb = 0; rb < right_i.size(); ++rb) {
+        auto& blk = tasks.blocks[rb];
+        blk.lr_ket_sizes = &tasks.lr_ket_sizes;
+        blk.left_rt = blk.right_rt = &left.index;
+        blk.rb_ket = rb;
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int rb = 0; rb < int(right_i.size()); ++rb) {
+        lshtm_t_tasks(left.index, left_i, right_i, physical_i, right_pb, unsigned(rb), tasks.blocks[rb]);
+        lshtm_tasks(mpo, view, view, left.index, left_pb, right_pb, unsigned(rb), tasks.blocks[rb], false);
+    }
+    std::vector<const double*> kv = block_view(ket, ket.left, true);
+    std::vector<const double*> lv = boundary_view(left);
+    // per-cohort products in parallel, added to dm in (rb_ket, cohort) order
+    std::vector<std::vector<std::pair<std::size_t, std::vector<double>>>> part(right_i.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int rb = 0; rb < int(right_i.size()); ++rb) {
+        const MPSBlock& blk = tasks.blocks[rb];
+        if (blk.data.empty()) continue;
+        TList T = blk.create_T_left(lv, kv);
+        for (const Cohort& c : blk.data) {
+            std::size_t k = dm.find(right_i[c.lb].first, right_i[c.lb].first);
+            if (k == dm.n_blocks()) throw std::runtime_error("alpha_dm_direct: missing dm block");
+            std::vector<double> acc(dm.b[k].d.size(), 0.0);
+            c.lbtm(T, acc.data(), alpha);
+            part[rb].push_back({k, std::move(acc)});
+        }
+    }
+    for (auto& pr : part)
+        for (auto& e : pr) daxpy(e.second.size(), 1.0, e.second.data(), dm.b[e.first].d.data());
+}
+
+// move_boundary.hpp:91-145
+void alpha_dm_direct_right(const MPSTensor& ket_in, const Boundary& right, const MPOTensor& mpo, BlockMatrix& dm, double alpha) {
+    MPSTensor ket = ket_in;
+    ket.make_right_paired();
+    const Index& physical_i = ket.phys;
+    const Index& right_i = ket.right;
+    const Index& left_i = ket.left;
+    ProductBasis right_pb(physical_i, right_i, true);
+    Schedule tasks;
+    tasks.lr_ket_sizes = left_i.sizes();
+    tasks.blocks.resize(left_i.size());
+    for (unsigned lb = 0; lb < left_i.size(); ++lb) {
+        auto& blk = tasks.blocks[lb];
+        blk.lr_ket_sizes = &tasks.lr_ket_sizes;
+        blk.left_rt = blk.right_rt = &right.index;
+        blk.rb_ket = lb;
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int lb = 0; lb < int(left_i.size()); ++lb) {
+        rshtm_t_tasks(right.index, left_i, right_i, physical_i, right_pb, unsigned(lb), tasks.blocks[lb]);
+        rshtm_tasks(mpo, right.index, left_i, right_i, physical_i, right_pb, unsigned(lb), tasks.blocks[lb], false);
+    }
+    std::vector<const double*> kv = block_view(ket, ket.left, true);
+    std::vector<const double*> rv = boundary_view(right);
+    std::vector<std::vector<std::pair<std::size_t, std::vector<double>>>> part(left_i.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int lb = 0; lb < int(left_i.size()); ++lb) {
+        const MPSBlock& blk = tasks.blocks[lb];
+        if (blk.data.empty()) continue;
+        TList T = blk.create_T(rv, kv);
+        for (const Cohort& c : blk.data) {
+            std::size_t k = dm.find(left_i[c.rb].first, left_i[c.rb].first);
+            if (k == dm.n_blocks()) throw std::runtime_error("alpha_dm_direct_right: missing dm block");
+            std::vector<double> acc(dm.b[k].d.size(), 0.0);
+            c.rbtm(T, acc.data(), alpha);
+            part[lb].push_back({k, std::move(acc)});
+        }
+    }
+    for (auto& pr : part)
+        for (auto& e : pr) daxpy(e.second.size(), 1.0, e.second.data(), dm.b[e.first].d.data());
+}
+
 }  // namespace orc

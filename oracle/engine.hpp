@@ -97,4 +97,9 @@ Boundary overlap_mpo_left_step(const MPSTensor& bra, const MPSTensor& ket, const
 Boundary overlap_mpo_right_step(const MPSTensor& bra, const MPSTensor& ket, const Boundary& right, const MPOTensor& mpo,
                                 bool symmetric);
 
+// density-matrix noise (contractions/boundary_ops/move_boundary.hpp:37-145): dm[rb] += alpha S S^T
+// (left, blocks of dm keyed by the ket's right sectors) / dm[lb] += alpha S^T S (right)
+void alpha_dm_direct(const MPSTensor& ket, const Boundary& left, const MPOTensor& mpo, BlockMatrix& dm, double alpha);
+void alpha_dm_direct_right(const MPSTensor& ket, const Boundary& right, const MPOTensor& mpo, BlockMatrix& dm, double alpha);
+
 }  // namespace orc

@@ -48,6 +48,7 @@ def lib(nthreads: int = 0):
                                       c_double, P(c_void_p)]
         L.orc_dmrg_free.argtypes = [c_void_p]
         L.orc_dmrg_set_mmax.argtypes = [c_void_p, c_size_t]
+        L.orc_dmrg_set_heev.argtypes = [c_void_p, c_int, c_double, c_double, c_double, c_int, c_int]
         L.orc_dmrg_sweep.argtypes = [c_void_p, c_int, P(c_double), P(c_double), P(c_double), P(ctypes.c_uint64), c_int,
                                      P(c_void_p), P(c_size_t)]
         L.orc_dmrg_stats.argtypes = [c_void_p, P(c_double)]
@@ -118,6 +119,12 @@ class OracleDMRG:
         b = ctypes.string_at(p, n.value)
         self.lib.orc_free(p)
         return b
+
+    def set_heev(self, heev: bool = True, alpha_initial: float = 1e-2, alpha_main: float = 1e-4,
+                 alpha_final: float = 1e-8, ngrowsweeps: int = 0, nmainsweeps: int = 0):
+        """twosite_truncation = heev (density matrix with noise) instead of svd."""
+        self.lib.orc_dmrg_set_heev(self.h, 1 if heev else 0, alpha_initial, alpha_main, alpha_final, ngrowsweeps,
+                                   nmainsweeps)
 
     def set_mmax(self, M: int):
         self.lib.orc_dmrg_set_mmax(self.h, M)

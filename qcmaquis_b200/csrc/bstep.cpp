@@ -285,9 +285,25 @@ std::unique_ptr<DevBoundary> finish_boundary(BoundaryIndexH& idx, cudaStream_t s
 
 }  // namespace
 
+namespace {
+// GEMM jobs that add into shared target blocks, run in rounds (round r = the r-th job of every
+// target) so that each block is summed in job order
+void run_accumulating(const std::vector<GemmJob>& jobs, const std::vector<std::size_t>& target, const double* A, uint64_t a_len,
+                      const double* B, uint64_t b_len, double* C, uint64_t c_len, Ctx& c) {
+    std::unordered_map<std::size_t, std::size_t> seen;
+    std::vector<std::vector<GemmJob>> rounds;
+    for (std::size_t i = 0; i < jobs.size(); ++i) {
+        const std::size_t r = seen[target[i]]++;
+        if (rounds.size() <= r) rounds.resize(r + 1);
+        rounds[r].push_back(jobs[i]);
+    }
+    for (auto& r : rounds) batched_gemm(r, A, a_len, B, b_len, C, c_len, c.gjobs, c.gtiles, c.s);
+}
+}  // namespace
+
 // ---------------------------------------------------------------------------
-std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold, const DMPS& ket, const MPOTensor& W,
-                                                 bool symmetric) {
+static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, const DMPS& ket, const MPOTensor& W,
+                                               bool symmetric, DensityNoise* dn) {
     if (!ket.right_paired) throw std::runtime_error("boundary_step_right: ket must be right-paired");
     const double tb0 = step_now();
     const BoundaryIndexH& R = Rold.idx;
@@ -441,19 +457,22 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
         s_len += P.s_len;
         P = BPart();
     }
-    if (symmetric) complement_transpose(nidx, W.herm_left, W.phase_left, false);
-    auto Rn = finish_boundary(nidx, c.s);
-    // prop_r: new_R[b] (ls_ket x ls_bra) = S_b * bra^T for all b of a cohort in one job
-    // (rows b-major in S; C row blocks = the cohort's MPO-index blocks)
+    std::unique_ptr<DevBoundary> Rn;
     std::vector<GemmJob> prop;
-    for (const Pend& pd : pend) {
-        const uint32_t ls = uint32_t(left[pd.lb_ket].second), lsb = uint32_t(left[pd.lb_bra].second);
-        GemmJob g{};
-        g.a_off = pd.s_off; g.lda = pd.nS * ls;
-        g.b_off = koff[pd.lb_bra]; g.ldb = lsb; g.tb = 1;
-        g.c_off = Rn->idx.data_off[pd.ci_new]; g.ldc = ls; g.crb = ls; g.c_bs = uint64_t(ls) * lsb;
-        g.M = pd.nS * ls; g.N = lsb; g.K = kcols[pd.lb_bra]; g.alpha = 1.0; g.beta = 0.0;
-        prop.push_back(g);
+    if (!dn) {
+        if (symmetric) complement_transpose(nidx, W.herm_left, W.phase_left, false);
+        Rn = finish_boundary(nidx, c.s);
+        // prop_r: new_R[b] (ls_ket x ls_bra) = S_b * bra^T for all b of a cohort in one job
+        // (rows b-major in S; C row blocks = the cohort's MPO-index blocks)
+        for (const Pend& pd : pend) {
+            const uint32_t ls = uint32_t(left[pd.lb_ket].second), lsb = uint32_t(left[pd.lb_bra].second);
+            GemmJob g{};
+            g.a_off = pd.s_off; g.lda = pd.nS * ls;
+            g.b_off = koff[pd.lb_bra]; g.ldb = lsb; g.tb = 1;
+            g.c_off = Rn->idx.data_off[pd.ci_new]; g.ldc = ls; g.crb = ls; g.c_bs = uint64_t(ls) * lsb;
+            g.M = pd.nS * ls; g.N = lsb; g.K = kcols[pd.lb_bra]; g.alpha = 1.0; g.beta = 0.0;
+            prop.push_back(g);
+        }
     }
     const double tb1 = step_now();
     // execute
@@ -470,15 +489,45 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold
     fill_coefficients(sb.d_units.get(), uint32_t(sb.units.size()), sb.d_sptr.get(), sb.d_went.get(), c.W.get(), sb.w_len, c.s);
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
               c.T.get(), c.S.get(), c.s);
-    // A = S scratch, B = ket data, C = new boundary: three different base pointers
-    batched_gemm(prop, c.S.get(), s_len, ket.b.d.get(), ket.b.total, Rn->data.get(), Rn->idx.total, c.gjobs, c.gtiles, c.s);
+    if (!dn) {
+        // A = S scratch, B = ket data, C = new boundary: three different base pointers
+        batched_gemm(prop, c.S.get(), s_len, ket.b.d.get(), ket.b.total, Rn->data.get(), Rn->idx.total, c.gjobs, c.gtiles, c.s);
+    } else {
+        // rbtm (tasks.cpp:364-380): dm[lb_bra] += alpha S^T S, S = (nS*ls_ket) x stripe
+        std::vector<GemmJob> acc;
+        std::vector<std::size_t> tgt;
+        for (const Pend& pd : pend) {
+            const std::size_t k = dn->dm->find_l(left[pd.lb_bra].first);
+            if (k == dn->dm->n()) throw std::runtime_error("rbtm: missing density-matrix block");
+            const uint32_t K = pd.nS * uint32_t(left[pd.lb_ket].second), st = kcols[pd.lb_bra];
+            if (dn->dm->rows[k] != st || dn->dm->cols[k] != st) throw std::runtime_error("rbtm: density-matrix block shape");
+            GemmJob g{};
+            g.a_off = pd.s_off; g.ta = 1; g.lda = K;
+            g.b_off = pd.s_off; g.ldb = K;
+            g.c_off = dn->dm->off[k]; g.ldc = st;
+            g.M = st; g.N = st; g.K = K; g.alpha = dn->alpha; g.beta = 1.0;
+            acc.push_back(g);
+            tgt.push_back(k);
+        }
+        run_accumulating(acc, tgt, c.S.get(), s_len, c.S.get(), s_len, dn->dm->d.get(), dn->dm->total, c);
+    }
     step_report("right", tb0, tbp, tb1, c.s);
     return Rn;
 }
 
+std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold, const DMPS& ket, const MPOTensor& W,
+                                                 bool symmetric) {
+    return step_right(c, Rold, ket, W, symmetric, nullptr);
+}
+
+void rbtm_accumulate(Ctx& c, const DevBoundary& R, const DMPS& ket_rp, const MPOTensor& W, DBlocks& dm, double alpha) {
+    DensityNoise dn{&dm, alpha};
+    step_right(c, R, ket_rp, W, false, &dn);
+}
+
 // ---------------------------------------------------------------------------
-std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold, const DMPS& ket, const DMPS& bra,
-                                                const MPOTensor& W, bool symmetric) {
+static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, const DMPS& ket, const DMPS& bra,
+                                              const MPOTensor& W, bool symmetric, DensityNoise* dn) {
     if (!ket.right_paired || bra.right_paired) throw std::runtime_error("boundary_step_left: ket right-paired, bra left-paired");
     const double tb0 = step_now();
     const BoundaryIndexH& L = Lold.idx;
@@ -636,18 +685,21 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
         s_len += P.s_len;
         P = BPart();
     }
-    if (symmetric) complement_transpose(nidx, W.herm_right, W.phase_right, true);
-    auto Ln = finish_boundary(nidx, c.s);
-    // prop_l: L_new (rs_bra x nS*rs_ket) = bra^T * S
+    std::unique_ptr<DevBoundary> Ln;
     std::vector<GemmJob> prop;
-    for (const Pend& pd : pend) {
-        GemmJob g{};
-        g.a_off = boff[pd.rb_bra]; g.ta = 1; g.lda = brows[pd.rb_bra];
-        g.b_off = pd.s_off; g.ldb = brows[pd.rb_bra];
-        g.c_off = Ln->idx.data_off[pd.ci_new]; g.ldc = uint32_t(right[pd.rb_bra].second);
-        g.M = uint32_t(right[pd.rb_bra].second); g.N = pd.nS * pd.rs_ket; g.K = brows[pd.rb_bra];
-        g.alpha = 1.0; g.beta = 0.0;
-        prop.push_back(g);
+    if (!dn) {
+        if (symmetric) complement_transpose(nidx, W.herm_right, W.phase_right, true);
+        Ln = finish_boundary(nidx, c.s);
+        // prop_l: L_new (rs_bra x nS*rs_ket) = bra^T * S
+        for (const Pend& pd : pend) {
+            GemmJob g{};
+            g.a_off = boff[pd.rb_bra]; g.ta = 1; g.lda = brows[pd.rb_bra];
+            g.b_off = pd.s_off; g.ldb = brows[pd.rb_bra];
+            g.c_off = Ln->idx.data_off[pd.ci_new]; g.ldc = uint32_t(right[pd.rb_bra].second);
+            g.M = uint32_t(right[pd.rb_bra].second); g.N = pd.nS * pd.rs_ket; g.K = brows[pd.rb_bra];
+            g.alpha = 1.0; g.beta = 0.0;
+            prop.push_back(g);
+        }
     }
     const double tb1 = step_now();
     Ctx::ensure(c.T, t_len ? t_len : 1);
@@ -660,9 +712,40 @@ std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold,
     fill_coefficients(sb.d_units.get(), uint32_t(sb.units.size()), sb.d_sptr.get(), sb.d_went.get(), c.W.get(), sb.w_len, c.s);
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
               c.T.get(), c.S.get(), c.s);
-    batched_gemm(prop, bra.b.d.get(), bra.b.total, c.S.get(), s_len, Ln->data.get(), Ln->idx.total, c.gjobs, c.gtiles, c.s);
+    if (!dn) {
+        batched_gemm(prop, bra.b.d.get(), bra.b.total, c.S.get(), s_len, Ln->data.get(), Ln->idx.total, c.gjobs, c.gtiles, c.s);
+    } else {
+        // lbtm (tasks.cpp:346-362): dm[rb_bra] += alpha S S^T, S = stripe x (nS*rs_ket)
+        std::vector<GemmJob> acc;
+        std::vector<std::size_t> tgt;
+        for (const Pend& pd : pend) {
+            const std::size_t k = dn->dm->find_r(right[pd.rb_bra].first);
+            if (k == dn->dm->n()) throw std::runtime_error("lbtm: missing density-matrix block");
+            const uint32_t st = brows[pd.rb_bra], K = pd.nS * pd.rs_ket;
+            if (dn->dm->rows[k] != st || dn->dm->cols[k] != st) throw std::runtime_error("lbtm: density-matrix block shape");
+            GemmJob g{};
+            g.a_off = pd.s_off; g.lda = st;
+            g.b_off = pd.s_off; g.tb = 1; g.ldb = st;
+            g.c_off = dn->dm->off[k]; g.ldc = st;
+            g.M = st; g.N = st; g.K = K; g.alpha = dn->alpha; g.beta = 1.0;
+            acc.push_back(g);
+            tgt.push_back(k);
+        }
+        run_accumulating(acc, tgt, c.S.get(), s_len, c.S.get(), s_len, dn->dm->d.get(), dn->dm->total, c);
+    }
     step_report("left", tb0, tbp, tb1, c.s);
     return Ln;
+}
+
+std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold, const DMPS& ket, const DMPS& bra,
+                                                const MPOTensor& W, bool symmetric) {
+    return step_left(c, Lold, ket, bra, W, symmetric, nullptr);
+}
+
+void lbtm_accumulate(Ctx& c, const DevBoundary& L, const DMPS& ket_rp, const DMPS& bra_lp, const MPOTensor& W, DBlocks& dm,
+                     double alpha) {
+    DensityNoise dn{&dm, alpha};
+    step_left(c, L, ket_rp, bra_lp, W, false, &dn);
 }
 
 }  // namespace qcm

@@ -192,6 +192,8 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     const qcm::MPO& m = qcm::mpo_of(mpo);
     if (m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: expected a single-site MPO");
     if (prm->jcd_maxiter < 1 || prm->jcd_maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: jcd_maxiter must be in 1..64");
+    if (prm->twosite_truncation != 0 && prm->twosite_truncation != 1)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: twosite_truncation must be 0 (svd) or 1 (heev)");
     if (prm->max_bond_dimension < 1 || prm->init_bond_dimension < 1)
         return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: bond dimensions must be positive");
     QCM_CUDA(cudaSetDevice(ctx->device));
@@ -203,6 +205,12 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     p.jcd_tol = prm->jcd_tol;
     p.jcd_maxiter = prm->jcd_maxiter;
     p.ecore = prm->ecore;
+    p.heev = prm->twosite_truncation == 1;
+    p.alpha_initial = prm->alpha_initial;
+    p.alpha_main = prm->alpha_main;
+    p.alpha_final = prm->alpha_final;
+    p.ngrowsweeps = prm->ngrowsweeps;
+    p.nmainsweeps = prm->nmainsweeps;
     qcm::MPO ts = qcm::make_twosite_mpo(m);
     auto d = std::make_unique<qcm_dmrg>();
     d->ctx = ctx;
@@ -228,6 +236,12 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     p.jcd_tol = prm->jcd_tol;
     p.jcd_maxiter = prm->jcd_maxiter;
     p.ecore = prm->ecore;
+    p.heev = prm->twosite_truncation == 1;
+    p.alpha_initial = prm->alpha_initial;
+    p.alpha_main = prm->alpha_main;
+    p.alpha_final = prm->alpha_final;
+    p.ngrowsweeps = prm->ngrowsweeps;
+    p.nmainsweeps = prm->nmainsweeps;
     qcm::Ctx tmp;
     tmp.s = ctx->stream;
     std::vector<qcm::DMPS> ms;

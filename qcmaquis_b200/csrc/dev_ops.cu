@@ -76,7 +76,7 @@ __global__ void k_bcopy(const CopyJob* __restrict__ jobs, uint32_t njobs, const 
     const uint64_t n = uint64_t(J.rows) * J.cols;
     for (uint64_t e = threadIdx.x; e < n; e += blockDim.x) {
         uint32_t j = uint32_t(e / J.rows), i = uint32_t(e - uint64_t(j) * J.rows);
-        double v = src[J.src_off + i + uint64_t(j) * J.src_ld];
+        double v = src[J.src_off + i + uint64_t(J.rev ? J.cols - 1 - j : j) * J.src_ld];
         if (!J.trans) dst[J.dst_off + i + uint64_t(j) * J.dst_ld] = v;
         else dst[J.dst_off + j + uint64_t(i) * J.dst_ld] = v;
     }

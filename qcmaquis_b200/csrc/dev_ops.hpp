@@ -27,10 +27,11 @@ struct GemmJob {
 };
 
 // dst[dst_off + i + j*dst_ld] = src[src_off + i + j*src_ld] (i < rows, j < cols);
-// with trans: dst[dst_off + j + i*dst_ld] = src[...] (transposed copy)
+// with trans: dst[dst_off + j + i*dst_ld] = src[...] (transposed copy);
+// with rev: source column j is read from column cols - 1 - j (reversed column order)
 struct CopyJob {
     uint64_t src_off, dst_off;
-    uint32_t rows, cols, src_ld, dst_ld, trans, pad;
+    uint32_t rows, cols, src_ld, dst_ld, trans, rev;
 };
 
 // Runs a list of GEMM jobs (all operands addressed from the three base pointers, whose

@@ -79,6 +79,34 @@ DMPS reshaped_right(Ctx& c, const DMPS& t) {
     return o;
 }
 
+// estimate_truncation (block_matrix_algorithms.h:136-183) on per-block values in descending order
+TruncResults estimate_cut(const std::vector<std::vector<double>>& vals, uint64_t Mmax, double cutoff,
+                          std::vector<uint32_t>& keep) {
+    std::vector<double> all;
+    for (auto& v : vals) all.insert(all.end(), v.begin(), v.end());
+    std::sort(all.begin(), all.end(), std::greater<double>());
+    TruncResults tr;
+    if (all.empty() || all[0] == 0.0) throw std::runtime_error("truncation: two-site tensor is zero");
+    double evalscut = cutoff * all[0];
+    if (all.size() > Mmax) evalscut = std::max(evalscut, all[Mmax]);
+    tr.smallest_ev = evalscut / all[0];
+    double tf = 0, tw = 0, sum = 0, sum2 = 0;
+    for (double x : all) {
+        sum += x; sum2 += x * x;
+        if (x < evalscut) { tf += x; tw += x * x; }
+    }
+    tr.truncated_fraction = tf / sum;
+    tr.truncated_weight = tw / sum2;
+    keep.assign(vals.size(), 0);
+    for (std::size_t k = 0; k < vals.size(); ++k) {
+        uint32_t n = 0;
+        while (n < vals[k].size() && !(vals[k][n] < evalscut)) ++n;
+        keep[k] = n;
+        tr.bond_dimension += n;
+    }
+    return tr;
+}
+
 Index sorted_basis(const std::vector<std::pair<Charge, std::size_t>>& v) {
     Index r;
     r.d = v;
@@ -378,28 +406,10 @@ TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMP
     if (sl) QCM_CUDA(cudaMemcpyAsync(hs.data(), S.get(), sl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
     QCM_CUDA(cudaStreamSynchronize(c.s));
 
-    // estimate_truncation (block_matrix_algorithms.h:136-183)
-    std::vector<double> all(hs);
-    std::sort(all.begin(), all.end(), std::greater<double>());
-    TruncResults tr;
-    if (all.empty() || all[0] == 0.0) throw std::runtime_error("truncation: two-site tensor is zero");
-    double evalscut = cutoff * all[0];
-    if (all.size() > Mmax) evalscut = std::max(evalscut, all[Mmax]);
-    tr.smallest_ev = evalscut / all[0];
-    double tf = 0, tw = 0, sum = 0, sum2 = 0;
-    for (double x : all) {
-        sum += x; sum2 += x * x;
-        if (x < evalscut) { tf += x; tw += x * x; }
-    }
-    tr.truncated_fraction = tf / sum;
-    tr.truncated_weight = tw / sum2;
-    std::vector<uint32_t> keep(nb, 0);
-    for (std::size_t k = 0; k < nb; ++k) {
-        uint32_t n = 0;
-        while (n < kk[k] && !(hs[so[k] + n] < evalscut)) ++n;
-        keep[k] = n;
-        tr.bond_dimension += n;
-    }
+    std::vector<std::vector<double>> vals(nb);
+    for (std::size_t k = 0; k < nb; ++k) vals[k].assign(hs.begin() + so[k], hs.begin() + so[k] + kk[k]);
+    std::vector<uint32_t> keep;
+    TruncResults tr = estimate_cut(vals, Mmax, cutoff, keep);
 
     // U[:, :keep] and V^T[:keep, :], with S multiplied into V^T (l2r) or U (r2l)
     m1 = DMPS(); m2 = DMPS();
@@ -434,6 +444,142 @@ TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMP
         ++i;
     }
     QCM_CUDA(cudaStreamSynchronize(c.s));  // U, S, V are released on return
+    return tr;
+}
+
+// ---------------------------------------------------------------------------
+// predict_split_l2r / _r2l (contractions/boundary_ops/prediction.hpp:152-236) with
+// heev_truncate (block_matrix_algorithms.h:299-355)
+TruncResults DTwoSite::predict_split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, double alpha, const DevBoundary& B,
+                                     const MPOTensor& W, DMPS& m1, DMPS& m2) {
+    if (alpha == 0.0) return split(c, l2r, Mmax, cutoff, m1, m2);
+    const std::size_t nb = both.n();
+    // reduced density matrix: both both^T (l2r, rows x rows) or both^T both (r2l, cols x cols)
+    DBlocks dm;
+    std::vector<GemmJob> jobs;
+    for (std::size_t k = 0; k < nb; ++k) {
+        const uint32_t m = both.rows[k], n = both.cols[k], d = l2r ? m : n;
+        dm.add(both.lc[k], both.lc[k], d, d);
+        GemmJob g{};
+        g.a_off = both.off[k]; g.lda = m; g.b_off = both.off[k]; g.ldb = m;
+        if (l2r) { g.tb = 1; g.M = m; g.N = m; g.K = n; }
+        else { g.ta = 1; g.M = n; g.N = n; g.K = m; }
+        g.c_off = dm.off.back(); g.ldc = d; g.alpha = 1.0; g.beta = 0.0;
+        jobs.push_back(g);
+    }
+    dm.allocate(c.s, true);
+    batched_gemm(jobs, both.d.get(), both.total, both.d.get(), both.total, dm.d.get(), dm.total, c.gjobs, c.gtiles, c.s);
+    // noise term on the both-paired data seen as a site tensor of the boundary step
+    {
+        DMPS tmp;
+        std::vector<std::pair<Charge, std::size_t>> fused;
+        for (std::size_t k = 0; k < nb; ++k) fused.push_back({both.lc[k], l2r ? both.cols[k] : both.rows[k]});
+        if (l2r) { tmp.phys = phys1; tmp.left = left; tmp.right = sorted_basis(fused); tmp.right_paired = false; }
+        else { tmp.phys = phys2; tmp.left = sorted_basis(fused); tmp.right = right; tmp.right_paired = true; }
+        tmp.b.lc = both.lc; tmp.b.rc = both.rc; tmp.b.rows = both.rows; tmp.b.cols = both.cols; tmp.b.off = both.off;
+        tmp.b.total = both.total;
+        tmp.b.allocate(c.s, false);
+        QCM_CUDA(cudaMemcpyAsync(tmp.b.d.get(), both.d.get(), std::max<uint64_t>(both.total, 1) * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, c.s));
+        if (l2r) {
+            DMPS ket = right_paired_copy(c, tmp);
+            lbtm_accumulate(c, B, ket, tmp, W, dm, alpha);
+        } else {
+            rbtm_accumulate(c, B, tmp, W, dm, alpha);
+        }
+    }
+    // heev per block (lanes, one host thread each), eigenvalues ascending on the device
+    std::vector<uint64_t> wo(nb);
+    uint64_t wl = 0;
+    for (std::size_t k = 0; k < nb; ++k) { wo[k] = wl; wl += dm.rows[k]; }
+    DBuf<double> Wv(std::max<uint64_t>(wl, 1));
+    int* info = c.sv->reserve_info(uint32_t(nb), c.s);
+    std::vector<std::size_t> order(nb);
+    for (std::size_t k = 0; k < nb; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](std::size_t x, std::size_t y) { return dm.rows[x] > dm.rows[y]; });
+    c.sv->fork(c.s);
+    std::string err;
+#pragma omp parallel for num_threads(Solver::LANES) schedule(static, 1)
+    for (int lane = 0; lane < Solver::LANES; ++lane) {
+        try {
+            QCM_CUDA(cudaSetDevice(c.device));
+            for (std::size_t i = std::size_t(lane); i < nb; i += Solver::LANES) {
+                const std::size_t k = order[i];
+                syevd_lane(*c.sv, lane, dm.d.get() + dm.off[k], int(dm.rows[k]), Wv.get() + wo[k], info + k);
+            }
+        } catch (const std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
+    c.sv->join(c.s);
+    c.sv->check(c.s);
+    std::vector<double> hw(wl);
+    if (wl) QCM_CUDA(cudaMemcpyAsync(hw.data(), Wv.get(), wl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    // descending order; the cut is on sqrt of the positive eigenvalues (others kept as they are)
+    std::vector<std::vector<double>> vals(nb);
+    for (std::size_t k = 0; k < nb; ++k) {
+        vals[k].resize(dm.rows[k]);
+        for (uint32_t i = 0; i < dm.rows[k]; ++i) {
+            const double x = hw[wo[k] + dm.rows[k] - 1 - i];
+            vals[k][i] = x > 0.0 ? std::sqrt(x) : x;
+        }
+    }
+    std::vector<uint32_t> keep;
+    TruncResults tr = estimate_cut(vals, Mmax, cutoff, keep);
+    tr.truncated_weight = tr.truncated_fraction;  // heev_truncate reports the fraction in both fields
+    // U = kept eigenvectors, descending (columns n-1, n-2, ...)
+    m1 = DMPS(); m2 = DMPS();
+    m1.phys = phys1; m1.left = left; m1.right_paired = false;
+    m2.phys = phys2; m2.right = right; m2.right_paired = true;
+    std::vector<std::pair<Charge, std::size_t>> mid;
+    for (std::size_t k = 0; k < nb; ++k) {
+        if (!keep[k]) continue;
+        mid.push_back({both.lc[k], keep[k]});
+        m1.b.add(both.lc[k], both.lc[k], both.rows[k], keep[k]);
+        m2.b.add(both.lc[k], both.lc[k], keep[k], both.cols[k]);
+    }
+    m1.right = sorted_basis(mid);
+    m2.left = m1.right;
+    m1.b.allocate(c.s, true);
+    m2.b.allocate(c.s, true);
+    std::vector<CopyJob> cj;
+    std::vector<GemmJob> gj;
+    std::size_t i = 0;
+    for (std::size_t k = 0; k < nb; ++k) {
+        if (!keep[k]) continue;
+        const uint32_t n = dm.rows[k], kp = keep[k], rows = both.rows[k], cols = both.cols[k];
+        const uint64_t src = dm.off[k] + uint64_t(n - kp) * n;  // last kp eigenvectors, read in reverse
+        GemmJob g{};
+        if (l2r) {
+            // site 1 = U (rows x kp); site 2 = U^T both (kp x cols)
+            cj.push_back(CopyJob{src, m1.b.off[i], n, kp, n, rows, 0, 1});
+            g.a_off = m1.b.off[i]; g.ta = 1; g.lda = rows;
+            g.b_off = both.off[k]; g.ldb = rows;
+            g.c_off = m2.b.off[i]; g.ldc = kp;
+            g.M = kp; g.N = cols; g.K = rows;
+        } else {
+            // site 2 = U^T (kp x cols); site 1 = both U = both (site 2)^T (rows x kp)
+            cj.push_back(CopyJob{src, m2.b.off[i], n, kp, n, kp, 1, 1});
+            g.a_off = both.off[k]; g.lda = rows;
+            g.b_off = m2.b.off[i]; g.tb = 1; g.ldb = kp;
+            g.c_off = m1.b.off[i]; g.ldc = rows;
+            g.M = rows; g.N = kp; g.K = cols;
+        }
+        g.alpha = 1.0; g.beta = 0.0;
+        gj.push_back(g);
+        ++i;
+    }
+    if (l2r) {
+        batched_copy(cj, dm.d.get(), dm.total, m1.b.d.get(), m1.b.total, c.cjobs, c.s);
+        batched_gemm(gj, m1.b.d.get(), m1.b.total, both.d.get(), both.total, m2.b.d.get(), m2.b.total, c.gjobs, c.gtiles, c.s);
+    } else {
+        batched_copy(cj, dm.d.get(), dm.total, m2.b.d.get(), m2.b.total, c.cjobs, c.s);
+        batched_gemm(gj, both.d.get(), both.total, m2.b.d.get(), m2.b.total, m1.b.d.get(), m1.b.total, c.gjobs, c.gtiles, c.s);
+    }
+    QCM_CUDA(cudaStreamSynchronize(c.s));
     return tr;
 }
 

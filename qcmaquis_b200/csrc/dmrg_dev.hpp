@@ -125,6 +125,11 @@ struct DTwoSite {
     void twin_to_both(Ctx& c);  // reshape_right_to_both
     // split_mps_l2r / split_mps_r2l with svd_truncate (block_matrix_algorithms.h:136-240)
     TruncResults split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMPS& m1, DMPS& m2);
+    // predict_split_l2r / _r2l (contractions/boundary_ops/prediction.hpp:152-236): reduced density
+    // matrix plus alpha times the boundary noise (B = L[site1] with W = mpo[site1] for l2r,
+    // R[site2+1] with mpo[site2] for r2l), truncated by heev; alpha = 0 is the SVD split
+    TruncResults predict_split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, double alpha, const DevBoundary& B,
+                               const MPOTensor& W, DMPS& m1, DMPS& m2);
 };
 
 // Jacobi-Davidson for the lowest eigenpair (ietl/jacobi.h:386-474 with gmres 0):
@@ -141,6 +146,17 @@ std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& R, c
 // trivial boundary: one cohort per sector, aux_dim blocks of ones (boundary.h / optimize.h:158-195)
 std::unique_ptr<DevBoundary> trivial_boundary(const Index& idx, uint32_t aux_dim, cudaStream_t s);
 
+// Density-matrix noise of the heev truncation (contractions/boundary_ops/move_boundary.hpp:37-145):
+// the boundary step's S build without Hermitian skipping, then dm[k] += alpha S S^T (lbtm, dm keyed
+// by the ket's right sectors) or alpha S^T S (rbtm, keyed by its left sectors), summed in cohort order.
+struct DensityNoise {
+    DBlocks* dm;
+    double alpha;
+};
+void lbtm_accumulate(Ctx& c, const DevBoundary& L, const DMPS& ket_rp, const DMPS& bra_lp, const MPOTensor& W, DBlocks& dm,
+                     double alpha);
+void rbtm_accumulate(Ctx& c, const DevBoundary& R, const DMPS& ket_rp, const MPOTensor& W, DBlocks& dm, double alpha);
+
 // complement_transpose of a boundary index (boundary.h:150-179; abelian conjugate correction 1)
 void complement_transpose(BoundaryIndexH& x, const std::vector<int32_t>& herm, const std::vector<int32_t>& phase, bool forward);
 
@@ -152,6 +168,10 @@ struct DMRGParams {
     double jcd_tol = 1e-10;
     int jcd_maxiter = 8;
     double ecore = 0.0;
+    // twosite_truncation = heev with its noise per sweep (ts_optimize.hpp:275-296)
+    bool heev = false;
+    double alpha_initial = 1e-2, alpha_main = 1e-4, alpha_final = 1e-8;
+    int ngrowsweeps = 0, nmainsweeps = 0;
 };
 
 struct DMRGStats {
@@ -175,6 +195,7 @@ struct DevDMRG {
     DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, std::vector<DMPS> sites,
             const DMRGParams& prm, cudaStream_t s);
     int next_step = 0;  // step index (0 .. 2L-3) the sweep continues with
+    int sweep_count = 0;  // completed sweeps
     void sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc);
     // run the current sweep up to (not including) step `stop`; appends energies / truncations
     void run_until(int stop, std::vector<double>& energies, std::vector<TruncResults>& trunc);

@@ -172,6 +172,16 @@ void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, 
                                  info, L.svdp));
 }
 
+void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info) {
+    if (n == 0) return;
+    Solver::Lane& L = sv.lane[l];
+    AllocStream scope(L.s);
+    int lwork = 0;
+    QCM_SOLVER(cusolverDnDsyevd_bufferSize(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, W, &lwork));
+    if (L.work.size() < std::size_t(lwork)) L.work.alloc(std::size_t(lwork));
+    QCM_SOLVER(cusolverDnDsyevd(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, W, L.work.get(), lwork, info));
+}
+
 namespace {
 // Householder QR of a (m x n, ld m) in place; leaves R in the upper triangle and Q's reflectors below
 void geqrf_orgqr(Solver& sv, cudaStream_t s, int m, int n, double* Rout, uint32_t ldr, int rmode, uint32_t rrows,

@@ -54,6 +54,10 @@ void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double*
 // the same on side lane `l` (between fork and join), status to *info; lanes may be driven
 // from different host threads (one thread per lane: the Jacobi SVD blocks its caller)
 void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, double* S, double* V, int* info);
+// Symmetric eigendecomposition (divide and conquer, lower triangle) on lane `l`: A (n x n, ld n)
+// is overwritten by the eigenvectors, W receives the eigenvalues in ascending order.
+// Replaces heevd('V') of alps/matrix/algorithms.hpp:374-396 (which then reverses the order).
+void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info);
 // Q (m x k, ld m), R (k x n, ld k, upper trapezoidal): A = Q R
 void qr_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* Q, double* R);
 // L (m x k, ld m, lower trapezoidal), Q (k x n, ld k): A = L Q

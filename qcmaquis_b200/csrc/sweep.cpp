@@ -285,8 +285,11 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     mark(3);
     energy = E + p.ecore;
     double t3_last = 0;
+    const double alpha = sweep_count < p.ngrowsweeps ? p.alpha_initial
+                         : (sweep_count < p.ngrowsweeps + p.nmainsweeps ? p.alpha_main : p.alpha_final);
     if (lr == 1) {
-        tr = tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+        tr = p.heev ? tst.predict_split(c, true, p.Mmax, p.cutoff, alpha, *left_[site1], mpo[site1], mps[site1], mps[site2])
+                    : tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
         mark(4);
         DBlocks t = normalize_left(c, mps[site2]);
         if (site2 < L - 1) multiply_from_left(c, mps[site2 + 1], t);
@@ -299,7 +302,8 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         QCM_CUDA(cudaStreamSynchronize(c.s));
         st.boundary_s += now_s() - t3;
     } else {
-        tr = tst.split(c, false, p.Mmax, p.cutoff, mps[site1], mps[site2]);
+        tr = p.heev ? tst.predict_split(c, false, p.Mmax, p.cutoff, alpha, *right_[site2 + 1], mpo[site2], mps[site1], mps[site2])
+                    : tst.split(c, false, p.Mmax, p.cutoff, mps[site1], mps[site2]);
         mark(4);
         DBlocks t = normalize_right(c, mps[site1]);
         if (site1 > 0) multiply_from_right(c, mps[site1 - 1], t);
@@ -330,7 +334,7 @@ void DevDMRG::run_until(int stop, std::vector<double>& energies, std::vector<Tru
         energies.push_back(E);
         trunc.push_back(tr);
     }
-    if (next_step == 2 * L - 2) next_step = 0;
+    if (next_step == 2 * L - 2) { next_step = 0; ++sweep_count; }
     st.total_s += now_s() - t_start;
 }
 

@@ -18,7 +18,17 @@ from .heff import Boundary, HeffPlan, MPSDesc, _sectors
 
 class DMRGParams(ctypes.Structure):
     _fields_ = [("max_bond_dimension", c_uint64), ("init_bond_dimension", c_uint64), ("truncation_cutoff", c_double),
-                ("jcd_tol", c_double), ("jcd_maxiter", ctypes.c_int32), ("ecore", c_double)]
+                ("jcd_tol", c_double), ("jcd_maxiter", ctypes.c_int32), ("ecore", c_double),
+                ("twosite_truncation", ctypes.c_int32), ("alpha_initial", c_double), ("alpha_main", c_double),
+                ("alpha_final", c_double), ("ngrowsweeps", ctypes.c_int32), ("nmainsweeps", ctypes.c_int32)]
+
+
+def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev):
+    """heev: None (svd truncation) or dict(alpha_initial, alpha_main, alpha_final, ngrowsweeps, nmainsweeps)."""
+    h = heev or {}
+    return DMRGParams(M, init_bd, cutoff, tol, maxiter, ecore, 1 if heev else 0, h.get("alpha_initial", 1e-2),
+                      h.get("alpha_main", 1e-4), h.get("alpha_final", 1e-8), h.get("ngrowsweeps", 0),
+                      h.get("nmainsweeps", 0))
 
 
 class TruncResult(ctypes.Structure):
@@ -82,10 +92,11 @@ class DMRG:
     """Two-site ground-state DMRG (TwoU1, init_state = const) with every step on the device."""
 
     def __init__(self, ctx, mpo, nup: int, ndown: int, max_bond_dimension: int, init_bond_dimension: int | None = None,
-                 truncation_cutoff: float = 1e-16, jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0):
+                 truncation_cutoff: float = 1e-16, jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0,
+                 heev: dict | None = None):
         self.ctx, self.mpo = ctx, mpo
-        p = DMRGParams(max_bond_dimension, init_bond_dimension or max_bond_dimension, truncation_cutoff, jcd_tol,
-                       jcd_maxiter, ecore)
+        p = _params(max_bond_dimension, init_bond_dimension or max_bond_dimension, truncation_cutoff, jcd_tol,
+                    jcd_maxiter, ecore, heev)
         h = c_void_p()
         check(lib.qcm_dmrg_create(ctx.h, mpo.handle, nup, ndown, ctypes.byref(p), ctypes.byref(h)), "qcm_dmrg_create")
         self.h = h
@@ -93,12 +104,12 @@ class DMRG:
 
     @classmethod
     def from_mps(cls, ctx, mpo, sites, max_bond_dimension: int, truncation_cutoff: float = 1e-16,
-                 jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0):
+                 jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0, heev: dict | None = None):
         """Restart from a given MPS: sites = [dict(phys, left, right, blocks)] with right-paired blocks
         (one per left sector, in sector order), sites 1 .. L-1 right-normalised."""
         self = cls.__new__(cls)
         self.ctx, self.mpo = ctx, mpo
-        p = DMRGParams(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore)
+        p = _params(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore, heev)
         descs = (MPSDesc * len(sites))()
         keep, ptrs = [], (P(c_double) * len(sites))()
         for i, st in enumerate(sites):

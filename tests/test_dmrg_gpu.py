@@ -152,3 +152,30 @@ def test_pending_problem_export_matches_oracle(gpu_ctx):
     del plan
     E2, _ = dev.run(2 * 8 - 2)
     assert len(E2) == 2 * 8 - 2 - 3 and dev.next_step == 0
+
+
+@pytest.mark.parametrize("L,M,sweeps", [(6, 16, 3), (8, 32, 3)])
+def test_heev_sweeps_match_oracle(gpu_ctx, L, M, sweeps):
+    """twosite_truncation = heev: reduced density matrix + alpha x lbtm / rbtm noise (grow, main, final
+    alphas over the sweeps), heev truncation; same initial MPS as the oracle, per-step energies 1e-10."""
+    from oracle.oracle import OracleDMRG
+    from qcmaquis_b200.dmrg import DMRG
+    from qcmaquis_b200.heff import parse_mps_tensor
+    noise = dict(alpha_initial=1e-2, alpha_main=1e-4, alpha_final=1e-8, ngrowsweeps=1, nmainsweeps=1)
+    h, V, e, m, ts, blob = qc_system(L)
+    ref = OracleDMRG(blob, L, L // 2, L // 2, M)
+    ref.set_heev(True, **noise)
+    sites = [parse_mps_tensor(ref.mps_export(i)) for i in range(L)]
+    dev = DMRG.from_mps(gpu_ctx, m, sites, M, heev=noise)
+    for s in range(sweeps):
+        E_ref, tw_ref, tf_ref, bd_ref = ref.sweep(s)
+        E, tr = dev.sweep()
+        assert np.abs(E - E_ref).max() < E_TOL, (s, E - E_ref)
+        bd = np.array([t["bond_dimension"] for t in tr])
+        assert np.array_equal(bd, bd_ref.astype(np.int64)), (s, bd, bd_ref)
+        # the cut is on sqrt(eigenvalue): each eigenvalue at rounding level (~1e-16 of the largest,
+        # solver dependent) enters the discarded fraction as ~1e-8, and a block can hold hundreds of
+        # them, so the fractions agree to ~1e-5 absolute while energies and kept dimensions are exact
+        tf = np.array([t["truncated_fraction"] for t in tr])
+        assert np.allclose(tf, tf_ref, rtol=1e-4, atol=1e-5), (s, tf, tf_ref)
+        assert np.allclose([t["truncated_weight"] for t in tr], tf)
