@@ -114,6 +114,15 @@ __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units,
     const uint16_t* ks = klist + tile.pad;
     const uint32_t nsteps = ks[0];
     const double* Wu = W + U.w_off;
+    // T offsets of the slices this thread copies, loaded one stage ahead of their use
+    uint64_t boff[S::B_PER];
+    auto load_offs = [&](uint32_t k0) {
+#pragma unroll
+        for (int rr = 0; rr < S::B_PER; ++rr) {
+            const uint32_t gk = k0 + uint32_t(tid + rr * NTHR) / S::BN;
+            boff[rr] = gk < U.nk ? __ldg(slice_off + U.slice0 + gk) : 0;
+        }
+    };
     auto issue = [&](int sidx, uint32_t k0) {
         Stage<S>& s = st[sidx];
         // A = W_u (lines x slices, column-major, ld nl)
@@ -132,17 +141,28 @@ __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units,
             int n = e % S::BN, k = e / S::BN;
             uint32_t gn = tile.n0 + n, gk = k0 + k;
             bool ok = gn < U.ne && gk < U.nk;
-            cp8(&s.B[k][n], ok ? T + __ldg(slice_off + U.slice0 + gk) + gn : T, ok);
+            cp8(&s.B[k][n], ok ? T + boff[rr] + gn : T, ok);
         }
         cp_commit();
     };
     Acc<S> acc;
     acc.zero();
-    if (nsteps) issue(0, uint32_t(ks[1]) * BK);
+    uint32_t knext = nsteps > 1 ? uint32_t(ks[2]) * BK : 0;
+    if (nsteps) {
+        load_offs(uint32_t(ks[1]) * BK);
+        issue(0, uint32_t(ks[1]) * BK);
+        if (nsteps > 1) load_offs(knext);
+    }
     for (uint32_t i = 0; i < nsteps; ++i) {
         cp_wait_all();
         __syncthreads();
-        if (i + 1 < nsteps) issue((i + 1) & 1, uint32_t(ks[2 + i]) * BK);
+        if (i + 1 < nsteps) {
+            issue((i + 1) & 1, knext);
+            if (i + 2 < nsteps) {
+                knext = uint32_t(ks[3 + i]) * BK;
+                load_offs(knext);
+            }
+        }
         mma_stage<S>(st[i & 1].A, st[i & 1].B, acc, warp, lane);
     }
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
