@@ -114,6 +114,7 @@ typedef struct {
     double flops_sdense;                      /* tensor-core work of the S build (dense unit GEMMs) */
     uint64_t launches;                        /* own kernels launched per apply */
     uint64_t w_len;                           /* doubles of the dense coefficient blocks of the S build */
+    double flops_sexec;                       /* tensor work the S-build tiles execute (padding included) */
 } qcm_heff_info;
 
 #define QCM_PLAN_BOOKKEEPING 1 /* keep the (cohort, unit, line, alpha) list for parity checks */

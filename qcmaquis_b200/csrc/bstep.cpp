@@ -216,7 +216,7 @@ void SBuild::validate(uint64_t t_len, uint64_t s_len) const {
                 throw std::runtime_error("S tile outside its work lists");
             const UnitD& u = units[t.item];
             for (uint32_t i = 0; i < klist[t.pad]; ++i)
-                if (uint32_t(klist[t.pad + 1 + i]) * 16 >= u.nk) throw std::runtime_error("S tile: k-step out of range");
+                if (uint32_t(klist[t.pad + 1 + i] >> 4) * 16 >= u.nk) throw std::runtime_error("S tile: k-step out of range");
         }
 }
 

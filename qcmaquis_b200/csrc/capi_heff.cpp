@@ -166,6 +166,7 @@ int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info) {
     info->n_kitems = p.kitems[0].size() + p.kitems[1].size() + p.kitems[2].size();
     info->launches = uint64_t(qcm::heff_launches_per_apply(p));
     info->w_len = p.w_len;
+    info->flops_sexec = p.flops_sexec;
     info->flops = p.flops;
     info->flops_t = p.flops_t;
     info->flops_ls = p.flops_ls;

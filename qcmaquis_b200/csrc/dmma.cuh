@@ -74,6 +74,27 @@ static __device__ __forceinline__ void mma_stage(const double (*A)[S::BM + PAD],
     }
 }
 
+// Same, skipping the 4-slice k groups whose bit in mask is clear (all-zero coefficients)
+template <class S>
+static __device__ __forceinline__ void mma_stage_masked(const double (*A)[S::BM + PAD], const double (*B)[S::BN + PAD],
+                                                 Acc<S>& acc, int warp, int lane, uint32_t mask) {
+    const int r = lane >> 2, q = lane & 3;
+    const int wm = warp % S::WM, wn = warp / S::WM;
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+        if (!((mask >> (kk / 4)) & 1u)) continue;
+        double a[S::FM], b[S::FN];
+#pragma unroll
+        for (int i = 0; i < S::FM; ++i) a[i] = A[kk + q][wm * S::FM * 8 + i * 8 + r];
+#pragma unroll
+        for (int j = 0; j < S::FN; ++j) b[j] = B[kk + q][wn * S::FN * 8 + j * 8 + r];
+#pragma unroll
+        for (int i = 0; i < S::FM; ++i)
+#pragma unroll
+            for (int j = 0; j < S::FN; ++j) dmma(acc.c[i][j], a[i], b[j]);
+    }
+}
+
 // Visit every accumulator element: f(m, n, value) with tile-local (m, n).
 template <class S, class F>
 static __device__ __forceinline__ void for_acc(const Acc<S>& acc, int warp, int lane, F f) {

@@ -139,9 +139,10 @@ inline uint32_t shape_bm(int s) { return s == SHAPE_16 ? 16 : (s == SHAPE_32 ? 3
 inline uint32_t shape_bn(int s) { return s == SHAPE_64 ? 64 : (s == SHAPE_128 ? 32 : 128); }
 
 // S-GEMM tiles of one unit.  ents[0..n) are the unit's coefficient entries.  The tile shape
-// is the one with the least tensor work counting only the (BM lines x 16 slices) coefficient
-// blocks that hold an entry; every m-tile's non-empty k-steps go to klist as (count, steps...)
-// and its tiles carry that list's offset in TileD::pad.
+// is the one with the least tensor work counting only the (BM lines x 4 slices) coefficient
+// groups that hold an entry; every m-tile's non-empty k-steps go to klist as (count, steps...),
+// a step being (k-step index << 4 | mask of its non-empty 4-slice groups), and its tiles carry
+// that list's offset in TileD::pad.
 void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_t n, std::vector<TileD>* utiles,
                     std::vector<uint16_t>& klist);
 
@@ -176,6 +177,7 @@ struct HeffPlan {
     // dense tensor-core work of the unit GEMMs (2 * lines * slices * elements)
     uint64_t g_elems = 0, g_reads = 0;
     double flops_sdense = 0;
+    double flops_sexec = 0;  // tensor work the S-GEMM tiles execute (active k-steps x tile area)
     // bookkeeping export rows: (lb_in, lb_out, ci, ci_eff, unit offset, ms, b1, mps_offset, ci_right, col) + alpha
     std::vector<uint32_t> bk_int;
     std::vector<double> bk_alpha;

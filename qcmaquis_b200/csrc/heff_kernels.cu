@@ -147,23 +147,27 @@ __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units,
     };
     Acc<S> acc;
     acc.zero();
-    uint32_t knext = nsteps > 1 ? uint32_t(ks[2]) * BK : 0;
+    // step entries: k-step index << 4 | mask of its non-empty 4-slice groups
+    uint32_t knext = nsteps > 1 ? uint32_t(ks[2] >> 4) * BK : 0;
     if (nsteps) {
-        load_offs(uint32_t(ks[1]) * BK);
-        issue(0, uint32_t(ks[1]) * BK);
+        load_offs(uint32_t(ks[1] >> 4) * BK);
+        issue(0, uint32_t(ks[1] >> 4) * BK);
         if (nsteps > 1) load_offs(knext);
     }
+    uint32_t mcur = nsteps ? (ks[1] & 15u) : 0;
     for (uint32_t i = 0; i < nsteps; ++i) {
         cp_wait_all();
         __syncthreads();
+        const uint32_t mask = mcur;
         if (i + 1 < nsteps) {
+            mcur = ks[2 + i] & 15u;
             issue((i + 1) & 1, knext);
             if (i + 2 < nsteps) {
-                knext = uint32_t(ks[3 + i]) * BK;
+                knext = uint32_t(ks[3 + i] >> 4) * BK;
                 load_offs(knext);
             }
         }
-        mma_stage<S>(st[i & 1].A, st[i & 1].B, acc, warp, lane);
+        mma_stage_masked<S>(st[i & 1].A, st[i & 1].B, acc, warp, lane, mask);
     }
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
         uint32_t gl = tile.m0 + m, gn = tile.n0 + n;
@@ -383,7 +387,7 @@ void upload_plan(HeffPlan& p) {
                 std::size_t(t.pad) + 1 + p.klist[t.pad] > p.klist.size())
                 throw std::runtime_error("heff plan: S tile outside its work lists");
             for (uint32_t i = 0; i < p.klist[t.pad]; ++i)
-                if (uint32_t(p.klist[t.pad + 1 + i]) * BK >= p.units[t.item].nk) throw std::runtime_error("heff plan: S tile k-step out of range");
+                if (uint32_t(p.klist[t.pad + 1 + i] >> 4) * BK >= p.units[t.item].nk) throw std::runtime_error("heff plan: S tile k-step out of range");
         }
     p.d_tjobs.upload(p.tjobs, s);
     for (int sh = 0; sh < N_SHAPES; ++sh) {

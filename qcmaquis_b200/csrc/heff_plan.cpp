@@ -82,18 +82,22 @@ struct U { uint32_t st, offset, ms, rb_out; std::vector<Em> em; std::vector<uint
 void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_t n, std::vector<TileD>* utiles,
                     std::vector<uint16_t>& klist) {
     if (!u.nl || !u.ne || !u.nk || !n) return;
-    constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK)
+    constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK), four DMMA k-groups of 4 slices
     const uint32_t nks = (u.nk + KS - 1) / KS;
-    // occupancy of (16 lines x 16 slices) coefficient blocks; coarser line tiles OR rows together
+    if (nks >= 4096) throw std::runtime_error("S unit: too many slices for the k-step list");
+    // occupancy of (16 lines x 4 slices) coefficient groups as a 4-bit mask per (16 lines x 16 slices)
+    // block; coarser line tiles OR rows together
     const uint32_t n16 = (u.nl + 15) / 16;
     std::vector<uint8_t> occ16(std::size_t(n16) * nks, 0);
-    for (std::size_t i = 0; i < n; ++i) occ16[std::size_t(ents[i].line / 16) * nks + ents[i].k / KS] = 1;
+    for (std::size_t i = 0; i < n; ++i)
+        occ16[std::size_t(ents[i].line / 16) * nks + ents[i].k / KS] |= uint8_t(1u << ((ents[i].k % KS) / 4));
     auto occ_at = [&](uint32_t bm, std::vector<uint8_t>& occ) {
         const uint32_t f = bm / 16, nmt = (u.nl + bm - 1) / bm;
         occ.assign(std::size_t(nmt) * nks, 0);
         for (uint32_t r = 0; r < n16; ++r)
             for (uint32_t ks = 0; ks < nks; ++ks) occ[std::size_t(r / f) * nks + ks] |= occ16[std::size_t(r) * nks + ks];
     };
+    auto groups = [](uint8_t m) { return (m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) + ((m >> 3) & 1); };
     // candidate shapes and a relative cost per tensor flop (the 16-row shape runs 2 x 4 fragments per warp)
     static const int cand[4] = {SHAPE_16, SHAPE_32, SHAPE_64, SHAPE_128};
     static const double eff[4] = {1.3, 1.0, 1.0, 1.05};
@@ -105,8 +109,8 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_
         const uint32_t nnt = (u.ne + bn - 1) / bn;
         occ_at(bm, occ);
         std::size_t on = 0;
-        for (uint8_t o : occ) on += o;
-        const double cost = eff[ci] * double(on) * bm * KS * double(nnt) * bn;
+        for (uint8_t o : occ) on += groups(o);
+        const double cost = eff[ci] * double(on) * bm * 4.0 * double(nnt) * bn;
         if (best < 0 || cost < best_cost) { best = ci; best_cost = cost; best_occ.swap(occ); }
     }
     const int sh = cand[best];
@@ -115,8 +119,10 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_
         const uint32_t off = uint32_t(klist.size());
         klist.push_back(0);
         uint16_t cnt = 0;
-        for (uint32_t ks = 0; ks < nks; ++ks)
-            if (best_occ[std::size_t(mt) * nks + ks]) { klist.push_back(uint16_t(ks)); ++cnt; }
+        for (uint32_t ks = 0; ks < nks; ++ks) {
+            const uint8_t m = best_occ[std::size_t(mt) * nks + ks];
+            if (m) { klist.push_back(uint16_t((ks << 4) | m)); ++cnt; }
+        }
         klist[off] = cnt;
         if (!cnt) continue;
         for (uint32_t n0 = 0; n0 < u.ne; n0 += bn) utiles[sh].push_back(TileD{item, mt * bm, n0, off});
@@ -399,7 +405,15 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         for (std::size_t k = 0; k < nu; ++k) {
             const uint32_t kb = uint32_t(p->klist.size());
             for (int sh = 0; sh < N_SHAPES; ++sh)
-                for (TileD t : ut[k].t[sh]) { t.pad += kb; p->utiles[sh].push_back(t); }
+                for (TileD t : ut[k].t[sh]) {
+                    for (uint32_t i = 0; i < ut[k].kl[t.pad]; ++i) {
+                        const uint16_t e = ut[k].kl[t.pad + 1 + i];
+                        p->flops_sexec += 2.0 * 4.0 * (((e & 1) + ((e >> 1) & 1) + ((e >> 2) & 1) + ((e >> 3) & 1))) *
+                                          shape_bm(sh) * shape_bn(sh);
+                    }
+                    t.pad += kb;
+                    p->utiles[sh].push_back(t);
+                }
             p->klist.insert(p->klist.end(), ut[k].kl.begin(), ut[k].kl.end());
         }
     }
