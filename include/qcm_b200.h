@@ -266,8 +266,11 @@ int qcm_dmrg_pending_plan(qcm_dmrg* d, double* twin, uint64_t cap, qcm_heff** ou
 /* Start vector of the pending step (*n = vec_len; twin may be NULL to query). */
 int qcm_dmrg_pending_twin(qcm_dmrg* d, double* twin, uint64_t cap, uint64_t* n);
 /* The pending step's frozen site problem as a "QSPB" v1 blob (twin + L + R, the
- * interchange format read by the test oracle).  Call with buf == NULL for *len. */
-int qcm_dmrg_pending_export(qcm_dmrg* d, void* buf, size_t cap, size_t* len);
+ * interchange format read by the test oracle).  Call with buf == NULL for *len.
+ * QCM_EXPORT_INDEX_ONLY: sectors and boundary indices only (blocks of width 0, cohorts
+ * without values), enough to rebuild the H_eff schedule on a host. */
+#define QCM_EXPORT_INDEX_ONLY 1
+int qcm_dmrg_pending_export(qcm_dmrg* d, int flags, void* buf, size_t cap, size_t* len);
 /* Current bond dimensions (right basis size of sites 0 .. L-2). */
 int qcm_dmrg_bond_dimensions(const qcm_dmrg* d, uint64_t* dims);
 void qcm_dmrg_free(qcm_dmrg* d);

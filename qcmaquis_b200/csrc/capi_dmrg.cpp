@@ -87,10 +87,11 @@ struct Blob {
         put<uint32_t>(uint32_t(i.size()));
         for (auto& e : i.d) { put<int32_t>(e.first.a); put<int32_t>(e.first.b); put<uint32_t>(uint32_t(e.second)); }
     }
-    void bnd(const qcm::DevBoundary& B, cudaStream_t s) {
+    void bnd(const qcm::DevBoundary& B, cudaStream_t s, bool with_data) {
         const qcm::BoundaryIndexH& x = B.idx;
-        std::vector<double> h(x.total);
-        if (x.total) QCM_CUDA(cudaMemcpyAsync(h.data(), B.data.get(), x.total * sizeof(double), cudaMemcpyDeviceToHost, s));
+        std::vector<double> h(with_data ? x.total : 0);
+        if (with_data && x.total)
+            QCM_CUDA(cudaMemcpyAsync(h.data(), B.data.get(), x.total * sizeof(double), cudaMemcpyDeviceToHost, s));
         QCM_CUDA(cudaStreamSynchronize(s));
         idx(x.bra); idx(x.ket);
         put<uint32_t>(x.n_cohorts()); put<uint32_t>(x.aux);
@@ -99,10 +100,12 @@ struct Blob {
             put<uint32_t>(x.lsz[ci]); put<uint32_t>(x.rsz[ci]); put<uint32_t>(x.nb[ci]);
             for (uint32_t b = 0; b < x.aux; ++b) put<int64_t>(x.offsets[std::size_t(ci) * x.aux + b]);
             for (uint32_t b = 0; b < x.aux; ++b) put<double>(x.cscale[std::size_t(ci) * x.aux + b]);
-            const uint64_t n = x.cohort_size(ci);
+            const uint64_t n = with_data ? x.cohort_size(ci) : 0;
             put<uint64_t>(n);
-            const uint8_t* p = reinterpret_cast<const uint8_t*>(h.data() + x.data_off[ci]);
-            b.insert(b.end(), p, p + n * sizeof(double));
+            if (n) {
+                const uint8_t* p = reinterpret_cast<const uint8_t*>(h.data() + x.data_off[ci]);
+                b.insert(b.end(), p, p + n * sizeof(double));
+            }
         }
     }
 };
@@ -315,7 +318,7 @@ int qcm_dmrg_pending_twin(qcm_dmrg* d, double* twin, uint64_t cap, uint64_t* n) 
     QCM_CATCH
 }
 
-int qcm_dmrg_pending_export(qcm_dmrg* d, void* buf, size_t cap, size_t* len) {
+int qcm_dmrg_pending_export(qcm_dmrg* d, int flags, void* buf, size_t cap, size_t* len) {
     QCM_TRY
     if (!d || !len) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_export: NULL argument");
     QCM_CUDA(cudaSetDevice(d->ctx->device));
@@ -330,15 +333,17 @@ int qcm_dmrg_pending_export(qcm_dmrg* d, void* buf, size_t cap, size_t* len) {
     w.put<uint32_t>(0x42505351u);  // "QSPB"
     w.put<uint32_t>(1);
     w.idx(phys); w.idx(left); w.idx(right);
+    const bool data = (flags & QCM_EXPORT_INDEX_ONLY) == 0;
     w.put<uint32_t>(uint32_t(left.size()));
     for (std::size_t lb = 0; lb < left.size(); ++lb) {
         w.put<int32_t>(left[lb].first.a); w.put<int32_t>(left[lb].first.b);
-        w.put<uint32_t>(uint32_t(left[lb].second)); w.put<uint32_t>(plan->x_cols[lb]);
+        w.put<uint32_t>(uint32_t(left[lb].second)); w.put<uint32_t>(data ? plan->x_cols[lb] : 0);
+        if (!data) continue;
         const uint8_t* p = reinterpret_cast<const uint8_t*>(x.data() + plan->x_off[lb]);
         w.b.insert(w.b.end(), p, p + uint64_t(left[lb].second) * plan->x_cols[lb] * sizeof(double));
     }
-    w.bnd(*e.left_[site1], e.c.s);
-    w.bnd(*e.right_[site2 + 1], e.c.s);
+    w.bnd(*e.left_[site1], e.c.s, data);
+    w.bnd(*e.right_[site2 + 1], e.c.s, data);
     *len = w.b.size();
     if (buf) {
         if (cap < w.b.size()) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_pending_export: buffer too small");

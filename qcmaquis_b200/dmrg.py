@@ -54,7 +54,7 @@ _lib._sig("qcm_dmrg_run", c_int, c_void_p, c_int, P(c_double), P(TruncResult), P
 _lib._sig("qcm_dmrg_next_step", c_int, c_void_p)
 _lib._sig("qcm_dmrg_pending_plan", c_int, c_void_p, P(c_double), c_uint64, P(c_void_p))
 _lib._sig("qcm_dmrg_pending_twin", c_int, c_void_p, P(c_double), c_uint64, P(c_uint64))
-_lib._sig("qcm_dmrg_pending_export", c_int, c_void_p, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
+_lib._sig("qcm_dmrg_pending_export", c_int, c_void_p, c_int, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
 _lib._sig("qcm_dmrg_sweep", c_int, c_void_p, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
 _lib._sig("qcm_dmrg_bond_dimensions", c_int, c_void_p, P(c_uint64))
@@ -161,12 +161,13 @@ class DMRG:
         assert x.size == plan.n
         return plan, x
 
-    def pending_export(self) -> bytes:
-        """The pending step's frozen site problem ("QSPB" v1)."""
+    def pending_export(self, index_only: bool = False) -> bytes:
+        """The pending step's frozen site problem ("QSPB" v1); index_only: sectors and boundary indices only."""
         n = ctypes.c_size_t()
-        check(lib.qcm_dmrg_pending_export(self.h, None, 0, ctypes.byref(n)), "qcm_dmrg_pending_export")
+        fl = 1 if index_only else 0
+        check(lib.qcm_dmrg_pending_export(self.h, fl, None, 0, ctypes.byref(n)), "qcm_dmrg_pending_export")
         buf = ctypes.create_string_buffer(n.value)
-        check(lib.qcm_dmrg_pending_export(self.h, buf, n.value, ctypes.byref(n)), "qcm_dmrg_pending_export")
+        check(lib.qcm_dmrg_pending_export(self.h, fl, buf, n.value, ctypes.byref(n)), "qcm_dmrg_pending_export")
         return buf.raw
 
     def stats(self) -> dict:
