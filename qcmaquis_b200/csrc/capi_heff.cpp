@@ -159,7 +159,7 @@ int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info) {
     info->n_tjobs = p.tjobs.size();
     info->n_ttiles = p.ttiles[0].size() + p.ttiles[1].size() + p.ttiles[2].size();
     info->n_gtasks = p.units.size();
-    info->n_alpha = p.went.size();
+    info->n_alpha = p.n_alpha;
     info->n_segs = p.segs.size();
     info->n_outs = p.outs.size();
     info->n_otiles = p.otiles[0].size() + p.otiles[1].size() + p.otiles[2].size();

@@ -103,32 +103,43 @@ struct OTileD {       // output tile of the L.S GEMM and its contiguous range of
 // several MPO terms may couple the same boundary block, input state and output state,
 // and the densified coefficient tile holds their sum -- and the unit's nk + 1 slice
 // pointers to sptr.
+struct PackScratch {  // reusable buffers of pack_unit_entries
+    std::vector<uint32_t> cnt, fill;
+    std::vector<WEntD, NoInitAlloc<WEntD>> sorted;
+};
+template <class WV, class PV>
+inline void pack_unit_entries(const WEntD* ents, std::size_t n, uint32_t nk, WV& went, PV& sptr, PackScratch& sc) {
+    // counting sort by slice; entries arrive in line order, so each slice's lines stay ascending
+    sc.cnt.assign(std::size_t(nk) + 1, 0);
+    for (std::size_t i = 0; i < n; ++i) sc.cnt[ents[i].k + 1]++;
+    for (uint32_t k = 0; k < nk; ++k) sc.cnt[k + 1] += sc.cnt[k];
+    sc.sorted.resize(n);
+    sc.fill.assign(sc.cnt.begin(), sc.cnt.end() - 1);
+    for (std::size_t i = 0; i < n; ++i) sc.sorted[sc.fill[ents[i].k]++] = ents[i];
+    auto by_line = [](const WEntD& x, const WEntD& y) { return x.line < y.line; };
+    for (uint32_t k = 0; k < nk; ++k)  // a slice's lines need not arrive sorted when lines repeat out of order
+        if (!std::is_sorted(sc.sorted.begin() + sc.cnt[k], sc.sorted.begin() + sc.cnt[k + 1], by_line))
+            std::stable_sort(sc.sorted.begin() + sc.cnt[k], sc.sorted.begin() + sc.cnt[k + 1], by_line);
+    const std::size_t w0 = went.size();
+    went.resize(w0 + n);
+    WEntD* out = went.data() + w0;
+    std::size_t m = 0;
+    sptr.push_back(uint32_t(w0));
+    for (uint32_t k = 0; k < nk; ++k) {
+        const std::size_t m0 = m;
+        for (uint32_t i = sc.cnt[k]; i < sc.cnt[k + 1]; ++i) {
+            const WEntD& e = sc.sorted[i];
+            if (m > m0 && out[m - 1].line == e.line) out[m - 1].a += e.a;
+            else out[m++] = e;
+        }
+        sptr.push_back(uint32_t(w0 + m));
+    }
+    went.resize(w0 + m);
+}
 template <class WV, class PV>
 inline void pack_unit_entries(std::vector<WEntD> ents, uint32_t nk, WV& went, PV& sptr) {
-    // counting sort by slice; entries arrive in line order, so each slice's lines stay ascending
-    std::vector<uint32_t> cnt(std::size_t(nk) + 1, 0);
-    for (const WEntD& e : ents) cnt[e.k + 1]++;
-    for (uint32_t k = 0; k < nk; ++k) cnt[k + 1] += cnt[k];
-    std::vector<WEntD> sorted(ents.size());
-    {
-        std::vector<uint32_t> fill(cnt.begin(), cnt.end() - 1);
-        for (const WEntD& e : ents) sorted[fill[e.k]++] = e;
-    }
-    for (uint32_t k = 0; k < nk; ++k)  // a slice's lines need not arrive sorted when lines repeat out of order
-        if (!std::is_sorted(sorted.begin() + cnt[k], sorted.begin() + cnt[k + 1],
-                            [](const WEntD& x, const WEntD& y) { return x.line < y.line; }))
-            std::stable_sort(sorted.begin() + cnt[k], sorted.begin() + cnt[k + 1],
-                             [](const WEntD& x, const WEntD& y) { return x.line < y.line; });
-    const uint32_t w0 = uint32_t(went.size());
-    sptr.push_back(w0);
-    for (uint32_t k = 0; k < nk; ++k) {
-        for (uint32_t i = cnt[k]; i < cnt[k + 1]; ++i) {
-            const WEntD& e = sorted[i];
-            if (went.size() > w0 && went.back().k == e.k && went.back().line == e.line) went.back().a += e.a;
-            else went.push_back(e);
-        }
-        sptr.push_back(uint32_t(went.size()));
-    }
+    PackScratch sc;
+    pack_unit_entries(ents.data(), ents.size(), nk, went, sptr, sc);
 }
 
 // DMMA tile shapes (rows x cols of the CTA tile).  GEMM jobs pick the class from their row
@@ -143,8 +154,26 @@ inline uint32_t shape_bn(int s) { return s == SHAPE_64 ? 64 : (s == SHAPE_128 ? 
 // groups that hold an entry; every m-tile's non-empty k-steps go to klist as (count, steps...),
 // a step being (k-step index << 4 | mask of its non-empty 4-slice groups), and its tiles carry
 // that list's offset in TileD::pad.
-void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_t n, std::vector<TileD>* utiles,
+// E is any entry type with members line and k (WEntD, LKD).
+template <class E>
+void add_unit_tiles(const UnitD& u, uint32_t item, const E* ents, std::size_t n, std::vector<TileD>* utiles,
                     std::vector<uint16_t>& klist);
+
+struct LKD { uint32_t line, k; };  // (line, slice) position of one coefficient term
+
+// Coefficient generation of one S unit on the device: every term of line l (MPO row
+// b1 = line_row[line0 + l]) is alpha = op value * R conj scale * MPO scale * L conj scale,
+// summed into W[w_off + l + slot * nl]; the term's slice id (T slice numbering of the ket
+// sector) maps to its slot through the unit's (slice id, slot) pairs sorted by id.
+struct WGenUnitD {
+    uint64_t w_off;
+    uint32_t ci;       // L cohort (conj scale row)
+    uint32_t st_out;   // output physical state of the unit
+    uint32_t line0, nl;
+    uint32_t map0, nk;  // sorted (slice id, slot) pairs at smap_id/smap_slot[map0 .. map0 + nk)
+};
+struct WGenInD { uint32_t cir, jbase; };  // per (unit, input state): R cohort and slice-id base, or WGEN_NONE
+constexpr uint32_t WGEN_NONE = 0xffffffffu;
 
 struct HeffPlan {
     Index phys, left, right;
@@ -158,10 +187,22 @@ struct HeffPlan {
 
     hvec<UnitD> units;
     std::vector<TileD> utiles[N_SHAPES];   // (unit, line tile m0, element tile n0)
-    hvec<uint32_t> line_b1, sptr;
+    hvec<uint32_t> line_b1;
     hvec<uint64_t> slice_off;
-    hvec<WEntD> went;
     uint64_t s_len = 0;
+    uint64_t n_alpha = 0;  // coefficient terms (before terms of one (line, slice) are summed)
+    // coefficient generation tables (see WGenUnitD)
+    hvec<WGenUnitD> wgunits;
+    hvec<WGenInD> wgin;          // units x nst
+    hvec<uint32_t> line_row;     // MPO row b1 of each line (line_b1 holds its S row block)
+    hvec<uint32_t> smap_id, smap_slot;
+    uint32_t nst = 0;
+    std::vector<uint32_t> m_rowptr, m_b2, m_op;  // MPO entries, CSR over b1
+    std::vector<double> m_scale;
+    std::vector<uint32_t> o_ptr, o_in;  // operator terms by (op, output state): (input state, value)
+    std::vector<double> o_val;
+    std::vector<int32_t> r_pos;   // R cohort x aux: block position of b2 in the cohort, or -1
+    uint32_t l_aux = 0, r_aux = 0;
     uint64_t w_len = 0;  // dense coefficient blocks of all units (doubles)
     std::vector<uint16_t> klist;  // non-empty k-steps per S-GEMM m-tile
 
@@ -190,9 +231,13 @@ struct HeffPlan {
     DBuf<double> d_P;
     DBuf<UnitD> d_units;
     DBuf<TileD> d_utiles[N_SHAPES];
-    DBuf<uint32_t> d_line_b1, d_sptr;
+    DBuf<uint32_t> d_line_b1;
     DBuf<uint64_t> d_slice_off;
-    DBuf<WEntD> d_went;
+    DBuf<WGenUnitD> d_wgunits;
+    DBuf<WGenInD> d_wgin;
+    DBuf<uint32_t> d_line_row, d_smap_id, d_smap_slot, d_m_rowptr, d_m_b2, d_m_op, d_o_ptr, d_o_in;
+    DBuf<double> d_m_scale, d_o_val, d_l_cs, d_r_cs;
+    DBuf<int32_t> d_r_pos;
     DBuf<double> d_W;
     DBuf<uint16_t> d_klist;
     DBuf<SegD> d_segs;
@@ -224,6 +269,8 @@ void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<T
 void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const uint32_t* line_b1,
                const uint64_t* slice_off, const uint16_t* klist, const double* W, const double* T, double* S,
                cudaStream_t s);
+// Computes every unit's coefficients into its dense block of W (w_len doubles, zeroed first).
+void generate_coefficients(HeffPlan& p);
 // Scatters every unit's coefficient entries into its dense block of W (w_len doubles, zeroed first).
 void fill_coefficients(const UnitD* units, uint32_t n_units, const uint32_t* sptr, const WEntD* went, double* W,
                        uint64_t w_len, cudaStream_t s);

@@ -190,6 +190,65 @@ __global__ void k_wfill(const UnitD* __restrict__ units, const uint32_t* __restr
     }
 }
 
+// One CTA per unit, one thread per line: the line's coefficient terms, in MPO-entry then
+// operator-term order, summed into W_u.  Products and sums are rounded separately (no
+// contraction), so W_u holds the same values as a host evaluation of the same terms.
+constexpr int WG_THR = 128;
+constexpr uint32_t WG_SMAP = 4096;  // (slice id, slot) pairs staged in shared memory
+constexpr uint32_t WG_NST = 64;     // physical states of the two-site basis
+__global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ units, const WGenInD* __restrict__ gin,
+                                                 uint32_t nst, const uint32_t* __restrict__ line_row,
+                                                 const uint32_t* __restrict__ smap_id, const uint32_t* __restrict__ smap_slot,
+                                                 const uint32_t* __restrict__ m_rowptr, const uint32_t* __restrict__ m_b2,
+                                                 const uint32_t* __restrict__ m_op, const double* __restrict__ m_scale,
+                                                 const uint32_t* __restrict__ o_ptr, const uint32_t* __restrict__ o_in,
+                                                 const double* __restrict__ o_val, const double* __restrict__ l_cs,
+                                                 uint32_t l_aux, const int32_t* __restrict__ r_pos,
+                                                 const double* __restrict__ r_cs, uint32_t r_aux, double* __restrict__ W,
+                                                 uint32_t* __restrict__ err) {
+    __shared__ uint32_t sid[WG_SMAP], sslot[WG_SMAP];
+    __shared__ WGenInD sin[WG_NST];
+    const WGenUnitD U = units[blockIdx.x];
+    const bool staged = U.nk <= WG_SMAP;
+    if (staged)
+        for (uint32_t i = threadIdx.x; i < U.nk; i += blockDim.x) {
+            sid[i] = smap_id[U.map0 + i];
+            sslot[i] = smap_slot[U.map0 + i];
+        }
+    for (uint32_t i = threadIdx.x; i < nst; i += blockDim.x) sin[i] = gin[std::size_t(blockIdx.x) * nst + i];
+    __syncthreads();
+    const uint32_t* ids = staged ? sid : smap_id + U.map0;
+    const uint32_t* slots = staged ? sslot : smap_slot + U.map0;
+    for (uint32_t line = threadIdx.x; line < U.nl; line += blockDim.x) {
+        const uint32_t b1 = line_row[U.line0 + line];
+        const double lsc = l_cs[std::size_t(U.ci) * l_aux + b1];
+        double* Wl = W + U.w_off + line;
+        for (uint32_t e = m_rowptr[b1]; e < m_rowptr[b1 + 1]; ++e) {
+            const uint32_t b2 = m_b2[e], op = m_op[e];
+            const double wsc = __dmul_rn(m_scale[e], lsc);
+            const std::size_t q = std::size_t(op) * nst + U.st_out;
+            for (uint32_t k = o_ptr[q]; k < o_ptr[q + 1]; ++k) {
+                const WGenInD g = sin[o_in[k]];
+                if (g.cir == WGEN_NONE) continue;
+                const std::size_t rq = std::size_t(g.cir) * r_aux + b2;
+                const int32_t pos = r_pos[rq];
+                if (pos < 0) continue;
+                const double a = __dmul_rn(__dmul_rn(o_val[k], r_cs[rq]), wsc);
+                const uint32_t id = g.jbase + uint32_t(pos);
+                uint32_t lo = 0, hi = U.nk;
+                while (lo < hi) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (ids[mid] < id) lo = mid + 1;
+                    else hi = mid;
+                }
+                if (lo >= U.nk || ids[lo] != id) { atomicOr(err, 1u); continue; }
+                double* w = Wl + uint64_t(slots[lo]) * U.nl;
+                *w = __dadd_rn(*w, a);
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // L.S GEMM, split-K: item = (output tile, segment, K range) -> partial tile P[item]
 template <class S>
@@ -359,6 +418,64 @@ void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<
     QCM_CUDA(cudaGetLastError());
 }
 
+void generate_coefficients(HeffPlan& p) {
+    cudaStream_t s = p.stream;
+    if (p.w_len) QCM_CUDA(cudaMemsetAsync(p.d_W.get(), 0, p.w_len * sizeof(double), s));
+    if (p.wgunits.empty()) return;
+    DBuf<uint32_t> err;
+    err.alloc(1);
+    QCM_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(uint32_t), s));
+    k_wgen<<<unsigned(p.wgunits.size()), WG_THR, 0, s>>>(
+        p.d_wgunits.get(), p.d_wgin.get(), p.nst, p.d_line_row.get(), p.d_smap_id.get(), p.d_smap_slot.get(),
+        p.d_m_rowptr.get(), p.d_m_b2.get(), p.d_m_op.get(), p.d_m_scale.get(), p.d_o_ptr.get(), p.d_o_in.get(),
+        p.d_o_val.get(), p.d_l_cs.get(), p.l_aux, p.d_r_pos.get(), p.d_r_cs.get(), p.r_aux, p.d_W.get(), err.get());
+    QCM_CUDA(cudaGetLastError());
+    uint32_t h = 0;
+    QCM_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    QCM_CUDA(cudaStreamSynchronize(s));
+    if (h) throw std::runtime_error("heff plan: coefficient term without a slice slot");
+}
+
+// Every index k_wgen derives from the plan tables stays inside its buffer.
+static void validate_wgen(const HeffPlan& p) {
+    const std::size_t nu = p.wgunits.size(), nst = p.nst;
+    const std::size_t l_coh = p.l_aux ? p.L->idx.cscale.size() / p.l_aux : 0;
+    const std::size_t r_coh = p.r_aux ? p.r_pos.size() / p.r_aux : 0;
+    auto bad = [](const char* what) { throw std::runtime_error(std::string("heff plan: coefficient tables: ") + what); };
+    if (nst > WG_NST || p.wgin.size() != nu * nst || nu != p.units.size()) bad("unit tables");
+    if (p.m_rowptr.empty() || p.m_rowptr.back() != p.m_b2.size() || p.m_op.size() != p.m_b2.size() ||
+        p.m_scale.size() != p.m_b2.size())
+        bad("MPO entries");
+    const std::size_t rows = p.m_rowptr.size() - 1;
+    const std::size_t nops = nst ? (p.o_ptr.size() - 1) / nst : 0;
+    if (p.o_ptr.size() != nops * nst + 1 || p.o_ptr.back() != p.o_in.size() || p.o_val.size() != p.o_in.size()) bad("operator terms");
+    for (std::size_t i = 0; i + 1 < p.m_rowptr.size(); ++i)
+        if (p.m_rowptr[i] > p.m_rowptr[i + 1]) bad("MPO row pointers");
+    for (std::size_t e = 0; e < p.m_b2.size(); ++e)
+        if (p.m_b2[e] >= p.r_aux || p.m_op[e] >= nops) bad("MPO entry");
+    for (std::size_t i = 0; i + 1 < p.o_ptr.size(); ++i)
+        if (p.o_ptr[i] > p.o_ptr[i + 1]) bad("operator pointers");
+    for (uint32_t v : p.o_in)
+        if (v >= nst) bad("operator input state");
+    if (p.R->idx.cscale.size() != p.r_pos.size() || p.l_aux != p.L->idx.aux) bad("boundary tables");
+    for (const WGenInD& g : p.wgin)
+        if (g.cir != WGEN_NONE && g.cir >= r_coh) bad("R cohort");
+    for (std::size_t u = 0; u < nu; ++u) {
+        const WGenUnitD& g = p.wgunits[u];
+        if (g.ci >= l_coh || g.st_out >= nst || std::size_t(g.line0) + g.nl > p.line_row.size() ||
+            std::size_t(g.map0) + g.nk > p.smap_id.size() || g.w_off + uint64_t(g.nl) * g.nk > p.w_len)
+            bad("unit extent");
+        for (uint32_t l = 0; l < g.nl; ++l) {
+            const uint32_t b1 = p.line_row[g.line0 + l];
+            if (b1 >= rows || b1 >= p.l_aux) bad("line");
+        }
+        for (uint32_t i = 0; i < g.nk; ++i) {
+            if (p.smap_slot[g.map0 + i] >= g.nk) bad("slot");
+            if (i && p.smap_id[g.map0 + i - 1] >= p.smap_id[g.map0 + i]) bad("slice ids not sorted");
+        }
+    }
+}
+
 void fill_coefficients(const UnitD* units, uint32_t n_units, const uint32_t* sptr, const WEntD* went, double* W,
                        uint64_t w_len, cudaStream_t s) {
     if (w_len) QCM_CUDA(cudaMemsetAsync(W, 0, w_len * sizeof(double), s));
@@ -396,11 +513,25 @@ void upload_plan(HeffPlan& p) {
         p.d_otiles[sh].upload(p.otiles[sh], s);
         p.d_kitems[sh].upload(p.kitems[sh], s);
     }
+    validate_wgen(p);
     p.d_units.upload(p.units, s);
     p.d_line_b1.upload(p.line_b1, s);
     p.d_slice_off.upload(p.slice_off, s);
-    p.d_sptr.upload(p.sptr, s);
-    p.d_went.upload(p.went, s);
+    p.d_wgunits.upload(p.wgunits, s);
+    p.d_wgin.upload(p.wgin, s);
+    p.d_line_row.upload(p.line_row, s);
+    p.d_smap_id.upload(p.smap_id, s);
+    p.d_smap_slot.upload(p.smap_slot, s);
+    p.d_m_rowptr.upload(p.m_rowptr, s);
+    p.d_m_b2.upload(p.m_b2, s);
+    p.d_m_op.upload(p.m_op, s);
+    p.d_m_scale.upload(p.m_scale, s);
+    p.d_o_ptr.upload(p.o_ptr, s);
+    p.d_o_in.upload(p.o_in, s);
+    p.d_o_val.upload(p.o_val, s);
+    p.d_l_cs.upload(p.L->idx.cscale, s);
+    p.d_r_cs.upload(p.R->idx.cscale, s);
+    p.d_r_pos.upload(p.r_pos, s);
     p.d_klist.upload(p.klist, s);
     p.d_segs.upload(p.segs, s);
     p.d_outs.upload(p.outs, s);
@@ -409,7 +540,7 @@ void upload_plan(HeffPlan& p) {
     p.d_P.alloc(p.p_len);
     // dense coefficient blocks, built once per plan and reused by every apply
     p.d_W.alloc(p.w_len ? p.w_len : 1);
-    fill_coefficients(p.d_units.get(), uint32_t(p.units.size()), p.d_sptr.get(), p.d_went.get(), p.d_W.get(), p.w_len, s);
+    generate_coefficients(p);
     QCM_CUDA(cudaStreamSynchronize(s));
 }
 

@@ -63,23 +63,34 @@ struct Part {
     std::vector<uint32_t> tjob_mps;  // mps column offset of each job (bookkeeping)
     uint64_t t_len = 0;
     std::vector<UnitD> units;
-    std::vector<uint32_t> line_b1, sptr;
+    std::vector<WGenUnitD> wgunits;
+    std::vector<WGenInD> wgin;
+    std::vector<uint32_t> line_b1, line_row, smap_id, smap_slot;
     std::vector<uint64_t> slice_off;
-    std::vector<WEntD> went;
-    uint64_t s_len = 0, w_len = 0;
+    uint64_t s_len = 0, w_len = 0, n_alpha = 0;
     std::vector<std::pair<uint32_t, SegD>> segs;
     double flops_t = 0, flops_s = 0, flops_ls = 0, flops_sdense = 0;
     uint64_t g_elems = 0, g_reads = 0;
     std::vector<uint32_t> bk_int;
     std::vector<double> bk_alpha;
+    std::vector<TileD> utiles[N_SHAPES];  // S-GEMM tiles, item = unit of this part, pad = klist offset
+    std::vector<uint16_t> klist;
+    double flops_sexec = 0;
 };
 
-struct Em { uint32_t line, slice; double a; uint32_t mps, cir, col; };
-struct U { uint32_t st, offset, ms, rb_out; std::vector<Em> em; std::vector<uint32_t> lines; };
+// Output state of a cohort and its coefficient terms: (line, slice id in the part's T
+// numbering), and with bookkeeping (mps column, R cohort, R column, alpha) per term.
+struct U {
+    uint32_t st, offset, ms, rb_out;
+    std::vector<LKD> em;
+    std::vector<uint32_t> lines, rows, bk;  // lines: S row block of each line, rows: its MPO row b1
+    std::vector<double> bk_a;
+};
 
 }  // namespace
 
-void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_t n, std::vector<TileD>* utiles,
+template <class E>
+void add_unit_tiles(const UnitD& u, uint32_t item, const E* ents, std::size_t n, std::vector<TileD>* utiles,
                     std::vector<uint16_t>& klist) {
     if (!u.nl || !u.ne || !u.nk || !n) return;
     constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK), four DMMA k-groups of 4 slices
@@ -128,6 +139,11 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const WEntD* ents, std::size_
         for (uint32_t n0 = 0; n0 < u.ne; n0 += bn) utiles[sh].push_back(TileD{item, mt * bm, n0, off});
     }
 }
+
+template void add_unit_tiles<WEntD>(const UnitD&, uint32_t, const WEntD*, std::size_t, std::vector<TileD>*,
+                                    std::vector<uint16_t>&);
+template void add_unit_tiles<LKD>(const UnitD&, uint32_t, const LKD*, std::size_t, std::vector<TileD>*,
+                                  std::vector<uint16_t>&);
 
 std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
                                           const Index& phys, const Index& left, const Index& right, bool bookkeeping) {
@@ -179,15 +195,63 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     for (std::size_t o = 0; o < nops; ++o) {
         const SparseOp& s = (*W.ops)[o];
         optr[o] = uint32_t(oin.size());
-        for (std::size_t e = 0; e < s.val.size(); ++e) { oin.push_back(s.in[e]); oout.push_back(s.out[e]); oval.push_back(s.val[e]); }
+        for (std::size_t e = 0; e < s.val.size(); ++e) {
+            if (s.in[e] >= nst || s.out[e] >= nst) throw std::runtime_error("heff plan: operator entry outside the physical basis");
+            oin.push_back(s.in[e]); oout.push_back(s.out[e]); oval.push_back(s.val[e]);
+        }
     }
     optr[nops] = uint32_t(oin.size());
+    // the same terms by (operator, output state), in their order within the operator
+    p->nst = nst;
+    p->o_ptr.assign(nops * nst + 1, 0);
+    for (std::size_t k = 0; k < oin.size(); ++k) {
+        const std::size_t o = std::size_t(std::upper_bound(optr.begin(), optr.end(), uint32_t(k)) - optr.begin()) - 1;
+        p->o_ptr[o * nst + oout[k] + 1]++;
+    }
+    for (std::size_t i = 0; i < nops * nst; ++i) p->o_ptr[i + 1] += p->o_ptr[i];
+    p->o_in.resize(oin.size());
+    p->o_val.resize(oin.size());
+    {
+        std::vector<uint32_t> fill(p->o_ptr.begin(), p->o_ptr.end() - 1);
+        for (std::size_t o = 0; o < nops; ++o)
+            for (uint32_t k = optr[o]; k < optr[o + 1]; ++k) {
+                const uint32_t d = fill[o * nst + oout[k]]++;
+                p->o_in[d] = oin[k];
+                p->o_val[d] = oval[k];
+            }
+    }
+    // MPO entries and boundary tables for the device coefficient generation
+    p->m_rowptr.assign(W.row_ptr.begin(), W.row_ptr.end());
+    p->m_b2.assign(W.b2.begin(), W.b2.end());
+    p->m_op.assign(W.op.begin(), W.op.end());
+    p->m_scale.assign(W.scale.begin(), W.scale.end());
+    if (p->m_rowptr.size() != std::size_t(W.rows) + 1 || p->m_b2.size() != p->m_rowptr.back() ||
+        p->m_op.size() != p->m_b2.size() || p->m_scale.size() != p->m_b2.size())
+        throw std::runtime_error("heff plan: inconsistent MPO tensor");
+    for (std::size_t e = 0; e < p->m_b2.size(); ++e)
+        if (p->m_b2[e] >= W.cols || p->m_op[e] >= nops) throw std::runtime_error("heff plan: MPO entry out of range");
+    p->l_aux = L.aux;
+    p->r_aux = R.aux;
+    // block position of (R cohort, b2): element offset / block size
+    p->r_pos.resize(R.offsets.size());
+    for (uint32_t c = 0; c < R.n_cohorts(); ++c) {
+        const int64_t bs = std::max<int64_t>(1, int64_t(R.lsz[c]) * R.rsz[c]);
+        for (uint32_t b = 0; b < R.aux; ++b) {
+            const int64_t o = R.offsets[std::size_t(c) * R.aux + b];
+            p->r_pos[std::size_t(c) * R.aux + b] = o < 0 ? -1 : int32_t(o / bs);
+        }
+    }
 
     std::vector<Part> parts(nl);
     const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
     auto tnow = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     const double t_a = tnow();
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel
+    {
+    // per-thread scratch, reused across cohorts
+    std::vector<U> units;
+    std::vector<uint32_t> slices, order;
+#pragma omp for schedule(dynamic, 1)
     for (int lbi = 0; lbi < int(nl); ++lbi) {
         const uint32_t lb_in = uint32_t(lbi);
         Part& P = parts[lb_in];
@@ -216,7 +280,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 P.tjob_mps.push_back(mps_off);
             }
         }
-        // slice numbering: slot of (job, b2 position); cleared after each unit
+        // slice ids: (job, b2 position) -> job_pos0[job] + position; slot of an id within the
+        // current unit, cleared after each unit
         std::vector<uint32_t> job_pos0(P.tjobs.size() + 1, 0);
         for (std::size_t k = 0; k < P.tjobs.size(); ++k)
             job_pos0[k + 1] = job_pos0[k] + (P.tjobs[k].brs ? P.tjobs[k].N / P.tjobs[k].brs : 0);
@@ -231,98 +296,121 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             const uint32_t nS = L.nb[ce];
             const uint32_t K_c = nS * ls_in;
             // units = output states whose right sector exists
-            std::vector<U> units;
+            std::size_t nu = 0;
             uint32_t stripe = 0;
             for (uint32_t st = 0; st < nst; ++st) {
                 const RSec& ro = rsec[std::size_t(lb_out) * nps + sm.sector[st]];
                 if (ro.rb == NONE) continue;
-                units.push_back(U{st, ro.off + uint32_t(sm.sub[st]) * ro.rs, ro.rs, ro.rb, {}, {}});
+                if (nu == units.size()) units.emplace_back();
+                U& x = units[nu++];
+                x.st = st; x.offset = ro.off + uint32_t(sm.sub[st]) * ro.rs; x.ms = ro.rs; x.rb_out = ro.rb;
+                x.em.clear(); x.lines.clear(); x.rows.clear(); x.bk.clear(); x.bk_a.clear();
                 stripe += ro.rs;
             }
             if (stripe != p->x_cols[lb_out]) throw std::runtime_error("heff plan: cohort stripe differs from the block width");
-            // per (input state, unit): R cohort, T job and slice geometry
+            // per (input state, unit): R cohort and slice-id base of its T job
             std::vector<int> unit_of(nst, -1);
-            for (std::size_t k = 0; k < units.size(); ++k) unit_of[units[k].st] = int(k);
-            const std::size_t nu = units.size();
-            std::vector<uint32_t> cir_t(std::size_t(nst) * nu, NONE), job_t(std::size_t(nst) * nu, NONE), rsin_t(nst, 0);
+            for (std::size_t k = 0; k < nu; ++k) unit_of[units[k].st] = int(k);
+            std::vector<WGenInD> gin(std::size_t(nst) * nu, WGenInD{NONE, NONE});
+            std::vector<uint32_t> rsin_t(nst, 0);
             for (uint32_t sti = 0; sti < nst; ++sti) {
                 const RSec& ri = rsec[std::size_t(lb_in) * nps + sm.sector[sti]];
                 if (ri.rb == NONE) continue;
                 rsin_t[sti] = ri.rs;
                 for (std::size_t k = 0; k < nu; ++k) {
-                    cir_t[sti * nu + k] = Rci[std::size_t(ri.rb) * nr + units[k].rb_out];
-                    job_t[sti * nu + k] = tj[std::size_t(sti) * nr + units[k].rb_out];
+                    const uint32_t cir = Rci[std::size_t(ri.rb) * nr + units[k].rb_out];
+                    const uint32_t job = tj[std::size_t(sti) * nr + units[k].rb_out];
+                    if (cir != NONE && job != NONE) gin[sti * nu + k] = WGenInD{cir, job_pos0[job]};
                 }
             }
-            const int64_t* Roff = R.offsets.data();
-            const double* Rcs = R.cscale.data();
+            const int32_t* Rpos = p->r_pos.data();
             const std::size_t Raux = R.aux;
             std::size_t n_alpha = 0;
             for (uint32_t b1 = 0; b1 < W.rows; ++b1) {
                 if (!L.has_block(ci, b1)) continue;
                 const uint32_t bpos = uint32_t(L.offset(ci, b1) / (int64_t(ls_in) * ls_out));
-                const double lsc = L.conj_scale(ci, b1);
                 for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
                     const uint32_t b2 = W.b2[e], op = W.op[e];
-                    const double wsc = W.scale[e] * lsc;
                     for (uint32_t k = optr[op]; k < optr[op + 1]; ++k) {
                         const int u = unit_of[oout[k]];
                         if (u < 0) continue;
                         const uint32_t sti = oin[k];
-                        const uint32_t cir = cir_t[sti * nu + u];
-                        if (cir == NONE) continue;
-                        const int64_t roff = Roff[cir * Raux + b2];
-                        if (roff < 0) continue;
-                        const uint32_t job = job_t[sti * nu + u];
-                        if (job == NONE) continue;
+                        const WGenInD g = gin[sti * nu + u];
+                        if (g.cir == NONE) continue;
+                        const int32_t pos = Rpos[g.cir * Raux + b2];
+                        if (pos < 0) continue;
                         U& un = units[u];
-                        const uint32_t col = uint32_t(roff / rsin_t[sti]);
-                        if (un.lines.empty() || un.lines.back() != bpos) un.lines.push_back(bpos);
-                        un.em.push_back(Em{uint32_t(un.lines.size() - 1), job_pos0[job] + col / un.ms,
-                                           oval[k] * Rcs[cir * Raux + b2] * wsc, P.tjob_mps[job], cir, col});
+                        if (un.lines.empty() || un.lines.back() != bpos) { un.lines.push_back(bpos); un.rows.push_back(b1); }
+                        un.em.push_back(LKD{uint32_t(un.lines.size() - 1), g.jbase + uint32_t(pos)});
+                        if (bookkeeping) {
+                            const uint32_t col = uint32_t(R.offset(g.cir, b2) / rsin_t[sti]);
+                            const uint32_t job = tj[std::size_t(sti) * nr + un.rb_out];
+                            const uint32_t row[3] = {P.tjob_mps[job], g.cir, col};
+                            un.bk.insert(un.bk.end(), row, row + 3);
+                            un.bk_a.push_back(oval[k] * R.conj_scale(g.cir, b2) * (W.scale[e] * L.conj_scale(ci, b1)));
+                        }
                         ++n_alpha;
                     }
                 }
             }
             if (n_alpha == 0) continue;
+            P.n_alpha += n_alpha;
             const uint64_t s_off = P.s_len;
             P.s_len += (uint64_t(K_c) * stripe + 31) / 32 * 32;
-            for (U& u : units) {
+            for (std::size_t ui = 0; ui < nu; ++ui) {
+                U& u = units[ui];
                 P.flops_s += 2.0 * ls_in * u.ms * double(u.em.size());
                 if (u.em.empty()) continue;
                 // number the unit's slices in first-use order
-                std::vector<uint32_t> slices;
-                for (Em& m : u.em) {
-                    uint32_t& sl = slot[m.slice];
-                    if (sl == NONE) { sl = uint32_t(slices.size()); slices.push_back(m.slice); }
+                slices.clear();
+                for (LKD& m : u.em) {
+                    uint32_t& sl = slot[m.k];
+                    if (sl == NONE) { sl = uint32_t(slices.size()); slices.push_back(m.k); }
+                    m.k = sl;
                 }
+                for (uint32_t gp : slices) slot[gp] = NONE;
                 UnitD ud{};
                 ud.s_off = s_off + uint64_t(u.offset) * K_c;
                 ud.line_stride = ls_in; ud.erows = ls_in; ud.col_stride = K_c; ud.ne = ls_in * u.ms;
                 ud.nl = uint32_t(u.lines.size()); ud.line0 = uint32_t(P.line_b1.size());
                 ud.nk = uint32_t(slices.size()); ud.slice0 = uint32_t(P.slice_off.size());
-                ud.sptr0 = uint32_t(P.sptr.size());
                 ud.w_off = P.w_len;
                 P.w_len += uint64_t(ud.nl) * ud.nk;
-                P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
                 for (uint32_t gp : slices) {
-                    // slot -> (job, b2 position) -> T offset of the slice
+                    // slice id -> (job, b2 position) -> T offset of the slice
                     uint32_t job = uint32_t(std::upper_bound(job_pos0.begin(), job_pos0.end(), gp) - job_pos0.begin()) - 1;
                     uint32_t pos = gp - job_pos0[job];
                     P.slice_off.push_back(P.tjobs[job].c_off + uint64_t(pos) * u.ms * ls_in);
                 }
-                // entries sorted by slice, duplicates of (line, slice) summed
-                std::vector<WEntD> ents;
-                ents.reserve(u.em.size());
-                for (Em& m : u.em) ents.push_back(WEntD{m.line, slot[m.slice], m.a});
-                pack_unit_entries(std::move(ents), ud.nk, P.went, P.sptr);
+                // coefficient generation: (slice id, slot) pairs sorted by id, input-state table
+                WGenUnitD wg{};
+                wg.w_off = ud.w_off; wg.ci = ci; wg.st_out = u.st;
+                wg.line0 = ud.line0; wg.nl = ud.nl; wg.map0 = uint32_t(P.smap_id.size()); wg.nk = ud.nk;
+                order.resize(slices.size());
+                for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
+                std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return slices[x] < slices[y]; });
+                for (uint32_t i : order) { P.smap_id.push_back(slices[i]); P.smap_slot.push_back(i); }
+                for (uint32_t sti = 0; sti < nst; ++sti) P.wgin.push_back(gin[sti * nu + ui]);
+                P.wgunits.push_back(wg);
                 if (bookkeeping)
-                    for (Em& m : u.em) {
-                        uint32_t row[10] = {lb_in, lb_out, ci, ce, u.offset, u.ms, u.lines[m.line], m.mps, m.cir, m.col};
+                    for (std::size_t i = 0; i < u.em.size(); ++i) {
+                        uint32_t row[10] = {lb_in, lb_out, ci, ce, u.offset, u.ms, u.lines[u.em[i].line],
+                                            u.bk[3 * i], u.bk[3 * i + 1], u.bk[3 * i + 2]};
                         P.bk_int.insert(P.bk_int.end(), row, row + 10);
-                        P.bk_alpha.push_back(m.a);
+                        P.bk_alpha.push_back(u.bk_a[i]);
                     }
-                for (uint32_t gp : slices) slot[gp] = NONE;
+                P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
+                P.line_row.insert(P.line_row.end(), u.rows.begin(), u.rows.end());
+                // S-GEMM tiles of the unit and the tensor work they execute
+                const std::size_t tb[4] = {P.utiles[0].size(), P.utiles[1].size(), P.utiles[2].size(), P.utiles[3].size()};
+                add_unit_tiles(ud, uint32_t(P.units.size()), u.em.data(), u.em.size(), P.utiles, P.klist);
+                for (int sh = 0; sh < N_SHAPES; ++sh)
+                    for (std::size_t t = tb[sh]; t < P.utiles[sh].size(); ++t) {
+                        const uint32_t o = P.utiles[sh][t].pad;
+                        uint32_t g = 0;
+                        for (uint32_t i = 0; i < P.klist[o]; ++i) g += __builtin_popcount(P.klist[o + 1 + i] & 15u);
+                        P.flops_sexec += 2.0 * 4.0 * g * shape_bm(sh) * shape_bn(sh);
+                    }
                 P.units.push_back(ud);
                 P.g_elems += uint64_t(ud.ne) * ud.nl;
                 P.g_reads += uint64_t(ud.ne) * u.em.size();
@@ -336,26 +424,37 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             P.segs.push_back({lb_out, sg});
         }
     }
+    }
 
     const double t_b = tnow();
     // ---- merge the parts in ket-sector order: prefix offsets, one allocation, parallel copy ----
-    struct Base { uint64_t t, s, w; uint32_t job, unit, line, slice, sptr, went; std::size_t bk; };
+    struct Base { uint64_t t, s, w, na; uint32_t job, unit, line, slice, smap, kl; std::size_t bk; std::size_t tile[N_SHAPES]; };
     std::vector<Base> base(nl + 1);
-    base[0] = Base{0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    base[0] = Base{};
     for (uint32_t i = 0; i < nl; ++i) {
         const Part& P = parts[i];
-        base[i + 1] = Base{base[i].t + P.t_len, base[i].s + P.s_len, base[i].w + P.w_len, base[i].job + uint32_t(P.tjobs.size()),
-                           base[i].unit + uint32_t(P.units.size()), base[i].line + uint32_t(P.line_b1.size()),
-                           base[i].slice + uint32_t(P.slice_off.size()), base[i].sptr + uint32_t(P.sptr.size()),
-                           base[i].went + uint32_t(P.went.size()), base[i].bk + P.bk_alpha.size()};
+        const Base& b = base[i];
+        Base& n = base[i + 1];
+        n = Base{b.t + P.t_len, b.s + P.s_len, b.w + P.w_len, b.na + P.n_alpha, b.job + uint32_t(P.tjobs.size()),
+                 b.unit + uint32_t(P.units.size()), b.line + uint32_t(P.line_b1.size()),
+                 b.slice + uint32_t(P.slice_off.size()), b.smap + uint32_t(P.smap_id.size()),
+                 b.kl + uint32_t(P.klist.size()), b.bk + P.bk_alpha.size(), {}};
+        for (int sh = 0; sh < N_SHAPES; ++sh) n.tile[sh] = b.tile[sh] + P.utiles[sh].size();
+        p->flops_sexec += P.flops_sexec;
     }
     const Base& tot = base[nl];
     p->tjobs.resize(tot.job);
     p->units.resize(tot.unit);
+    p->wgunits.resize(tot.unit);
+    p->wgin.resize(std::size_t(tot.unit) * nst);
     p->line_b1.resize(tot.line);
+    p->line_row.resize(tot.line);
     p->slice_off.resize(tot.slice);
-    p->sptr.resize(tot.sptr);
-    p->went.resize(tot.went);
+    p->smap_id.resize(tot.smap);
+    p->smap_slot.resize(tot.smap);
+    p->klist.resize(tot.kl);
+    p->n_alpha = tot.na;
+    for (int sh = 0; sh < N_SHAPES; ++sh) p->utiles[sh].resize(tot.tile[sh]);
     if (bookkeeping) { p->bk_int.resize(tot.bk * 10); p->bk_alpha.resize(tot.bk); }
 #pragma omp parallel for schedule(dynamic, 1)
     for (int ii = 0; ii < int(nl); ++ii) {
@@ -364,20 +463,34 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         for (std::size_t k = 0; k < P.tjobs.size(); ++k) { TJobD j = P.tjobs[k]; j.c_off += B.t; p->tjobs[B.job + k] = j; }
         for (std::size_t k = 0; k < P.units.size(); ++k) {
             UnitD u = P.units[k];
-            u.s_off += B.s; u.line0 += B.line; u.slice0 += B.slice; u.sptr0 += B.sptr; u.w_off += B.w;
+            u.s_off += B.s; u.line0 += B.line; u.slice0 += B.slice; u.w_off += B.w;
             p->units[B.unit + k] = u;
+            WGenUnitD g = P.wgunits[k];
+            g.w_off += B.w; g.line0 += B.line; g.map0 += B.smap;
+            p->wgunits[B.unit + k] = g;
         }
+        std::copy(P.wgin.begin(), P.wgin.end(), p->wgin.begin() + std::size_t(B.unit) * nst);
         std::copy(P.line_b1.begin(), P.line_b1.end(), p->line_b1.begin() + B.line);
+        std::copy(P.line_row.begin(), P.line_row.end(), p->line_row.begin() + B.line);
         for (std::size_t k = 0; k < P.slice_off.size(); ++k) p->slice_off[B.slice + k] = P.slice_off[k] + B.t;
-        for (std::size_t k = 0; k < P.sptr.size(); ++k) p->sptr[B.sptr + k] = P.sptr[k] + B.went;
-        std::copy(P.went.begin(), P.went.end(), p->went.begin() + B.went);
+        std::copy(P.smap_id.begin(), P.smap_id.end(), p->smap_id.begin() + B.smap);
+        std::copy(P.smap_slot.begin(), P.smap_slot.end(), p->smap_slot.begin() + B.smap);
         if (bookkeeping) {
             std::copy(P.bk_int.begin(), P.bk_int.end(), p->bk_int.begin() + B.bk * 10);
             std::copy(P.bk_alpha.begin(), P.bk_alpha.end(), p->bk_alpha.begin() + B.bk);
         }
+        std::copy(P.klist.begin(), P.klist.end(), p->klist.begin() + B.kl);
+        for (int sh = 0; sh < N_SHAPES; ++sh)
+            for (std::size_t k = 0; k < P.utiles[sh].size(); ++k) {
+                TileD t = P.utiles[sh][k];
+                t.item += B.unit; t.pad += B.kl;
+                p->utiles[sh][B.tile[sh] + k] = t;
+            }
         for (auto& sg : P.segs) sg.second.s_off += B.s;
-        P.tjobs = {}; P.tjob_mps = {}; P.units = {}; P.line_b1 = {}; P.slice_off = {}; P.sptr = {}; P.went = {};
-        P.bk_int = {}; P.bk_alpha = {};
+        for (int sh = 0; sh < N_SHAPES; ++sh) P.utiles[sh] = {};
+        P.klist = {};
+        P.tjobs = {}; P.tjob_mps = {}; P.units = {}; P.wgunits = {}; P.wgin = {}; P.line_b1 = {}; P.line_row = {}; P.slice_off = {};
+        P.smap_id = {}; P.smap_slot = {}; P.bk_int = {}; P.bk_alpha = {};
     }
     p->t_len = tot.t;
     p->s_len = tot.s;
@@ -391,32 +504,6 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     }
     for (uint32_t j = 0; j < p->tjobs.size(); ++j)
         if (p->tjobs[j].M && p->tjobs[j].N) add_tiles(p->ttiles, j, p->tjobs[j].M, p->tjobs[j].N);
-    {
-        // S-GEMM tiles and their non-empty k-steps, per unit in parallel, then concatenated in unit order
-        const std::size_t nu = p->units.size();
-        struct UT { std::vector<TileD> t[N_SHAPES]; std::vector<uint16_t> kl; };
-        std::vector<UT> ut(nu);
-#pragma omp parallel for schedule(dynamic, 16)
-        for (long long kk = 0; kk < (long long)nu; ++kk) {
-            const UnitD& u = p->units[kk];
-            const uint32_t e0 = p->sptr[u.sptr0], e1 = p->sptr[u.sptr0 + u.nk];
-            add_unit_tiles(u, uint32_t(kk), p->went.data() + e0, e1 - e0, ut[kk].t, ut[kk].kl);
-        }
-        for (std::size_t k = 0; k < nu; ++k) {
-            const uint32_t kb = uint32_t(p->klist.size());
-            for (int sh = 0; sh < N_SHAPES; ++sh)
-                for (TileD t : ut[k].t[sh]) {
-                    for (uint32_t i = 0; i < ut[k].kl[t.pad]; ++i) {
-                        const uint16_t e = ut[k].kl[t.pad + 1 + i];
-                        p->flops_sexec += 2.0 * 4.0 * (((e & 1) + ((e >> 1) & 1) + ((e >> 2) & 1) + ((e >> 3) & 1))) *
-                                          shape_bm(sh) * shape_bn(sh);
-                    }
-                    t.pad += kb;
-                    p->utiles[sh].push_back(t);
-                }
-            p->klist.insert(p->klist.end(), ut[k].kl.begin(), ut[k].kl.end());
-        }
-    }
     // output blocks, their segments (lb_in order) and split-K items
     for (uint32_t lb_out = 0; lb_out < nl; ++lb_out) {
         if (per_out[lb_out].empty()) continue;
@@ -446,47 +533,10 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         }
         p->outs.push_back(o);
     }
-    if (tdbg) {
-        std::fprintf(stderr, "plan: tables+parts %.3f s, merge %.3f s\n", t_b - t_a, tnow() - t_b);
-        // S-build unit shapes: useful (nalpha), dense (nl*nk) and tile-padded work
-        double w_alpha = 0, w_dense = 0, w_pad = 0;
-        uint64_t hist_nl[8] = {0}, hist_nk[8] = {0};
-        double fl_nl[8] = {0}, fl_nk[8] = {0};
-        auto bin = [](uint32_t v) { int b = 0; while (b < 7 && v > (4u << b)) ++b; return b; };  // <=4,8,...,256,>256
-        for (const UnitD& u : p->units) {
-            const uint32_t na = p->sptr[u.sptr0 + u.nk] - p->sptr[u.sptr0];
-            const int sh = shape_for_rows(u.nl);
-            const double bm = shape_bm(sh), bn = shape_bn(sh);
-            w_alpha += 2.0 * na * u.ne;
-            w_dense += 2.0 * u.nl * double(u.nk) * u.ne;
-            w_pad += 2.0 * std::ceil(u.nl / bm) * bm * std::ceil(u.nk / 16.0) * 16.0 * std::ceil(u.ne / bn) * bn;
-            hist_nl[bin(u.nl)]++; hist_nk[bin(u.nk)]++;
-            fl_nl[bin(u.nl)] += 2.0 * u.nl * double(u.nk) * u.ne;
-            fl_nk[bin(u.nk)] += 2.0 * u.nl * double(u.nk) * u.ne;
-        }
-        std::fprintf(stderr, "plan: %zu units, %zu coefficients, %zu S tiles, S work alpha %.3e dense %.3e padded %.3e flop\n",
-                     p->units.size(), p->went.size(), p->utiles[0].size() + p->utiles[1].size() + p->utiles[2].size() + p->utiles[3].size(),
-                     w_alpha, w_dense, w_pad);
-        // k-step occupancy of the coefficient tiles: work if all-zero (BM x 16) blocks were skipped
-        for (int bmq : {16, 32, 64, 128}) {
-            double w_skip = 0, w_full = 0;
-            for (const UnitD& u : p->units) {
-                const uint32_t nmt = (u.nl + bmq - 1) / bmq, nks = (u.nk + 15) / 16;
-                std::vector<uint8_t> occ(std::size_t(nmt) * nks, 0);
-                for (uint32_t w = p->sptr[u.sptr0]; w < p->sptr[u.sptr0 + u.nk]; ++w)
-                    occ[std::size_t(p->went[w].line / bmq) * nks + p->went[w].k / 16] = 1;
-                std::size_t on = 0;
-                for (uint8_t o : occ) on += o;
-                w_skip += 2.0 * on * bmq * 16.0 * u.ne;
-                w_full += 2.0 * nmt * bmq * nks * 16.0 * u.ne;
-            }
-            std::fprintf(stderr, "  BM %3d: padded (lines, slices) work %.3e, nonzero-block work %.3e (%.2f)\n", bmq, w_full, w_skip,
-                         w_skip / w_full);
-        }
-        for (int b = 0; b < 8; ++b)
-            std::fprintf(stderr, "  bin <=%u: nl units %llu (dense flop %.2e) | nk units %llu (dense flop %.2e)\n", 4u << b,
-                         (unsigned long long)hist_nl[b], fl_nl[b], (unsigned long long)hist_nk[b], fl_nk[b]);
-    }
+    if (tdbg)
+        std::fprintf(stderr, "plan: tables+parts %.3f s, merge %.3f s; %zu units, %llu coefficient terms, %zu S tiles, "
+                     "%.3e dense coefficients\n", t_b - t_a, tnow() - t_b, p->units.size(), (unsigned long long)p->n_alpha,
+                     p->utiles[0].size() + p->utiles[1].size() + p->utiles[2].size() + p->utiles[3].size(), double(p->w_len));
     uint64_t pl = 0;
     for (int sh = 0; sh < N_SHAPES; ++sh) pl = std::max<uint64_t>(pl, uint64_t(p->kitems[sh].size()) * shape_bm(sh) * shape_bn(sh));
     p->p_len = pl;
