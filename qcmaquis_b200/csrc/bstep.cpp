@@ -95,23 +95,30 @@ struct BPart {
     std::vector<Coh> coh;
 };
 
-struct Ent { uint32_t line_key; uint64_t slice; double a; };
+// One cohort's terms of one unit: lines = distinct MPO line indices in visiting order (they
+// ascend), terms = (local line, slice id)
+struct UnitTerms {
+    std::vector<uint32_t> majors, rows;
+    std::vector<LKD> em;
+    void clear() { majors.clear(); rows.clear(); em.clear(); }
+    void add(uint32_t major, uint32_t id) {
+        if (majors.empty() || majors.back() != major) majors.push_back(major);
+        em.push_back(LKD{uint32_t(majors.size() - 1), id});
+    }
+};
 
-// Units of one cohort -> SBuild (lines = finalize positions)
+// Units of one cohort -> SBuild; S row block of a line = pos[its MPO index] (finalize positions)
 void emit_units(BPart& P, const std::vector<uint32_t>& pos, uint64_t s_off, const std::vector<uint64_t>& unit_off,
-                uint64_t line_stride, const std::vector<uint32_t>& erows, uint32_t col_stride,
-                const std::vector<uint32_t>& ne, std::vector<std::vector<Ent>>& em) {
-    for (std::size_t u = 0; u < em.size(); ++u) {
-        if (em[u].empty()) continue;
-        std::vector<uint32_t> lines;
-        std::vector<SBuild::E> ents;
-        ents.reserve(em[u].size());
-        for (const Ent& x : em[u]) {
-            const uint32_t p = pos[x.line_key];
-            if (lines.empty() || lines.back() != p) lines.push_back(p);
-            ents.push_back(SBuild::E{uint32_t(lines.size() - 1), x.slice, x.a});
-        }
-        P.sb.add_unit(s_off + unit_off[u], line_stride, erows[u], col_stride, ne[u], lines, ents);
+                uint64_t line_stride, const std::vector<uint32_t>& erows, uint32_t col_stride, const std::vector<uint32_t>& ne,
+                const std::vector<uint32_t>& ust, std::vector<UnitTerms>& ut, const std::vector<WGenInD>& gin, uint32_t nst,
+                std::vector<uint32_t>& slot, const JobSlices& js) {
+    for (std::size_t u = 0; u < ust.size(); ++u) {
+        UnitTerms& x = ut[u];
+        if (x.em.empty()) continue;
+        x.rows.resize(x.majors.size());
+        for (std::size_t l = 0; l < x.majors.size(); ++l) x.rows[l] = pos[x.majors[l]];
+        P.sb.add_unit(s_off + unit_off[u], line_stride, erows[u], col_stride, ne[u], ust[u], x.rows, x.majors, x.em, slot, js,
+                      &gin[u * nst]);
     }
 }
 
@@ -121,20 +128,24 @@ template <class Part>
 void merge_sbuilds(std::vector<Part>& parts, SBuild& dst, const std::vector<uint64_t>& t_base,
                    const std::vector<uint64_t>& s_base) {
     const std::size_t np = parts.size();
-    struct B { std::size_t unit, line, slice, sptr, went, kl; uint64_t w; std::size_t tile[N_SHAPES]; };
+    const uint32_t nst = dst.cg.nst;
+    struct B { std::size_t unit, line, slice, smap, kl; uint64_t w; std::size_t tile[N_SHAPES]; };
     std::vector<B> base(np + 1);
     base[0] = B{};
     for (std::size_t i = 0; i < np; ++i) {
         const SBuild& x = parts[i].sb;
         B b = base[i];
-        b.unit += x.units.size(); b.line += x.line_b1.size(); b.slice += x.slice_off.size(); b.sptr += x.sptr.size();
-        b.went += x.went.size(); b.kl += x.klist.size(); b.w += x.w_len;
+        b.unit += x.units.size(); b.line += x.line_b1.size(); b.slice += x.slice_off.size(); b.smap += x.cg.smap_id.size();
+        b.kl += x.klist.size(); b.w += x.w_len;
         for (int k = 0; k < N_SHAPES; ++k) b.tile[k] += x.utiles[k].size();
         base[i + 1] = b;
     }
     const B& tot = base[np];
-    dst.units.resize(tot.unit); dst.line_b1.resize(tot.line); dst.slice_off.resize(tot.slice); dst.sptr.resize(tot.sptr);
-    dst.went.resize(tot.went); dst.klist.resize(tot.kl); dst.w_len = tot.w;
+    dst.units.resize(tot.unit); dst.line_b1.resize(tot.line); dst.slice_off.resize(tot.slice);
+    dst.klist.resize(tot.kl); dst.w_len = tot.w;
+    CoefGen& cg = dst.cg;
+    cg.units.resize(tot.unit); cg.gin.resize(tot.unit * nst); cg.line_major.resize(tot.line); cg.line_scale.resize(tot.line);
+    cg.smap_id.resize(tot.smap); cg.smap_slot.resize(tot.smap); cg.w_len = tot.w;
     for (int k = 0; k < N_SHAPES; ++k) dst.utiles[k].resize(tot.tile[k]);
 #pragma omp parallel for schedule(dynamic, 1)
     for (long long ii = 0; ii < (long long)np; ++ii) {
@@ -142,14 +153,19 @@ void merge_sbuilds(std::vector<Part>& parts, SBuild& dst, const std::vector<uint
         const B& b = base[ii];
         for (std::size_t k = 0; k < x.units.size(); ++k) {
             UnitD u = x.units[k];
-            u.s_off += s_base[ii]; u.line0 += uint32_t(b.line); u.slice0 += uint32_t(b.slice); u.sptr0 += uint32_t(b.sptr);
-            u.w_off += b.w;
+            u.s_off += s_base[ii]; u.line0 += uint32_t(b.line); u.slice0 += uint32_t(b.slice); u.w_off += b.w;
             dst.units[b.unit + k] = u;
+            WGenUnitD g = x.cg.units[k];
+            g.w_off += b.w; g.line0 += uint32_t(b.line); g.map0 += uint32_t(b.smap);
+            cg.units[b.unit + k] = g;
         }
+        std::copy(x.cg.gin.begin(), x.cg.gin.end(), cg.gin.begin() + b.unit * nst);
+        std::copy(x.cg.line_major.begin(), x.cg.line_major.end(), cg.line_major.begin() + b.line);
+        std::copy(x.cg.line_scale.begin(), x.cg.line_scale.end(), cg.line_scale.begin() + b.line);
+        std::copy(x.cg.smap_id.begin(), x.cg.smap_id.end(), cg.smap_id.begin() + b.smap);
+        std::copy(x.cg.smap_slot.begin(), x.cg.smap_slot.end(), cg.smap_slot.begin() + b.smap);
         std::copy(x.line_b1.begin(), x.line_b1.end(), dst.line_b1.begin() + b.line);
         for (std::size_t k = 0; k < x.slice_off.size(); ++k) dst.slice_off[b.slice + k] = x.slice_off[k] + t_base[ii];
-        for (std::size_t k = 0; k < x.sptr.size(); ++k) dst.sptr[b.sptr + k] = x.sptr[k] + uint32_t(b.went);
-        std::copy(x.went.begin(), x.went.end(), dst.went.begin() + b.went);
         std::copy(x.klist.begin(), x.klist.end(), dst.klist.begin() + b.kl);
         for (int sh = 0; sh < N_SHAPES; ++sh)
             for (std::size_t k = 0; k < x.utiles[sh].size(); ++k) {
@@ -163,42 +179,46 @@ void merge_sbuilds(std::vector<Part>& parts, SBuild& dst, const std::vector<uint
 
 }  // namespace
 
-void SBuild::add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint32_t col_stride, uint32_t ne,
-                      const std::vector<uint32_t>& lines, const std::vector<E>& ents) {
+uint64_t JobSlices::offset(uint32_t id) const {
+    const std::size_t j = std::size_t(std::upper_bound(pos0.begin(), pos0.end(), id) - pos0.begin());
+    if (j == 0 || j >= pos0.size()) throw std::runtime_error("S unit: slice id outside the T jobs");
+    return c_off[j - 1] + uint64_t(id - pos0[j - 1]) * bsize[j - 1];
+}
+
+void SBuild::add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint32_t col_stride, uint32_t ne, uint32_t st_out,
+                      const std::vector<uint32_t>& rows, const std::vector<uint32_t>& majors, std::vector<LKD>& ents,
+                      std::vector<uint32_t>& slot, const JobSlices& js, const WGenInD* in_row) {
     if (ents.empty() || ne == 0) return;
-    // slices numbered in first-use order (open-addressing table keyed by the T offset)
-    std::size_t cap = 16;
-    while (cap < 2 * ents.size()) cap <<= 1;
-    std::vector<uint64_t> key(cap, ~uint64_t(0));
-    std::vector<uint32_t> val(cap);
-    std::vector<uint64_t> slices;
-    std::vector<uint32_t> ek(ents.size());
-    for (std::size_t i = 0; i < ents.size(); ++i) {
-        const uint64_t sl = ents[i].slice;
-        std::size_t h = std::size_t((sl * 0x9E3779B97F4A7C15ull) >> 17) & (cap - 1);
-        while (key[h] != ~uint64_t(0) && key[h] != sl) h = (h + 1) & (cap - 1);
-        if (key[h] == ~uint64_t(0)) { key[h] = sl; val[h] = uint32_t(slices.size()); slices.push_back(sl); }
-        ek[i] = val[h];
+    // slices numbered in first-use order
+    std::vector<uint32_t> slices;
+    for (LKD& e : ents) {
+        uint32_t& sl = slot[e.k];
+        if (sl == NONE) { sl = uint32_t(slices.size()); slices.push_back(e.k); }
+        e.k = sl;
     }
+    for (uint32_t id : slices) slot[id] = NONE;
     UnitD u{};
     u.s_off = s_off; u.line_stride = line_stride; u.erows = erows; u.col_stride = col_stride; u.ne = ne;
-    u.nl = uint32_t(lines.size()); u.line0 = uint32_t(line_b1.size());
-    u.nk = uint32_t(slices.size()); u.slice0 = uint32_t(slice_off.size()); u.sptr0 = uint32_t(sptr.size());
+    u.nl = uint32_t(rows.size()); u.line0 = uint32_t(line_b1.size());
+    u.nk = uint32_t(slices.size()); u.slice0 = uint32_t(slice_off.size());
     u.w_off = w_len;
     w_len += uint64_t(u.nl) * u.nk;
-    line_b1.insert(line_b1.end(), lines.begin(), lines.end());
-    slice_off.insert(slice_off.end(), slices.begin(), slices.end());
-    std::vector<WEntD> es(ents.size());
-    for (std::size_t i = 0; i < ents.size(); ++i) es[i] = WEntD{ents[i].line, ek[i], ents[i].a};
-    pack_unit_entries(std::move(es), u.nk, went, sptr);
-    const uint32_t e0 = sptr[u.sptr0], e1 = sptr[u.sptr0 + u.nk];
-    add_unit_tiles(u, uint32_t(units.size()), went.data() + e0, e1 - e0, utiles, klist);
+    line_b1.insert(line_b1.end(), rows.begin(), rows.end());
+    for (uint32_t id : slices) slice_off.push_back(js.offset(id));
+    const std::vector<double> ones(u.nl, 1.0);
+    cg.add_unit(u.w_off, st_out, majors.data(), ones.data(), u.nl, slices, in_row);
+    add_unit_tiles(u, uint32_t(units.size()), ents.data(), ents.size(), utiles, klist);
     units.push_back(u);
 }
 
 void SBuild::validate(uint64_t t_len, uint64_t s_len) const {
-    for (const UnitD& u : units) {
+    if (cg.units.size() != units.size() || cg.w_len != w_len) throw std::runtime_error("S build: coefficient tables differ from the units");
+    for (std::size_t i = 0; i < units.size(); ++i) {
+        const UnitD& u = units[i];
         if (!u.ne || !u.nl) continue;
+        const WGenUnitD& g = cg.units[i];
+        if (g.w_off != u.w_off || g.nl != u.nl || g.nk != u.nk || g.line0 != u.line0)
+            throw std::runtime_error("S build: coefficient unit differs from its S unit");
         if (u.w_off + uint64_t(u.nl) * u.nk > w_len) throw std::runtime_error("device work list out of bounds: coefficient block");
         if (u.erows == 0 || u.ne % u.erows) throw std::runtime_error("S unit: element count is not a whole number of columns");
         uint32_t maxline = 0;
@@ -207,8 +227,6 @@ void SBuild::validate(uint64_t t_len, uint64_t s_len) const {
         if (last >= s_len) throw std::runtime_error("device work list out of bounds: S unit");
         for (uint32_t k = 0; k < u.nk; ++k)
             if (slice_off[u.slice0 + k] + u.ne > t_len) throw std::runtime_error("device work list out of bounds: T slice");
-        for (uint32_t w = sptr[u.sptr0]; w < sptr[u.sptr0 + u.nk]; ++w)
-            if (went[w].line >= u.nl || went[w].k >= u.nk) throw std::runtime_error("S unit: coefficient index out of range");
     }
     for (int sh = 0; sh < N_SHAPES; ++sh)
         for (const TileD& t : utiles[sh]) {
@@ -224,10 +242,9 @@ void SBuild::upload(cudaStream_t s) {
     d_units.upload(units, s);
     for (int k = 0; k < N_SHAPES; ++k) d_utiles[k].upload(utiles[k], s);
     d_line_b1.upload(line_b1, s);
-    d_sptr.upload(sptr, s);
     d_slice_off.upload(slice_off, s);
-    d_went.upload(went, s);
     d_klist.upload(klist, s);
+    cg.upload(s);
 }
 
 void complement_transpose(BoundaryIndexH& x, const std::vector<int32_t>& herm, const std::vector<int32_t>& phase, bool forward) {
@@ -336,16 +353,30 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
     cohort_tables(R, right, right, Rci, Rce);
     const OpCSR oc(W);
 
+    // coefficient generation: lines iterate MPO rows b1, slices come from R_old cohorts
+    SBuild sb;
+    sb.cg.set_mpo(W, nst, true);
+    sb.cg.set_boundary(R);
+    const int32_t* Rpos = sb.cg.b_pos.data();
+    const std::size_t Raux = R.aux;
+
     std::vector<BPart> parts(nl);
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int lbi = 0; lbi < int(nl); ++lbi) {
+    std::string err;
+#pragma omp parallel
+    {
+    std::vector<UnitTerms> ut;
+#pragma omp for schedule(dynamic, 1)
+    for (int lbi = 0; lbi < int(nl); ++lbi) try {
         const uint32_t lb_ket = uint32_t(lbi);
         if (!kok[lb_ket]) continue;
         BPart& P = parts[lb_ket];
+        P.sb.cg.nst = nst;
         const Charge lc_ket = left[lb_ket].first;
         const uint32_t ls_ket = uint32_t(left[lb_ket].second);
-        // T jobs (rshtm_t_tasks): one per (input state, bra right sector)
+        // T jobs (rshtm_t_tasks): one per (input state, bra right sector); slice ids per R block
         std::vector<uint32_t> tj(std::size_t(nst) * nr, NONE);
+        JobSlices js;
+        std::vector<uint32_t> tj_first, tj_count;
         for (uint32_t st = 0; st < nst; ++st) {
             const RSec& ri = rsec[std::size_t(lb_ket) * nps + sm.sector[st]];
             if (ri.rb == NONE) continue;
@@ -360,10 +391,13 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
                 j.M = ls_ket; j.K = ri.rs; j.brs = R.rsz[ci]; j.N = R.nb[ce] * j.brs; j.lda = ls_ket;
                 j.tr = ci != ce;
                 tj[std::size_t(st) * nr + rbb] = uint32_t(P.tjobs.size());
+                tj_first.push_back(js.add(j.c_off, uint64_t(j.brs) * j.M, R.nb[ce]));
+                tj_count.push_back(R.nb[ce]);
                 P.t_len += (uint64_t(j.M) * j.N + 31) / 32 * 32;
                 P.tjobs.push_back(j);
             }
         }
+        std::vector<uint32_t> slot(js.pos0.back() + 1, NONE);
         // cohorts (rshtm_tasks)
         std::vector<int> unit_of(nst, -1);
         std::vector<uint32_t> line_count(W.rows, 0), pos(W.rows, NONE);
@@ -383,7 +417,23 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
                 uoff.push_back(uint64_t(ro.off + uint32_t(sm.sub[st]) * ro.rs));
                 uer.push_back(ls_ket); une.push_back(ls_ket * ro.rs);
             }
-            std::vector<std::vector<Ent>> em(ust.size());
+            const std::size_t nu = ust.size();
+            if (ut.size() < nu) ut.resize(nu);
+            for (std::size_t u = 0; u < nu; ++u) ut[u].clear();
+            // (R cohort, first slice id) of each (unit, input state) and its number of blocks
+            std::vector<WGenInD> gin(nu * nst, WGenInD{WGEN_NONE, WGEN_NONE});
+            std::vector<uint32_t> gcnt(nu * nst, 0);
+            for (uint32_t sti = 0; sti < nst; ++sti) {
+                const RSec& ri = rsec[std::size_t(lb_ket) * nps + sm.sector[sti]];
+                if (ri.rb == NONE) continue;
+                for (std::size_t u = 0; u < nu; ++u) {
+                    const uint32_t ci = Rci[std::size_t(ri.rb) * nr + urbb[u]];
+                    const uint32_t job = tj[std::size_t(sti) * nr + urbb[u]];
+                    if (ci == NONE || job == NONE) continue;
+                    gin[u * nst + sti] = WGenInD{ci, tj_first[job]};
+                    gcnt[u * nst + sti] = tj_count[job];
+                }
+            }
             std::fill(line_count.begin(), line_count.end(), 0);
             for (uint32_t b1 = 0; b1 < W.rows; ++b1) {
                 if (symmetric && lc_ket < lc_bra && W.herm_left[b1] >= 0) continue;
@@ -392,16 +442,13 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
                     for (uint32_t k = oc.ptr[o]; k < oc.ptr[o + 1]; ++k) {
                         const int u = unit_of[oc.out[k]];
                         if (u < 0) continue;
-                        const uint32_t sti = oc.in[k];
-                        const RSec& ri = rsec[std::size_t(lb_ket) * nps + sm.sector[sti]];
-                        if (ri.rb == NONE) continue;
-                        const uint32_t ci = Rci[std::size_t(ri.rb) * nr + urbb[u]];
-                        if (ci == NONE || !R.has_block(ci, b2)) continue;
-                        const uint32_t job = tj[std::size_t(sti) * nr + urbb[u]];
-                        if (job == NONE) continue;
-                        const uint64_t col = uint64_t(R.offset(ci, b2)) / ri.rs;
-                        const double a = oc.val[k] * R.conj_scale(ci, b2) * W.scale[e];
-                        em[u].push_back(Ent{b1, P.tjobs[job].c_off + col * ls_ket, a});
+                        const std::size_t gi = std::size_t(u) * nst + oc.in[k];
+                        const WGenInD g = gin[gi];
+                        if (g.c == WGEN_NONE) continue;
+                        const int32_t bp = Rpos[g.c * Raux + b2];
+                        if (bp < 0) continue;
+                        if (uint32_t(bp) >= gcnt[gi]) throw std::runtime_error("boundary_step_right: R block position outside its T job");
+                        ut[u].add(b1, g.jbase + uint32_t(bp));
                         line_count[b1]++;
                     }
                 }
@@ -414,19 +461,23 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
             const uint64_t s_off = P.s_len;
             P.s_len += (uint64_t(K_c) * kcols[lb_bra] + 31) / 32 * 32;
             for (auto& x : uoff) x *= K_c;
-            emit_units(P, pos, s_off, uoff, ls_ket, uer, K_c, une, em);
+            emit_units(P, pos, s_off, uoff, ls_ket, uer, K_c, une, ust, ut, gin, nst, slot, js);
             BPart::Coh ch{lb_ket, lb_bra, nS, s_off, std::vector<int64_t>(W.rows, -1)};
             for (uint32_t b1 = 0; b1 < W.rows; ++b1)
                 if (pos[b1] != NONE) ch.offs[b1] = int64_t(pos[b1]) * ls_ket * ls_bra;
             P.coh.push_back(std::move(ch));
         }
+    } catch (const std::exception& e) {
+#pragma omp critical
+        err = e.what();
     }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
 
     const double tbp = step_now();
     // merge in ket-sector order; new index (BoundaryIndex(ket_left_i, bra_left_i))
     std::vector<TJobD> tjobs;
     std::vector<TileD> ttiles[N_SHAPES];
-    SBuild sb;
     uint64_t t_len = 0, s_len = 0;
     BoundaryIndexH nidx;
     nidx.bra = left; nidx.ket = left; nidx.aux = W.rows;
@@ -486,7 +537,7 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
     run_tgemm(c.tjobs.get(), c.ttiles, ttiles, ket.b.d.get(), Rold.data.get(), c.T.get(), c.s);
     if (s_len) QCM_CUDA(cudaMemsetAsync(c.S.get(), 0, s_len * sizeof(double), c.s));
     Ctx::ensure(c.W, sb.w_len ? sb.w_len : 1);
-    fill_coefficients(sb.d_units.get(), uint32_t(sb.units.size()), sb.d_sptr.get(), sb.d_went.get(), c.W.get(), sb.w_len, c.s);
+    sb.cg.generate(c.W.get(), c.s);
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
               c.T.get(), c.S.get(), c.s);
     if (!dn) {
@@ -567,16 +618,30 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
     cohort_tables(L, left, left, Lci, Lce);
     const OpCSR oc(W);
 
+    // coefficient generation: lines iterate MPO columns b2, slices come from L_old cohorts
+    SBuild sb;
+    sb.cg.set_mpo(W, nst, false);
+    sb.cg.set_boundary(L);
+    const int32_t* Lpos = sb.cg.b_pos.data();
+    const std::size_t Laux = L.aux;
+
     std::vector<BPart> parts(nr);
-#pragma omp parallel for schedule(dynamic, 1)
-    for (int rbi = 0; rbi < int(nr); ++rbi) {
+    std::string err;
+#pragma omp parallel
+    {
+    std::vector<UnitTerms> ut;
+#pragma omp for schedule(dynamic, 1)
+    for (int rbi = 0; rbi < int(nr); ++rbi) try {
         const uint32_t rb_ket = uint32_t(rbi);
         BPart& P = parts[rb_ket];
+        P.sb.cg.nst = nst;
         const Charge rc_ket = right[rb_ket].first;
         const uint32_t rs_ket = uint32_t(right[rb_ket].second);
-        // T jobs (lshtm_t_tasks): per (input state, bra left sector), nb GEMMs of ls_bra x rs_ket
+        // T jobs (lshtm_t_tasks): per (input state, bra left sector), nb GEMMs of ls_bra x rs_ket;
+        // slice ids per L block
         std::vector<uint32_t> tj(std::size_t(nst) * nl, NONE);
-        std::vector<uint64_t> tj_off;
+        JobSlices js;
+        std::vector<uint32_t> tj_first, tj_count;
         for (uint32_t st = 0; st < nst; ++st) {
             const LSec& li = lsec[std::size_t(rb_ket) * nps + sm.sector[st]];
             if (li.lb == NONE || !kok[li.lb]) continue;
@@ -587,8 +652,9 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
                 const uint32_t ce = Lce[std::size_t(lb_bra) * nl + li.lb];
                 const uint32_t ls_bra = uint32_t(left[lb_bra].second), nb = L.nb[ce];
                 const uint64_t c_off = P.t_len;
-                tj[std::size_t(st) * nl + lb_bra] = uint32_t(tj_off.size());
-                tj_off.push_back(c_off);
+                tj[std::size_t(st) * nl + lb_bra] = uint32_t(tj_first.size());
+                tj_first.push_back(js.add(c_off, uint64_t(ls_bra) * rs_ket, nb));
+                tj_count.push_back(nb);
                 P.t_len += (uint64_t(ls_bra) * rs_ket * nb + 31) / 32 * 32;
                 if (nb == 0) continue;
                 // all nb blocks of the cohort in one job: A and C row blocks = MPO-index blocks
@@ -601,6 +667,7 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
                 P.tgemm.push_back(g);
             }
         }
+        std::vector<uint32_t> slot(js.pos0.back() + 1, NONE);
         // cohorts (lshtm_tasks)
         std::vector<int> unit_of(nst, -1);
         std::vector<uint32_t> line_count(W.cols, 0), pos(W.cols, NONE);
@@ -619,7 +686,23 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
                 uoff.push_back(uint64_t(lo.boff + uint32_t(sm.sub[st]) * lo.ls));
                 uer.push_back(lo.ls); une.push_back(lo.ls * rs_ket);
             }
-            std::vector<std::vector<Ent>> em(ust.size());
+            const std::size_t nu = ust.size();
+            if (ut.size() < nu) ut.resize(nu);
+            for (std::size_t u = 0; u < nu; ++u) ut[u].clear();
+            // (L cohort, first slice id) of each (unit, input state) and its number of blocks
+            std::vector<WGenInD> gin(nu * nst, WGenInD{WGEN_NONE, WGEN_NONE});
+            std::vector<uint32_t> gcnt(nu * nst, 0);
+            for (uint32_t sti = 0; sti < nst; ++sti) {
+                const LSec& li = lsec[std::size_t(rb_ket) * nps + sm.sector[sti]];
+                if (li.lb == NONE || !kok[li.lb]) continue;
+                for (std::size_t u = 0; u < nu; ++u) {
+                    const uint32_t ci = Lci[std::size_t(ulb[u]) * nl + li.lb];
+                    const uint32_t job = tj[std::size_t(sti) * nl + ulb[u]];
+                    if (ci == NONE || job == NONE) continue;
+                    gin[u * nst + sti] = WGenInD{ci, tj_first[job]};
+                    gcnt[u * nst + sti] = tj_count[job];
+                }
+            }
             std::fill(line_count.begin(), line_count.end(), 0);
             for (uint32_t b2 = 0; b2 < W.cols; ++b2) {
                 if (symmetric && rc_bra < rc_ket && W.herm_right[b2] >= 0) continue;
@@ -628,16 +711,13 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
                     for (uint32_t k = oc.ptr[o]; k < oc.ptr[o + 1]; ++k) {
                         const int u = unit_of[oc.out[k]];
                         if (u < 0) continue;
-                        const uint32_t sti = oc.in[k];
-                        const LSec& li = lsec[std::size_t(rb_ket) * nps + sm.sector[sti]];
-                        if (li.lb == NONE || !kok[li.lb]) continue;
-                        const uint32_t ci = Lci[std::size_t(ulb[u]) * nl + li.lb];
-                        if (ci == NONE || !L.has_block(ci, b1)) continue;
-                        const uint32_t job = tj[std::size_t(sti) * nl + ulb[u]];
-                        if (job == NONE) continue;
-                        const uint64_t col = uint64_t(L.offset(ci, b1)) / li.ls;
-                        const double a = oc.val[k] * L.conj_scale(ci, b1) * W.scale[e];
-                        em[u].push_back(Ent{b2, tj_off[job] + col * rs_ket, a});
+                        const std::size_t gi = std::size_t(u) * nst + oc.in[k];
+                        const WGenInD g = gin[gi];
+                        if (g.c == WGEN_NONE) continue;
+                        const int32_t bp = Lpos[g.c * Laux + b1];
+                        if (bp < 0) continue;
+                        if (uint32_t(bp) >= gcnt[gi]) throw std::runtime_error("boundary_step_left: L block position outside its T job");
+                        ut[u].add(b2, g.jbase + uint32_t(bp));
                         line_count[b2]++;
                     }
                 }
@@ -647,18 +727,22 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
             if (nS == 0) continue;
             const uint64_t s_off = P.s_len;
             P.s_len += (uint64_t(stripe) * nS * rs_ket + 31) / 32 * 32;
-            emit_units(P, pos, s_off, uoff, uint64_t(rs_ket) * stripe, uer, stripe, une, em);
+            emit_units(P, pos, s_off, uoff, uint64_t(rs_ket) * stripe, uer, stripe, une, ust, ut, gin, nst, slot, js);
             BPart::Coh ch{rb_bra, rb_ket, nS, s_off, std::vector<int64_t>(W.cols, -1)};
             for (uint32_t b2 = 0; b2 < W.cols; ++b2)
                 if (pos[b2] != NONE) ch.offs[b2] = int64_t(pos[b2]) * rs_bra * rs_ket;
             P.coh.push_back(std::move(ch));
         }
+    } catch (const std::exception& e) {
+#pragma omp critical
+        err = e.what();
     }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
 
     const double tbp = step_now();
     // merge in ket-sector order; new index (BoundaryIndex(bra_right_i, ket_right_i))
     std::vector<GemmJob> tj_gemm;
-    SBuild sb;
     uint64_t t_len = 0, s_len = 0;
     BoundaryIndexH nidx;
     nidx.bra = right; nidx.ket = right; nidx.aux = W.cols;
@@ -709,7 +793,7 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
     sb.upload(c.s);
     if (s_len) QCM_CUDA(cudaMemsetAsync(c.S.get(), 0, s_len * sizeof(double), c.s));
     Ctx::ensure(c.W, sb.w_len ? sb.w_len : 1);
-    fill_coefficients(sb.d_units.get(), uint32_t(sb.units.size()), sb.d_sptr.get(), sb.d_went.get(), c.W.get(), sb.w_len, c.s);
+    sb.cg.generate(c.W.get(), c.s);
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
               c.T.get(), c.S.get(), c.s);
     if (!dn) {

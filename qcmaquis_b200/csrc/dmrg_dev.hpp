@@ -57,24 +57,39 @@ struct DMPS {
 };
 
 // Work lists of the unit S-GEMM (shared by H_eff and the boundary steps)
+// T slices of a schedule part: job j owns slice ids [pos0[j], pos0[j + 1]); slice id
+// pos0[j] + b starts at T offset c_off[j] + b * bsize[j].
+struct JobSlices {
+    std::vector<uint32_t> pos0{0};
+    std::vector<uint64_t> c_off, bsize;
+    uint32_t add(uint64_t off, uint64_t bs, uint32_t nblocks) {  // returns the job's first id
+        const uint32_t first = pos0.back();
+        pos0.push_back(first + nblocks); c_off.push_back(off); bsize.push_back(bs);
+        return first;
+    }
+    uint64_t offset(uint32_t id) const;
+};
+
 struct SBuild {
     hvec<UnitD> units;
     std::vector<TileD> utiles[N_SHAPES];
-    hvec<uint32_t> line_b1, sptr;
+    hvec<uint32_t> line_b1;  // S row block of each line
     hvec<uint64_t> slice_off;
-    hvec<WEntD> went;
     uint64_t w_len = 0;  // dense coefficient blocks (doubles)
     std::vector<uint16_t> klist;  // non-empty k-steps per S-GEMM m-tile
+    CoefGen cg;  // coefficient generation: per-unit tables here, MPO and boundary tables on the merged build
     DBuf<UnitD> d_units;
     DBuf<uint16_t> d_klist;
     DBuf<TileD> d_utiles[N_SHAPES];
-    DBuf<uint32_t> d_line_b1, d_sptr;
+    DBuf<uint32_t> d_line_b1;
     DBuf<uint64_t> d_slice_off;
-    DBuf<WEntD> d_went;
-    struct E { uint32_t line; uint64_t slice; double a; };
-    // lines[i] = output line position of local line i; entries reference local lines
-    void add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint32_t col_stride, uint32_t ne,
-                  const std::vector<uint32_t>& lines, const std::vector<E>& ents);
+    // One unit: local line i writes S row block rows[i] and iterates MPO index majors[i]; terms
+    // are (local line, slice id) and leave as (local line, slot).  slot is a scratch table over
+    // the part's slice ids, all NONE on entry and on return; in_row = the nst (cohort, id base)
+    // pairs of the unit's input states.
+    void add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint32_t col_stride, uint32_t ne, uint32_t st_out,
+                  const std::vector<uint32_t>& rows, const std::vector<uint32_t>& majors, std::vector<LKD>& ents,
+                  std::vector<uint32_t>& slot, const JobSlices& js, const WGenInD* in_row);
     void upload(cudaStream_t s);
     // throws unless every unit's S writes and T slice reads lie inside [0, s_len) and [0, t_len)
     void validate(uint64_t t_len, uint64_t s_len) const;

@@ -75,12 +75,8 @@ struct UnitD {        // S rows of one cohort unit: S_u (lines x elements) = W_u
     uint32_t line0;        // first entry in line_b1[]
     uint32_t nk;           // distinct T slices referenced
     uint32_t slice0;       // first entry in slice_off[]
-    uint32_t sptr0;        // first of nk + 1 entry pointers in sptr[]
+    uint32_t pad;
     uint64_t w_off;        // dense coefficient block W_u (nl x nk, column-major) in the W buffer
-};
-struct WEntD {        // coefficient alpha at (line, slice) of a unit; entries sorted by slice
-    uint32_t line, k;
-    double a;
 };
 struct SegD {         // K segment of an output block: L cohort (M x nS*ls_in, maybe tile-transposed) times S (ldS = nS*ls_in)
     uint64_t l_off, s_off;
@@ -98,50 +94,6 @@ struct OTileD {       // output tile of the L.S GEMM and its contiguous range of
     uint32_t out, m0, n0, part0, nparts, pad0, pad1, pad2;
 };
 
-// Appends one unit's coefficient entries (line, slice k, alpha) to went, sorted by
-// (slice, line), with entries that share (line, slice) summed in their input order --
-// several MPO terms may couple the same boundary block, input state and output state,
-// and the densified coefficient tile holds their sum -- and the unit's nk + 1 slice
-// pointers to sptr.
-struct PackScratch {  // reusable buffers of pack_unit_entries
-    std::vector<uint32_t> cnt, fill;
-    std::vector<WEntD, NoInitAlloc<WEntD>> sorted;
-};
-template <class WV, class PV>
-inline void pack_unit_entries(const WEntD* ents, std::size_t n, uint32_t nk, WV& went, PV& sptr, PackScratch& sc) {
-    // counting sort by slice; entries arrive in line order, so each slice's lines stay ascending
-    sc.cnt.assign(std::size_t(nk) + 1, 0);
-    for (std::size_t i = 0; i < n; ++i) sc.cnt[ents[i].k + 1]++;
-    for (uint32_t k = 0; k < nk; ++k) sc.cnt[k + 1] += sc.cnt[k];
-    sc.sorted.resize(n);
-    sc.fill.assign(sc.cnt.begin(), sc.cnt.end() - 1);
-    for (std::size_t i = 0; i < n; ++i) sc.sorted[sc.fill[ents[i].k]++] = ents[i];
-    auto by_line = [](const WEntD& x, const WEntD& y) { return x.line < y.line; };
-    for (uint32_t k = 0; k < nk; ++k)  // a slice's lines need not arrive sorted when lines repeat out of order
-        if (!std::is_sorted(sc.sorted.begin() + sc.cnt[k], sc.sorted.begin() + sc.cnt[k + 1], by_line))
-            std::stable_sort(sc.sorted.begin() + sc.cnt[k], sc.sorted.begin() + sc.cnt[k + 1], by_line);
-    const std::size_t w0 = went.size();
-    went.resize(w0 + n);
-    WEntD* out = went.data() + w0;
-    std::size_t m = 0;
-    sptr.push_back(uint32_t(w0));
-    for (uint32_t k = 0; k < nk; ++k) {
-        const std::size_t m0 = m;
-        for (uint32_t i = sc.cnt[k]; i < sc.cnt[k + 1]; ++i) {
-            const WEntD& e = sc.sorted[i];
-            if (m > m0 && out[m - 1].line == e.line) out[m - 1].a += e.a;
-            else out[m++] = e;
-        }
-        sptr.push_back(uint32_t(w0 + m));
-    }
-    went.resize(w0 + m);
-}
-template <class WV, class PV>
-inline void pack_unit_entries(std::vector<WEntD> ents, uint32_t nk, WV& went, PV& sptr) {
-    PackScratch sc;
-    pack_unit_entries(ents.data(), ents.size(), nk, went, sptr, sc);
-}
-
 // DMMA tile shapes (rows x cols of the CTA tile).  GEMM jobs pick the class from their row
 // count (16 x 128, 32 x 128, 64 x 64); S-build units also use 128 x 32 (see add_unit_tiles).
 enum { SHAPE_16 = 0, SHAPE_32 = 1, SHAPE_64 = 2, SHAPE_128 = 3, N_SHAPES = 4 };
@@ -149,31 +101,74 @@ inline int shape_for_rows(uint32_t M) { return M <= 16 ? SHAPE_16 : (M <= 32 ? S
 inline uint32_t shape_bm(int s) { return s == SHAPE_16 ? 16 : (s == SHAPE_32 ? 32 : (s == SHAPE_64 ? 64 : 128)); }
 inline uint32_t shape_bn(int s) { return s == SHAPE_64 ? 64 : (s == SHAPE_128 ? 32 : 128); }
 
+struct LKD { uint32_t line, k; };  // (line, slice) position of one coefficient term
+
 // S-GEMM tiles of one unit.  ents[0..n) are the unit's coefficient entries.  The tile shape
 // is the one with the least tensor work counting only the (BM lines x 4 slices) coefficient
 // groups that hold an entry; every m-tile's non-empty k-steps go to klist as (count, steps...),
 // a step being (k-step index << 4 | mask of its non-empty 4-slice groups), and its tiles carry
 // that list's offset in TileD::pad.
-// E is any entry type with members line and k (WEntD, LKD).
-template <class E>
-void add_unit_tiles(const UnitD& u, uint32_t item, const E* ents, std::size_t n, std::vector<TileD>* utiles,
+void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t n, std::vector<TileD>* utiles,
                     std::vector<uint16_t>& klist);
 
-struct LKD { uint32_t line, k; };  // (line, slice) position of one coefficient term
 
-// Coefficient generation of one S unit on the device: every term of line l (MPO row
-// b1 = line_row[line0 + l]) is alpha = op value * R conj scale * MPO scale * L conj scale,
-// summed into W[w_off + l + slot * nl]; the term's slice id (T slice numbering of the ket
-// sector) maps to its slot through the unit's (slice id, slot) pairs sorted by id.
+// Dense coefficient blocks W_u of S units, computed on the device (k_wgen).  Line l of a
+// unit iterates the MPO entries of its line index m = line_major[line0 + l] (a row b1 or a
+// column b2, depending on how m_ptr groups the entries), and every operator term of an entry
+// with the unit's output state adds
+//     alpha = op value * boundary conj scale(c, x) * (MPO scale * line_scale[line0 + l])
+// at W[w_off + l + slot * nl], where x is the entry's other MPO index, c the boundary cohort
+// of (unit, input state), and slot the unit's slot of slice id jbase(unit, input state) +
+// block position of x in cohort c.  Terms of one line are summed in entry, then operator-term
+// order by one thread, with products and sums rounded separately.
 struct WGenUnitD {
     uint64_t w_off;
-    uint32_t ci;       // L cohort (conj scale row)
     uint32_t st_out;   // output physical state of the unit
     uint32_t line0, nl;
     uint32_t map0, nk;  // sorted (slice id, slot) pairs at smap_id/smap_slot[map0 .. map0 + nk)
+    uint32_t pad;
 };
-struct WGenInD { uint32_t cir, jbase; };  // per (unit, input state): R cohort and slice-id base, or WGEN_NONE
+struct WGenInD { uint32_t c, jbase; };  // per (unit, input state): boundary cohort and slice-id base, or WGEN_NONE
 constexpr uint32_t WGEN_NONE = 0xffffffffu;
+
+struct CoefGen {
+    hvec<WGenUnitD> units;
+    hvec<WGenInD> gin;  // units x nst
+    hvec<uint32_t> line_major;
+    hvec<double> line_scale;
+    hvec<uint32_t> smap_id, smap_slot;
+    uint32_t nst = 0;
+    std::vector<uint32_t> m_ptr, m_other, m_op;  // MPO entries grouped by line index
+    std::vector<double> m_scale;
+    std::vector<uint32_t> o_ptr, o_in;  // operator terms by (operator, output state): input state, value
+    std::vector<double> o_val;
+    std::vector<int32_t> b_pos;  // boundary cohort x aux: block position of the MPO index, or -1
+    const std::vector<double>* b_cs = nullptr;  // boundary conj scales (cohort x aux)
+    uint32_t b_aux = 0;
+    uint64_t w_len = 0;
+
+    DBuf<WGenUnitD> d_units;
+    DBuf<WGenInD> d_gin;
+    DBuf<uint32_t> d_line_major, d_smap_id, d_smap_slot, d_m_ptr, d_m_other, d_m_op, d_o_ptr, d_o_in, d_err;
+    DBuf<double> d_line_scale, d_m_scale, d_o_val, d_b_cs;
+    DBuf<int32_t> d_b_pos;
+
+    // MPO entries by row b1 (other index b2) or by column b2 (other index b1, in increasing b1),
+    // and the operator terms; nst = physical states
+    void set_mpo(const MPOTensor& W, uint32_t nst, bool by_row);
+    void set_boundary(const BoundaryIndexH& B);
+    // appends one unit: its lines (MPO index and scale each), slot -> slice id, and the
+    // (cohort, slice-id base) of each of the nst input states
+    void add_unit(uint64_t w_off, uint32_t st_out, const uint32_t* majors, const double* scales, uint32_t nl,
+                  const std::vector<uint32_t>& slices, const WGenInD* in_row);
+    // appends the per-unit tables of another builder (part) with its lines, slice-map and
+    // coefficient-block bases
+    void append_units(const CoefGen& part, uint32_t line_base, uint32_t map_base, uint64_t w_base);
+    void validate() const;  // throws unless every index k_wgen derives stays in its buffer
+    void upload(cudaStream_t s);
+    // W (w_len doubles) = coefficient blocks; waits for the stream and throws if a term had no slot
+    void generate(double* W, cudaStream_t s);
+};
 
 struct HeffPlan {
     Index phys, left, right;
@@ -191,18 +186,7 @@ struct HeffPlan {
     hvec<uint64_t> slice_off;
     uint64_t s_len = 0;
     uint64_t n_alpha = 0;  // coefficient terms (before terms of one (line, slice) are summed)
-    // coefficient generation tables (see WGenUnitD)
-    hvec<WGenUnitD> wgunits;
-    hvec<WGenInD> wgin;          // units x nst
-    hvec<uint32_t> line_row;     // MPO row b1 of each line (line_b1 holds its S row block)
-    hvec<uint32_t> smap_id, smap_slot;
-    uint32_t nst = 0;
-    std::vector<uint32_t> m_rowptr, m_b2, m_op;  // MPO entries, CSR over b1
-    std::vector<double> m_scale;
-    std::vector<uint32_t> o_ptr, o_in;  // operator terms by (op, output state): (input state, value)
-    std::vector<double> o_val;
-    std::vector<int32_t> r_pos;   // R cohort x aux: block position of b2 in the cohort, or -1
-    uint32_t l_aux = 0, r_aux = 0;
+    CoefGen cg;            // coefficient blocks of the units (lines iterate MPO rows b1)
     uint64_t w_len = 0;  // dense coefficient blocks of all units (doubles)
     std::vector<uint16_t> klist;  // non-empty k-steps per S-GEMM m-tile
 
@@ -233,11 +217,6 @@ struct HeffPlan {
     DBuf<TileD> d_utiles[N_SHAPES];
     DBuf<uint32_t> d_line_b1;
     DBuf<uint64_t> d_slice_off;
-    DBuf<WGenUnitD> d_wgunits;
-    DBuf<WGenInD> d_wgin;
-    DBuf<uint32_t> d_line_row, d_smap_id, d_smap_slot, d_m_rowptr, d_m_b2, d_m_op, d_o_ptr, d_o_in;
-    DBuf<double> d_m_scale, d_o_val, d_l_cs, d_r_cs;
-    DBuf<int32_t> d_r_pos;
     DBuf<double> d_W;
     DBuf<uint16_t> d_klist;
     DBuf<SegD> d_segs;
@@ -269,11 +248,6 @@ void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<T
 void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const uint32_t* line_b1,
                const uint64_t* slice_off, const uint16_t* klist, const double* W, const double* T, double* S,
                cudaStream_t s);
-// Computes every unit's coefficients into its dense block of W (w_len doubles, zeroed first).
-void generate_coefficients(HeffPlan& p);
-// Scatters every unit's coefficient entries into its dense block of W (w_len doubles, zeroed first).
-void fill_coefficients(const UnitD* units, uint32_t n_units, const uint32_t* sptr, const WEntD* went, double* W,
-                       uint64_t w_len, cudaStream_t s);
 // Same apply with caller-provided scratch: Tb (t_len), Sb (s_len) and Pb (p_len) doubles.
 void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* Tb, double* Sb, double* Pb);
 

@@ -9,9 +9,10 @@
 //
 //   k_tgemm   : T[ti] = psi_slab * R[ci_eff] (per-block transposed when the R
 //               cohort is stored as its Hermitian partner)         (tasks.cpp:707-752)
-//   k_sgemm   : S rows of a cohort unit = W_u (lines x slices, the unit's MPO
-//               coefficients as a dense block, scattered once per plan by
-//               k_wfill) * T slices.
+//   k_wgen    : W_u (lines x slices) = the unit's MPO coefficient terms summed into
+//               a dense block, once per plan, from the MPO, operator and boundary
+//               tables (one thread per line)
+//   k_sgemm   : S rows of a cohort unit = W_u * T slices.
 //               Replaces the alpha-weighted gather (gpu_dgemm_ddot.cu:282-359,
 //               tasks.cpp:466-494) by a tensor-core GEMM.
 //   k_lspart  : split-K partial tiles of y[lb_out] = sum_cohorts L[ci_eff] * S
@@ -179,32 +180,21 @@ __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units,
     });
 }
 
-// One CTA per unit: its coefficient entries into the dense block W_u (duplicates were merged on the host)
-__global__ void k_wfill(const UnitD* __restrict__ units, const uint32_t* __restrict__ sptr, const WEntD* __restrict__ went,
-                        double* __restrict__ W) {
-    const UnitD U = units[blockIdx.x];
-    const uint32_t e0 = sptr[U.sptr0], e1 = sptr[U.sptr0 + U.nk];
-    for (uint32_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-        const WEntD w = went[e];
-        W[U.w_off + w.line + uint64_t(w.k) * U.nl] = w.a;
-    }
-}
-
-// One CTA per unit, one thread per line: the line's coefficient terms, in MPO-entry then
-// operator-term order, summed into W_u.  Products and sums are rounded separately (no
+// One CTA per unit, one thread per line: the line's coefficient terms (CoefGen), in MPO-entry
+// then operator-term order, summed into W_u.  Products and sums are rounded separately (no
 // contraction), so W_u holds the same values as a host evaluation of the same terms.
 constexpr int WG_THR = 128;
 constexpr uint32_t WG_SMAP = 4096;  // (slice id, slot) pairs staged in shared memory
-constexpr uint32_t WG_NST = 64;     // physical states of the two-site basis
+constexpr uint32_t WG_NST = 64;     // physical states of the basis
 __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ units, const WGenInD* __restrict__ gin,
-                                                 uint32_t nst, const uint32_t* __restrict__ line_row,
+                                                 uint32_t nst, const uint32_t* __restrict__ line_major,
+                                                 const double* __restrict__ line_scale,
                                                  const uint32_t* __restrict__ smap_id, const uint32_t* __restrict__ smap_slot,
-                                                 const uint32_t* __restrict__ m_rowptr, const uint32_t* __restrict__ m_b2,
+                                                 const uint32_t* __restrict__ m_ptr, const uint32_t* __restrict__ m_other,
                                                  const uint32_t* __restrict__ m_op, const double* __restrict__ m_scale,
                                                  const uint32_t* __restrict__ o_ptr, const uint32_t* __restrict__ o_in,
-                                                 const double* __restrict__ o_val, const double* __restrict__ l_cs,
-                                                 uint32_t l_aux, const int32_t* __restrict__ r_pos,
-                                                 const double* __restrict__ r_cs, uint32_t r_aux, double* __restrict__ W,
+                                                 const double* __restrict__ o_val, const int32_t* __restrict__ b_pos,
+                                                 const double* __restrict__ b_cs, uint32_t b_aux, double* __restrict__ W,
                                                  uint32_t* __restrict__ err) {
     __shared__ uint32_t sid[WG_SMAP], sslot[WG_SMAP];
     __shared__ WGenInD sin[WG_NST];
@@ -220,20 +210,20 @@ __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ u
     const uint32_t* ids = staged ? sid : smap_id + U.map0;
     const uint32_t* slots = staged ? sslot : smap_slot + U.map0;
     for (uint32_t line = threadIdx.x; line < U.nl; line += blockDim.x) {
-        const uint32_t b1 = line_row[U.line0 + line];
-        const double lsc = l_cs[std::size_t(U.ci) * l_aux + b1];
+        const uint32_t m = line_major[U.line0 + line];
+        const double lsc = line_scale[U.line0 + line];
         double* Wl = W + U.w_off + line;
-        for (uint32_t e = m_rowptr[b1]; e < m_rowptr[b1 + 1]; ++e) {
-            const uint32_t b2 = m_b2[e], op = m_op[e];
+        for (uint32_t e = m_ptr[m]; e < m_ptr[m + 1]; ++e) {
+            const uint32_t x = m_other[e], op = m_op[e];
             const double wsc = __dmul_rn(m_scale[e], lsc);
             const std::size_t q = std::size_t(op) * nst + U.st_out;
             for (uint32_t k = o_ptr[q]; k < o_ptr[q + 1]; ++k) {
                 const WGenInD g = sin[o_in[k]];
-                if (g.cir == WGEN_NONE) continue;
-                const std::size_t rq = std::size_t(g.cir) * r_aux + b2;
-                const int32_t pos = r_pos[rq];
+                if (g.c == WGEN_NONE) continue;
+                const std::size_t bq = std::size_t(g.c) * b_aux + x;
+                const int32_t pos = b_pos[bq];
                 if (pos < 0) continue;
-                const double a = __dmul_rn(__dmul_rn(o_val[k], r_cs[rq]), wsc);
+                const double a = __dmul_rn(__dmul_rn(o_val[k], b_cs[bq]), wsc);
                 const uint32_t id = g.jbase + uint32_t(pos);
                 uint32_t lo = 0, hi = U.nk;
                 while (lo < hi) {
@@ -248,6 +238,82 @@ __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ u
         }
     }
 }
+
+}  // namespace
+
+void CoefGen::validate() const {
+    const std::size_t nu = units.size();
+    auto bad = [](const char* what) { throw std::runtime_error(std::string("coefficient tables: ") + what); };
+    if (nst > WG_NST || gin.size() != nu * nst || line_scale.size() != line_major.size() || smap_slot.size() != smap_id.size())
+        bad("unit tables");
+    if (m_ptr.empty() || m_ptr.back() != m_other.size() || m_op.size() != m_other.size() || m_scale.size() != m_other.size())
+        bad("MPO entries");
+    const std::size_t nmaj = m_ptr.size() - 1;
+    const std::size_t nops = nst ? (o_ptr.size() - 1) / nst : 0;
+    if (o_ptr.empty() || o_ptr.size() != nops * nst + 1 || o_ptr.back() != o_in.size() || o_val.size() != o_in.size())
+        bad("operator terms");
+    for (std::size_t i = 0; i < nmaj; ++i)
+        if (m_ptr[i] > m_ptr[i + 1]) bad("MPO pointers");
+    for (std::size_t e = 0; e < m_other.size(); ++e)
+        if (m_other[e] >= b_aux || m_op[e] >= nops) bad("MPO entry");
+    for (std::size_t i = 0; i + 1 < o_ptr.size(); ++i)
+        if (o_ptr[i] > o_ptr[i + 1]) bad("operator pointers");
+    for (uint32_t v : o_in)
+        if (v >= nst) bad("operator input state");
+    if (!b_cs || b_cs->size() != b_pos.size() || (b_aux && b_pos.size() % b_aux)) bad("boundary tables");
+    const std::size_t ncoh = b_aux ? b_pos.size() / b_aux : 0;
+    for (const WGenInD& g : gin)
+        if (g.c != WGEN_NONE && g.c >= ncoh) bad("boundary cohort");
+    for (const WGenUnitD& g : units) {
+        if (g.st_out >= nst || std::size_t(g.line0) + g.nl > line_major.size() || std::size_t(g.map0) + g.nk > smap_id.size() ||
+            g.w_off + uint64_t(g.nl) * g.nk > w_len)
+            bad("unit extent");
+        for (uint32_t l = 0; l < g.nl; ++l)
+            if (line_major[g.line0 + l] >= nmaj) bad("line index");
+        for (uint32_t i = 0; i < g.nk; ++i) {
+            if (smap_slot[g.map0 + i] >= g.nk) bad("slot");
+            if (i && smap_id[g.map0 + i - 1] >= smap_id[g.map0 + i]) bad("slice ids not sorted");
+        }
+    }
+}
+
+void CoefGen::upload(cudaStream_t s) {
+    validate();
+    d_units.upload(units, s);
+    d_gin.upload(gin, s);
+    d_line_major.upload(line_major, s);
+    d_line_scale.upload(line_scale, s);
+    d_smap_id.upload(smap_id, s);
+    d_smap_slot.upload(smap_slot, s);
+    d_m_ptr.upload(m_ptr, s);
+    d_m_other.upload(m_other, s);
+    d_m_op.upload(m_op, s);
+    d_m_scale.upload(m_scale, s);
+    d_o_ptr.upload(o_ptr, s);
+    d_o_in.upload(o_in, s);
+    d_o_val.upload(o_val, s);
+    d_b_pos.upload(b_pos, s);
+    d_b_cs.upload(*b_cs, s);
+}
+
+void CoefGen::generate(double* W, cudaStream_t s) {
+    if (w_len) QCM_CUDA(cudaMemsetAsync(W, 0, w_len * sizeof(double), s));
+    if (units.empty()) return;
+    if (d_units.size() < units.size()) throw std::runtime_error("coefficient tables: not uploaded");
+    d_err.alloc(1);
+    QCM_CUDA(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
+    k_wgen<<<unsigned(units.size()), WG_THR, 0, s>>>(d_units.get(), d_gin.get(), nst, d_line_major.get(), d_line_scale.get(),
+                                                     d_smap_id.get(), d_smap_slot.get(), d_m_ptr.get(), d_m_other.get(),
+                                                     d_m_op.get(), d_m_scale.get(), d_o_ptr.get(), d_o_in.get(), d_o_val.get(),
+                                                     d_b_pos.get(), d_b_cs.get(), b_aux, W, d_err.get());
+    QCM_CUDA(cudaGetLastError());
+    uint32_t h = 0;
+    QCM_CUDA(cudaMemcpyAsync(&h, d_err.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    QCM_CUDA(cudaStreamSynchronize(s));
+    if (h) throw std::runtime_error("coefficient tables: a term has no slice slot");
+}
+
+namespace {
 
 // ---------------------------------------------------------------------------
 // L.S GEMM, split-K: item = (output tile, segment, K range) -> partial tile P[item]
@@ -418,70 +484,6 @@ void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<
     QCM_CUDA(cudaGetLastError());
 }
 
-void generate_coefficients(HeffPlan& p) {
-    cudaStream_t s = p.stream;
-    if (p.w_len) QCM_CUDA(cudaMemsetAsync(p.d_W.get(), 0, p.w_len * sizeof(double), s));
-    if (p.wgunits.empty()) return;
-    DBuf<uint32_t> err;
-    err.alloc(1);
-    QCM_CUDA(cudaMemsetAsync(err.get(), 0, sizeof(uint32_t), s));
-    k_wgen<<<unsigned(p.wgunits.size()), WG_THR, 0, s>>>(
-        p.d_wgunits.get(), p.d_wgin.get(), p.nst, p.d_line_row.get(), p.d_smap_id.get(), p.d_smap_slot.get(),
-        p.d_m_rowptr.get(), p.d_m_b2.get(), p.d_m_op.get(), p.d_m_scale.get(), p.d_o_ptr.get(), p.d_o_in.get(),
-        p.d_o_val.get(), p.d_l_cs.get(), p.l_aux, p.d_r_pos.get(), p.d_r_cs.get(), p.r_aux, p.d_W.get(), err.get());
-    QCM_CUDA(cudaGetLastError());
-    uint32_t h = 0;
-    QCM_CUDA(cudaMemcpyAsync(&h, err.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    QCM_CUDA(cudaStreamSynchronize(s));
-    if (h) throw std::runtime_error("heff plan: coefficient term without a slice slot");
-}
-
-// Every index k_wgen derives from the plan tables stays inside its buffer.
-static void validate_wgen(const HeffPlan& p) {
-    const std::size_t nu = p.wgunits.size(), nst = p.nst;
-    const std::size_t l_coh = p.l_aux ? p.L->idx.cscale.size() / p.l_aux : 0;
-    const std::size_t r_coh = p.r_aux ? p.r_pos.size() / p.r_aux : 0;
-    auto bad = [](const char* what) { throw std::runtime_error(std::string("heff plan: coefficient tables: ") + what); };
-    if (nst > WG_NST || p.wgin.size() != nu * nst || nu != p.units.size()) bad("unit tables");
-    if (p.m_rowptr.empty() || p.m_rowptr.back() != p.m_b2.size() || p.m_op.size() != p.m_b2.size() ||
-        p.m_scale.size() != p.m_b2.size())
-        bad("MPO entries");
-    const std::size_t rows = p.m_rowptr.size() - 1;
-    const std::size_t nops = nst ? (p.o_ptr.size() - 1) / nst : 0;
-    if (p.o_ptr.size() != nops * nst + 1 || p.o_ptr.back() != p.o_in.size() || p.o_val.size() != p.o_in.size()) bad("operator terms");
-    for (std::size_t i = 0; i + 1 < p.m_rowptr.size(); ++i)
-        if (p.m_rowptr[i] > p.m_rowptr[i + 1]) bad("MPO row pointers");
-    for (std::size_t e = 0; e < p.m_b2.size(); ++e)
-        if (p.m_b2[e] >= p.r_aux || p.m_op[e] >= nops) bad("MPO entry");
-    for (std::size_t i = 0; i + 1 < p.o_ptr.size(); ++i)
-        if (p.o_ptr[i] > p.o_ptr[i + 1]) bad("operator pointers");
-    for (uint32_t v : p.o_in)
-        if (v >= nst) bad("operator input state");
-    if (p.R->idx.cscale.size() != p.r_pos.size() || p.l_aux != p.L->idx.aux) bad("boundary tables");
-    for (const WGenInD& g : p.wgin)
-        if (g.cir != WGEN_NONE && g.cir >= r_coh) bad("R cohort");
-    for (std::size_t u = 0; u < nu; ++u) {
-        const WGenUnitD& g = p.wgunits[u];
-        if (g.ci >= l_coh || g.st_out >= nst || std::size_t(g.line0) + g.nl > p.line_row.size() ||
-            std::size_t(g.map0) + g.nk > p.smap_id.size() || g.w_off + uint64_t(g.nl) * g.nk > p.w_len)
-            bad("unit extent");
-        for (uint32_t l = 0; l < g.nl; ++l) {
-            const uint32_t b1 = p.line_row[g.line0 + l];
-            if (b1 >= rows || b1 >= p.l_aux) bad("line");
-        }
-        for (uint32_t i = 0; i < g.nk; ++i) {
-            if (p.smap_slot[g.map0 + i] >= g.nk) bad("slot");
-            if (i && p.smap_id[g.map0 + i - 1] >= p.smap_id[g.map0 + i]) bad("slice ids not sorted");
-        }
-    }
-}
-
-void fill_coefficients(const UnitD* units, uint32_t n_units, const uint32_t* sptr, const WEntD* went, double* W,
-                       uint64_t w_len, cudaStream_t s) {
-    if (w_len) QCM_CUDA(cudaMemsetAsync(W, 0, w_len * sizeof(double), s));
-    if (n_units) k_wfill<<<n_units, 128, 0, s>>>(units, sptr, went, W);
-    QCM_CUDA(cudaGetLastError());
-}
 
 int heff_launches_per_apply(const HeffPlan& p) {
     int n = 0;
@@ -513,25 +515,10 @@ void upload_plan(HeffPlan& p) {
         p.d_otiles[sh].upload(p.otiles[sh], s);
         p.d_kitems[sh].upload(p.kitems[sh], s);
     }
-    validate_wgen(p);
     p.d_units.upload(p.units, s);
     p.d_line_b1.upload(p.line_b1, s);
     p.d_slice_off.upload(p.slice_off, s);
-    p.d_wgunits.upload(p.wgunits, s);
-    p.d_wgin.upload(p.wgin, s);
-    p.d_line_row.upload(p.line_row, s);
-    p.d_smap_id.upload(p.smap_id, s);
-    p.d_smap_slot.upload(p.smap_slot, s);
-    p.d_m_rowptr.upload(p.m_rowptr, s);
-    p.d_m_b2.upload(p.m_b2, s);
-    p.d_m_op.upload(p.m_op, s);
-    p.d_m_scale.upload(p.m_scale, s);
-    p.d_o_ptr.upload(p.o_ptr, s);
-    p.d_o_in.upload(p.o_in, s);
-    p.d_o_val.upload(p.o_val, s);
-    p.d_l_cs.upload(p.L->idx.cscale, s);
-    p.d_r_cs.upload(p.R->idx.cscale, s);
-    p.d_r_pos.upload(p.r_pos, s);
+    p.cg.upload(s);
     p.d_klist.upload(p.klist, s);
     p.d_segs.upload(p.segs, s);
     p.d_outs.upload(p.outs, s);
@@ -540,7 +527,7 @@ void upload_plan(HeffPlan& p) {
     p.d_P.alloc(p.p_len);
     // dense coefficient blocks, built once per plan and reused by every apply
     p.d_W.alloc(p.w_len ? p.w_len : 1);
-    generate_coefficients(p);
+    p.cg.generate(p.d_W.get(), s);
     QCM_CUDA(cudaStreamSynchronize(s));
 }
 

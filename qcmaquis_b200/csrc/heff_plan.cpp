@@ -63,9 +63,8 @@ struct Part {
     std::vector<uint32_t> tjob_mps;  // mps column offset of each job (bookkeeping)
     uint64_t t_len = 0;
     std::vector<UnitD> units;
-    std::vector<WGenUnitD> wgunits;
-    std::vector<WGenInD> wgin;
-    std::vector<uint32_t> line_b1, line_row, smap_id, smap_slot;
+    CoefGen cg;  // part-local coefficient-generation units
+    std::vector<uint32_t> line_b1;
     std::vector<uint64_t> slice_off;
     uint64_t s_len = 0, w_len = 0, n_alpha = 0;
     std::vector<std::pair<uint32_t, SegD>> segs;
@@ -89,8 +88,7 @@ struct U {
 
 }  // namespace
 
-template <class E>
-void add_unit_tiles(const UnitD& u, uint32_t item, const E* ents, std::size_t n, std::vector<TileD>* utiles,
+void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t n, std::vector<TileD>* utiles,
                     std::vector<uint16_t>& klist) {
     if (!u.nl || !u.ne || !u.nk || !n) return;
     constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK), four DMMA k-groups of 4 slices
@@ -140,10 +138,95 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const E* ents, std::size_t n,
     }
 }
 
-template void add_unit_tiles<WEntD>(const UnitD&, uint32_t, const WEntD*, std::size_t, std::vector<TileD>*,
-                                    std::vector<uint16_t>&);
-template void add_unit_tiles<LKD>(const UnitD&, uint32_t, const LKD*, std::size_t, std::vector<TileD>*,
-                                  std::vector<uint16_t>&);
+void CoefGen::set_mpo(const MPOTensor& W, uint32_t nst_, bool by_row) {
+    nst = nst_;
+    const std::size_t nops = W.ops->size(), nent = W.b2.size();
+    if (W.b1.size() != nent || W.op.size() != nent || W.scale.size() != nent) throw std::runtime_error("coefficient tables: inconsistent MPO tensor");
+    if (by_row) {
+        if (W.row_ptr.size() != std::size_t(W.rows) + 1 || W.row_ptr.back() != nent) throw std::runtime_error("coefficient tables: MPO row pointers");
+        m_ptr.assign(W.row_ptr.begin(), W.row_ptr.end());
+        m_other.assign(W.b2.begin(), W.b2.end());
+        m_op.assign(W.op.begin(), W.op.end());
+        m_scale.assign(W.scale.begin(), W.scale.end());
+    } else {
+        if (W.col_ptr.size() != std::size_t(W.cols) + 1 || W.col_ptr.back() != nent || W.col_ent.size() != nent)
+            throw std::runtime_error("coefficient tables: MPO column pointers");
+        m_ptr.assign(W.col_ptr.begin(), W.col_ptr.end());
+        m_other.resize(nent); m_op.resize(nent); m_scale.resize(nent);
+        for (std::size_t q = 0; q < nent; ++q) {
+            const uint32_t e = W.col_ent[q];
+            if (e >= nent) throw std::runtime_error("coefficient tables: MPO column entry");
+            m_other[q] = W.b1[e]; m_op[q] = W.op[e]; m_scale[q] = W.scale[e];
+        }
+    }
+    for (std::size_t q = 0; q < nent; ++q)
+        if (m_op[q] >= nops) throw std::runtime_error("coefficient tables: MPO operator index");
+    // operator terms grouped by (operator, output state), in their order within the operator
+    o_ptr.assign(nops * nst + 1, 0);
+    for (std::size_t o = 0; o < nops; ++o) {
+        const SparseOp& op = (*W.ops)[o];
+        for (std::size_t e = 0; e < op.val.size(); ++e) {
+            if (op.in[e] >= nst || op.out[e] >= nst) throw std::runtime_error("coefficient tables: operator entry outside the physical basis");
+            o_ptr[o * nst + op.out[e] + 1]++;
+        }
+    }
+    for (std::size_t i = 0; i < nops * nst; ++i) o_ptr[i + 1] += o_ptr[i];
+    o_in.resize(o_ptr.back());
+    o_val.resize(o_ptr.back());
+    std::vector<uint32_t> fill(o_ptr.begin(), o_ptr.end() - 1);
+    for (std::size_t o = 0; o < nops; ++o) {
+        const SparseOp& op = (*W.ops)[o];
+        for (std::size_t e = 0; e < op.val.size(); ++e) {
+            const uint32_t d = fill[o * nst + op.out[e]]++;
+            o_in[d] = op.in[e];
+            o_val[d] = op.val[e];
+        }
+    }
+}
+
+void CoefGen::set_boundary(const BoundaryIndexH& B) {
+    b_aux = B.aux;
+    b_cs = &B.cscale;
+    b_pos.resize(B.offsets.size());
+    for (uint32_t c = 0; c < B.n_cohorts(); ++c) {
+        const int64_t bs = std::max<int64_t>(1, int64_t(B.lsz[c]) * B.rsz[c]);
+        for (uint32_t b = 0; b < B.aux; ++b) {
+            const int64_t o = B.offsets[std::size_t(c) * B.aux + b];
+            b_pos[std::size_t(c) * B.aux + b] = o < 0 ? -1 : int32_t(o / bs);
+        }
+    }
+}
+
+void CoefGen::append_units(const CoefGen& x, uint32_t line_base, uint32_t map_base, uint64_t w_base) {
+    for (WGenUnitD g : x.units) {
+        g.w_off += w_base; g.line0 += line_base; g.map0 += map_base;
+        units.push_back(g);
+    }
+    gin.insert(gin.end(), x.gin.begin(), x.gin.end());
+    line_major.insert(line_major.end(), x.line_major.begin(), x.line_major.end());
+    line_scale.insert(line_scale.end(), x.line_scale.begin(), x.line_scale.end());
+    smap_id.insert(smap_id.end(), x.smap_id.begin(), x.smap_id.end());
+    smap_slot.insert(smap_slot.end(), x.smap_slot.begin(), x.smap_slot.end());
+}
+
+void CoefGen::add_unit(uint64_t w_off, uint32_t st_out, const uint32_t* majors, const double* scales, uint32_t nl,
+                       const std::vector<uint32_t>& slices, const WGenInD* in_row) {
+    WGenUnitD g{};
+    g.w_off = w_off; g.st_out = st_out;
+    g.line0 = uint32_t(line_major.size()); g.nl = nl;
+    g.map0 = uint32_t(smap_id.size()); g.nk = uint32_t(slices.size());
+    line_major.insert(line_major.end(), majors, majors + nl);
+    line_scale.insert(line_scale.end(), scales, scales + nl);
+    const std::size_t m0 = smap_id.size();
+    for (uint32_t i = 0; i < g.nk; ++i) { smap_id.push_back(slices[i]); smap_slot.push_back(i); }
+    // (slice id, slot) pairs sorted by id
+    std::vector<std::pair<uint32_t, uint32_t>> pr(g.nk);
+    for (uint32_t i = 0; i < g.nk; ++i) pr[i] = {slices[i], i};
+    std::sort(pr.begin(), pr.end());
+    for (uint32_t i = 0; i < g.nk; ++i) { smap_id[m0 + i] = pr[i].first; smap_slot[m0 + i] = pr[i].second; }
+    gin.insert(gin.end(), in_row, in_row + nst);
+    units.push_back(g);
+}
 
 std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
                                           const Index& phys, const Index& left, const Index& right, bool bookkeeping) {
@@ -201,46 +284,9 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         }
     }
     optr[nops] = uint32_t(oin.size());
-    // the same terms by (operator, output state), in their order within the operator
-    p->nst = nst;
-    p->o_ptr.assign(nops * nst + 1, 0);
-    for (std::size_t k = 0; k < oin.size(); ++k) {
-        const std::size_t o = std::size_t(std::upper_bound(optr.begin(), optr.end(), uint32_t(k)) - optr.begin()) - 1;
-        p->o_ptr[o * nst + oout[k] + 1]++;
-    }
-    for (std::size_t i = 0; i < nops * nst; ++i) p->o_ptr[i + 1] += p->o_ptr[i];
-    p->o_in.resize(oin.size());
-    p->o_val.resize(oin.size());
-    {
-        std::vector<uint32_t> fill(p->o_ptr.begin(), p->o_ptr.end() - 1);
-        for (std::size_t o = 0; o < nops; ++o)
-            for (uint32_t k = optr[o]; k < optr[o + 1]; ++k) {
-                const uint32_t d = fill[o * nst + oout[k]]++;
-                p->o_in[d] = oin[k];
-                p->o_val[d] = oval[k];
-            }
-    }
-    // MPO entries and boundary tables for the device coefficient generation
-    p->m_rowptr.assign(W.row_ptr.begin(), W.row_ptr.end());
-    p->m_b2.assign(W.b2.begin(), W.b2.end());
-    p->m_op.assign(W.op.begin(), W.op.end());
-    p->m_scale.assign(W.scale.begin(), W.scale.end());
-    if (p->m_rowptr.size() != std::size_t(W.rows) + 1 || p->m_b2.size() != p->m_rowptr.back() ||
-        p->m_op.size() != p->m_b2.size() || p->m_scale.size() != p->m_b2.size())
-        throw std::runtime_error("heff plan: inconsistent MPO tensor");
-    for (std::size_t e = 0; e < p->m_b2.size(); ++e)
-        if (p->m_b2[e] >= W.cols || p->m_op[e] >= nops) throw std::runtime_error("heff plan: MPO entry out of range");
-    p->l_aux = L.aux;
-    p->r_aux = R.aux;
-    // block position of (R cohort, b2): element offset / block size
-    p->r_pos.resize(R.offsets.size());
-    for (uint32_t c = 0; c < R.n_cohorts(); ++c) {
-        const int64_t bs = std::max<int64_t>(1, int64_t(R.lsz[c]) * R.rsz[c]);
-        for (uint32_t b = 0; b < R.aux; ++b) {
-            const int64_t o = R.offsets[std::size_t(c) * R.aux + b];
-            p->r_pos[std::size_t(c) * R.aux + b] = o < 0 ? -1 : int32_t(o / bs);
-        }
-    }
+    // coefficient generation: lines iterate MPO rows b1, slices come from R cohorts
+    p->cg.set_mpo(W, nst, true);
+    p->cg.set_boundary(R);
 
     std::vector<Part> parts(nl);
     const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
@@ -250,11 +296,13 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     {
     // per-thread scratch, reused across cohorts
     std::vector<U> units;
-    std::vector<uint32_t> slices, order;
+    std::vector<uint32_t> slices;
+    std::vector<double> lscale;
 #pragma omp for schedule(dynamic, 1)
     for (int lbi = 0; lbi < int(nl); ++lbi) {
         const uint32_t lb_in = uint32_t(lbi);
         Part& P = parts[lb_in];
+        P.cg.nst = nst;
         const uint32_t ls_in = uint32_t(left[lb_in].second);
         // ---- T jobs: one per (input state, bra right sector) ----
         std::vector<uint32_t> tj(std::size_t(nst) * nr, NONE);
@@ -311,7 +359,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             // per (input state, unit): R cohort and slice-id base of its T job
             std::vector<int> unit_of(nst, -1);
             for (std::size_t k = 0; k < nu; ++k) unit_of[units[k].st] = int(k);
-            std::vector<WGenInD> gin(std::size_t(nst) * nu, WGenInD{NONE, NONE});
+            std::vector<WGenInD> gin(nu * nst, WGenInD{WGEN_NONE, WGEN_NONE});  // [unit][input state]
             std::vector<uint32_t> rsin_t(nst, 0);
             for (uint32_t sti = 0; sti < nst; ++sti) {
                 const RSec& ri = rsec[std::size_t(lb_in) * nps + sm.sector[sti]];
@@ -320,10 +368,10 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 for (std::size_t k = 0; k < nu; ++k) {
                     const uint32_t cir = Rci[std::size_t(ri.rb) * nr + units[k].rb_out];
                     const uint32_t job = tj[std::size_t(sti) * nr + units[k].rb_out];
-                    if (cir != NONE && job != NONE) gin[sti * nu + k] = WGenInD{cir, job_pos0[job]};
+                    if (cir != NONE && job != NONE) gin[k * nst + sti] = WGenInD{cir, job_pos0[job]};
                 }
             }
-            const int32_t* Rpos = p->r_pos.data();
+            const int32_t* Rpos = p->cg.b_pos.data();
             const std::size_t Raux = R.aux;
             std::size_t n_alpha = 0;
             for (uint32_t b1 = 0; b1 < W.rows; ++b1) {
@@ -335,19 +383,19 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                         const int u = unit_of[oout[k]];
                         if (u < 0) continue;
                         const uint32_t sti = oin[k];
-                        const WGenInD g = gin[sti * nu + u];
-                        if (g.cir == NONE) continue;
-                        const int32_t pos = Rpos[g.cir * Raux + b2];
+                        const WGenInD g = gin[std::size_t(u) * nst + sti];
+                        if (g.c == WGEN_NONE) continue;
+                        const int32_t pos = Rpos[g.c * Raux + b2];
                         if (pos < 0) continue;
                         U& un = units[u];
                         if (un.lines.empty() || un.lines.back() != bpos) { un.lines.push_back(bpos); un.rows.push_back(b1); }
                         un.em.push_back(LKD{uint32_t(un.lines.size() - 1), g.jbase + uint32_t(pos)});
                         if (bookkeeping) {
-                            const uint32_t col = uint32_t(R.offset(g.cir, b2) / rsin_t[sti]);
+                            const uint32_t col = uint32_t(R.offset(g.c, b2) / rsin_t[sti]);
                             const uint32_t job = tj[std::size_t(sti) * nr + un.rb_out];
-                            const uint32_t row[3] = {P.tjob_mps[job], g.cir, col};
+                            const uint32_t row[3] = {P.tjob_mps[job], g.c, col};
                             un.bk.insert(un.bk.end(), row, row + 3);
-                            un.bk_a.push_back(oval[k] * R.conj_scale(g.cir, b2) * (W.scale[e] * L.conj_scale(ci, b1)));
+                            un.bk_a.push_back(oval[k] * R.conj_scale(g.c, b2) * (W.scale[e] * L.conj_scale(ci, b1)));
                         }
                         ++n_alpha;
                     }
@@ -382,16 +430,10 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     uint32_t pos = gp - job_pos0[job];
                     P.slice_off.push_back(P.tjobs[job].c_off + uint64_t(pos) * u.ms * ls_in);
                 }
-                // coefficient generation: (slice id, slot) pairs sorted by id, input-state table
-                WGenUnitD wg{};
-                wg.w_off = ud.w_off; wg.ci = ci; wg.st_out = u.st;
-                wg.line0 = ud.line0; wg.nl = ud.nl; wg.map0 = uint32_t(P.smap_id.size()); wg.nk = ud.nk;
-                order.resize(slices.size());
-                for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
-                std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return slices[x] < slices[y]; });
-                for (uint32_t i : order) { P.smap_id.push_back(slices[i]); P.smap_slot.push_back(i); }
-                for (uint32_t sti = 0; sti < nst; ++sti) P.wgin.push_back(gin[sti * nu + ui]);
-                P.wgunits.push_back(wg);
+                // coefficient generation: lines with their L conj scales, slot -> slice id
+                lscale.resize(ud.nl);
+                for (uint32_t l = 0; l < ud.nl; ++l) lscale[l] = L.conj_scale(ci, u.rows[l]);
+                P.cg.add_unit(ud.w_off, u.st, u.rows.data(), lscale.data(), ud.nl, slices, &gin[ui * nst]);
                 if (bookkeeping)
                     for (std::size_t i = 0; i < u.em.size(); ++i) {
                         uint32_t row[10] = {lb_in, lb_out, ci, ce, u.offset, u.ms, u.lines[u.em[i].line],
@@ -400,7 +442,6 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                         P.bk_alpha.push_back(u.bk_a[i]);
                     }
                 P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
-                P.line_row.insert(P.line_row.end(), u.rows.begin(), u.rows.end());
                 // S-GEMM tiles of the unit and the tensor work they execute
                 const std::size_t tb[4] = {P.utiles[0].size(), P.utiles[1].size(), P.utiles[2].size(), P.utiles[3].size()};
                 add_unit_tiles(ud, uint32_t(P.units.size()), u.em.data(), u.em.size(), P.utiles, P.klist);
@@ -437,7 +478,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         Base& n = base[i + 1];
         n = Base{b.t + P.t_len, b.s + P.s_len, b.w + P.w_len, b.na + P.n_alpha, b.job + uint32_t(P.tjobs.size()),
                  b.unit + uint32_t(P.units.size()), b.line + uint32_t(P.line_b1.size()),
-                 b.slice + uint32_t(P.slice_off.size()), b.smap + uint32_t(P.smap_id.size()),
+                 b.slice + uint32_t(P.slice_off.size()), b.smap + uint32_t(P.cg.smap_id.size()),
                  b.kl + uint32_t(P.klist.size()), b.bk + P.bk_alpha.size(), {}};
         for (int sh = 0; sh < N_SHAPES; ++sh) n.tile[sh] = b.tile[sh] + P.utiles[sh].size();
         p->flops_sexec += P.flops_sexec;
@@ -445,13 +486,15 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     const Base& tot = base[nl];
     p->tjobs.resize(tot.job);
     p->units.resize(tot.unit);
-    p->wgunits.resize(tot.unit);
-    p->wgin.resize(std::size_t(tot.unit) * nst);
+    CoefGen& cg = p->cg;
+    cg.units.resize(tot.unit);
+    cg.gin.resize(std::size_t(tot.unit) * nst);
+    cg.line_major.resize(tot.line);
+    cg.line_scale.resize(tot.line);
+    cg.smap_id.resize(tot.smap);
+    cg.smap_slot.resize(tot.smap);
     p->line_b1.resize(tot.line);
-    p->line_row.resize(tot.line);
     p->slice_off.resize(tot.slice);
-    p->smap_id.resize(tot.smap);
-    p->smap_slot.resize(tot.smap);
     p->klist.resize(tot.kl);
     p->n_alpha = tot.na;
     for (int sh = 0; sh < N_SHAPES; ++sh) p->utiles[sh].resize(tot.tile[sh]);
@@ -465,16 +508,17 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             UnitD u = P.units[k];
             u.s_off += B.s; u.line0 += B.line; u.slice0 += B.slice; u.w_off += B.w;
             p->units[B.unit + k] = u;
-            WGenUnitD g = P.wgunits[k];
+            WGenUnitD g = P.cg.units[k];
             g.w_off += B.w; g.line0 += B.line; g.map0 += B.smap;
-            p->wgunits[B.unit + k] = g;
+            cg.units[B.unit + k] = g;
         }
-        std::copy(P.wgin.begin(), P.wgin.end(), p->wgin.begin() + std::size_t(B.unit) * nst);
+        std::copy(P.cg.gin.begin(), P.cg.gin.end(), cg.gin.begin() + std::size_t(B.unit) * nst);
+        std::copy(P.cg.line_major.begin(), P.cg.line_major.end(), cg.line_major.begin() + B.line);
+        std::copy(P.cg.line_scale.begin(), P.cg.line_scale.end(), cg.line_scale.begin() + B.line);
         std::copy(P.line_b1.begin(), P.line_b1.end(), p->line_b1.begin() + B.line);
-        std::copy(P.line_row.begin(), P.line_row.end(), p->line_row.begin() + B.line);
         for (std::size_t k = 0; k < P.slice_off.size(); ++k) p->slice_off[B.slice + k] = P.slice_off[k] + B.t;
-        std::copy(P.smap_id.begin(), P.smap_id.end(), p->smap_id.begin() + B.smap);
-        std::copy(P.smap_slot.begin(), P.smap_slot.end(), p->smap_slot.begin() + B.smap);
+        std::copy(P.cg.smap_id.begin(), P.cg.smap_id.end(), cg.smap_id.begin() + B.smap);
+        std::copy(P.cg.smap_slot.begin(), P.cg.smap_slot.end(), cg.smap_slot.begin() + B.smap);
         if (bookkeeping) {
             std::copy(P.bk_int.begin(), P.bk_int.end(), p->bk_int.begin() + B.bk * 10);
             std::copy(P.bk_alpha.begin(), P.bk_alpha.end(), p->bk_alpha.begin() + B.bk);
@@ -489,12 +533,13 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         for (auto& sg : P.segs) sg.second.s_off += B.s;
         for (int sh = 0; sh < N_SHAPES; ++sh) P.utiles[sh] = {};
         P.klist = {};
-        P.tjobs = {}; P.tjob_mps = {}; P.units = {}; P.wgunits = {}; P.wgin = {}; P.line_b1 = {}; P.line_row = {}; P.slice_off = {};
-        P.smap_id = {}; P.smap_slot = {}; P.bk_int = {}; P.bk_alpha = {};
+        P.tjobs = {}; P.tjob_mps = {}; P.units = {}; P.cg = CoefGen(); P.line_b1 = {}; P.slice_off = {};
+        P.bk_int = {}; P.bk_alpha = {};
     }
     p->t_len = tot.t;
     p->s_len = tot.s;
     p->w_len = tot.w;
+    cg.w_len = tot.w;
     std::vector<std::vector<SegD>> per_out(nl);
     for (uint32_t i = 0; i < nl; ++i) {
         const Part& P = parts[i];
