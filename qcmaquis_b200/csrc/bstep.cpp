@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
+#include <string>
 #include <unordered_map>
 
 #include "dmrg_dev.hpp"

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <stdexcept>
+#include <string>
 
 #include "heff.hpp"
 
@@ -292,6 +293,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
     auto tnow = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     const double t_a = tnow();
+    std::string err;
 #pragma omp parallel
     {
     // per-thread scratch, reused across cohorts
@@ -299,7 +301,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     std::vector<uint32_t> slices;
     std::vector<double> lscale;
 #pragma omp for schedule(dynamic, 1)
-    for (int lbi = 0; lbi < int(nl); ++lbi) {
+    for (int lbi = 0; lbi < int(nl); ++lbi) try {
         const uint32_t lb_in = uint32_t(lbi);
         Part& P = parts[lb_in];
         P.cg.nst = nst;
@@ -464,8 +466,12 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             sg.ls_in = ls_in; sg.nS = nS; sg.tr = (ci != ce) ? 1 : 0;
             P.segs.push_back({lb_out, sg});
         }
+    } catch (const std::exception& e) {
+#pragma omp critical
+        err = e.what();
     }
     }
+    if (!err.empty()) throw std::runtime_error(err);
 
     const double t_b = tnow();
     // ---- merge the parts in ket-sector order: prefix offsets, one allocation, parallel copy ----
