@@ -96,6 +96,91 @@ struct BPart {
     std::vector<Coh> coh;
 };
 
+// MPO entries bucketed by the charge difference D of the (bra, ket) sector pair they can
+// contribute to.  In a symmetric boundary every block (cohort, b) has the same cohort charge
+// difference q(b), and a TwoU1 operator changes the charge by a fixed amount, so an entry
+// (line m, other index x, operator o) contributes only when D = sign * q(x) + dq(o), with
+// (sign, the operator's change) fixed by the step direction.  Entries whose key is not
+// defined (an index seen with two differences, an operator with mixed changes) go to every
+// bucket; entries whose other index has no block in the boundary contribute nothing and are
+// dropped.  Within a bucket the entries keep the line order of the MPO tensor.
+struct EntryBuckets {
+    std::vector<Charge> keys;
+    std::vector<std::vector<uint32_t>> ptr, ent;  // per bucket: CSR over lines -> entry index
+    int wild = -1;                                // bucket of the keyless entries alone
+    int find(Charge d) const {
+        for (std::size_t i = 0; i < keys.size(); ++i)
+            if (keys[i] == d) return int(i);
+        return wild;
+    }
+};
+
+// by_row: lines = rows b1 (entry order of row_ptr), other index b2, key = -q(b2) - dq;
+// otherwise lines = columns b2 (col_ptr / col_ent order), other index b1, key = q(b1) + dq.
+EntryBuckets bucket_entries(const MPOTensor& W, const BoundaryIndexH& B, const Index& phys, bool by_row) {
+    StateMap sm(phys);
+    const uint32_t nst = uint32_t(sm.nstates());
+    // q(b): cohort charge difference (bra - ket) of the blocks at MPO index b
+    std::vector<Charge> qb(B.aux);
+    std::vector<uint8_t> qstate(B.aux, 0);  // 0 = no block, 1 = defined, 2 = inconsistent
+    for (uint32_t c = 0; c < B.n_cohorts(); ++c) {
+        const Charge d = B.bra[B.cbra[c]].first - B.ket[B.cket[c]].first;
+        for (uint32_t b = 0; b < B.aux; ++b) {
+            if (B.offsets[std::size_t(c) * B.aux + b] < 0) continue;
+            if (qstate[b] == 0) { qb[b] = d; qstate[b] = 1; }
+            else if (qstate[b] == 1 && !(qb[b] == d)) qstate[b] = 2;
+        }
+    }
+    // dq(o) = q(out) - q(in) of every term of operator o
+    const std::size_t nops = W.ops->size();
+    std::vector<Charge> dq(nops);
+    std::vector<uint8_t> dstate(nops, 0);
+    for (std::size_t o = 0; o < nops; ++o) {
+        const SparseOp& op = (*W.ops)[o];
+        for (std::size_t e = 0; e < op.val.size(); ++e) {
+            if (op.in[e] >= nst || op.out[e] >= nst) { dstate[o] = 2; break; }
+            const Charge d = phys[sm.sector[op.out[e]]].first - phys[sm.sector[op.in[e]]].first;
+            if (dstate[o] == 0) { dq[o] = d; dstate[o] = 1; }
+            else if (!(dq[o] == d)) { dstate[o] = 2; break; }
+        }
+    }
+    const uint32_t nlines = by_row ? W.rows : W.cols;
+    const std::vector<uint32_t>& lptr = by_row ? W.row_ptr : W.col_ptr;
+    EntryBuckets eb;
+    // key of each entry (in line order): bucket index, -2 = keyless, -1 = dropped
+    std::vector<int> kb(W.b1.size(), -1);
+    for (uint32_t m = 0; m < nlines; ++m)
+        for (uint32_t q = lptr[m]; q < lptr[m + 1]; ++q) {
+            const uint32_t e = by_row ? q : W.col_ent[q];
+            const uint32_t x = by_row ? W.b2[e] : W.b1[e], o = W.op[e];
+            if (x >= B.aux || qstate[x] == 0) continue;  // no block: the entry contributes nothing
+            if (qstate[x] == 2 || dstate[o] != 1) { kb[q] = -2; continue; }
+            const Charge key = by_row ? -qb[x] - dq[o] : qb[x] + dq[o];
+            std::size_t i = 0;
+            while (i < eb.keys.size() && !(eb.keys[i] == key)) ++i;
+            if (i == eb.keys.size()) eb.keys.push_back(key);
+            kb[q] = int(i);
+        }
+    const std::size_t nk = eb.keys.size();
+    eb.wild = int(nk);
+    eb.ptr.assign(nk + 1, std::vector<uint32_t>(nlines + 1, 0));
+    eb.ent.assign(nk + 1, {});
+    for (uint32_t m = 0; m < nlines; ++m) {
+        for (std::size_t i = 0; i <= nk; ++i) eb.ptr[i][m] = uint32_t(eb.ent[i].size());
+        for (uint32_t q = lptr[m]; q < lptr[m + 1]; ++q) {
+            const uint32_t e = by_row ? q : W.col_ent[q];
+            if (kb[q] == -1) continue;
+            if (kb[q] == -2) {
+                for (std::size_t i = 0; i <= nk; ++i) eb.ent[i].push_back(e);
+            } else {
+                eb.ent[std::size_t(kb[q])].push_back(e);
+            }
+        }
+    }
+    for (std::size_t i = 0; i <= nk; ++i) eb.ptr[i][nlines] = uint32_t(eb.ent[i].size());
+    return eb;
+}
+
 // One cohort's terms of one unit: lines = distinct MPO line indices in visiting order (they
 // ascend), terms = (local line, slice id)
 struct UnitTerms {
@@ -360,6 +445,7 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
     sb.cg.set_boundary(R);
     const int32_t* Rpos = sb.cg.b_pos.data();
     const std::size_t Raux = R.aux;
+    const EntryBuckets eb = bucket_entries(W, R, phys, true);
 
     std::vector<BPart> parts(nl);
     std::string err;
@@ -436,10 +522,14 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
                 }
             }
             std::fill(line_count.begin(), line_count.end(), 0);
+            const int bk = eb.find(lc_bra - lc_ket);
+            const std::vector<uint32_t>& bptr = eb.ptr[bk];
+            const std::vector<uint32_t>& bent = eb.ent[bk];
             for (uint32_t b1 = 0; b1 < W.rows; ++b1) {
+                if (bptr[b1] == bptr[b1 + 1]) continue;
                 if (symmetric && lc_ket < lc_bra && W.herm_left[b1] >= 0) continue;
-                for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
-                    const uint32_t b2 = W.b2[e], o = W.op[e];
+                for (uint32_t qi = bptr[b1]; qi < bptr[b1 + 1]; ++qi) {
+                    const uint32_t e = bent[qi], b2 = W.b2[e], o = W.op[e];
                     for (uint32_t k = oc.ptr[o]; k < oc.ptr[o + 1]; ++k) {
                         const int u = unit_of[oc.out[k]];
                         if (u < 0) continue;
@@ -625,6 +715,7 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
     sb.cg.set_boundary(L);
     const int32_t* Lpos = sb.cg.b_pos.data();
     const std::size_t Laux = L.aux;
+    const EntryBuckets eb = bucket_entries(W, L, phys, false);
 
     std::vector<BPart> parts(nr);
     std::string err;
@@ -705,10 +796,14 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
                 }
             }
             std::fill(line_count.begin(), line_count.end(), 0);
+            const int bk = eb.find(rc_bra - rc_ket);
+            const std::vector<uint32_t>& bptr = eb.ptr[bk];
+            const std::vector<uint32_t>& bent = eb.ent[bk];
             for (uint32_t b2 = 0; b2 < W.cols; ++b2) {
+                if (bptr[b2] == bptr[b2 + 1]) continue;
                 if (symmetric && rc_bra < rc_ket && W.herm_right[b2] >= 0) continue;
-                for (uint32_t q = W.col_ptr[b2]; q < W.col_ptr[b2 + 1]; ++q) {
-                    const uint32_t e = W.col_ent[q], b1 = W.b1[e], o = W.op[e];
+                for (uint32_t qi = bptr[b2]; qi < bptr[b2 + 1]; ++qi) {
+                    const uint32_t e = bent[qi], b1 = W.b1[e], o = W.op[e];
                     for (uint32_t k = oc.ptr[o]; k < oc.ptr[o + 1]; ++k) {
                         const int u = unit_of[oc.out[k]];
                         if (u < 0) continue;
