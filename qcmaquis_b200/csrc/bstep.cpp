@@ -50,22 +50,13 @@ void add_tiles(std::vector<TileD>* tiles, uint32_t item, uint32_t M, uint32_t N)
         for (uint32_t m0 = 0; m0 < M; m0 += bm) tiles[sh].push_back(TileD{item, m0, n0, 0});
 }
 
-// sparse operator entries of an MPO tensor, CSR per operator
+// sparse operator entries of an MPO tensor, CSR per operator (the tensor's cached tables)
 struct OpCSR {
-    std::vector<uint32_t> ptr, in, out;
-    std::vector<double> val;
-    explicit OpCSR(const MPOTensor& W) {
-        const std::size_t n = W.ops->size();
-        ptr.assign(n + 1, 0);
-        for (std::size_t o = 0; o < n; ++o) {
-            const SparseOp& s = (*W.ops)[o];
-            ptr[o] = uint32_t(in.size());
-            in.insert(in.end(), s.in.begin(), s.in.end());
-            out.insert(out.end(), s.out.begin(), s.out.end());
-            val.insert(val.end(), s.val.begin(), s.val.end());
-        }
-        ptr[n] = uint32_t(in.size());
-    }
+    std::shared_ptr<const MPOTables> t;
+    const std::vector<uint32_t>& ptr;
+    const std::vector<uint32_t>& in;
+    const std::vector<uint32_t>& out;
+    explicit OpCSR(const MPOTensor& W) : t(W.tables()), ptr(t->optr), in(t->oin), out(t->oout) {}
 };
 
 // cohort of (sector a, sector b) by positions, and its storage partner
@@ -441,7 +432,8 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
 
     // coefficient generation: lines iterate MPO rows b1, slices come from R_old cohorts
     SBuild sb;
-    sb.cg.set_mpo(W, nst, true);
+    sb.cg.set_mpo(W, true);
+    if (sb.cg.nst != nst) throw std::runtime_error("boundary_step_right: MPO physical basis differs from the MPS");
     sb.cg.set_boundary(R);
     const int32_t* Rpos = sb.cg.b_pos.data();
     const std::size_t Raux = R.aux;
@@ -711,7 +703,8 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
 
     // coefficient generation: lines iterate MPO columns b2, slices come from L_old cohorts
     SBuild sb;
-    sb.cg.set_mpo(W, nst, false);
+    sb.cg.set_mpo(W, false);
+    if (sb.cg.nst != nst) throw std::runtime_error("boundary_step_left: MPO physical basis differs from the MPS");
     sb.cg.set_boundary(L);
     const int32_t* Lpos = sb.cg.b_pos.data();
     const std::size_t Laux = L.aux;

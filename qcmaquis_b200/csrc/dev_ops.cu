@@ -83,15 +83,35 @@ __global__ void k_bcopy(const CopyJob* __restrict__ jobs, uint32_t njobs, const 
 }
 
 // out[j] = <V_j, w>; one CTA per j, fixed-order tree reduction (deterministic)
-__global__ void __launch_bounds__(256) k_dots(const double* __restrict__ V, uint64_t ldv, const double* __restrict__ w,
-                                              uint64_t n, double* __restrict__ out) {
+// partial sums of <V_j, w>: block (b, j) takes i = b*256 + t (+ k * DOT_PARTS*256), two
+// interleaved accumulators per thread, then a tree over the block
+__global__ void __launch_bounds__(256) k_dots_part(const double* __restrict__ V, uint64_t ldv, const double* __restrict__ w,
+                                                   uint64_t n, double* __restrict__ part) {
     __shared__ double red[256];
-    const double* v = V + blockIdx.x * ldv;
-    double s = 0.0;
-    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) s = fma(v[i], w[i], s);
-    red[threadIdx.x] = s;
+    const double* v = V + uint64_t(blockIdx.y) * ldv;
+    const uint64_t stride = uint64_t(DOT_PARTS) * 256;
+    double s0 = 0.0, s1 = 0.0;
+    uint64_t i = uint64_t(blockIdx.x) * 256 + threadIdx.x;
+    for (; i + stride < n; i += 2 * stride) {
+        s0 = fma(v[i], w[i], s0);
+        s1 = fma(v[i + stride], w[i + stride], s1);
+    }
+    if (i < n) s0 = fma(v[i], w[i], s0);
+    red[threadIdx.x] = s0 + s1;
     __syncthreads();
     for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[uint64_t(blockIdx.y) * DOT_PARTS + blockIdx.x] = red[0];
+}
+
+// out[j] = tree sum of the DOT_PARTS partials of product j
+__global__ void __launch_bounds__(DOT_PARTS) k_dots_sum(const double* __restrict__ part, double* __restrict__ out) {
+    __shared__ double red[DOT_PARTS];
+    red[threadIdx.x] = part[uint64_t(blockIdx.x) * DOT_PARTS + threadIdx.x];
+    __syncthreads();
+    for (int h = DOT_PARTS / 2; h > 0; h >>= 1) {
         if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
         __syncthreads();
     }
@@ -193,9 +213,12 @@ void batched_copy(const std::vector<CopyJob>& jobs, const double* src, uint64_t 
     QCM_CUDA(cudaStreamSynchronize(s));
 }
 
-void dev_dots(const double* V, uint64_t ldv, uint32_t m, const double* w, uint64_t n, double* out, cudaStream_t s) {
+void dev_dots(const double* V, uint64_t ldv, uint32_t m, const double* w, uint64_t n, double* out, double* scratch,
+              cudaStream_t s) {
     if (!m) return;
-    k_dots<<<m, 256, 0, s>>>(V, ldv, w, n, out);
+    if (m > 65535) throw std::runtime_error("dev_dots: too many products");
+    k_dots_part<<<dim3(DOT_PARTS, m), 256, 0, s>>>(V, ldv, w, n, scratch);
+    k_dots_sum<<<m, DOT_PARTS, 0, s>>>(scratch, out);
     QCM_CUDA(cudaGetLastError());
 }
 

@@ -45,8 +45,13 @@ void batched_copy(const std::vector<CopyJob>& jobs, const double* src, uint64_t 
 // throws unless the rows x cols column-major sub-matrix at off (leading dimension ld) lies in [0, len)
 void check_extent(uint64_t off, uint64_t rows, uint64_t cols, uint64_t ld, uint64_t len, const char* what);
 
-// Vector algebra (length n): out[j] = <V_j, w> for j < m (V_j at V + j*ldv), written to device out
-void dev_dots(const double* V, uint64_t ldv, uint32_t m, const double* w, uint64_t n, double* out, cudaStream_t s);
+// Vector algebra (length n): out[j] = <V_j, w> for j < m (V_j at V + j*ldv), written to device out.
+// Two passes: DOT_PARTS partial sums per product over a fixed strided partition of [0, n), then
+// a fixed-order tree over the partials, so the result is reproducible and does not depend on
+// the device; scratch holds m * DOT_PARTS doubles.
+constexpr unsigned DOT_PARTS = 256;
+void dev_dots(const double* V, uint64_t ldv, uint32_t m, const double* w, uint64_t n, double* out, double* scratch,
+              cudaStream_t s);
 // y = sum_j c[j] * V_j  (c on device, m <= 64), or y += ...
 void dev_lincomb(const double* V, uint64_t ldv, uint32_t m, const double* c, uint64_t n, double* y, bool accumulate,
                  cudaStream_t s);

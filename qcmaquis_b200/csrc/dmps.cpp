@@ -163,8 +163,8 @@ DMPS right_paired_copy(Ctx& c, const DMPS& t) {
 
 double norm2(Ctx& c, const DBlocks& b) {
     if (!b.total) return 0.0;
-    Ctx::ensure(c.scal, 64);
-    dev_dots(b.d.get(), 0, 1, b.d.get(), b.total, c.scal.get(), c.s);
+    Ctx::ensure(c.scal, 64 + DOT_PARTS);
+    dev_dots(b.d.get(), 0, 1, b.d.get(), b.total, c.scal.get(), c.scal.get() + 64, c.s);
     double r = 0;
     QCM_CUDA(cudaMemcpyAsync(&r, c.scal.get(), sizeof(double), cudaMemcpyDeviceToHost, c.s));
     QCM_CUDA(cudaStreamSynchronize(c.s));

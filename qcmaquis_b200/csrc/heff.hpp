@@ -131,6 +131,22 @@ struct WGenUnitD {
 struct WGenInD { uint32_t c, jbase; };  // per (unit, input state): boundary cohort and slice-id base, or WGEN_NONE
 constexpr uint32_t WGEN_NONE = 0xffffffffu;
 
+struct MPOTables {
+    uint32_t nst = 0;     // states of the physical index
+    std::size_t nops = 0;
+    // operator terms, CSR per operator: (input state, output state, value)
+    std::vector<uint32_t> optr, oin, oout;
+    std::vector<double> oval;
+    // the same grouped by (operator, output state), in their order within the operator
+    std::vector<uint32_t> o_ptr, o_in;
+    std::vector<double> o_val;
+    // MPO entries by row b1 (other index b2) and by column b2 (other index b1, increasing b1)
+    std::vector<uint32_t> row_ptr, row_other, row_op, col_ptr, col_other, col_op;
+    std::vector<double> row_scale, col_scale;
+    uint32_t rows = 0, cols = 0;
+};
+std::shared_ptr<const MPOTables> build_mpo_tables(const MPOTensor& W);
+
 struct CoefGen {
     hvec<WGenUnitD> units;
     hvec<WGenInD> gin;  // units x nst
@@ -138,10 +154,8 @@ struct CoefGen {
     hvec<double> line_scale;
     hvec<uint32_t> smap_id, smap_slot;
     uint32_t nst = 0;
-    std::vector<uint32_t> m_ptr, m_other, m_op;  // MPO entries grouped by line index
-    std::vector<double> m_scale;
-    std::vector<uint32_t> o_ptr, o_in;  // operator terms by (operator, output state): input state, value
-    std::vector<double> o_val;
+    std::shared_ptr<const MPOTables> mt;  // MPO entries (by row or column) and operator terms
+    bool by_row = true;
     std::vector<int32_t> b_pos;  // boundary cohort x aux: block position of the MPO index, or -1
     const std::vector<double>* b_cs = nullptr;  // boundary conj scales (cohort x aux)
     uint32_t b_aux = 0;
@@ -154,8 +168,8 @@ struct CoefGen {
     DBuf<int32_t> d_b_pos;
 
     // MPO entries by row b1 (other index b2) or by column b2 (other index b1, in increasing b1),
-    // and the operator terms; nst = physical states
-    void set_mpo(const MPOTensor& W, uint32_t nst, bool by_row);
+    // and the operator terms
+    void set_mpo(const MPOTensor& W, bool by_row);
     void set_boundary(const BoundaryIndexH& B);
     // appends one unit: its lines (MPO index and scale each), slot -> slice id, and the
     // (cohort, slice-id base) of each of the nst input states

@@ -244,22 +244,12 @@ __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ u
 void CoefGen::validate() const {
     const std::size_t nu = units.size();
     auto bad = [](const char* what) { throw std::runtime_error(std::string("coefficient tables: ") + what); };
+    if (!mt || mt->nst != nst) bad("MPO tables");
     if (nst > WG_NST || gin.size() != nu * nst || line_scale.size() != line_major.size() || smap_slot.size() != smap_id.size())
         bad("unit tables");
-    if (m_ptr.empty() || m_ptr.back() != m_other.size() || m_op.size() != m_other.size() || m_scale.size() != m_other.size())
-        bad("MPO entries");
-    const std::size_t nmaj = m_ptr.size() - 1;
-    const std::size_t nops = nst ? (o_ptr.size() - 1) / nst : 0;
-    if (o_ptr.empty() || o_ptr.size() != nops * nst + 1 || o_ptr.back() != o_in.size() || o_val.size() != o_in.size())
-        bad("operator terms");
-    for (std::size_t i = 0; i < nmaj; ++i)
-        if (m_ptr[i] > m_ptr[i + 1]) bad("MPO pointers");
-    for (std::size_t e = 0; e < m_other.size(); ++e)
-        if (m_other[e] >= b_aux || m_op[e] >= nops) bad("MPO entry");
-    for (std::size_t i = 0; i + 1 < o_ptr.size(); ++i)
-        if (o_ptr[i] > o_ptr[i + 1]) bad("operator pointers");
-    for (uint32_t v : o_in)
-        if (v >= nst) bad("operator input state");
+    // the MPO tables were checked when built (indices inside the tensor); here: against the boundary
+    const uint32_t nmaj = by_row ? mt->rows : mt->cols, nother = by_row ? mt->cols : mt->rows;
+    if (nother > b_aux) bad("MPO index outside the boundary");
     if (!b_cs || b_cs->size() != b_pos.size() || (b_aux && b_pos.size() % b_aux)) bad("boundary tables");
     const std::size_t ncoh = b_aux ? b_pos.size() / b_aux : 0;
     for (const WGenInD& g : gin)
@@ -285,13 +275,13 @@ void CoefGen::upload(cudaStream_t s) {
     d_line_scale.upload(line_scale, s);
     d_smap_id.upload(smap_id, s);
     d_smap_slot.upload(smap_slot, s);
-    d_m_ptr.upload(m_ptr, s);
-    d_m_other.upload(m_other, s);
-    d_m_op.upload(m_op, s);
-    d_m_scale.upload(m_scale, s);
-    d_o_ptr.upload(o_ptr, s);
-    d_o_in.upload(o_in, s);
-    d_o_val.upload(o_val, s);
+    d_m_ptr.upload(by_row ? mt->row_ptr : mt->col_ptr, s);
+    d_m_other.upload(by_row ? mt->row_other : mt->col_other, s);
+    d_m_op.upload(by_row ? mt->row_op : mt->col_op, s);
+    d_m_scale.upload(by_row ? mt->row_scale : mt->col_scale, s);
+    d_o_ptr.upload(mt->o_ptr, s);
+    d_o_in.upload(mt->o_in, s);
+    d_o_val.upload(mt->o_val, s);
     d_b_pos.upload(b_pos, s);
     d_b_cs.upload(*b_cs, s);
 }

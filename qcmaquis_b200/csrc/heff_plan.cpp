@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -139,50 +140,72 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t 
     }
 }
 
-void CoefGen::set_mpo(const MPOTensor& W, uint32_t nst_, bool by_row) {
-    nst = nst_;
-    const std::size_t nops = W.ops->size(), nent = W.b2.size();
-    if (W.b1.size() != nent || W.op.size() != nent || W.scale.size() != nent) throw std::runtime_error("coefficient tables: inconsistent MPO tensor");
-    if (by_row) {
-        if (W.row_ptr.size() != std::size_t(W.rows) + 1 || W.row_ptr.back() != nent) throw std::runtime_error("coefficient tables: MPO row pointers");
-        m_ptr.assign(W.row_ptr.begin(), W.row_ptr.end());
-        m_other.assign(W.b2.begin(), W.b2.end());
-        m_op.assign(W.op.begin(), W.op.end());
-        m_scale.assign(W.scale.begin(), W.scale.end());
-    } else {
-        if (W.col_ptr.size() != std::size_t(W.cols) + 1 || W.col_ptr.back() != nent || W.col_ent.size() != nent)
-            throw std::runtime_error("coefficient tables: MPO column pointers");
-        m_ptr.assign(W.col_ptr.begin(), W.col_ptr.end());
-        m_other.resize(nent); m_op.resize(nent); m_scale.resize(nent);
-        for (std::size_t q = 0; q < nent; ++q) {
-            const uint32_t e = W.col_ent[q];
-            if (e >= nent) throw std::runtime_error("coefficient tables: MPO column entry");
-            m_other[q] = W.b1[e]; m_op[q] = W.op[e]; m_scale[q] = W.scale[e];
-        }
-    }
-    for (std::size_t q = 0; q < nent; ++q)
-        if (m_op[q] >= nops) throw std::runtime_error("coefficient tables: MPO operator index");
-    // operator terms grouped by (operator, output state), in their order within the operator
-    o_ptr.assign(nops * nst + 1, 0);
+std::shared_ptr<const MPOTables> build_mpo_tables(const MPOTensor& W) {
+    auto t = std::make_shared<MPOTables>();
+    t->nst = uint32_t(StateMap(W.phys).nstates());
+    t->nops = W.ops ? W.ops->size() : 0;
+    t->rows = W.rows; t->cols = W.cols;
+    const uint32_t nst = t->nst;
+    const std::size_t nops = t->nops, nent = W.b2.size();
+    if (W.b1.size() != nent || W.op.size() != nent || W.scale.size() != nent) throw std::runtime_error("MPO tables: inconsistent MPO tensor");
+    if (W.row_ptr.size() != std::size_t(W.rows) + 1 || W.row_ptr.back() != nent || W.col_ptr.size() != std::size_t(W.cols) + 1 ||
+        W.col_ptr.back() != nent || W.col_ent.size() != nent)
+        throw std::runtime_error("MPO tables: MPO tensor is not finalized");
+    for (std::size_t i = 0; i < W.rows; ++i)
+        if (W.row_ptr[i] > W.row_ptr[i + 1]) throw std::runtime_error("MPO tables: row pointers");
+    for (std::size_t i = 0; i < W.cols; ++i)
+        if (W.col_ptr[i] > W.col_ptr[i + 1]) throw std::runtime_error("MPO tables: column pointers");
+    for (std::size_t e = 0; e < nent; ++e)
+        if (W.b1[e] >= W.rows || W.b2[e] >= W.cols || W.op[e] >= nops || W.col_ent[e] >= nent)
+            throw std::runtime_error("MPO tables: entry out of range");
+    // operator terms
+    t->optr.assign(nops + 1, 0);
     for (std::size_t o = 0; o < nops; ++o) {
         const SparseOp& op = (*W.ops)[o];
+        if (op.in.size() != op.val.size() || op.out.size() != op.val.size()) throw std::runtime_error("MPO tables: operator arrays");
+        t->optr[o] = uint32_t(t->oin.size());
         for (std::size_t e = 0; e < op.val.size(); ++e) {
-            if (op.in[e] >= nst || op.out[e] >= nst) throw std::runtime_error("coefficient tables: operator entry outside the physical basis");
-            o_ptr[o * nst + op.out[e] + 1]++;
+            if (op.in[e] >= nst || op.out[e] >= nst) throw std::runtime_error("MPO tables: operator entry outside the physical basis");
+            t->oin.push_back(op.in[e]); t->oout.push_back(op.out[e]); t->oval.push_back(op.val[e]);
         }
     }
-    for (std::size_t i = 0; i < nops * nst; ++i) o_ptr[i + 1] += o_ptr[i];
-    o_in.resize(o_ptr.back());
-    o_val.resize(o_ptr.back());
-    std::vector<uint32_t> fill(o_ptr.begin(), o_ptr.end() - 1);
-    for (std::size_t o = 0; o < nops; ++o) {
-        const SparseOp& op = (*W.ops)[o];
-        for (std::size_t e = 0; e < op.val.size(); ++e) {
-            const uint32_t d = fill[o * nst + op.out[e]]++;
-            o_in[d] = op.in[e];
-            o_val[d] = op.val[e];
+    t->optr[nops] = uint32_t(t->oin.size());
+    t->o_ptr.assign(nops * nst + 1, 0);
+    for (std::size_t o = 0; o < nops; ++o)
+        for (uint32_t k = t->optr[o]; k < t->optr[o + 1]; ++k) t->o_ptr[o * nst + t->oout[k] + 1]++;
+    for (std::size_t i = 0; i < nops * nst; ++i) t->o_ptr[i + 1] += t->o_ptr[i];
+    t->o_in.resize(t->oin.size());
+    t->o_val.resize(t->oin.size());
+    std::vector<uint32_t> fill(t->o_ptr.begin(), t->o_ptr.end() - 1);
+    for (std::size_t o = 0; o < nops; ++o)
+        for (uint32_t k = t->optr[o]; k < t->optr[o + 1]; ++k) {
+            const uint32_t d = fill[o * nst + t->oout[k]]++;
+            t->o_in[d] = t->oin[k];
+            t->o_val[d] = t->oval[k];
         }
+    // entries by row and by column
+    t->row_ptr = W.row_ptr;
+    t->row_other = W.b2; t->row_op = W.op; t->row_scale = W.scale;
+    t->col_ptr = W.col_ptr;
+    t->col_other.resize(nent); t->col_op.resize(nent); t->col_scale.resize(nent);
+    for (std::size_t q = 0; q < nent; ++q) {
+        const uint32_t e = W.col_ent[q];
+        t->col_other[q] = W.b1[e]; t->col_op[q] = W.op[e]; t->col_scale[q] = W.scale[e];
     }
+    return t;
+}
+
+std::shared_ptr<const MPOTables> MPOTensor::tables() const {
+    static std::mutex m;
+    std::lock_guard<std::mutex> g(m);
+    if (!tables_) tables_ = build_mpo_tables(*this);
+    return tables_;
+}
+
+void CoefGen::set_mpo(const MPOTensor& W, bool row) {
+    mt = W.tables();
+    nst = mt->nst;
+    by_row = row;
 }
 
 void CoefGen::set_boundary(const BoundaryIndexH& B) {
@@ -236,6 +259,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     if (!(phys == W.phys)) throw std::runtime_error("heff plan: MPS physical index differs from the MPO's");
     if (W.rows != L.aux || W.cols != R.aux)
         throw std::runtime_error("heff plan: MPO bond dimensions do not match the boundaries");
+    const double t_0 = std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
     auto p = std::make_unique<HeffPlan>();
     p->phys = phys; p->left = left; p->right = right;
     p->L = &Lb; p->R = &Rb;
@@ -272,21 +296,15 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             Rci[std::size_t(a) * nr + b] = ci;
             Rcie[std::size_t(a) * nr + b] = ce;
         }
-    // op entries, CSR per operator: (input state, output state, value)
-    const std::size_t nops = W.ops->size();
-    std::vector<uint32_t> optr(nops + 1, 0), oin, oout;
-    std::vector<double> oval;
-    for (std::size_t o = 0; o < nops; ++o) {
-        const SparseOp& s = (*W.ops)[o];
-        optr[o] = uint32_t(oin.size());
-        for (std::size_t e = 0; e < s.val.size(); ++e) {
-            if (s.in[e] >= nst || s.out[e] >= nst) throw std::runtime_error("heff plan: operator entry outside the physical basis");
-            oin.push_back(s.in[e]); oout.push_back(s.out[e]); oval.push_back(s.val[e]);
-        }
-    }
-    optr[nops] = uint32_t(oin.size());
+    // operator terms, CSR per operator: (input state, output state, value)
+    const std::shared_ptr<const MPOTables> mt = W.tables();
+    if (mt->nst != nst) throw std::runtime_error("heff plan: MPO physical basis differs");
+    const std::vector<uint32_t>& optr = mt->optr;
+    const std::vector<uint32_t>& oin = mt->oin;
+    const std::vector<uint32_t>& oout = mt->oout;
+    const std::vector<double>& oval = mt->oval;
     // coefficient generation: lines iterate MPO rows b1, slices come from R cohorts
-    p->cg.set_mpo(W, nst, true);
+    p->cg.set_mpo(W, true);
     p->cg.set_boundary(R);
 
     std::vector<Part> parts(nl);
@@ -585,8 +603,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         p->outs.push_back(o);
     }
     if (tdbg)
-        std::fprintf(stderr, "plan: tables+parts %.3f s, merge %.3f s; %zu units, %llu coefficient terms, %zu S tiles, "
-                     "%.3e dense coefficients\n", t_b - t_a, tnow() - t_b, p->units.size(), (unsigned long long)p->n_alpha,
+        std::fprintf(stderr, "plan: tables %.4f s, parts %.4f s, merge %.4f s; %zu units, %llu coefficient terms, %zu S tiles, "
+                     "%.3e dense coefficients\n", t_a - t_0, t_b - t_a, tnow() - t_b, p->units.size(), (unsigned long long)p->n_alpha,
                      p->utiles[0].size() + p->utiles[1].size() + p->utiles[2].size() + p->utiles[3].size(), double(p->w_len));
     uint64_t pl = 0;
     for (int sh = 0; sh < N_SHAPES; ++sh) pl = std::max<uint64_t>(pl, uint64_t(p->kitems[sh].size()) * shape_bm(sh) * shape_bn(sh));

@@ -26,6 +26,8 @@ struct SparseOp {
     std::vector<double> val;
 };
 
+struct MPOTables;  // lookup tables derived from a finalized tensor (operator terms, entry layouts)
+
 struct MPOTensor {
     uint32_t rows = 1, cols = 1;
     // entries sorted by (b1, b2); several consecutive entries may share (b1, b2)
@@ -40,6 +42,10 @@ struct MPOTensor {
     std::vector<uint32_t> row_ptr;   // CSR over entries (entries already row sorted)
     std::vector<uint32_t> col_ptr, col_ent;  // CSC: entries of column b2, increasing b1
     void finalize();
+    // derived tables, built (and checked) on first use and shared by every schedule built
+    // from this tensor; finalize() drops them
+    std::shared_ptr<const MPOTables> tables() const;
+    mutable std::shared_ptr<const MPOTables> tables_;
 };
 
 struct MPO {

@@ -30,6 +30,7 @@
 namespace qcm {
 
 void MPOTensor::finalize() {
+    tables_.reset();
     row_ptr.assign(rows + 1, 0);
     for (auto r : b1) row_ptr[r + 1]++;
     for (uint32_t r = 0; r < rows; ++r) row_ptr[r + 1] += row_ptr[r];

@@ -38,13 +38,14 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
     const uint64_t n = p.x_len, ld = (n + 31) / 32 * 32;
     // V[0..maxiter), VA[0..maxiter), u, r
     Ctx::ensure(c.jd, (2 * uint64_t(maxiter) + 2) * ld);
-    Ctx::ensure(c.scal, 256);
+    Ctx::ensure(c.scal, 256 + 64 * uint64_t(DOT_PARTS));
     Ctx::ensure(c.coef, 64);
     double* V = c.jd.get();
     double* VA = V + uint64_t(maxiter) * ld;
     double* u = VA + uint64_t(maxiter) * ld;
     double* r = u + ld;
     double* sc = c.scal.get();
+    double* dsc = sc + 256;  // dot-product partials
     auto Vi = [&](int i) { return V + uint64_t(i) * ld; };
     auto VAi = [&](int i) { return VA + uint64_t(i) * ld; };
     QCM_CUDA(cudaMemcpyAsync(Vi(0), x, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
@@ -56,12 +57,12 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         // modified Gram-Schmidt against V[0..it), repeated once if the norm dropped below 1/4
         auto mgs = [&]() {
             for (int i = 0; i < it; ++i) {
-                dev_dots(Vi(i), 0, 1, t, n, sc + 2 + i, c.s);
+                dev_dots(Vi(i), 0, 1, t, n, sc + 2 + i, dsc, c.s);
                 dev_axpy_dscalar(sc + 2 + i, -1.0, Vi(i), t, n, c.s);
             }
-            dev_dots(t, 0, 1, t, n, sc + 1, c.s);
+            dev_dots(t, 0, 1, t, n, sc + 1, dsc, c.s);
         };
-        dev_dots(t, 0, 1, t, n, sc, c.s);
+        dev_dots(t, 0, 1, t, n, sc, dsc, c.s);
         mgs();
         double h2[2];
         download(c, sc, h2, 2);
@@ -74,7 +75,7 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         dev_axpby(1.0 / tn, t, 0.0, t, n, c.s);
         heff_apply_device(p, t, VAi(it));
         // column it of the projected matrix: <V_i, A V_it>
-        dev_dots(V, ld, uint32_t(it + 1), VAi(it), n, sc + 80, c.s);
+        dev_dots(V, ld, uint32_t(it + 1), VAi(it), n, sc + 80, dsc, c.s);
         std::vector<double> col(it + 1);
         download(c, sc + 80, col.data(), col.size());
         for (int i = 0; i <= it; ++i) M[i + std::size_t(it) * maxiter] = col[i];
@@ -84,9 +85,9 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         // r = A u - theta u
         dev_lincomb(VA, ld, uint32_t(it + 1), c.coef.get(), n, r, false, c.s);
         dev_axpby(-theta, u, 1.0, r, n, c.s);
-        dev_dots(r, 0, 1, r, n, sc + 160, c.s);
-        dev_dots(r, 0, 1, u, n, sc + 161, c.s);
-        dev_dots(u, 0, 1, u, n, sc + 162, c.s);
+        dev_dots(r, 0, 1, r, n, sc + 160, dsc, c.s);
+        dev_dots(r, 0, 1, u, n, sc + 161, dsc, c.s);
+        dev_dots(u, 0, 1, u, n, sc + 162, dsc, c.s);
         double h3[3];
         download(c, sc + 160, h3, 3);
         ++it;
