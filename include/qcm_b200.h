@@ -275,6 +275,28 @@ int qcm_dmrg_pending_export(qcm_dmrg* d, int flags, void* buf, size_t cap, size_
 int qcm_dmrg_bond_dimensions(const qcm_dmrg* d, uint64_t* dims);
 void qcm_dmrg_free(qcm_dmrg* d);
 
+/* ---- block-matrix truncation ----------------------------------------------
+ * Replaces svd_truncate (block_matrix_algorithms.h:185-240 with estimate_truncation,
+ * :136-183) and heev_truncate (:299-355) for a block matrix given as n_blocks
+ * column-major host blocks concatenated in block order.
+ *
+ * qcm_truncate_svd: thin SVD of every block on the device, then the largest singular
+ * values over all blocks are kept (at most max_bond_dimension of them plus ties, none
+ * below cutoff * s_max).  Outputs per block k, packed in block order with keep[k]
+ * columns: U_k (rows x keep, ld rows), S_k (keep, descending), Vt_k (keep x cols, ld keep).
+ * Size U, S, Vt for keep = min(rows, cols).  A block larger than 1024 in both
+ * dimensions is refused. */
+int qcm_truncate_svd(qcm_ctx* ctx, uint32_t n_blocks, const uint32_t* rows, const uint32_t* cols, const double* blocks,
+                     uint64_t max_bond_dimension, double cutoff, uint32_t* keep, double* U, double* S, double* Vt,
+                     qcm_trunc_result* result);
+/* qcm_truncate_heev: symmetric blocks (density matrices, dims[k] x dims[k]); the cut is on
+ * sqrt of the positive eigenvalues and the truncated fraction is reported in both
+ * truncated_weight and truncated_fraction (as heev_truncate does).  Outputs per block:
+ * U_k (dims x keep, the kept eigenvectors in descending eigenvalue order) and evals
+ * (the kept eigenvalues, descending). */
+int qcm_truncate_heev(qcm_ctx* ctx, uint32_t n_blocks, const uint32_t* dims, const double* blocks, uint64_t max_bond_dimension,
+                      double cutoff, uint32_t* keep, double* U, double* evals, qcm_trunc_result* result);
+
 /* FP64 throughput probes on the current device (TFLOP/s): DMMA (mma.sync
  * m8n8k4 .f64) and DFMA loops.  Roofline denominators of the FP64 form. */
 int qcm_probe_fp64_peaks(double* dmma_tflops, double* dfma_tflops);

@@ -1,5 +1,6 @@
 // ORACLE -- TEST INFRASTRUCTURE ONLY.  extern "C" entry points used by tests/, smoke()
 // and bench.py (cpu_baseline / --impl reference) through ctypes.
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -28,6 +29,26 @@ struct W {
 }  // namespace
 
 struct orc_dmrg { DMRG* d; };
+
+namespace {
+// block k of the host list gets charges (n - 1 - k, 0), so BlockMatrix keeps the input order
+BlockMatrix host_blocks(uint32_t n, const uint32_t* rows, const uint32_t* cols, const double* data) {
+    BlockMatrix M;
+    uint64_t h = 0;
+    for (uint32_t k = 0; k < n; ++k) {
+        Mat m(rows[k], cols[k]);
+        std::copy(data + h, data + h + m.d.size(), m.d.begin());
+        h += m.d.size();
+        M.lc.push_back(Q(int(n - 1 - k), 0));
+        M.rc.push_back(Q(int(n - 1 - k), 0));
+        M.b.push_back(std::move(m));
+    }
+    return M;
+}
+void put_result(const TruncationResults& t, double* res) {
+    res[0] = double(t.bond_dimension); res[1] = t.truncated_weight; res[2] = t.truncated_fraction; res[3] = t.smallest_ev;
+}
+}  // namespace
 
 extern "C" {
 
@@ -211,6 +232,67 @@ int orc_schedule_export(const void* snap, size_t n, const void* mpo_blob, size_t
         *out = dup_blob(w.b, len);
         return 0;
     } catch (const std::exception& e) { return fail(e.what()); }
+}
+
+// svd_truncate on host blocks (column-major, concatenated): per block k keep[k], U_k (rows x
+// keep), S_k (keep), Vt_k (keep x cols) packed in block order; res = (bond dimension,
+// truncated weight, truncated fraction, smallest ev)
+int orc_truncate_svd(uint32_t n, const uint32_t* rows, const uint32_t* cols, const double* blocks, uint64_t Mmax, double cutoff,
+                     uint32_t* keep, double* U, double* S, double* Vt, double* res) {
+    try {
+        BlockMatrix M = host_blocks(n, rows, cols, blocks);
+        BlockMatrix Ub, Vb;
+        std::vector<std::vector<double>> Sv;
+        const TruncationResults tr = svd_truncate(M, Ub, Vb, Sv, cutoff, Mmax);
+        uint64_t pu = 0, ps = 0, pv = 0;
+        std::size_t si = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            const Q q(int(n - 1 - k), 0);
+            const std::size_t i = Ub.find(q, q);
+            if (i == Ub.n_blocks()) { keep[k] = 0; continue; }
+            const Mat& u = Ub.b[i];
+            const Mat& v = Vb.b[Vb.find(q, q)];
+            keep[k] = uint32_t(u.c);
+            std::copy(u.d.begin(), u.d.end(), U + pu);
+            std::copy(Sv[si].begin(), Sv[si].end(), S + ps);
+            std::copy(v.d.begin(), v.d.end(), Vt + pv);
+            pu += u.d.size(); ps += Sv[si].size(); pv += v.d.size();
+            ++si;
+        }
+        put_result(tr, res);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e.what());
+    }
+}
+
+// heev_truncate on host symmetric blocks: per block keep[k], U_k (dim x keep, descending) and
+// the kept eigenvalues (descending), packed in block order
+int orc_truncate_heev(uint32_t n, const uint32_t* dims, const double* blocks, uint64_t Mmax, double cutoff, uint32_t* keep,
+                      double* U, double* evals, double* res) {
+    try {
+        BlockMatrix dm = host_blocks(n, dims, dims, blocks);
+        BlockMatrix Ub;
+        const TruncationResults tr = heev_truncate(dm, Ub, cutoff, Mmax);
+        uint64_t pu = 0, pe = 0;
+        for (uint32_t k = 0; k < n; ++k) {
+            const Q q(int(n - 1 - k), 0);
+            const std::size_t i = Ub.find(q, q);
+            if (i == Ub.n_blocks()) { keep[k] = 0; continue; }
+            const Mat& u = Ub.b[i];
+            keep[k] = uint32_t(u.c);
+            std::copy(u.d.begin(), u.d.end(), U + pu);
+            Mat ev;
+            std::vector<double> w;
+            heev_desc(dm.b[k], ev, w);
+            std::copy(w.begin(), w.begin() + long(u.c), evals + pe);
+            pu += u.d.size(); pe += u.c;
+        }
+        put_result(tr, res);
+        return 0;
+    } catch (const std::exception& e) {
+        return fail(e.what());
+    }
 }
 
 }  // extern "C"

@@ -58,6 +58,11 @@ def lib(nthreads: int = 0):
                                      c_int, P(c_double), P(c_double)]
         L.orc_schedule_export.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_void_p), P(c_size_t),
                                           P(c_double)]
+        U32 = P(ctypes.c_uint32)
+        L.orc_truncate_svd.argtypes = [ctypes.c_uint32, U32, U32, P(c_double), ctypes.c_uint64, c_double, U32, P(c_double),
+                                       P(c_double), P(c_double), P(c_double)]
+        L.orc_truncate_heev.argtypes = [ctypes.c_uint32, U32, P(c_double), ctypes.c_uint64, c_double, U32, P(c_double),
+                                        P(c_double), P(c_double)]
         _check(L, L.orc_init(openblas_path().encode(), nthreads))
         _lib = L
     return _lib
@@ -164,3 +169,61 @@ def schedule_export(snap: bytes, mpo_blob: bytes, site1: int):
     b = ctypes.string_at(p, n.value)
     L.orc_free(p)
     return b, fl.value
+
+
+def _u32(a):
+    return a.ctypes.data_as(P(ctypes.c_uint32))
+
+
+def truncate_svd(blocks, max_bond_dimension: int, cutoff: float):
+    """svd_truncate (block_matrix_algorithms.h:185-240) of a list of 2-D blocks:
+    ([(U, S, Vt) per block, kept columns only], dict(bond_dimension, truncated_weight,
+    truncated_fraction, smallest_ev))."""
+    L = lib()
+    bl = [np.asarray(b, dtype=np.float64) for b in blocks]
+    rows = np.array([b.shape[0] for b in bl], dtype=np.uint32)
+    cols = np.array([b.shape[1] for b in bl], dtype=np.uint32)
+    k = np.minimum(rows, cols).astype(np.int64)
+    data = np.ascontiguousarray(np.concatenate([b.ravel(order="F") for b in bl]))
+    U = np.zeros(max(1, int((rows * k).sum()))); S = np.zeros(max(1, int(k.sum()))); Vt = np.zeros(max(1, int((k * cols).sum())))
+    keep = np.zeros(len(bl), dtype=np.uint32)
+    res = np.zeros(4)
+    _check(L, L.orc_truncate_svd(len(bl), _u32(rows), _u32(cols), _dp(data), max_bond_dimension, cutoff, _u32(keep), _dp(U),
+                                 _dp(S), _dp(Vt), _dp(res)))
+    return unpack_svd(rows, cols, keep, U, S, Vt), _result(res)
+
+
+def truncate_heev(blocks, max_bond_dimension: int, cutoff: float):
+    """heev_truncate (block_matrix_algorithms.h:299-355) of a list of symmetric blocks:
+    ([(U, evals) per block, kept eigenpairs, descending], result dict)."""
+    L = lib()
+    bl = [np.asarray(b, dtype=np.float64) for b in blocks]
+    dims = np.array([b.shape[0] for b in bl], dtype=np.uint32)
+    data = np.ascontiguousarray(np.concatenate([b.ravel(order="F") for b in bl]))
+    U = np.zeros(max(1, int((dims.astype(np.int64) ** 2).sum()))); ev = np.zeros(max(1, int(dims.sum())))
+    keep = np.zeros(len(bl), dtype=np.uint32)
+    res = np.zeros(4)
+    _check(L, L.orc_truncate_heev(len(bl), _u32(dims), _dp(data), max_bond_dimension, cutoff, _u32(keep), _dp(U), _dp(ev),
+                                  _dp(res)))
+    return unpack_heev(dims, keep, U, ev), _result(res)
+
+
+def _result(res):
+    return {"bond_dimension": int(res[0]), "truncated_weight": res[1], "truncated_fraction": res[2], "smallest_ev": res[3]}
+
+
+def unpack_svd(rows, cols, keep, U, S, Vt):
+    """Per block (U rows x keep, S keep, Vt keep x cols) from the packed column-major arrays."""
+    out, pu, ps, pv = [], 0, 0, 0
+    for m, n, kp in zip(rows.tolist(), cols.tolist(), keep.tolist()):
+        out.append((U[pu:pu + m * kp].reshape(kp, m).T.copy(), S[ps:ps + kp].copy(), Vt[pv:pv + kp * n].reshape(n, kp).T.copy()))
+        pu += m * kp; ps += kp; pv += kp * n
+    return out
+
+
+def unpack_heev(dims, keep, U, ev):
+    out, pu, pe = [], 0, 0
+    for n, kp in zip(dims.tolist(), keep.tolist()):
+        out.append((U[pu:pu + n * kp].reshape(kp, n).T.copy(), ev[pe:pe + kp].copy()))
+        pu += n * kp; pe += kp
+    return out

@@ -8,6 +8,8 @@
 // svd_truncate / estimate_truncation (block_matrix_algorithms.h:136-240) with
 // the per-block SVDs on the device and the global cut on the host.
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <stdexcept>
 #include <string>
@@ -364,53 +366,106 @@ void DTwoSite::twin_to_both(Ctx& c) {
     batched_copy(cj, twin.b.d.get(), twin.b.total, both.d.get(), both.total, c.cjobs, c.s);
 }
 
-TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMPS& m1, DMPS& m2) {
+BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff) {
     const std::size_t nb = both.n();
-    std::vector<uint64_t> uo(nb), so(nb), vo(nb);
-    std::vector<uint32_t> kk(nb);
+    BlockSVD r;
+    r.uo.resize(nb); r.so.resize(nb); r.vo.resize(nb); r.kk.resize(nb);
     uint64_t ul = 0, sl = 0, vl = 0;
     for (std::size_t k = 0; k < nb; ++k) {
-        kk[k] = std::min(both.rows[k], both.cols[k]);
-        uo[k] = ul; ul += (uint64_t(both.rows[k]) * kk[k] + 31) / 32 * 32;
-        so[k] = sl; sl += kk[k];
-        vo[k] = vl; vl += (uint64_t(both.cols[k]) * kk[k] + 31) / 32 * 32;
+        r.kk[k] = std::min(both.rows[k], both.cols[k]);
+        r.uo[k] = ul; ul += (uint64_t(both.rows[k]) * r.kk[k] + 31) / 32 * 32;
+        r.so[k] = sl; sl += r.kk[k];
+        r.vo[k] = vl; vl += (uint64_t(both.cols[k]) * r.kk[k] + 31) / 32 * 32;
     }
-    DBuf<double> U(std::max<uint64_t>(ul, 1)), S(std::max<uint64_t>(sl, 1)), V(std::max<uint64_t>(vl, 1));
-    // independent block SVDs on the solver's side lanes, largest first, round robin
-    std::vector<std::size_t> order(nb);
-    for (std::size_t k = 0; k < nb; ++k) order[k] = k;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](std::size_t x, std::size_t y) { return both.elems(x) > both.elems(y); });
-    int* info = c.sv->reserve_info(uint32_t(nb), c.s);
-    c.sv->fork(c.s);
-    // cuSOLVER's Jacobi SVD returns only when its block is done, so each lane gets its own host thread
-    std::string err;
-#pragma omp parallel for num_threads(Solver::LANES) schedule(static, 1)
-    for (int lane = 0; lane < Solver::LANES; ++lane) {
-        try {
-            QCM_CUDA(cudaSetDevice(c.device));
-            for (std::size_t i = std::size_t(lane); i < nb; i += Solver::LANES) {
-                const std::size_t k = order[i];
-                svd_thin_lane(*c.sv, lane, both.d.get() + both.off[k], int(both.rows[k]), int(both.cols[k]), U.get() + uo[k],
-                              S.get() + so[k], V.get() + vo[k], info + k);
+    r.u_len = std::max<uint64_t>(ul, 1); r.s_len = std::max<uint64_t>(sl, 1); r.v_len = std::max<uint64_t>(vl, 1);
+    r.U.alloc(r.u_len); r.S.alloc(r.s_len); r.V.alloc(r.v_len);
+    // all block SVDs in one launch (one-sided Jacobi, one CTA per block)
+    std::vector<SvdJob> sj;
+    uint64_t wl = 0;
+    for (std::size_t k = 0; k < nb; ++k) {
+        if (!r.kk[k]) continue;
+        sj.push_back(SvdJob{both.off[k], r.uo[k], r.so[k], r.vo[k], wl, both.rows[k], both.cols[k], uint32_t(k), 0});
+        wl += jacobi_svd_scratch(both.rows[k], both.cols[k]);
+    }
+    DBuf<double> Wj(std::max<uint64_t>(wl, 1));
+    DBuf<int> zc(std::max<std::size_t>(nb, 1));
+    // QCM_SVD_STATS=1 prints the kernel time and the Jacobi sweeps of every batch
+    static const bool stats = std::getenv("QCM_SVD_STATS") != nullptr;
+    DBuf<int> swp;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (stats) {
+        swp.alloc(std::max<std::size_t>(nb, 1));
+        QCM_CUDA(cudaMemsetAsync(swp.get(), 0, std::max<std::size_t>(nb, 1) * sizeof(int), c.s));
+        QCM_CUDA(cudaEventCreate(&e0));
+        QCM_CUDA(cudaEventCreate(&e1));
+        QCM_CUDA(cudaEventRecord(e0, c.s));
+    }
+    batched_jacobi_svd(sj, both.d.get(), both.total, r.U.get(), r.u_len, r.S.get(), r.s_len, r.V.get(), r.v_len, Wj.get(),
+                       std::max<uint64_t>(wl, 1), zc.get(), c.sjobs, c.s, stats ? swp.get() : nullptr);
+    if (stats) {
+        QCM_CUDA(cudaEventRecord(e1, c.s));
+        QCM_CUDA(cudaEventSynchronize(e1));
+        float ms = 0;
+        QCM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        std::vector<int> hsw(nb, 0);
+        if (nb) QCM_CUDA(cudaMemcpyAsync(hsw.data(), swp.get(), nb * sizeof(int), cudaMemcpyDeviceToHost, c.s));
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        uint32_t mr = 0, mc = 0;
+        for (std::size_t k = 0; k < nb; ++k) { mr = std::max(mr, both.rows[k]); mc = std::max(mc, both.cols[k]); }
+        std::fprintf(stderr, "[svd] %zu blocks (max %u x %u): %.3f ms, sweeps max %d\n", nb, mr, mc, ms,
+                     hsw.empty() ? 0 : *std::max_element(hsw.begin(), hsw.end()));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    std::vector<double> hs(sl);
+    std::vector<int> hz(nb, 0);
+    if (sl) QCM_CUDA(cudaMemcpyAsync(hs.data(), r.S.get(), sl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    if (nb) QCM_CUDA(cudaMemcpyAsync(hz.data(), zc.get(), nb * sizeof(int), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    r.vals.assign(nb, {});
+    for (std::size_t k = 0; k < nb; ++k) r.vals[k].assign(hs.begin() + r.so[k], hs.begin() + r.so[k] + r.kk[k]);
+    {
+        // a kept singular value of exactly zero needs an orthonormal completion of its singular
+        // vectors: such blocks are recomputed by cuSOLVER's gesvdj
+        std::vector<uint32_t> keep0;
+        estimate_cut(r.vals, Mmax, cutoff, keep0);
+        std::vector<std::size_t> redo;
+        for (std::size_t k = 0; k < nb; ++k)
+            if (hz[k] && keep0[k] + uint32_t(hz[k]) > r.kk[k]) redo.push_back(k);
+        if (!redo.empty()) {
+            if (!c.sv) c.sv = std::make_unique<Solver>();
+            int* info = c.sv->reserve_info(uint32_t(redo.size()), c.s);
+            c.sv->fork(c.s);
+            for (std::size_t i = 0; i < redo.size(); ++i) {
+                const std::size_t k = redo[i];
+                svd_thin_lane(*c.sv, 0, both.d.get() + both.off[k], int(both.rows[k]), int(both.cols[k]), r.U.get() + r.uo[k],
+                              r.S.get() + r.so[k], r.V.get() + r.vo[k], info + i);
             }
-        } catch (const std::exception& e) {
-#pragma omp critical
-            err = e.what();
+            c.sv->join(c.s);
+            c.sv->check(c.s);
+            for (std::size_t k : redo)
+                QCM_CUDA(cudaMemcpyAsync(hs.data() + r.so[k], r.S.get() + r.so[k], r.kk[k] * sizeof(double), cudaMemcpyDeviceToHost,
+                                         c.s));
+            QCM_CUDA(cudaStreamSynchronize(c.s));
+            for (std::size_t k : redo) r.vals[k].assign(hs.begin() + r.so[k], hs.begin() + r.so[k] + r.kk[k]);
         }
     }
-    if (!err.empty()) throw std::runtime_error(err);
-    c.sv->join(c.s);
-    c.sv->check(c.s);
-    std::vector<double> hs(sl);
-    if (sl) QCM_CUDA(cudaMemcpyAsync(hs.data(), S.get(), sl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
-    QCM_CUDA(cudaStreamSynchronize(c.s));
+    r.tr = estimate_cut(r.vals, Mmax, cutoff, r.keep);
+    return r;
+}
 
-    std::vector<std::vector<double>> vals(nb);
-    for (std::size_t k = 0; k < nb; ++k) vals[k].assign(hs.begin() + so[k], hs.begin() + so[k] + kk[k]);
-    std::vector<uint32_t> keep;
-    TruncResults tr = estimate_cut(vals, Mmax, cutoff, keep);
-
+TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMPS& m1, DMPS& m2) {
+    const std::size_t nb = both.n();
+    BlockSVD sv = svd_truncate(c, both, Mmax, cutoff);
+    const std::vector<uint32_t>& keep = sv.keep;
+    const TruncResults tr = sv.tr;
+    const std::vector<uint64_t>& uo = sv.uo;
+    const std::vector<uint64_t>& so = sv.so;
+    const std::vector<uint64_t>& vo = sv.vo;
+    DBuf<double>& U = sv.U;
+    DBuf<double>& S = sv.S;
+    DBuf<double>& V = sv.V;
+    const uint64_t ul = sv.u_len, vl = sv.v_len;
     // U[:, :keep] and V^T[:keep, :], with S multiplied into V^T (l2r) or U (r2l)
     m1 = DMPS(); m2 = DMPS();
     m1.phys = phys1; m1.left = left; m1.right_paired = false;
@@ -445,6 +500,59 @@ TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMP
     }
     QCM_CUDA(cudaStreamSynchronize(c.s));  // U, S, V are released on return
     return tr;
+}
+
+BlockHeev heev_truncate(Ctx& c, DBlocks& dm, uint64_t Mmax, double cutoff) {
+    const std::size_t nb = dm.n();
+    for (std::size_t k = 0; k < nb; ++k)
+        if (dm.rows[k] != dm.cols[k]) throw std::runtime_error("heev_truncate: density-matrix block is not square");
+    if (!c.sv) c.sv = std::make_unique<Solver>();
+    // heev per block (lanes, one host thread each), eigenvalues ascending on the device
+    std::vector<uint64_t> wo(nb);
+    uint64_t wl = 0;
+    for (std::size_t k = 0; k < nb; ++k) { wo[k] = wl; wl += dm.rows[k]; }
+    DBuf<double> Wv(std::max<uint64_t>(wl, 1));
+    int* info = c.sv->reserve_info(uint32_t(nb), c.s);
+    std::vector<std::size_t> order(nb);
+    for (std::size_t k = 0; k < nb; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](std::size_t x, std::size_t y) { return dm.rows[x] > dm.rows[y]; });
+    c.sv->fork(c.s);
+    std::string err;
+#pragma omp parallel for num_threads(Solver::LANES) schedule(static, 1)
+    for (int lane = 0; lane < Solver::LANES; ++lane) {
+        try {
+            QCM_CUDA(cudaSetDevice(c.device));
+            for (std::size_t i = std::size_t(lane); i < nb; i += Solver::LANES) {
+                const std::size_t k = order[i];
+                syevd_lane(*c.sv, lane, dm.d.get() + dm.off[k], int(dm.rows[k]), Wv.get() + wo[k], info + k);
+            }
+        } catch (const std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
+    c.sv->join(c.s);
+    c.sv->check(c.s);
+    std::vector<double> hw(wl);
+    if (wl) QCM_CUDA(cudaMemcpyAsync(hw.data(), Wv.get(), wl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    // descending order; the cut is on sqrt of the positive eigenvalues (others kept as they are)
+    std::vector<std::vector<double>> vals(nb);
+    for (std::size_t k = 0; k < nb; ++k) {
+        vals[k].resize(dm.rows[k]);
+        for (uint32_t i = 0; i < dm.rows[k]; ++i) {
+            const double x = hw[wo[k] + dm.rows[k] - 1 - i];
+            vals[k][i] = x > 0.0 ? std::sqrt(x) : x;
+        }
+    }
+    BlockHeev r;
+    r.tr = estimate_cut(vals, Mmax, cutoff, r.keep);
+    r.tr.truncated_weight = r.tr.truncated_fraction;  // heev_truncate reports the fraction in both fields
+    r.evals.assign(nb, {});
+    for (std::size_t k = 0; k < nb; ++k)
+        for (uint32_t i = 0; i < dm.rows[k]; ++i) r.evals[k].push_back(hw[wo[k] + dm.rows[k] - 1 - i]);
+    return r;
 }
 
 // ---------------------------------------------------------------------------
@@ -488,48 +596,9 @@ TruncResults DTwoSite::predict_split(Ctx& c, bool l2r, uint64_t Mmax, double cut
             rbtm_accumulate(c, B, tmp, W, dm, alpha);
         }
     }
-    // heev per block (lanes, one host thread each), eigenvalues ascending on the device
-    std::vector<uint64_t> wo(nb);
-    uint64_t wl = 0;
-    for (std::size_t k = 0; k < nb; ++k) { wo[k] = wl; wl += dm.rows[k]; }
-    DBuf<double> Wv(std::max<uint64_t>(wl, 1));
-    int* info = c.sv->reserve_info(uint32_t(nb), c.s);
-    std::vector<std::size_t> order(nb);
-    for (std::size_t k = 0; k < nb; ++k) order[k] = k;
-    std::stable_sort(order.begin(), order.end(), [&](std::size_t x, std::size_t y) { return dm.rows[x] > dm.rows[y]; });
-    c.sv->fork(c.s);
-    std::string err;
-#pragma omp parallel for num_threads(Solver::LANES) schedule(static, 1)
-    for (int lane = 0; lane < Solver::LANES; ++lane) {
-        try {
-            QCM_CUDA(cudaSetDevice(c.device));
-            for (std::size_t i = std::size_t(lane); i < nb; i += Solver::LANES) {
-                const std::size_t k = order[i];
-                syevd_lane(*c.sv, lane, dm.d.get() + dm.off[k], int(dm.rows[k]), Wv.get() + wo[k], info + k);
-            }
-        } catch (const std::exception& e) {
-#pragma omp critical
-            err = e.what();
-        }
-    }
-    if (!err.empty()) throw std::runtime_error(err);
-    c.sv->join(c.s);
-    c.sv->check(c.s);
-    std::vector<double> hw(wl);
-    if (wl) QCM_CUDA(cudaMemcpyAsync(hw.data(), Wv.get(), wl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
-    QCM_CUDA(cudaStreamSynchronize(c.s));
-    // descending order; the cut is on sqrt of the positive eigenvalues (others kept as they are)
-    std::vector<std::vector<double>> vals(nb);
-    for (std::size_t k = 0; k < nb; ++k) {
-        vals[k].resize(dm.rows[k]);
-        for (uint32_t i = 0; i < dm.rows[k]; ++i) {
-            const double x = hw[wo[k] + dm.rows[k] - 1 - i];
-            vals[k][i] = x > 0.0 ? std::sqrt(x) : x;
-        }
-    }
-    std::vector<uint32_t> keep;
-    TruncResults tr = estimate_cut(vals, Mmax, cutoff, keep);
-    tr.truncated_weight = tr.truncated_fraction;  // heev_truncate reports the fraction in both fields
+    BlockHeev hv = heev_truncate(c, dm, Mmax, cutoff);
+    const std::vector<uint32_t>& keep = hv.keep;
+    const TruncResults tr = hv.tr;
     // U = kept eigenvectors, descending (columns n-1, n-2, ...)
     m1 = DMPS(); m2 = DMPS();
     m1.phys = phys1; m1.left = left; m1.right_paired = false;

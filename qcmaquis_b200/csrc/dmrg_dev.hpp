@@ -104,6 +104,7 @@ struct Ctx {
     DBuf<GemmJob> gjobs;
     DBuf<uint32_t> gtiles;
     DBuf<CopyJob> cjobs;
+    DBuf<SvdJob> sjobs;
     DBuf<TJobD> tjobs;
     DBuf<TileD> ttiles[N_SHAPES];
     DBuf<int> info;
@@ -129,6 +130,29 @@ struct TruncResults {
     uint64_t bond_dimension = 0;
     double truncated_weight = 0, truncated_fraction = 0, smallest_ev = 0;
 };
+
+// svd_truncate (block_matrix_algorithms.h:185-240) of device blocks: per block a thin SVD (U
+// rows x k at uo, S k descending at so, V cols x k at vo, k = min(rows, cols)), then
+// estimate_truncation over all singular values: keep[k] of block k are kept.
+struct BlockSVD {
+    std::vector<uint64_t> uo, so, vo;
+    std::vector<uint32_t> kk, keep;
+    std::vector<std::vector<double>> vals;  // singular values per block, descending
+    DBuf<double> U, S, V;
+    uint64_t u_len = 0, s_len = 0, v_len = 0;
+    TruncResults tr;
+};
+BlockSVD svd_truncate(Ctx& c, const DBlocks& M, uint64_t Mmax, double cutoff);
+// heev_truncate (block_matrix_algorithms.h:299-355) of device symmetric blocks: dm is
+// overwritten by its eigenvectors (ascending eigenvalue order, so the kept ones are the last
+// keep[k] columns read backwards); the cut is on sqrt of the positive eigenvalues and the
+// truncated fraction is reported in both fields.
+struct BlockHeev {
+    std::vector<uint32_t> keep;
+    std::vector<std::vector<double>> evals;  // eigenvalues per block, descending
+    TruncResults tr;
+};
+BlockHeev heev_truncate(Ctx& c, DBlocks& dm, uint64_t Mmax, double cutoff);
 
 // TwoSiteTensor (mp_tensors/twositetensor.hpp:29-199, ts_reshape.h)
 struct DTwoSite {

@@ -172,6 +172,209 @@ void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, 
                                  info, L.svdp));
 }
 
+// ---------------------------------------------------------------------------
+// One-sided Jacobi SVD (Hestenes).  G (r x c, ld r) is A when m >= n and A^T otherwise; its
+// columns are rotated pairwise until mutually orthogonal, and the rotations accumulate in Q
+// (c x c, ld c, starting at I).  Then G = Vg diag(sigma) with sigma_j = |G_j|, and
+// A = G Q^T (m >= n: U = G / sigma, V = Q) or A^T = G Q^T (m < n: U = Q, V = G / sigma).
+// Column pairs follow the circle (round-robin) ordering, c' - 1 rounds of c'/2 disjoint
+// pairs per sweep (c' = c rounded up to even, pairs with the padding column skipped); a
+// half-warp takes a pair: gamma = G_p . G_q with alpha = |G_p|^2, beta = |G_q|^2 tracked in
+// shared memory (recomputed at the start of every sweep, updated exactly by alpha -= t gamma,
+// beta += t gamma after a rotation), and if |gamma| > r eps sqrt(alpha beta) (the rounding
+// level of a length-r dot product) the rotation with t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)),
+// zeta = (beta - alpha) / (2 gamma), c = rsqrt(1 + t^2), s = c t makes them orthogonal.
+// Sweeps end when one performs no rotation (at most JMAX_SWEEPS).
+namespace {
+constexpr int JTHR = 1024;
+constexpr int JMAX_SWEEPS = 40;
+constexpr double JEPS = 2.220446049250313e-16;  // unit roundoff of double
+constexpr uint32_t JSMEM_DOUBLES = 27000;  // dynamic shared memory (with the 12 KiB static part, under 227 KiB)
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// sum over the 16 lanes of each half-warp (all 32 lanes call it)
+__device__ __forceinline__ double half_sum(double v) {
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ jobs, const double* __restrict__ A,
+                                                     double* __restrict__ U, double* __restrict__ S, double* __restrict__ V,
+                                                     double* __restrict__ Wg, int use_smem, int* __restrict__ zero_count,
+                                                     int* __restrict__ sweeps_used) {
+    extern __shared__ double smem[];
+    __shared__ int rotated;
+    __shared__ uint32_t rank_of[1024];
+    __shared__ double nrm[1024];
+    const SvdJob J = jobs[blockIdx.x];
+    const bool tall = J.m >= J.n;
+    const uint32_t r = tall ? J.m : J.n, c = tall ? J.n : J.m;
+    double* G = use_smem ? smem : Wg + J.w_off;
+    double* Q = G + uint64_t(r) * c;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = JTHR / 32;
+    // G = A or A^T, Q = I
+    const double* a = A + J.a_off;
+    for (uint64_t i = tid; i < uint64_t(r) * c; i += JTHR) {
+        const uint32_t row = uint32_t(i % r), col = uint32_t(i / r);
+        G[i] = tall ? a[row + uint64_t(col) * J.m] : a[col + uint64_t(row) * J.m];
+    }
+    for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
+    __syncthreads();
+    const uint32_t cp = c + (c & 1u);  // players, padded to even
+    const double tol2 = (JEPS * double(r)) * (JEPS * double(r));
+    const uint32_t grp = uint32_t(tid) >> 4, hl = uint32_t(tid) & 15u, ngrp = JTHR / 16;
+    for (int sweep = 0; sweep < JMAX_SWEEPS && c > 1; ++sweep) {
+        if (tid == 0) rotated = 0;
+        for (uint32_t j = warp; j < c; j += nwarp) {
+            const double* g = G + uint64_t(j) * r;
+            double x = 0.0;
+            for (uint32_t i = lane; i < r; i += 32) x = fma(g[i], g[i], x);
+            x = warp_sum(x);
+            if (lane == 0) nrm[j] = x;
+        }
+        __syncthreads();
+        for (uint32_t k = 0; k + 1 < cp; ++k) {
+            // one pair per half-warp; every lane runs the same number of passes so the half-warp
+            // shuffles never diverge
+            for (uint32_t pass = 0; pass * ngrp < cp / 2; ++pass) {
+                const uint32_t t = pass * ngrp + grp;
+                const uint32_t i0 = t, i1 = cp - 1 - t;
+                uint32_t p = 0, q = 0;
+                bool act = t < cp / 2;
+                if (act) {
+                    p = i0 == 0 ? 0 : (i0 - 1 + k) % (cp - 1) + 1;
+                    q = i1 == 0 ? 0 : (i1 - 1 + k) % (cp - 1) + 1;
+                    act = p < c && q < c;
+                }
+                double* gp = G + uint64_t(p) * r;
+                double* gq = G + uint64_t(q) * r;
+                double ga = 0.0;
+                if (act)
+                    for (uint32_t i = hl; i < r; i += 16) ga = fma(gp[i], gq[i], ga);
+                ga = half_sum(ga);
+                const double al = act ? nrm[p] : 0.0, be = act ? nrm[q] : 0.0;
+                const bool rot = act && ga * ga > tol2 * (al * be);
+                if (rot) {
+                    const double zeta = (be - al) / (2.0 * ga);
+                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    const double cs = rsqrt(1.0 + tt * tt), sn = cs * tt;
+                    for (uint32_t i = hl; i < r; i += 16) {
+                        const double x = gp[i], y = gq[i];
+                        gp[i] = cs * x - sn * y;
+                        gq[i] = sn * x + cs * y;
+                    }
+                    double* qp = Q + uint64_t(p) * c;
+                    double* qq = Q + uint64_t(q) * c;
+                    for (uint32_t i = hl; i < c; i += 16) {
+                        const double x = qp[i], y = qq[i];
+                        qp[i] = cs * x - sn * y;
+                        qq[i] = sn * x + cs * y;
+                    }
+                    if (hl == 0) {
+                        nrm[p] = al - tt * ga;
+                        nrm[q] = be + tt * ga;
+                        rotated = 1;
+                    }
+                }
+                __syncwarp();
+            }
+            __syncthreads();
+        }
+        const int any = rotated;
+        __syncthreads();
+        if (sweeps_used && tid == 0) sweeps_used[J.id] = sweep + 1;
+        if (!any) break;
+    }
+    // sigma_j = |G_j| into S (unsorted, temporarily), then ranks by descending sigma (ties by index)
+    double* sv = S + J.s_off;
+    for (uint32_t j = warp; j < c; j += nwarp) {
+        const double* g = G + uint64_t(j) * r;
+        double x = 0.0;
+        for (uint32_t i = lane; i < r; i += 32) x = fma(g[i], g[i], x);
+        x = warp_sum(x);
+        if (lane == 0) sv[j] = sqrt(x);
+    }
+    __syncthreads();
+    for (uint32_t j = tid; j < c; j += JTHR) {
+        const double x = sv[j];
+        uint32_t rk = 0;
+        for (uint32_t i = 0; i < c; ++i) {
+            const double y = sv[i];
+            rk += (y > x || (y == x && i < j)) ? 1u : 0u;
+        }
+        rank_of[j] = rk;
+    }
+    __syncthreads();
+    // outputs in sorted order: the normalised G columns and Q's columns
+    double* Gout = tall ? U + J.u_off : V + J.v_off;   // r x c, ld r
+    double* Qout = tall ? V + J.v_off : U + J.u_off;   // c x c, ld c
+    for (uint64_t i = tid; i < uint64_t(r) * c; i += JTHR) {
+        const uint32_t row = uint32_t(i % r), col = uint32_t(i / r);
+        const double sg = sv[col];
+        Gout[row + uint64_t(rank_of[col]) * r] = sg > 0.0 ? G[i] / sg : 0.0;
+    }
+    for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) {
+        const uint32_t row = uint32_t(i % c), col = uint32_t(i / c);
+        Qout[row + uint64_t(rank_of[col]) * c] = Q[i];
+    }
+    __syncthreads();
+    // sigma in sorted order (through the scratch column space, G is no longer needed)
+    for (uint32_t j = tid; j < c; j += JTHR) G[rank_of[j]] = sv[j];
+    __syncthreads();
+    int zeros = 0;
+    for (uint32_t j = tid; j < c; j += JTHR) {
+        sv[j] = G[j];
+        zeros += G[j] == 0.0 ? 1 : 0;
+    }
+    if (zeros) atomicAdd(zero_count + J.id, zeros);
+}
+}  // namespace
+
+uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n) {
+    const uint64_t r = std::max(m, n), c = std::min(m, n);
+    return r * c + c * c;
+}
+
+void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
+                        uint64_t s_len, double* V, uint64_t v_len, double* W, uint64_t w_len, int* zero_count,
+                        DBuf<SvdJob>& jobbuf, cudaStream_t s, int* sweeps_used) {
+    // smem launch for the blocks whose work matrices fit, global scratch for the rest
+    std::vector<SvdJob> small, large;
+    uint64_t smax = 0;
+    for (const SvdJob& j : jobs) {
+        const uint64_t k = std::min(j.m, j.n);
+        if (!j.m || !j.n) continue;
+        if (k > 1024) throw std::runtime_error("batched_jacobi_svd: block larger than 1024 in both dimensions");
+        if (j.a_off + uint64_t(j.m) * j.n > a_len || j.u_off + uint64_t(j.m) * k > u_len || j.s_off + k > s_len ||
+            j.v_off + uint64_t(j.n) * k > v_len || j.w_off + jacobi_svd_scratch(j.m, j.n) > w_len)
+            throw std::runtime_error("batched_jacobi_svd: block outside its buffers");
+        const uint64_t need = jacobi_svd_scratch(j.m, j.n);
+        if (need <= JSMEM_DOUBLES) { small.push_back(j); smax = std::max(smax, need); }
+        else large.push_back(j);
+    }
+    uint32_t nid = 0;
+    for (const SvdJob& j : jobs) nid = std::max(nid, j.id + 1);
+    if (nid) QCM_CUDA(cudaMemsetAsync(zero_count, 0, nid * sizeof(int), s));
+    std::vector<SvdJob> all(small);
+    all.insert(all.end(), large.begin(), large.end());
+    if (all.empty()) return;
+    jobbuf.upload(all, s);
+    if (!small.empty()) {
+        const std::size_t bytes = smax * sizeof(double);
+        QCM_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+        k_jacobi_svd<<<unsigned(small.size()), JTHR, bytes, s>>>(jobbuf.get(), A, U, S, V, W, 1, zero_count, sweeps_used);
+        QCM_CUDA(cudaGetLastError());
+    }
+    if (!large.empty()) {
+        k_jacobi_svd<<<unsigned(large.size()), JTHR, 0, s>>>(jobbuf.get() + small.size(), A, U, S, V, W, 0, zero_count,
+                                                              sweeps_used);
+        QCM_CUDA(cudaGetLastError());
+    }
+}
+
 void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info) {
     if (n == 0) return;
     Solver::Lane& L = sv.lane[l];

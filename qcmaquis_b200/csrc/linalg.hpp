@@ -54,6 +54,22 @@ void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double*
 // the same on side lane `l` (between fork and join), status to *info; lanes may be driven
 // from different host threads (one thread per lane: the Jacobi SVD blocks its caller)
 void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, double* S, double* V, int* info);
+// Thin SVDs of many small blocks in one launch (one-sided Jacobi, one CTA per block):
+// A_j (m x n, ld m) = U_j diag(S_j) V_j^T with U_j (m x k, ld m), S_j descending (k), V_j
+// (n x k, ld n), k = min(m, n) -- the layout of gesvdj with econ = 1.  A singular value that
+// is exactly zero leaves a zero column in U_j (m >= n) or V_j (m < n); zero_count[id] counts them
+// (zero_count has an entry for every id); sweeps_used (optional, same indexing) receives the
+// number of Jacobi sweeps each block took.
+struct SvdJob {
+    uint64_t a_off, u_off, s_off, v_off, w_off;  // w_off: scratch of jacobi_svd_scratch(m, n) doubles
+    uint32_t m, n;
+    uint32_t id, pad;  // zero_count[id] receives the block's number of zero singular values
+};
+uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n);
+// A, U, S, V, W: base pointers of the offsets in jobs (host list, validated against the lengths)
+void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
+                        uint64_t s_len, double* V, uint64_t v_len, double* W, uint64_t w_len, int* zero_count,
+                        DBuf<SvdJob>& jobbuf, cudaStream_t s, int* sweeps_used = nullptr);
 // Symmetric eigendecomposition (divide and conquer, lower triangle) on lane `l`: A (n x n, ld n)
 // is overwritten by the eigenvectors, W receives the eigenvalues in ascending order.
 // Replaces heevd('V') of alps/matrix/algorithms.hpp:374-396 (which then reverses the order).

@@ -59,6 +59,56 @@ _lib._sig("qcm_dmrg_sweep", c_int, c_void_p, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
 _lib._sig("qcm_dmrg_bond_dimensions", c_int, c_void_p, P(c_uint64))
 _lib._sig("qcm_dmrg_free", None, c_void_p)
+_U32 = P(ctypes.c_uint32)
+_lib._sig("qcm_truncate_svd", c_int, c_void_p, ctypes.c_uint32, _U32, _U32, P(c_double), c_uint64, c_double, _U32,
+          P(c_double), P(c_double), P(c_double), P(TruncResult))
+_lib._sig("qcm_truncate_heev", c_int, c_void_p, ctypes.c_uint32, _U32, P(c_double), c_uint64, c_double, _U32, P(c_double),
+          P(c_double), P(TruncResult))
+
+
+def _u32(a: np.ndarray):
+    return a.ctypes.data_as(_U32)
+
+
+def truncate_svd(ctx, blocks, max_bond_dimension: int, cutoff: float = 1e-16):
+    """svd_truncate of a block matrix (list of 2-D blocks) on the device: ([(U, S, Vt) per block,
+    kept columns only], truncation result dict)."""
+    bl = [np.asarray(b, dtype=np.float64) for b in blocks]
+    rows = np.array([b.shape[0] for b in bl], dtype=np.uint32)
+    cols = np.array([b.shape[1] for b in bl], dtype=np.uint32)
+    k = np.minimum(rows, cols).astype(np.int64)
+    data = np.ascontiguousarray(np.concatenate([b.ravel(order="F") for b in bl]))
+    U = np.zeros(max(1, int((rows * k).sum())))
+    S = np.zeros(max(1, int(k.sum())))
+    Vt = np.zeros(max(1, int((k * cols).sum())))
+    keep = np.zeros(len(bl), dtype=np.uint32)
+    r = TruncResult()
+    check(lib.qcm_truncate_svd(ctx.h, len(bl), _u32(rows), _u32(cols), _lib.dptr(data), max_bond_dimension, cutoff, _u32(keep),
+                               _lib.dptr(U), _lib.dptr(S), _lib.dptr(Vt), ctypes.byref(r)), "qcm_truncate_svd")
+    out, pu, ps, pv = [], 0, 0, 0
+    for m, n, kp in zip(rows.tolist(), cols.tolist(), keep.tolist()):
+        out.append((U[pu:pu + m * kp].reshape(kp, m).T.copy(), S[ps:ps + kp].copy(), Vt[pv:pv + kp * n].reshape(n, kp).T.copy()))
+        pu += m * kp; ps += kp; pv += kp * n
+    return out, {f: getattr(r, f) for f, _ in TruncResult._fields_}
+
+
+def truncate_heev(ctx, blocks, max_bond_dimension: int, cutoff: float = 1e-16):
+    """heev_truncate of symmetric blocks on the device: ([(U, evals) per block, kept eigenpairs in
+    descending order], truncation result dict; truncated_weight = truncated_fraction)."""
+    bl = [np.asarray(b, dtype=np.float64) for b in blocks]
+    dims = np.array([b.shape[0] for b in bl], dtype=np.uint32)
+    data = np.ascontiguousarray(np.concatenate([b.ravel(order="F") for b in bl]))
+    U = np.zeros(max(1, int((dims.astype(np.int64) ** 2).sum())))
+    ev = np.zeros(max(1, int(dims.sum())))
+    keep = np.zeros(len(bl), dtype=np.uint32)
+    r = TruncResult()
+    check(lib.qcm_truncate_heev(ctx.h, len(bl), _u32(dims), _lib.dptr(data), max_bond_dimension, cutoff, _u32(keep),
+                                _lib.dptr(U), _lib.dptr(ev), ctypes.byref(r)), "qcm_truncate_heev")
+    out, pu, pe = [], 0, 0
+    for n, kp in zip(dims.tolist(), keep.tolist()):
+        out.append((U[pu:pu + n * kp].reshape(kp, n).T.copy(), ev[pe:pe + kp].copy()))
+        pu += n * kp; pe += kp
+    return out, {f: getattr(r, f) for f, _ in TruncResult._fields_}
 
 
 def jd_solve(plan, x0: np.ndarray, tol: float = 1e-10, maxiter: int = 8):
