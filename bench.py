@@ -19,6 +19,12 @@ plan stream, L2 flushed between steps), summed over ranks / max over ranks.
 of psi and D2H of H.psi inside the timed region).  The path does not shard
 across GPUs here (one B200 per solve): N > 1 runs N independent replicas.
 
+"mixed" reports the mixed-precision form of the same step (S build as 3xTF32 on
+the tensor cores, T-GEMM and L.S in FP64) with the same timing rules, its
+deviation from the oracle, and (unless --no-mixed-sweep) the same sweeps run
+with every Jacobi-Davidson solve in the mixed form (FP64 Rayleigh quotient per
+step): sweep times and the energy deviation from the FP64 sweeps.
+
 The reference arm (--impl reference) times the CPU restatement of the same
 H.psi (the oracle: OpenMP over ket sectors, OpenBLAS dgemm) on the same frozen
 problem, exported by the device engine as a "QSPB" blob.
@@ -51,6 +57,7 @@ def parse():
     ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed-sweep", action="store_true", help="skip the mixed-precision sweeps (bench of the apply only)")
     return ap.parse_args()
 
 
@@ -181,6 +188,81 @@ def run_reference(a, world, rank, pg):
     print(json.dumps(line), flush=True)
 
 
+def measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob, site, x_host, form="mixed"):
+    """A mixed-precision form on the same frozen problem: S build 3xTF32 on the tensor cores
+    (FP32 accumulation), T-GEMM and L.S in FP64; same timing rules as the FP64 form."""
+    import torch
+    from qcmaquis_b200._lib import lib, check
+    from qcmaquis_b200.heff import precision_mode
+    mode = precision_mode(form)
+    for _ in range(a.warmup):
+        plan.apply_device(xd.data_ptr(), yd.data_ptr(), precision=form)
+    torch.cuda.synchronize()
+    times, phases = [], []
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ms = plan.profile(xd.data_ptr(), yd.data_ptr(), precision=form)
+        times.append(ms[3])
+        phases.append(ms[:3])
+    torch.cuda.synchronize()
+    total_ms = float(sum(times))
+    e2e_t = []
+    for _ in range(a.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        check(lib.qcm_heff_apply_mode(plan.h, xp, yp, mode), "qcm_heff_apply_mode")
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = float(sum(e2e_t))
+    if pg is not None:
+        t = torch.tensor([total_ms, e2e_s], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms, e2e_s = float(t[0].item()), float(t[1].item())
+    ph = np.mean(np.array(phases), axis=0)
+    y_mixed = yh.numpy().copy()
+    out = {"value": info["flops"] * a.steps * world / (total_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
+           "ms_per_step": total_ms / a.steps,
+           "form": ("S build 3xTF32 (mma.sync m16n8k8, FP32 operands split at the fragment loads, FP32 accumulation), "
+                    "T-GEMM and L.S FP64") if mode == 1 else
+                   ("S build 3xTF32 from operands split in HBM: 16/32-line tiles on tcgen05 (accumulator in tensor memory), "
+                    "others on mma.sync; T-GEMM and L.S FP64"),
+           "e2e": {"value": info["flops"] * a.steps * world / e2e_s / 1e9, "unit": "GFLOP/s",
+                   "h2d_bytes_per_step": 8 * plan.n, "d2h_bytes_per_step": 8 * plan.n},
+           "phase_ms": {"k_tgemm": float(ph[0]), "k_sgemm_x3": float(ph[1]), "k_lspart+k_lsreduce": float(ph[2])},
+           "s_build_tflops": info["flops_s"] / (ph[1] * 1e-3) / 1e12,
+           "s_build_executed_tf32_tflops": 3 * info["flops_sexec"] / (ph[1] * 1e-3) / 1e12}
+    if snap is not None:
+        from oracle.oracle import heff_apply
+        y_ref, _, _ = heff_apply(snap, blob, site, x_host)
+        out["max_rel_err_vs_oracle"] = float(np.abs(y_mixed - y_ref).max() / np.abs(y_ref).max())
+    return out
+
+
+def mixed_sweeps(a, ctx, blob, sinfo):
+    """The same sweeps with every JD in the mixed form (FP64 Rayleigh quotient per step): times and
+    the per-sweep energy deviation from the FP64 device sweeps."""
+    from qcmaquis_b200.mpo import MPO
+    from qcmaquis_b200.dmrg import DMRG
+    m = MPO.from_blob(blob)
+    d = DMRG(ctx, m, a.L // 2, a.L // 2, a.M, a.init_bd, precision="mixed")
+    out = []
+    for s in range(a.sweeps):
+        st0 = d.stats()
+        t0 = time.perf_counter()
+        E, tr = d.sweep()
+        dt = time.perf_counter() - t0
+        st1 = d.stats()
+        e64 = sinfo["sweeps"][s]["energy_min"]
+        out.append({"sweep": s, "seconds": dt, "energy_min": float(E.min()), "energy_dev_vs_fp64": float(E.min() - e64),
+                    "max_bond_dimension": int(max(t["bond_dimension"] for t in tr)),
+                    "hpsi_mixed": int(st1["hpsi_count"] - st0["hpsi_count"]),
+                    "hpsi_fp64": int(st1["hpsi_count_fp64"] - st0["hpsi_count_fp64"]),
+                    "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}})
+    del d
+    return out
+
+
 def run_b200(a, world, rank, local, pg):
     import torch
     from qcmaquis_b200 import heff
@@ -269,6 +351,11 @@ def run_b200(a, world, rank, local, pg):
         roof["executed_tflops"] = info["flops_sexec"] / (ph[1] * 1e-3) / 1e12
         roof["executed_frac"] = roof["executed_tflops"] / dmma_peak
     roof["phase_ms"] = {k: float(v) for k, v in zip(names, ph)}
+    mixed = measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob, site, x_host)
+    mixed["tensor_memory_form"] = measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob,
+                                                site, x_host, form="mixed_tc")
+    if not a.no_mixed_sweep:
+        mixed["sweep"] = mixed_sweeps(a, ctx, blob, sinfo)
     cpu = None
     if want_cpu:
         cpu = cpu_baseline(snap, blob, site, x_host, info["flops"])
@@ -284,7 +371,7 @@ def run_b200(a, world, rank, local, pg):
                 "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
                 "gpu_launches": int(info["launches"]) * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
                 "fp64_peaks_tflops": {"dmma": dmma_peak, "dfma": dfma_peak},
-                "max_rel_err_vs_oracle": rel}
+                "max_rel_err_vs_oracle": rel, "mixed": mixed}
         print(json.dumps(line), flush=True)
     del plan, d
     if pg is not None:

@@ -150,6 +150,25 @@ int qcm_heff_apply(qcm_heff* h, const double* x, double* y);
 /* Same with device pointers, enqueued on the context stream (asynchronous). */
 int qcm_heff_apply_device(qcm_heff* h, const double* x_dev, double* y_dev);
 
+/* Precision forms of H_eff . psi (the reference has only the FP64 one):
+ * QCM_PRECISION_FP64  -- the plain form, every contraction in FP64 (DMMA).
+ * QCM_PRECISION_MIXED -- the S build (the coefficient-weighted sum over T slices, ~3/4 of the
+ *   work) runs on the tensor cores as 3xTF32 (hi/lo split of FP32 operands, three TF32
+ *   products per term, FP32 accumulation): relative error ~1e-7 instead of ~1e-16; T-GEMM,
+ *   L.S GEMM, input and output stay FP64.  mma.sync m16n8k8 TF32 fragments, FP32 operands split
+ *   at the fragment loads; the first mixed apply of a plan copies its coefficient blocks to FP32
+ *   (HBM: half the FP64 blocks again); T in FP32 reuses the FP64 T buffer.
+ * QCM_PRECISION_MIXED_TC -- the same arithmetic with the 16- and 32-line S tiles on tcgen05
+ *   (TF32 MMAs issued by one thread from shared-memory descriptors, accumulator in tensor memory)
+ *   from operands split in HBM (coefficient blocks: as much again as the FP64 ones).  A tile
+ *   that gives up on a bounded wait is reported as an error by the next synchronising call
+ *   (qcm_heff_apply_mode, qcm_heff_profile_mode, qcm_jd_solve_mode). */
+#define QCM_PRECISION_FP64 0
+#define QCM_PRECISION_MIXED 1
+#define QCM_PRECISION_MIXED_TC 2
+int qcm_heff_apply_mode(qcm_heff* h, const double* x, double* y, int precision);
+int qcm_heff_apply_device_mode(qcm_heff* h, const double* x_dev, double* y_dev, int precision);
+
 /* Bookkeeping rows (parity checks; plan built with QCM_PLAN_BOOKKEEPING):
  * ints[10*i..] = (lb_in, lb_out, ci, ci_eff, unit_offset, ms, b1_row,
  * mps_offset, ci_right, column), alpha[i].  Call with ints == NULL for *n. */
@@ -157,6 +176,7 @@ int qcm_heff_bookkeeping(const qcm_heff* h, uint32_t* ints, double* alpha, uint6
 /* One device apply with CUDA events between the phases, synchronous:
  * ms[0] T-GEMM, ms[1] S gather, ms[2] L.S GEMM, ms[3] whole H.psi. */
 int qcm_heff_profile(qcm_heff* h, const double* x_dev, double* y_dev, float* ms);
+int qcm_heff_profile_mode(qcm_heff* h, const double* x_dev, double* y_dev, float* ms, int precision);
 void qcm_heff_free(qcm_heff* h);
 
 /* No counterpart in the reference.  For callers that cannot allocate device memory
@@ -187,6 +207,12 @@ int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, double* y_de
  * (solver/solver.cpp:14-28 -> solve_ietl_jcd, ietl_jacobi_davidson.h:35-76,
  * ietl/jacobi.h:386-474).  Returns the eigenvalue in *eval (no core energy). */
 int qcm_jd_solve(qcm_heff* h, const double* x0, double tol, int maxiter, double* out, double* eval, int* iters);
+/* Same with a precision form of the H.psi (QCM_PRECISION_*).  Mixed: every iteration uses the
+ * mixed H.psi and stops once |r| <= max(tol, 1e-7) |theta| (or at maxiter); the returned
+ * eigenvalue is the FP64 Rayleigh quotient of the final vector (one more FP64 H.psi), whose
+ * error is of second order in the vector's. */
+int qcm_jd_solve_mode(qcm_heff* h, const double* x0, double tol, int maxiter, int precision, double* out, double* eval,
+                      int* iters);
 
 /* New environment from one MPS site tensor, given right-paired (its blocks
  * ls x stripe, column-major, concatenated in left-sector order, as for
@@ -227,6 +253,8 @@ typedef struct {
     int32_t twosite_truncation;   /* 0: svd, 1: heev on the reduced density matrix with noise alpha */
     double alpha_initial, alpha_main, alpha_final; /* noise of sweeps < ngrowsweeps, < + nmainsweeps, later */
     int32_t ngrowsweeps, nmainsweeps;
+    int32_t hpsi_precision;       /* QCM_PRECISION_FP64, or QCM_PRECISION_MIXED: JD with the mixed H.psi
+                                     and an FP64 Rayleigh quotient of each step's final vector */
 } qcm_dmrg_params;
 /* block_matrix_algorithms.h:48-63 */
 typedef struct {
@@ -237,6 +265,8 @@ typedef struct {
     uint64_t hpsi_count;
     double hpsi_flops; /* reference flop count (ScheduleNew::total_flops) summed over the applies */
     double plan_s, jd_s, trunc_s, boundary_s, total_s; /* wall time per phase, summed over sweeps */
+    uint64_t hpsi_count_fp64;  /* mixed form: the FP64 Rayleigh-quotient applies (not in hpsi_count) */
+    double hpsi_flops_fp64;
 } qcm_dmrg_stats;
 
 /* mpo: single-site QC MPO; nup/ndown: u1_total_charge1/2.  Builds the const

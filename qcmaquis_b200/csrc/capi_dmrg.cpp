@@ -120,7 +120,14 @@ void fill_sectors(const qcm::Index& x, qcm_sector* out) {
 extern "C" {
 
 int qcm_jd_solve(qcm_heff* h, const double* x0, double tol, int maxiter, double* out, double* eval, int* iters) {
+    return qcm_jd_solve_mode(h, x0, tol, maxiter, QCM_PRECISION_FP64, out, eval, iters);
+}
+
+int qcm_jd_solve_mode(qcm_heff* h, const double* x0, double tol, int maxiter, int precision, double* out, double* eval,
+                      int* iters) {
     QCM_TRY
+    if (precision < QCM_PRECISION_FP64 || precision > QCM_PRECISION_MIXED_TC)
+        return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_mode: unknown precision mode");
     if (!h || !x0 || !out || !eval) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: NULL argument");
     if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: host-only plan");
     if (maxiter < 1 || maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve: maxiter must be in 1..64");
@@ -131,7 +138,7 @@ int qcm_jd_solve(qcm_heff* h, const double* x0, double tol, int maxiter, double*
     qcm::DBuf<double> x(p.x_len ? p.x_len : 1);
     QCM_CUDA(cudaMemcpyAsync(x.get(), x0, p.x_len * sizeof(double), cudaMemcpyHostToDevice, c.s));
     int it = 0;
-    *eval = qcm::jacobi_davidson(c, p, x.get(), tol, maxiter, it);
+    *eval = qcm::jacobi_davidson(c, p, x.get(), tol, maxiter, it, precision);
     QCM_CUDA(cudaMemcpyAsync(out, x.get(), p.x_len * sizeof(double), cudaMemcpyDeviceToHost, c.s));
     QCM_CUDA(cudaStreamSynchronize(c.s));
     if (iters) *iters = it;
@@ -214,6 +221,9 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     p.alpha_final = prm->alpha_final;
     p.ngrowsweeps = prm->ngrowsweeps;
     p.nmainsweeps = prm->nmainsweeps;
+    if (prm->hpsi_precision < QCM_PRECISION_FP64 || prm->hpsi_precision > QCM_PRECISION_MIXED_TC)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg: unknown hpsi_precision");
+    p.precision = prm->hpsi_precision;
     qcm::MPO ts = qcm::make_twosite_mpo(m);
     auto d = std::make_unique<qcm_dmrg>();
     d->ctx = ctx;
@@ -245,6 +255,9 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     p.alpha_final = prm->alpha_final;
     p.ngrowsweeps = prm->ngrowsweeps;
     p.nmainsweeps = prm->nmainsweeps;
+    if (prm->hpsi_precision < QCM_PRECISION_FP64 || prm->hpsi_precision > QCM_PRECISION_MIXED_TC)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg: unknown hpsi_precision");
+    p.precision = prm->hpsi_precision;
     qcm::Ctx tmp;
     tmp.s = ctx->stream;
     std::vector<qcm::DMPS> ms;
@@ -375,6 +388,8 @@ int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* s) {
     const qcm::DMRGStats& t = d->e->st;
     s->hpsi_count = t.hpsi_count;
     s->hpsi_flops = t.hpsi_flops;
+    s->hpsi_count_fp64 = t.hpsi_count64;
+    s->hpsi_flops_fp64 = t.hpsi_flops64;
     s->plan_s = t.plan_s;
     s->jd_s = t.jd_s;
     s->trunc_s = t.trunc_s;

@@ -1,5 +1,6 @@
 // C-ABI: context, resident boundaries and the H_eff plan / apply (the H.psi callback).
 #include <cstring>
+#include <string>
 #include <memory>
 #include <vector>
 
@@ -222,6 +223,61 @@ int qcm_heff_profile(qcm_heff* h, const double* x_dev, double* y_dev, float* ms)
     for (auto& e : ev) QCM_CUDA(cudaEventCreate(&e));
     qcm::heff_apply_device(*h->p, x_dev, y_dev, ev);
     QCM_CUDA(cudaEventSynchronize(ev[3]));
+    for (int i = 0; i < 3; ++i) QCM_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+    QCM_CUDA(cudaEventElapsedTime(&ms[3], ev[0], ev[3]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    return QCM_OK;
+    QCM_CATCH
+}
+
+namespace {
+int check_mode(int precision, const char* who) {
+    if (precision != QCM_PRECISION_FP64 && precision != QCM_PRECISION_MIXED && precision != QCM_PRECISION_MIXED_TC)
+        return qcm::fail(QCM_ERR_ARG, std::string(who) + ": unknown precision mode");
+    return QCM_OK;
+}
+void apply_mode(qcm::HeffPlan& p, const double* x, double* y, int precision, cudaEvent_t* ev = nullptr) {
+    if (precision == QCM_PRECISION_FP64) qcm::heff_apply_device(p, x, y, ev);
+    else qcm::heff_apply_device_mixed(p, x, y, ev, precision == QCM_PRECISION_MIXED_TC);
+}
+}  // namespace
+
+int qcm_heff_apply_device_mode(qcm_heff* h, const double* x_dev, double* y_dev, int precision) {
+    QCM_TRY
+    if (!h || !x_dev || !y_dev) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device_mode: NULL argument");
+    if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device_mode: host-only plan");
+    if (int rc = check_mode(precision, "qcm_heff_apply_device_mode")) return rc;
+    apply_mode(*h->p, x_dev, y_dev, precision);
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_heff_apply_mode(qcm_heff* h, const double* x, double* y, int precision) {
+    QCM_TRY
+    if (!h || !x || !y) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_mode: NULL argument");
+    if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_mode: host-only plan");
+    if (int rc = check_mode(precision, "qcm_heff_apply_mode")) return rc;
+    qcm::HeffPlan& p = *h->p;
+    qcm::AllocStream scope(p.stream);
+    if (p.d_x.size() < p.x_len) { p.d_x.alloc(p.x_len); p.d_y.alloc(p.x_len); }
+    QCM_CUDA(cudaMemcpyAsync(p.d_x.get(), x, p.x_len * sizeof(double), cudaMemcpyHostToDevice, p.stream));
+    apply_mode(p, p.d_x.get(), p.d_y.get(), precision);
+    QCM_CUDA(cudaMemcpyAsync(y, p.d_y.get(), p.x_len * sizeof(double), cudaMemcpyDeviceToHost, p.stream));
+    QCM_CUDA(cudaStreamSynchronize(p.stream));
+    if (precision != QCM_PRECISION_FP64) qcm::check_mixed(p);
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_heff_profile_mode(qcm_heff* h, const double* x_dev, double* y_dev, float* ms, int precision) {
+    QCM_TRY
+    if (!h || !h->ctx || !x_dev || !y_dev || !ms) return qcm::fail(QCM_ERR_ARG, "qcm_heff_profile_mode: bad argument");
+    if (int rc = check_mode(precision, "qcm_heff_profile_mode")) return rc;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) QCM_CUDA(cudaEventCreate(&e));
+    apply_mode(*h->p, x_dev, y_dev, precision, ev);
+    QCM_CUDA(cudaEventSynchronize(ev[3]));
+    if (precision != QCM_PRECISION_FP64) qcm::check_mixed(*h->p);
     for (int i = 0; i < 3; ++i) QCM_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
     QCM_CUDA(cudaEventElapsedTime(&ms[3], ev[0], ev[3]));
     for (auto& e : ev) cudaEventDestroy(e);

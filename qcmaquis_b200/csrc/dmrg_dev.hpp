@@ -173,7 +173,12 @@ struct DTwoSite {
 
 // Jacobi-Davidson for the lowest eigenpair (ietl/jacobi.h:386-474 with gmres 0):
 // x (device, plan vector layout) holds the start vector and receives the eigenvector.
-double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters);
+// mixed: every H.psi in the mixed form (heff_apply_device_mixed), stopping once the residual
+// is below max(tol, MIXED_RESIDUAL_FLOOR) |theta|, then one FP64 H.psi for the Rayleigh quotient
+// of the final vector (the returned eigenvalue).
+constexpr double MIXED_RESIDUAL_FLOOR = 1e-7;
+// precision: 0 FP64, 1 mixed, 2 mixed with the tensor-memory S build (QCM_PRECISION_*)
+double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters, int precision = 0);
 
 // Boundary steps (contractions/boundary_ops/move_boundary.hpp:147-404): new left boundary
 // from L[site] and mps[site]; new right boundary from R[site+1] and mps[site].
@@ -211,10 +216,13 @@ struct DMRGParams {
     bool heev = false;
     double alpha_initial = 1e-2, alpha_main = 1e-4, alpha_final = 1e-8;
     int ngrowsweeps = 0, nmainsweeps = 0;
+    int precision = 0;  // H.psi form of the JD (QCM_PRECISION_*); mixed: FP64 Rayleigh quotient per step
 };
 
 struct DMRGStats {
     uint64_t hpsi_count = 0;
+    uint64_t hpsi_count64 = 0;   // mixed form: the extra FP64 applies (Rayleigh quotients)
+    double hpsi_flops64 = 0;
     double hpsi_flops = 0, hpsi_ms = 0;  // reference flop count and device time of the H.psi applies
     double plan_s = 0, jd_s = 0, trunc_s = 0, boundary_s = 0, total_s = 0;
 };

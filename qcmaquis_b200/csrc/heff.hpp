@@ -236,6 +236,11 @@ struct HeffPlan {
     DBuf<SegD> d_segs;
     DBuf<OutD> d_outs;
     DBuf<double> d_T, d_S;
+    // mixed forms: the coefficient blocks in FP32 (w_len floats) and split into TF32 hi and lo
+    // (2 w_len floats), each made on the first apply that needs it; T in FP32 (or its hi and lo)
+    // is written into the bytes of d_T; error word of the tensor-memory path's waits
+    DBuf<float> d_W32, d_W32s;
+    DBuf<uint32_t> d_merr;
     DBuf<double> d_x, d_y;  // staging for host-buffer applies
 
     const DevBoundary* L = nullptr;
@@ -256,6 +261,18 @@ void upload_plan(HeffPlan& p);
 // gather and after the L.S GEMM.
 void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev = nullptr);
 int heff_launches_per_apply(const HeffPlan& p);
+// Mixed-precision H.psi (same layout and stream as heff_apply_device): the S build in 3xTF32 on
+// the tensor cores from FP32 operands, T-GEMM and L.S in FP64.  The first call makes the FP32
+// copy of the coefficient blocks (prepare_mixed).
+// tc: the tensor-memory (tcgen05) S build for the 16- and 32-line tiles from pre-split operands
+void heff_apply_device_mixed(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev = nullptr, bool tc = false);
+void prepare_mixed(HeffPlan& p, bool tc);
+// waits for the plan's stream and throws if a mixed S-build tile gave up on a bounded wait
+void check_mixed(HeffPlan& p);
+void run_sgemm_mixed(const HeffPlan& p, bool tc, const float* Wh, const float* Wl, const float* Th, const float* Tl, double* S,
+                     uint32_t* err, cudaStream_t s);
+void split_tf32(const double* x, float* hi, float* lo, uint64_t n, cudaStream_t s);
+void to_f32(const double* x, float* y, uint64_t n, cudaStream_t s);
 // Grouped T-GEMM and unit S-GEMM launches over prepared work lists (three tile shapes each).
 void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const double* x,
                const double* R, double* T, cudaStream_t s);

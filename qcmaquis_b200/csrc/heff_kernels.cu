@@ -36,7 +36,7 @@ using namespace dm;
 template <class S>
 __global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, const TileD* __restrict__ tiles,
                                                 const double* __restrict__ x, const double* __restrict__ R,
-                                                double* __restrict__ T) {
+                                                double* __restrict__ T, float* __restrict__ Thi, float* __restrict__ Tlo) {
     __shared__ Stage<S> st[2];
     __shared__ uint64_t colbase[S::BN];
     const TileD tile = tiles[blockIdx.x];
@@ -96,7 +96,21 @@ __global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, 
     }
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
         uint32_t gm = tile.m0 + m, gn = tile.n0 + n;
-        if (gm < J.M && gn < J.N) T[J.c_off + gm + uint64_t(gn) * J.M] = v;
+        if (gm < J.M && gn < J.N) {
+            const uint64_t o = J.c_off + gm + uint64_t(gn) * J.M;
+            if (Thi && !Tlo) {
+                Thi[o] = float(v);  // mixed form: T in FP32, split by the S build
+            } else if (Thi) {
+                // mixed form (tensor-memory path): T as TF32 hi + lo (round to nearest)
+                uint32_t h, l;
+                asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(float(v)));
+                asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(l) : "f"(float(v - double(__uint_as_float(h)))));
+                Thi[o] = __uint_as_float(h);
+                Tlo[o] = __uint_as_float(l);
+            } else {
+                T[o] = v;
+            }
+        }
     });
 }
 
@@ -393,10 +407,11 @@ __global__ void __launch_bounds__(256) k_lsreduce(const OTileD* __restrict__ oti
 }
 
 template <class S>
-void launch_t(HeffPlan& p, int sh, const double* x, double* Tb, cudaStream_t s) {
+void launch_t(HeffPlan& p, int sh, const double* x, double* Tb, cudaStream_t s, float* Thi = nullptr,
+              float* Tlo = nullptr) {
     if (!p.ttiles[sh].empty())
         k_tgemm<S><<<unsigned(p.ttiles[sh].size()), NTHR, 0, s>>>(p.d_tjobs.get(), p.d_ttiles[sh].get(), x,
-                                                                  p.R->data.get(), Tb);
+                                                                  p.R->data.get(), Tb, Thi, Tlo);
 }
 
 template <class S>
@@ -439,10 +454,64 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
     if (ev) QCM_CUDA(cudaEventRecord(ev[3], s));
     QCM_CUDA(cudaGetLastError());
 }
+// Mixed form: the T-GEMM (FP64 DMMA) writes T in FP32, the S build runs 3xTF32 on the tensor
+// cores from the FP32 coefficient blocks, the L.S GEMM stays FP64.
+void apply_mixed_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, bool tc) {
+    cudaStream_t s = p.stream;
+    prepare_mixed(p, tc);
+    if (ev) QCM_CUDA(cudaEventRecord(ev[0], s));
+    QCM_CUDA(cudaMemsetAsync(y, 0, p.x_len * sizeof(double), s));
+    // T in FP32, or its hi and lo, lives in the bytes of the FP64 T buffer (t_len doubles = 2 t_len floats)
+    double* Tb = p.d_T.get();
+    float* Thi = reinterpret_cast<float*>(Tb);
+    float* Tlo = tc ? Thi + p.t_len : nullptr;
+    launch_t<Sh16>(p, SHAPE_16, x, Tb, s, Thi, Tlo);
+    launch_t<Sh32>(p, SHAPE_32, x, Tb, s, Thi, Tlo);
+    launch_t<Sh64>(p, SHAPE_64, x, Tb, s, Thi, Tlo);
+    if (ev) QCM_CUDA(cudaEventRecord(ev[1], s));
+    double* Sb = p.d_S.get();
+    if (p.s_len) QCM_CUDA(cudaMemsetAsync(Sb, 0, p.s_len * sizeof(double), s));
+    if (tc) run_sgemm_mixed(p, true, p.d_W32s.get(), p.d_W32s.get() + p.w_len, Thi, Tlo, Sb, p.d_merr.get(), s);
+    else run_sgemm_mixed(p, false, p.d_W32.get(), nullptr, Thi, nullptr, Sb, p.d_merr.get(), s);
+    if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
+    launch_ls<Sh16>(p, SHAPE_16, Sb, p.d_P.get(), y, s);
+    launch_ls<Sh32>(p, SHAPE_32, Sb, p.d_P.get(), y, s);
+    launch_ls<Sh64>(p, SHAPE_64, Sb, p.d_P.get(), y, s);
+    if (ev) QCM_CUDA(cudaEventRecord(ev[3], s));
+    QCM_CUDA(cudaGetLastError());
+}
 }  // namespace
 
 void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev) {
     apply_impl(p, x, y, ev, p.d_T.get(), p.d_S.get(), p.d_P.get());
+}
+
+void prepare_mixed(HeffPlan& p, bool tc) {
+    AllocStream scope(p.stream);
+    if (!p.d_merr.size()) {
+        p.d_merr.alloc(1);
+        QCM_CUDA(cudaMemsetAsync(p.d_merr.get(), 0, sizeof(uint32_t), p.stream));
+    }
+    if (tc && !p.d_W32s.size()) {
+        p.d_W32s.alloc(2 * std::max<uint64_t>(p.w_len, 1));
+        split_tf32(p.d_W.get(), p.d_W32s.get(), p.d_W32s.get() + p.w_len, p.w_len, p.stream);
+    }
+    if (!tc && !p.d_W32.size()) {
+        p.d_W32.alloc(std::max<uint64_t>(p.w_len, 1));
+        to_f32(p.d_W.get(), p.d_W32.get(), p.w_len, p.stream);
+    }
+}
+
+void check_mixed(HeffPlan& p) {
+    if (!p.d_merr.size()) return;
+    uint32_t h = 0;
+    QCM_CUDA(cudaMemcpyAsync(&h, p.d_merr.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, p.stream));
+    QCM_CUDA(cudaStreamSynchronize(p.stream));
+    if (h) throw std::runtime_error("mixed H_eff: an S-build tile gave up waiting for its tensor-core MMAs");
+}
+
+void heff_apply_device_mixed(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, bool tc) {
+    apply_mixed_impl(p, x, y, ev, tc);
 }
 
 void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* Tb, double* Sb, double* Pb) {
@@ -452,11 +521,11 @@ void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* 
 void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const double* x,
                const double* R, double* T, cudaStream_t s) {
     if (!htiles[SHAPE_16].empty())
-        k_tgemm<Sh16><<<unsigned(htiles[SHAPE_16].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_16].get(), x, R, T);
+        k_tgemm<Sh16><<<unsigned(htiles[SHAPE_16].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_16].get(), x, R, T, nullptr, nullptr);
     if (!htiles[SHAPE_32].empty())
-        k_tgemm<Sh32><<<unsigned(htiles[SHAPE_32].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_32].get(), x, R, T);
+        k_tgemm<Sh32><<<unsigned(htiles[SHAPE_32].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_32].get(), x, R, T, nullptr, nullptr);
     if (!htiles[SHAPE_64].empty())
-        k_tgemm<Sh64><<<unsigned(htiles[SHAPE_64].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_64].get(), x, R, T);
+        k_tgemm<Sh64><<<unsigned(htiles[SHAPE_64].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_64].get(), x, R, T, nullptr, nullptr);
     QCM_CUDA(cudaGetLastError());
 }
 

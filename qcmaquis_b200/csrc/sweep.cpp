@@ -33,7 +33,8 @@ void download(Ctx& c, const double* d, double* h, std::size_t n) {
 }
 }  // namespace
 
-double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters) {
+double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters, int precision) {
+    const bool mixed = precision != 0;
     if (maxiter < 1 || maxiter > 64) throw std::runtime_error("jacobi_davidson: maxiter must be in 1..64");
     const uint64_t n = p.x_len, ld = (n + 31) / 32 * 32;
     // V[0..maxiter), VA[0..maxiter), u, r
@@ -73,7 +74,8 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
             tn = std::sqrt(h2[0]);
         }
         dev_axpby(1.0 / tn, t, 0.0, t, n, c.s);
-        heff_apply_device(p, t, VAi(it));
+        if (mixed) heff_apply_device_mixed(p, t, VAi(it), nullptr, precision == 2);
+        else heff_apply_device(p, t, VAi(it));
         // column it of the projected matrix: <V_i, A V_it>
         dev_dots(V, ld, uint32_t(it + 1), VAi(it), n, sc + 80, dsc, c.s);
         std::vector<double> col(it + 1);
@@ -92,7 +94,20 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         download(c, sc + 160, h3, 3);
         ++it;
         const double rn = std::sqrt(h3[0]);
-        if (rn <= tol * std::fabs(theta) || rn < tol || it >= maxiter) {
+        // the mixed H.psi carries ~1e-7 relative error: its residual cannot fall below that level
+        const double rtol = mixed ? std::max(tol, MIXED_RESIDUAL_FLOOR) : tol;
+        if (rn <= rtol * std::fabs(theta) || rn < tol || it >= maxiter) {
+            if (mixed) {
+                // FP64 Rayleigh quotient of the final vector: its error is O(|r|^2 / gap), so the
+                // energy keeps FP64 accuracy although the vector carries the mixed form's error
+                heff_apply_device(p, u, r);
+                dev_dots(u, 0, 1, r, n, sc + 163, dsc, c.s);
+                dev_dots(u, 0, 1, u, n, sc + 164, dsc, c.s);
+                double q[2];
+                download(c, sc + 163, q, 2);
+                theta = q[0] / q[1];
+                check_mixed(p);
+            }
             QCM_CUDA(cudaMemcpyAsync(x, u, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
             iters = it;
             return theta;
@@ -275,12 +290,16 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     const double t1 = now_s();
     st.plan_s += t1 - t0;
     int iters = 0;
-    const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters);
+    const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters, p.precision);
     QCM_CUDA(cudaStreamSynchronize(c.s));
     const double t2 = now_s();
     st.jd_s += t2 - t1;
     st.hpsi_count += uint64_t(iters);
     st.hpsi_flops += double(iters) * plan->flops;
+    if (p.precision != 0) {
+        st.hpsi_count64 += 1;  // the FP64 Rayleigh-quotient apply
+        st.hpsi_flops64 += plan->flops;
+    }
     plan.reset();
     tst.twin_to_both(c);
     mark(3);

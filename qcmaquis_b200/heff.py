@@ -72,6 +72,20 @@ _lib._sig("qcm_heff_apply_device", c_int, c_void_p, c_void_p, c_void_p)
 _lib._sig("qcm_heff_bookkeeping", c_int, c_void_p, P(c_uint32), P(c_double), c_uint64, P(c_uint64))
 _lib._sig("qcm_heff_profile", c_int, c_void_p, c_void_p, c_void_p, P(ctypes.c_float))
 _lib._sig("qcm_heff_apply_device_noalloc", c_int, c_void_p, c_void_p, c_void_p)
+_lib._sig("qcm_heff_apply_mode", c_int, c_void_p, P(c_double), P(c_double), c_int)
+_lib._sig("qcm_heff_apply_device_mode", c_int, c_void_p, c_void_p, c_void_p, c_int)
+_lib._sig("qcm_heff_profile_mode", c_int, c_void_p, c_void_p, c_void_p, P(ctypes.c_float), c_int)
+
+# precision forms of H_eff . psi (QCM_PRECISION_*)
+FP64, MIXED, MIXED_TC = 0, 1, 2
+
+
+def precision_mode(precision) -> int:
+    """"fp64" / "mixed" / "mixed_tc" (or 0 / 1 / 2) -> QCM_PRECISION_*."""
+    m = {"fp64": FP64, "mixed": MIXED, "mixed_tc": MIXED_TC, FP64: FP64, MIXED: MIXED, MIXED_TC: MIXED_TC}
+    if precision not in m:
+        raise ValueError(f"unknown precision {precision!r}")
+    return m[precision]
 NOALLOC_SCRATCH_DOUBLES = 8 * 1024 * 1024
 _lib._sig("qcm_heff_free", None, c_void_p)
 _lib._sig("qcm_probe_fp64_peaks", c_int, P(c_double), P(c_double))
@@ -318,15 +332,24 @@ class HeffPlan:
         self.n = int(info.vec_len)
         return self
 
-    def apply(self, x: np.ndarray) -> np.ndarray:
+    def apply(self, x: np.ndarray, precision="fp64") -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)
         assert x.size == self.n
         y = np.empty_like(x)
-        check(lib.qcm_heff_apply(self.h, _lib.dptr(x), _lib.dptr(y)), "qcm_heff_apply")
+        mode = precision_mode(precision)
+        if mode == FP64:
+            check(lib.qcm_heff_apply(self.h, _lib.dptr(x), _lib.dptr(y)), "qcm_heff_apply")
+        else:
+            check(lib.qcm_heff_apply_mode(self.h, _lib.dptr(x), _lib.dptr(y), mode), "qcm_heff_apply_mode")
         return y
 
-    def apply_device(self, x_ptr: int, y_ptr: int):
-        check(lib.qcm_heff_apply_device(self.h, c_void_p(x_ptr), c_void_p(y_ptr)), "qcm_heff_apply_device")
+    def apply_device(self, x_ptr: int, y_ptr: int, precision="fp64"):
+        mode = precision_mode(precision)
+        if mode == FP64:
+            check(lib.qcm_heff_apply_device(self.h, c_void_p(x_ptr), c_void_p(y_ptr)), "qcm_heff_apply_device")
+        else:
+            check(lib.qcm_heff_apply_device_mode(self.h, c_void_p(x_ptr), c_void_p(y_ptr), mode),
+                  "qcm_heff_apply_device_mode")
 
     def apply_device_noalloc(self, x_ptr: int, y_ptr: int):
         """apply_device without any device allocation: scratch in the library's fixed 64 MiB array
@@ -334,10 +357,11 @@ class HeffPlan:
         check(lib.qcm_heff_apply_device_noalloc(self.h, c_void_p(x_ptr), c_void_p(y_ptr)),
               "qcm_heff_apply_device_noalloc")
 
-    def profile(self, x_ptr: int, y_ptr: int):
+    def profile(self, x_ptr: int, y_ptr: int, precision="fp64"):
         """Per-phase device times (ms): T-GEMM, S gather, L.S GEMM, total."""
         ms = (ctypes.c_float * 4)()
-        check(lib.qcm_heff_profile(self.h, c_void_p(x_ptr), c_void_p(y_ptr), ms), "qcm_heff_profile")
+        check(lib.qcm_heff_profile_mode(self.h, c_void_p(x_ptr), c_void_p(y_ptr), ms, precision_mode(precision)),
+              "qcm_heff_profile_mode")
         return list(ms)
 
     def bookkeeping(self):
