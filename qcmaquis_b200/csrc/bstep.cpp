@@ -279,11 +279,12 @@ void SBuild::add_unit(uint64_t s_off, uint64_t line_stride, uint32_t erows, uint
     u.nl = uint32_t(rows.size()); u.line0 = uint32_t(line_b1.size());
     u.nk = uint32_t(slices.size()); u.slice0 = uint32_t(slice_off.size());
     u.w_off = w_len;
-    w_len += uint64_t(u.nl) * u.nk;
+    u.wld = coef_ld(u.nl);
+    w_len += uint64_t(u.wld) * u.nk;
     line_b1.insert(line_b1.end(), rows.begin(), rows.end());
     for (uint32_t id : slices) slice_off.push_back(js.offset(id));
     const std::vector<double> ones(u.nl, 1.0);
-    cg.add_unit(u.w_off, st_out, majors.data(), ones.data(), u.nl, slices, in_row);
+    cg.add_unit(u.w_off, u.wld, st_out, majors.data(), ones.data(), u.nl, slices, in_row);
     add_unit_tiles(u, uint32_t(units.size()), ents.data(), ents.size(), utiles, klist);
     units.push_back(u);
 }
@@ -294,9 +295,10 @@ void SBuild::validate(uint64_t t_len, uint64_t s_len) const {
         const UnitD& u = units[i];
         if (!u.ne || !u.nl) continue;
         const WGenUnitD& g = cg.units[i];
-        if (g.w_off != u.w_off || g.nl != u.nl || g.nk != u.nk || g.line0 != u.line0)
+        if (g.w_off != u.w_off || g.wld != u.wld || g.nl != u.nl || g.nk != u.nk || g.line0 != u.line0)
             throw std::runtime_error("S build: coefficient unit differs from its S unit");
-        if (u.w_off + uint64_t(u.nl) * u.nk > w_len) throw std::runtime_error("device work list out of bounds: coefficient block");
+        if (u.wld < u.nl || u.wld % 4 || u.w_off % 4 || u.w_off + uint64_t(u.wld) * u.nk > w_len)
+            throw std::runtime_error("device work list out of bounds: coefficient block");
         if (u.erows == 0 || u.ne % u.erows) throw std::runtime_error("S unit: element count is not a whole number of columns");
         uint32_t maxline = 0;
         for (uint32_t l = 0; l < u.nl; ++l) maxline = std::max(maxline, line_b1[u.line0 + l]);
@@ -364,7 +366,8 @@ void validate_tjobs(const std::vector<TJobD>& jobs, uint64_t a_len, uint64_t b_l
         check_extent(j.a_off, j.M, j.K, j.lda, a_len, "T-GEMM psi slab");
         if (j.N && j.K && j.b_off + uint64_t(j.N) * j.K > b_len) throw std::runtime_error("device work list out of bounds: T-GEMM boundary");
         if (j.brs == 0 || j.N % j.brs) throw std::runtime_error("T job: width is not a whole number of blocks");
-        if (j.c_off + uint64_t(j.M) * j.N > t_len) throw std::runtime_error("device work list out of bounds: T output");
+        if (j.sst < j.brs * j.M || j.sst % 4 || j.c_off % 4 || j.c_off + uint64_t(j.N / j.brs) * j.sst > t_len)
+            throw std::runtime_error("device work list out of bounds: T output");
     }
 }
 
@@ -469,10 +472,11 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
                 j.c_off = P.t_len;
                 j.M = ls_ket; j.K = ri.rs; j.brs = R.rsz[ci]; j.N = R.nb[ce] * j.brs; j.lda = ls_ket;
                 j.tr = ci != ce;
+                j.sst = slice_stride(j.brs, j.M);
                 tj[std::size_t(st) * nr + rbb] = uint32_t(P.tjobs.size());
-                tj_first.push_back(js.add(j.c_off, uint64_t(j.brs) * j.M, R.nb[ce]));
+                tj_first.push_back(js.add(j.c_off, j.sst, R.nb[ce]));
                 tj_count.push_back(R.nb[ce]);
-                P.t_len += (uint64_t(j.M) * j.N + 31) / 32 * 32;
+                P.t_len += (uint64_t(R.nb[ce]) * j.sst + 31) / 32 * 32;
                 P.tjobs.push_back(j);
             }
         }
@@ -738,16 +742,17 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
                 const uint32_t ls_bra = uint32_t(left[lb_bra].second), nb = L.nb[ce];
                 const uint64_t c_off = P.t_len;
                 tj[std::size_t(st) * nl + lb_bra] = uint32_t(tj_first.size());
-                tj_first.push_back(js.add(c_off, uint64_t(ls_bra) * rs_ket, nb));
+                const uint32_t bs = slice_stride(rs_ket, ls_bra);  // each T_b block 16-byte aligned
+                tj_first.push_back(js.add(c_off, bs, nb));
                 tj_count.push_back(nb);
-                P.t_len += (uint64_t(ls_bra) * rs_ket * nb + 31) / 32 * 32;
+                P.t_len += (uint64_t(bs) * nb + 31) / 32 * 32;
                 if (nb == 0) continue;
                 // all nb blocks of the cohort in one job: A and C row blocks = MPO-index blocks
                 GemmJob g{};
                 g.a_off = L.data_off[ce]; g.arb = ls_bra; g.a_bs = uint64_t(ls_bra) * ls_ket;
                 g.ta = (ci != ce); g.lda = g.ta ? ls_ket : ls_bra;
                 g.b_off = koff[li.lb] + uint64_t(mo) * ls_ket; g.ldb = ls_ket;
-                g.c_off = c_off; g.crb = ls_bra; g.c_bs = uint64_t(ls_bra) * rs_ket; g.ldc = ls_bra;
+                g.c_off = c_off; g.crb = ls_bra; g.c_bs = bs; g.ldc = ls_bra;
                 g.M = nb * ls_bra; g.N = rs_ket; g.K = ls_ket; g.alpha = 1.0; g.beta = 0.0;
                 P.tgemm.push_back(g);
             }

@@ -64,7 +64,15 @@ struct DevBoundary {
 struct TJobD {        // T[c_off] (M x N) = psi[a_off] (M x K, lda) * Rop (K x N)
     uint64_t a_off, b_off, c_off;
     uint32_t M, K, N, lda, brs, tr;  // Rop(k, n) = R[b_off + (n/brs)*K*brs + (tr ? n%brs + k*brs : k + (n%brs)*K)]
+    // T is stored as N / brs slices (blocks of brs columns, M x brs column-major) sst elements
+    // apart: column n at c_off + (n / brs) * sst + (n % brs) * M; sst = brs * M rounded up to 4
+    // elements, so every slice starts on a 16-byte boundary (FP32 and FP64)
+    uint32_t sst, pad;
 };
+// slice stride of a T job: brs * M rounded up to a multiple of 4 elements
+inline uint32_t slice_stride(uint32_t brs, uint32_t M) { return (brs * M + 3u) / 4u * 4u; }
+// leading dimension of a dense coefficient block: lines rounded up to a multiple of 4
+inline uint32_t coef_ld(uint32_t nl) { return (nl + 3u) / 4u * 4u; }
 struct UnitD {        // S rows of one cohort unit: S_u (lines x elements) = W_u (lines x slices) * slices
     uint64_t s_off;        // S offset of (line 0, element 0) of the unit
     uint64_t line_stride;  // S offset step per line
@@ -75,7 +83,7 @@ struct UnitD {        // S rows of one cohort unit: S_u (lines x elements) = W_u
     uint32_t line0;        // first entry in line_b1[]
     uint32_t nk;           // distinct T slices referenced
     uint32_t slice0;       // first entry in slice_off[]
-    uint32_t pad;
+    uint32_t wld;          // leading dimension of W_u (nl rounded up to 4; rows nl .. wld - 1 are zero)
     uint64_t w_off;        // dense coefficient block W_u (nl x nk, column-major) in the W buffer
 };
 struct SegD {         // K segment of an output block: L cohort (M x nS*ls_in, maybe tile-transposed) times S (ldS = nS*ls_in)
@@ -126,7 +134,7 @@ struct WGenUnitD {
     uint32_t st_out;   // output physical state of the unit
     uint32_t line0, nl;
     uint32_t map0, nk;  // sorted (slice id, slot) pairs at smap_id/smap_slot[map0 .. map0 + nk)
-    uint32_t pad;
+    uint32_t wld;       // leading dimension of the unit's coefficient block
 };
 struct WGenInD { uint32_t c, jbase; };  // per (unit, input state): boundary cohort and slice-id base, or WGEN_NONE
 constexpr uint32_t WGEN_NONE = 0xffffffffu;
@@ -173,7 +181,7 @@ struct CoefGen {
     void set_boundary(const BoundaryIndexH& B);
     // appends one unit: its lines (MPO index and scale each), slot -> slice id, and the
     // (cohort, slice-id base) of each of the nst input states
-    void add_unit(uint64_t w_off, uint32_t st_out, const uint32_t* majors, const double* scales, uint32_t nl,
+    void add_unit(uint64_t w_off, uint32_t wld, uint32_t st_out, const uint32_t* majors, const double* scales, uint32_t nl,
                   const std::vector<uint32_t>& slices, const WGenInD* in_row);
     // appends the per-unit tables of another builder (part) with its lines, slice-map and
     // coefficient-block bases

@@ -97,7 +97,8 @@ __global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, 
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
         uint32_t gm = tile.m0 + m, gn = tile.n0 + n;
         if (gm < J.M && gn < J.N) {
-            const uint64_t o = J.c_off + gm + uint64_t(gn) * J.M;
+            const uint32_t blk = gn / J.brs;
+            const uint64_t o = J.c_off + uint64_t(blk) * J.sst + uint64_t(gn - blk * J.brs) * J.M + gm;
             if (Thi && !Tlo) {
                 Thi[o] = float(v);  // mixed form: T in FP32, split by the S build
             } else if (Thi) {
@@ -147,7 +148,7 @@ __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units,
             int m = e % S::BM, k = e / S::BM;
             uint32_t gm = tile.m0 + m, gk = k0 + k;
             bool ok = gm < U.nl && gk < U.nk;
-            cp8(&s.A[k][m], ok ? Wu + gm + uint64_t(gk) * U.nl : W, ok);
+            cp8(&s.A[k][m], ok ? Wu + gm + uint64_t(gk) * U.wld : W, ok);
         }
         // B row k = T slice k (ne contiguous elements)
 #pragma unroll
@@ -246,7 +247,7 @@ __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ u
                     else hi = mid;
                 }
                 if (lo >= U.nk || ids[lo] != id) { atomicOr(err, 1u); continue; }
-                double* w = Wl + uint64_t(slots[lo]) * U.nl;
+                double* w = Wl + uint64_t(slots[lo]) * U.wld;
                 *w = __dadd_rn(*w, a);
             }
         }
@@ -270,7 +271,7 @@ void CoefGen::validate() const {
         if (g.c != WGEN_NONE && g.c >= ncoh) bad("boundary cohort");
     for (const WGenUnitD& g : units) {
         if (g.st_out >= nst || std::size_t(g.line0) + g.nl > line_major.size() || std::size_t(g.map0) + g.nk > smap_id.size() ||
-            g.w_off + uint64_t(g.nl) * g.nk > w_len)
+            g.wld < g.nl || g.w_off + uint64_t(g.wld) * g.nk > w_len)
             bad("unit extent");
         for (uint32_t l = 0; l < g.nl; ++l)
             if (line_major[g.line0 + l] >= nmaj) bad("line index");
@@ -557,8 +558,15 @@ int heff_launches_per_apply(const HeffPlan& p) {
 void upload_plan(HeffPlan& p) {
     cudaStream_t s = p.stream;
     for (const UnitD& u : p.units)
-        if (u.w_off + uint64_t(u.nl) * u.nk > p.w_len || (u.nk && u.slice0 + u.nk > p.slice_off.size()))
+        if (u.wld < u.nl || u.wld % 4 || u.w_off % 4 || u.w_off + uint64_t(u.wld) * u.nk > p.w_len ||
+            (u.nk && u.slice0 + u.nk > p.slice_off.size()))
             throw std::runtime_error("heff plan: unit outside its work lists");
+    for (const TJobD& j : p.tjobs)
+        if (j.brs == 0 || j.N % j.brs || j.sst < j.brs * j.M || j.sst % 4 || j.c_off % 4 ||
+            j.c_off + uint64_t(j.N / j.brs) * j.sst > p.t_len)
+            throw std::runtime_error("heff plan: T job outside the T buffer");
+    for (std::size_t k = 0; k < p.slice_off.size(); ++k)
+        if (p.slice_off[k] % 4) throw std::runtime_error("heff plan: T slice not 16-byte aligned");
     for (int sh = 0; sh < N_SHAPES; ++sh)
         for (const TileD& t : p.utiles[sh]) {
             if (t.item >= p.units.size() || std::size_t(t.pad) >= p.klist.size() ||

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(XTHR) k_sgemm_x3(const UnitD* __restrict__ uni
             const int m = e % S::BM, k = e / S::BM;
             const uint32_t gm = tile.m0 + m, gk = k0 + k;
             const bool ok = gm < U.nl && gk < U.nk;
-            const uint64_t o = ok ? U.w_off + gm + uint64_t(gk) * U.nl : 0;
+            const uint64_t o = ok ? U.w_off + gm + uint64_t(gk) * U.wld : 0;
             cp4(&s.Ah[k][m], Wh + o, ok);
             if (PRE) cp4(&s.Al[k][m], Wl + o, ok);
         }
@@ -329,7 +329,7 @@ __global__ void __launch_bounds__(XTHR) k_sgemm_tc(const UnitD* __restrict__ uni
             const int l = e % BML, k = e / BML;
             const uint32_t gl = tile.m0 + l, gk = k0 + k;
             const bool ok = gl < U.nl && gk < U.nk;
-            const uint64_t o = ok ? U.w_off + gl + uint64_t(gk) * U.nl : 0;
+            const uint64_t o = ok ? U.w_off + gl + uint64_t(gk) * U.wld : 0;
             const int i = tc_idx<BML>(l, k);
             cp4(&s.Bh[i], Wh + o, ok);
             cp4(&s.Bl[i], Wl + o, ok);

@@ -233,10 +233,10 @@ void CoefGen::append_units(const CoefGen& x, uint32_t line_base, uint32_t map_ba
     smap_slot.insert(smap_slot.end(), x.smap_slot.begin(), x.smap_slot.end());
 }
 
-void CoefGen::add_unit(uint64_t w_off, uint32_t st_out, const uint32_t* majors, const double* scales, uint32_t nl,
+void CoefGen::add_unit(uint64_t w_off, uint32_t wld, uint32_t st_out, const uint32_t* majors, const double* scales, uint32_t nl,
                        const std::vector<uint32_t>& slices, const WGenInD* in_row) {
     WGenUnitD g{};
-    g.w_off = w_off; g.st_out = st_out;
+    g.w_off = w_off; g.wld = wld; g.st_out = st_out;
     g.line0 = uint32_t(line_major.size()); g.nl = nl;
     g.map0 = uint32_t(smap_id.size()); g.nk = uint32_t(slices.size());
     line_major.insert(line_major.end(), majors, majors + nl);
@@ -341,9 +341,10 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 j.c_off = P.t_len;
                 j.M = ls_in; j.K = ri.rs; j.brs = R.rsz[ci]; j.N = R.nb[ce] * j.brs; j.lda = ls_in;
                 j.tr = (ci != ce) ? 1 : 0;
+                j.sst = slice_stride(j.brs, j.M);
                 P.flops_t += 2.0 * ls_in * double(R.cohort_size(ce));
                 tj[std::size_t(st) * nr + rbb] = uint32_t(P.tjobs.size());
-                P.t_len += (uint64_t(j.M) * j.N + 31) / 32 * 32;
+                P.t_len += (uint64_t(R.nb[ce]) * j.sst + 31) / 32 * 32;
                 P.tjobs.push_back(j);
                 P.tjob_mps.push_back(mps_off);
             }
@@ -443,17 +444,18 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 ud.nl = uint32_t(u.lines.size()); ud.line0 = uint32_t(P.line_b1.size());
                 ud.nk = uint32_t(slices.size()); ud.slice0 = uint32_t(P.slice_off.size());
                 ud.w_off = P.w_len;
-                P.w_len += uint64_t(ud.nl) * ud.nk;
+                ud.wld = coef_ld(ud.nl);
+                P.w_len += uint64_t(ud.wld) * ud.nk;
                 for (uint32_t gp : slices) {
                     // slice id -> (job, b2 position) -> T offset of the slice
                     uint32_t job = uint32_t(std::upper_bound(job_pos0.begin(), job_pos0.end(), gp) - job_pos0.begin()) - 1;
                     uint32_t pos = gp - job_pos0[job];
-                    P.slice_off.push_back(P.tjobs[job].c_off + uint64_t(pos) * u.ms * ls_in);
+                    P.slice_off.push_back(P.tjobs[job].c_off + uint64_t(pos) * P.tjobs[job].sst);
                 }
                 // coefficient generation: lines with their L conj scales, slot -> slice id
                 lscale.resize(ud.nl);
                 for (uint32_t l = 0; l < ud.nl; ++l) lscale[l] = L.conj_scale(ci, u.rows[l]);
-                P.cg.add_unit(ud.w_off, u.st, u.rows.data(), lscale.data(), ud.nl, slices, &gin[ui * nst]);
+                P.cg.add_unit(ud.w_off, ud.wld, u.st, u.rows.data(), lscale.data(), ud.nl, slices, &gin[ui * nst]);
                 if (bookkeeping)
                     for (std::size_t i = 0; i < u.em.size(); ++i) {
                         uint32_t row[10] = {lb_in, lb_out, ci, ce, u.offset, u.ms, u.lines[u.em[i].line],
@@ -475,7 +477,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 P.units.push_back(ud);
                 P.g_elems += uint64_t(ud.ne) * ud.nl;
                 P.g_reads += uint64_t(ud.ne) * u.em.size();
-                P.flops_sdense += 2.0 * ud.nl * ud.nk * double(ud.ne);
+                P.flops_sdense += 2.0 * ud.nl * ud.nk * double(ud.ne);  // padding lines not counted
             }
             P.flops_ls += 2.0 * ls_out * ls_in * double(nS) * stripe;
             SegD sg{};
