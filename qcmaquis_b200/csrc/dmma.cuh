@@ -22,6 +22,11 @@ static __device__ __forceinline__ void cp8(double* smem, const double* gmem, boo
     unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(pred ? 8 : 0));
 }
+// 16-byte asynchronous copy (both addresses 16-byte aligned); a false predicate writes zeros
+static __device__ __forceinline__ void cp16(void* smem, const void* gmem, bool pred) {
+    unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(pred ? 16 : 0));
+}
 static __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 static __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 
@@ -39,7 +44,7 @@ using Sh64 = Shape<2, 2, 4, 4>;  // 64 x 64
 using Sh128 = Shape<4, 1, 4, 4>; // 128 x 32
 
 template <class S>
-struct Stage {
+struct __align__(16) Stage {
     double A[BK][S::BM + PAD];
     double B[BK][S::BN + PAD];
 };

@@ -94,25 +94,46 @@ __global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, 
         if (kc + 1 < nk) issue((kc + 1) & 1, (kc + 1) * BK);
         mma_stage<S>(st[kc & 1].A, st[kc & 1].B, acc, warp, lane);
     }
-    for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
-        uint32_t gm = tile.m0 + m, gn = tile.n0 + n;
-        if (gm < J.M && gn < J.N) {
-            const uint32_t blk = gn / J.brs;
-            const uint64_t o = J.c_off + uint64_t(blk) * J.sst + uint64_t(gn - blk * J.brs) * J.M + gm;
-            if (Thi && !Tlo) {
-                Thi[o] = float(v);  // mixed form: T in FP32, split by the S build
-            } else if (Thi) {
-                // mixed form (tensor-memory path): T as TF32 hi + lo (round to nearest)
-                uint32_t h, l;
-                asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(float(v)));
-                asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(l) : "f"(float(v - double(__uint_as_float(h)))));
-                Thi[o] = __uint_as_float(h);
-                Tlo[o] = __uint_as_float(l);
-            } else {
-                T[o] = v;
-            }
+    // the thread's output columns: FN fragments x 2 columns each; their T offsets once (slice
+    // blk at blk * sst, column within it at (n % brs) * M)
+    const int r = lane >> 2, q = lane & 3;
+    const int wm = warp % S::WM, wn = warp / S::WM;
+    uint64_t cof[S::FN][2];
+    bool cok[S::FN][2];
+#pragma unroll
+    for (int j = 0; j < S::FN; ++j)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const uint32_t gn = tile.n0 + wn * S::FN * 8 + j * 8 + q * 2 + c;
+            cok[j][c] = gn < J.N;
+            const uint32_t blk = cok[j][c] ? gn / J.brs : 0;
+            cof[j][c] = J.c_off + uint64_t(blk) * J.sst + uint64_t(gn - blk * J.brs) * J.M;
         }
-    });
+#pragma unroll
+    for (int i = 0; i < S::FM; ++i) {
+        const uint32_t gm = tile.m0 + wm * S::FM * 8 + i * 8 + r;
+        if (gm >= J.M) continue;
+#pragma unroll
+        for (int j = 0; j < S::FN; ++j)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                if (!cok[j][c]) continue;
+                const double v = acc.c[i][j][c];
+                const uint64_t o = cof[j][c] + gm;
+                if (Thi && !Tlo) {
+                    Thi[o] = float(v);  // mixed form: T in FP32, split by the S build
+                } else if (Thi) {
+                    // mixed form (tensor-memory path): T as TF32 hi + lo (round to nearest)
+                    uint32_t h, l;
+                    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(h) : "f"(float(v)));
+                    asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(l) : "f"(float(v - double(__uint_as_float(h)))));
+                    Thi[o] = __uint_as_float(h);
+                    Tlo[o] = __uint_as_float(l);
+                } else {
+                    T[o] = v;
+                }
+            }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -130,34 +151,39 @@ __global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units,
     const uint16_t* ks = klist + tile.pad;
     const uint32_t nsteps = ks[0];
     const double* Wu = W + U.w_off;
+    // 16-byte chunks (2 doubles): W_u columns (ld wld, rows nl .. wld - 1 zero) and T slices (sst
+    // apart, 16-byte aligned) are read 16 bytes at a time; a chunk past the slice's ne elements
+    // is not read, one that straddles ne reads the slice's padding into columns the epilogue drops
+    constexpr int ACH = S::BM / 2 * BK, BCH = S::BN / 2 * BK;
+    static_assert(ACH % NTHR == 0 && BCH % NTHR == 0, "whole chunks per thread");
     // T offsets of the slices this thread copies, loaded one stage ahead of their use
-    uint64_t boff[S::B_PER];
+    uint64_t boff[BCH / NTHR];
     auto load_offs = [&](uint32_t k0) {
 #pragma unroll
-        for (int rr = 0; rr < S::B_PER; ++rr) {
-            const uint32_t gk = k0 + uint32_t(tid + rr * NTHR) / S::BN;
+        for (int rr = 0; rr < BCH / NTHR; ++rr) {
+            const uint32_t gk = k0 + uint32_t(tid + rr * NTHR) / (S::BN / 2);
             boff[rr] = gk < U.nk ? __ldg(slice_off + U.slice0 + gk) : 0;
         }
     };
     auto issue = [&](int sidx, uint32_t k0) {
         Stage<S>& s = st[sidx];
-        // A = W_u (lines x slices, column-major, ld nl)
+        // A = W_u (lines x slices, column-major, ld wld)
 #pragma unroll
-        for (int rr = 0; rr < S::A_PER; ++rr) {
-            int e = tid + rr * NTHR;
-            int m = e % S::BM, k = e / S::BM;
-            uint32_t gm = tile.m0 + m, gk = k0 + k;
-            bool ok = gm < U.nl && gk < U.nk;
-            cp8(&s.A[k][m], ok ? Wu + gm + uint64_t(gk) * U.wld : W, ok);
+        for (int rr = 0; rr < ACH / NTHR; ++rr) {
+            const int c = tid + rr * NTHR;
+            const int m = 2 * (c % (S::BM / 2)), k = c / (S::BM / 2);
+            const uint32_t gm = tile.m0 + m, gk = k0 + k;
+            const bool ok = gm < U.wld && gk < U.nk;
+            cp16(&s.A[k][m], ok ? Wu + gm + uint64_t(gk) * U.wld : W, ok);
         }
         // B row k = T slice k (ne contiguous elements)
 #pragma unroll
-        for (int rr = 0; rr < S::B_PER; ++rr) {
-            int e = tid + rr * NTHR;
-            int n = e % S::BN, k = e / S::BN;
-            uint32_t gn = tile.n0 + n, gk = k0 + k;
-            bool ok = gn < U.ne && gk < U.nk;
-            cp8(&s.B[k][n], ok ? T + boff[rr] + gn : T, ok);
+        for (int rr = 0; rr < BCH / NTHR; ++rr) {
+            const int c = tid + rr * NTHR;
+            const int n = 2 * (c % (S::BN / 2)), k = c / (S::BN / 2);
+            const uint32_t gn = tile.n0 + n, gk = k0 + k;
+            const bool ok = gn < U.ne && gk < U.nk;
+            cp16(&s.B[k][n], ok ? T + boff[rr] + gn : T, ok);
         }
         cp_commit();
     };

@@ -63,7 +63,7 @@ using X128 = XShape<4, 1, 2, 4>;  // 128 x 32
 // PRE: operands pre-split in HBM (hi and lo arrays); otherwise single FP32 values split at the
 // fragment loads
 template <class S, bool PRE>
-struct XStage {
+struct __align__(16) XStage {
     float Ah[XBK][S::BM + S::PA], Al[PRE ? XBK : 1][S::BM + S::PA];
     float Bh[XBK][S::BN + S::PB], Bl[PRE ? XBK : 1][S::BN + S::PB];
 };
@@ -78,6 +78,10 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
 __device__ __forceinline__ void cp4(float* smem, const float* gmem, bool pred) {
     const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(pred ? 4 : 0));
+}
+__device__ __forceinline__ void cp16(void* smem, const void* gmem, bool pred) {
+    const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(pred ? 16 : 0));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
@@ -105,35 +109,42 @@ __global__ void __launch_bounds__(XTHR) k_sgemm_x3(const UnitD* __restrict__ uni
     const int wm = warp % S::WM, wn = warp / S::WM;
     const uint16_t* ks = klist + tile.pad;
     const uint32_t nsteps = ks[0];
-    uint64_t boff[S::B_PER];
+    // 16-byte chunks (4 floats) along the W_u columns (ld wld, rows nl .. wld - 1 zero) and the
+    // T slices (16-byte aligned); a chunk past a slice's ne elements is not read, one that
+    // straddles ne reads the slice's padding into columns the epilogue drops
+    constexpr int ACH = S::BM / 4 * XBK, BCH = S::BN / 4 * XBK;
+    constexpr int ARND = (ACH + XTHR - 1) / XTHR, BRND = BCH / XTHR;
+    static_assert(BCH % XTHR == 0, "whole B chunks per thread");
+    uint64_t boff[BRND];
     auto load_offs = [&](uint32_t k0) {
 #pragma unroll
-        for (int rr = 0; rr < S::B_PER; ++rr) {
-            const uint32_t gk = k0 + uint32_t(tid + rr * XTHR) / S::BN;
+        for (int rr = 0; rr < BRND; ++rr) {
+            const uint32_t gk = k0 + uint32_t(tid + rr * XTHR) / (S::BN / 4);
             boff[rr] = gk < U.nk ? __ldg(slice_off + U.slice0 + gk) : 0;
         }
     };
     auto issue = [&](int sidx, uint32_t k0) {
         XStage<S, PRE>& s = st[sidx];
 #pragma unroll
-        for (int rr = 0; rr < S::A_PER; ++rr) {
-            const int e = tid + rr * XTHR;
-            const int m = e % S::BM, k = e / S::BM;
+        for (int rr = 0; rr < ARND; ++rr) {
+            const int c = tid + rr * XTHR;
+            if (ACH % XTHR != 0 && c >= ACH) break;
+            const int m = 4 * (c % (S::BM / 4)), k = c / (S::BM / 4);
             const uint32_t gm = tile.m0 + m, gk = k0 + k;
-            const bool ok = gm < U.nl && gk < U.nk;
+            const bool ok = gm < U.wld && gk < U.nk;
             const uint64_t o = ok ? U.w_off + gm + uint64_t(gk) * U.wld : 0;
-            cp4(&s.Ah[k][m], Wh + o, ok);
-            if (PRE) cp4(&s.Al[k][m], Wl + o, ok);
+            cp16(&s.Ah[k][m], Wh + o, ok);
+            if (PRE) cp16(&s.Al[k][m], Wl + o, ok);
         }
 #pragma unroll
-        for (int rr = 0; rr < S::B_PER; ++rr) {
-            const int e = tid + rr * XTHR;
-            const int n = e % S::BN, k = e / S::BN;
+        for (int rr = 0; rr < BRND; ++rr) {
+            const int c = tid + rr * XTHR;
+            const int n = 4 * (c % (S::BN / 4)), k = c / (S::BN / 4);
             const uint32_t gn = tile.n0 + n, gk = k0 + k;
             const bool ok = gn < U.ne && gk < U.nk;
             const uint64_t o = ok ? boff[rr] + gn : 0;
-            cp4(&s.Bh[k][n], Th + o, ok);
-            if (PRE) cp4(&s.Bl[k][n], Tl + o, ok);
+            cp16(&s.Bh[k][n], Th + o, ok);
+            if (PRE) cp16(&s.Bl[k][n], Tl + o, ok);
         }
         cp_commit();
     };
