@@ -200,7 +200,7 @@ int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, double* y_de
 /* Eigensolver, boundary propagation and the two-site sweep                   */
 /* ------------------------------------------------------------------------ */
 
-/* Lowest eigenpair of H_eff by Jacobi-Davidson (no GMRES inner solve), start
+/* Lowest eigenpair of H_eff by Jacobi-Davidson (no GMRES inner solve, no ortho vectors), start
  * vector x0, eigenvector to out (host buffers of vec_len doubles, the
  * qcm_heff_apply layout); search space and updates in HBM.  Replaces
  * solve<double>(out, initial, SH, ortho = {}, jcd_gmres = 0, tol, maxiter)
@@ -213,6 +213,19 @@ int qcm_jd_solve(qcm_heff* h, const double* x0, double tol, int maxiter, double*
  * error is of second order in the vector's. */
 int qcm_jd_solve_mode(qcm_heff* h, const double* x0, double tol, int maxiter, int precision, double* out, double* eval,
                       int* iters);
+/* The full solver seam: solve<double>(out, initial, SH, ortho_vecs, jcd_gmres, jcd_tol, jcd_max_iter)
+ * (solver/solver.h:64-68, solver.cpp:14-28 -> solve_ietl_jcd, ietl_jacobi_davidson.h:35-76).
+ * ortho[i] (i < n_ortho; host, vec_len doubles each) are states the solution is kept orthogonal to
+ * (excited states): they are Gram-Schmidt'd among themselves, then projected out of the start
+ * vector, of every new search direction and of A u (DavidsonVS::project, ietl_interface_dv.h:94-99);
+ * at most vec_len - 1 are used.  gmres (0..64, ietl_jcd_gmres) is the GMRES iteration count of each
+ * correction equation (I - uu*)(A - theta)(I - uu*) t = -r, started from t0 = -r + (r.u)/(u.u) u with
+ * absolute tolerance 2^-(it+1) (jcd_gmres_solver, ietl/jacobi.h:126-164; ietl_gmres,
+ * ietl/gmres.h:78-146); 0 uses t0.  As in the reference, GMRES keeps only the directions before its
+ * last inner step, so gmres = 1 gives the same result as 0 at one more H.psi per correction.
+ * *applies (may be NULL): H.psi applies made (the mixed form's FP64 Rayleigh quotient excluded). */
+int qcm_jd_solve_ex(qcm_heff* h, const double* x0, const double* const* ortho, int n_ortho, int gmres, double tol,
+                    int maxiter, int precision, double* out, double* eval, int* iters, int* applies);
 
 /* New environment from one MPS site tensor, given right-paired (its blocks
  * ls x stripe, column-major, concatenated in left-sector order, as for
@@ -255,6 +268,7 @@ typedef struct {
     int32_t ngrowsweeps, nmainsweeps;
     int32_t hpsi_precision;       /* QCM_PRECISION_FP64, or QCM_PRECISION_MIXED: JD with the mixed H.psi
                                      and an FP64 Rayleigh quotient of each step's final vector */
+    int32_t jcd_gmres;            /* ietl_jcd_gmres (0..64): GMRES iterations per JD correction */
 } qcm_dmrg_params;
 /* block_matrix_algorithms.h:48-63 */
 typedef struct {

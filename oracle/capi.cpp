@@ -98,6 +98,13 @@ int orc_dmrg_set_heev(orc_dmrg* h, int heev, double a_init, double a_main, doubl
     return 0;
 }
 
+// ietl_jcd_gmres of the sweep's solves
+int orc_dmrg_set_gmres(orc_dmrg* h, int gmres) {
+    if (gmres < 0) return fail("orc_dmrg_set_gmres: gmres < 0");
+    h->d->p.jcd_gmres = gmres;
+    return 0;
+}
+
 // energies/tw/tf/bond: arrays of 2L-2.  If stop_step >= 0, the frozen site problem of
 // that step is returned in *snap (free with orc_free) and the sweep stops there.
 int orc_dmrg_sweep(orc_dmrg* h, int sweep, double* energies, double* tw, double* tf, uint64_t* bond, int stop_step,
@@ -193,6 +200,47 @@ int orc_heff_apply(const void* snap, size_t n, const void* mpo_blob, size_t mn, 
         auto t1 = std::chrono::steady_clock::now();
         if (flops) *flops = double(sched->total_flops);
         if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count() / std::max(1, repeat);
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
+// Jacobi-Davidson on a frozen site problem (solve_ietl_jcd, ietl_jacobi_davidson.h:35-76): start
+// vector x0, n_ortho ortho vectors of len doubles each (contiguous), GMRES(gmres) corrections.
+int orc_jd_solve(const void* snap, size_t n, const void* mpo_blob, size_t mn, int site1, const double* x0, size_t len,
+                 const double* ortho, int n_ortho, int gmres, double tol, int maxiter, double* out, double* eval,
+                 int* iters, int* applies) {
+    try {
+        bool ts = false;
+        auto mpo = load_mpo_blob(static_cast<const uint8_t*>(mpo_blob), mn, ts);
+        MPOTensor W = ts ? mpo[site1] : make_twosite_mpo(mpo[site1], mpo[site1 + 1]);
+        MPSTensor twin;
+        Boundary Lb, Rb;
+        load_site_problem(static_cast<const uint8_t*>(snap), n, twin, Lb, Rb);
+        auto sched = create_contraction_schedule(twin, Lb, Rb, W);
+        std::vector<std::size_t> off(twin.left.size(), SIZE_MAX);
+        std::size_t tot = 0;
+        for (std::size_t k = 0; k < twin.data.n_blocks(); ++k) {
+            off[twin.left.position(twin.data.lc[k])] = tot;
+            tot += twin.data.b[k].d.size();
+        }
+        if (tot != len) return fail("orc_jd_solve: vector length mismatch");
+        if (maxiter < 1 || gmres < 0 || n_ortho < 0) return fail("orc_jd_solve: bad iteration counts");
+        auto mult = [&](const std::vector<double>& x, std::vector<double>& y) {
+            std::vector<const double*> xv(twin.left.size(), nullptr);
+            std::vector<double*> yv(twin.left.size(), nullptr);
+            for (std::size_t lb = 0; lb < off.size(); ++lb)
+                if (off[lb] != SIZE_MAX) { xv[lb] = x.data() + off[lb]; yv[lb] = y.data() + off[lb]; }
+            std::fill(y.begin(), y.end(), 0.0);
+            super_hamil_mv(*sched, Lb, Rb, xv, yv);
+        };
+        std::vector<std::vector<double>> O;
+        O.resize(std::size_t(n_ortho));
+        for (int i = 0; i < n_ortho; ++i) O[i].assign(ortho + std::size_t(i) * len, ortho + std::size_t(i + 1) * len);
+        std::vector<double> x(x0, x0 + len), xo;
+        int it = 0;
+        *eval = jacobi_davidson(mult, x, tol, maxiter, xo, it, gmres, O, applies);
+        std::copy(xo.begin(), xo.end(), out);
+        if (iters) *iters = it;
         return 0;
     } catch (const std::exception& e) { return fail(e.what()); }
 }

@@ -393,42 +393,142 @@ void multiply_from_right(MPSTensor& t, const BlockMatrix& N) {
 }
 
 // ---------------------------------------------------------------------------
-// Jacobi-Davidson (ietl/jacobi.h:386-474; jcd_gmres_solver with max_iter 0 at :141-157)
+// Jacobi-Davidson for the lowest eigenpair: solve_ietl_jcd (dmrg/solver/ietl_jacobi_davidson.h:35-76)
+// -> jacobi_davidson::calculate_eigenvalue (ietl/jacobi.h:386-474), the correction equation by
+// jcd_gmres_solver (ietl/jacobi.h:126-164) through ietl_gmres (ietl/gmres.h:78-146) on the operator
+// (I - uu*)(A - theta)(I - uu*) (jcd_solver_operator, ietl/jacobi.h:249-268), and the projection
+// against the ortho vectors (DavidsonVS::project, dmrg/solver/ietl_interface_dv.h:94-99).
+namespace {
+using Vec = std::vector<double>;
+double vdot(const Vec& a, const Vec& b) {
+    double s = 0;
+    for (std::size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
+    return s;
+}
+void vaxpy(double a, const Vec& x, Vec& y) {
+    for (std::size_t i = 0; i < y.size(); ++i) y[i] += a * x[i];
+}
+
+// GeneratePlaneRotation / ApplyPlaneRotation (ietl/gmres.h:40-66)
+void gen_rot(double dx, double dy, double& cs, double& sn) {
+    if (dy == 0.0) { cs = 1; sn = 0; }
+    else if (std::fabs(dy) > std::fabs(dx)) { double t = dx / dy; sn = 1.0 / std::sqrt(1.0 + t * t); cs = t * sn; }
+    else { double t = dy / dx; cs = 1.0 / std::sqrt(1.0 + t * t); sn = t * cs; }
+}
+void apply_rot(double& dx, double& dy, double cs, double sn) {
+    const double r0 = cs * dx + sn * dy, r1 = -sn * dx + cs * dy;
+    dx = r0; dy = r1;
+}
+
+// ietl_gmres::operator() (ietl/gmres.h:92-146).  On a break at inner step i the update uses the
+// first i directions only (Update(H, s, i), :66-75 and :140), as the reference does.
+Vec gmres(const std::function<void(const Vec&, Vec&)>& A, const Vec& b, const Vec& x0, double abs_tol, int max_iter) {
+    const std::size_t m = std::size_t(max_iter);
+    Vec s(m + 1, 0.0), cs(m + 1, 0.0), sn(m + 1, 0.0);
+    std::vector<Vec> v(m + 1);
+    A(x0, v[0]);
+    Vec r = b;
+    vaxpy(-1.0, v[0], r);
+    s[0] = std::sqrt(vdot(r, r));
+    if (std::fabs(s[0]) < abs_tol) return x0;
+    v[0] = r;
+    for (double& e : v[0]) e /= s[0];
+    std::vector<double> H((m + 1) * (m + 1), 0.0);
+    auto h = [&](std::size_t i, std::size_t j) -> double& { return H[i + j * (m + 1)]; };
+    std::size_t i = 0;
+    Vec w;
+    for (; i + 1 < m; ++i) {
+        A(v[i], w);
+        for (std::size_t k = 0; k <= i; ++k) {
+            h(k, i) = vdot(w, v[k]);
+            vaxpy(-h(k, i), v[k], w);
+        }
+        h(i + 1, i) = std::sqrt(vdot(w, w));
+        v[i + 1] = w;
+        for (double& e : v[i + 1]) e /= h(i + 1, i);
+        for (std::size_t k = 0; k < i; ++k) apply_rot(h(k, i), h(k + 1, i), cs[k], sn[k]);
+        gen_rot(h(i, i), h(i + 1, i), cs[i], sn[i]);
+        apply_rot(h(i, i), h(i + 1, i), cs[i], sn[i]);
+        apply_rot(s[i], s[i + 1], cs[i], sn[i]);
+        if (std::fabs(s[i + 1]) < abs_tol) break;
+    }
+    Vec y(s.begin(), s.begin() + i);
+    for (std::ptrdiff_t a = std::ptrdiff_t(i) - 1; a >= 0; --a) {
+        y[a] /= h(a, a);
+        for (std::ptrdiff_t c = a - 1; c >= 0; --c) y[c] -= h(c, a) * y[a];
+    }
+    Vec out = x0;
+    for (std::size_t k = 0; k < i; ++k) vaxpy(y[k], v[k], out);
+    return out;
+}
+}  // namespace
+
 double jacobi_davidson(const std::function<void(const std::vector<double>&, std::vector<double>&)>& mult,
-                       const std::vector<double>& x0, double tol, int maxiter, std::vector<double>& out, int& iters) {
+                       const std::vector<double>& x0, double tol, int maxiter, std::vector<double>& out, int& iters,
+                       int gmres_iter, const std::vector<std::vector<double>>& ortho_in, int* applies) {
     const std::size_t n = x0.size();
-    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
-        double s = 0; for (std::size_t i = 0; i < n; ++i) s += a[i] * b[i]; return s; };
-    auto nrm = [&](const std::vector<double>& a) { return std::sqrt(dot(a, a)); };
-    std::vector<std::vector<double>> V(maxiter), VA(maxiter);
+    int napply = 0;
+    auto A = [&](const Vec& x, Vec& y) { y.assign(n, 0.0); mult(x, y); ++napply; };
+    // ortho vectors: at most n - 1, Gram-Schmidt among themselves (ietl_jacobi_davidson.h:41-48)
+    std::vector<Vec> O(ortho_in.begin(), ortho_in.begin() + std::min(ortho_in.size(), n ? n - 1 : 0));
+    for (std::size_t a = 1; a < O.size(); ++a)
+        for (std::size_t b = 0; b < a; ++b) vaxpy(-vdot(O[b], O[a]) / vdot(O[b], O[b]), O[b], O[a]);
+    auto project = [&](Vec& t) { for (const Vec& o : O) vaxpy(-vdot(o, t) / vdot(o, o), o, t); };
+    auto nrm = [&](const Vec& a) { return std::sqrt(vdot(a, a)); };
+    std::vector<Vec> V(maxiter), VA(maxiter);
     std::vector<double> M(std::size_t(maxiter) * maxiter, 0.0);
     V[0] = x0;
+    project(V[0]);
     int it = 0;
     double theta = 0;
-    std::vector<double> s, u(n), uA(n);
+    std::vector<double> s;
+    Vec u(n), uA(n);
     while (true) {
-        std::vector<double>& t = V[it];
+        Vec& t = V[it];
         double tau = nrm(t);
-        for (int i = 1; i <= it; ++i) { double d = dot(V[i - 1], t); for (std::size_t k = 0; k < n; ++k) t[k] -= d * V[i - 1][k]; }
+        for (int i = 1; i <= it; ++i) vaxpy(-vdot(V[i - 1], t), V[i - 1], t);
         if (nrm(t) < 0.25 * tau)
-            for (int i = 1; i <= it; ++i) { double d = dot(V[i - 1], t); for (std::size_t k = 0; k < n; ++k) t[k] -= d * V[i - 1][k]; }
+            for (int i = 1; i <= it; ++i) vaxpy(-vdot(V[i - 1], t), V[i - 1], t);
+        project(t);
         double tn = nrm(t);
         for (auto& x : t) x /= tn;
-        VA[it].assign(n, 0.0);
-        mult(t, VA[it]);
-        for (int i = 1; i <= it + 1; ++i) M[(i - 1) + std::size_t(it) * maxiter] = dot(V[i - 1], VA[it]);
+        A(t, VA[it]);
+        for (int i = 1; i <= it + 1; ++i) M[(i - 1) + std::size_t(it) * maxiter] = vdot(V[i - 1], VA[it]);
         dsyevx_lowest(M.data(), maxiter, it + 1, tol, theta, s);
         for (std::size_t k = 0; k < n; ++k) { u[k] = V[0][k] * s[0]; uA[k] = VA[0][k] * s[0]; }
         for (int j = 1; j <= it; ++j)
             for (std::size_t k = 0; k < n; ++k) { u[k] += V[j][k] * s[j]; uA[k] += VA[j][k] * s[j]; }
-        std::vector<double>& r = uA;
-        for (std::size_t k = 0; k < n; ++k) r[k] -= theta * u[k];
+        project(uA);
+        Vec& r = uA;
+        vaxpy(-theta, u, r);
         ++it;
         double rn = nrm(r);
-        if (rn <= tol * std::fabs(theta) || rn < tol || it >= maxiter) { out = u; iters = it; return theta; }
-        double dru = dot(r, u), duu = dot(u, u);
-        V[it].assign(n, 0.0);
-        for (std::size_t k = 0; k < n; ++k) V[it][k] = -r[k] + dru / duu * u[k];
+        if (rn <= tol * std::fabs(theta) || rn < tol || it >= maxiter) {
+            out = u;
+            iters = it;
+            if (applies) *applies = napply;
+            return theta;
+        }
+        // jcd_gmres_solver::operator() (ietl/jacobi.h:141-157): start t0 = -r + (r.u)/(u.u) u, then
+        // GMRES(max_iter = ietl_jcd_gmres) on -r with abs_tol 2^-(it+1)
+        const double dru = vdot(r, u), duu = vdot(u, u);
+        Vec t0(n);
+        for (std::size_t k = 0; k < n; ++k) t0[k] = -r[k] + dru / duu * u[k];
+        if (gmres_iter > 0) {
+            const double th = theta;
+            auto op = [&](const Vec& x, Vec& y) {
+                Vec t2 = x;
+                vaxpy(-vdot(u, x), u, t2);
+                A(t2, y);
+                vaxpy(-th, t2, y);
+                vaxpy(-vdot(u, y), u, y);
+            };
+            Vec inh(n);
+            for (std::size_t k = 0; k < n; ++k) inh[k] = -r[k];
+            V[it] = gmres(op, inh, t0, 1.0 / std::pow(2.0, double(it + 1)), gmres_iter);
+        } else {
+            V[it] = std::move(t0);
+        }
     }
 }
 
@@ -572,7 +672,7 @@ void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<Trunca
         };
         std::vector<double> xo;
         int iters = 0;
-        double E = jacobi_davidson(mult, x0, p.jcd_tol, p.jcd_maxiter, xo, iters);
+        double E = jacobi_davidson(mult, x0, p.jcd_tol, p.jcd_maxiter, xo, iters, p.jcd_gmres);
         jd_time += now_s() - t1;
         for (std::size_t k = 0; k < twin.data.n_blocks(); ++k)
             std::copy(xo.begin() + off[k], xo.begin() + off[k] + twin.data.b[k].d.size(), twin.data.b[k].d.begin());

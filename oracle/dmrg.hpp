@@ -50,9 +50,12 @@ BlockMatrix normalize_right(MPSTensor& t);
 void multiply_from_left(MPSTensor& t, const BlockMatrix& N);
 void multiply_from_right(MPSTensor& t, const BlockMatrix& N);
 
-// Jacobi-Davidson for the lowest eigenpair (ietl/jacobi.h:386-474, gmres = 0)
+// Jacobi-Davidson for the lowest eigenpair (solve_ietl_jcd, ietl_jacobi_davidson.h:35-76; ietl/jacobi.h:386-474):
+// correction equation by GMRES(gmres) (ietl/gmres.h:78-146; 0 = the projected residual only), search space
+// kept orthogonal to `ortho`; *applies = mult calls
 double jacobi_davidson(const std::function<void(const std::vector<double>&, std::vector<double>&)>& mult,
-                       const std::vector<double>& x0, double tol, int maxiter, std::vector<double>& out, int& iters);
+                       const std::vector<double>& x0, double tol, int maxiter, std::vector<double>& out, int& iters,
+                       int gmres = 0, const std::vector<std::vector<double>>& ortho = {}, int* applies = nullptr);
 
 struct DMRGParams {
     std::size_t Mmax = 64;
@@ -60,6 +63,7 @@ struct DMRGParams {
     double cutoff = 1e-16;
     double jcd_tol = 1e-10;
     int jcd_maxiter = 8;
+    int jcd_gmres = 0;  // ietl_jcd_gmres
     double ecore = 0.0;
     // twosite_truncation = heev and its noise (ts_optimize.hpp:275-296)
     bool heev = false;

@@ -58,6 +58,9 @@ def lib(nthreads: int = 0):
                                      c_int, P(c_double), P(c_double)]
         L.orc_schedule_export.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_void_p), P(c_size_t),
                                           P(c_double)]
+        L.orc_jd_solve.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), c_size_t, P(c_double), c_int,
+                                   c_int, c_double, c_int, P(c_double), P(c_double), P(c_int), P(c_int)]
+        L.orc_dmrg_set_gmres.argtypes = [c_void_p, c_int]
         U32 = P(ctypes.c_uint32)
         L.orc_truncate_svd.argtypes = [ctypes.c_uint32, U32, U32, P(c_double), ctypes.c_uint64, c_double, U32, P(c_double),
                                        P(c_double), P(c_double), P(c_double)]
@@ -131,6 +134,10 @@ class OracleDMRG:
         self.lib.orc_dmrg_set_heev(self.h, 1 if heev else 0, alpha_initial, alpha_main, alpha_final, ngrowsweeps,
                                    nmainsweeps)
 
+    def set_gmres(self, gmres: int):
+        """ietl_jcd_gmres of the sweep's Jacobi-Davidson solves."""
+        _check(self.lib, self.lib.orc_dmrg_set_gmres(self.h, gmres))
+
     def set_mmax(self, M: int):
         self.lib.orc_dmrg_set_mmax(self.h, M)
 
@@ -157,6 +164,22 @@ def heff_apply(snap: bytes, mpo_blob: bytes, site1: int, x: np.ndarray, repeat: 
     _check(L, L.orc_heff_apply(sb, len(snap), mb, len(mpo_blob), site1, _dp(x), _dp(y), x.size, repeat,
                                ctypes.byref(fl), ctypes.byref(sec)))
     return y, fl.value, sec.value
+
+
+def jd_solve(snap: bytes, mpo_blob: bytes, site1: int, x0: np.ndarray, tol: float = 1e-10, maxiter: int = 8,
+             ortho=(), gmres: int = 0):
+    """Oracle Jacobi-Davidson on a frozen site problem: (eigenvalue, vector, iterations, H_eff applies)."""
+    L = lib()
+    x0 = np.ascontiguousarray(x0, dtype=np.float64)
+    O = np.ascontiguousarray(np.array(ortho, dtype=np.float64).reshape(len(ortho), x0.size))
+    out = np.zeros_like(x0)
+    ev, it, na = c_double(), c_int(), c_int()
+    sb = ctypes.create_string_buffer(snap, len(snap))
+    mb = ctypes.create_string_buffer(mpo_blob, len(mpo_blob))
+    _check(L, L.orc_jd_solve(sb, len(snap), mb, len(mpo_blob), site1, _dp(x0), x0.size, _dp(O) if len(ortho) else None,
+                             len(ortho), gmres, tol, maxiter, _dp(out), ctypes.byref(ev), ctypes.byref(it),
+                             ctypes.byref(na)))
+    return ev.value, out, it.value, na.value
 
 
 def schedule_export(snap: bytes, mpo_blob: bytes, site1: int):

@@ -146,6 +146,43 @@ int qcm_jd_solve_mode(qcm_heff* h, const double* x0, double tol, int maxiter, in
     QCM_CATCH
 }
 
+int qcm_jd_solve_ex(qcm_heff* h, const double* x0, const double* const* ortho, int n_ortho, int gmres, double tol,
+                    int maxiter, int precision, double* out, double* eval, int* iters, int* applies) {
+    QCM_TRY
+    if (precision < QCM_PRECISION_FP64 || precision > QCM_PRECISION_MIXED_TC)
+        return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_ex: unknown precision mode");
+    if (!h || !x0 || !out || !eval) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_ex: NULL argument");
+    if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_ex: host-only plan");
+    if (maxiter < 1 || maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_ex: maxiter must be in 1..64");
+    if (gmres < 0 || gmres > qcm::JD_MAX_GMRES) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_ex: gmres must be in 0..64");
+    if (n_ortho < 0 || (n_ortho > 0 && !ortho)) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_ex: bad ortho vectors");
+    for (int i = 0; i < n_ortho; ++i)
+        if (!ortho[i]) return qcm::fail(QCM_ERR_ARG, "qcm_jd_solve_ex: NULL ortho vector");
+    qcm::HeffPlan& p = *h->p;
+    qcm::AllocStream scope(p.stream);
+    qcm::Ctx c;
+    c.s = p.stream;
+    const uint64_t n = p.x_len;
+    qcm::DBuf<double> x(n ? n : 1);
+    QCM_CUDA(cudaMemcpyAsync(x.get(), x0, n * sizeof(double), cudaMemcpyHostToDevice, c.s));
+    qcm::DBuf<double> ov(n_ortho > 0 && n ? uint64_t(n_ortho) * n : 1);
+    for (int i = 0; i < n_ortho; ++i)
+        QCM_CUDA(cudaMemcpyAsync(ov.get() + uint64_t(i) * n, ortho[i], n * sizeof(double), cudaMemcpyHostToDevice, c.s));
+    qcm::JDOptions o;
+    o.gmres = gmres;
+    o.ortho = ov.get();
+    o.n_ortho = n_ortho;
+    o.ortho_ld = n;
+    int it = 0, na = 0;
+    *eval = qcm::jacobi_davidson(c, p, x.get(), tol, maxiter, it, precision, &o, &na);
+    QCM_CUDA(cudaMemcpyAsync(out, x.get(), n * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    if (iters) *iters = it;
+    if (applies) *applies = na;
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_boundary_step_left(qcm_ctx* ctx, const qcm_boundary* L, const qcm_mpo* mpo, int site, const qcm_mps_desc* mps,
                            const double* data_rp, int symmetric, qcm_boundary** out) {
     return boundary_step(ctx, L, mpo, site, mps, data_rp, symmetric, true, out);
@@ -202,6 +239,8 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     const qcm::MPO& m = qcm::mpo_of(mpo);
     if (m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: expected a single-site MPO");
     if (prm->jcd_maxiter < 1 || prm->jcd_maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: jcd_maxiter must be in 1..64");
+    if (prm->jcd_gmres < 0 || prm->jcd_gmres > qcm::JD_MAX_GMRES)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: jcd_gmres must be in 0..64");
     if (prm->twosite_truncation != 0 && prm->twosite_truncation != 1)
         return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: twosite_truncation must be 0 (svd) or 1 (heev)");
     if (prm->max_bond_dimension < 1 || prm->init_bond_dimension < 1)
@@ -214,6 +253,7 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     p.cutoff = prm->truncation_cutoff;
     p.jcd_tol = prm->jcd_tol;
     p.jcd_maxiter = prm->jcd_maxiter;
+    p.jcd_gmres = prm->jcd_gmres;
     p.ecore = prm->ecore;
     p.heev = prm->twosite_truncation == 1;
     p.alpha_initial = prm->alpha_initial;
@@ -240,6 +280,8 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     const qcm::MPO& m = qcm::mpo_of(mpo);
     if (m.twosite) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: expected a single-site MPO");
     if (prm->jcd_maxiter < 1 || prm->jcd_maxiter > 64) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: jcd_maxiter must be in 1..64");
+    if (prm->jcd_gmres < 0 || prm->jcd_gmres > qcm::JD_MAX_GMRES)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: jcd_gmres must be in 0..64");
     QCM_CUDA(cudaSetDevice(ctx->device));
     qcm::AllocStream scope(ctx->stream);
     qcm::DMRGParams p;
@@ -248,6 +290,7 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     p.cutoff = prm->truncation_cutoff;
     p.jcd_tol = prm->jcd_tol;
     p.jcd_maxiter = prm->jcd_maxiter;
+    p.jcd_gmres = prm->jcd_gmres;
     p.ecore = prm->ecore;
     p.heev = prm->twosite_truncation == 1;
     p.alpha_initial = prm->alpha_initial;

@@ -171,14 +171,30 @@ struct DTwoSite {
                                const MPOTensor& W, DMPS& m1, DMPS& m2);
 };
 
-// Jacobi-Davidson for the lowest eigenpair (ietl/jacobi.h:386-474 with gmres 0):
-// x (device, plan vector layout) holds the start vector and receives the eigenvector.
+// Jacobi-Davidson for the lowest eigenpair (solve_ietl_jcd, solver/ietl_jacobi_davidson.h:35-76;
+// ietl/jacobi.h:386-474): x (device, plan vector layout) holds the start vector and receives the
+// eigenvector.
 // mixed: every H.psi in the mixed form (heff_apply_device_mixed), stopping once the residual
 // is below max(tol, MIXED_RESIDUAL_FLOOR) |theta|, then one FP64 H.psi for the Rayleigh quotient
 // of the final vector (the returned eigenvalue).
 constexpr double MIXED_RESIDUAL_FLOOR = 1e-7;
-// precision: 0 FP64, 1 mixed, 2 mixed with the tensor-memory S build (QCM_PRECISION_*)
-double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters, int precision = 0);
+// Beyond the plain solve: the correction equation (I - uu*)(A - theta)(I - uu*) t = -r solved by
+// GMRES with `gmres` iterations from t0 = -r + (r.u)/(u.u) u (jcd_gmres_solver, ietl/jacobi.h:126-164;
+// ietl_gmres, ietl/gmres.h:78-146; 0 = t0 itself), and the search space kept orthogonal to n_ortho
+// vectors (excited states; DavidsonVS::project, solver/ietl_interface_dv.h:94-99), device pointers in
+// the plan vector layout, ortho_ld doubles apart, Gram-Schmidt'd among themselves first.
+struct JDOptions {
+    int gmres = 0;
+    const double* ortho = nullptr;
+    int n_ortho = 0;
+    uint64_t ortho_ld = 0;
+};
+constexpr int JD_MAX_GMRES = 64;
+// precision: 0 FP64, 1 mixed, 2 mixed with the tensor-memory S build (QCM_PRECISION_*).
+// *applies (may be null): the H_eff applies of the solve in its own form (the mixed form's FP64
+// Rayleigh quotient not included).
+double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters, int precision = 0,
+                       const JDOptions* opt = nullptr, int* applies = nullptr);
 
 // Boundary steps (contractions/boundary_ops/move_boundary.hpp:147-404): new left boundary
 // from L[site] and mps[site]; new right boundary from R[site+1] and mps[site].
@@ -211,6 +227,7 @@ struct DMRGParams {
     double cutoff = 1e-16;
     double jcd_tol = 1e-10;
     int jcd_maxiter = 8;
+    int jcd_gmres = 0;  // ietl_jcd_gmres
     double ecore = 0.0;
     // twosite_truncation = heev with its noise per sweep (ts_optimize.hpp:275-296)
     bool heev = false;

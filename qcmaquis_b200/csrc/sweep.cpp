@@ -1,9 +1,10 @@
 // Jacobi-Davidson eigensolver and the two-site DMRG sweep on the device.
 //
-// JD (ietl/jacobi.h:386-474, jcd_gmres_solver with max_iter 0 at :141-157): the
-// search space, its H images and every vector update live in HBM; only the
-// Rayleigh-Ritz matrix (<= maxiter^2 numbers), its eigenvector and three norms
-// per iteration cross to the host.  Dot products use a fixed-order reduction,
+// JD (ietl/jacobi.h:386-474, GMRES corrections ietl/gmres.h:78-146, ortho
+// vectors ietl_interface_dv.h:94-99): the search space, its H images, the
+// GMRES basis and every vector update live in HBM; only the Rayleigh-Ritz
+// matrix (<= maxiter^2 numbers), its eigenvector, the GMRES Hessenberg columns
+// and a few norms per iteration cross to the host.  Dot products use a fixed-order reduction,
 // so a solve is reproducible run to run.
 //
 // Sweep (optimize/ts_optimize.hpp:114-362): per step, two-site tensor -> H_eff
@@ -33,26 +34,143 @@ void download(Ctx& c, const double* d, double* h, std::size_t n) {
 }
 }  // namespace
 
-double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters, int precision) {
+namespace {
+// GeneratePlaneRotation / ApplyPlaneRotation (ietl/gmres.h:40-66)
+void gen_rot(double dx, double dy, double& cs, double& sn) {
+    if (dy == 0.0) { cs = 1; sn = 0; }
+    else if (std::fabs(dy) > std::fabs(dx)) { const double t = dx / dy; sn = 1.0 / std::sqrt(1.0 + t * t); cs = t * sn; }
+    else { const double t = dy / dx; cs = 1.0 / std::sqrt(1.0 + t * t); sn = t * cs; }
+}
+void apply_rot(double& dx, double& dy, double cs, double sn) {
+    const double r0 = cs * dx + sn * dy, r1 = -sn * dx + cs * dy;
+    dx = r0;
+    dy = r1;
+}
+}  // namespace
+
+double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters, int precision,
+                       const JDOptions* opt, int* applies) {
     const bool mixed = precision != 0;
     if (maxiter < 1 || maxiter > 64) throw std::runtime_error("jacobi_davidson: maxiter must be in 1..64");
+    const int gm = opt ? opt->gmres : 0;
+    if (gm < 0 || gm > JD_MAX_GMRES) throw std::runtime_error("jacobi_davidson: gmres must be in 0..64");
     const uint64_t n = p.x_len, ld = (n + 31) / 32 * 32;
-    // V[0..maxiter), VA[0..maxiter), u, r
-    Ctx::ensure(c.jd, (2 * uint64_t(maxiter) + 2) * ld);
+    // at most n - 1 ortho vectors (solver/ietl_jacobi_davidson.h:41-42)
+    int no = opt ? opt->n_ortho : 0;
+    if (no < 0) throw std::runtime_error("jacobi_davidson: negative ortho vector count");
+    if (uint64_t(no) >= n) no = n ? int(n - 1) : 0;
+    if (no > 0 && (!opt->ortho || opt->ortho_ld < n)) throw std::runtime_error("jacobi_davidson: bad ortho vectors");
+    // V[0..maxiter), VA[0..maxiter), u, r, the ortho vectors, the GMRES basis (gm + 1) and the
+    // correction operator's temporary
+    const uint64_t nvec = 2 * uint64_t(maxiter) + 2 + uint64_t(no) + (gm > 0 ? uint64_t(gm) + 2 : 0);
+    Ctx::ensure(c.jd, nvec * ld);
     Ctx::ensure(c.scal, 256 + 64 * uint64_t(DOT_PARTS));
     Ctx::ensure(c.coef, 64);
     double* V = c.jd.get();
     double* VA = V + uint64_t(maxiter) * ld;
     double* u = VA + uint64_t(maxiter) * ld;
     double* r = u + ld;
+    double* O = r + ld;
+    double* G = O + uint64_t(no) * ld;
+    double* tmp = G + uint64_t(gm + 1) * ld;
+    // scalar slots: 0-1 norms, 2.. MGS dots, 80.. Rayleigh-Ritz column, 160-164 residual / Rayleigh
+    // quotient, 170.. GMRES Hessenberg column and |w|^2, 241-242 operator dots, 243-246 projections
     double* sc = c.scal.get();
     double* dsc = sc + 256;  // dot-product partials
     auto Vi = [&](int i) { return V + uint64_t(i) * ld; };
     auto VAi = [&](int i) { return VA + uint64_t(i) * ld; };
+    auto Oi = [&](int i) { return O + uint64_t(i) * ld; };
+    auto Gi = [&](int i) { return G + uint64_t(i) * ld; };
+    int napply = 0;
+    auto apply = [&](const double* in, double* out) {
+        if (mixed) heff_apply_device_mixed(p, in, out, nullptr, precision == 2);
+        else heff_apply_device(p, in, out);
+        ++napply;
+    };
+    // ortho vectors: copies, Gram-Schmidt among themselves in order (ietl_jacobi_davidson.h:43-47)
+    std::vector<double> inv_oo(std::size_t(no > 0 ? no : 0));
+    for (int a = 0; a < no; ++a) {
+        QCM_CUDA(cudaMemcpyAsync(Oi(a), opt->ortho + uint64_t(a) * opt->ortho_ld, n * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, c.s));
+        for (int b = 0; b < a; ++b) {
+            dev_dots(Oi(b), 0, 1, Oi(a), n, sc + 243, dsc, c.s);
+            dev_axpy_dscalar(sc + 243, -inv_oo[b], Oi(b), Oi(a), n, c.s);
+        }
+        dev_dots(Oi(a), 0, 1, Oi(a), n, sc + 244, dsc, c.s);
+        double oo = 0.0;
+        download(c, sc + 244, &oo, 1);
+        if (!(oo > 0.0) || !std::isfinite(oo))
+            throw std::runtime_error("jacobi_davidson: ortho vector of zero norm after Gram-Schmidt");
+        inv_oo[a] = 1.0 / oo;
+    }
+    // t -= (o.t)/(o.o) o for each ortho vector in turn
+    auto project = [&](double* t) {
+        for (int a = 0; a < no; ++a) {
+            dev_dots(Oi(a), 0, 1, t, n, sc + 243, dsc, c.s);
+            dev_axpy_dscalar(sc + 243, -inv_oo[a], Oi(a), t, n, c.s);
+        }
+    };
     QCM_CUDA(cudaMemcpyAsync(Vi(0), x, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
+    project(Vi(0));
     std::vector<double> M(std::size_t(maxiter) * maxiter, 0.0), s;
     int it = 0;
     double theta = 0.0;
+    // (I - uu*)(A - theta)(I - uu*) x -> y (jcd_solver_operator, ietl/jacobi.h:249-268; u has unit norm)
+    auto op = [&](const double* xin, double* y) {
+        dev_dots(u, 0, 1, xin, n, sc + 241, dsc, c.s);
+        QCM_CUDA(cudaMemcpyAsync(tmp, xin, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
+        dev_axpy_dscalar(sc + 241, -1.0, u, tmp, n, c.s);
+        apply(tmp, y);
+        dev_axpby(-theta, tmp, 1.0, y, n, c.s);
+        dev_dots(u, 0, 1, y, n, sc + 242, dsc, c.s);
+        dev_axpy_dscalar(sc + 242, -1.0, u, y, n, c.s);
+    };
+    // ietl_gmres::operator() (ietl/gmres.h:92-146) for b = -r from xt (in: t0, out: the solution).
+    // A break at inner step i keeps the first i directions (Update(H, s, i)), as the reference does.
+    auto gmres = [&](double* xt, double abs_tol) {
+        const int m = gm;
+        std::vector<double> sv(std::size_t(m) + 1, 0.0), cs(std::size_t(m) + 1, 0.0), sn(std::size_t(m) + 1, 0.0);
+        std::vector<double> H(std::size_t(m + 1) * (m + 1), 0.0);
+        auto h = [&](int i, int j) -> double& { return H[std::size_t(i) + std::size_t(j) * (m + 1)]; };
+        op(xt, Gi(0));
+        dev_axpby(-1.0, r, -1.0, Gi(0), n, c.s);  // b - A x0
+        dev_dots(Gi(0), 0, 1, Gi(0), n, sc + 246, dsc, c.s);
+        double s0 = 0.0;
+        download(c, sc + 246, &s0, 1);
+        sv[0] = std::sqrt(s0);
+        if (std::fabs(sv[0]) < abs_tol) return;
+        dev_axpby(1.0 / sv[0], Gi(0), 0.0, Gi(0), n, c.s);
+        int i = 0;
+        std::vector<double> col(std::size_t(m) + 1);
+        for (; i + 1 < m; ++i) {
+            double* w = Gi(i + 1);
+            op(Gi(i), w);
+            for (int k = 0; k <= i; ++k) {
+                dev_dots(Gi(k), 0, 1, w, n, sc + 170 + k, dsc, c.s);
+                dev_axpy_dscalar(sc + 170 + k, -1.0, Gi(k), w, n, c.s);
+            }
+            dev_dots(w, 0, 1, w, n, sc + 170 + i + 1, dsc, c.s);
+            download(c, sc + 170, col.data(), std::size_t(i) + 2);
+            for (int k = 0; k <= i; ++k) h(k, i) = col[k];
+            h(i + 1, i) = std::sqrt(col[i + 1]);
+            // an exact breakdown leaves w = 0: the rotation below zeroes the residual and ends the loop
+            // before the direction would be used
+            if (h(i + 1, i) != 0.0) dev_axpby(1.0 / h(i + 1, i), w, 0.0, w, n, c.s);
+            for (int k = 0; k < i; ++k) apply_rot(h(k, i), h(k + 1, i), cs[k], sn[k]);
+            gen_rot(h(i, i), h(i + 1, i), cs[i], sn[i]);
+            apply_rot(h(i, i), h(i + 1, i), cs[i], sn[i]);
+            apply_rot(sv[i], sv[i + 1], cs[i], sn[i]);
+            if (std::fabs(sv[i + 1]) < abs_tol) break;
+        }
+        if (i == 0) return;
+        std::vector<double> y(sv.begin(), sv.begin() + i);
+        for (int a = i - 1; a >= 0; --a) {
+            y[a] /= h(a, a);
+            for (int b = a - 1; b >= 0; --b) y[b] -= h(b, a) * y[a];
+        }
+        QCM_CUDA(cudaMemcpyAsync(c.coef.get(), y.data(), y.size() * sizeof(double), cudaMemcpyHostToDevice, c.s));
+        dev_lincomb(G, ld, uint32_t(i), c.coef.get(), n, xt, true, c.s);
+    };
     while (true) {
         double* t = Vi(it);
         // modified Gram-Schmidt against V[0..it), repeated once if the norm dropped below 1/4
@@ -73,9 +191,14 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
             download(c, sc + 1, h2, 1);
             tn = std::sqrt(h2[0]);
         }
+        if (no > 0) {
+            project(t);
+            dev_dots(t, 0, 1, t, n, sc + 245, dsc, c.s);
+            download(c, sc + 245, h2, 1);
+            tn = std::sqrt(h2[0]);
+        }
         dev_axpby(1.0 / tn, t, 0.0, t, n, c.s);
-        if (mixed) heff_apply_device_mixed(p, t, VAi(it), nullptr, precision == 2);
-        else heff_apply_device(p, t, VAi(it));
+        apply(t, VAi(it));
         // column it of the projected matrix: <V_i, A V_it>
         dev_dots(V, ld, uint32_t(it + 1), VAi(it), n, sc + 80, dsc, c.s);
         std::vector<double> col(it + 1);
@@ -84,8 +207,9 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         sym_lowest_eigenpair(M.data(), maxiter, it + 1, theta, s);
         QCM_CUDA(cudaMemcpyAsync(c.coef.get(), s.data(), s.size() * sizeof(double), cudaMemcpyHostToDevice, c.s));
         dev_lincomb(V, ld, uint32_t(it + 1), c.coef.get(), n, u, false, c.s);
-        // r = A u - theta u
+        // r = A u - theta u, A u projected against the ortho vectors
         dev_lincomb(VA, ld, uint32_t(it + 1), c.coef.get(), n, r, false, c.s);
+        project(r);
         dev_axpby(-theta, u, 1.0, r, n, c.s);
         dev_dots(r, 0, 1, r, n, sc + 160, dsc, c.s);
         dev_dots(r, 0, 1, u, n, sc + 161, dsc, c.s);
@@ -110,11 +234,13 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
             }
             QCM_CUDA(cudaMemcpyAsync(x, u, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
             iters = it;
+            if (applies) *applies = napply;
             return theta;
         }
-        // correction t = -r + (r.u)/(u.u) u
+        // correction t0 = -r + (r.u)/(u.u) u, then GMRES on -r with abs_tol 2^-(it+1)
         dev_axpby(-1.0, r, 0.0, Vi(it), n, c.s);
         dev_axpby(h3[1] / h3[2], u, 1.0, Vi(it), n, c.s);
+        if (gm > 0) gmres(Vi(it), 1.0 / std::pow(2.0, double(it + 1)));
     }
 }
 
@@ -289,13 +415,16 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     QCM_CUDA(cudaStreamSynchronize(c.s));
     const double t1 = now_s();
     st.plan_s += t1 - t0;
-    int iters = 0;
-    const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters, p.precision);
+    int iters = 0, napply = 0;
+    JDOptions jo;
+    jo.gmres = p.jcd_gmres;
+    const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters, p.precision, &jo,
+                                     &napply);
     QCM_CUDA(cudaStreamSynchronize(c.s));
     const double t2 = now_s();
     st.jd_s += t2 - t1;
-    st.hpsi_count += uint64_t(iters);
-    st.hpsi_flops += double(iters) * plan->flops;
+    st.hpsi_count += uint64_t(napply);
+    st.hpsi_flops += double(napply) * plan->flops;
     if (p.precision != 0) {
         st.hpsi_count64 += 1;  // the FP64 Rayleigh-quotient apply
         st.hpsi_flops64 += plan->flops;

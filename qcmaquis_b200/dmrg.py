@@ -21,16 +21,17 @@ class DMRGParams(ctypes.Structure):
                 ("jcd_tol", c_double), ("jcd_maxiter", ctypes.c_int32), ("ecore", c_double),
                 ("twosite_truncation", ctypes.c_int32), ("alpha_initial", c_double), ("alpha_main", c_double),
                 ("alpha_final", c_double), ("ngrowsweeps", ctypes.c_int32), ("nmainsweeps", ctypes.c_int32),
-                ("hpsi_precision", ctypes.c_int32)]
+                ("hpsi_precision", ctypes.c_int32), ("jcd_gmres", ctypes.c_int32)]
 
 
-def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64"):
+def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmres=0):
     """heev: None (svd truncation) or dict(alpha_initial, alpha_main, alpha_final, ngrowsweeps, nmainsweeps);
-    precision: "fp64" or "mixed" (JD with the mixed H.psi and an FP64 Rayleigh quotient per step)."""
+    precision: "fp64" or "mixed" (JD with the mixed H.psi and an FP64 Rayleigh quotient per step);
+    gmres: ietl_jcd_gmres, GMRES iterations per JD correction."""
     h = heev or {}
     return DMRGParams(M, init_bd, cutoff, tol, maxiter, ecore, 1 if heev else 0, h.get("alpha_initial", 1e-2),
                       h.get("alpha_main", 1e-4), h.get("alpha_final", 1e-8), h.get("ngrowsweeps", 0),
-                      h.get("nmainsweeps", 0), precision_mode(precision))
+                      h.get("nmainsweeps", 0), precision_mode(precision), gmres)
 
 
 class TruncResult(ctypes.Structure):
@@ -46,6 +47,8 @@ class DMRGStats(ctypes.Structure):
 
 _lib._sig("qcm_jd_solve", c_int, c_void_p, P(c_double), c_double, c_int, P(c_double), P(c_double), P(c_int))
 _lib._sig("qcm_jd_solve_mode", c_int, c_void_p, P(c_double), c_double, c_int, c_int, P(c_double), P(c_double), P(c_int))
+_lib._sig("qcm_jd_solve_ex", c_int, c_void_p, P(c_double), P(P(c_double)), c_int, c_int, c_double, c_int, c_int,
+          P(c_double), P(c_double), P(c_int), P(c_int))
 _lib._sig("qcm_boundary_step_left", c_int, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), P(c_double), c_int,
           P(c_void_p))
 _lib._sig("qcm_boundary_step_right", c_int, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), P(c_double), c_int,
@@ -115,16 +118,27 @@ def truncate_heev(ctx, blocks, max_bond_dimension: int, cutoff: float = 1e-16):
     return out, {f: getattr(r, f) for f, _ in TruncResult._fields_}
 
 
-def jd_solve(plan, x0: np.ndarray, tol: float = 1e-10, maxiter: int = 8, precision="fp64"):
-    """Lowest eigenpair of a plan's H_eff from start vector x0: (eigenvalue, eigenvector, iterations).
-    precision "mixed": iterations with the mixed H.psi, eigenvalue = FP64 Rayleigh quotient."""
+def jd_solve(plan, x0: np.ndarray, tol: float = 1e-10, maxiter: int = 8, precision="fp64", ortho=(), gmres: int = 0,
+             return_applies: bool = False):
+    """Lowest eigenpair of a plan's H_eff from start vector x0: (eigenvalue, eigenvector, iterations[, applies]).
+    precision "mixed": iterations with the mixed H.psi, eigenvalue = FP64 Rayleigh quotient.
+    ortho: states the solution is kept orthogonal to (excited states); gmres: GMRES iterations per
+    correction equation (ietl_jcd_gmres)."""
     x0 = np.ascontiguousarray(x0, dtype=np.float64)
     assert x0.size == plan.n
     out = np.empty_like(x0)
-    ev, it = c_double(), c_int()
-    check(lib.qcm_jd_solve_mode(plan.h, _lib.dptr(x0), tol, maxiter, precision_mode(precision), _lib.dptr(out),
-                                ctypes.byref(ev), ctypes.byref(it)), "qcm_jd_solve_mode")
-    return ev.value, out, it.value
+    ev, it, na = c_double(), c_int(), c_int()
+    if len(ortho) == 0 and gmres == 0 and not return_applies:
+        check(lib.qcm_jd_solve_mode(plan.h, _lib.dptr(x0), tol, maxiter, precision_mode(precision), _lib.dptr(out),
+                                    ctypes.byref(ev), ctypes.byref(it)), "qcm_jd_solve_mode")
+        return ev.value, out, it.value
+    keep = [np.ascontiguousarray(o, dtype=np.float64) for o in ortho]
+    for o in keep:
+        assert o.size == plan.n
+    ptrs = (P(c_double) * max(1, len(keep)))(*[_lib.dptr(o) for o in keep])
+    check(lib.qcm_jd_solve_ex(plan.h, _lib.dptr(x0), ptrs, len(keep), gmres, tol, maxiter, precision_mode(precision),
+                              _lib.dptr(out), ctypes.byref(ev), ctypes.byref(it), ctypes.byref(na)), "qcm_jd_solve_ex")
+    return (ev.value, out, it.value, na.value) if return_applies else (ev.value, out, it.value)
 
 
 def boundary_step(ctx, B: Boundary, mpo, site: int, phys, left, right, data_rp: np.ndarray, side: str,
@@ -148,10 +162,10 @@ class DMRG:
 
     def __init__(self, ctx, mpo, nup: int, ndown: int, max_bond_dimension: int, init_bond_dimension: int | None = None,
                  truncation_cutoff: float = 1e-16, jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0,
-                 heev: dict | None = None, precision="fp64"):
+                 heev: dict | None = None, precision="fp64", jcd_gmres: int = 0):
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, init_bond_dimension or max_bond_dimension, truncation_cutoff, jcd_tol,
-                    jcd_maxiter, ecore, heev, precision)
+                    jcd_maxiter, ecore, heev, precision, jcd_gmres)
         h = c_void_p()
         check(lib.qcm_dmrg_create(ctx.h, mpo.handle, nup, ndown, ctypes.byref(p), ctypes.byref(h)), "qcm_dmrg_create")
         self.h = h
@@ -160,13 +174,13 @@ class DMRG:
     @classmethod
     def from_mps(cls, ctx, mpo, sites, max_bond_dimension: int, truncation_cutoff: float = 1e-16,
                  jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0, heev: dict | None = None,
-                 precision="fp64"):
+                 precision="fp64", jcd_gmres: int = 0):
         """Restart from a given MPS: sites = [dict(phys, left, right, blocks)] with right-paired blocks
         (one per left sector, in sector order), sites 1 .. L-1 right-normalised."""
         self = cls.__new__(cls)
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore, heev,
-                    precision)
+                    precision, jcd_gmres)
         descs = (MPSDesc * len(sites))()
         keep, ptrs = [], (P(c_double) * len(sites))()
         for i, st in enumerate(sites):
