@@ -57,6 +57,16 @@ int qcm_mpo_serialize(const qcm_mpo* m, void* buf, size_t cap, size_t* len);
 int qcm_mpo_deserialize(const void* buf, size_t len, qcm_mpo** out);
 void qcm_mpo_free(qcm_mpo* m);
 
+/* Entries of MPO tensor `site`, in the tensor's entry order (sorted by (b1, b2); an entry is one
+ * operator term: row b1, column b2, operator index op, scale), as MPOTensor stores them
+ * (mp_tensors/mpotensor.h; the scale is the coefficient the adjoint differentiates).  *n = entry
+ * count; with every array NULL only *n is set; otherwise cap must be >= *n. */
+int qcm_mpo_tensor_terms(const qcm_mpo* m, int site, uint32_t* b1, uint32_t* b2, uint32_t* op, double* scale, uint64_t cap,
+                         uint64_t* n);
+/* Replace the scales of MPO tensor `site` (n = its entry count, finite values).  Plans made from
+ * the MPO before the call keep their coefficients. */
+int qcm_mpo_set_scales(qcm_mpo* m, int site, const double* scale, uint64_t n);
+
 /* ------------------------------------------------------------------------ */
 /* Context, resident boundaries, H_eff plan                                   */
 /* ------------------------------------------------------------------------ */
@@ -195,6 +205,20 @@ void qcm_heff_free(qcm_heff* h);
  * race.  Enqueued on the context stream (asynchronous). */
 #define QCM_NOALLOC_SCRATCH_DOUBLES (8u * 1024u * 1024u)
 int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, double* y_dev);
+
+/* Adjoint of the H_eff apply (the differentiation form; no counterpart in the reference, which has
+ * no derivative of its schedule).  For f = ybar . H_eff x (host buffers of vec_len doubles):
+ *   psi_bar   = H_eff^T ybar, which is H_eff ybar: the two-site H_eff of a Hermitian MPO is symmetric;
+ *   coeff_bar[e] = df / d scale_e for every entry e of the plan's two-site MPO tensor, in the tensor's
+ *                  entry order (qcm_mpo_tensor_terms on the two-site MPO at the plan's site), with the
+ *                  boundaries held fixed; qcm_heff_adjoint_terms gives the count.
+ * f is linear in the scales: the schedule's coefficients alpha (site_hamil_tasks.hpp:41-137) are
+ * scale_e times a product of operator and conjugation factors, and S = sum alpha T (tasks.cpp:466-494).
+ * The gradient runs the apply's contractions transposed on the device: Sbar = L^T ybar, per S-build
+ * unit Wbar = Sbar T^T (FP64 tensor cores), then a fixed-order sum per entry (deterministic).
+ * psi_bar or coeff_bar may be NULL (x is read only for coeff_bar). */
+int qcm_heff_adjoint(qcm_heff* h, const double* x, const double* ybar, double* psi_bar, double* coeff_bar);
+int qcm_heff_adjoint_terms(const qcm_heff* h, uint64_t* n_terms);
 
 /* ------------------------------------------------------------------------ */
 /* Eigensolver, boundary propagation and the two-site sweep                   */

@@ -245,6 +245,40 @@ int orc_jd_solve(const void* snap, size_t n, const void* mpo_blob, size_t mn, in
     } catch (const std::exception& e) { return fail(e.what()); }
 }
 
+// Adjoint of H_eff x on a frozen site problem (the differentiation form): psi_bar = H ybar (H_eff is
+// symmetric) and grad[e] = d (ybar . H x) / d scale_e for the n_terms entries of the site's two-site
+// MPO tensor, in the tensor's entry order.
+int orc_heff_adjoint(const void* snap, size_t n, const void* mpo_blob, size_t mn, int site1, const double* x,
+                     const double* ybar, size_t len, double* psi_bar, double* grad, size_t n_terms) {
+    try {
+        bool ts = false;
+        auto mpo = load_mpo_blob(static_cast<const uint8_t*>(mpo_blob), mn, ts);
+        MPOTensor W = ts ? mpo[site1] : make_twosite_mpo(mpo[site1], mpo[site1 + 1]);
+        if (n_terms != W.scale.size()) return fail("orc_heff_adjoint: term count mismatch");
+        MPSTensor twin;
+        Boundary Lb, Rb;
+        load_site_problem(static_cast<const uint8_t*>(snap), n, twin, Lb, Rb);
+        auto sched = create_contraction_schedule(twin, Lb, Rb, W);
+        std::vector<const double*> xv(twin.left.size(), nullptr), yb(twin.left.size(), nullptr);
+        std::vector<double*> pv(twin.left.size(), nullptr);
+        std::size_t off = 0;
+        for (std::size_t k = 0; k < twin.data.n_blocks(); ++k) {
+            std::size_t lb = twin.left.position(twin.data.lc[k]);
+            xv[lb] = x + off;
+            yb[lb] = ybar + off;
+            pv[lb] = psi_bar + off;
+            off += twin.data.b[k].d.size();
+        }
+        if (off != len) return fail("orc_heff_adjoint: vector length mismatch");
+        std::fill(psi_bar, psi_bar + len, 0.0);
+        super_hamil_mv(*sched, Lb, Rb, yb, pv);
+        std::vector<double> g;
+        scale_gradient(*sched, Lb, Rb, xv, yb, n_terms, g);
+        std::copy(g.begin(), g.end(), grad);
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
 // Flat export of the schedule (bookkeeping parity).  Layout ("QSCH" v1):
 // u32 nblocks; per block: u32 ntj, ntj x (u32 mps_offset, ci, ci_eff, lb_ket);
 //   u32 ncoh; per cohort: u32 lb, rb, ls, rs, ci, ci_eff, nSrows, stripe, nunits;

@@ -224,13 +224,19 @@ std::size_t MPSBlock::n_flops(const BoundaryIndex& right) const {
 namespace {
 
 // create_schedule/op_iterate.hpp:38-70 (abelian: all four couplings equal the scale)
+// term / dcoupling (H_eff schedules): the MPO entry of the alphas and their coupling without the
+// entry's scale, recorded for the scale gradient
 void op_iterate(const SiteOp& W, std::size_t w_block, double coupling, Cohort& cg, unsigned s, unsigned m2_size,
-                const TiLookup& tl, unsigned mps_offset, unsigned ci, unsigned boundary_col) {
+                const TiLookup& tl, unsigned mps_offset, unsigned ci, unsigned boundary_col,
+                unsigned term = std::numeric_limits<unsigned>::max(), double dcoupling = 0.0) {
     const OpBlock& blk = W.blocks[w_block];
     for (std::size_t e = 0; e < blk.coeff.size(); ++e) {
         double scale = blk.coeff[e] * coupling;
         unsigned ti = tl.get(mps_offset + blk.ss1[e] * m2_size, ci);
-        if (ti < std::numeric_limits<unsigned>::max()) cg.push_back(s, blk.ss2[e], scale, ti, boundary_col);
+        if (ti < std::numeric_limits<unsigned>::max()) {
+            cg.push_back(s, blk.ss2[e], scale, ti, boundary_col);
+            if (term != std::numeric_limits<unsigned>::max()) cg.push_term(s, blk.ss2[e], term, blk.coeff[e] * dcoupling);
+        }
     }
 }
 
@@ -300,7 +306,9 @@ void shtm_tasks(const MPOTensor& mpo, const BoundaryIndex& left, const BoundaryI
                             unsigned in_offset = unsigned(right_pb(phys_in, rc_in));
                             long right_offset = right.offset(ci_right, b2);
                             double scale = right.conjugate_scale(ci_right, b2) * mpo.scale[e] * left.conjugate_scale(ci, b1);
-                            op_iterate(W, wb, scale, cohort, s, rs_in, tl, in_offset, ci_right, unsigned(right_offset / rs_in));
+                            double dscale = right.conjugate_scale(ci_right, b2) * left.conjugate_scale(ci, b1);
+                            op_iterate(W, wb, scale, cohort, s, rs_in, tl, in_offset, ci_right, unsigned(right_offset / rs_in),
+                                       e, dscale);
                         }
                     }
                 }
@@ -512,6 +520,59 @@ void super_hamil_mv(const Schedule& sched, const Boundary& left, const Boundary&
             const std::vector<double>& buf = part[bc.first][bc.second];
             daxpy(buf.size(), 1.0, buf.data(), y[o]);
         }
+}
+
+void scale_gradient(const Schedule& sched, const Boundary& left, const Boundary& right, const std::vector<const double*>& x,
+                    const std::vector<const double*>& ybar, std::size_t n_terms, std::vector<double>& grad) {
+    std::vector<const double*> lv = boundary_view(left), rv = boundary_view(right);
+    const std::size_t nb = sched.blocks.size();
+    std::vector<std::vector<double>> part(nb);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int b = 0; b < int(nb); ++b) {
+        const MPSBlock& blk = sched.blocks[b];
+        if (blk.data.empty()) continue;
+        part[b].assign(n_terms, 0.0);
+        TList T = blk.create_T(rv, x);
+        for (const Cohort& c : blk.data) {
+            if (!ybar[c.rb]) continue;
+            // Sbar (K x stripe) = L_eff^T ybar[lb_out], L_eff (ls_out x K) as contract uses it
+            const int M = int(c.rs), N = int(c.stripe), K = int(c.nSrows * c.ls);
+            const double* luse = lv[c.ci_eff];
+            std::vector<double> lbuf;
+            if (c.ci != c.ci_eff) {
+                lbuf.resize(std::size_t(M) * K);
+                tr_tile_v(c.ls, c.rs, c.nSrows, lv[c.ci_eff], lbuf.data());
+                luse = lbuf.data();
+            }
+            std::vector<double> sbar(std::size_t(K) * N);
+            dgemm('T', 'N', K, N, M, 1.0, luse, M, ybar[c.rb], M, 0.0, sbar.data(), K);
+            // create_s_r's element map: S[K (offset + col) + bb ls + i] += alpha T[ti][(tidx1 + col) ls + i]
+            for (const SUnit& u : c.suv) {
+                if (u.alpha.empty()) continue;
+                if (u.term.size() != u.alpha.size()) throw std::runtime_error("scale_gradient: schedule without term records");
+                unsigned seeker = 0;
+                for (std::size_t l = 0; l < u.b2s.size(); ++l) {
+                    const std::size_t bb = u.b1[l];
+                    for (unsigned ia = seeker; ia < seeker + u.b2s[l]; ++ia) {
+                        const std::vector<double>& Tt = T[u.tidx[2 * ia]];
+                        const std::size_t t1 = u.tidx[2 * ia + 1];
+                        double abar = 0.0;
+                        for (unsigned col = 0; col < u.ms; ++col) {
+                            const double* sp = sbar.data() + std::size_t(K) * (u.offset + col) + bb * c.ls;
+                            const double* tp = Tt.data() + (t1 + col) * c.ls;
+                            for (unsigned i = 0; i < c.ls; ++i) abar += sp[i] * tp[i];
+                        }
+                        part[b][u.term[ia]] += abar * u.dalpha[ia];
+                    }
+                    seeker += u.b2s[l];
+                }
+            }
+        }
+    }
+    grad.assign(n_terms, 0.0);
+    for (std::size_t b = 0; b < nb; ++b)
+        if (!part[b].empty())
+            for (std::size_t e = 0; e < n_terms; ++e) grad[e] += part[b][e];
 }
 
 Boundary overlap_mpo_left_step(const MPSTensor& bra_in, const MPSTensor& ket_in, const Boundary& left, const MPOTensor& mpo,

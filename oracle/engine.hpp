@@ -17,6 +17,9 @@ struct SUnit {
     std::vector<double> alpha;
     std::vector<unsigned> b2s, b1;
     unsigned b2count = 0;
+    // H_eff schedules only: per alpha, its MPO entry and d alpha / d (entry scale)
+    std::vector<unsigned> term;
+    std::vector<double> dalpha;
     void push_back(double s, unsigned ti, unsigned col) { alpha.push_back(s); b2count++; tidx.push_back(ti); tidx.push_back(col); }
     unsigned add_line(unsigned b) {
         unsigned ret = b2count;
@@ -38,6 +41,10 @@ struct Cohort {
     Cohort(const std::vector<std::size_t>& phys_i, unsigned l_block, unsigned r_block, unsigned l_size, unsigned r_size,
            unsigned ci_, unsigned ci_eff_, unsigned mpodim, bool left = false);
     void push_back(unsigned s, unsigned ss2, double scale, unsigned ti, unsigned col) { suv[sfold[s] + ss2].push_back(scale, ti, col); }
+    void push_term(unsigned s, unsigned ss2, unsigned e, double d) {
+        suv[sfold[s] + ss2].term.push_back(e);
+        suv[sfold[s] + ss2].dalpha.push_back(d);
+    }
     void add_line(unsigned b1) { for (auto& su : suv) mpo_offsets[b1] += su.add_line(b1); }
     void add_unit(unsigned s, unsigned ss, unsigned m_size, unsigned offset) {
         for (unsigned i = 0; i < ss; ++i) { suv[sfold[s] + i].offset = i * m_size + offset; suv[sfold[s] + i].ms = m_size; stripe += m_size; }
@@ -90,6 +97,10 @@ std::unique_ptr<Schedule> create_contraction_schedule(MPSTensor& initial, const 
 // super_hamil_mv (solver/super_hamil_mv.hpp:100-155), CPU branch; x, y = right-paired block data
 void super_hamil_mv(const Schedule& sched, const Boundary& left, const Boundary& right,
                     const std::vector<const double*>& x, const std::vector<double*>& y);
+// Adjoint of super_hamil_mv with respect to the scales of the MPO entries (the differentiation form):
+// grad[e] = d (ybar . H x) / d scale_e for every entry e of the schedule's MPO tensor (n_terms entries)
+void scale_gradient(const Schedule& sched, const Boundary& left, const Boundary& right, const std::vector<const double*>& x,
+                    const std::vector<const double*>& ybar, std::size_t n_terms, std::vector<double>& grad);
 
 // boundary steps (contractions/boundary_ops/move_boundary.hpp:147-404)
 Boundary overlap_mpo_left_step(const MPSTensor& bra, const MPSTensor& ket, const Boundary& left, const MPOTensor& mpo,

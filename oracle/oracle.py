@@ -61,6 +61,8 @@ def lib(nthreads: int = 0):
         L.orc_jd_solve.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), c_size_t, P(c_double), c_int,
                                    c_int, c_double, c_int, P(c_double), P(c_double), P(c_int), P(c_int)]
         L.orc_dmrg_set_gmres.argtypes = [c_void_p, c_int]
+        L.orc_heff_adjoint.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), P(c_double), c_size_t,
+                                       P(c_double), P(c_double), c_size_t]
         U32 = P(ctypes.c_uint32)
         L.orc_truncate_svd.argtypes = [ctypes.c_uint32, U32, U32, P(c_double), ctypes.c_uint64, c_double, U32, P(c_double),
                                        P(c_double), P(c_double), P(c_double)]
@@ -180,6 +182,20 @@ def jd_solve(snap: bytes, mpo_blob: bytes, site1: int, x0: np.ndarray, tol: floa
                              len(ortho), gmres, tol, maxiter, _dp(out), ctypes.byref(ev), ctypes.byref(it),
                              ctypes.byref(na)))
     return ev.value, out, it.value, na.value
+
+
+def heff_adjoint(snap: bytes, mpo_blob: bytes, site1: int, x: np.ndarray, ybar: np.ndarray, n_terms: int):
+    """Oracle adjoint of H_eff x: (psi_bar = H ybar, d(ybar . H x)/d scale per two-site MPO entry)."""
+    L = lib()
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    ybar = np.ascontiguousarray(ybar, dtype=np.float64)
+    pb = np.zeros_like(x)
+    g = np.zeros(n_terms)
+    sb = ctypes.create_string_buffer(snap, len(snap))
+    mb = ctypes.create_string_buffer(mpo_blob, len(mpo_blob))
+    _check(L, L.orc_heff_adjoint(sb, len(snap), mb, len(mpo_blob), site1, _dp(x), _dp(ybar), x.size, _dp(pb), _dp(g),
+                                 n_terms))
+    return pb, g
 
 
 def schedule_export(snap: bytes, mpo_blob: bytes, site1: int):

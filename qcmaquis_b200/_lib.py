@@ -48,6 +48,9 @@ _sig("qcm_mpo_length", c_int, c_void_p)
 _sig("qcm_mpo_serialize", c_int, c_void_p, c_void_p, c_size_t, P(c_size_t))
 _sig("qcm_mpo_deserialize", c_int, c_void_p, c_size_t, P(c_void_p))
 _sig("qcm_mpo_free", None, c_void_p)
+_sig("qcm_mpo_tensor_terms", c_int, c_void_p, c_int, P(ctypes.c_uint32), P(ctypes.c_uint32), P(ctypes.c_uint32),
+     P(c_double), ctypes.c_uint64, P(ctypes.c_uint64))
+_sig("qcm_mpo_set_scales", c_int, c_void_p, c_int, P(c_double), ctypes.c_uint64)
 
 
 def dptr(a):

@@ -269,6 +269,32 @@ int qcm_heff_apply_mode(qcm_heff* h, const double* x, double* y, int precision) 
     QCM_CATCH
 }
 
+int qcm_heff_adjoint_terms(const qcm_heff* h, uint64_t* n_terms) {
+    if (!h || !h->p || !n_terms) return qcm::fail(QCM_ERR_ARG, "qcm_heff_adjoint_terms: NULL argument");
+    *n_terms = qcm::heff_adjoint_terms(*h->p);
+    return QCM_OK;
+}
+
+int qcm_heff_adjoint(qcm_heff* h, const double* x, const double* ybar, double* psi_bar, double* coeff_bar) {
+    QCM_TRY
+    if (!h || !ybar || (coeff_bar && !x)) return qcm::fail(QCM_ERR_ARG, "qcm_heff_adjoint: NULL argument");
+    if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_heff_adjoint: host-only plan");
+    qcm::HeffPlan& p = *h->p;
+    qcm::AllocStream scope(p.stream);
+    const uint64_t n = p.x_len, nt = qcm::heff_adjoint_terms(p);
+    qcm::DBuf<double> dv(2 * n + 1), dpb(psi_bar ? n + 1 : 0), dcb(coeff_bar ? nt + 1 : 0);
+    double* dx = dv.get();
+    double* dyb = dv.get() + n;
+    if (coeff_bar) QCM_CUDA(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, p.stream));
+    QCM_CUDA(cudaMemcpyAsync(dyb, ybar, n * sizeof(double), cudaMemcpyHostToDevice, p.stream));
+    qcm::heff_adjoint_device(p, dx, dyb, psi_bar ? dpb.get() : nullptr, coeff_bar ? dcb.get() : nullptr);
+    if (psi_bar) QCM_CUDA(cudaMemcpyAsync(psi_bar, dpb.get(), n * sizeof(double), cudaMemcpyDeviceToHost, p.stream));
+    if (coeff_bar && nt) QCM_CUDA(cudaMemcpyAsync(coeff_bar, dcb.get(), nt * sizeof(double), cudaMemcpyDeviceToHost, p.stream));
+    QCM_CUDA(cudaStreamSynchronize(p.stream));
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_heff_profile_mode(qcm_heff* h, const double* x_dev, double* y_dev, float* ms, int precision) {
     QCM_TRY
     if (!h || !h->ctx || !x_dev || !y_dev || !ms) return qcm::fail(QCM_ERR_ARG, "qcm_heff_profile_mode: bad argument");

@@ -1,4 +1,6 @@
 // C-ABI: MPO construction (input prep for the two-site H_eff path).
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <exception>
 #include <string>
@@ -55,6 +57,40 @@ int qcm_mpo_deserialize(const void* buf, size_t len, qcm_mpo** out) {
     auto* p = new qcm_mpo;
     p->m = qcm::deserialize_mpo(static_cast<const uint8_t*>(buf), len);
     *out = p;
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_mpo_tensor_terms(const qcm_mpo* m, int site, uint32_t* b1, uint32_t* b2, uint32_t* op, double* scale, uint64_t cap,
+                         uint64_t* n) {
+    QCM_TRY
+    if (!m || !n) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_tensor_terms: bad arguments");
+    if (site < 0 || std::size_t(site) >= m->m.t.size()) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_tensor_terms: site out of range");
+    const qcm::MPOTensor& t = m->m.t[std::size_t(site)];
+    const std::size_t ne = t.scale.size();
+    *n = ne;
+    if (!b1 && !b2 && !op && !scale) return QCM_OK;
+    if (cap < ne) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_tensor_terms: buffers too small");
+    for (std::size_t e = 0; e < ne; ++e) {
+        if (b1) b1[e] = t.b1[e];
+        if (b2) b2[e] = t.b2[e];
+        if (op) op[e] = t.op[e];
+        if (scale) scale[e] = t.scale[e];
+    }
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_mpo_set_scales(qcm_mpo* m, int site, const double* scale, uint64_t n) {
+    QCM_TRY
+    if (!m || !scale) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_set_scales: bad arguments");
+    if (site < 0 || std::size_t(site) >= m->m.t.size()) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_set_scales: site out of range");
+    qcm::MPOTensor& t = m->m.t[std::size_t(site)];
+    if (n != t.scale.size()) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_set_scales: entry count mismatch");
+    for (uint64_t e = 0; e < n; ++e)
+        if (!std::isfinite(scale[e])) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_set_scales: non-finite scale");
+    std::copy(scale, scale + n, t.scale.begin());
+    t.finalize();  // drops the derived tables; plans built before keep theirs
     return QCM_OK;
     QCM_CATCH
 }

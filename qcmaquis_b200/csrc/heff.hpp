@@ -192,6 +192,8 @@ struct CoefGen {
     void generate(double* W, cudaStream_t s);
 };
 
+struct HeffAdjointWork;  // work lists and buffers of the adjoint, made on its first call
+
 struct HeffPlan {
     Index phys, left, right;
     std::vector<uint64_t> x_off;  // block offset per left sector (right-paired blocks, ls x stripe)
@@ -251,6 +253,8 @@ struct HeffPlan {
     DBuf<uint32_t> d_merr;
     DBuf<double> d_x, d_y;  // staging for host-buffer applies
 
+    std::shared_ptr<HeffAdjointWork> adj;
+
     const DevBoundary* L = nullptr;
     const DevBoundary* R = nullptr;
     cudaStream_t stream = nullptr;
@@ -268,6 +272,14 @@ void upload_plan(HeffPlan& p);
 // ev (optional, 4 events) is recorded before the T-GEMM, after it, after the S
 // gather and after the L.S GEMM.
 void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev = nullptr);
+// The apply's T-GEMM alone: T (t_len doubles, the plan's slice layout) from x, FP64.
+void heff_tgemm_device(HeffPlan& p, const double* x, double* T);
+// Adjoint of the apply (the differentiation form) for f = ybar . H_eff x, device pointers on
+// p.stream: psi_bar = H_eff ybar (H_eff is symmetric for a Hermitian MPO) and coeff_bar[e] =
+// df / d scale_e for the heff_adjoint_terms(p) entries of the plan's two-site MPO tensor, in the
+// tensor's entry order; either output may be null.  Uses the plan's T and S buffers.
+void heff_adjoint_device(HeffPlan& p, const double* x, const double* ybar, double* psi_bar, double* coeff_bar);
+uint64_t heff_adjoint_terms(const HeffPlan& p);
 int heff_launches_per_apply(const HeffPlan& p);
 // Mixed-precision H.psi (same layout and stream as heff_apply_device): the S build in 3xTF32 on
 // the tensor cores from FP32 operands, T-GEMM and L.S in FP64.  The first call makes the FP32

@@ -513,6 +513,13 @@ void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev)
     apply_impl(p, x, y, ev, p.d_T.get(), p.d_S.get(), p.d_P.get());
 }
 
+void heff_tgemm_device(HeffPlan& p, const double* x, double* T) {
+    launch_t<Sh16>(p, SHAPE_16, x, T, p.stream);
+    launch_t<Sh32>(p, SHAPE_32, x, T, p.stream);
+    launch_t<Sh64>(p, SHAPE_64, x, T, p.stream);
+    QCM_CUDA(cudaGetLastError());
+}
+
 void prepare_mixed(HeffPlan& p, bool tc) {
     AllocStream scope(p.stream);
     if (!p.d_merr.size()) {

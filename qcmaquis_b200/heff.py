@@ -68,6 +68,8 @@ _lib._sig("qcm_boundary_download", c_int, c_void_p, P(Sector), P(Sector), P(c_ui
 _lib._sig("qcm_heff_plan_create", c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), c_int, P(c_void_p))
 _lib._sig("qcm_heff_get_info", c_int, c_void_p, P(HeffInfo))
 _lib._sig("qcm_heff_apply", c_int, c_void_p, P(c_double), P(c_double))
+_lib._sig("qcm_heff_adjoint", c_int, c_void_p, P(c_double), P(c_double), P(c_double), P(c_double))
+_lib._sig("qcm_heff_adjoint_terms", c_int, c_void_p, P(c_uint64))
 _lib._sig("qcm_heff_apply_device", c_int, c_void_p, c_void_p, c_void_p)
 _lib._sig("qcm_heff_bookkeeping", c_int, c_void_p, P(c_uint32), P(c_double), c_uint64, P(c_uint64))
 _lib._sig("qcm_heff_profile", c_int, c_void_p, c_void_p, c_void_p, P(ctypes.c_float))
@@ -342,6 +344,20 @@ class HeffPlan:
         else:
             check(lib.qcm_heff_apply_mode(self.h, _lib.dptr(x), _lib.dptr(y), mode), "qcm_heff_apply_mode")
         return y
+
+    def adjoint(self, x: np.ndarray, ybar: np.ndarray):
+        """Adjoint of the apply for f = ybar . H_eff x: (psi_bar = H_eff^T ybar, coeff_bar = df/d scale per
+        entry of the plan's two-site MPO tensor, in entry order)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        ybar = np.ascontiguousarray(ybar, dtype=np.float64)
+        assert x.size == self.n and ybar.size == self.n
+        nt = c_uint64()
+        check(lib.qcm_heff_adjoint_terms(self.h, ctypes.byref(nt)), "qcm_heff_adjoint_terms")
+        pb = np.empty_like(x)
+        cb = np.empty(nt.value)
+        check(lib.qcm_heff_adjoint(self.h, _lib.dptr(x), _lib.dptr(ybar), _lib.dptr(pb), _lib.dptr(cb)),
+              "qcm_heff_adjoint")
+        return pb, cb
 
     def apply_device(self, x_ptr: int, y_ptr: int, precision="fp64"):
         mode = precision_mode(precision)

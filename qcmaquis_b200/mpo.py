@@ -55,6 +55,24 @@ class MPO:
     def tensors(self):
         return parse_blob(self.blob())
 
+    def copy(self) -> "MPO":
+        return MPO.from_blob(self.blob())
+
+    def terms(self, site: int):
+        """Entries of tensor `site` in entry order: dict of b1, b2, op (uint32) and scale (float64)."""
+        n = ctypes.c_uint64()
+        check(lib.qcm_mpo_tensor_terms(self._h, site, None, None, None, None, 0, ctypes.byref(n)), "qcm_mpo_tensor_terms")
+        out = {k: np.zeros(n.value, dtype=np.uint32) for k in ("b1", "b2", "op")}
+        out["scale"] = np.zeros(n.value)
+        u32 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        check(lib.qcm_mpo_tensor_terms(self._h, site, u32(out["b1"]), u32(out["b2"]), u32(out["op"]),
+                                       _lib.dptr(out["scale"]), n.value, ctypes.byref(n)), "qcm_mpo_tensor_terms")
+        return out
+
+    def set_scales(self, site: int, scale: np.ndarray):
+        scale = np.ascontiguousarray(scale, dtype=np.float64)
+        check(lib.qcm_mpo_set_scales(self._h, site, _lib.dptr(scale), scale.size), "qcm_mpo_set_scales")
+
     def __del__(self):
         if getattr(self, "_h", None) and self._h.value:
             lib.qcm_mpo_free(self._h)
