@@ -241,6 +241,28 @@ def measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, 
     return out
 
 
+def measure_adjoint(a, plan, x_host, blob, site):
+    """The differentiation form on the same frozen problem: qcm_heff_adjoint with host buffers (x and
+    ybar in, psi_bar and the gradient per two-site MPO entry out), wall time per call."""
+    rng = np.random.default_rng(a.seed)
+    ybar = rng.standard_normal(x_host.size)
+    pb, g = plan.adjoint(x_host, ybar)  # first call: work lists and buffers
+    reps = 3
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        pb, g = plan.adjoint(x_host, ybar)
+    dt = (time.perf_counter() - t0) / reps
+    # f = ybar . H x is linear in the scales: the gradient contracted with the scales gives f back
+    from qcmaquis_b200.mpo import MPO
+    terms = MPO.from_blob(blob).twosite().terms(site)["scale"]  # same builder: the plan's entry order
+    f = float(ybar @ plan.apply(x_host))
+    return {"ms_per_call": dt * 1e3, "n_terms": int(g.size), "h2d_bytes": 16 * x_host.size,
+            "d2h_bytes": 8 * (x_host.size + g.size),
+            "euler_check_rel": abs(float(g @ terms) - f) / abs(f),
+            "note": "psi_bar = H ybar and d(ybar.Hx)/d scale per entry; sum_e scale_e * grad_e = ybar.Hx (f is linear "
+                    "in the scales) is the consistency check"}
+
+
 def mixed_sweeps(a, ctx, blob, sinfo):
     """The same sweeps with every JD in the mixed form (FP64 Rayleigh quotient per step): times and
     the per-sweep energy deviation from the FP64 device sweeps."""
@@ -356,6 +378,7 @@ def run_b200(a, world, rank, local, pg):
     mixed = measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob, site, x_host)
     mixed["tensor_memory_form"] = measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob,
                                                 site, x_host, form="mixed_tc")
+    adjoint = measure_adjoint(a, plan, x_host, blob, site)
     if not a.no_mixed_sweep:
         mixed["sweep"] = mixed_sweeps(a, ctx, blob, sinfo)
     cpu = None
@@ -373,7 +396,7 @@ def run_b200(a, world, rank, local, pg):
                 "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
                 "gpu_launches": int(info["launches"]) * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
                 "fp64_peaks_tflops": {"dmma": dmma_peak, "dfma": dfma_peak},
-                "max_rel_err_vs_oracle": rel, "mixed": mixed}
+                "max_rel_err_vs_oracle": rel, "mixed": mixed, "adjoint": adjoint}
         print(json.dumps(line), flush=True)
     del plan, d
     if pg is not None:

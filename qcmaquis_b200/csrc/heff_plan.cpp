@@ -88,10 +88,34 @@ struct U {
     std::vector<double> bk_a;
 };
 
+// Orders a unit's slots by the set of 16-line groups that use them (sig: nw words per slot; first-use
+// order among equal sets): slots used by the same line tiles then share the S-GEMM's 4-slot k-groups, so
+// fewer groups per line tile are occupied and each holds more coefficients.  slices is permuted;
+// rank[old slot] = new slot.
+void cluster_slots(std::vector<uint32_t>& slices, uint32_t nl, const std::vector<uint64_t>& sig,
+                   std::vector<uint32_t>& order, std::vector<uint32_t>& rank, std::vector<uint32_t>& tmp) {
+    const uint32_t nk = uint32_t(slices.size()), nw = (nl + 1023) / 1024;
+    rank.resize(nk);
+    for (uint32_t i = 0; i < nk; ++i) rank[i] = i;
+    if (nk < 2 || !nw) return;
+    order.resize(nk);
+    for (uint32_t i = 0; i < nk; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+        for (uint32_t w = nw; w-- > 0;) {
+            const uint64_t x = sig[std::size_t(a) * nw + w], y = sig[std::size_t(b) * nw + w];
+            if (x != y) return x < y;
+        }
+        return false;
+    });
+    for (uint32_t i = 0; i < nk; ++i) rank[order[i]] = i;
+    tmp.assign(slices.begin(), slices.end());
+    for (uint32_t i = 0; i < nk; ++i) slices[i] = tmp[order[i]];
+}
+
 }  // namespace
 
 void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t n, std::vector<TileD>* utiles,
-                    std::vector<uint16_t>& klist) {
+                    std::vector<uint16_t>& klist, const uint32_t* slot_rank) {
     if (!u.nl || !u.ne || !u.nk || !n) return;
     constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK), four DMMA k-groups of 4 slices
     const uint32_t nks = (u.nk + KS - 1) / KS;
@@ -100,8 +124,14 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t 
     // block; coarser line tiles OR rows together
     const uint32_t n16 = (u.nl + 15) / 16;
     std::vector<uint8_t> occ16(std::size_t(n16) * nks, 0);
-    for (std::size_t i = 0; i < n; ++i)
-        occ16[std::size_t(ents[i].line / 16) * nks + ents[i].k / KS] |= uint8_t(1u << ((ents[i].k % KS) / 4));
+    if (slot_rank)
+        for (std::size_t i = 0; i < n; ++i) {
+            const uint32_t k = slot_rank[ents[i].k];
+            occ16[std::size_t(ents[i].line / 16) * nks + k / KS] |= uint8_t(1u << ((k % KS) / 4));
+        }
+    else
+        for (std::size_t i = 0; i < n; ++i)
+            occ16[std::size_t(ents[i].line / 16) * nks + ents[i].k / KS] |= uint8_t(1u << ((ents[i].k % KS) / 4));
     auto occ_at = [&](uint32_t bm, std::vector<uint8_t>& occ) {
         const uint32_t f = bm / 16, nmt = (u.nl + bm - 1) / bm;
         occ.assign(std::size_t(nmt) * nks, 0);
@@ -318,6 +348,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     std::vector<U> units;
     std::vector<uint32_t> slices;
     std::vector<double> lscale;
+    std::vector<uint64_t> csig;
+    std::vector<uint32_t> corder, crank, ctmp;
 #pragma omp for schedule(dynamic, 1)
     for (int lbi = 0; lbi < int(nl); ++lbi) try {
         const uint32_t lb_in = uint32_t(lbi);
@@ -430,14 +462,25 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 U& u = units[ui];
                 P.flops_s += 2.0 * ls_in * u.ms * double(u.em.size());
                 if (u.em.empty()) continue;
-                // number the unit's slices in first-use order
+                // number the unit's slices in first-use order, with the 16-line groups using each
                 slices.clear();
+                const uint32_t nw16 = (uint32_t(u.lines.size()) + 1023) / 1024;  // 64-bit words of 16-line groups
+                csig.clear();
                 for (LKD& m : u.em) {
                     uint32_t& sl = slot[m.k];
-                    if (sl == NONE) { sl = uint32_t(slices.size()); slices.push_back(m.k); }
+                    if (sl == NONE) {
+                        sl = uint32_t(slices.size());
+                        slices.push_back(m.k);
+                        csig.resize(csig.size() + nw16, 0);
+                    }
                     m.k = sl;
+                    const uint32_t g = m.line >> 4;
+                    csig[std::size_t(sl) * nw16 + (g >> 6)] |= 1ull << (g & 63);
                 }
                 for (uint32_t gp : slices) slot[gp] = NONE;
+                cluster_slots(slices, uint32_t(u.lines.size()), csig, corder, crank, ctmp);
+                if (bookkeeping)
+                    for (LKD& m : u.em) m.k = crank[m.k];
                 UnitD ud{};
                 ud.s_off = s_off + uint64_t(u.offset) * K_c;
                 ud.line_stride = ls_in; ud.erows = ls_in; ud.col_stride = K_c; ud.ne = ls_in * u.ms;
@@ -466,7 +509,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
                 // S-GEMM tiles of the unit and the tensor work they execute
                 const std::size_t tb[4] = {P.utiles[0].size(), P.utiles[1].size(), P.utiles[2].size(), P.utiles[3].size()};
-                add_unit_tiles(ud, uint32_t(P.units.size()), u.em.data(), u.em.size(), P.utiles, P.klist);
+                add_unit_tiles(ud, uint32_t(P.units.size()), u.em.data(), u.em.size(), P.utiles, P.klist,
+                               bookkeeping ? nullptr : crank.data());
                 for (int sh = 0; sh < N_SHAPES; ++sh)
                     for (std::size_t t = tb[sh]; t < P.utiles[sh].size(); ++t) {
                         const uint32_t o = P.utiles[sh][t].pad;
