@@ -115,10 +115,9 @@ struct LKD { uint32_t line, k; };  // (line, slice) position of one coefficient 
 // is the one with the least tensor work counting only the (BM lines x 4 slices) coefficient
 // groups that hold an entry; every m-tile's non-empty k-steps go to klist as (count, steps...),
 // a step being (k-step index << 4 | mask of its non-empty 4-slice groups), and its tiles carry
-// that list's offset in TileD::pad.  slot_rank (optional): the slot of term i is slot_rank[ents[i].k].
+// that list's offset in TileD::pad.
 void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t n, std::vector<TileD>* utiles,
-                    std::vector<uint16_t>& klist,
-                    const uint32_t* slot_rank = nullptr);
+                    std::vector<uint16_t>& klist);
 
 
 // Dense coefficient blocks W_u of S units, computed on the device (k_wgen).  Line l of a

@@ -20,7 +20,10 @@
 //               (deterministic; replaces cublasDgemm + atomic_add, tasks.cpp:315-344)
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <stdexcept>
 
 #include "dmma.cuh"
@@ -627,8 +630,18 @@ void upload_plan(HeffPlan& p) {
     p.d_P.alloc(p.p_len);
     // dense coefficient blocks, built once per plan and reused by every apply
     p.d_W.alloc(p.w_len ? p.w_len : 1);
+    static const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
+    auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+    double t0 = 0;
+    if (tdbg) {
+        QCM_CUDA(cudaStreamSynchronize(s));
+        t0 = now();
+    }
     p.cg.generate(p.d_W.get(), s);
     QCM_CUDA(cudaStreamSynchronize(s));
+    if (tdbg)
+        std::fprintf(stderr, "plan upload: coefficient generation %.4f s (%llu terms, %llu coefficients)\n", now() - t0,
+                     (unsigned long long)p.n_alpha, (unsigned long long)p.w_len);
 }
 
 }  // namespace qcm

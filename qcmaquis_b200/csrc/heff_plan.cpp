@@ -83,91 +83,145 @@ struct Part {
 // numbering), and with bookkeeping (mps column, R cohort, R column, alpha) per term.
 struct U {
     uint32_t st, offset, ms, rb_out;
-    std::vector<LKD> em;
+    uint64_t nterms = 0;
+    std::vector<uint32_t> sl;   // slot -> slice id, first-use order
+    std::vector<uint64_t> sig;  // per slot, nw words: the 16-line groups of its lines
+    uint32_t nw = 0;
+    std::vector<LKD> em;        // (line, slot) per term, with bookkeeping only
     std::vector<uint32_t> lines, rows, bk;  // lines: S row block of each line, rows: its MPO row b1
     std::vector<double> bk_a;
 };
 
-// Orders a unit's slots by the set of 16-line groups that use them (sig: nw words per slot; first-use
-// order among equal sets): slots used by the same line tiles then share the S-GEMM's 4-slot k-groups, so
-// fewer groups per line tile are occupied and each holds more coefficients.  slices is permuted;
-// rank[old slot] = new slot.
-void cluster_slots(std::vector<uint32_t>& slices, uint32_t nl, const std::vector<uint64_t>& sig,
-                   std::vector<uint32_t>& order, std::vector<uint32_t>& rank, std::vector<uint32_t>& tmp) {
-    const uint32_t nk = uint32_t(slices.size()), nw = (nl + 1023) / 1024;
-    rank.resize(nk);
-    for (uint32_t i = 0; i < nk; ++i) rank[i] = i;
-    if (nk < 2 || !nw) return;
-    order.resize(nk);
-    for (uint32_t i = 0; i < nk; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-        for (uint32_t w = nw; w-- > 0;) {
-            const uint64_t x = sig[std::size_t(a) * nw + w], y = sig[std::size_t(b) * nw + w];
-            if (x != y) return x < y;
-        }
-        return false;
-    });
-    for (uint32_t i = 0; i < nk; ++i) rank[order[i]] = i;
-    tmp.assign(slices.begin(), slices.end());
-    for (uint32_t i = 0; i < nk; ++i) slices[i] = tmp[order[i]];
-}
+// (unit, input state) of a cohort: the R block positions of the input state's cohort (null: the
+// unit has no T job for it) and the slice-id base of its T job
+struct GRef {
+    const int32_t* rp;
+    uint32_t jbase;
+};
 
 }  // namespace
 
-void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t n, std::vector<TileD>* utiles,
-                    std::vector<uint16_t>& klist, const uint32_t* slot_rank) {
-    if (!u.nl || !u.ne || !u.nk || !n) return;
-    constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK), four DMMA k-groups of 4 slices
-    const uint32_t nks = (u.nk + KS - 1) / KS;
-    if (nks >= 4096) throw std::runtime_error("S unit: too many slices for the k-step list");
-    // occupancy of (16 lines x 4 slices) coefficient groups as a 4-bit mask per (16 lines x 16 slices)
-    // block; coarser line tiles OR rows together
+namespace {
+
+constexpr uint32_t KS = 16;  // k-step of the S-GEMM (dm::BK), four DMMA k-groups of 4 slices
+
+// S-GEMM tiling of a unit: the shape and the occupancy at its line tiles (one 4-bit mask of non-empty
+// 4-slot groups per (line tile, k-step))
+struct TileChoice {
+    int sh = -1;
+    double cost = 0;
+    std::vector<uint8_t> occ;
+};
+
+// The cheapest shape for an occupancy occ16 (n16 x nks: 16-line groups x k-steps).  Coarser line
+// tiles OR rows together; the cost is the tensor work of the occupied groups, weighted per shape
+// (the 16-row shape runs 2 x 4 fragments per warp).
+void choose_shape(const UnitD& u, const uint8_t* occ16, uint32_t nks, TileChoice& best, std::vector<uint8_t>& occ) {
     const uint32_t n16 = (u.nl + 15) / 16;
-    std::vector<uint8_t> occ16(std::size_t(n16) * nks, 0);
-    if (slot_rank)
-        for (std::size_t i = 0; i < n; ++i) {
-            const uint32_t k = slot_rank[ents[i].k];
-            occ16[std::size_t(ents[i].line / 16) * nks + k / KS] |= uint8_t(1u << ((k % KS) / 4));
-        }
-    else
-        for (std::size_t i = 0; i < n; ++i)
-            occ16[std::size_t(ents[i].line / 16) * nks + ents[i].k / KS] |= uint8_t(1u << ((ents[i].k % KS) / 4));
-    auto occ_at = [&](uint32_t bm, std::vector<uint8_t>& occ) {
-        const uint32_t f = bm / 16, nmt = (u.nl + bm - 1) / bm;
+    auto groups = [](uint8_t m) { return (m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) + ((m >> 3) & 1); };
+    static const int cand[4] = {SHAPE_16, SHAPE_32, SHAPE_64, SHAPE_128};
+    static const double eff[4] = {1.3, 1.0, 1.0, 1.05};
+    for (int ci = 0; ci < 4; ++ci) {
+        const uint32_t bm = shape_bm(cand[ci]), bn = shape_bn(cand[ci]);
+        const uint32_t f = bm / 16, nmt = (u.nl + bm - 1) / bm, nnt = (u.ne + bn - 1) / bn;
         occ.assign(std::size_t(nmt) * nks, 0);
         for (uint32_t r = 0; r < n16; ++r)
             for (uint32_t ks = 0; ks < nks; ++ks) occ[std::size_t(r / f) * nks + ks] |= occ16[std::size_t(r) * nks + ks];
-    };
-    auto groups = [](uint8_t m) { return (m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) + ((m >> 3) & 1); };
-    // candidate shapes and a relative cost per tensor flop (the 16-row shape runs 2 x 4 fragments per warp)
-    static const int cand[4] = {SHAPE_16, SHAPE_32, SHAPE_64, SHAPE_128};
-    static const double eff[4] = {1.3, 1.0, 1.0, 1.05};
-    int best = -1;
-    double best_cost = 0;
-    std::vector<uint8_t> occ, best_occ;
-    for (int ci = 0; ci < 4; ++ci) {
-        const uint32_t bm = shape_bm(cand[ci]), bn = shape_bn(cand[ci]);
-        const uint32_t nnt = (u.ne + bn - 1) / bn;
-        occ_at(bm, occ);
         std::size_t on = 0;
         for (uint8_t o : occ) on += groups(o);
         const double cost = eff[ci] * double(on) * bm * 4.0 * double(nnt) * bn;
-        if (best < 0 || cost < best_cost) { best = ci; best_cost = cost; best_occ.swap(occ); }
+        if (best.sh < 0 || cost < best.cost) { best.sh = cand[ci]; best.cost = cost; best.occ.swap(occ); }
     }
-    const int sh = cand[best];
+}
+
+void emit_tiles(const UnitD& u, uint32_t item, const TileChoice& c, std::vector<TileD>* utiles,
+                std::vector<uint16_t>& klist) {
+    const uint32_t nks = (u.nk + KS - 1) / KS;
+    const int sh = c.sh;
     const uint32_t bm = shape_bm(sh), bn = shape_bn(sh), nmt = (u.nl + bm - 1) / bm;
     for (uint32_t mt = 0; mt < nmt; ++mt) {
         const uint32_t off = uint32_t(klist.size());
         klist.push_back(0);
         uint16_t cnt = 0;
         for (uint32_t ks = 0; ks < nks; ++ks) {
-            const uint8_t m = best_occ[std::size_t(mt) * nks + ks];
+            const uint8_t m = c.occ[std::size_t(mt) * nks + ks];
             if (m) { klist.push_back(uint16_t((ks << 4) | m)); ++cnt; }
         }
         klist[off] = cnt;
         if (!cnt) continue;
         for (uint32_t n0 = 0; n0 < u.ne; n0 += bn) utiles[sh].push_back(TileD{item, mt * bm, n0, off});
     }
+}
+
+uint32_t checked_ksteps(const UnitD& u) {
+    const uint32_t nks = (u.nk + KS - 1) / KS;
+    if (nks >= 4096) throw std::runtime_error("S unit: too many slices for the k-step list");
+    return nks;
+}
+
+// Slot order and tiling of an H_eff unit from its slot signatures: sig[slot * nw + w] bit r set where a
+// line of 16-line group 64 w + r uses the slot.  For each tile height (16, 32, 64, 128 lines) the slots
+// are sorted by the line tiles that use them (then by the 16-line groups; first-use order among
+// equal sets), so that slots used by the same line tiles share 4-slot k-groups; the ordering and shape
+// of least tensor work are kept.  order[new slot] = old slot.
+void plan_unit_tiles(const UnitD& u, const uint64_t* sig, uint32_t nw, std::vector<uint32_t>& order, TileChoice& best) {
+    const uint32_t nk = u.nk;
+    order.resize(nk);
+    for (uint32_t i = 0; i < nk; ++i) order[i] = i;
+    if (!u.nl || !u.ne || !nk) return;
+    const uint32_t nks = checked_ksteps(u), n16 = (u.nl + 15) / 16;
+    std::vector<uint64_t> key;
+    std::vector<uint32_t> ord(nk);
+    std::vector<uint8_t> occ16, scratch;
+    for (uint32_t f : {1u, 2u, 4u, 8u}) {
+        if (f > 1 && (n16 + f / 2 - 1) / (f / 2) <= 1) break;  // one coarse tile: the same order as before
+        const uint32_t nc = (n16 + f - 1) / f, ncw = (nc + 63) / 64;
+        key.assign(std::size_t(nk) * ncw, 0);
+        for (uint32_t sl = 0; sl < nk; ++sl)
+            for (uint32_t w = 0; w < nw; ++w)
+                for (uint64_t bits = sig[std::size_t(sl) * nw + w]; bits; bits &= bits - 1) {
+                    const uint32_t c = (64 * w + uint32_t(__builtin_ctzll(bits))) / f;
+                    key[std::size_t(sl) * ncw + c / 64] |= 1ull << (c % 64);
+                }
+        for (uint32_t i = 0; i < nk; ++i) ord[i] = i;
+        std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+            for (uint32_t w = ncw; w-- > 0;) {
+                const uint64_t x = key[std::size_t(a) * ncw + w], y = key[std::size_t(b) * ncw + w];
+                if (x != y) return x < y;
+            }
+            for (uint32_t w = nw; w-- > 0;) {
+                const uint64_t x = sig[std::size_t(a) * nw + w], y = sig[std::size_t(b) * nw + w];
+                if (x != y) return x < y;
+            }
+            return false;
+        });
+        occ16.assign(std::size_t(n16) * nks, 0);
+        for (uint32_t i = 0; i < nk; ++i) {
+            const uint32_t sl = ord[i];
+            const uint8_t bit = uint8_t(1u << ((i % KS) / 4));
+            for (uint32_t w = 0; w < nw; ++w)
+                for (uint64_t bits = sig[std::size_t(sl) * nw + w]; bits; bits &= bits - 1)
+                    occ16[std::size_t(64 * w + uint32_t(__builtin_ctzll(bits))) * nks + i / KS] |= bit;
+        }
+        TileChoice c;
+        choose_shape(u, occ16.data(), nks, c, scratch);
+        if (best.sh < 0 || c.cost < best.cost) { best = std::move(c); order = ord; }
+    }
+}
+
+}  // namespace
+
+void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t n, std::vector<TileD>* utiles,
+                    std::vector<uint16_t>& klist) {
+    if (!u.nl || !u.ne || !u.nk || !n) return;
+    const uint32_t nks = checked_ksteps(u), n16 = (u.nl + 15) / 16;
+    // occupancy of (16 lines x 4 slices) coefficient groups as a 4-bit mask per (16 lines x 16 slices) block
+    std::vector<uint8_t> occ16(std::size_t(n16) * nks, 0), scratch;
+    for (std::size_t i = 0; i < n; ++i)
+        occ16[std::size_t(ents[i].line / 16) * nks + ents[i].k / KS] |= uint8_t(1u << ((ents[i].k % KS) / 4));
+    TileChoice c;
+    choose_shape(u, occ16.data(), nks, c, scratch);
+    emit_tiles(u, item, c, utiles, klist);
 }
 
 std::shared_ptr<const MPOTables> build_mpo_tables(const MPOTensor& W) {
@@ -332,7 +386,10 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     const std::vector<uint32_t>& optr = mt->optr;
     const std::vector<uint32_t>& oin = mt->oin;
     const std::vector<uint32_t>& oout = mt->oout;
-    const std::vector<double>& oval = mt->oval;
+    // the same grouped by (operator, output state), in their order within the operator
+    const std::vector<uint32_t>& og_ptr = mt->o_ptr;
+    const std::vector<uint32_t>& og_in = mt->o_in;
+    const std::vector<double>& og_val = mt->o_val;
     // coefficient generation: lines iterate MPO rows b1, slices come from R cohorts
     p->cg.set_mpo(W, true);
     p->cg.set_boundary(R);
@@ -348,8 +405,9 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     std::vector<U> units;
     std::vector<uint32_t> slices;
     std::vector<double> lscale;
-    std::vector<uint64_t> csig;
     std::vector<uint32_t> corder, crank, ctmp;
+    std::vector<GRef> gref;
+    std::vector<std::pair<uint32_t, uint32_t>> lrows;
 #pragma omp for schedule(dynamic, 1)
     for (int lbi = 0; lbi < int(nl); ++lbi) try {
         const uint32_t lb_in = uint32_t(lbi);
@@ -406,12 +464,11 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 U& x = units[nu++];
                 x.st = st; x.offset = ro.off + uint32_t(sm.sub[st]) * ro.rs; x.ms = ro.rs; x.rb_out = ro.rb;
                 x.em.clear(); x.lines.clear(); x.rows.clear(); x.bk.clear(); x.bk_a.clear();
+                x.nterms = 0; x.sl.clear(); x.sig.clear();
                 stripe += ro.rs;
             }
             if (stripe != p->x_cols[lb_out]) throw std::runtime_error("heff plan: cohort stripe differs from the block width");
             // per (input state, unit): R cohort and slice-id base of its T job
-            std::vector<int> unit_of(nst, -1);
-            for (std::size_t k = 0; k < nu; ++k) unit_of[units[k].st] = int(k);
             std::vector<WGenInD> gin(nu * nst, WGenInD{WGEN_NONE, WGEN_NONE});  // [unit][input state]
             std::vector<uint32_t> rsin_t(nst, 0);
             for (uint32_t sti = 0; sti < nst; ++sti) {
@@ -424,35 +481,63 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     if (cir != NONE && job != NONE) gin[k * nst + sti] = WGenInD{cir, job_pos0[job]};
                 }
             }
+            // L blocks of the cohort: MPO row b1 and its S row block
+            lrows.clear();
+            for (uint32_t b1 = 0; b1 < W.rows; ++b1)
+                if (L.has_block(ci, b1)) lrows.push_back({b1, uint32_t(L.offset(ci, b1) / (int64_t(ls_in) * ls_out))});
+            const uint32_t nw16 = (uint32_t(lrows.size()) + 1023) / 1024;  // signature words: 64 groups of 16 lines
+            // per (unit, input state): the R block positions of the input state's cohort and the
+            // slice-id base of its T job (rp = null: no T job)
             const int32_t* Rpos = p->cg.b_pos.data();
             const std::size_t Raux = R.aux;
+            gref.assign(nu * nst, GRef{nullptr, 0});
+            for (std::size_t i = 0; i < nu * nst; ++i)
+                if (gin[i].c != WGEN_NONE) gref[i] = GRef{Rpos + std::size_t(gin[i].c) * Raux, gin[i].jbase};
+            // each unit's terms in (b1, MPO entry, operator term) order: slots numbered at first use, the
+            // 16-line groups of every slot's lines recorded, lines appended once they have a term
             std::size_t n_alpha = 0;
-            for (uint32_t b1 = 0; b1 < W.rows; ++b1) {
-                if (!L.has_block(ci, b1)) continue;
-                const uint32_t bpos = uint32_t(L.offset(ci, b1) / (int64_t(ls_in) * ls_out));
-                for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
-                    const uint32_t b2 = W.b2[e], op = W.op[e];
-                    for (uint32_t k = optr[op]; k < optr[op + 1]; ++k) {
-                        const int u = unit_of[oout[k]];
-                        if (u < 0) continue;
-                        const uint32_t sti = oin[k];
-                        const WGenInD g = gin[std::size_t(u) * nst + sti];
-                        if (g.c == WGEN_NONE) continue;
-                        const int32_t pos = Rpos[g.c * Raux + b2];
-                        if (pos < 0) continue;
-                        U& un = units[u];
-                        if (un.lines.empty() || un.lines.back() != bpos) { un.lines.push_back(bpos); un.rows.push_back(b1); }
-                        un.em.push_back(LKD{uint32_t(un.lines.size() - 1), g.jbase + uint32_t(pos)});
-                        if (bookkeeping) {
-                            const uint32_t col = uint32_t(R.offset(g.c, b2) / rsin_t[sti]);
-                            const uint32_t job = tj[std::size_t(sti) * nr + un.rb_out];
-                            const uint32_t row[3] = {P.tjob_mps[job], g.c, col};
-                            un.bk.insert(un.bk.end(), row, row + 3);
-                            un.bk_a.push_back(oval[k] * R.conj_scale(g.c, b2) * (W.scale[e] * L.conj_scale(ci, b1)));
+            for (std::size_t ui = 0; ui < nu; ++ui) {
+                U& un = units[ui];
+                un.nw = nw16;
+                const GRef* gu = gref.data() + ui * nst;
+                for (const auto& lr : lrows) {
+                    const uint32_t b1 = lr.first, line = uint32_t(un.lines.size());
+                    const uint64_t before = un.nterms;
+                    const uint32_t gw = (line >> 4) >> 6;
+                    const uint64_t gbit = 1ull << ((line >> 4) & 63);
+                    for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
+                        const uint32_t b2 = W.b2[e];
+                        const std::size_t q = std::size_t(W.op[e]) * nst + un.st;
+                        for (uint32_t k = og_ptr[q]; k < og_ptr[q + 1]; ++k) {
+                            const uint32_t sti = og_in[k];
+                            const GRef g = gu[sti];
+                            if (!g.rp) continue;
+                            const int32_t pos = g.rp[b2];
+                            if (pos < 0) continue;
+                            const uint32_t id = g.jbase + uint32_t(pos);
+                            uint32_t& sl = slot[id];
+                            if (sl == NONE) {
+                                sl = uint32_t(un.sl.size());
+                                un.sl.push_back(id);
+                                un.sig.resize(un.sig.size() + nw16, 0);
+                            }
+                            un.sig[std::size_t(sl) * nw16 + gw] |= gbit;
+                            ++un.nterms;
+                            if (bookkeeping) {
+                                un.em.push_back(LKD{line, sl});
+                                const uint32_t c = gin[ui * nst + sti].c;
+                                const uint32_t col = uint32_t(R.offset(c, b2) / rsin_t[sti]);
+                                const uint32_t job = tj[std::size_t(sti) * nr + un.rb_out];
+                                const uint32_t row[3] = {P.tjob_mps[job], c, col};
+                                un.bk.insert(un.bk.end(), row, row + 3);
+                                un.bk_a.push_back(og_val[k] * R.conj_scale(c, b2) * (W.scale[e] * L.conj_scale(ci, b1)));
+                            }
                         }
-                        ++n_alpha;
                     }
+                    if (un.nterms != before) { un.lines.push_back(lr.second); un.rows.push_back(b1); }
                 }
+                for (uint32_t id : un.sl) slot[id] = NONE;
+                n_alpha += un.nterms;
             }
             if (n_alpha == 0) continue;
             P.n_alpha += n_alpha;
@@ -460,28 +545,21 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             P.s_len += (uint64_t(K_c) * stripe + 31) / 32 * 32;
             for (std::size_t ui = 0; ui < nu; ++ui) {
                 U& u = units[ui];
-                P.flops_s += 2.0 * ls_in * u.ms * double(u.em.size());
-                if (u.em.empty()) continue;
-                // number the unit's slices in first-use order, with the 16-line groups using each
-                slices.clear();
-                const uint32_t nw16 = (uint32_t(u.lines.size()) + 1023) / 1024;  // 64-bit words of 16-line groups
-                csig.clear();
-                for (LKD& m : u.em) {
-                    uint32_t& sl = slot[m.k];
-                    if (sl == NONE) {
-                        sl = uint32_t(slices.size());
-                        slices.push_back(m.k);
-                        csig.resize(csig.size() + nw16, 0);
-                    }
-                    m.k = sl;
-                    const uint32_t g = m.line >> 4;
-                    csig[std::size_t(sl) * nw16 + (g >> 6)] |= 1ull << (g & 63);
-                }
-                for (uint32_t gp : slices) slot[gp] = NONE;
-                cluster_slots(slices, uint32_t(u.lines.size()), csig, corder, crank, ctmp);
-                if (bookkeeping)
-                    for (LKD& m : u.em) m.k = crank[m.k];
+                P.flops_s += 2.0 * ls_in * u.ms * double(u.nterms);
+                if (!u.nterms) continue;
+                slices.assign(u.sl.begin(), u.sl.end());
+                // slot order and S-GEMM tiling from the slot signatures
                 UnitD ud{};
+                ud.nl = uint32_t(u.lines.size()); ud.nk = uint32_t(slices.size()); ud.ne = ls_in * u.ms;
+                TileChoice tch;
+                plan_unit_tiles(ud, u.sig.data(), u.nw, corder, tch);
+                ctmp.assign(slices.begin(), slices.end());
+                for (std::size_t i = 0; i < slices.size(); ++i) slices[i] = ctmp[corder[i]];
+                if (bookkeeping) {
+                    crank.resize(slices.size());
+                    for (uint32_t i = 0; i < uint32_t(slices.size()); ++i) crank[corder[i]] = i;
+                    for (LKD& m : u.em) m.k = crank[m.k];
+                }
                 ud.s_off = s_off + uint64_t(u.offset) * K_c;
                 ud.line_stride = ls_in; ud.erows = ls_in; ud.col_stride = K_c; ud.ne = ls_in * u.ms;
                 ud.nl = uint32_t(u.lines.size()); ud.line0 = uint32_t(P.line_b1.size());
@@ -509,8 +587,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
                 // S-GEMM tiles of the unit and the tensor work they execute
                 const std::size_t tb[4] = {P.utiles[0].size(), P.utiles[1].size(), P.utiles[2].size(), P.utiles[3].size()};
-                add_unit_tiles(ud, uint32_t(P.units.size()), u.em.data(), u.em.size(), P.utiles, P.klist,
-                               bookkeeping ? nullptr : crank.data());
+                emit_tiles(ud, uint32_t(P.units.size()), tch, P.utiles, P.klist);
                 for (int sh = 0; sh < N_SHAPES; ++sh)
                     for (std::size_t t = tb[sh]; t < P.utiles[sh].size(); ++t) {
                         const uint32_t o = P.utiles[sh][t].pad;
@@ -520,7 +597,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     }
                 P.units.push_back(ud);
                 P.g_elems += uint64_t(ud.ne) * ud.nl;
-                P.g_reads += uint64_t(ud.ne) * u.em.size();
+                P.g_reads += uint64_t(ud.ne) * u.nterms;
                 P.flops_sdense += 2.0 * ud.nl * ud.nk * double(ud.ne);  // padding lines not counted
             }
             P.flops_ls += 2.0 * ls_out * ls_in * double(nS) * stripe;
