@@ -485,6 +485,13 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             lrows.clear();
             for (uint32_t b1 = 0; b1 < W.rows; ++b1)
                 if (L.has_block(ci, b1)) lrows.push_back({b1, uint32_t(L.offset(ci, b1) / (int64_t(ls_in) * ls_out))});
+            // lines in decreasing MPO row length (the rows with most terms first; stable): lines of similar
+            // density share S-GEMM line tiles, so the tiles of sparse lines occupy few slot groups
+            // (executed tensor work at the L=24, M=512 middle bond: -18 %)
+            std::stable_sort(lrows.begin(), lrows.end(), [&](const std::pair<uint32_t, uint32_t>& a,
+                                                             const std::pair<uint32_t, uint32_t>& b) {
+                return W.row_ptr[a.first + 1] - W.row_ptr[a.first] > W.row_ptr[b.first + 1] - W.row_ptr[b.first];
+            });
             const uint32_t nw16 = (uint32_t(lrows.size()) + 1023) / 1024;  // signature words: 64 groups of 16 lines
             // per (unit, input state): the R block positions of the input state's cohort and the
             // slice-id base of its T job (rp = null: no T job)
