@@ -420,20 +420,25 @@ __global__ void __launch_bounds__(NTHR) k_lspart(const KItemD* __restrict__ item
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) { Pt[m + n * S::BM] = v; });
 }
 
-// Sum the partial tiles of each output tile in item order and write y.
+// Sum the partial tiles of each output tile in item order and write y.  Grid: (output tile, 256-element
+// chunk of the tile).
 template <class S>
 __global__ void __launch_bounds__(256) k_lsreduce(const OTileD* __restrict__ otiles, const OutD* __restrict__ outs,
                                                   const double* __restrict__ P, double* __restrict__ y) {
+    // one thread per tile element (blockIdx.y: the tile's 256-element chunk): the element's partials are
+    // added in item order; the unrolled loop keeps several of its loads in flight
     const OTileD ot = otiles[blockIdx.x];
     const OutD O = outs[ot.out];
-    for (int e = threadIdx.x; e < S::BM * S::BN; e += blockDim.x) {
-        const int m = e % S::BM, n = e / S::BM;
-        const uint32_t gm = ot.m0 + m, gn = ot.n0 + n;
-        if (gm >= O.M || gn >= O.N) continue;
-        double s = 0.0;
-        for (uint32_t p = 0; p < ot.nparts; ++p) s += P[uint64_t(ot.part0 + p) * S::BM * S::BN + e];
-        y[O.y_off + gm + uint64_t(gn) * O.M] = s;
-    }
+    const int e = int(blockIdx.y) * int(blockDim.x) + int(threadIdx.x);
+    if (e >= S::BM * S::BN) return;
+    const int m = e % S::BM, n = e / S::BM;
+    const uint32_t gm = ot.m0 + m, gn = ot.n0 + n;
+    if (gm >= O.M || gn >= O.N) return;
+    const double* Pe = P + uint64_t(ot.part0) * S::BM * S::BN + e;
+    double s = 0.0;
+#pragma unroll 8
+    for (uint32_t p = 0; p < ot.nparts; ++p) s += Pe[uint64_t(p) * S::BM * S::BN];
+    y[O.y_off + gm + uint64_t(gn) * O.M] = s;
 }
 
 template <class S>
@@ -456,7 +461,8 @@ void launch_ls(HeffPlan& p, int sh, const double* Sb, double* Pb, double* y, cud
     if (p.kitems[sh].empty()) return;
     k_lspart<S><<<unsigned(p.kitems[sh].size()), NTHR, 0, s>>>(p.d_kitems[sh].get(), p.d_otiles[sh].get(), p.d_outs.get(),
                                                                p.d_segs.get(), p.L->data.get(), Sb, Pb);
-    k_lsreduce<S><<<unsigned(p.otiles[sh].size()), 256, 0, s>>>(p.d_otiles[sh].get(), p.d_outs.get(), Pb, y);
+    const dim3 rg(unsigned(p.otiles[sh].size()), unsigned((S::BM * S::BN + 255) / 256));
+    k_lsreduce<S><<<rg, 256, 0, s>>>(p.d_otiles[sh].get(), p.d_outs.get(), Pb, y);
 }
 
 }  // namespace
