@@ -395,7 +395,24 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     p->cg.set_boundary(R);
 
     std::vector<Part> parts(nl);
+    // ket sectors in decreasing estimated work (the L blocks of their cohorts), so that dynamic
+    // scheduling starts the largest parts first and no large part is left for the end
+    std::vector<uint32_t> part_order(nl);
+    {
+        std::vector<uint64_t> est(nl, 0);
+        for (uint32_t a = 0; a < nl; ++a) {
+            part_order[a] = a;
+            for (uint32_t b = 0; b < nl; ++b) {
+                const uint32_t ci = L.cohort_index(left[b].first, left[a].first);
+                if (ci == L.n_cohorts()) continue;
+                const uint32_t ce = L.tr[ci] ? L.cohort_index(left[a].first, left[b].first) : ci;
+                if (ce < L.n_cohorts()) est[a] += L.nb[ce];
+            }
+        }
+        std::stable_sort(part_order.begin(), part_order.end(), [&](uint32_t x, uint32_t y) { return est[x] > est[y]; });
+    }
     const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
+    std::vector<double> part_s(tdbg ? nl : 0);
     auto tnow = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     const double t_a = tnow();
     std::string err;
@@ -409,9 +426,10 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     std::vector<GRef> gref;
     std::vector<std::pair<uint32_t, uint32_t>> lrows;
 #pragma omp for schedule(dynamic, 1)
-    for (int lbi = 0; lbi < int(nl); ++lbi) try {
-        const uint32_t lb_in = uint32_t(lbi);
+    for (int oi = 0; oi < int(nl); ++oi) try {
+        const uint32_t lb_in = part_order[std::size_t(oi)];
         Part& P = parts[lb_in];
+        const double tp0 = tdbg ? tnow() : 0.0;
         P.cg.nst = nst;
         const uint32_t ls_in = uint32_t(left[lb_in].second);
         // ---- T jobs: one per (input state, bra right sector) ----
@@ -614,6 +632,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             sg.ls_in = ls_in; sg.nS = nS; sg.tr = (ci != ce) ? 1 : 0;
             P.segs.push_back({lb_out, sg});
         }
+        if (tdbg) part_s[lb_in] = tnow() - tp0;
     } catch (const std::exception& e) {
 #pragma omp critical
         err = e.what();
@@ -732,10 +751,14 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         }
         p->outs.push_back(o);
     }
-    if (tdbg)
-        std::fprintf(stderr, "plan: tables %.4f s, parts %.4f s, merge %.4f s; %zu units, %llu coefficient terms, %zu S tiles, "
-                     "%.3e dense coefficients\n", t_a - t_0, t_b - t_a, tnow() - t_b, p->units.size(), (unsigned long long)p->n_alpha,
+    if (tdbg) {
+        double psum = 0, pmax = 0;
+        for (double t : part_s) { psum += t; pmax = std::max(pmax, t); }
+        std::fprintf(stderr, "plan: tables %.4f s, parts %.4f s (sum %.4f s, largest %.4f s), merge %.4f s; %zu units, %llu "
+                     "coefficient terms, %zu S tiles, %.3e dense coefficients\n", t_a - t_0, t_b - t_a, psum, pmax, tnow() - t_b,
+                     p->units.size(), (unsigned long long)p->n_alpha,
                      p->utiles[0].size() + p->utiles[1].size() + p->utiles[2].size() + p->utiles[3].size(), double(p->w_len));
+    }
     uint64_t pl = 0;
     for (int sh = 0; sh < N_SHAPES; ++sh) pl = std::max<uint64_t>(pl, uint64_t(p->kitems[sh].size()) * shape_bm(sh) * shape_bn(sh));
     p->p_len = pl;

@@ -203,8 +203,8 @@ __device__ __forceinline__ double half_sum(double v) {
 
 __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ jobs, const double* __restrict__ A,
                                                      double* __restrict__ U, double* __restrict__ S, double* __restrict__ V,
-                                                     double* __restrict__ Wg, int use_smem, int* __restrict__ zero_count,
-                                                     int* __restrict__ sweeps_used) {
+                                                     double* __restrict__ Wg, uint32_t smem_doubles,
+                                                     int* __restrict__ zero_count, int* __restrict__ sweeps_used) {
     extern __shared__ double smem[];
     __shared__ int rotated;
     __shared__ uint32_t rank_of[1024];
@@ -212,8 +212,14 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
     const SvdJob J = jobs[blockIdx.x];
     const bool tall = J.m >= J.n;
     const uint32_t r = tall ? J.m : J.n, c = tall ? J.n : J.m;
-    double* G = use_smem ? smem : Wg + J.w_off;
-    double* Q = G + uint64_t(r) * c;
+    // work matrix G (r x c) and rotations Q (c x c): both in the launch's shared memory when they fit,
+    // else G there and Q in the block's global scratch (L2-resident), else both in the scratch
+    const uint64_t rc = uint64_t(r) * c;
+    double* G;
+    double* Q;
+    if (rc + uint64_t(c) * c <= smem_doubles) { G = smem; Q = smem + rc; }
+    else if (rc <= smem_doubles) { G = smem; Q = Wg + J.w_off + rc; }
+    else { G = Wg + J.w_off; Q = G + rc; }
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = JTHR / 32;
     // G = A or A^T, Q = I
     const double* a = A + J.a_off;
@@ -341,7 +347,8 @@ uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n) {
 void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
                         uint64_t s_len, double* V, uint64_t v_len, double* W, uint64_t w_len, int* zero_count,
                         DBuf<SvdJob>& jobbuf, cudaStream_t s, int* sweeps_used) {
-    // smem launch for the blocks whose work matrices fit, global scratch for the rest
+    // one launch for the blocks whose work matrix G fits in shared memory (their rotations Q too where
+    // they fit), one with both in the global scratch for the rest
     std::vector<SvdJob> small, large;
     uint64_t smax = 0;
     for (const SvdJob& j : jobs) {
@@ -351,8 +358,9 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
         if (j.a_off + uint64_t(j.m) * j.n > a_len || j.u_off + uint64_t(j.m) * k > u_len || j.s_off + k > s_len ||
             j.v_off + uint64_t(j.n) * k > v_len || j.w_off + jacobi_svd_scratch(j.m, j.n) > w_len)
             throw std::runtime_error("batched_jacobi_svd: block outside its buffers");
-        const uint64_t need = jacobi_svd_scratch(j.m, j.n);
-        if (need <= JSMEM_DOUBLES) { small.push_back(j); smax = std::max(smax, need); }
+        // shared memory for G (r x c) and, where it fits too, Q (c x c)
+        const uint64_t need = jacobi_svd_scratch(j.m, j.n), rc = std::max(j.m, j.n) * uint64_t(k);
+        if (rc <= JSMEM_DOUBLES) { small.push_back(j); smax = std::max(smax, need <= JSMEM_DOUBLES ? need : rc); }
         else large.push_back(j);
     }
     uint32_t nid = 0;
@@ -365,11 +373,12 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
     if (!small.empty()) {
         const std::size_t bytes = smax * sizeof(double);
         QCM_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-        k_jacobi_svd<<<unsigned(small.size()), JTHR, bytes, s>>>(jobbuf.get(), A, U, S, V, W, 1, zero_count, sweeps_used);
+        k_jacobi_svd<<<unsigned(small.size()), JTHR, bytes, s>>>(jobbuf.get(), A, U, S, V, W, uint32_t(smax), zero_count,
+                                                                 sweeps_used);
         QCM_CUDA(cudaGetLastError());
     }
     if (!large.empty()) {
-        k_jacobi_svd<<<unsigned(large.size()), JTHR, 0, s>>>(jobbuf.get() + small.size(), A, U, S, V, W, 0, zero_count,
+        k_jacobi_svd<<<unsigned(large.size()), JTHR, 0, s>>>(jobbuf.get() + small.size(), A, U, S, V, W, 0u, zero_count,
                                                               sweeps_used);
         QCM_CUDA(cudaGetLastError());
     }

@@ -40,6 +40,9 @@ CASES = {
     "cutoff": ([(50, 40), (20, 20)], None, 1000, 1e-1),
     # work matrices larger than the shared-memory path
     "global_path": ([(200, 180), (33, 300), (7, 7)], None, 150, 1e-16),
+    # a block whose work matrix fits in shared memory but not together with its rotations (hybrid
+    # placement), in one launch with blocks that fit entirely
+    "hybrid_path": ([(174, 109), (120, 110), (5, 5)], None, 250, 1e-16),
 }
 
 
