@@ -316,6 +316,20 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
 int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* params, const qcm_mps_desc* sites,
                              const double* const* data, qcm_dmrg** out);
 int qcm_dmrg_length(const qcm_dmrg* d);
+/* Excited states (ts_optimize.hpp:217-223, optimize.h:134-172): n_states ortho states (for example
+ * converged lower states), each given as L site tensors sites[o*L + i] / data[o*L + i] (right-paired, as
+ * for qcm_dmrg_create_from_mps; same physical basis and end sectors as the DMRG state).  From then on
+ * every step's Jacobi-Davidson keeps its solution orthogonal to the ortho states' projections onto the
+ * step's two-site basis (site_ortho_boundaries, contractions/special.hpp:38-62), and the overlap
+ * boundaries with each ortho state (mps.h:175-219) move with the sweep.  Call between sweeps, before
+ * the first step of a sweep; replaces earlier ortho states (n_states = 0 clears them). */
+int qcm_dmrg_set_ortho(qcm_dmrg* d, int n_states, const qcm_mps_desc* sites, const double* const* data);
+/* Site tensor `site` of the current MPS as a "QMPS" v1 blob: u32 magic 0x53504D51, u32 1; Index phys,
+ * left, right (u32 count, then i32 a, i32 b, u32 dim per sector); u32 blocks, then per block i32 a, i32 b
+ * (left charge), u32 rows, u32 cols and rows x cols doubles (right-paired, column-major).  Call with
+ * buf == NULL for *len.  Between steps the MPS is the state the sweep has reached (checkpoints, ortho
+ * states for a later excited-state run). */
+int qcm_dmrg_export_site(qcm_dmrg* d, int site, void* buf, size_t cap, size_t* len);
 /* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL); only
  * between sweeps (see qcm_dmrg_run). */
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);

@@ -98,6 +98,23 @@ int orc_dmrg_set_heev(orc_dmrg* h, int heev, double a_init, double a_main, doubl
     return 0;
 }
 
+// excited states: n_states ortho states of L site tensors each ("QMPS" blobs, state-major), kept
+// orthogonal to every solution; call at the start of a sweep
+int orc_dmrg_set_ortho(orc_dmrg* h, int n_states, const void* const* blobs, const size_t* lens) {
+    try {
+        DMRG& d = *h->d;
+        if (n_states < 0 || (n_states > 0 && (!blobs || !lens))) return fail("orc_dmrg_set_ortho: bad arguments");
+        std::vector<std::vector<MPSTensor>> st(static_cast<std::size_t>(n_states));
+        for (int o = 0; o < n_states; ++o)
+            for (int i = 0; i < d.L; ++i) {
+                const std::size_t k = std::size_t(o) * d.L + i;
+                st[o].push_back(load_mps_tensor(static_cast<const uint8_t*>(blobs[k]), lens[k]));
+            }
+        d.set_ortho(std::move(st));
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
 // ietl_jcd_gmres of the sweep's solves
 int orc_dmrg_set_gmres(orc_dmrg* h, int gmres) {
     if (gmres < 0) return fail("orc_dmrg_set_gmres: gmres < 0");

@@ -22,6 +22,19 @@ Mat matmul(const Mat& A, const Mat& B) {
     return C;
 }
 // block_matrix gemm (block_matrix_algorithms.h:64-90) for charge-diagonal operands
+Mat matmul_tn(const Mat& A, const Mat& B) {  // A^T B
+    Mat C(A.c, B.c);
+    if (A.r && A.c && B.c)
+        dgemm('T', 'N', int(A.c), int(B.c), int(A.r), 1.0, A.d.data(), int(A.r), B.d.data(), int(B.r), 0.0, C.d.data(), int(A.c));
+    return C;
+}
+Mat matmul_nt(const Mat& A, const Mat& B) {  // A B^T
+    Mat C(A.r, B.r);
+    if (A.r && B.r && A.c)
+        dgemm('N', 'T', int(A.r), int(B.r), int(A.c), 1.0, A.d.data(), int(A.r), B.d.data(), int(B.r), 0.0, C.d.data(), int(A.r));
+    return C;
+}
+
 BlockMatrix bm_gemm(const BlockMatrix& A, const BlockMatrix& B) {
     BlockMatrix C;
     for (std::size_t k = 0; k < A.n_blocks(); ++k) {
@@ -629,6 +642,113 @@ DMRG::DMRG(std::vector<MPOTensor> mpo_single, int nup, int ndown, const DMRGPara
     for (int i = L - 1; i >= 0; --i) right_[i] = overlap_mpo_right_step(mps[i], mps[i], right_[i + 1], mpo[i], true);
 }
 
+// ---------------------------------------------------------------------------
+// Excited states.  overlap_left_step (mp_tensors/mps.h:178-197): t = left * ket (right-paired), reshaped
+// to left-paired over the bra's left basis, then bra^T t.
+BlockMatrix ortho_left_step(const MPSTensor& bra_in, const MPSTensor& ket_in, const BlockMatrix& left) {
+    MPSTensor bra = bra_in, ket = ket_in;
+    bra.make_left_paired();
+    ket.make_right_paired();
+    MPSTensor t;
+    t.phys = ket.phys; t.left = bra.left; t.right = ket.right; t.pairing = RightPaired;
+    t.data = bm_gemm(left, ket.data);
+    t.make_left_paired();
+    BlockMatrix out;
+    for (std::size_t k = 0; k < bra.data.n_blocks(); ++k) {
+        const std::size_t j = t.data.find(bra.data.rc[k], bra.data.rc[k]);
+        if (j == t.data.n_blocks()) continue;
+        out.insert(bra.data.rc[k], bra.data.rc[k], matmul_tn(bra.data.b[k], t.data.b[j]));
+    }
+    return out;
+}
+
+// overlap_right_step (mp_tensors/mps.h:200-219): t = ket (left-paired) * right^T, reshaped to right-paired
+// over the bra's right basis, then bra t^T.
+BlockMatrix ortho_right_step(const MPSTensor& bra_in, const MPSTensor& ket_in, const BlockMatrix& right) {
+    MPSTensor bra = bra_in, ket = ket_in;
+    bra.make_right_paired();
+    ket.make_left_paired();
+    MPSTensor t;
+    t.phys = ket.phys; t.left = ket.left; t.right = bra.right; t.pairing = LeftPaired;
+    for (std::size_t k = 0; k < ket.data.n_blocks(); ++k) {
+        const std::size_t j = right.find(ket.data.rc[k], ket.data.rc[k]);
+        if (j == right.n_blocks()) continue;
+        t.data.insert(ket.data.rc[k], ket.data.rc[k], matmul_nt(ket.data.b[k], right.b[j]));
+    }
+    t.make_right_paired();
+    BlockMatrix out;
+    for (std::size_t k = 0; k < bra.data.n_blocks(); ++k) {
+        const std::size_t j = t.data.find(bra.data.lc[k], bra.data.lc[k]);
+        if (j == t.data.n_blocks()) continue;
+        out.insert(bra.data.lc[k], bra.data.lc[k], matmul_nt(bra.data.b[k], t.data.b[j]));
+    }
+    return out;
+}
+
+// site_ortho_boundaries (contractions/special.hpp:38-62): left * ortho twin, then each (phys state,
+// right sector) column slice times right^T, placed in the current twin's right-paired layout; blocks and
+// slices the ortho product does not reach stay zero
+std::vector<double> ortho_vector(const MPSTensor& twin, const MPSTensor& ortho_in, const BlockMatrix& left,
+                                 const BlockMatrix& right) {
+    MPSTensor ot = ortho_in;
+    ot.make_right_paired();
+    ProductBasis cur_pb(twin.phys, twin.right, true), ort_pb(ot.phys, ot.right, true);
+    std::vector<double> v;
+    for (std::size_t k = 0; k < twin.data.n_blocks(); ++k) {
+        const Q lc = twin.data.lc[k];
+        Mat blk(twin.data.b[k].r, twin.data.b[k].c);
+        const std::size_t jl = left.find(lc, lc), jo = ot.data.find(lc, lc);
+        if (jl < left.n_blocks() && jo < ot.data.n_blocks()) {
+            const Mat t = matmul(left.b[jl], ot.data.b[jo]);
+            for (std::size_t s = 0; s < twin.phys.size(); ++s) {
+                const Q ph = twin.phys[s].first, rc = lc + ph;
+                if (!twin.right.has(rc) || !ot.right.has(rc)) continue;
+                const std::size_t jr = right.find(rc, rc);
+                if (jr == right.n_blocks()) continue;
+                const std::size_t rs_c = twin.right.size_of_block(rc), rs_o = ot.right.size_of_block(rc);
+                for (std::size_t ss = 0; ss < twin.phys[s].second; ++ss) {
+                    const std::size_t oc = ort_pb(ph, rc) + ss * rs_o, cc = cur_pb(ph, rc) + ss * rs_c;
+                    Mat slice(t.r, rs_o);
+                    for (std::size_t j = 0; j < rs_o; ++j)
+                        for (std::size_t i = 0; i < t.r; ++i) slice(i, j) = t(i, oc + j);
+                    const Mat pr = matmul_nt(slice, right.b[jr]);
+                    for (std::size_t j = 0; j < rs_c; ++j)
+                        for (std::size_t i = 0; i < pr.r; ++i) blk(i, cc + j) = pr(i, j);
+                }
+            }
+        }
+        v.insert(v.end(), blk.d.begin(), blk.d.end());
+    }
+    return v;
+}
+
+namespace {
+// left_boundary_bm / right_boundary_bm (mp_tensors/mps.hpp:241-264): unit blocks of the end index
+BlockMatrix unit_boundary(const Index& i) {
+    BlockMatrix b;
+    for (std::size_t k = 0; k < i.size(); ++k) {
+        Mat m(i[k].second, i[k].second);
+        for (std::size_t d = 0; d < i[k].second; ++d) m(d, d) = 1.0;
+        b.insert(i[k].first, i[k].first, std::move(m));
+    }
+    return b;
+}
+}  // namespace
+
+void DMRG::set_ortho(std::vector<std::vector<MPSTensor>> states) {
+    for (auto& st : states)
+        if (int(st.size()) != L) throw std::runtime_error("set_ortho: an ortho state with the wrong length");
+    ortho_mps = std::move(states);
+    const std::size_t n = ortho_mps.size();
+    ortho_left_.assign(n, std::vector<BlockMatrix>(L + 1));
+    ortho_right_.assign(n, std::vector<BlockMatrix>(L + 1));
+    for (std::size_t o = 0; o < n; ++o) {
+        ortho_left_[o][0] = unit_boundary(mps[0].left);
+        ortho_right_[o][L] = unit_boundary(mps[L - 1].right);
+        for (int i = L - 1; i >= 0; --i) ortho_right_[o][i] = ortho_right_step(mps[i], ortho_mps[o][i], ortho_right_[o][i + 1]);
+    }
+}
+
 void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc, int stop_step,
                  std::vector<uint8_t>* snap) {
     energies.clear();
@@ -670,9 +790,15 @@ void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<Trunca
             hpsi_count++;
             hpsi_flops += sched->total_flops;
         };
+        // ortho vectors of this step (ts_optimize.hpp:217-223)
+        std::vector<std::vector<double>> ortho_vecs;
+        for (std::size_t o = 0; o < ortho_mps.size(); ++o) {
+            TwoSite ts_o(ortho_mps[o][site1], ortho_mps[o][site2]);
+            ortho_vecs.push_back(ortho_vector(twin, ts_o.make_mps(), ortho_left_[o][site1], ortho_right_[o][site2 + 1]));
+        }
         std::vector<double> xo;
         int iters = 0;
-        double E = jacobi_davidson(mult, x0, p.jcd_tol, p.jcd_maxiter, xo, iters, p.jcd_gmres);
+        double E = jacobi_davidson(mult, x0, p.jcd_tol, p.jcd_maxiter, xo, iters, p.jcd_gmres, ortho_vecs);
         jd_time += now_s() - t1;
         for (std::size_t k = 0; k < twin.data.n_blocks(); ++k)
             std::copy(xo.begin() + off[k], xo.begin() + off[k] + twin.data.b[k].d.size(), twin.data.b[k].d.begin());
@@ -699,6 +825,8 @@ void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<Trunca
             double t3 = now_s();
             trunc_time += t3 - t2;
             left_[site2] = overlap_mpo_left_step(mps[site1], mps[site1], left_[site1], mpo[site1], true);
+            for (std::size_t o = 0; o < ortho_mps.size(); ++o)
+                ortho_left_[o][site2] = ortho_left_step(mps[site1], ortho_mps[o][site1], ortho_left_[o][site1]);
             boundary_time += now_s() - t3;
         } else {
             if (p.heev) tst.predict_split_r2l(p.Mmax, p.cutoff, alpha, right_[site2 + 1], mpo[site2], mps[site1], mps[site2], tr);
@@ -708,6 +836,8 @@ void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<Trunca
             double t3 = now_s();
             trunc_time += t3 - t2;
             right_[site2] = overlap_mpo_right_step(mps[site2], mps[site2], right_[site2 + 1], mpo[site2], true);
+            for (std::size_t o = 0; o < ortho_mps.size(); ++o)
+                ortho_right_[o][site2] = ortho_right_step(mps[site2], ortho_mps[o][site2], ortho_right_[o][site2 + 1]);
             boundary_time += now_s() - t3;
         }
         trunc.push_back(tr);
@@ -802,6 +932,23 @@ std::vector<uint8_t> save_mps_tensor(const MPSTensor& m0) {
         for (double v : m.data.b[k].d) w.put<double>(v);
     }
     return w.b;
+}
+
+MPSTensor load_mps_tensor(const uint8_t* p, std::size_t n) {
+    R r{p, n};
+    if (r.get<uint32_t>() != 0x53504D51u || r.get<uint32_t>() != 1) throw std::runtime_error("bad MPS tensor blob");
+    MPSTensor m;
+    m.phys = r.idx(); m.left = r.idx(); m.right = r.idx();
+    m.pairing = RightPaired;
+    const uint32_t nb = r.get<uint32_t>();
+    for (uint32_t k = 0; k < nb; ++k) {
+        int a = r.get<int32_t>(), b = r.get<int32_t>();
+        uint32_t rows = r.get<uint32_t>(), cols = r.get<uint32_t>();
+        Mat x(rows, cols);
+        for (auto& v : x.d) v = r.get<double>();
+        m.data.insert(Q(a, b), Q(a, b), std::move(x));
+    }
+    return m;
 }
 
 std::vector<uint8_t> save_boundary_step(int side, int site, const MPSTensor& m0, const Boundary& in, const Boundary& out) {

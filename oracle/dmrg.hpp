@@ -82,6 +82,13 @@ struct DMRG {
     std::size_t hpsi_flops = 0;
 
     DMRG(std::vector<MPOTensor> mpo_single, int nup, int ndown, const DMRGParams& prm);
+    // excited states (ts_optimize.hpp:217-223, optimize.h:134-172): ortho states the solution is kept
+    // orthogonal to, and per state the overlap boundaries with the current MPS (rows current, columns
+    // ortho).  set_ortho expects the sweep to start (the MPS canonised to site 0) and builds the right
+    // boundaries.
+    std::vector<std::vector<MPSTensor>> ortho_mps;
+    std::vector<std::vector<BlockMatrix>> ortho_left_, ortho_right_;
+    void set_ortho(std::vector<std::vector<MPSTensor>> states);
     // one full two-site sweep (ts_optimize.hpp:114-362); energies per step.
     // If stop_step >= 0 the sweep stops before solving that step and the
     // frozen site problem is written to *snap.
@@ -95,6 +102,15 @@ void load_site_problem(const uint8_t* p, std::size_t n, MPSTensor& twin, Boundar
 
 // one site tensor ("QMPS" v1): Index phys, left, right; right-paired blocks as in QSPB
 std::vector<uint8_t> save_mps_tensor(const MPSTensor& m);
+MPSTensor load_mps_tensor(const uint8_t* p, std::size_t n);
+
+// overlap boundaries of the excited-state sweep (mp_tensors/mps.h:175-219), bra = the current MPS, ket =
+// an ortho state, and an ortho state's projection onto the current two-site basis in the twin's block
+// layout (contractions/special.hpp:38-62)
+BlockMatrix ortho_left_step(const MPSTensor& bra, const MPSTensor& ket, const BlockMatrix& left);
+BlockMatrix ortho_right_step(const MPSTensor& bra, const MPSTensor& ket, const BlockMatrix& right);
+std::vector<double> ortho_vector(const MPSTensor& twin, const MPSTensor& ortho_twin, const BlockMatrix& left,
+                                 const BlockMatrix& right);
 
 // boundary step case ("QBSP" v1): side (0 left, 1 right), site; the site tensor (right-paired,
 // same block layout as QSPB); the input boundary; the oracle's output boundary

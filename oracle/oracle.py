@@ -61,6 +61,7 @@ def lib(nthreads: int = 0):
         L.orc_jd_solve.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), c_size_t, P(c_double), c_int,
                                    c_int, c_double, c_int, P(c_double), P(c_double), P(c_int), P(c_int)]
         L.orc_dmrg_set_gmres.argtypes = [c_void_p, c_int]
+        L.orc_dmrg_set_ortho.argtypes = [c_void_p, c_int, P(c_void_p), P(c_size_t)]
         L.orc_heff_adjoint.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), P(c_double), c_size_t,
                                        P(c_double), P(c_double), c_size_t]
         U32 = P(ctypes.c_uint32)
@@ -135,6 +136,15 @@ class OracleDMRG:
         """twosite_truncation = heev (density matrix with noise) instead of svd."""
         self.lib.orc_dmrg_set_heev(self.h, 1 if heev else 0, alpha_initial, alpha_main, alpha_final, ngrowsweeps,
                                    nmainsweeps)
+
+    def set_ortho(self, states):
+        """Excited states: states = [[site blob ("QMPS", mps_export) for each site] per ortho state]; every
+        solution is kept orthogonal to them.  Call at the start of a sweep."""
+        blobs = [b for st in states for b in st]
+        bufs = [ctypes.create_string_buffer(b, len(b)) for b in blobs]
+        ptrs = (c_void_p * max(1, len(bufs)))(*[ctypes.cast(b, c_void_p) for b in bufs])
+        lens = (c_size_t * max(1, len(bufs)))(*[len(b) for b in blobs])
+        _check(self.lib, self.lib.orc_dmrg_set_ortho(self.h, len(states), ptrs, lens))
 
     def set_gmres(self, gmres: int):
         """ietl_jcd_gmres of the sweep's Jacobi-Davidson solves."""

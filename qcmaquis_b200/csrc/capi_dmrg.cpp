@@ -317,6 +317,61 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     QCM_CATCH
 }
 
+int qcm_dmrg_export_site(qcm_dmrg* d, int site, void* buf, size_t cap, size_t* len) {
+    QCM_TRY
+    if (!d || !len) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_export_site: NULL argument");
+    qcm::DevDMRG& e = *d->e;
+    if (site < 0 || site >= e.L) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_export_site: site out of range");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
+    const qcm::DMPS t = qcm::right_paired_copy(e.c, e.mps[std::size_t(site)]);
+    std::vector<double> h(t.b.total);
+    if (t.b.total)
+        QCM_CUDA(cudaMemcpyAsync(h.data(), t.b.d.get(), t.b.total * sizeof(double), cudaMemcpyDeviceToHost, e.c.s));
+    QCM_CUDA(cudaStreamSynchronize(e.c.s));
+    std::vector<uint8_t> w;
+    auto put = [&](const void* p, std::size_t n) { const uint8_t* b = static_cast<const uint8_t*>(p); w.insert(w.end(), b, b + n); };
+    auto u32 = [&](uint32_t v) { put(&v, 4); };
+    auto i32 = [&](int32_t v) { put(&v, 4); };
+    auto idx = [&](const qcm::Index& i) {
+        u32(uint32_t(i.size()));
+        for (auto& x : i.d) { i32(x.first.a); i32(x.first.b); u32(uint32_t(x.second)); }
+    };
+    u32(0x53504D51u);  // "QMPS"
+    u32(1);
+    idx(t.phys); idx(t.left); idx(t.right);
+    u32(uint32_t(t.b.n()));
+    for (std::size_t k = 0; k < t.b.n(); ++k) {
+        i32(t.b.lc[k].a); i32(t.b.lc[k].b); u32(t.b.rows[k]); u32(t.b.cols[k]);
+        put(h.data() + t.b.off[k], t.b.elems(k) * sizeof(double));
+    }
+    *len = w.size();
+    if (buf) {
+        if (cap < w.size()) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_export_site: buffer too small");
+        std::memcpy(buf, w.data(), w.size());
+    }
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_set_ortho(qcm_dmrg* d, int n_states, const qcm_mps_desc* sites, const double* const* data) {
+    QCM_TRY
+    if (!d || n_states < 0 || (n_states > 0 && (!sites || !data))) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_set_ortho: bad arguments");
+    qcm::DevDMRG& e = *d->e;
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
+    std::vector<std::vector<qcm::DMPS>> st(static_cast<std::size_t>(n_states));
+    for (int o = 0; o < n_states; ++o)
+        for (int i = 0; i < e.L; ++i) {
+            const std::size_t k = std::size_t(o) * e.L + i;
+            if (!data[k]) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_set_ortho: NULL site data");
+            st[o].push_back(upload_mps(e.c, &sites[k], data[k]));
+        }
+    e.set_ortho(std::move(st));
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_dmrg_length(const qcm_dmrg* d) { return d ? d->e->L : -1; }
 
 int qcm_dmrg_run(qcm_dmrg* d, int stop_step, double* energies, qcm_trunc_result* trunc, int* n_steps) {

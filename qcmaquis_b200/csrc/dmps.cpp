@@ -163,6 +163,17 @@ DMPS right_paired_copy(Ctx& c, const DMPS& t) {
     return o;
 }
 
+DMPS left_paired_copy(Ctx& c, const DMPS& t) {
+    if (t.right_paired) return reshaped_left(c, t);
+    DMPS o;
+    o.phys = t.phys; o.left = t.left; o.right = t.right; o.right_paired = false;
+    o.b.lc = t.b.lc; o.b.rc = t.b.rc; o.b.rows = t.b.rows; o.b.cols = t.b.cols; o.b.off = t.b.off; o.b.total = t.b.total;
+    o.b.allocate(c.s, false);
+    QCM_CUDA(cudaMemcpyAsync(o.b.d.get(), t.b.d.get(), std::max<uint64_t>(t.b.total, 1) * sizeof(double),
+                             cudaMemcpyDeviceToDevice, c.s));
+    return o;
+}
+
 double norm2(Ctx& c, const DBlocks& b) {
     if (!b.total) return 0.0;
     Ctx::ensure(c.scal, 64 + DOT_PARTS);

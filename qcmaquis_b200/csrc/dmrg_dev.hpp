@@ -117,6 +117,20 @@ DBlocks layout_left_paired(const Index& phys, const Index& left, const Index& ri
 void make_left_paired(Ctx& c, DMPS& t);
 void make_right_paired(Ctx& c, DMPS& t);
 DMPS right_paired_copy(Ctx& c, const DMPS& t);
+DMPS left_paired_copy(Ctx& c, const DMPS& t);
+
+// ---- excited states (mp_tensors/mps.h:175-219, contractions/special.hpp:38-62) ----
+// Overlap boundaries between the current MPS (bra) and an ortho state (ket): one block per charge,
+// rows on the bra's sector, columns on the ket's.
+// unit blocks of an end index (left_boundary_bm / right_boundary_bm, mps.hpp:241-264)
+DBlocks unit_blocks(Ctx& c, const Index& i);
+// overlap_left_step: bra left-paired, ket right-paired; returns the boundary one site further right
+DBlocks ortho_left_step(Ctx& c, const DMPS& bra, const DMPS& ket, const DBlocks& left);
+// overlap_right_step: bra right-paired, ket left-paired; returns the boundary one site further left
+DBlocks ortho_right_step(Ctx& c, const DMPS& bra, const DMPS& ket, const DBlocks& right);
+// site_ortho_boundaries: the ortho twin projected onto the current twin's basis, written to v (device,
+// twin.b.total doubles, the twin's right-paired block layout); zero where the ortho product has no block
+void ortho_vector(Ctx& c, const DMPS& twin, const DMPS& ortho_twin, const DBlocks& left, const DBlocks& right, double* v);
 double norm2(Ctx& c, const DBlocks& b);
 void scale(Ctx& c, DBlocks& b, double f);
 // normalize_left/right (mpstensor.hpp:242-300): QR / LQ per block; returns R / L as a block matrix
@@ -258,6 +272,13 @@ struct DevDMRG {
     // given MPS (right-normalised on sites 1 .. L-1, as after canonize(0))
     DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, std::vector<DMPS> sites,
             const DMRGParams& prm, cudaStream_t s);
+    // excited states (ts_optimize.hpp:217-223, optimize.h:134-172): ortho states in both pairings and
+    // their overlap boundaries with the current MPS
+    std::vector<std::vector<DMPS>> ortho_lp, ortho_rp;
+    std::vector<std::vector<DBlocks>> ortho_left_, ortho_right_;
+    // sets the ortho states (right-paired site tensors, one vector per state) at the start of a sweep
+    // and builds their right boundaries
+    void set_ortho(std::vector<std::vector<DMPS>> states_rp);
     int next_step = 0;  // step index (0 .. 2L-3) the sweep continues with
     int sweep_count = 0;  // completed sweeps
     void sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc);

@@ -384,6 +384,37 @@ void DevDMRG::init_boundaries() {
     QCM_CUDA(cudaStreamSynchronize(c.s));
 }
 
+void DevDMRG::set_ortho(std::vector<std::vector<DMPS>> states_rp) {
+    if (next_step != 0) throw std::runtime_error("DMRG: ortho states are set at the start of a sweep");
+    for (auto& st : states_rp) {
+        if (int(st.size()) != L) throw std::runtime_error("DMRG: an ortho state has the wrong length");
+        for (int i = 0; i < L; ++i)
+            if (!st[i].right_paired || !(st[i].phys == mps[i].phys)) throw std::runtime_error("DMRG: ortho state site tensor mismatch");
+        if (!(st[0].left == mps[0].left) || !(st[L - 1].right == mps[L - 1].right))
+            throw std::runtime_error("DMRG: ortho state with different end sectors");
+    }
+    ortho_rp = std::move(states_rp);
+    const std::size_t n = ortho_rp.size();
+    ortho_lp.clear();
+    ortho_lp.resize(n);
+    ortho_left_.clear();
+    ortho_left_.resize(n);
+    ortho_right_.clear();
+    ortho_right_.resize(n);
+    for (std::size_t o = 0; o < n; ++o) {
+        for (int i = 0; i < L; ++i) ortho_lp[o].push_back(left_paired_copy(c, ortho_rp[o][i]));
+        ortho_left_[o].resize(L + 1);
+        ortho_right_[o].resize(L + 1);
+        ortho_left_[o][0] = unit_blocks(c, mps[0].left);
+        ortho_right_[o][L] = unit_blocks(c, mps[L - 1].right);
+        for (int i = L - 1; i >= 0; --i) {
+            make_right_paired(c, mps[i]);
+            ortho_right_[o][i] = ortho_right_step(c, mps[i], ortho_lp[o][i], ortho_right_[o][i + 1]);
+        }
+    }
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+}
+
 void DevDMRG::step_sites(int _site, int& lr, int& site1, int& site2) const {
     const int site = (_site < L - 1) ? _site : 2 * L - 2 - _site;
     if (_site < L - 1) { lr = 1; site1 = site; site2 = site + 1; }
@@ -418,6 +449,20 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     int iters = 0, napply = 0;
     JDOptions jo;
     jo.gmres = p.jcd_gmres;
+    // ortho vectors of this step (ts_optimize.hpp:217-223)
+    DBuf<double> ovec;
+    if (!ortho_rp.empty()) {
+        const uint64_t nx = tst.twin.b.total;
+        ovec.alloc(ortho_rp.size() * (nx ? nx : 1));
+        for (std::size_t o = 0; o < ortho_rp.size(); ++o) {
+            DTwoSite tso;
+            tso.build(c, ortho_lp[o][site1], ortho_rp[o][site2]);
+            ortho_vector(c, tst.twin, tso.twin, ortho_left_[o][site1], ortho_right_[o][site2 + 1], ovec.get() + o * nx);
+        }
+        jo.ortho = ovec.get();
+        jo.n_ortho = int(ortho_rp.size());
+        jo.ortho_ld = nx;
+    }
     const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters, p.precision, &jo,
                                      &napply);
     QCM_CUDA(cudaStreamSynchronize(c.s));
@@ -448,6 +493,8 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         st.trunc_s += t3 - t2;
         DMPS ket = right_paired_copy(c, mps[site1]);
         left_[site2] = boundary_step_left(c, *left_[site1], ket, mps[site1], mpo[site1], true);
+        for (std::size_t o = 0; o < ortho_rp.size(); ++o)
+            ortho_left_[o][site2] = ortho_left_step(c, mps[site1], ortho_rp[o][site1], ortho_left_[o][site1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
         st.boundary_s += now_s() - t3;
     } else {
@@ -461,6 +508,8 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         t3_last = t3;
         st.trunc_s += t3 - t2;
         right_[site2] = boundary_step_right(c, *right_[site2 + 1], mps[site2], mpo[site2], true);
+        for (std::size_t o = 0; o < ortho_rp.size(); ++o)
+            ortho_right_[o][site2] = ortho_right_step(c, mps[site2], ortho_lp[o][site2], ortho_right_[o][site2 + 1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
         st.boundary_s += now_s() - t3;
     }

@@ -57,6 +57,8 @@ _lib._sig("qcm_dmrg_create", c_int, c_void_p, c_void_p, c_int, c_int, P(DMRGPara
 _lib._sig("qcm_dmrg_create_from_mps", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)),
           P(c_void_p))
 _lib._sig("qcm_dmrg_length", c_int, c_void_p)
+_lib._sig("qcm_dmrg_set_ortho", c_int, c_void_p, c_int, P(MPSDesc), P(P(c_double)))
+_lib._sig("qcm_dmrg_export_site", c_int, c_void_p, c_int, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
 _lib._sig("qcm_dmrg_run", c_int, c_void_p, c_int, P(c_double), P(TruncResult), P(c_int))
 _lib._sig("qcm_dmrg_next_step", c_int, c_void_p)
 _lib._sig("qcm_dmrg_pending_plan", c_int, c_void_p, P(c_double), c_uint64, P(c_void_p))
@@ -157,6 +159,23 @@ def boundary_step(ctx, B: Boundary, mpo, site: int, phys, left, right, data_rp: 
     return Boundary.from_handle(ctx, h)
 
 
+def _pack_sites(sites):
+    """MPS site tensors (dict(phys, left, right, blocks), right-paired blocks in left-sector order) as C-ABI
+    descriptors and data pointers; keep holds the arrays the pointers refer to."""
+    descs = (MPSDesc * len(sites))()
+    keep, ptrs = [], (P(c_double) * len(sites))()
+    for i, st in enumerate(sites):
+        if [tuple(b[0]) for b in st["blocks"]] != [tuple(x[:2]) for x in st["left"]]:
+            raise ValueError(f"site {i}: expected one right-paired block per left sector, in sector order")
+        ps, ls, rs = _sectors(st["phys"]), _sectors(st["left"]), _sectors(st["right"])
+        data = np.ascontiguousarray(np.concatenate([blk.T.ravel() for (_, blk) in st["blocks"]]))
+        keep += [ps, ls, rs, data]
+        descs[i].n_phys, descs[i].n_left, descs[i].n_right = len(st["phys"]), len(st["left"]), len(st["right"])
+        descs[i].phys, descs[i].left, descs[i].right = ps, ls, rs
+        ptrs[i] = _lib.dptr(data)
+    return descs, ptrs, keep
+
+
 class DMRG:
     """Two-site ground-state DMRG (TwoU1, init_state = const) with every step on the device."""
 
@@ -181,17 +200,7 @@ class DMRG:
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore, heev,
                     precision, jcd_gmres)
-        descs = (MPSDesc * len(sites))()
-        keep, ptrs = [], (P(c_double) * len(sites))()
-        for i, st in enumerate(sites):
-            if [tuple(b[0]) for b in st["blocks"]] != [tuple(x[:2]) for x in st["left"]]:
-                raise ValueError(f"site {i}: expected one right-paired block per left sector, in sector order")
-            ps, ls, rs = _sectors(st["phys"]), _sectors(st["left"]), _sectors(st["right"])
-            data = np.ascontiguousarray(np.concatenate([blk.T.ravel() for (_, blk) in st["blocks"]]))
-            keep += [ps, ls, rs, data]
-            descs[i].n_phys, descs[i].n_left, descs[i].n_right = len(st["phys"]), len(st["left"]), len(st["right"])
-            descs[i].phys, descs[i].left, descs[i].right = ps, ls, rs
-            ptrs[i] = _lib.dptr(data)
+        descs, ptrs, keep = _pack_sites(sites)
         h = c_void_p()
         check(lib.qcm_dmrg_create_from_mps(ctx.h, mpo.handle, ctypes.byref(p), descs, ptrs, ctypes.byref(h)),
               "qcm_dmrg_create_from_mps")
@@ -240,6 +249,24 @@ class DMRG:
         buf = ctypes.create_string_buffer(n.value)
         check(lib.qcm_dmrg_pending_export(self.h, fl, buf, n.value, ctypes.byref(n)), "qcm_dmrg_pending_export")
         return buf.raw
+
+    def export_mps(self):
+        """The current MPS as "QMPS" site blobs (right-paired; heff.parse_mps_tensor reads them)."""
+        out = []
+        for i in range(self.L):
+            n = ctypes.c_size_t()
+            check(lib.qcm_dmrg_export_site(self.h, i, None, 0, ctypes.byref(n)), "qcm_dmrg_export_site")
+            buf = ctypes.create_string_buffer(n.value)
+            check(lib.qcm_dmrg_export_site(self.h, i, buf, n.value, ctypes.byref(n)), "qcm_dmrg_export_site")
+            out.append(buf.raw)
+        return out
+
+    def set_ortho(self, states):
+        """Excited states: states = [[site dicts of an ortho state, as for from_mps]]; every step's solution
+        is kept orthogonal to their projections (ts_optimize.hpp:217-223).  Call at the start of a sweep."""
+        sites = [st for state in states for st in state]
+        descs, ptrs, keep = _pack_sites(sites)
+        check(lib.qcm_dmrg_set_ortho(self.h, len(states), descs, ptrs), "qcm_dmrg_set_ortho")
 
     def stats(self) -> dict:
         s = DMRGStats()
