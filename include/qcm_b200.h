@@ -330,6 +330,12 @@ int qcm_dmrg_set_ortho(qcm_dmrg* d, int n_states, const qcm_mps_desc* sites, con
  * buf == NULL for *len.  Between steps the MPS is the state the sweep has reached (checkpoints, ortho
  * states for a later excited-state run). */
 int qcm_dmrg_export_site(qcm_dmrg* d, int site, void* buf, size_t cap, size_t* len);
+/* Spin-summed one-particle density matrix of the current MPS, gamma[i + j*L] = <Psi| sum_s a+_is a_js |Psi>
+ * (L x L, symmetric; the oneptdm measurement, lib/interface/cpp_maquis.cpp:235-366), which is the energy
+ * derivative dE/dh_ij of the Hamiltonian sum_ij h_ij sum_s a+_is a_js + ... (Hellmann-Feynman).  Computed
+ * between sweeps as the expectation values of the one-body operators of h = e_ij + e_ji (their QC MPOs,
+ * bond dimension <= 6) through left boundary steps over the whole MPS: L(L+1)/2 contractions. */
+int qcm_dmrg_measure_1rdm(qcm_dmrg* d, double* gamma);
 /* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL); only
  * between sweeps (see qcm_dmrg_run). */
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);

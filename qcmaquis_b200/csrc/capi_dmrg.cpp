@@ -1,3 +1,4 @@
+#include <algorithm>
 // C-ABI: Jacobi-Davidson solve, boundary steps, boundary download and the two-site sweep.
 #include <cstring>
 #include <memory>
@@ -313,6 +314,30 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     d->ctx = ctx;
     d->e = std::make_unique<qcm::DevDMRG>(m.t, ts.t, std::move(ms), p, ctx->stream);
     *out = d.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_measure_1rdm(qcm_dmrg* d, double* gamma) {
+    QCM_TRY
+    if (!d || !gamma) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_measure_1rdm: NULL argument");
+    qcm::DevDMRG& e = *d->e;
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
+    const int L = e.L;
+    std::vector<double> h(std::size_t(L) * L, 0.0), V(std::size_t(L) * L * L * L, 0.0);
+    for (int i = 0; i < L; ++i)
+        for (int j = i; j < L; ++j) {
+            // the one-body operator sum_s (a+_is a_js + a+_js a_is) as the QC MPO of h = e_ij + e_ji, V = 0
+            std::fill(h.begin(), h.end(), 0.0);
+            h[std::size_t(i) + std::size_t(j) * L] = 1.0;
+            h[std::size_t(j) + std::size_t(i) * L] = 1.0;
+            const qcm::MPO O = qcm::build_qc_mpo(L, h.data(), V.data(), 1e-20);
+            const double x = e.expectation(O.t);
+            const double g = i == j ? x : 0.5 * x;
+            gamma[std::size_t(i) + std::size_t(j) * L] = g;
+            gamma[std::size_t(j) + std::size_t(i) * L] = g;
+        }
     return QCM_OK;
     QCM_CATCH
 }

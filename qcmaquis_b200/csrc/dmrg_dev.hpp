@@ -279,6 +279,9 @@ struct DevDMRG {
     // sets the ortho states (right-paired site tensors, one vector per state) at the start of a sweep
     // and builds their right boundaries
     void set_ortho(std::vector<std::vector<DMPS>> states_rp);
+    // <Psi|W|Psi> / <Psi|Psi> of the current MPS between sweeps (the MPS canonised to site 0) for an MPO W
+    // of the same physical basis: left boundary steps through every site
+    double expectation(const std::vector<MPOTensor>& W);
     int next_step = 0;  // step index (0 .. 2L-3) the sweep continues with
     int sweep_count = 0;  // completed sweeps
     void sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc);

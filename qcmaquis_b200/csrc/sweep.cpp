@@ -415,6 +415,31 @@ void DevDMRG::set_ortho(std::vector<std::vector<DMPS>> states_rp) {
     QCM_CUDA(cudaStreamSynchronize(c.s));
 }
 
+double DevDMRG::expectation(const std::vector<MPOTensor>& W) {
+    if (next_step != 0) throw std::runtime_error("DMRG: expectation values are taken between sweeps");
+    if (int(W.size()) != L) throw std::runtime_error("DMRG: operator MPO of the wrong length");
+    std::unique_ptr<DevBoundary> B = trivial_boundary(mps[0].left, W[0].rows, c.s);
+    for (int k = 0; k < L; ++k) {
+        if (!(W[k].phys == mps[k].phys)) throw std::runtime_error("DMRG: operator MPO with another physical basis");
+        make_left_paired(c, mps[k]);
+        DMPS ket = right_paired_copy(c, mps[k]);
+        B = boundary_step_left(c, *B, ket, mps[k], W[k], true);
+    }
+    // the last boundary: one cohort (the end sector, dimension 1) with W[L-1].cols = 1 block of 1 x 1
+    const BoundaryIndexH& x = B->idx;
+    if (x.n_cohorts() != 1 || x.aux != 1 || x.lsz[0] != 1 || x.rsz[0] != 1 || x.offsets[0] < 0)
+        throw std::runtime_error("DMRG: unexpected final boundary of an expectation value");
+    const uint64_t at = x.data_off[0] + uint64_t(x.offsets[0]);
+    if (at >= B->data.size()) throw std::runtime_error("DMRG: final boundary outside its buffer");
+    double v = 0.0;
+    QCM_CUDA(cudaMemcpyAsync(&v, B->data.get() + at, sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    // sites 1 .. L-1 are right-normalised between sweeps: the norm lives in site 0
+    const double n2 = norm2(c, mps[0].b);
+    if (!(n2 > 0.0)) throw std::runtime_error("DMRG: zero state");
+    return v / n2;
+}
+
 void DevDMRG::step_sites(int _site, int& lr, int& site1, int& site2) const {
     const int site = (_site < L - 1) ? _site : 2 * L - 2 - _site;
     if (_site < L - 1) { lr = 1; site1 = site; site2 = site + 1; }

@@ -59,6 +59,7 @@ _lib._sig("qcm_dmrg_create_from_mps", c_int, c_void_p, c_void_p, P(DMRGParams), 
 _lib._sig("qcm_dmrg_length", c_int, c_void_p)
 _lib._sig("qcm_dmrg_set_ortho", c_int, c_void_p, c_int, P(MPSDesc), P(P(c_double)))
 _lib._sig("qcm_dmrg_export_site", c_int, c_void_p, c_int, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
+_lib._sig("qcm_dmrg_measure_1rdm", c_int, c_void_p, P(c_double))
 _lib._sig("qcm_dmrg_run", c_int, c_void_p, c_int, P(c_double), P(TruncResult), P(c_int))
 _lib._sig("qcm_dmrg_next_step", c_int, c_void_p)
 _lib._sig("qcm_dmrg_pending_plan", c_int, c_void_p, P(c_double), c_uint64, P(c_void_p))
@@ -260,6 +261,12 @@ class DMRG:
             check(lib.qcm_dmrg_export_site(self.h, i, buf, n.value, ctypes.byref(n)), "qcm_dmrg_export_site")
             out.append(buf.raw)
         return out
+
+    def measure_1rdm(self) -> np.ndarray:
+        """Spin-summed one-particle density matrix (L x L) of the current MPS, between sweeps."""
+        g = np.zeros((self.L, self.L))
+        check(lib.qcm_dmrg_measure_1rdm(self.h, _lib.dptr(g)), "qcm_dmrg_measure_1rdm")
+        return g  # symmetric: column-major and row-major agree
 
     def set_ortho(self, states):
         """Excited states: states = [[site dicts of an ortho state, as for from_mps]]; every step's solution
