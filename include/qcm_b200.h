@@ -336,6 +336,12 @@ int qcm_dmrg_export_site(qcm_dmrg* d, int site, void* buf, size_t cap, size_t* l
  * between sweeps as the expectation values of the one-body operators of h = e_ij + e_ji (their QC MPOs,
  * bond dimension <= 6) through left boundary steps over the whole MPS: L(L+1)/2 contractions. */
 int qcm_dmrg_measure_1rdm(qcm_dmrg* d, double* gamma);
+/* Two-body energy gradient of the current MPS (the twoptdm measurement in the form the integrals enter):
+ * G[p + q L + r L^2 + s L^3] (L^4 doubles) with E_2 = sum_pqrs V_pqrs G_pqrs for every V of the 8-fold
+ * symmetry of real (pq|rs), i.e. dE/dV_pqrs; G is 1/2 the spin-summed two-particle density matrix
+ * symmetrised over the 8 index permutations.  One expectation value per unique integral (the QC MPO of
+ * the integral's orbit): about L^4 / 8 contractions, for small and moderate L. */
+int qcm_dmrg_measure_2rdm_grad(qcm_dmrg* d, double* G);
 /* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL); only
  * between sweeps (see qcm_dmrg_run). */
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);

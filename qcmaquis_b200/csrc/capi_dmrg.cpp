@@ -342,6 +342,39 @@ int qcm_dmrg_measure_1rdm(qcm_dmrg* d, double* gamma) {
     QCM_CATCH
 }
 
+int qcm_dmrg_measure_2rdm_grad(qcm_dmrg* d, double* G) {
+    QCM_TRY
+    if (!d || !G) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_measure_2rdm_grad: NULL argument");
+    qcm::DevDMRG& e = *d->e;
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
+    const int L = e.L;
+    const std::size_t L2 = std::size_t(L) * L;
+    auto at = [&](int p, int q, int r, int t) { return std::size_t(p) + std::size_t(q) * L + std::size_t(r) * L2 + std::size_t(t) * L2 * L; };
+    std::vector<double> h(L2, 0.0), V(L2 * L2, 0.0);
+    // one orbit of index quadruples per unique integral (pq|rs), p >= q, r >= s, (p,q) >= (r,s)
+    for (int p = 0; p < L; ++p)
+        for (int q = 0; q <= p; ++q)
+            for (int r = 0; r <= p; ++r)
+                for (int t = 0; t <= r; ++t) {
+                    if (r == p && t > q) continue;
+                    const int orb[8][4] = {{p, q, r, t}, {q, p, r, t}, {p, q, t, r}, {q, p, t, r},
+                                           {r, t, p, q}, {t, r, p, q}, {r, t, q, p}, {t, r, q, p}};
+                    std::vector<std::size_t> pos;
+                    for (const auto& o : orb) {
+                        const std::size_t k = at(o[0], o[1], o[2], o[3]);
+                        if (std::find(pos.begin(), pos.end(), k) == pos.end()) pos.push_back(k);
+                    }
+                    std::fill(V.begin(), V.end(), 0.0);
+                    for (std::size_t k : pos) V[k] = 1.0;
+                    const qcm::MPO O = qcm::build_qc_mpo(L, h.data(), V.data(), 1e-20);
+                    const double x = e.expectation(O.t) / double(pos.size());
+                    for (std::size_t k : pos) G[k] = x;
+                }
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_dmrg_export_site(qcm_dmrg* d, int site, void* buf, size_t cap, size_t* len) {
     QCM_TRY
     if (!d || !len) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_export_site: NULL argument");

@@ -60,6 +60,7 @@ _lib._sig("qcm_dmrg_length", c_int, c_void_p)
 _lib._sig("qcm_dmrg_set_ortho", c_int, c_void_p, c_int, P(MPSDesc), P(P(c_double)))
 _lib._sig("qcm_dmrg_export_site", c_int, c_void_p, c_int, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
 _lib._sig("qcm_dmrg_measure_1rdm", c_int, c_void_p, P(c_double))
+_lib._sig("qcm_dmrg_measure_2rdm_grad", c_int, c_void_p, P(c_double))
 _lib._sig("qcm_dmrg_run", c_int, c_void_p, c_int, P(c_double), P(TruncResult), P(c_int))
 _lib._sig("qcm_dmrg_next_step", c_int, c_void_p)
 _lib._sig("qcm_dmrg_pending_plan", c_int, c_void_p, P(c_double), c_uint64, P(c_void_p))
@@ -267,6 +268,12 @@ class DMRG:
         g = np.zeros((self.L, self.L))
         check(lib.qcm_dmrg_measure_1rdm(self.h, _lib.dptr(g)), "qcm_dmrg_measure_1rdm")
         return g  # symmetric: column-major and row-major agree
+
+    def measure_2rdm_grad(self) -> np.ndarray:
+        """dE/dV_pqrs (L^4, [p, q, r, s]) of the current MPS for 8-fold symmetric integrals, between sweeps."""
+        G = np.zeros(self.L ** 4)
+        check(lib.qcm_dmrg_measure_2rdm_grad(self.h, _lib.dptr(G)), "qcm_dmrg_measure_2rdm_grad")
+        return G.reshape((self.L,) * 4, order="F")
 
     def set_ortho(self, states):
         """Excited states: states = [[site dicts of an ortho state, as for from_mps]]; every step's solution
