@@ -293,7 +293,14 @@ typedef struct {
     int32_t hpsi_precision;       /* QCM_PRECISION_FP64, or QCM_PRECISION_MIXED: JD with the mixed H.psi
                                      and an FP64 Rayleigh quotient of each step's final vector */
     int32_t jcd_gmres;            /* ietl_jcd_gmres (0..64): GMRES iterations per JD correction */
+    int32_t optimization;         /* QCM_OPTIMIZATION_TWOSITE (ts_optimize) or QCM_OPTIMIZATION_SINGLESITE
+                                     (ss_optimize.hpp:59-186: 2L steps per sweep, sites 0 .. L-1 then
+                                     L-1 .. 0, each solved with the single-site MPO tensor and grown by
+                                     the density-matrix prediction with noise alpha_*; twosite_truncation
+                                     does not apply) */
 } qcm_dmrg_params;
+#define QCM_OPTIMIZATION_TWOSITE 0
+#define QCM_OPTIMIZATION_SINGLESITE 1
 /* block_matrix_algorithms.h:48-63 */
 typedef struct {
     uint64_t bond_dimension;
@@ -316,6 +323,8 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
 int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* params, const qcm_mps_desc* sites,
                              const double* const* data, qcm_dmrg** out);
 int qcm_dmrg_length(const qcm_dmrg* d);
+/* Steps of one sweep: 2L - 2 (two-site) or 2L (single-site). */
+int qcm_dmrg_steps_per_sweep(const qcm_dmrg* d);
 /* Excited states (ts_optimize.hpp:217-223, optimize.h:134-172): n_states ortho states (for example
  * converged lower states), each given as L site tensors sites[o*L + i] / data[o*L + i] (right-paired, as
  * for qcm_dmrg_create_from_mps; same physical basis and end sectors as the DMRG state).  From then on
@@ -342,17 +351,19 @@ int qcm_dmrg_measure_1rdm(qcm_dmrg* d, double* gamma);
  * symmetrised over the 8 index permutations.  One expectation value per unique integral (the QC MPO of
  * the integral's orbit): about L^4 / 8 contractions, for small and moderate L. */
 int qcm_dmrg_measure_2rdm_grad(qcm_dmrg* d, double* G);
-/* One sweep (2L - 2 steps): energies[2L-2], trunc[2L-2] (may be NULL); only
- * between sweeps (see qcm_dmrg_run). */
+/* One sweep (qcm_dmrg_steps_per_sweep steps: 2L - 2 two-site, 2L single-site): energies[steps],
+ * trunc[steps] (may be NULL); only between sweeps (see qcm_dmrg_run).  Single-site steps that end a
+ * half-sweep (site L-1 left to right, site 0 right to left) canonise without truncation and report
+ * zero truncation results. */
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);
 int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* stats);
-/* Run the current sweep up to (not including) step stop_step (2L - 2 completes
- * it); energies / trunc receive one entry per step run (may be NULL), *n_steps
- * their count. */
+/* Run the current sweep up to (not including) step stop_step (steps_per_sweep
+ * completes it); energies / trunc receive one entry per step run (may be NULL),
+ * *n_steps their count. */
 int qcm_dmrg_run(qcm_dmrg* d, int stop_step, double* energies, qcm_trunc_result* trunc, int* n_steps);
-/* Step index (0 .. 2L-3) the current sweep continues with. */
+/* Step index (0 .. steps_per_sweep - 1) the current sweep continues with. */
 int qcm_dmrg_next_step(const qcm_dmrg* d);
-/* H_eff plan of the pending step (its boundaries are the sweep's own: the plan
+/* (Two-site sweeps.)  H_eff plan of the pending step (its boundaries are the sweep's own: the plan
  * is valid until the sweep continues) and, if twin != NULL, its start vector
  * (vec_len doubles, cap = buffer length).  Replaces the snapshot of the site
  * problem that ts_optimize hands to solve_site_problem (ts_optimize.hpp:185-240). */

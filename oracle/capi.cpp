@@ -116,13 +116,21 @@ int orc_dmrg_set_ortho(orc_dmrg* h, int n_states, const void* const* blobs, cons
 }
 
 // ietl_jcd_gmres of the sweep's solves
+// optimization = singlesite (1) or twosite (0); a sweep then has 2L (or 2L - 2) steps
+int orc_dmrg_set_single_site(orc_dmrg* h, int on) {
+    h->d->p.single_site = on != 0;
+    return 0;
+}
+
+int orc_dmrg_steps_per_sweep(orc_dmrg* h) { return h->d->steps_per_sweep(); }
+
 int orc_dmrg_set_gmres(orc_dmrg* h, int gmres) {
     if (gmres < 0) return fail("orc_dmrg_set_gmres: gmres < 0");
     h->d->p.jcd_gmres = gmres;
     return 0;
 }
 
-// energies/tw/tf/bond: arrays of 2L-2.  If stop_step >= 0, the frozen site problem of
+// energies/tw/tf/bond: arrays of steps_per_sweep.  If stop_step >= 0, the frozen site problem of
 // that step is returned in *snap (free with orc_free) and the sweep stops there.
 int orc_dmrg_sweep(orc_dmrg* h, int sweep, double* energies, double* tw, double* tf, uint64_t* bond, int stop_step,
                    void** snap, size_t* snap_len) {

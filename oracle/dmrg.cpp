@@ -365,6 +365,51 @@ void TwoSite::predict_split_r2l(std::size_t Mmax, double cutoff, double alpha, c
     m1.phys = phys1; m1.left = left; m1.right = V.right_basis(); m1.pairing = LeftPaired; m1.data = V;
 }
 
+TruncationResults grow_l2r(MPSTensor& a, MPSTensor& b, const Boundary& left, const MPOTensor& mpo, double alpha,
+                           double cutoff, std::size_t Mmax) {
+    a.make_left_paired();
+    // alpha_dm (prediction.hpp:41-55): a a^T per right sector, then the noise term
+    BlockMatrix dm;
+    for (std::size_t k = 0; k < a.data.n_blocks(); ++k) dm.insert(a.data.lc[k], a.data.rc[k], matmul_nt(a.data.b[k], a.data.b[k]));
+    alpha_dm_direct(a, left, mpo, dm, alpha);
+    BlockMatrix U;
+    TruncationResults tr = heev_truncate(dm, U, cutoff, Mmax);
+    BlockMatrix t;  // U^T a: kept states x old right sector
+    for (std::size_t k = 0; k < U.n_blocks(); ++k) {
+        const std::size_t j = a.data.find(U.lc[k], U.rc[k]);
+        t.insert(U.rc[k], a.data.rc[j], matmul_tn(U.b[k], a.data.b[j]));
+    }
+    multiply_from_left(b, t);
+    a.data = U;
+    a.right = U.right_basis();
+    return tr;
+}
+
+TruncationResults grow_r2l(MPSTensor& a, MPSTensor& b, const Boundary& right, const MPOTensor& mpo, double alpha,
+                           double cutoff, std::size_t Mmax) {
+    a.make_right_paired();
+    // alpha_dm_right (prediction.hpp:57-71): a^T a per left sector, then the noise term
+    BlockMatrix dm;
+    for (std::size_t k = 0; k < a.data.n_blocks(); ++k) dm.insert(a.data.lc[k], a.data.rc[k], matmul_tn(a.data.b[k], a.data.b[k]));
+    alpha_dm_direct_right(a, right, mpo, dm, alpha);
+    BlockMatrix U;
+    TruncationResults tr = heev_truncate(dm, U, cutoff, Mmax);
+    BlockMatrix t, Ut;  // a U: old left sector x kept states; U^T the new right-paired site tensor
+    for (std::size_t k = 0; k < U.n_blocks(); ++k) {
+        const std::size_t j = a.data.find(U.lc[k], U.rc[k]);
+        t.insert(a.data.lc[j], U.rc[k], matmul(a.data.b[j], U.b[k]));
+        const Mat& u = U.b[k];
+        Mat ut(u.c, u.r);
+        for (std::size_t c = 0; c < u.c; ++c)
+            for (std::size_t r = 0; r < u.r; ++r) ut(c, r) = u(r, c);
+        Ut.insert(U.rc[k], U.lc[k], std::move(ut));
+    }
+    multiply_from_right(b, t);
+    a.data = Ut;
+    a.left = Ut.left_basis();
+    return tr;
+}
+
 BlockMatrix normalize_left(MPSTensor& t) {
     t.make_left_paired();
     BlockMatrix Qm, R;
@@ -749,8 +794,91 @@ void DMRG::set_ortho(std::vector<std::vector<MPSTensor>> states) {
     }
 }
 
+void DMRG::sweep_single(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc) {
+    energies.clear();
+    trunc.clear();
+    for (int _site = 0; _site < 2 * L; ++_site) {
+        const int lr = _site < L ? 1 : -1;
+        const int site = _site < L ? _site : 2 * L - 1 - _site;  // to_site (ss_optimize.hpp:57-62)
+        MPSTensor& x = mps[site];
+        x.make_right_paired();
+        // solve_site_problem with the single-site MPO (ss_optimize.hpp:120)
+        double t0 = now_s();
+        auto sched = create_contraction_schedule(x, left_[site], right_[site + 1], mpo[site]);
+        double t1 = now_s();
+        schedule_time += t1 - t0;
+        std::vector<std::size_t> off;
+        std::size_t tot = 0;
+        for (auto& b : x.data.b) { off.push_back(tot); tot += b.d.size(); }
+        std::vector<double> x0(tot);
+        for (std::size_t k = 0; k < x.data.n_blocks(); ++k) std::copy(x.data.b[k].d.begin(), x.data.b[k].d.end(), x0.begin() + off[k]);
+        auto mult = [&](const std::vector<double>& in, std::vector<double>& out) {
+            double h0 = now_s();
+            std::vector<const double*> xv(x.left.size(), nullptr);
+            std::vector<double*> yv(x.left.size(), nullptr);
+            std::fill(out.begin(), out.end(), 0.0);
+            for (std::size_t lb = 0; lb < x.left.size(); ++lb) {
+                std::size_t k = x.data.find(x.left[lb].first, x.left[lb].first);
+                if (k == x.data.n_blocks()) continue;
+                xv[lb] = in.data() + off[k];
+                yv[lb] = out.data() + off[k];
+            }
+            super_hamil_mv(*sched, left_[site], right_[site + 1], xv, yv);
+            hpsi_time += now_s() - h0;
+            hpsi_count++;
+            hpsi_flops += sched->total_flops;
+        };
+        // ortho vectors (ss_optimize.hpp:104-109)
+        std::vector<std::vector<double>> ortho_vecs;
+        for (std::size_t o = 0; o < ortho_mps.size(); ++o) {
+            MPSTensor ot = ortho_mps[o][site];
+            ot.make_right_paired();
+            ortho_vecs.push_back(ortho_vector(x, ot, ortho_left_[o][site], ortho_right_[o][site + 1]));
+        }
+        std::vector<double> xo;
+        int iters = 0;
+        double E = jacobi_davidson(mult, x0, p.jcd_tol, p.jcd_maxiter, xo, iters, p.jcd_gmres, ortho_vecs);
+        jd_time += now_s() - t1;
+        for (std::size_t k = 0; k < x.data.n_blocks(); ++k)
+            std::copy(xo.begin() + off[k], xo.begin() + off[k] + x.data.b[k].d.size(), x.data.b[k].d.begin());
+        energies.push_back(E + p.ecore);
+        // alpha, cutoff and Mmax of this sweep (ss_optimize.hpp:143-155)
+        const double alpha = sweep_no < p.ngrowsweeps ? p.alpha_initial
+                             : (sweep_no < p.ngrowsweeps + p.nmainsweeps ? p.alpha_main : p.alpha_final);
+        TruncationResults tr;
+        double t2 = now_s();
+        if (lr == 1) {
+            // ss_optimize.hpp:158-173
+            if (site < L - 1) tr = grow_l2r(x, mps[site + 1], left_[site], mpo[site], alpha, p.cutoff, p.Mmax);
+            else normalize_left(x);
+            double t3 = now_s();
+            trunc_time += t3 - t2;
+            left_[site + 1] = overlap_mpo_left_step(x, x, left_[site], mpo[site], true);
+            for (std::size_t o = 0; o < ortho_mps.size(); ++o)
+                ortho_left_[o][site + 1] = ortho_left_step(x, ortho_mps[o][site], ortho_left_[o][site]);
+            boundary_time += now_s() - t3;
+        } else {
+            // ss_optimize.hpp:174-186
+            if (site > 0) tr = grow_r2l(x, mps[site - 1], right_[site + 1], mpo[site], alpha, p.cutoff, p.Mmax);
+            else normalize_right(x);
+            double t3 = now_s();
+            trunc_time += t3 - t2;
+            right_[site] = overlap_mpo_right_step(x, x, right_[site + 1], mpo[site], true);
+            for (std::size_t o = 0; o < ortho_mps.size(); ++o)
+                ortho_right_[o][site] = ortho_right_step(x, ortho_mps[o][site], ortho_right_[o][site + 1]);
+            boundary_time += now_s() - t3;
+        }
+        trunc.push_back(tr);
+    }
+}
+
 void DMRG::sweep(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc, int stop_step,
                  std::vector<uint8_t>* snap) {
+    if (p.single_site) {
+        if (stop_step >= 0) throw std::runtime_error("DMRG: site-problem snapshots of two-site sweeps only");
+        sweep_single(sweep_no, energies, trunc);
+        return;
+    }
     energies.clear();
     trunc.clear();
     for (int _site = 0; _site < 2 * L - 2; ++_site) {

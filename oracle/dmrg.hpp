@@ -69,7 +69,20 @@ struct DMRGParams {
     bool heev = false;
     double alpha_initial = 1e-2, alpha_main = 1e-4, alpha_final = 1e-8;
     int ngrowsweeps = 0, nmainsweeps = 0;
+    // optimization = singlesite (ss_optimize.hpp:59-186): 2L steps per sweep, every step grown by the
+    // density-matrix prediction with the alpha above
+    bool single_site = false;
 };
+
+// grow_l2r_sweep / grow_r2l_sweep (contractions/engine.hpp:85-123): the optimised site tensor a is
+// replaced by the kept eigenvectors of its reduced density matrix plus alpha times the boundary noise
+// (predict_new_state_*_sweep, contractions/boundary_ops/prediction.hpp:77-131), and the neighbour b takes
+// the projection of the old a onto them (predict_lanczos_*_sweep, :93-148).  l2r: a left-paired result,
+// b = (U^T a) b; r2l: a = U^T right-paired, b = b (a U).
+TruncationResults grow_l2r(MPSTensor& a, MPSTensor& b, const Boundary& left, const MPOTensor& mpo, double alpha,
+                           double cutoff, std::size_t Mmax);
+TruncationResults grow_r2l(MPSTensor& a, MPSTensor& b, const Boundary& right, const MPOTensor& mpo, double alpha,
+                           double cutoff, std::size_t Mmax);
 
 struct DMRG {
     int L;
@@ -94,6 +107,9 @@ struct DMRG {
     // frozen site problem is written to *snap.
     void sweep(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc, int stop_step = -1,
                std::vector<uint8_t>* snap = nullptr);
+    // one single-site sweep (ss_optimize.hpp:59-186): sites 0 .. L-1 left to right, then L-1 .. 0
+    void sweep_single(int sweep_no, std::vector<double>& energies, std::vector<TruncationResults>& trunc);
+    int steps_per_sweep() const { return p.single_site ? 2 * L : 2 * L - 2; }
 };
 
 // frozen site problem ("QSPB" v1): twin MPS (right-paired) + L + R boundaries

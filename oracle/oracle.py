@@ -61,6 +61,8 @@ def lib(nthreads: int = 0):
         L.orc_jd_solve.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), c_size_t, P(c_double), c_int,
                                    c_int, c_double, c_int, P(c_double), P(c_double), P(c_int), P(c_int)]
         L.orc_dmrg_set_gmres.argtypes = [c_void_p, c_int]
+        L.orc_dmrg_set_single_site.argtypes = [c_void_p, c_int]
+        L.orc_dmrg_steps_per_sweep.argtypes = [c_void_p]
         L.orc_dmrg_set_ortho.argtypes = [c_void_p, c_int, P(c_void_p), P(c_size_t)]
         L.orc_heff_adjoint.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), P(c_double), c_size_t,
                                        P(c_double), P(c_double), c_size_t]
@@ -97,8 +99,13 @@ class OracleDMRG:
                                                   ctypes.byref(h)))
         self.h = h
 
+    def set_single_site(self, on: bool = True):
+        """optimization = singlesite (ss_optimize): 2L steps per sweep, each grown by the density-matrix
+        prediction with the noise of set_heev's alphas."""
+        _check(self.lib, self.lib.orc_dmrg_set_single_site(self.h, 1 if on else 0))
+
     def sweep(self, sweep: int = 0):
-        n = 2 * self.L - 2
+        n = self.lib.orc_dmrg_steps_per_sweep(self.h)
         E, tw, tf = np.zeros(n), np.zeros(n), np.zeros(n)
         bd = np.zeros(n, dtype=np.uint64)
         _check(self.lib, self.lib.orc_dmrg_sweep(self.h, sweep, _dp(E), _dp(tw), _dp(tf),

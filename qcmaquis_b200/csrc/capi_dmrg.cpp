@@ -234,6 +234,32 @@ int qcm_boundary_download(const qcm_boundary* b, qcm_sector* bra, qcm_sector* ke
     QCM_CATCH
 }
 
+namespace {
+// qcm_dmrg_params -> DMRGParams; returns an error message for values outside their ranges
+const char* to_params(const qcm_dmrg_params& prm, qcm::DMRGParams& p) {
+    if (prm.hpsi_precision < QCM_PRECISION_FP64 || prm.hpsi_precision > QCM_PRECISION_MIXED_TC)
+        return "qcm_dmrg: unknown hpsi_precision";
+    if (prm.optimization != QCM_OPTIMIZATION_TWOSITE && prm.optimization != QCM_OPTIMIZATION_SINGLESITE)
+        return "qcm_dmrg: optimization must be QCM_OPTIMIZATION_TWOSITE or QCM_OPTIMIZATION_SINGLESITE";
+    p.Mmax = prm.max_bond_dimension;
+    p.init_bond_dimension = prm.init_bond_dimension;
+    p.cutoff = prm.truncation_cutoff;
+    p.jcd_tol = prm.jcd_tol;
+    p.jcd_maxiter = prm.jcd_maxiter;
+    p.jcd_gmres = prm.jcd_gmres;
+    p.ecore = prm.ecore;
+    p.heev = prm.twosite_truncation == 1;
+    p.alpha_initial = prm.alpha_initial;
+    p.alpha_main = prm.alpha_main;
+    p.alpha_final = prm.alpha_final;
+    p.ngrowsweeps = prm.ngrowsweeps;
+    p.nmainsweeps = prm.nmainsweeps;
+    p.precision = prm.hpsi_precision;
+    p.single_site = prm.optimization == QCM_OPTIMIZATION_SINGLESITE;
+    return nullptr;
+}
+}  // namespace
+
 int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const qcm_dmrg_params* prm, qcm_dmrg** out) {
     QCM_TRY
     if (!ctx || !mpo || !prm || !out) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create: NULL argument");
@@ -249,22 +275,7 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
     QCM_CUDA(cudaSetDevice(ctx->device));
     qcm::AllocStream scope(ctx->stream);
     qcm::DMRGParams p;
-    p.Mmax = prm->max_bond_dimension;
-    p.init_bond_dimension = prm->init_bond_dimension;
-    p.cutoff = prm->truncation_cutoff;
-    p.jcd_tol = prm->jcd_tol;
-    p.jcd_maxiter = prm->jcd_maxiter;
-    p.jcd_gmres = prm->jcd_gmres;
-    p.ecore = prm->ecore;
-    p.heev = prm->twosite_truncation == 1;
-    p.alpha_initial = prm->alpha_initial;
-    p.alpha_main = prm->alpha_main;
-    p.alpha_final = prm->alpha_final;
-    p.ngrowsweeps = prm->ngrowsweeps;
-    p.nmainsweeps = prm->nmainsweeps;
-    if (prm->hpsi_precision < QCM_PRECISION_FP64 || prm->hpsi_precision > QCM_PRECISION_MIXED_TC)
-        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg: unknown hpsi_precision");
-    p.precision = prm->hpsi_precision;
+    if (const char* err = to_params(*prm, p)) return qcm::fail(QCM_ERR_ARG, err);
     qcm::MPO ts = qcm::make_twosite_mpo(m);
     auto d = std::make_unique<qcm_dmrg>();
     d->ctx = ctx;
@@ -286,22 +297,7 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     QCM_CUDA(cudaSetDevice(ctx->device));
     qcm::AllocStream scope(ctx->stream);
     qcm::DMRGParams p;
-    p.Mmax = prm->max_bond_dimension;
-    p.init_bond_dimension = prm->init_bond_dimension;
-    p.cutoff = prm->truncation_cutoff;
-    p.jcd_tol = prm->jcd_tol;
-    p.jcd_maxiter = prm->jcd_maxiter;
-    p.jcd_gmres = prm->jcd_gmres;
-    p.ecore = prm->ecore;
-    p.heev = prm->twosite_truncation == 1;
-    p.alpha_initial = prm->alpha_initial;
-    p.alpha_main = prm->alpha_main;
-    p.alpha_final = prm->alpha_final;
-    p.ngrowsweeps = prm->ngrowsweeps;
-    p.nmainsweeps = prm->nmainsweeps;
-    if (prm->hpsi_precision < QCM_PRECISION_FP64 || prm->hpsi_precision > QCM_PRECISION_MIXED_TC)
-        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg: unknown hpsi_precision");
-    p.precision = prm->hpsi_precision;
+    if (const char* err = to_params(*prm, p)) return qcm::fail(QCM_ERR_ARG, err);
     qcm::Ctx tmp;
     tmp.s = ctx->stream;
     std::vector<qcm::DMPS> ms;
@@ -431,6 +427,8 @@ int qcm_dmrg_set_ortho(qcm_dmrg* d, int n_states, const qcm_mps_desc* sites, con
 }
 
 int qcm_dmrg_length(const qcm_dmrg* d) { return d ? d->e->L : -1; }
+
+int qcm_dmrg_steps_per_sweep(const qcm_dmrg* d) { return d ? d->e->steps_per_sweep() : -1; }
 
 int qcm_dmrg_run(qcm_dmrg* d, int stop_step, double* energies, qcm_trunc_result* trunc, int* n_steps) {
     QCM_TRY

@@ -664,3 +664,116 @@ TruncResults DTwoSite::predict_split(Ctx& c, bool l2r, uint64_t Mmax, double cut
 }
 
 }  // namespace qcm
+
+namespace qcm {
+
+// ---------------------------------------------------------------------------
+// single-site growth (contractions/engine.hpp:85-123, boundary_ops/prediction.hpp:41-148)
+TruncResults grow_l2r(Ctx& c, DMPS& a, DMPS& b, const DevBoundary& L, const MPOTensor& W, double alpha, uint64_t Mmax,
+                      double cutoff) {
+    make_left_paired(c, a);
+    const std::size_t nb = a.b.n();
+    // alpha_dm: a a^T per right sector, plus alpha times the noise of the left boundary step
+    DBlocks dm;
+    std::vector<GemmJob> jobs;
+    for (std::size_t k = 0; k < nb; ++k) {
+        const uint32_t m = a.b.rows[k], n = a.b.cols[k];
+        dm.add(a.b.rc[k], a.b.rc[k], m, m);
+        GemmJob g{};
+        g.a_off = a.b.off[k]; g.lda = m; g.b_off = a.b.off[k]; g.ldb = m; g.tb = 1;
+        g.M = m; g.N = m; g.K = n; g.c_off = dm.off.back(); g.ldc = m; g.alpha = 1.0; g.beta = 0.0;
+        jobs.push_back(g);
+    }
+    dm.allocate(c.s, true);
+    batched_gemm(jobs, a.b.d.get(), a.b.total, a.b.d.get(), a.b.total, dm.d.get(), dm.total, c.gjobs, c.gtiles, c.s);
+    {
+        DMPS ket = right_paired_copy(c, a);
+        lbtm_accumulate(c, L, ket, a, W, dm, alpha);
+    }
+    BlockHeev hv = heev_truncate(c, dm, Mmax, cutoff);
+    // new a = U (kept eigenvectors, descending); t = U^T a_old (kept x old right sector)
+    DMPS u;
+    u.phys = a.phys; u.left = a.left; u.right_paired = false;
+    DBlocks t;
+    std::vector<std::pair<Charge, std::size_t>> kept;
+    std::vector<CopyJob> cj;
+    std::vector<GemmJob> gj;
+    for (std::size_t k = 0; k < nb; ++k) {
+        const uint32_t kp = hv.keep[k];
+        if (!kp) continue;
+        const uint32_t n = dm.rows[k], cols = a.b.cols[k];
+        kept.push_back({a.b.rc[k], kp});
+        u.b.add(a.b.rc[k], a.b.rc[k], n, kp);
+        t.add(a.b.rc[k], a.b.rc[k], kp, cols);
+        cj.push_back(CopyJob{dm.off[k] + uint64_t(n - kp) * n, u.b.off.back(), n, kp, n, n, 0, 1});
+        GemmJob g{};
+        g.a_off = u.b.off.back(); g.ta = 1; g.lda = n;
+        g.b_off = a.b.off[k]; g.ldb = n;
+        g.c_off = t.off.back(); g.ldc = kp;
+        g.M = kp; g.N = cols; g.K = n; g.alpha = 1.0; g.beta = 0.0;
+        gj.push_back(g);
+    }
+    u.right = sorted_basis(kept);
+    u.b.allocate(c.s, true);
+    t.allocate(c.s, true);
+    batched_copy(cj, dm.d.get(), dm.total, u.b.d.get(), u.b.total, c.cjobs, c.s);
+    batched_gemm(gj, u.b.d.get(), u.b.total, a.b.d.get(), a.b.total, t.d.get(), t.total, c.gjobs, c.gtiles, c.s);
+    multiply_from_left(c, b, t);
+    a = std::move(u);
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    return hv.tr;
+}
+
+TruncResults grow_r2l(Ctx& c, DMPS& a, DMPS& b, const DevBoundary& R, const MPOTensor& W, double alpha, uint64_t Mmax,
+                      double cutoff) {
+    make_right_paired(c, a);
+    const std::size_t nb = a.b.n();
+    // alpha_dm_right: a^T a per left sector, plus alpha times the noise of the right boundary step
+    DBlocks dm;
+    std::vector<GemmJob> jobs;
+    for (std::size_t k = 0; k < nb; ++k) {
+        const uint32_t m = a.b.rows[k], n = a.b.cols[k];
+        dm.add(a.b.lc[k], a.b.lc[k], n, n);
+        GemmJob g{};
+        g.a_off = a.b.off[k]; g.lda = m; g.b_off = a.b.off[k]; g.ldb = m; g.ta = 1;
+        g.M = n; g.N = n; g.K = m; g.c_off = dm.off.back(); g.ldc = n; g.alpha = 1.0; g.beta = 0.0;
+        jobs.push_back(g);
+    }
+    dm.allocate(c.s, true);
+    batched_gemm(jobs, a.b.d.get(), a.b.total, a.b.d.get(), a.b.total, dm.d.get(), dm.total, c.gjobs, c.gtiles, c.s);
+    rbtm_accumulate(c, R, a, W, dm, alpha);
+    BlockHeev hv = heev_truncate(c, dm, Mmax, cutoff);
+    // new a = U^T (right-paired, kept x phys.right); t = a_old U (old left sector x kept)
+    DMPS u;
+    u.phys = a.phys; u.right = a.right; u.right_paired = true;
+    DBlocks t;
+    std::vector<std::pair<Charge, std::size_t>> kept;
+    std::vector<CopyJob> cj;
+    std::vector<GemmJob> gj;
+    for (std::size_t k = 0; k < nb; ++k) {
+        const uint32_t kp = hv.keep[k];
+        if (!kp) continue;
+        const uint32_t n = dm.rows[k], rows = a.b.rows[k];
+        kept.push_back({a.b.lc[k], kp});
+        u.b.add(a.b.lc[k], a.b.lc[k], kp, n);
+        t.add(a.b.lc[k], a.b.lc[k], rows, kp);
+        cj.push_back(CopyJob{dm.off[k] + uint64_t(n - kp) * n, u.b.off.back(), n, kp, n, kp, 1, 1});
+        GemmJob g{};
+        g.a_off = a.b.off[k]; g.lda = rows;
+        g.b_off = u.b.off.back(); g.tb = 1; g.ldb = kp;
+        g.c_off = t.off.back(); g.ldc = rows;
+        g.M = rows; g.N = kp; g.K = n; g.alpha = 1.0; g.beta = 0.0;
+        gj.push_back(g);
+    }
+    u.left = sorted_basis(kept);
+    u.b.allocate(c.s, true);
+    t.allocate(c.s, true);
+    batched_copy(cj, dm.d.get(), dm.total, u.b.d.get(), u.b.total, c.cjobs, c.s);
+    batched_gemm(gj, a.b.d.get(), a.b.total, u.b.d.get(), u.b.total, t.d.get(), t.total, c.gjobs, c.gtiles, c.s);
+    multiply_from_right(c, b, t);
+    a = std::move(u);
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    return hv.tr;
+}
+
+}  // namespace qcm

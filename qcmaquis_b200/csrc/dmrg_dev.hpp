@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <memory>
 #include <vector>
 
@@ -185,6 +186,17 @@ struct DTwoSite {
                                const MPOTensor& W, DMPS& m1, DMPS& m2);
 };
 
+// Single-site growth (grow_l2r_sweep / grow_r2l_sweep, contractions/engine.hpp:85-123): the optimised
+// site tensor a becomes the kept eigenvectors of its reduced density matrix plus alpha times the boundary
+// noise (predict_new_state_*_sweep, contractions/boundary_ops/prediction.hpp:77-131; L = left boundary of
+// a's site for l2r, R = right boundary of the site after a for r2l, W = a's MPO tensor), and the
+// neighbour b takes the projection of the old a (predict_lanczos_*_sweep, :93-148): l2r a = U
+// (left-paired), b = (U^T a) b; r2l a = U^T (right-paired), b = b (a U).
+TruncResults grow_l2r(Ctx& c, DMPS& a, DMPS& b, const DevBoundary& L, const MPOTensor& W, double alpha, uint64_t Mmax,
+                      double cutoff);
+TruncResults grow_r2l(Ctx& c, DMPS& a, DMPS& b, const DevBoundary& R, const MPOTensor& W, double alpha, uint64_t Mmax,
+                      double cutoff);
+
 // Jacobi-Davidson for the lowest eigenpair (solve_ietl_jcd, solver/ietl_jacobi_davidson.h:35-76;
 // ietl/jacobi.h:386-474): x (device, plan vector layout) holds the start vector and receives the
 // eigenvector.
@@ -248,6 +260,9 @@ struct DMRGParams {
     double alpha_initial = 1e-2, alpha_main = 1e-4, alpha_final = 1e-8;
     int ngrowsweeps = 0, nmainsweeps = 0;
     int precision = 0;  // H.psi form of the JD (QCM_PRECISION_*); mixed: FP64 Rayleigh quotient per step
+    // optimization = singlesite (ss_optimize.hpp:59-186): 2L steps per sweep over sites 0 .. L-1, L-1 .. 0,
+    // each solved with the single-site MPO tensor and grown with the alphas above (heev does not apply)
+    bool single_site = false;
 };
 
 struct DMRGStats {
@@ -282,7 +297,8 @@ struct DevDMRG {
     // <Psi|W|Psi> / <Psi|Psi> of the current MPS between sweeps (the MPS canonised to site 0) for an MPO W
     // of the same physical basis: left boundary steps through every site
     double expectation(const std::vector<MPOTensor>& W);
-    int next_step = 0;  // step index (0 .. 2L-3) the sweep continues with
+    int next_step = 0;  // step index (0 .. steps_per_sweep() - 1) the sweep continues with
+    int steps_per_sweep() const { return p.single_site ? 2 * L : 2 * L - 2; }
     int sweep_count = 0;  // completed sweeps
     void sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc);
     // run the current sweep up to (not including) step `stop`; appends energies / truncations
@@ -297,6 +313,10 @@ struct DevDMRG {
   private:
     void init_boundaries();
     void step(int step, double& energy, TruncResults& tr);
+    void step_single(int step, double& energy, TruncResults& tr);
+    int last_iters = 0;  // JD iterations of the last step
+    // JD of one step's plan with this object's ortho vectors (built by make_ortho) and its statistics
+    double solve(HeffPlan& plan, DMPS& x, const std::function<void(std::size_t, double*)>& make_ortho);
 };
 
 }  // namespace qcm

@@ -327,6 +327,25 @@ DMPS const_tensor(Ctx& c, const Index& sd, const Index& ld, const Index& rd, dou
     for (std::size_t k = 0; k < t.b.n(); ++k) dev_fill(t.b.d.get() + t.b.off[k], t.b.elems(k), val, c.s);
     return t;
 }
+// a right-paired site tensor in the packed block layout of the H_eff vector
+DMPS packed_right(Ctx& c, const DMPS& t) {
+    if (!t.right_paired) throw std::runtime_error("DMRG: expected a right-paired site tensor");
+    DMPS o;
+    o.phys = t.phys; o.left = t.left; o.right = t.right; o.right_paired = true;
+    o.b = layout_right_paired(t.phys, t.left, t.right, true);
+    o.b.allocate(c.s, true);
+    std::vector<CopyJob> cj;
+    for (std::size_t k = 0; k < o.b.n(); ++k) {
+        const std::size_t ks = t.b.find_l(o.b.lc[k]);
+        if (ks == t.b.n()) continue;
+        if (t.b.rows[ks] != o.b.rows[k] || t.b.cols[ks] != o.b.cols[k])
+            throw std::runtime_error("DMRG: site tensor block differs from its right-paired layout");
+        cj.push_back(CopyJob{t.b.off[ks], o.b.off[k], o.b.rows[k], o.b.cols[k], t.b.rows[ks], o.b.rows[k], 0, 0});
+    }
+    if (cj.size() != t.b.n()) throw std::runtime_error("DMRG: site tensor has blocks outside its indices");
+    if (!cj.empty()) batched_copy(cj, t.b.d.get(), t.b.total, o.b.d.get(), o.b.total, c.cjobs, c.s);
+    return o;
+}
 }  // namespace
 
 DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, int nup, int ndown,
@@ -446,6 +465,34 @@ void DevDMRG::step_sites(int _site, int& lr, int& site1, int& site2) const {
     else { lr = -1; site1 = site - 1; site2 = site; }
 }
 
+double DevDMRG::solve(HeffPlan& plan, DMPS& x, const std::function<void(std::size_t, double*)>& make_ortho) {
+    const double t1 = now_s();
+    int iters = 0, napply = 0;
+    JDOptions jo;
+    jo.gmres = p.jcd_gmres;
+    // ortho vectors of this step (ts_optimize.hpp:217-223, ss_optimize.hpp:104-109)
+    DBuf<double> ovec;
+    if (!ortho_rp.empty()) {
+        const uint64_t nx = x.b.total;
+        ovec.alloc(ortho_rp.size() * (nx ? nx : 1));
+        for (std::size_t o = 0; o < ortho_rp.size(); ++o) make_ortho(o, ovec.get() + o * nx);
+        jo.ortho = ovec.get();
+        jo.n_ortho = int(ortho_rp.size());
+        jo.ortho_ld = nx;
+    }
+    const double E = jacobi_davidson(c, plan, x.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters, p.precision, &jo, &napply);
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    st.jd_s += now_s() - t1;
+    st.hpsi_count += uint64_t(napply);
+    st.hpsi_flops += double(napply) * plan.flops;
+    if (p.precision != 0) {
+        st.hpsi_count64 += 1;  // the FP64 Rayleigh-quotient apply
+        st.hpsi_flops64 += plan.flops;
+    }
+    last_iters = iters;
+    return E;
+}
+
 void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     int lr, site1, site2;
     step_sites(_site, lr, site1, site2);
@@ -471,34 +518,12 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     QCM_CUDA(cudaStreamSynchronize(c.s));
     const double t1 = now_s();
     st.plan_s += t1 - t0;
-    int iters = 0, napply = 0;
-    JDOptions jo;
-    jo.gmres = p.jcd_gmres;
-    // ortho vectors of this step (ts_optimize.hpp:217-223)
-    DBuf<double> ovec;
-    if (!ortho_rp.empty()) {
-        const uint64_t nx = tst.twin.b.total;
-        ovec.alloc(ortho_rp.size() * (nx ? nx : 1));
-        for (std::size_t o = 0; o < ortho_rp.size(); ++o) {
-            DTwoSite tso;
-            tso.build(c, ortho_lp[o][site1], ortho_rp[o][site2]);
-            ortho_vector(c, tst.twin, tso.twin, ortho_left_[o][site1], ortho_right_[o][site2 + 1], ovec.get() + o * nx);
-        }
-        jo.ortho = ovec.get();
-        jo.n_ortho = int(ortho_rp.size());
-        jo.ortho_ld = nx;
-    }
-    const double E = jacobi_davidson(c, *plan, tst.twin.b.d.get(), p.jcd_tol, p.jcd_maxiter, iters, p.precision, &jo,
-                                     &napply);
-    QCM_CUDA(cudaStreamSynchronize(c.s));
+    const double E = solve(*plan, tst.twin, [&](std::size_t o, double* v) {
+        DTwoSite tso;
+        tso.build(c, ortho_lp[o][site1], ortho_rp[o][site2]);
+        ortho_vector(c, tst.twin, tso.twin, ortho_left_[o][site1], ortho_right_[o][site2 + 1], v);
+    });
     const double t2 = now_s();
-    st.jd_s += t2 - t1;
-    st.hpsi_count += uint64_t(napply);
-    st.hpsi_flops += double(napply) * plan->flops;
-    if (p.precision != 0) {
-        st.hpsi_count64 += 1;  // the FP64 Rayleigh-quotient apply
-        st.hpsi_flops64 += plan->flops;
-    }
     plan.reset();
     tst.twin_to_both(c);
     mark(3);
@@ -542,32 +567,88 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         const double tend = now_s();
         std::fprintf(stderr,
                      "[step %d] twosite %.4f plan %.4f upload %.4f jd %.4f (%d) t2b %.4f svd %.4f qr %.4f bstep %.4f total %.4f\n",
-                     _site, tt[1] - tt[0], tt[2] - tt[1], t1 - tt[2], t2 - t1, iters, tt[3] - t2, tt[4] - tt[3],
+                     _site, tt[1] - tt[0], tt[2] - tt[1], t1 - tt[2], t2 - t1, last_iters, tt[3] - t2, tt[4] - tt[3],
                      t3_last - tt[4], tend - t3_last, tend - tt[0]);
     }
 }
 
+void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
+    // to_site (ss_optimize.hpp:57-62): sites 0 .. L-1 left to right, then L-1 .. 0
+    const int lr = _site < L ? 1 : -1;
+    const int site = _site < L ? _site : 2 * L - 1 - _site;
+    const double t0 = now_s();
+    make_right_paired(c, mps[site]);
+    DMPS x = packed_right(c, mps[site]);
+    // solve_site_problem with the single-site MPO tensor (ss_optimize.hpp:120)
+    auto plan = build_heff_plan(*left_[site], *right_[site + 1], mpo[site], x.phys, x.left, x.right, false);
+    plan->stream = c.s;
+    if (plan->x_len != x.b.total) throw std::runtime_error("DMRG: site tensor layout differs from the plan");
+    upload_plan(*plan);
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    st.plan_s += now_s() - t0;
+    const double E = solve(*plan, x, [&](std::size_t o, double* v) {
+        ortho_vector(c, x, ortho_rp[o][site], ortho_left_[o][site], ortho_right_[o][site + 1], v);
+    });
+    plan.reset();
+    mps[site] = std::move(x);
+    energy = E + p.ecore;
+    // alpha, cutoff and Mmax of this sweep (ss_optimize.hpp:143-155)
+    const double alpha = sweep_count < p.ngrowsweeps ? p.alpha_initial
+                         : (sweep_count < p.ngrowsweeps + p.nmainsweeps ? p.alpha_main : p.alpha_final);
+    tr = TruncResults();
+    const double t2 = now_s();
+    if (lr == 1) {
+        // ss_optimize.hpp:158-173
+        if (site < L - 1) tr = grow_l2r(c, mps[site], mps[site + 1], *left_[site], mpo[site], alpha, p.Mmax, p.cutoff);
+        else normalize_left(c, mps[site]);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        const double t3 = now_s();
+        st.trunc_s += t3 - t2;
+        DMPS ket = right_paired_copy(c, mps[site]);
+        left_[site + 1] = boundary_step_left(c, *left_[site], ket, mps[site], mpo[site], true);
+        for (std::size_t o = 0; o < ortho_rp.size(); ++o)
+            ortho_left_[o][site + 1] = ortho_left_step(c, mps[site], ortho_rp[o][site], ortho_left_[o][site]);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        st.boundary_s += now_s() - t3;
+    } else {
+        // ss_optimize.hpp:174-186
+        if (site > 0) tr = grow_r2l(c, mps[site], mps[site - 1], *right_[site + 1], mpo[site], alpha, p.Mmax, p.cutoff);
+        else normalize_right(c, mps[site]);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        const double t3 = now_s();
+        st.trunc_s += t3 - t2;
+        right_[site] = boundary_step_right(c, *right_[site + 1], mps[site], mpo[site], true);
+        for (std::size_t o = 0; o < ortho_rp.size(); ++o)
+            ortho_right_[o][site] = ortho_right_step(c, mps[site], ortho_lp[o][site], ortho_right_[o][site + 1]);
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        st.boundary_s += now_s() - t3;
+    }
+}
+
 void DevDMRG::run_until(int stop, std::vector<double>& energies, std::vector<TruncResults>& trunc) {
-    if (stop < next_step || stop > 2 * L - 2) throw std::runtime_error("DMRG: stop step outside the current sweep");
+    const int n = steps_per_sweep();
+    if (stop < next_step || stop > n) throw std::runtime_error("DMRG: stop step outside the current sweep");
     const double t_start = now_s();
     for (; next_step < stop; ++next_step) {
         double E = 0;
         TruncResults tr;
-        step(next_step, E, tr);
+        if (p.single_site) step_single(next_step, E, tr);
+        else step(next_step, E, tr);
         energies.push_back(E);
         trunc.push_back(tr);
     }
-    if (next_step == 2 * L - 2) { next_step = 0; ++sweep_count; }
+    if (next_step == n) { next_step = 0; ++sweep_count; }
     st.total_s += now_s() - t_start;
 }
 
 void DevDMRG::sweep(std::vector<double>& energies, std::vector<TruncResults>& trunc) {
     energies.clear();
     trunc.clear();
-    run_until(2 * L - 2, energies, trunc);
+    run_until(steps_per_sweep(), energies, trunc);
 }
 
 void DevDMRG::pending_twin(std::vector<double>& twin) {
+    if (p.single_site) throw std::runtime_error("DMRG: pending site problems of two-site sweeps only");
     int lr, site1, site2;
     step_sites(next_step, lr, site1, site2);
     make_left_paired(c, mps[site1]);
@@ -582,6 +663,7 @@ void DevDMRG::pending_twin(std::vector<double>& twin) {
 
 std::unique_ptr<HeffPlan> DevDMRG::pending_plan(std::vector<double>* twin, Index* phys_out, Index* left_out,
                                                 Index* right_out) {
+    if (p.single_site) throw std::runtime_error("DMRG: pending site problems of two-site sweeps only");
     int lr, site1, site2;
     step_sites(next_step, lr, site1, site2);
     make_left_paired(c, mps[site1]);

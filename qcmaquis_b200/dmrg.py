@@ -21,17 +21,24 @@ class DMRGParams(ctypes.Structure):
                 ("jcd_tol", c_double), ("jcd_maxiter", ctypes.c_int32), ("ecore", c_double),
                 ("twosite_truncation", ctypes.c_int32), ("alpha_initial", c_double), ("alpha_main", c_double),
                 ("alpha_final", c_double), ("ngrowsweeps", ctypes.c_int32), ("nmainsweeps", ctypes.c_int32),
-                ("hpsi_precision", ctypes.c_int32), ("jcd_gmres", ctypes.c_int32)]
+                ("hpsi_precision", ctypes.c_int32), ("jcd_gmres", ctypes.c_int32), ("optimization", ctypes.c_int32)]
 
 
-def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmres=0):
+OPTIMIZATION = {"twosite": 0, "singlesite": 1}
+
+
+def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmres=0, optimization="twosite"):
     """heev: None (svd truncation) or dict(alpha_initial, alpha_main, alpha_final, ngrowsweeps, nmainsweeps);
     precision: "fp64" or "mixed" (JD with the mixed H.psi and an FP64 Rayleigh quotient per step);
-    gmres: ietl_jcd_gmres, GMRES iterations per JD correction."""
+    gmres: ietl_jcd_gmres, GMRES iterations per JD correction;
+    optimization: "twosite" (ts_optimize) or "singlesite" (ss_optimize: the alphas of heev, or its defaults,
+    are the noise of every step's growth)."""
+    if optimization not in OPTIMIZATION:
+        raise ValueError(f"optimization must be one of {sorted(OPTIMIZATION)}")
     h = heev or {}
     return DMRGParams(M, init_bd, cutoff, tol, maxiter, ecore, 1 if heev else 0, h.get("alpha_initial", 1e-2),
                       h.get("alpha_main", 1e-4), h.get("alpha_final", 1e-8), h.get("ngrowsweeps", 0),
-                      h.get("nmainsweeps", 0), precision_mode(precision), gmres)
+                      h.get("nmainsweeps", 0), precision_mode(precision), gmres, OPTIMIZATION[optimization])
 
 
 class TruncResult(ctypes.Structure):
@@ -57,6 +64,7 @@ _lib._sig("qcm_dmrg_create", c_int, c_void_p, c_void_p, c_int, c_int, P(DMRGPara
 _lib._sig("qcm_dmrg_create_from_mps", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)),
           P(c_void_p))
 _lib._sig("qcm_dmrg_length", c_int, c_void_p)
+_lib._sig("qcm_dmrg_steps_per_sweep", c_int, c_void_p)
 _lib._sig("qcm_dmrg_set_ortho", c_int, c_void_p, c_int, P(MPSDesc), P(P(c_double)))
 _lib._sig("qcm_dmrg_export_site", c_int, c_void_p, c_int, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
 _lib._sig("qcm_dmrg_measure_1rdm", c_int, c_void_p, P(c_double))
@@ -179,40 +187,43 @@ def _pack_sites(sites):
 
 
 class DMRG:
-    """Two-site ground-state DMRG (TwoU1, init_state = const) with every step on the device."""
+    """Ground-state DMRG (TwoU1, init_state = const) with every step on the device: two-site sweeps
+    (ts_optimize) or single-site sweeps (ss_optimize, optimization="singlesite")."""
 
     def __init__(self, ctx, mpo, nup: int, ndown: int, max_bond_dimension: int, init_bond_dimension: int | None = None,
                  truncation_cutoff: float = 1e-16, jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0,
-                 heev: dict | None = None, precision="fp64", jcd_gmres: int = 0):
+                 heev: dict | None = None, precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite"):
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, init_bond_dimension or max_bond_dimension, truncation_cutoff, jcd_tol,
-                    jcd_maxiter, ecore, heev, precision, jcd_gmres)
+                    jcd_maxiter, ecore, heev, precision, jcd_gmres, optimization)
         h = c_void_p()
         check(lib.qcm_dmrg_create(ctx.h, mpo.handle, nup, ndown, ctypes.byref(p), ctypes.byref(h)), "qcm_dmrg_create")
         self.h = h
         self.L = lib.qcm_dmrg_length(h)
+        self.steps = lib.qcm_dmrg_steps_per_sweep(h)
 
     @classmethod
     def from_mps(cls, ctx, mpo, sites, max_bond_dimension: int, truncation_cutoff: float = 1e-16,
                  jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0, heev: dict | None = None,
-                 precision="fp64", jcd_gmres: int = 0):
+                 precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite"):
         """Restart from a given MPS: sites = [dict(phys, left, right, blocks)] with right-paired blocks
         (one per left sector, in sector order), sites 1 .. L-1 right-normalised."""
         self = cls.__new__(cls)
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore, heev,
-                    precision, jcd_gmres)
+                    precision, jcd_gmres, optimization)
         descs, ptrs, keep = _pack_sites(sites)
         h = c_void_p()
         check(lib.qcm_dmrg_create_from_mps(ctx.h, mpo.handle, ctypes.byref(p), descs, ptrs, ctypes.byref(h)),
               "qcm_dmrg_create_from_mps")
         self.h = h
         self.L = lib.qcm_dmrg_length(h)
+        self.steps = lib.qcm_dmrg_steps_per_sweep(h)
         return self
 
     def sweep(self):
-        """One sweep: (energies[2L-2], list of truncation dicts)."""
-        n = 2 * self.L - 2
+        """One sweep: (energies[steps], list of truncation dicts); steps = 2L - 2 (two-site) or 2L."""
+        n = self.steps
         E = np.zeros(n)
         tr = (TruncResult * n)()
         check(lib.qcm_dmrg_sweep(self.h, _lib.dptr(E), tr), "qcm_dmrg_sweep")
@@ -220,7 +231,7 @@ class DMRG:
 
     def run(self, stop_step: int):
         """Run the current sweep up to (not including) step stop_step: (energies, truncation dicts)."""
-        n = 2 * self.L - 2
+        n = self.steps
         E = np.zeros(n)
         tr = (TruncResult * n)()
         k = c_int()
