@@ -103,6 +103,22 @@ def test_device_single_site_reaches_fci(gpu_ctx):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("precision,gmres", [("mixed", 0), ("fp64", 4)])
+def test_device_single_site_forms(gpu_ctx, precision, gmres):
+    """The single-site sweep with the mixed H.psi (FP64 Rayleigh quotient per step) and with GMRES(4)
+    corrections: the FCI ground state to 1e-8."""
+    from qcmaquis_b200.dmrg import DMRG
+    L = L_SS
+    h, V, e, m, ts, blob = qc_system(L)
+    w = fci_levels(L)
+    d = DMRG(gpu_ctx, m, L // 2, L // 2, 64, init_bond_dimension=8, heev=NOISE, optimization="singlesite",
+             precision=precision, jcd_gmres=gmres)
+    for _ in range(8):
+        E, tr = d.sweep()
+    assert abs(E.min() - w[0]) < 1e-8, E.min() - w[0]
+
+
+@pytest.mark.gpu
 def test_device_single_site_excited_state_matches_oracle(gpu_ctx):
     """Single-site sweeps kept orthogonal to a ground state (ss_optimize.hpp:104-109): step energies equal
     the oracle's and converge to the first excited FCI level.  Near the chain's end the density matrix is
