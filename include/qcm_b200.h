@@ -67,6 +67,59 @@ int qcm_mpo_tensor_terms(const qcm_mpo* m, int site, uint32_t* b1, uint32_t* b2,
  * the MPO before the call keep their coefficients. */
 int qcm_mpo_set_scales(qcm_mpo* m, int site, const double* scale, uint64_t n);
 
+/* One MPO tensor as the reference's MPOTensor holds it (mp_tensors/mpotensor.h:46-135 with
+ * mpotensor_detail.h:141-186), in flat arrays:
+ *   rows, cols          row_dim() / col_dim();
+ *   terms               one per (b1, b2, operator) summand: row b1 < rows, column b2 < cols,
+ *                       operator index op < n_ops and its scale (the term_descriptor of
+ *                       at(b1, b2)); any order, several terms may share (b1, b2);
+ *   site operators      operator k has the entries op_ptr[k] .. op_ptr[k+1]-1, each
+ *                       <op_out|O|op_in> = op_val over the physical basis's flat states (state =
+ *                       first state of its sector + sub-index, sectors in phys order);
+ *   physical index      n_phys sectors (phys_charge[2*s], phys_charge[2*s+1]) = (N_up, N_down)
+ *                       of size phys_size[s], in strictly descending charge order;
+ *   Hermitian pairs     herm_left[b] (b < rows) / herm_right[b] (b < cols): the partner index of
+ *                       b, b itself for a self-adjoint index, or -1 (Hermitian::conj; bond
+ *                       properties leftBond().conj() / rightBond().conj()); phase_* the +-1 phase
+ *                       of the pair (Hermitian::phase).  NULL arrays mean no pairs on that bond.
+ * The two tensors on either side of a bond must give it the same dimension and pairs. */
+typedef struct qcm_mpo_tensor_desc {
+    uint32_t rows, cols;
+    uint64_t n_terms;
+    const uint32_t* b1;
+    const uint32_t* b2;
+    const uint32_t* op;
+    const double* scale;
+    uint32_t n_ops;
+    const uint64_t* op_ptr;
+    const uint32_t* op_in;
+    const uint32_t* op_out;
+    const double* op_val;
+    uint32_t n_phys;
+    const int32_t* phys_charge;
+    const uint32_t* phys_size;
+    const int32_t* herm_left;
+    const int32_t* phase_left;
+    const int32_t* herm_right;
+    const int32_t* phase_right;
+} qcm_mpo_tensor_desc;
+
+/* An MPO of `length` tensors to be filled by qcm_mpo_set_tensor (twosite != 0: the tensors are
+ * two-site tensors, as make_twosite_mpo returns them).  This is the seam through which a host
+ * code hands its own MPO<Matrix, SymmGroup> (mp_tensors/mpo.h) to this library, e.g. each tensor
+ * of ts_cache_mpo (optimize/ts_optimize.hpp:98-101) for the H_eff plans.  An unset tensor is an
+ * error when the MPO is used. */
+int qcm_mpo_create(int length, int twosite, qcm_mpo** out);
+/* Sets tensor `site` from d (copied; validated: indices in range, pairs symmetric
+ * (herm[herm[b]] == b), phases +-1, operator entries inside the physical basis). */
+int qcm_mpo_set_tensor(qcm_mpo* m, int site, const qcm_mpo_tensor_desc* d);
+/* rows, cols, operator count and physical sector count of tensor `site` (any may be NULL). */
+int qcm_mpo_tensor_info(const qcm_mpo* m, int site, uint32_t* rows, uint32_t* cols, uint32_t* n_ops, uint32_t* n_phys);
+/* Hermitian pairs and phases of tensor `site`'s left (rows entries) and right (cols entries)
+ * bonds, as described above (any may be NULL). */
+int qcm_mpo_tensor_hermitian(const qcm_mpo* m, int site, int32_t* herm_left, int32_t* phase_left, int32_t* herm_right,
+                             int32_t* phase_right);
+
 /* ------------------------------------------------------------------------ */
 /* Context, resident boundaries, H_eff plan                                   */
 /* ------------------------------------------------------------------------ */
@@ -125,6 +178,7 @@ typedef struct {
     uint64_t launches;                        /* own kernels launched per apply */
     uint64_t w_len;                           /* doubles of the dense coefficient blocks of the S build */
     double flops_sexec;                       /* tensor work the S-build tiles execute (padding included) */
+    uint64_t p_len;                           /* doubles of the L.S split-K partial tiles */
 } qcm_heff_info;
 
 #define QCM_PLAN_BOOKKEEPING 1 /* keep the (cohort, unit, line, alpha) list for parity checks */
@@ -194,15 +248,21 @@ void qcm_heff_free(qcm_heff* h);
  * allocator (a cudaMalloc here may fail or fragment it) or a solver loop that
  * must not stall on cudaFree's device-wide synchronisation -- this variant of
  * qcm_heff_apply_device calls no cudaMalloc/cudaFree and no allocating library
- * routine.  Its scratch (T slices, S, split-K partials) lives in one fixed
- * static device array of QCM_NOALLOC_SCRATCH_DOUBLES doubles (64 MiB), which
- * every GPU that loads this library holds until the process exits.  Plans
- * needing more scratch are rejected with QCM_ERR_ARG.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress) once;
- * make that first call before any stream capture.  All calls on a device share
- * the array and it keeps the last call's contents (S is cleared inside each
- * call): calls that overlap on the GPU -- other streams, other threads --
- * race.  Enqueued on the context stream (asynchronous). */
+ * routine.  It is the FP64 form only (QCM_PRECISION_FP64), whatever precision
+ * the plan's other applies use.  Its scratch (T slices, S, split-K partials,
+ * qcm_heff_info t_len + s_len + p_len, each rounded up to 32) lives in one
+ * fixed static device array of QCM_NOALLOC_SCRATCH_DOUBLES doubles (64 MiB),
+ * which every GPU that loads this library holds until the process exits.  Plans
+ * needing more scratch are rejected with QCM_ERR_ARG.  qcm_ctx_create looks the
+ * array's device address up on its device (cudaGetSymbolAddress, which also
+ * makes the device load the array): create the context before the host
+ * allocator reserves HBM and before any stream capture.  The address belongs to
+ * the context: after cudaDeviceReset the context and its plans are invalid.
+ * All calls on a device share the array and it keeps the last call's contents
+ * (S is cleared inside each call): calls that overlap on the GPU -- other
+ * streams, other threads -- race.  Makes the context's device current for the
+ * call and restores the caller's.  Enqueued on the context stream
+ * (asynchronous). */
 #define QCM_NOALLOC_SCRATCH_DOUBLES (8u * 1024u * 1024u)
 int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, double* y_dev);
 

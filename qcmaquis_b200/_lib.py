@@ -53,6 +53,23 @@ _sig("qcm_mpo_tensor_terms", c_int, c_void_p, c_int, P(ctypes.c_uint32), P(ctype
 _sig("qcm_mpo_set_scales", c_int, c_void_p, c_int, P(c_double), ctypes.c_uint64)
 
 
+class MPOTensorDesc(ctypes.Structure):
+    """qcm_mpo_tensor_desc"""
+    _fields_ = [("rows", c_uint32), ("cols", c_uint32), ("n_terms", c_uint64),
+                ("b1", P(c_uint32)), ("b2", P(c_uint32)), ("op", P(c_uint32)), ("scale", P(c_double)),
+                ("n_ops", c_uint32), ("op_ptr", P(c_uint64)), ("op_in", P(c_uint32)), ("op_out", P(c_uint32)),
+                ("op_val", P(c_double)), ("n_phys", c_uint32), ("phys_charge", P(ctypes.c_int32)),
+                ("phys_size", P(c_uint32)), ("herm_left", P(ctypes.c_int32)), ("phase_left", P(ctypes.c_int32)),
+                ("herm_right", P(ctypes.c_int32)), ("phase_right", P(ctypes.c_int32))]
+
+
+_sig("qcm_mpo_create", c_int, c_int, c_int, P(c_void_p))
+_sig("qcm_mpo_set_tensor", c_int, c_void_p, c_int, P(MPOTensorDesc))
+_sig("qcm_mpo_tensor_info", c_int, c_void_p, c_int, P(c_uint32), P(c_uint32), P(c_uint32), P(c_uint32))
+_sig("qcm_mpo_tensor_hermitian", c_int, c_void_p, c_int, P(ctypes.c_int32), P(ctypes.c_int32), P(ctypes.c_int32),
+     P(ctypes.c_int32))
+
+
 def dptr(a):
     """double* of a C-contiguous float64 numpy array."""
     return a.ctypes.data_as(P(c_double))

@@ -34,11 +34,14 @@ int qcm_ctx_create(int device, qcm_ctx** out) {
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return qcm::fail(QCM_ERR_NODEV, "no CUDA device (no CPU fallback)");
     if (device < 0 || device >= n) return qcm::fail(QCM_ERR_ARG, "qcm_ctx_create: bad device index");
     QCM_CUDA(cudaSetDevice(device));
-    auto* c = new qcm_ctx;
+    auto c = std::make_unique<qcm_ctx>();
     c->device = device;
+    // the allocation-free apply's array is loaded on this device now, not at its first call, so
+    // that its memory is taken before a host allocator reserves the rest of HBM
+    c->noalloc_scratch = qcm::noalloc_scratch_address();
     QCM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     qcm::register_stream(c->stream);
-    *out = c;
+    *out = c.release();
     return QCM_OK;
     QCM_CATCH
 }
@@ -177,6 +180,7 @@ int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info) {
     info->flops_sdense = p.flops_sdense;
     info->l_len = p.L ? p.L->idx.total : 0;
     info->r_len = p.R ? p.R->idx.total : 0;
+    info->p_len = p.p_len;
     return QCM_OK;
 }
 

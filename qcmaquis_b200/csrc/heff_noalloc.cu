@@ -5,13 +5,14 @@
 // hold nearly all of HBM, so a cudaMalloc here fails or fragments it), or an
 // inner solver loop that must not stall, since cudaFree synchronises the whole
 // device.  qcm_heff_apply_device_noalloc serves them.  It runs the same
-// T-GEMM -> S build -> split-K L.S kernels as qcm_heff_apply_device.  Its
-// scratch (T, S and the split-K partial tiles) is not the plan's buffers but
-// the fixed array below, which every GPU that loads this library holds until
-// the process exits.
+// T-GEMM -> S build -> split-K L.S kernels as qcm_heff_apply_device (FP64).
+// Its scratch (T, S and the split-K partial tiles) is not the plan's buffers
+// but the fixed array below, which every GPU that loads this library holds
+// until the process exits.  Each context looks the array's device address up
+// when it is created (qcm_ctx_create), so the apply itself does no set-up.
 #include <cuda_runtime.h>
 
-#include <mutex>
+#include <string>
 
 #include "../../include/qcm_b200.h"
 #include "capi_types.hpp"
@@ -24,26 +25,35 @@ namespace {
 // QCM_NOALLOC_SCRATCH_DOUBLES doubles (64 MiB), shared by every call on a device.
 static __device__ __align__(256) double g_noalloc_scratch[QCM_NOALLOC_SCRATCH_DOUBLES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double* g_scratch_ptr[kMaxDevices] = {};
+}  // namespace
 
-// Device address of the scratch array on the current device, looked up once per
-// device (the array's host-side name is only a stand-in, never a device address).
-double* scratch_for_current_device() {
-    int dev = 0;
-    QCM_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) throw std::runtime_error("qcm_heff_apply_device_noalloc: device index out of range");
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_ptr[dev]) {
-        void* ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess)
-            throw qcm::cuda_error(std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
-        g_scratch_ptr[dev] = static_cast<double*>(ptr);
-    }
-    return g_scratch_ptr[dev];
+namespace qcm {
+
+// The array's host-side name is only a stand-in: its device address on the current device comes
+// from cudaGetSymbolAddress, which loads this file's module there if it is not loaded yet.
+double* noalloc_scratch_address() {
+    void* ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) throw cuda_error(std::string("cudaGetSymbolAddress(noalloc scratch): ") + cudaGetErrorString(e));
+    return static_cast<double*>(ptr);
 }
+
+}  // namespace qcm
+
+namespace {
+
+// makes a device current for one call and gives the caller's back
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        QCM_CUDA(cudaGetDevice(&prev));
+        if (prev != dev) QCM_CUDA(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 
 uint64_t round32(uint64_t n) { return (n + 31) / 32 * 32; }
 
@@ -60,8 +70,9 @@ extern "C" int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, d
                                           " scratch doubles, the fixed array holds " +
                                           std::to_string(uint64_t(QCM_NOALLOC_SCRATCH_DOUBLES)) +
                                           "; use qcm_heff_apply_device for this plan");
-    QCM_CUDA(cudaSetDevice(h->ctx->device));
-    double* base = scratch_for_current_device();
+    if (!h->ctx->noalloc_scratch) return qcm::fail(QCM_ERR_INTERNAL, "qcm_heff_apply_device_noalloc: context without scratch address");
+    DeviceGuard dg(h->ctx->device);
+    double* base = h->ctx->noalloc_scratch;
     double* Tb = base;
     double* Sb = Tb + round32(p.t_len);
     double* Pb = Sb + round32(p.s_len);

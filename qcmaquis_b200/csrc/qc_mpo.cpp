@@ -248,6 +248,44 @@ struct Builder {
         }
     }
 
+    // Hermitian conjugate of an interned local operator: the id of its normalised
+    // transpose and the sign that normalisation took out (false: not in the table)
+    bool conj_op(uint32_t id, uint32_t& cid, int& sign) const {
+        const Mat4& M = ops.mats[id];
+        Mat4 t;
+        for (int o = 0; o < 4; ++o)
+            for (int i = 0; i < 4; ++i) t[o * 4 + i] = M[i * 4 + o];
+        int f = -1;
+        for (int k = 0; k < 16; ++k) if (t[k] != 0.0) { f = k; break; }
+        if (f < 0) return false;
+        sign = t[f] > 0 ? 1 : -1;
+        if (sign < 0) for (auto& x : t) x = -x;
+        auto it = ops.ids.find(t);
+        if (it == ops.ids.end()) return false;
+        cid = it->second;
+        return true;
+    }
+
+    // Conjugate of an L or R key: every (site, operator) pair replaced by the operator's
+    // transpose.  The bond operator of the conjugate key is the adjoint of this key's up to
+    // the product of the normalisation signs over the key's own sites, on both sides of the
+    // bond (the coefficients of conjugate terms carry the same signs), which is the phase.
+    bool conj_key(uint64_t key, uint64_t& ckey, int& phase) const {
+        const uint64_t n = key >> 60;
+        ckey = n << 60;
+        phase = 1;
+        for (uint64_t j = 0; j < n; ++j) {
+            const int shift = int(30 * (1 - j));
+            const uint64_t pr = (key >> shift) & ((uint64_t(1) << 30) - 1);
+            uint32_t cid;
+            int s;
+            if (!conj_op(uint32_t(pr & 0xFFFF), cid, s)) return false;
+            phase *= s;
+            ckey |= ((pr & ~uint64_t(0xFFFF)) | cid) << shift;
+        }
+        return true;
+    }
+
     MPO finish(double cutoff) {
         // pass-through transitions of L and R keys over their extents
         for (auto& kv : Lkeys) {
@@ -283,6 +321,34 @@ struct Builder {
             bdim[p + 1] = n;
         }
 
+        // Hermitian pairs per bond (the reference registers them in create_mpo,
+        // tagged_mpo_maker_optim.hpp:292-307): an L or R key and its conjugate key are
+        // partners, a key equal to its conjugate is self-adjoint; V and D, the keys
+        // without operators, are left unregistered as the reference leaves its trivial keys
+        std::vector<std::vector<int32_t>> bherm(L + 1), bphase(L + 1);
+        for (int p = -1; p <= L - 1; ++p) {
+            auto& m = bond[p + 1];
+            auto& hv = bherm[p + 1];
+            auto& ph = bphase[p + 1];
+            hv.assign(bdim[p + 1], -1);
+            ph.assign(bdim[p + 1], 1);
+            for (auto& kv : m) {
+                const uint32_t t = kv.first >> 28, id = kv.first & ((1u << 28) - 1);
+                if (t != T_L && t != T_R) continue;
+                const auto& keys = (t == T_L) ? Lkeys : Rkeys;
+                const uint64_t key = (t == T_L) ? Lkey_of[id] : Rkey_of[id];
+                uint64_t ckey;
+                int phase;
+                if (!conj_key(key, ckey, phase)) continue;
+                auto ck = keys.find(ckey);
+                if (ck == keys.end()) continue;
+                auto cb = m.find((t << 28) | ck->second.id);
+                if (cb == m.end()) continue;
+                hv[kv.second] = int32_t(cb->second);
+                ph[kv.second] = phase;
+            }
+        }
+
         auto sops = std::make_shared<std::vector<SparseOp>>();
         for (auto& M : ops.mats) {
             SparseOp s;
@@ -316,6 +382,8 @@ struct Builder {
                 return a.op < b.op;
             });
             for (auto& e : es) { T.b1.push_back(e.b1); T.b2.push_back(e.b2); T.op.push_back(e.op); T.scale.push_back(e.v); }
+            T.herm_left = bherm[y]; T.phase_left = bphase[y];
+            T.herm_right = bherm[y + 1]; T.phase_right = bphase[y + 1];
             T.finalize();
         }
         return mpo;

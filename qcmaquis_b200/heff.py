@@ -48,7 +48,8 @@ class HeffInfo(ctypes.Structure):
                 ("n_ttiles", c_uint64), ("n_gtasks", c_uint64), ("n_alpha", c_uint64), ("n_segs", c_uint64),
                 ("n_outs", c_uint64), ("n_otiles", c_uint64), ("flops", c_double), ("flops_t", c_double),
                 ("flops_ls", c_double), ("flops_s", c_double), ("g_elems", c_uint64), ("g_reads", c_uint64),
-                ("l_len", c_uint64), ("r_len", c_uint64), ("n_kitems", c_uint64), ("flops_sdense", c_double), ("launches", c_uint64), ("w_len", c_uint64), ("flops_sexec", c_double)]
+                ("l_len", c_uint64), ("r_len", c_uint64), ("n_kitems", c_uint64), ("flops_sdense", c_double), ("launches", c_uint64), ("w_len", c_uint64), ("flops_sexec", c_double),
+                ("p_len", c_uint64)]
 
 
 class BoundaryInfo(ctypes.Structure):

@@ -33,6 +33,58 @@ class MPO:
         check(lib.qcm_mpo_deserialize(buf, len(blob), ctypes.byref(out)), "qcm_mpo_deserialize")
         return cls(out)
 
+    @classmethod
+    def from_tensors(cls, tensors, twosite: bool = False) -> "MPO":
+        """MPO handed in tensor by tensor (qcm_mpo_create + qcm_mpo_set_tensor), from dicts in the
+        layout parse_blob returns (herm_left / herm_right: (n, 2) arrays of partner and phase, or None)."""
+        out = ctypes.c_void_p()
+        check(lib.qcm_mpo_create(len(tensors), int(twosite), ctypes.byref(out)), "qcm_mpo_create")
+        m = cls(out)
+        for site, t in enumerate(tensors):
+            m.set_tensor(site, t)
+        return m
+
+    def set_tensor(self, site: int, t) -> None:
+        u32 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        i32 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        keep = []
+
+        def arr(x, dt):
+            a = np.ascontiguousarray(x, dtype=dt)
+            keep.append(a)
+            return a
+        b1, b2, op = arr(t["b1"], np.uint32), arr(t["b2"], np.uint32), arr(t["op"], np.uint32)
+        sc = arr(t["scale"], np.float64)
+        ops = t["ops"]
+        ptr = arr(np.concatenate([[0], np.cumsum([len(o) for o in ops])]), np.uint64)
+        oin = arr(np.concatenate([o["inp"] for o in ops]) if ops else [], np.uint32)
+        oout = arr(np.concatenate([o["out"] for o in ops]) if ops else [], np.uint32)
+        oval = arr(np.concatenate([o["val"] for o in ops]) if ops else [], np.float64)
+        pc = arr([[a, b] for (a, b, _) in t["phys"]], np.int32)
+        ps = arr([s for (_, _, s) in t["phys"]], np.uint32)
+        d = _lib.MPOTensorDesc(rows=t["rows"], cols=t["cols"], n_terms=b1.size, b1=u32(b1), b2=u32(b2), op=u32(op),
+                               scale=_lib.dptr(sc), n_ops=len(ops),
+                               op_ptr=ptr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), op_in=u32(oin),
+                               op_out=u32(oout), op_val=_lib.dptr(oval), n_phys=len(t["phys"]),
+                               phys_charge=i32(pc), phys_size=u32(ps))
+        for side in ("left", "right"):
+            h = t.get("herm_" + side)
+            if h is not None:
+                hh = arr(np.asarray(h)[:, 0], np.int32)
+                ph = arr(np.asarray(h)[:, 1], np.int32)
+                setattr(d, "herm_" + side, i32(hh))
+                setattr(d, "phase_" + side, i32(ph))
+        check(lib.qcm_mpo_set_tensor(self._h, site, ctypes.byref(d)), "qcm_mpo_set_tensor")
+
+    def hermitian(self, site: int):
+        """(herm_left, phase_left, herm_right, phase_right) of tensor `site` (qcm_mpo_tensor_hermitian)."""
+        r, c = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib.qcm_mpo_tensor_info(self._h, site, ctypes.byref(r), ctypes.byref(c), None, None), "qcm_mpo_tensor_info")
+        out = [np.zeros(n, np.int32) for n in (r.value, r.value, c.value, c.value)]
+        i32 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        check(lib.qcm_mpo_tensor_hermitian(self._h, site, *[i32(a) for a in out]), "qcm_mpo_tensor_hermitian")
+        return tuple(out)
+
     def twosite(self) -> "MPO":
         out = ctypes.c_void_p()
         check(lib.qcm_mpo_make_twosite(self._h, ctypes.byref(out)), "qcm_mpo_make_twosite")

@@ -10,18 +10,43 @@ from qcmaquis_b200.fcidump import synthetic_integrals, hubbard_ladder_integrals
 from qcmaquis_b200.mpo import MPO
 
 
+def gauge_signed(tensors, seed):
+    """The same MPO with a random sign on bond indices (column b of W[p] and row b of W[p+1]
+    negated together); a Hermitian pair with one negated member gets phase -1, so boundaries
+    built from it carry conjugate scales of -1 (BoundaryIndex::conjugate_scale)."""
+    rng = np.random.default_rng(seed)
+    ts = [dict(t) for t in tensors]
+    for p in range(len(ts) - 1):
+        n = ts[p]["cols"]
+        s = np.where(rng.random(n) < 0.5, -1.0, 1.0)
+        s[:1] = 1.0
+        hr = ts[p]["herm_right"].copy()
+        for b in range(n):
+            if hr[b, 0] >= 0:
+                hr[b, 1] = int(hr[b, 1] * s[b] * s[hr[b, 0]])
+        ts[p]["scale"] = ts[p]["scale"] * s[ts[p]["b2"]]
+        ts[p]["herm_right"] = hr
+        ts[p + 1]["scale"] = ts[p + 1]["scale"] * s[ts[p + 1]["b1"]]
+        ts[p + 1]["herm_left"] = hr.copy()
+    return ts
+
+
 @functools.lru_cache(maxsize=None)
-def qc_system(L: int, seed: int = 0):
+def qc_system(L: int, seed: int = 0, gauge=None):
+    """Integrals, single-site MPO, two-site MPO and MPO blob; gauge = seed of a sign gauge on the
+    MPO's bond indices (gauge_signed), None for the plain MPO."""
     h, V, e = synthetic_integrals(L, seed)
     m = MPO.qc(h, V)
+    if gauge is not None:
+        m = MPO.from_tensors(gauge_signed(m.tensors(), gauge))
     return h, V, e, m, m.twosite(), m.blob()
 
 
 @functools.lru_cache(maxsize=None)
-def snapshot(L: int, M: int, sweeps_before: int, step: int, seed: int = 0):
+def snapshot(L: int, M: int, sweeps_before: int, step: int, seed: int = 0, gauge=None):
     """Frozen site problem (QSPB blob) of `step` in sweep `sweeps_before` (oracle DMRG)."""
     from oracle.oracle import OracleDMRG
-    h, V, e, m, ts, blob = qc_system(L, seed)
+    h, V, e, m, ts, blob = qc_system(L, seed, gauge)
     d = OracleDMRG(blob, L, L // 2, L // 2, M)
     for s in range(sweeps_before):
         d.sweep(s)
@@ -99,18 +124,36 @@ def dense_site_tensor(phys, left, right, blocks):
     return A
 
 
+def boundary_cohort_of(b):
+    """(bra charge, ket charge) -> cohort index of a boundary dict."""
+    return {(tuple(b["bra"][int(i)][:2]), tuple(b["ket"][int(j)][:2])): ci
+            for ci, (i, j) in enumerate(zip(b["cohort_bra"], b["cohort_ket"]))}
+
+
 def dense_boundary(b):
-    """B[aux, bra, ket] of a boundary dict (cohort blocks bra size x ket size)."""
+    """B[aux, bra, ket] of a boundary dict (cohort blocks bra size x ket size).
+
+    A transposed cohort (tr) stores no data: its block k is conjugate_scale times the transpose
+    of the block at offsets[k] of the partner cohort (bra and ket charges swapped), as
+    BoundaryIndex::complement_transpose sets it up (boundary.h:161-191)."""
     bo, bn = _offsets(b["bra"])
     ko, kn = _offsets(b["ket"])
     aux = b["aux"]
+    where = boundary_cohort_of(b)
     B = np.zeros((aux, bn, kn))
     for ci in range(len(b["cohort_bra"])):
-        if b["tr"][ci]:
-            assert (b["offsets"][ci * aux:(ci + 1) * aux] < 0).all()
-            continue
         i, j = int(b["cohort_bra"][ci]), int(b["cohort_ket"][ci])
         r, c = b["bra"][i][2], b["ket"][j][2]
+        if b["tr"][ci]:
+            ce = where[(tuple(b["ket"][j][:2]), tuple(b["bra"][i][:2]))]
+            assert not b["tr"][ce]
+            base = int(b["data_offset"][ce])
+            for k in range(aux):
+                o = int(b["offsets"][ci * aux + k])
+                if o >= 0:
+                    blk = b["data"][base + o: base + o + r * c].reshape(r, c)  # partner block c x r, column-major
+                    B[k, bo[i]:bo[i] + r, ko[j]:ko[j] + c] = b["cscale"][ci * aux + k] * blk
+            continue
         base = int(b["data_offset"][ci])
         for k in range(aux):
             o = int(b["offsets"][ci * aux + k])

@@ -73,5 +73,8 @@ def test_schedule_bookkeeping_matches_oracle(L, M, sw, step):
     assert [r[:10] for r in ro] == [r[:10] for r in rp]
     assert max(abs(a[10] - b[10]) for a, b in zip(ro, rp)) <= 1e-15 * max(abs(a[10]) for a in ro)
     assert plan.info["flops"] == fl
+    if L == 8:
+        # the Hermitian-paired MPO stores half the off-diagonal cohorts: transposed ones are read
+        assert any(r[2] != r[3] for r in ro)
     with pytest.raises(_lib.QcmError, match="host-only"):
         plan.apply(np.zeros(plan.n))

@@ -37,10 +37,10 @@ def _cohorts(b):
     return out
 
 
-def _step_case(L, M, sweeps_before, step, side, seed=0):
+def _step_case(L, M, sweeps_before, step, side, seed=0, gauge=None):
     from oracle.oracle import OracleDMRG
     from qcmaquis_b200.heff import parse_boundary_step
-    h, V, e, m, ts, blob = qc_system(L, seed)
+    h, V, e, m, ts, blob = qc_system(L, seed, gauge)
     d = OracleDMRG(blob, L, L // 2, L // 2, M)
     for s in range(sweeps_before):
         d.sweep(s)
@@ -50,11 +50,19 @@ def _step_case(L, M, sweeps_before, step, side, seed=0):
     return m, parse_boundary_step(d.boundary_export(side, site))
 
 
-@pytest.mark.parametrize("L,M,sw,step,side", [(6, 16, 0, 2, 0), (6, 16, 1, 3, 1), (8, 32, 1, 3, 0), (8, 32, 1, 4, 1)])
-def test_boundary_step_matches_oracle(gpu_ctx, L, M, sw, step, side):
+@pytest.mark.parametrize("L,M,sw,step,side,gauge", [(6, 16, 0, 2, 0, None), (6, 16, 1, 3, 1, None), (8, 32, 1, 3, 0, None),
+                                                    (8, 32, 1, 4, 1, None), (8, 32, 1, 3, 0, 3), (8, 32, 1, 4, 1, 3)])
+def test_boundary_step_matches_oracle(gpu_ctx, L, M, sw, step, side, gauge):
+    """Input and output boundaries hold transposed (Hermitian-partner) cohorts; with the sign-gauged
+    MPO some of their conjugate scales are -1."""
     from qcmaquis_b200.dmrg import boundary_step
     from qcmaquis_b200.heff import Boundary
-    m, case = _step_case(L, M, sw, step, side)
+    m, case = _step_case(L, M, sw, step, side, 0, gauge)
+    if L >= 8:
+        for k in ("B_in", "B_out"):
+            assert case[k]["tr"].sum() > 0
+        if gauge is not None:
+            assert (case["B_in"]["cscale"] == -1.0).any() and (case["B_out"]["cscale"] == -1.0).any()
     data_rp = np.concatenate([blk.T.ravel() for (_, blk) in case["blocks"]])
     B = Boundary(gpu_ctx, case["B_in"])
     out = boundary_step(gpu_ctx, B, m, case["site"], case["phys"], case["left"], case["right"], data_rp,
@@ -91,15 +99,16 @@ def test_jd_matches_oracle_step_energy(gpu_ctx, L, M, sw, step):
     assert abs(np.dot(vec, hv) - ev) < 1e-9
 
 
-@pytest.mark.parametrize("L,M,sweeps", [(6, 16, 3), (8, 32, 3)])
-def test_sweep_energies_match_oracle(gpu_ctx, L, M, sweeps):
+@pytest.mark.parametrize("L,M,sweeps,gauge", [(6, 16, 3, None), (8, 32, 3, None), (8, 32, 2, 3)])
+def test_sweep_energies_match_oracle(gpu_ctx, L, M, sweeps, gauge):
     """Both engines start from the oracle's initial MPS.  (The const initial state itself is
     not reproducible across LAPACK implementations: normalize_left QR-factorises rank-1
-    all-ones blocks, and the orthonormal completion of Q is fixed by rounding.)"""
+    all-ones blocks, and the orthonormal completion of Q is fixed by rounding.)  Boundaries are
+    Hermitian-compressed; with the sign-gauged MPO their conjugate scales include -1."""
     from oracle.oracle import OracleDMRG
     from qcmaquis_b200.dmrg import DMRG
     from qcmaquis_b200.heff import parse_mps_tensor
-    h, V, e, m, ts, blob = qc_system(L)
+    h, V, e, m, ts, blob = qc_system(L, 0, gauge)
     ref = OracleDMRG(blob, L, L // 2, L // 2, M)
     sites = [parse_mps_tensor(ref.mps_export(i)) for i in range(L)]
     dev = DMRG.from_mps(gpu_ctx, m, sites, M)

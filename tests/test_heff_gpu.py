@@ -9,16 +9,29 @@ from helpers import qc_system, snapshot, site_of_step
 
 pytestmark = pytest.mark.gpu
 
-# (L, M, sweeps before, step): left-to-right and right-to-left steps, ends and middle
-CASES = [(6, 16, 1, 0), (6, 16, 1, 2), (6, 16, 1, 7), (8, 64, 1, 3), (8, 64, 1, 10), (8, 64, 2, 12), (10, 48, 1, 4)]
+# (L, M, sweeps before, step, MPO sign gauge): left-to-right and right-to-left steps, ends and
+# middle; the gauged MPO's Hermitian pairs carry phase -1 (conjugate scales of -1)
+CASES = [(6, 16, 1, 0, None), (6, 16, 1, 2, None), (6, 16, 1, 7, None), (8, 64, 1, 3, None), (8, 64, 1, 10, None),
+         (8, 64, 2, 12, None), (10, 48, 1, 4, None), (8, 64, 1, 3, 11), (10, 48, 1, 13, 5)]
 
 
-@pytest.mark.parametrize("L,M,sw,step", CASES)
-def test_heff_matches_oracle(gpu_ctx, L, M, sw, step):
-    snap = snapshot(L, M, sw, step)
-    h, V, e, m, ts, blob = qc_system(L, 0)
+def transposed_cohorts(b):
+    """(transposed cohorts, blocks with conjugate scale != 1) of a boundary dict."""
+    return int(np.sum(b["tr"])), int(np.sum(b["cscale"] != 1.0))
+
+
+@pytest.mark.parametrize("L,M,sw,step,gauge", CASES)
+def test_heff_matches_oracle(gpu_ctx, L, M, sw, step, gauge):
+    snap = snapshot(L, M, sw, step, 0, gauge)
+    h, V, e, m, ts, blob = qc_system(L, 0, gauge)
     site = site_of_step(L, step)
     p = heff.parse_site_problem(snap)
+    if L >= 8:
+        # the reference's storage: half the off-diagonal cohorts are transposed Hermitian partners
+        ntr = [transposed_cohorts(p[k]) for k in ("L", "R")]
+        assert ntr[0][0] > 0 and ntr[1][0] > 0
+        if gauge is not None:
+            assert ntr[0][1] + ntr[1][1] > 0
     plan = heff.plan_from_problem(gpu_ctx, p, ts, site)
     x0 = heff.twin_vector(p)
     rng = np.random.default_rng(step)

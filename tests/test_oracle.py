@@ -113,3 +113,25 @@ def test_oracle_boundary_step_matches_dense_contraction(sw, step, side):
     ref = dense_boundary_step(case, parse_blob(blob)[site])
     got = dense_boundary(case["B_out"])
     assert np.abs(ref - got).max() <= 1e-13 * np.abs(ref).max()
+
+
+def test_oracle_hermitian_boundaries_and_gauge_phases():
+    """Boundaries built with the MPO's Hermitian pairs (complement_transpose) store transposed
+    cohorts; a sign gauge on the MPO's bond indices gives conjugate scales of -1 and leaves every
+    step energy of the sweeps unchanged."""
+    from qcmaquis_b200.heff import parse_boundary_step
+    L, M = 8, 32
+    h, V, e, m, ts, blob = qc_system(L)
+    gblob = qc_system(L, 0, 11)[5]
+    runs = []
+    for b in (blob, gblob):
+        d = OracleDMRG(b, L, 4, 4, M)
+        runs.append([d.sweep(s)[0] for s in range(2)])
+        d.snapshot(2, 3)
+        c = parse_boundary_step(d.boundary_export(0, 3))
+        B = c["B_out"]
+        assert B["tr"].sum() > 0
+        if b is gblob:
+            assert (B["cscale"] == -1.0).any()
+    for a, g in zip(*runs):
+        assert np.abs(a - g).max() < 1e-10
