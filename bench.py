@@ -2,39 +2,46 @@
 """Benchmark of the two-site DMRG effective-Hamiltonian hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--L 24] [--M 512] [--init-bd 64] [--sweeps 2] [--seed 0]
+                    [--L 24] [--M 512] [--seed 0] [--sweeps 8]
 
-Workload: the seeded synthetic ab-initio Hamiltonian of the precision-form
-configuration (L = 24 orbitals, N = 24 electrons, TwoU1 Sz = 0, M = 512; FP64
-plain form).  Setup (untimed): the device engine runs `--sweeps` full two-site
-sweeps from the const initial state (each timed on its own and reported under
-"sweep"), then continues the next sweep up to the middle bond (step L/2 - 1)
-and freezes that site problem.
+Workload (both arms build it the same way, without running a sweep): the seeded
+synthetic ab-initio Hamiltonian of the precision-form configuration (L = 24
+orbitals, N = 24 electrons, TwoU1 Sz = 0, seed 0) and an MPS whose bond sectors
+are those of a converged M = 512 two-site DMRG state of it (recorded in
+tests/golden/bench_sectors_L24_M512.json by tests/golden/make_bench_sectors.py),
+with site-tensor entries drawn from numpy.random.default_rng(seed).  The frozen
+site problem is the two-site problem at the middle bond (sites L/2 - 1, L/2):
+left boundaries over the sites before it and right boundaries over the sites
+after it, built from that MPS with the MPO's Hermitian pairs (the reference's
+init_left_right(mpo, site), optimize/optimize.h:158-195).
 
-A step is one H_eff . psi (the Davidson callback, super_hamil_mv) on that
-frozen problem.  `value` = reference work count (ScheduleNew::total_flops,
+A step is one H_eff . psi (the Davidson callback, super_hamil_mv) on that frozen
+problem.  `value` = reference work count (ScheduleNew::total_flops,
 solver/tasks.cpp:388-398, 777-796) x steps / device time (CUDA events on the
 plan stream, L2 flushed between steps), summed over ranks / max over ranks.
 `e2e` is the same metric through qcm_heff_apply with pinned host buffers (H2D
 of psi and D2H of H.psi inside the timed region).  The path does not shard
 across GPUs here (one B200 per solve): N > 1 runs N independent replicas.
 
-"mixed" reports the mixed-precision form of the same step (S build as 3xTF32 on
-the tensor cores, T-GEMM and L.S in FP64) with the same timing rules, its
-deviation from the oracle, and (unless --no-mixed-sweep) the same sweeps run
-with every Jacobi-Davidson solve in the mixed form (FP64 Rayleigh quotient per
-step): sweep times and the energy deviation from the FP64 sweeps.
+Reported beside the metric (not part of it): the mixed-precision forms of the
+same step; the adjoint; `--sweeps` full two-site sweeps of the configuration
+from the const initial state in the FP64 form and in the mixed form (per-sweep
+time, energy, truncated weight and the mixed form's deviations); one
+single-site sweep; the boundary storage with and without the Hermitian pairs.
 
 The reference arm (--impl reference) times the CPU restatement of the same
-H.psi (the oracle: OpenMP over ket sectors, OpenBLAS dgemm) on the same frozen
-problem, exported by the device engine as a "QSPB" blob.
+H.psi (the oracle: OpenMP over ket sectors, OpenBLAS dgemm, all host threads)
+on the same frozen problem, which it builds itself (the oracle's boundary steps
+over the same MPS); it loads no library of the device path.
 """
 from __future__ import annotations
 
 import argparse
+import importlib.util
 import json
 import os
 import statistics
+import struct
 import subprocess
 import sys
 import time
@@ -53,83 +60,111 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--L", type=int, default=24)
     ap.add_argument("--M", type=int, default=512)
-    ap.add_argument("--init-bd", type=int, default=64)
-    ap.add_argument("--sweeps", type=int, default=2)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--sweeps", type=int, default=8, help="sweeps of the FP64 / mixed sweep comparison (0: none)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-mixed-sweep", action="store_true", help="skip the mixed-precision sweeps (bench of the apply only)")
-    ap.add_argument("--no-single-site-sweep", action="store_true", help="skip the single-site sweep after the two-site ones")
+    ap.add_argument("--no-mixed-sweep", action="store_true", help="skip the mixed-precision sweeps")
+    ap.add_argument("--no-single-site-sweep", action="store_true", help="skip the single-site sweep")
+    ap.add_argument("--no-extras", action="store_true", help="the metric only (no sweeps, forms, adjoint)")
     return ap.parse_args()
 
 
-def workload_name(a):
-    return (f"two-site H_eff.psi, synthetic ab-initio L={a.L} N={a.L} TwoU1 Sz=0 seed {a.seed}, M={a.M} "
-            f"(init_bond_dimension {a.init_bd}), middle bond after {a.sweeps} sweeps")
+# ---------------------------------------------------------------------------
+# the frozen problem's inputs (numpy only: shared by both arms)
+
+def _fcidump():
+    """The integral recipe module, loaded from its file (importing the package would load the device library)."""
+    spec = importlib.util.spec_from_file_location("qcm_fcidump", os.path.join(ROOT, "qcmaquis_b200", "fcidump.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
-def frozen_problem(a, device: int, export: bool):
-    """Device sweeps, then the middle-bond site problem: (ctx, dmrg, plan, x, mpo_blob, snap, site, sweep_info)."""
-    from qcmaquis_b200.fcidump import synthetic_integrals
-    from qcmaquis_b200.mpo import MPO
-    from qcmaquis_b200.heff import Context
-    from qcmaquis_b200.dmrg import DMRG
-    h, V, e = synthetic_integrals(a.L, a.seed)
-    m = MPO.qc(h, V)
-    ctx = Context(device)
-    t0 = time.perf_counter()
-    d = DMRG(ctx, m, a.L // 2, a.L // 2, a.M, a.init_bd)
-    t_init = time.perf_counter() - t0
-    sweeps = []
-    for s in range(a.sweeps):
-        st0 = d.stats()
-        t0 = time.perf_counter()
-        E, tr = d.sweep()
-        dt = time.perf_counter() - t0
-        st1 = d.stats()
-        sweeps.append({"sweep": s, "seconds": dt, "energy_min": float(E.min()),
-                       "max_bond_dimension": int(max(t["bond_dimension"] for t in tr)),
-                       "hpsi": int(st1["hpsi_count"] - st0["hpsi_count"]),
-                       "hpsi_gflop": (st1["hpsi_flops"] - st0["hpsi_flops"]) / 1e9,
-                       "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}})
-    if not a.no_single_site_sweep:
-        sweeps_ss = single_site_sweep(a, ctx, m, d, sweeps[-1]["energy_min"])
-    site = a.L // 2 - 1
-    d.run(site)
-    plan, x = d.pending_plan()
-    snap = d.pending_export() if export else None
-    info = {"init_s": t_init, "sweeps": sweeps, "site": site}
-    if not a.no_single_site_sweep:
-        info["single_site"] = sweeps_ss
-    return ctx, d, plan, x, m.blob(), snap, site, info
+def bond_sectors(a):
+    path = os.path.join(ROOT, "tests", "golden", f"bench_sectors_L{a.L}_M{a.M}.json")
+    with open(path) as f:
+        d = json.load(f)
+    if d["L"] != a.L or d["M"] != a.M:
+        raise ValueError(f"{path}: sector fixture for another configuration")
+    return [tuple(p) for p in d["phys"]], [[tuple(s) for s in b] for b in d["bonds"]], os.path.basename(path)
 
 
-def single_site_sweep(a, ctx, m, d, e_ts):
-    """One single-site sweep (optimization = singlesite: 2L steps, density-matrix growth with noise 1e-8)
-    from the two-site sweeps' MPS at the same Mmax: its time, phases and H.psi work, and its lowest energy
-    against the last two-site sweep's.  Reported beside the metric; a failure is recorded, not raised."""
-    from qcmaquis_b200.dmrg import DMRG
-    from qcmaquis_b200.heff import parse_mps_tensor
-    try:
-        sites = [parse_mps_tensor(b) for b in d.export_mps()]
-        noise = dict(alpha_initial=1e-8, alpha_main=1e-8, alpha_final=1e-8)
-        s = DMRG.from_mps(ctx, m, sites, a.M, heev=noise, optimization="singlesite")
-        del sites
-        st0 = s.stats()
-        t0 = time.perf_counter()
-        E, tr = s.sweep()
-        dt = time.perf_counter() - t0
-        st1 = s.stats()
-        out = {"steps": int(E.size), "seconds": dt, "energy_min": float(E.min()),
-               "energy_dev_vs_twosite": float(E.min() - e_ts),
-               "max_bond_dimension": int(max(t["bond_dimension"] for t in tr)),
-               "hpsi": int(st1["hpsi_count"] - st0["hpsi_count"]),
-               "hpsi_gflop": (st1["hpsi_flops"] - st0["hpsi_flops"]) / 1e9,
-               "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}}
-        del s
-        return out
-    except Exception as ex:  # reported beside the metric, never in place of it
-        return {"error": f"{type(ex).__name__}: {ex}"}
+def synthetic_mps(phys, bonds, seed):
+    """Site tensors (dict(phys, left, right, blocks)) over the given bond sectors, right-paired: one block per
+    left sector (rows: its size; columns: the phys sectors in order, each with the right sector it leads to),
+    entries N(0, 1) / sqrt(4 D_left), drawn site by site and block by block from default_rng(seed)."""
+    rng = np.random.default_rng(seed)
+    sites = []
+    for i in range(len(bonds) - 1):
+        left, right = bonds[i], bonds[i + 1]
+        rsize = {(s[0], s[1]): s[2] for s in right}
+        dleft = sum(s[2] for s in left)
+        blocks = []
+        for (qa, qb, ls) in left:
+            stripe = sum(d * rsize.get((qa + pa, qb + pb), 0) for (pa, pb, d) in phys)
+            if stripe == 0:
+                raise ValueError(f"site {i}: left sector {(qa, qb)} reaches no right sector")
+            blocks.append(((qa, qb), rng.standard_normal((ls, stripe)) / np.sqrt(4.0 * dleft)))
+        sites.append(dict(phys=list(phys), left=list(left), right=list(right), blocks=blocks))
+    return sites
 
+
+def qmps_blob(site):
+    """A site tensor as a "QMPS" v1 blob (right-paired blocks, column-major)."""
+    out = [struct.pack("<II", 0x53504D51, 1)]
+    for idx in (site["phys"], site["left"], site["right"]):
+        out.append(struct.pack("<I", len(idx)))
+        out += [struct.pack("<iiI", int(s[0]), int(s[1]), int(s[2])) for s in idx]
+    out.append(struct.pack("<I", len(site["blocks"])))
+    for (ch, blk) in site["blocks"]:
+        out.append(struct.pack("<iiII", ch[0], ch[1], blk.shape[0], blk.shape[1]))
+        out.append(np.ascontiguousarray(blk.T, dtype="<f8").tobytes())
+    return b"".join(out)
+
+
+def twin_of_problem(snap: bytes) -> np.ndarray:
+    """The two-site tensor of a "QSPB" v1 site problem as the H_eff vector (its blocks, column-major, in order)."""
+    off = 8
+    for _ in range(3):
+        (n,) = struct.unpack_from("<I", snap, off)
+        off += 4 + 12 * n
+    (nb,) = struct.unpack_from("<I", snap, off)
+    off += 4
+    parts = []
+    for _ in range(nb):
+        _, _, r, c = struct.unpack_from("<iiII", snap, off)
+        off += 16
+        parts.append(np.frombuffer(snap, dtype="<f8", count=r * c, offset=off))
+        off += 8 * r * c
+    return np.concatenate(parts)
+
+
+def problem_inputs(a):
+    fd = _fcidump()
+    h, V, e = fd.synthetic_integrals(a.L, a.seed)
+    phys, bonds, fixture = bond_sectors(a)
+    sites = synthetic_mps(phys, bonds, a.seed)
+    return h, V, sites, a.L // 2 - 1, fixture
+
+
+def config_of(a, fixture, flops):
+    return {"workload": (f"two-site H_eff.psi at the middle bond (sites {a.L // 2 - 1}, {a.L // 2}) of the synthetic "
+                         f"ab-initio Hamiltonian L={a.L} N={a.L} TwoU1 Sz=0 seed {a.seed}; MPS with the bond sectors of "
+                         f"a converged M={a.M} state ({fixture}), entries N(0,1) from default_rng({a.seed})"),
+            "L": a.L, "N": a.L, "M": a.M, "seed": a.seed, "site": a.L // 2 - 1, "flops_per_step": float(flops),
+            "boundaries": "Hermitian-paired MPO bonds (transposed partner cohorts)",
+            "l2": "flushed between steps (256 MiB write)"}
+
+
+def oracle_problem(h, V, sites, site1):
+    """The frozen problem built by the oracle alone: (mpo blob, QSPB snapshot, twin vector)."""
+    from oracle.oracle import mpo_blob_qc, site_problem
+    blob = mpo_blob_qc(h, V)
+    snap = site_problem(blob, [qmps_blob(s) for s in sites], site1)
+    return blob, snap, twin_of_problem(snap)
+
+
+# ---------------------------------------------------------------------------
 
 class Clocks:
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
@@ -175,10 +210,10 @@ def dist_setup(a):
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pg = None
-    if world > 1:
+    if world > 1 and a.impl == "b200":
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl" if a.impl == "b200" else "gloo", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
     return world, rank, local, pg
 
@@ -194,36 +229,63 @@ def cpu_baseline(snap, blob, site, x, flops, budget_s=20.0):
                       f"OpenBLAS dgemm), {sec * 1e3:.1f} ms each"}
 
 
-def run_reference(a, world, rank, pg):
+def run_reference(a, world, rank):
+    """The oracle's H.psi on the same frozen problem, with all host threads (rank 0 only)."""
     if rank != 0:
         return
     from oracle.oracle import heff_apply, lib as olib
-    ctx, d, plan, x, blob, snap, site, sinfo = frozen_problem(a, 0, export=True)
-    flops = plan.info["flops"]
-    del plan, d
+    h, V, sites, site1, fixture = problem_inputs(a)
+    blob, snap, x = oracle_problem(h, V, sites, site1)
     for _ in range(a.warmup):
-        heff_apply(snap, blob, site, x, repeat=1)
+        heff_apply(snap, blob, site1, x, repeat=1)
     t0 = time.perf_counter()
-    _, flops_o, sec = heff_apply(snap, blob, site, x, repeat=a.steps)
+    _, flops, sec = heff_apply(snap, blob, site1, x, repeat=a.steps)
     wall = time.perf_counter() - t0
-    val = flops_o / sec / 1e9
+    val = flops / sec / 1e9
     cores = olib().orc_max_threads()
     line = {"impl": "reference", "metric": "H_eff.psi GFLOP/s (FP64 plain form)", "value": val, "unit": "GFLOP/s",
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": sec * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "init_bond_dimension": a.init_bd,
-                       "seed": a.seed, "flops_per_step": flops_o},
+            "config": config_of(a, fixture, flops),
             "cpu_baseline": {"value": val, "unit": "GFLOP/s", "cores": cores, "kind": "port",
                              "sample": f"{a.steps} H_eff.psi applies ({wall:.1f} s) with all host threads"},
             "e2e": {"value": val, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "frozen problem produced by the device engine (untimed) and exported as a QSPB blob"}
-    assert abs(flops_o - flops) <= 1e-9 * flops, "oracle and device work counts differ"
+            "note": "the oracle builds the frozen problem itself (its boundary steps over the same MPS, untimed)"}
     print(json.dumps(line), flush=True)
 
 
-def measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob, site, x_host, form="mixed"):
-    """A mixed-precision form on the same frozen problem: S build 3xTF32 on the tensor cores
-    (FP32 accumulation), T-GEMM and L.S in FP64; same timing rules as the FP64 form."""
+# ---------------------------------------------------------------------------
+# device arm
+
+def device_problem(ctx, h, V, sites, site1, M, hermitian=True):
+    """The frozen problem on the device: (dmrg, plan, x, mpo).  The device builds the boundaries from the
+    same MPS (qcm_dmrg_create_from_mps_at); hermitian=False drops the MPO's Hermitian pairs."""
+    from qcmaquis_b200.dmrg import DMRG
+    from qcmaquis_b200.mpo import MPO
+    m = MPO.qc(h, V)
+    if not hermitian:
+        ts = m.tensors()
+        for t in ts:
+            t["herm_left"], t["herm_right"] = None, None
+        m = MPO.from_tensors(ts)
+    d = DMRG.from_mps(ctx, m, sites, M, initial_site=site1)
+    plan, x = d.pending_plan()
+    return d, plan, x, m
+
+
+def boundary_storage(d, plan):
+    """Stored doubles and cohorts (transposed ones among them) of the pending step's two boundaries."""
+    from qcmaquis_b200.heff import parse_site_problem
+    p = parse_site_problem(d.pending_export(index_only=True))
+    nc = sum(len(p[k]["tr"]) for k in ("L", "R"))
+    ntr = sum(int(p[k]["tr"].sum()) for k in ("L", "R"))
+    return {"doubles": int(plan.info["l_len"] + plan.info["r_len"]), "cohorts": nc, "transposed_cohorts": ntr,
+            "stored_cohorts": nc - ntr, "flops_per_step": float(plan.info["flops"])}
+
+
+def measure_mixed(a, plan, xd, yd, xp, yp, hb, flush, info, world, pg, dev, snap, blob, site, x_host, form="mixed"):
+    """A mixed-precision form on the same frozen problem (S build 3xTF32 on the tensor cores, FP32
+    accumulation; T-GEMM and L.S in FP64), same timing rules as the FP64 form."""
     import torch
     from qcmaquis_b200._lib import lib, check
     from qcmaquis_b200.heff import precision_mode
@@ -255,7 +317,7 @@ def measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, 
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         total_ms, e2e_s = float(t[0].item()), float(t[1].item())
     ph = np.mean(np.array(phases), axis=0)
-    y_mixed = yh.numpy().copy()
+    y_mixed = hb["y"].numpy().copy()
     out = {"value": info["flops"] * a.steps * world / (total_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
            "ms_per_step": total_ms / a.steps,
            "form": ("S build 3xTF32 (mma.sync m16n8k8, FP32 operands split at the fragment loads, FP32 accumulation), "
@@ -274,7 +336,7 @@ def measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, 
     return out
 
 
-def measure_adjoint(a, plan, x_host, blob, site):
+def measure_adjoint(a, plan, x_host, mpo, site):
     """The differentiation form on the same frozen problem: qcm_heff_adjoint with host buffers (x and
     ybar in, psi_bar and the gradient per two-site MPO entry out), wall time per call."""
     rng = np.random.default_rng(a.seed)
@@ -286,8 +348,7 @@ def measure_adjoint(a, plan, x_host, blob, site):
         pb, g = plan.adjoint(x_host, ybar)
     dt = (time.perf_counter() - t0) / reps
     # f = ybar . H x is linear in the scales: the gradient contracted with the scales gives f back
-    from qcmaquis_b200.mpo import MPO
-    terms = MPO.from_blob(blob).twosite().terms(site)["scale"]  # same builder: the plan's entry order
+    terms = mpo.twosite().terms(site)["scale"]
     f = float(ybar @ plan.apply(x_host))
     return {"ms_per_call": dt * 1e3, "n_terms": int(g.size), "h2d_bytes": 16 * x_host.size,
             "d2h_bytes": 8 * (x_host.size + g.size),
@@ -296,53 +357,103 @@ def measure_adjoint(a, plan, x_host, blob, site):
                     "in the scales) is the consistency check"}
 
 
-def mixed_sweeps(a, ctx, blob, sinfo):
-    """The same sweeps with every JD in the mixed form (FP64 Rayleigh quotient per step): times and
-    the per-sweep energy deviation from the FP64 device sweeps."""
-    from qcmaquis_b200.mpo import MPO
+def sweep_record(d, E, tr, dt, st0, st1, s):
+    tw = np.array([t["truncated_weight"] for t in tr])
+    return {"sweep": s, "seconds": dt, "energy_min": float(E.min()), "truncated_weight_max": float(tw.max()),
+            "truncated_weight_sum": float(tw.sum()),
+            "max_bond_dimension": int(max(t["bond_dimension"] for t in tr)),
+            "hpsi": int(st1["hpsi_count"] - st0["hpsi_count"]),
+            "hpsi_fp64_rayleigh": int(st1["hpsi_count_fp64"] - st0["hpsi_count_fp64"]),
+            "hpsi_gflop": (st1["hpsi_flops"] - st0["hpsi_flops"]) / 1e9,
+            "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}}
+
+
+def run_sweeps(a, ctx, h, V, precision):
+    """`a.sweeps` two-site sweeps of the configuration from the const initial state (init_bond_dimension 64)."""
     from qcmaquis_b200.dmrg import DMRG
-    m = MPO.from_blob(blob)
-    d = DMRG(ctx, m, a.L // 2, a.L // 2, a.M, a.init_bd, precision="mixed")
+    from qcmaquis_b200.mpo import MPO
+    m = MPO.qc(h, V)
+    d = DMRG(ctx, m, a.L // 2, a.L // 2, a.M, 64, precision=precision)
     out = []
     for s in range(a.sweeps):
         st0 = d.stats()
         t0 = time.perf_counter()
         E, tr = d.sweep()
         dt = time.perf_counter() - t0
-        st1 = d.stats()
-        e64 = sinfo["sweeps"][s]["energy_min"]
-        out.append({"sweep": s, "seconds": dt, "energy_min": float(E.min()), "energy_dev_vs_fp64": float(E.min() - e64),
-                    "max_bond_dimension": int(max(t["bond_dimension"] for t in tr)),
-                    "hpsi_mixed": int(st1["hpsi_count"] - st0["hpsi_count"]),
-                    "hpsi_fp64": int(st1["hpsi_count_fp64"] - st0["hpsi_count_fp64"]),
-                    "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}})
-    del d
+        out.append(sweep_record(d, E, tr, dt, st0, d.stats(), s))
+    return d, m, out
+
+
+def single_site_sweep(a, ctx, m, d, e_ts):
+    """One single-site sweep (optimization = singlesite: 2L steps, density-matrix growth with noise 1e-8)
+    from the two-site sweeps' MPS at the same Mmax: its time, phases and H.psi work, and its lowest energy
+    against the last two-site sweep's.  A failure is recorded, not raised."""
+    from qcmaquis_b200.dmrg import DMRG
+    from qcmaquis_b200.heff import parse_mps_tensor
+    try:
+        sites = [parse_mps_tensor(b) for b in d.export_mps()]
+        noise = dict(alpha_initial=1e-8, alpha_main=1e-8, alpha_final=1e-8)
+        s = DMRG.from_mps(ctx, m, sites, a.M, heev=noise, optimization="singlesite")
+        del sites
+        st0 = s.stats()
+        t0 = time.perf_counter()
+        E, tr = s.sweep()
+        dt = time.perf_counter() - t0
+        st1 = s.stats()
+        out = {"steps": int(E.size), "seconds": dt, "energy_min": float(E.min()),
+               "energy_dev_vs_twosite": float(E.min() - e_ts),
+               "max_bond_dimension": int(max(t["bond_dimension"] for t in tr)),
+               "hpsi": int(st1["hpsi_count"] - st0["hpsi_count"]),
+               "hpsi_gflop": (st1["hpsi_flops"] - st0["hpsi_flops"]) / 1e9,
+               "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}}
+        del s
+        return out
+    except Exception as ex:  # reported beside the metric, never in place of it
+        return {"error": f"{type(ex).__name__}: {ex}"}
+
+
+def sweep_comparison(a, ctx, h, V):
+    """FP64 and mixed-form sweeps from the same const state: per-sweep time, energy, truncated weight, and
+    the mixed form's deviations from the FP64 sweeps (the FP64 device sweeps match the oracle's to 1e-10 Eh
+    in the parity tests)."""
+    d64, m, fp64 = run_sweeps(a, ctx, h, V, "fp64")
+    out = {"sweeps": a.sweeps, "init_bond_dimension": 64, "fp64": fp64}
+    if not a.no_single_site_sweep:
+        out["single_site"] = single_site_sweep(a, ctx, m, d64, fp64[-1]["energy_min"])
+    del d64
+    if not a.no_mixed_sweep:
+        dmx, _, mixed = run_sweeps(a, ctx, h, V, "mixed")
+        del dmx
+        for r, r64 in zip(mixed, fp64):
+            r["energy_dev_vs_fp64"] = r["energy_min"] - r64["energy_min"]
+            r["truncated_weight_sum_dev_vs_fp64"] = r["truncated_weight_sum"] - r64["truncated_weight_sum"]
+        out["mixed"] = mixed
+        out["max_abs_energy_dev"] = max(abs(r["energy_dev_vs_fp64"]) for r in mixed)
     return out
 
 
 def run_b200(a, world, rank, local, pg):
+    import ctypes
     import torch
     from qcmaquis_b200 import heff
+    from qcmaquis_b200._lib import lib, check, P, c_double
     torch.cuda.set_device(local)
-    want_cpu = rank == 0 and world == 1 and not a.no_cpu_baseline
-    ctx, d, plan, x_host, blob, snap, site, sinfo = frozen_problem(a, local, export=want_cpu)
+    dev = torch.device("cuda", local)
+    h, V, sites, site1, fixture = problem_inputs(a)
+    ctx = heff.Context(local)
+    d, plan, x_host, mpo = device_problem(ctx, h, V, sites, site1, a.M)
     info = plan.info
     n = plan.n
-    dev = torch.device("cuda", local)
     xd = torch.from_numpy(x_host).to(dev)
     yd = torch.empty_like(xd)
     flush = torch.empty(int(256 * 2**20 // 4), dtype=torch.float32, device=dev)  # 256 MiB > L2 (126 MB)
-    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
     dmma_peak, dfma_peak = heff.probe_fp64_peaks()
     torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()  # sampled from the warm-up on, stopped after the timed region
-    # warm-up (plan stream; the context stream is separate from torch's)
     for _ in range(a.warmup):
         plan.apply_device(xd.data_ptr(), yd.data_ptr())
     ctx.synchronize()
-    prof = [plan.profile(xd.data_ptr(), yd.data_ptr()) for _ in range(3)]
     # timed region: per-step CUDA events on the plan's stream via qcm_heff_profile
     if pg is not None:
         pg.barrier()
@@ -368,8 +479,6 @@ def run_b200(a, world, rank, local, pg):
     # e2e through the C-ABI with pinned host buffers
     xh = torch.from_numpy(x_host).pin_memory()
     yh = torch.empty_like(xh).pin_memory()
-    import ctypes
-    from qcmaquis_b200._lib import lib, check, P, c_double
     xp = ctypes.cast(xh.data_ptr(), P(c_double))
     yp = ctypes.cast(yh.data_ptr(), P(c_double))
     for _ in range(2):
@@ -387,12 +496,20 @@ def run_b200(a, world, rank, local, pg):
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_val = info["flops"] * a.steps * world / e2e_s / 1e9
-    # correctness guard on the timed problem: device result vs the oracle
-    rel = None
-    if snap is not None:
+    y_dev = yh.numpy().copy()
+    # the checker: the oracle builds the same problem itself; the device result against it, and the
+    # device's own twin against the oracle's
+    snap = blob = None
+    rel = twin_rel = None
+    want_oracle = rank == 0 and not a.no_cpu_baseline
+    if want_oracle:
         from oracle.oracle import heff_apply
-        y_ref, _, _ = heff_apply(snap, blob, site, x_host)
-        rel = float(np.abs(yh.numpy() - y_ref).max() / np.abs(y_ref).max())
+        blob, snap, x_or = oracle_problem(h, V, sites, site1)
+        twin_rel = float(np.abs(x_or - x_host).max() / np.abs(x_or).max())
+        y_ref, flops_or, _ = heff_apply(snap, blob, site1, x_host)
+        rel = float(np.abs(y_dev - y_ref).max() / np.abs(y_ref).max())
+        if flops_or != info["flops"]:
+            raise RuntimeError(f"device and oracle work counts differ: {info['flops']} vs {flops_or}")
     # roofline of the dominant kernel (phase): reference flop count of the phase / its device time
     ph = np.mean(np.array(phases), axis=0)
     names = ["k_tgemm", "k_sgemm", "k_lspart+k_lsreduce"]
@@ -404,34 +521,41 @@ def run_b200(a, world, rank, local, pg):
             "algorithmic": "reference flop count of the phase (ScheduleNew::total_flops terms)",
             "peak_source": "FP64 DMMA probe qcm_probe_fp64_peaks (of measured)"}
     if dom == 1:
-        # tensor work the S-GEMM tiles really issue (padding included) over the same time
         roof["executed_tflops"] = info["flops_sexec"] / (ph[1] * 1e-3) / 1e12
         roof["executed_frac"] = roof["executed_tflops"] / dmma_peak
     roof["phase_ms"] = {k: float(v) for k, v in zip(names, ph)}
-    mixed = measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob, site, x_host)
-    mixed["tensor_memory_form"] = measure_mixed(a, plan, xd, yd, xp, yp, xh, yh, flush, info, world, pg, dev, snap, blob,
-                                                site, x_host, form="mixed_tc")
-    adjoint = measure_adjoint(a, plan, x_host, blob, site)
-    if not a.no_mixed_sweep:
-        mixed["sweep"] = mixed_sweeps(a, ctx, blob, sinfo)
+    extras = {}
+    if not a.no_extras:
+        hb = {"xh": xh, "y": yh}
+        mixed = measure_mixed(a, plan, xd, yd, xp, yp, hb, flush, info, world, pg, dev, snap, blob, site1, x_host)
+        mixed["tensor_memory_form"] = measure_mixed(a, plan, xd, yd, xp, yp, hb, flush, info, world, pg, dev, snap,
+                                                    blob, site1, x_host, form="mixed_tc")
+        extras["mixed"] = mixed
+        extras["adjoint"] = measure_adjoint(a, plan, x_host, mpo, site1)
+        herm = boundary_storage(d, plan)
+        del plan, d
+        dn, pn, _, _ = device_problem(ctx, h, V, sites, site1, a.M, hermitian=False)
+        extras["boundary_storage"] = {"hermitian_pairs": herm, "no_pairs": boundary_storage(dn, pn)}
+        del pn, dn
+        if a.sweeps > 0:
+            extras["sweep"] = sweep_comparison(a, ctx, h, V)
     cpu = None
-    if want_cpu:
-        cpu = cpu_baseline(snap, blob, site, x_host, info["flops"])
+    if want_oracle and world == 1:
+        cpu = cpu_baseline(snap, blob, site1, x_host, info["flops"])
     if rank == 0:
         line = {"metric": "H_eff.psi GFLOP/s (FP64 plain form)", "value": value, "unit": "GFLOP/s", "n_gpus": world,
                 "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": workload_name(a), "L": a.L, "M": a.M, "init_bond_dimension": a.init_bd,
-                           "seed": a.seed, "vec_len": n, "flops_per_step": info["flops"],
-                           "coefficient_block_doubles": info["w_len"], "s_len": info["s_len"], "t_len": info["t_len"],
-                           "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
-                "sweep": sinfo,
+                "config": config_of(a, fixture, info["flops"]),
+                "plan": {"vec_len": n, "coefficient_block_doubles": info["w_len"], "s_len": info["s_len"],
+                         "t_len": info["t_len"], "p_len": info["p_len"], "l_len": info["l_len"], "r_len": info["r_len"],
+                         "parallelism": f"replicas x{world}"},
                 "e2e": {"value": e2e_val, "unit": "GFLOP/s", "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
                 "gpu_launches": int(info["launches"]) * a.steps, "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
                 "fp64_peaks_tflops": {"dmma": dmma_peak, "dfma": dfma_peak},
-                "max_rel_err_vs_oracle": rel, "mixed": mixed, "adjoint": adjoint}
+                "max_rel_err_vs_oracle": rel, "twin_max_rel_diff_vs_oracle": twin_rel}
+        line.update(extras)
         print(json.dumps(line), flush=True)
-    del plan, d
     if pg is not None:
         pg.destroy_process_group()
 
@@ -440,9 +564,7 @@ def main():
     a = parse()
     world, rank, local, pg = dist_setup(a)
     if a.impl == "reference":
-        run_reference(a, world, rank, pg)
-        if pg is not None:
-            pg.destroy_process_group()
+        run_reference(a, world, rank)
         return
     run_b200(a, world, rank, local, pg)
 

@@ -382,6 +382,13 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
  * (the state canonize(0) leaves).  The right boundaries are built on the device. */
 int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* params, const qcm_mps_desc* sites,
                              const double* const* data, qcm_dmrg** out);
+/* Same, resuming the sweep at initial_site (ts_optimize initial_site_, optimize/ts_optimize.hpp:50-57):
+ * left boundaries over sites 0 .. initial_site-1 and right boundaries over L-1 .. initial_site, as
+ * init_left_right(mpo, initial_site) builds them (optimize/optimize.h:158-195); the next step is
+ * initial_site of the left-to-right half-sweep (qcm_dmrg_pending_plan gives its site problem).  The
+ * boundaries are built from the given MPS as it is (no optimisation or canonisation). */
+int qcm_dmrg_create_from_mps_at(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* params, const qcm_mps_desc* sites,
+                                const double* const* data, int initial_site, qcm_dmrg** out);
 int qcm_dmrg_length(const qcm_dmrg* d);
 /* Steps of one sweep: 2L - 2 (two-site) or 2L (single-site). */
 int qcm_dmrg_steps_per_sweep(const qcm_dmrg* d);

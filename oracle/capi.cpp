@@ -6,6 +6,7 @@
 #include <string>
 
 #include "dmrg.hpp"
+#include "mpo.hpp"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -72,6 +73,32 @@ int orc_max_threads(void) {
 }
 
 void orc_free(void* p) { std::free(p); }
+
+// The QC MPO of integrals h (L x L) and V (L^4), built by the package's builder (input preparation),
+// as a "QMPO" blob; free with orc_free.
+int orc_mpo_build_qc(int L, const double* h, const double* V, double cutoff, void** out, size_t* len) {
+    try {
+        if (L < 2 || !h || !V || !out || !len) return fail("orc_mpo_build_qc: bad arguments");
+        *out = dup_blob(qcm::serialize_mpo(qcm::build_qc_mpo(L, h, V, cutoff)), len);
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
+
+// The two-site site problem ("QSPB") at (site1, site1 + 1) of the MPS given as n_sites "QMPS" blobs,
+// with boundaries built from that MPS (no optimisation); free with orc_free.
+int orc_site_problem(const void* mpo_blob, size_t mn, int n_sites, const void* const* blobs, const size_t* lens, int site1,
+                     void** out, size_t* len) {
+    try {
+        bool ts = false;
+        auto mpo = load_mpo_blob(static_cast<const uint8_t*>(mpo_blob), mn, ts);
+        if (ts) return fail("orc_site_problem: expected a single-site MPO");
+        if (n_sites != int(mpo.size()) || !blobs || !lens || !out || !len) return fail("orc_site_problem: bad arguments");
+        std::vector<MPSTensor> mps;
+        for (int i = 0; i < n_sites; ++i) mps.push_back(load_mps_tensor(static_cast<const uint8_t*>(blobs[i]), lens[i]));
+        *out = dup_blob(site_problem_from_mps(mpo, mps, site1), len);
+        return 0;
+    } catch (const std::exception& e) { return fail(e.what()); }
+}
 
 int orc_dmrg_create(const void* blob, size_t n, int nup, int ndown, size_t Mmax, size_t init_bd, double cutoff, double tol,
                     int maxiter, double ecore, orc_dmrg** out) {

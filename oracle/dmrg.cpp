@@ -1046,6 +1046,17 @@ std::vector<uint8_t> save_site_problem(const MPSTensor& twin0, const Boundary& L
     return w.b;
 }
 
+std::vector<uint8_t> site_problem_from_mps(const std::vector<MPOTensor>& mpo, const std::vector<MPSTensor>& mps, int site1) {
+    const int L = int(mps.size());
+    if (int(mpo.size()) != L || site1 < 0 || site1 + 1 >= L) throw std::runtime_error("site problem: bad site or lengths");
+    Boundary left = trivial_boundary(mps[0].left, mpo[0].rows);
+    for (int i = 0; i < site1; ++i) left = overlap_mpo_left_step(mps[i], mps[i], left, mpo[i], true);
+    Boundary right = trivial_boundary(mps[L - 1].right, mpo[L - 1].cols);
+    for (int i = L - 1; i > site1 + 1; --i) right = overlap_mpo_right_step(mps[i], mps[i], right, mpo[i], true);
+    TwoSite tst(mps[site1], mps[site1 + 1]);
+    return save_site_problem(tst.make_mps(), left, right);
+}
+
 std::vector<uint8_t> save_mps_tensor(const MPSTensor& m0) {
     MPSTensor m = m0;
     m.make_right_paired();

@@ -114,6 +114,10 @@ struct DMRG {
 
 // frozen site problem ("QSPB" v1): twin MPS (right-paired) + L + R boundaries
 std::vector<uint8_t> save_site_problem(const MPSTensor& twin, const Boundary& L, const Boundary& R);
+// The two-site problem at (site1, site1 + 1) of a given MPS: left boundaries over sites 0 .. site1-1 and
+// right boundaries over L-1 .. site1+2, as init_left_right(mpo, site1) builds them (optimize.h:158-195;
+// symmetric steps, optimize.h:134-156), and the fused two-site tensor; exported as "QSPB".
+std::vector<uint8_t> site_problem_from_mps(const std::vector<MPOTensor>& mpo, const std::vector<MPSTensor>& mps, int site1);
 void load_site_problem(const uint8_t* p, std::size_t n, MPSTensor& twin, Boundary& L, Boundary& R);
 
 // one site tensor ("QMPS" v1): Index phys, left, right; right-paired blocks as in QSPB

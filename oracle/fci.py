@@ -95,6 +95,18 @@ class FCI:
                        return_eigenvectors=False)
         return np.sort(w)
 
+    def ground_state(self, tol: float = 1e-13):
+        """Lowest eigenpair (energy, normalised vector) by ARPACK."""
+        op = spla.LinearOperator((self.dim, self.dim), matvec=self.matvec, dtype=np.float64)
+        rng = np.random.default_rng(7)
+        w, Z = spla.eigsh(op, k=1, which="SA", tol=tol, v0=rng.standard_normal(self.dim))
+        c = Z[:, 0]
+        return float(w[0]), c / np.linalg.norm(c)
+
+    def one_rdm(self, c):
+        """Spin-summed one-particle density matrix gamma_pq = <c| sum_s a+_ps a_qs |c>."""
+        return np.array([[c @ (self.E[p][q] @ c) for q in range(self.L)] for p in range(self.L)])
+
     def dense(self):
         return np.column_stack([self.matvec(col) for col in np.eye(self.dim)])
 

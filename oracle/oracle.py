@@ -54,6 +54,8 @@ def lib(nthreads: int = 0):
         L.orc_dmrg_stats.argtypes = [c_void_p, P(c_double)]
         L.orc_dmrg_boundary_export.argtypes = [c_void_p, c_int, c_int, P(c_void_p), P(c_size_t)]
         L.orc_dmrg_mps_export.argtypes = [c_void_p, c_int, P(c_void_p), P(c_size_t)]
+        L.orc_mpo_build_qc.argtypes = [c_int, P(c_double), P(c_double), c_double, P(c_void_p), P(c_size_t)]
+        L.orc_site_problem.argtypes = [c_void_p, c_size_t, c_int, P(c_void_p), P(c_size_t), c_int, P(c_void_p), P(c_size_t)]
         L.orc_heff_apply.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_double), P(c_double), c_size_t,
                                      c_int, P(c_double), P(c_double)]
         L.orc_schedule_export.argtypes = [c_void_p, c_size_t, c_void_p, c_size_t, c_int, P(c_void_p), P(c_size_t),
@@ -170,6 +172,33 @@ class OracleDMRG:
         if getattr(self, "h", None) is not None and self.h.value:
             self.lib.orc_dmrg_free(self.h)
             self.h = c_void_p()
+
+
+def mpo_blob_qc(h: np.ndarray, V: np.ndarray, cutoff: float = 1e-20) -> bytes:
+    """QC MPO blob ("QMPO") of the integrals, built inside the oracle library (no product library)."""
+    L = lib()
+    h = np.ascontiguousarray(h, dtype=np.float64)
+    V = np.ascontiguousarray(V, dtype=np.float64)
+    p, n = c_void_p(), c_size_t()
+    _check(L, L.orc_mpo_build_qc(h.shape[0], _dp(h), _dp(V), cutoff, ctypes.byref(p), ctypes.byref(n)))
+    b = ctypes.string_at(p, n.value)
+    L.orc_free(p)
+    return b
+
+
+def site_problem(mpo_blob: bytes, site_blobs, site1: int) -> bytes:
+    """Frozen two-site problem ("QSPB") at (site1, site1 + 1) of the MPS given as "QMPS" blobs: boundaries
+    from init_left_right(mpo, site1) on that MPS, no optimisation."""
+    L = lib()
+    mb = ctypes.create_string_buffer(mpo_blob, len(mpo_blob))
+    bufs = [ctypes.create_string_buffer(b, len(b)) for b in site_blobs]
+    ptrs = (c_void_p * len(bufs))(*[ctypes.cast(b, c_void_p) for b in bufs])
+    lens = (c_size_t * len(bufs))(*[len(b) for b in site_blobs])
+    p, n = c_void_p(), c_size_t()
+    _check(L, L.orc_site_problem(mb, len(mpo_blob), len(bufs), ptrs, lens, site1, ctypes.byref(p), ctypes.byref(n)))
+    b = ctypes.string_at(p, n.value)
+    L.orc_free(p)
+    return b
 
 
 def heff_apply(snap: bytes, mpo_blob: bytes, site1: int, x: np.ndarray, repeat: int = 1):

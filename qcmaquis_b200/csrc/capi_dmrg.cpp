@@ -287,6 +287,11 @@ int qcm_dmrg_create(qcm_ctx* ctx, const qcm_mpo* mpo, int nup, int ndown, const 
 
 int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* prm, const qcm_mps_desc* sites,
                              const double* const* data, qcm_dmrg** out) {
+    return qcm_dmrg_create_from_mps_at(ctx, mpo, prm, sites, data, 0, out);
+}
+
+int qcm_dmrg_create_from_mps_at(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_params* prm, const qcm_mps_desc* sites,
+                                const double* const* data, int initial_site, qcm_dmrg** out) {
     QCM_TRY
     if (!ctx || !mpo || !prm || !sites || !data || !out) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_create_from_mps: NULL argument");
     const qcm::MPO& m = qcm::mpo_of(mpo);
@@ -308,7 +313,7 @@ int qcm_dmrg_create_from_mps(qcm_ctx* ctx, const qcm_mpo* mpo, const qcm_dmrg_pa
     qcm::MPO ts = qcm::make_twosite_mpo(m);
     auto d = std::make_unique<qcm_dmrg>();
     d->ctx = ctx;
-    d->e = std::make_unique<qcm::DevDMRG>(m.t, ts.t, std::move(ms), p, ctx->stream);
+    d->e = std::make_unique<qcm::DevDMRG>(m.t, ts.t, std::move(ms), p, ctx->stream, initial_site);
     *out = d.release();
     return QCM_OK;
     QCM_CATCH

@@ -284,9 +284,11 @@ struct DevDMRG {
     // const MPS over the allowed sectors of (nup, ndown), canonised to site 0
     DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, int nup, int ndown,
             const DMRGParams& prm, cudaStream_t s);
-    // given MPS (right-normalised on sites 1 .. L-1, as after canonize(0))
+    // given MPS (right-normalised on sites 1 .. L-1, as after canonize(0)); initial_site > 0 resumes the
+    // sweep at that site (ts_optimize's initial site): left boundaries over sites 0 .. site-1, right
+    // boundaries over L-1 .. site (init_left_right(mpo, site), optimize.h:158-195), next step = site
     DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, std::vector<DMPS> sites,
-            const DMRGParams& prm, cudaStream_t s);
+            const DMRGParams& prm, cudaStream_t s, int initial_site = 0);
     // excited states (ts_optimize.hpp:217-223, optimize.h:134-172): ortho states in both pairings and
     // their overlap boundaries with the current MPS
     std::vector<std::vector<DMPS>> ortho_lp, ortho_rp;
@@ -311,7 +313,7 @@ struct DevDMRG {
     void step_sites(int step, int& lr, int& site1, int& site2) const;
 
   private:
-    void init_boundaries();
+    void init_boundaries(int site = 0);
     void step(int step, double& energy, TruncResults& tr);
     void step_single(int step, double& energy, TruncResults& tr);
     int last_iters = 0;  // JD iterations of the last step

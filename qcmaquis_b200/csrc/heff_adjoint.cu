@@ -233,12 +233,20 @@ HeffAdjointWork& adjoint_work(HeffPlan& p) {
     for (const OutD& o : p.outs)
         for (uint32_t k = 0; k < o.seg_count; ++k) {
             const SegD& sg = p.segs[o.seg_start + k];
-            if (sg.tr) throw std::runtime_error("heff adjoint: transposed boundary cohorts are not supported");
             GemmJob j{};
             j.a_off = sg.l_off; j.b_off = o.y_off; j.c_off = sg.s_off;
             j.M = sg.nS * sg.ls_in; j.N = o.N; j.K = o.M;
-            j.lda = o.M; j.ldb = o.M; j.ldc = sg.nS * sg.ls_in;
-            j.ta = 1; j.tb = 0; j.alpha = 1.0; j.beta = 0.0;
+            j.ldb = o.M; j.ldc = sg.nS * sg.ls_in;
+            j.tb = 0; j.alpha = 1.0; j.beta = 0.0;
+            if (!sg.tr) {
+                // L_eff = the cohort's nS blocks (M x ls_in each) side by side: Sbar = L_eff^T ybar
+                j.lda = o.M; j.ta = 1;
+            } else {
+                // a transposed cohort reads its Hermitian partner's blocks (ls_in x M each), so block b of
+                // L_eff^T is the stored block itself: row blocks of ls_in rows, block b at b * M * ls_in
+                j.lda = sg.ls_in; j.ta = 0;
+                j.arb = sg.ls_in; j.a_bs = uint64_t(o.M) * sg.ls_in;
+            }
             w->sjobs.push_back(j);
         }
     cudaStream_t s = p.stream;

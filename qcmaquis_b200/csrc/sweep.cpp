@@ -378,7 +378,7 @@ DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTens
 }
 
 DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTensor>& twosite, std::vector<DMPS> sites,
-                 const DMRGParams& prm, cudaStream_t s)
+                 const DMRGParams& prm, cudaStream_t s, int initial_site)
     : mpo(single), ts_mpo(twosite), mps(std::move(sites)), p(prm) {
     c.s = s;
     QCM_CUDA(cudaGetDevice(&c.device));
@@ -388,18 +388,26 @@ DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTens
         throw std::runtime_error("DMRG: need L site tensors, L MPO tensors and L - 1 two-site tensors");
     for (int i = 0; i + 1 < L; ++i)
         if (!(mps[i].right == mps[i + 1].left)) throw std::runtime_error("DMRG: site tensors do not share their bond indices");
-    init_boundaries();
+    const int last = p.single_site ? L - 1 : L - 2;
+    if (initial_site < 0 || initial_site > last) throw std::runtime_error("DMRG: initial site outside the left-to-right half-sweep");
+    init_boundaries(initial_site);
 }
 
-void DevDMRG::init_boundaries() {
+void DevDMRG::init_boundaries(int site) {
     left_.resize(L + 1);
     right_.resize(L + 1);
     left_[0] = trivial_boundary(mps[0].left, mpo[0].rows, c.s);
     right_[L] = trivial_boundary(mps[L - 1].right, mpo[L - 1].cols, c.s);
-    for (int i = L - 1; i >= 0; --i) {
+    for (int i = 0; i < site; ++i) {
+        make_left_paired(c, mps[i]);
+        DMPS ket = right_paired_copy(c, mps[i]);
+        left_[i + 1] = boundary_step_left(c, *left_[i], ket, mps[i], mpo[i], true);
+    }
+    for (int i = L - 1; i >= site; --i) {
         make_right_paired(c, mps[i]);
         right_[i] = boundary_step_right(c, *right_[i + 1], mps[i], mpo[i], true);
     }
+    next_step = site;
     QCM_CUDA(cudaStreamSynchronize(c.s));
 }
 

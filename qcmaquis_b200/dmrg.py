@@ -62,6 +62,7 @@ _lib._sig("qcm_boundary_step_right", c_int, c_void_p, c_void_p, c_void_p, c_int,
           P(c_void_p))
 _lib._sig("qcm_dmrg_create", c_int, c_void_p, c_void_p, c_int, c_int, P(DMRGParams), P(c_void_p))
 _lib._sig("qcm_dmrg_create_from_mps", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)),
+_lib._sig("qcm_dmrg_create_from_mps_at", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)), c_int,
           P(c_void_p))
 _lib._sig("qcm_dmrg_length", c_int, c_void_p)
 _lib._sig("qcm_dmrg_steps_per_sweep", c_int, c_void_p)
@@ -205,17 +206,18 @@ class DMRG:
     @classmethod
     def from_mps(cls, ctx, mpo, sites, max_bond_dimension: int, truncation_cutoff: float = 1e-16,
                  jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0, heev: dict | None = None,
-                 precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite"):
+                 precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite", initial_site: int = 0):
         """Restart from a given MPS: sites = [dict(phys, left, right, blocks)] with right-paired blocks
-        (one per left sector, in sector order), sites 1 .. L-1 right-normalised."""
+        (one per left sector, in sector order), sites 1 .. L-1 right-normalised.  initial_site > 0 resumes
+        the sweep at that site (boundaries built from the given MPS, qcm_dmrg_create_from_mps_at)."""
         self = cls.__new__(cls)
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore, heev,
                     precision, jcd_gmres, optimization)
         descs, ptrs, keep = _pack_sites(sites)
         h = c_void_p()
-        check(lib.qcm_dmrg_create_from_mps(ctx.h, mpo.handle, ctypes.byref(p), descs, ptrs, ctypes.byref(h)),
-              "qcm_dmrg_create_from_mps")
+        check(lib.qcm_dmrg_create_from_mps_at(ctx.h, mpo.handle, ctypes.byref(p), descs, ptrs, initial_site,
+                                              ctypes.byref(h)), "qcm_dmrg_create_from_mps_at")
         self.h = h
         self.L = lib.qcm_dmrg_length(h)
         self.steps = lib.qcm_dmrg_steps_per_sweep(h)

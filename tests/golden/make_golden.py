@@ -8,6 +8,11 @@
   given, otherwise the committed value is kept.
 * *_fci: exact diagonalisation (oracle/fci.py); config 1 uses the dense
   4900 x 4900 eigensolver.
+* hubbard_ladder_6x2_local_density_{up,down}_reference: the per-site densities
+  the same reference test asserts (reference_value('Local density up'/'down'),
+  tolerance 1e-3), read from that file like the energy;
+  hubbard_ladder_6x2_fci_local_density: gamma_ii / 2 of the exact ground state
+  (N_up = N_down, so each spin carries half the spin-summed density).
 * config1_oracle_sweep_energies: per-sweep energies (min over the sweep's
   steps, results_collector.h:147) of the oracle's two-site DMRG for config 1
   (L=8, N=8, TwoU1 Sz=0, M=64, 4 sweeps, tol 1e-10, maxiter 8, const init).
@@ -38,8 +43,17 @@ def main():
         txt = open(os.path.join(sys.argv[1], "dmrg/regression/applications/dmrg/test_fermiladder_ts.py")).read()
         ref = float(re.search(r"Energy\D*?([0-9]+\.[0-9]+)", txt).group(1))
     g["hubbard_ladder_6x2_reference"] = ref
+    for spin in ("up", "down"):
+        key = f"hubbard_ladder_6x2_local_density_{spin}_reference"
+        g[key] = old.get(key)
+        if len(sys.argv) > 1:
+            m = re.search(r"reference_value\('Local density " + spin + r"',\s*value=\[([^\]]*)\]", txt)
+            g[key] = [float(v) for v in m.group(1).split(",")]
     h, V, e = hubbard_ladder_integrals(6)
     g["hubbard_ladder_6x2_fci"] = fci_energy(h, V, e, 10, 10)
+    f = FCI(h, V, e, 10, 10)
+    E0, c0 = f.ground_state()
+    g["hubbard_ladder_6x2_fci_local_density"] = [float(x) / 2 for x in np.diag(f.one_rdm(c0))]
     h, V, e = synthetic_integrals(8, 0)
     g["config1_fci"] = float(np.linalg.eigvalsh(FCI(h, V, e, 4, 4).dense())[0])
     m = MPO.qc(h, V)

@@ -207,6 +207,15 @@ def test_ladder_reference_energy_on_device(gpu_ctx):
     assert abs(Es[-1] - ref) / ref < 1e-3  # the reference test's own tolerance
     assert abs(Es[-1] - ref) < 1e-8
     assert abs(Es[-1] - golden["hubbard_ladder_6x2_fci"]) < 1e-8
+    # the same test's local densities (reference_value 'Local density up' / 'down', tolerance 1e-3): the
+    # device MPS's one-particle density matrix, half its diagonal per spin (N_up = N_down)
+    g = dev.measure_1rdm()
+    n_spin = np.diag(g) / 2
+    for spin in ("up", "down"):
+        dref = np.array(golden[f"hubbard_ladder_6x2_local_density_{spin}_reference"])
+        assert np.abs(n_spin - dref).max() < 1e-3
+        assert np.abs(n_spin - dref).max() < 1e-6, (n_spin, dref)
+    assert abs(np.trace(g) - 20.0) < 1e-8
 
 
 @pytest.mark.parametrize("nup,ndown", [(4, 3), (3, 3)])

@@ -24,6 +24,17 @@ def test_fci_matches_golden():
     assert abs(E - GOLDEN["hubbard_ladder_6x2_fci"]) < 1e-10
 
 
+def test_fci_ladder_densities_match_reference_values():
+    """The reference test's per-site densities (test_fermiladder_ts.py, 'Local density up/down') equal the
+    exact ground state's (gamma_ii / 2 per spin) far inside the test's own tolerance 1e-3."""
+    fci = np.array(GOLDEN["hubbard_ladder_6x2_fci_local_density"])
+    for spin in ("up", "down"):
+        ref = np.array(GOLDEN[f"hubbard_ladder_6x2_local_density_{spin}_reference"])
+        assert ref.shape == (12,)
+        assert np.abs(fci - ref).max() < 1e-3
+        assert np.abs(fci - ref).max() < 1e-9
+
+
 def test_oracle_ladder_reference_energy():
     """Oracle two-site DMRG reproduces the reference's golden ladder energy."""
     h, V, e = hubbard_ladder_integrals(6)
