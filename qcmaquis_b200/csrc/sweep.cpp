@@ -62,7 +62,9 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
     if (no > 0 && (!opt->ortho || opt->ortho_ld < n)) throw std::runtime_error("jacobi_davidson: bad ortho vectors");
     // V[0..maxiter), VA[0..maxiter), u, r, the ortho vectors, the GMRES basis (gm + 1) and the
     // correction operator's temporary
-    const uint64_t nvec = 2 * uint64_t(maxiter) + 2 + uint64_t(no) + (gm > 0 ? uint64_t(gm) + 2 : 0);
+    // (+ three vectors for the mixed form's FP64 correction: H u, t, H t)
+    const uint64_t nmx = mixed ? 3 : 0;
+    const uint64_t nvec = 2 * uint64_t(maxiter) + 2 + uint64_t(no) + (gm > 0 ? uint64_t(gm) + 2 : 0) + nmx;
     Ctx::ensure(c.jd, nvec * ld);
     Ctx::ensure(c.scal, 256 + 64 * uint64_t(DOT_PARTS));
     Ctx::ensure(c.coef, 64);
@@ -73,6 +75,7 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
     double* O = r + ld;
     double* G = O + uint64_t(no) * ld;
     double* tmp = G + uint64_t(gm + 1) * ld;
+    double* MX = V + (nvec - nmx) * ld;
     // scalar slots: 0-1 norms, 2.. MGS dots, 80.. Rayleigh-Ritz column, 160-164 residual / Rayleigh
     // quotient, 170.. GMRES Hessenberg column and |w|^2, 241-242 operator dots, 243-246 projections
     double* sc = c.scal.get();
@@ -109,6 +112,69 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
             dev_dots(Oi(a), 0, 1, t, n, sc + 243, dsc, c.s);
             dev_axpy_dscalar(sc + 243, -inv_oo[a], Oi(a), t, n, c.s);
         }
+    };
+    // The mixed form's FP64 residual correction (north star form 1): u (the mixed solve's vector) gets an
+    // FP64 apply for its Rayleigh quotient and residual; then, while that residual is above tol |theta|
+    // and steps remain, one Jacobi-Davidson step in FP64: t = -r + (r.u)/(u.u) u projected and made
+    // orthogonal to u, Rayleigh-Ritz on span{u, t} (2 x 2, FP64 H.psi of t).  Returns the FP64
+    // eigenvalue, u normalised.
+    const double mixed_floor = opt ? opt->mixed_floor : MIXED_RESIDUAL_FLOOR;
+    const int mixed_refine = opt ? opt->mixed_refine : 0;
+    int fp64_applies = 0;
+    auto fp64_correction = [&](double* uu, double* rr, double th) -> double {
+        double* Hu = MX;
+        double* t = MX + ld;
+        double* Ht = MX + 2 * ld;
+        dev_dots(uu, 0, 1, uu, n, sc + 164, dsc, c.s);
+        double q[3];
+        download(c, sc + 164, q, 1);
+        dev_axpby(1.0 / std::sqrt(q[0]), uu, 0.0, uu, n, c.s);
+        heff_apply_device(p, uu, Hu);
+        ++fp64_applies;
+        project(Hu);
+        dev_dots(uu, 0, 1, Hu, n, sc + 163, dsc, c.s);
+        download(c, sc + 163, q, 1);
+        th = q[0];
+        for (int k = 0;; ++k) {
+            // r = Hu - theta u (FP64)
+            QCM_CUDA(cudaMemcpyAsync(rr, Hu, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
+            dev_axpby(-th, uu, 1.0, rr, n, c.s);
+            dev_dots(rr, 0, 1, rr, n, sc + 160, dsc, c.s);
+            dev_dots(rr, 0, 1, uu, n, sc + 161, dsc, c.s);
+            download(c, sc + 160, q, 2);
+            const double rn64 = std::sqrt(q[0]);
+            if (k >= mixed_refine || rn64 <= tol * std::fabs(th) || rn64 < tol) break;
+            // t = -r + (r.u) u, projected, orthogonal to u, normalised
+            dev_axpby(-1.0, rr, 0.0, t, n, c.s);
+            dev_axpby(q[1], uu, 1.0, t, n, c.s);
+            project(t);
+            dev_dots(uu, 0, 1, t, n, sc + 165, dsc, c.s);
+            dev_axpy_dscalar(sc + 165, -1.0, uu, t, n, c.s);
+            dev_dots(t, 0, 1, t, n, sc + 166, dsc, c.s);
+            download(c, sc + 166, q, 1);
+            if (!(q[0] > 0.0)) break;
+            dev_axpby(1.0 / std::sqrt(q[0]), t, 0.0, t, n, c.s);
+            heff_apply_device(p, t, Ht);
+            ++fp64_applies;
+            project(Ht);
+            dev_dots(t, 0, 1, Ht, n, sc + 167, dsc, c.s);
+            dev_dots(uu, 0, 1, Ht, n, sc + 168, dsc, c.s);
+            download(c, sc + 167, q, 2);
+            // lowest eigenpair of [[th, b], [b, d]]
+            const double a11 = th, b = q[1], d = q[0];
+            const double mid = 0.5 * (a11 + d), half = 0.5 * (a11 - d);
+            const double lam = mid - std::sqrt(half * half + b * b);
+            // eigenvector (cu, ct) of lam, normalised
+            double cu = b, ct = lam - a11;
+            if (std::fabs(cu) + std::fabs(ct) == 0.0) { cu = 1.0; ct = 0.0; }
+            const double nrm = std::sqrt(cu * cu + ct * ct);
+            cu /= nrm;
+            ct /= nrm;
+            dev_axpby(ct, t, cu, uu, n, c.s);
+            dev_axpby(ct, Ht, cu, Hu, n, c.s);
+            th = lam;
+        }
+        return th;
     };
     QCM_CUDA(cudaMemcpyAsync(Vi(0), x, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
     project(Vi(0));
@@ -219,22 +285,16 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         ++it;
         const double rn = std::sqrt(h3[0]);
         // the mixed H.psi carries ~1e-7 relative error: its residual cannot fall below that level
-        const double rtol = mixed ? std::max(tol, MIXED_RESIDUAL_FLOOR) : tol;
+        const double rtol = mixed ? std::max(tol, mixed_floor) : tol;
         if (rn <= rtol * std::fabs(theta) || rn < tol || it >= maxiter) {
             if (mixed) {
-                // FP64 Rayleigh quotient of the final vector: its error is O(|r|^2 / gap), so the
-                // energy keeps FP64 accuracy although the vector carries the mixed form's error
-                heff_apply_device(p, u, r);
-                dev_dots(u, 0, 1, r, n, sc + 163, dsc, c.s);
-                dev_dots(u, 0, 1, u, n, sc + 164, dsc, c.s);
-                double q[2];
-                download(c, sc + 163, q, 2);
-                theta = q[0] / q[1];
                 check_mixed(p);
+                theta = fp64_correction(u, r, theta);
             }
             QCM_CUDA(cudaMemcpyAsync(x, u, n * sizeof(double), cudaMemcpyDeviceToDevice, c.s));
             iters = it;
             if (applies) *applies = napply;
+            if (opt) const_cast<JDOptions*>(opt)->fp64_applies = fp64_applies;
             return theta;
         }
         // correction t0 = -r + (r.u)/(u.u) u, then GMRES on -r with abs_tol 2^-(it+1)
@@ -478,6 +538,8 @@ double DevDMRG::solve(HeffPlan& plan, DMPS& x, const std::function<void(std::siz
     int iters = 0, napply = 0;
     JDOptions jo;
     jo.gmres = p.jcd_gmres;
+    jo.mixed_floor = p.mixed_floor;
+    jo.mixed_refine = p.mixed_refine;
     // ortho vectors of this step (ts_optimize.hpp:217-223, ss_optimize.hpp:104-109)
     DBuf<double> ovec;
     if (!ortho_rp.empty()) {
@@ -494,8 +556,8 @@ double DevDMRG::solve(HeffPlan& plan, DMPS& x, const std::function<void(std::siz
     st.hpsi_count += uint64_t(napply);
     st.hpsi_flops += double(napply) * plan.flops;
     if (p.precision != 0) {
-        st.hpsi_count64 += 1;  // the FP64 Rayleigh-quotient apply
-        st.hpsi_flops64 += plan.flops;
+        st.hpsi_count64 += uint64_t(jo.fp64_applies);  // the FP64 residual correction's applies
+        st.hpsi_flops64 += double(jo.fp64_applies) * plan.flops;
     }
     last_iters = iters;
     return E;

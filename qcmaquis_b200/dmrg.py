@@ -21,15 +21,19 @@ class DMRGParams(ctypes.Structure):
                 ("jcd_tol", c_double), ("jcd_maxiter", ctypes.c_int32), ("ecore", c_double),
                 ("twosite_truncation", ctypes.c_int32), ("alpha_initial", c_double), ("alpha_main", c_double),
                 ("alpha_final", c_double), ("ngrowsweeps", ctypes.c_int32), ("nmainsweeps", ctypes.c_int32),
-                ("hpsi_precision", ctypes.c_int32), ("jcd_gmres", ctypes.c_int32), ("optimization", ctypes.c_int32)]
+                ("hpsi_precision", ctypes.c_int32), ("jcd_gmres", ctypes.c_int32), ("optimization", ctypes.c_int32),
+                ("mixed_residual_floor", c_double), ("mixed_fp64_refine", ctypes.c_int32)]
 
 
 OPTIMIZATION = {"twosite": 0, "singlesite": 1}
 
 
-def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmres=0, optimization="twosite"):
+def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmres=0, optimization="twosite",
+            mixed_floor=0.0, mixed_refine=1):
     """heev: None (svd truncation) or dict(alpha_initial, alpha_main, alpha_final, ngrowsweeps, nmainsweeps);
-    precision: "fp64" or "mixed" (JD with the mixed H.psi and an FP64 Rayleigh quotient per step);
+    precision: "fp64" or "mixed" (JD with the mixed H.psi, then the FP64 residual correction: the FP64
+    Rayleigh quotient and up to mixed_refine FP64 correction steps; mixed_floor: residual floor of the
+    mixed iterations, 0 for the default 1e-7);
     gmres: ietl_jcd_gmres, GMRES iterations per JD correction;
     optimization: "twosite" (ts_optimize) or "singlesite" (ss_optimize: the alphas of heev, or its defaults,
     are the noise of every step's growth)."""
@@ -38,7 +42,8 @@ def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmr
     h = heev or {}
     return DMRGParams(M, init_bd, cutoff, tol, maxiter, ecore, 1 if heev else 0, h.get("alpha_initial", 1e-2),
                       h.get("alpha_main", 1e-4), h.get("alpha_final", 1e-8), h.get("ngrowsweeps", 0),
-                      h.get("nmainsweeps", 0), precision_mode(precision), gmres, OPTIMIZATION[optimization])
+                      h.get("nmainsweeps", 0), precision_mode(precision), gmres, OPTIMIZATION[optimization],
+                      mixed_floor, mixed_refine)
 
 
 class TruncResult(ctypes.Structure):
@@ -62,6 +67,7 @@ _lib._sig("qcm_boundary_step_right", c_int, c_void_p, c_void_p, c_void_p, c_int,
           P(c_void_p))
 _lib._sig("qcm_dmrg_create", c_int, c_void_p, c_void_p, c_int, c_int, P(DMRGParams), P(c_void_p))
 _lib._sig("qcm_dmrg_create_from_mps", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)),
+          P(c_void_p))
 _lib._sig("qcm_dmrg_create_from_mps_at", c_int, c_void_p, c_void_p, P(DMRGParams), P(MPSDesc), P(P(c_double)), c_int,
           P(c_void_p))
 _lib._sig("qcm_dmrg_length", c_int, c_void_p)
@@ -193,10 +199,11 @@ class DMRG:
 
     def __init__(self, ctx, mpo, nup: int, ndown: int, max_bond_dimension: int, init_bond_dimension: int | None = None,
                  truncation_cutoff: float = 1e-16, jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0,
-                 heev: dict | None = None, precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite"):
+                 heev: dict | None = None, precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite",
+                 mixed_floor: float = 0.0, mixed_refine: int = 1):
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, init_bond_dimension or max_bond_dimension, truncation_cutoff, jcd_tol,
-                    jcd_maxiter, ecore, heev, precision, jcd_gmres, optimization)
+                    jcd_maxiter, ecore, heev, precision, jcd_gmres, optimization, mixed_floor, mixed_refine)
         h = c_void_p()
         check(lib.qcm_dmrg_create(ctx.h, mpo.handle, nup, ndown, ctypes.byref(p), ctypes.byref(h)), "qcm_dmrg_create")
         self.h = h
@@ -206,14 +213,15 @@ class DMRG:
     @classmethod
     def from_mps(cls, ctx, mpo, sites, max_bond_dimension: int, truncation_cutoff: float = 1e-16,
                  jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0, heev: dict | None = None,
-                 precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite", initial_site: int = 0):
+                 precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite", initial_site: int = 0,
+                 mixed_floor: float = 0.0, mixed_refine: int = 1):
         """Restart from a given MPS: sites = [dict(phys, left, right, blocks)] with right-paired blocks
         (one per left sector, in sector order), sites 1 .. L-1 right-normalised.  initial_site > 0 resumes
         the sweep at that site (boundaries built from the given MPS, qcm_dmrg_create_from_mps_at)."""
         self = cls.__new__(cls)
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, max_bond_dimension, truncation_cutoff, jcd_tol, jcd_maxiter, ecore, heev,
-                    precision, jcd_gmres, optimization)
+                    precision, jcd_gmres, optimization, mixed_floor, mixed_refine)
         descs, ptrs, keep = _pack_sites(sites)
         h = c_void_p()
         check(lib.qcm_dmrg_create_from_mps_at(ctx.h, mpo.handle, ctypes.byref(p), descs, ptrs, initial_site,

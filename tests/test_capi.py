@@ -78,3 +78,9 @@ def test_schedule_bookkeeping_matches_oracle(L, M, sw, step):
         assert any(r[2] != r[3] for r in ro)
     with pytest.raises(_lib.QcmError, match="host-only"):
         plan.apply(np.zeros(plan.n))
+
+
+def test_package_modules_import():
+    import importlib
+    for m in ("qcmaquis_b200.heff", "qcmaquis_b200.dmrg", "qcmaquis_b200.mpo", "qcmaquis_b200.fcidump"):
+        importlib.import_module(m)
