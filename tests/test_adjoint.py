@@ -122,3 +122,48 @@ def test_device_energy_gradient(gpu_ctx):
                       gmres=8)[0]
         fd = (Ep - Em) / (2 * STEP)
         assert abs(fd - g @ D) <= 1e-6 * max(abs(fd), 1.0), (fd, g @ D)
+
+
+@pytest.mark.gpu
+def test_config4_energy_gradient_finite_differences(gpu_ctx):
+    """The differentiation form's configuration (L=16, N=16, TwoU1 Sz=0, M=256): after device sweeps, at the
+    middle bond's converged lowest eigenvector psi the adjoint with x = ybar = psi is dE/d scale for every
+    two-site MPO entry (Hellmann-Feynman, boundaries fixed).  Central differences of the lowest eigenvalue
+    (step 1e-5 relative to each scale, 20 seeded random directions) agree to 1e-6 relative, for the FP64
+    eigensolver and for the mixed one (mixed H.psi, FP64 Rayleigh quotient)."""
+    from qcmaquis_b200 import heff
+    from qcmaquis_b200.dmrg import DMRG, jd_solve
+    L, M = 16, 256
+    h, V, e, m, ts, blob = qc_system(L, 0)
+    d = DMRG(gpu_ctx, m, L // 2, L // 2, M, 64)
+    for _ in range(3):
+        d.sweep()
+    site = L // 2 - 1
+    d.run(site)
+    p = heff.parse_site_problem(d.pending_export())
+    del d
+    plan = heff.plan_from_problem(gpu_ctx, p, ts, site)
+    x0 = heff.twin_vector(p)
+    E, psi, it = jd_solve(plan, x0, 1e-13, 64, gmres=8)
+    psi = psi / np.linalg.norm(psi)
+    _, g = plan.adjoint(psi, psi)
+    assert abs(g @ ts.terms(site)["scale"] - E) <= 1e-10 * abs(E)  # Euler: E is linear in the scales
+    sc = ts.terms(site)["scale"]
+    rng = np.random.default_rng(4)
+    errs, errs_mixed = [], []
+    for k in range(N_DIRECTIONS):
+        D = rng.standard_normal(sc.size) * np.abs(sc)
+        pp = heff.plan_from_problem(gpu_ctx, p, perturbed(ts, site, sc, D, STEP), site)
+        pm = heff.plan_from_problem(gpu_ctx, p, perturbed(ts, site, sc, D, -STEP), site)
+        Ep = jd_solve(pp, psi, 1e-13, 64, gmres=8)[0]
+        Em = jd_solve(pm, psi, 1e-13, 64, gmres=8)[0]
+        fd = (Ep - Em) / (2 * STEP)
+        errs.append(abs(fd - g @ D) / max(abs(fd), 1e-3 * abs(E)))
+        if k < 5:
+            Ep = jd_solve(pp, psi, 1e-13, 64, precision="mixed")[0]
+            Em = jd_solve(pm, psi, 1e-13, 64, precision="mixed")[0]
+            fd = (Ep - Em) / (2 * STEP)
+            errs_mixed.append(abs(fd - g @ D) / max(abs(fd), 1e-3 * abs(E)))
+        del pp, pm
+    assert max(errs) < 1e-6, errs
+    assert max(errs_mixed) < 1e-6, errs_mixed

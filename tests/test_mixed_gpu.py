@@ -70,9 +70,10 @@ def test_mixed_jd_matches_oracle_step_energy(gpu_ctx, L, M, sw, step, form):
     assert abs(vec @ plan.apply(vec) / (vec @ vec) - ev) < 1e-10
 
 
-@pytest.mark.parametrize("L,M,sweeps", [(8, 32, 3)])
+@pytest.mark.parametrize("L,M,sweeps", [(8, 32, 3), (12, 128, 4)])
 def test_mixed_sweeps_match_oracle(gpu_ctx, L, M, sweeps):
-    """Both engines start from the oracle's initial MPS; the device runs every JD in the mixed form."""
+    """Both engines start from the oracle's initial MPS; the device runs every JD in the mixed form (with
+    its FP64 residual correction) and the oracle in FP64: every sweep's energy within 1e-6 Eh."""
     from oracle.oracle import OracleDMRG
     from qcmaquis_b200.dmrg import DMRG
     from qcmaquis_b200.heff import parse_mps_tensor
@@ -87,10 +88,15 @@ def test_mixed_sweeps_match_oracle(gpu_ctx, L, M, sweeps):
         # the sweep energy (minimum over its steps, as the reference reports it) within the target
         assert abs(E.min() - E_ref.min()) < SWEEP_TOL, (s, E.min() - E_ref.min())
         dev_steps.append(np.abs(E - E_ref).max())
-        bd = np.array([t["bond_dimension"] for t in tr])
-        assert np.array_equal(bd, bd_ref.astype(np.int64)), (s, bd, bd_ref)
+        if M <= 32:
+            # (at M = 128 the cut meets singular values that the mixed vectors move by ~1e-7)
+            bd = np.array([t["bond_dimension"] for t in tr])
+            assert np.array_equal(bd, bd_ref.astype(np.int64)), (s, bd, bd_ref)
     # step energies of a growing sweep follow the unconverged JD path (8 iterations), so they
     # differ more than the precision does; once converged every step is within the target
     assert dev_steps[-1] < SWEEP_TOL, dev_steps
     st = dev.stats()
-    assert st["hpsi_count_fp64"] == sweeps * (2 * L - 2)  # one FP64 Rayleigh quotient per step
+    # the FP64 residual correction: the Rayleigh quotient of each step's final vector, and at most
+    # one FP64 correction step (the default mixed_refine)
+    nsteps = sweeps * (2 * L - 2)
+    assert nsteps <= st["hpsi_count_fp64"] <= 2 * nsteps
