@@ -358,9 +358,10 @@ typedef struct {
                                      L-1 .. 0, each solved with the single-site MPO tensor and grown by
                                      the density-matrix prediction with noise alpha_*; twosite_truncation
                                      does not apply) */
-    double mixed_residual_floor;  /* QCM_PRECISION_MIXED*: the mixed iterations of a step's JD stop once
-                                     |r| <= max(jcd_tol, this) |theta| (<= 0: 1e-7, the mixed H.psi's
-                                     relative error level) */
+    double mixed_residual_floor;  /* QCM_PRECISION_MIXED*: the mixed iterations of a step's JD stop as the
+                                     FP64 ones do (|r| <= jcd_tol |theta| or jcd_maxiter), and also once
+                                     |r| <= this |theta| and |r| no longer halves: below the mixed H.psi's
+                                     relative error the residual is noise (<= 0: 1e-7) */
     int32_t mixed_fp64_refine;    /* QCM_PRECISION_MIXED*: FP64 residual-correction steps after them (0: only
                                      the FP64 Rayleigh quotient of the final vector); each is one FP64
                                      H.psi and one Jacobi-Davidson step while |r| > jcd_tol |theta| */

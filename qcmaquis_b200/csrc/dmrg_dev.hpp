@@ -200,8 +200,9 @@ TruncResults grow_r2l(Ctx& c, DMPS& a, DMPS& b, const DevBoundary& R, const MPOT
 // Jacobi-Davidson for the lowest eigenpair (solve_ietl_jcd, solver/ietl_jacobi_davidson.h:35-76;
 // ietl/jacobi.h:386-474): x (device, plan vector layout) holds the start vector and receives the
 // eigenvector.
-// mixed: every H.psi in the mixed form (heff_apply_device_mixed), stopping once the residual
-// is below max(tol, mixed_floor) |theta|; then the FP64 residual correction: one FP64 H.psi gives the
+// mixed: every H.psi in the mixed form (heff_apply_device_mixed), stopping by the FP64 rule or once
+// the residual is below mixed_floor |theta| and no longer halves; then the FP64 residual correction:
+// one FP64 H.psi gives the
 // Rayleigh quotient and the FP64 residual of the final vector, and up to mixed_refine Jacobi-Davidson
 // steps in FP64 (the correction t = -r + (r.u)/(u.u) u, Rayleigh-Ritz on span{u, t}, one FP64 H.psi
 // each) improve it while its FP64 residual is above tol |theta|.  The returned eigenvalue is FP64.
@@ -266,7 +267,7 @@ struct DMRGParams {
     int ngrowsweeps = 0, nmainsweeps = 0;
     int precision = 0;  // H.psi form of the JD (QCM_PRECISION_*); mixed: FP64 Rayleigh quotient per step
     double mixed_floor = MIXED_RESIDUAL_FLOOR;  // mixed JD: residual floor of its mixed iterations
-    int mixed_refine = 1;                       // mixed JD: FP64 correction steps at most
+    int mixed_refine = 0;                       // mixed JD: FP64 correction steps at most
     // optimization = singlesite (ss_optimize.hpp:59-186): 2L steps per sweep over sites 0 .. L-1, L-1 .. 0,
     // each solved with the single-site MPO tensor and grown with the alphas above (heev does not apply)
     bool single_site = false;

@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
@@ -121,6 +122,7 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
     const double mixed_floor = opt ? opt->mixed_floor : MIXED_RESIDUAL_FLOOR;
     const int mixed_refine = opt ? opt->mixed_refine : 0;
     int fp64_applies = 0;
+    double rn_prev = std::numeric_limits<double>::infinity();
     auto fp64_correction = [&](double* uu, double* rr, double th) -> double {
         double* Hu = MX;
         double* t = MX + ld;
@@ -284,9 +286,12 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         download(c, sc + 160, h3, 3);
         ++it;
         const double rn = std::sqrt(h3[0]);
-        // the mixed H.psi carries ~1e-7 relative error: its residual cannot fall below that level
-        const double rtol = mixed ? std::max(tol, mixed_floor) : tol;
-        if (rn <= rtol * std::fabs(theta) || rn < tol || it >= maxiter) {
+        // The mixed H.psi carries ~1e-7 relative error, so its residual is noise below that level:
+        // the mixed iterations follow the FP64 stopping rule, and also stop once the residual is
+        // below mixed_floor |theta| and no longer halves (the FP64 solve would converge there)
+        const bool stalled = mixed && rn <= mixed_floor * std::fabs(theta) && rn > 0.5 * rn_prev;
+        rn_prev = rn;
+        if (rn <= tol * std::fabs(theta) || rn < tol || it >= maxiter || stalled) {
             if (mixed) {
                 check_mixed(p);
                 theta = fp64_correction(u, r, theta);

@@ -29,7 +29,7 @@ OPTIMIZATION = {"twosite": 0, "singlesite": 1}
 
 
 def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmres=0, optimization="twosite",
-            mixed_floor=0.0, mixed_refine=1):
+            mixed_floor=0.0, mixed_refine=0):
     """heev: None (svd truncation) or dict(alpha_initial, alpha_main, alpha_final, ngrowsweeps, nmainsweeps);
     precision: "fp64" or "mixed" (JD with the mixed H.psi, then the FP64 residual correction: the FP64
     Rayleigh quotient and up to mixed_refine FP64 correction steps; mixed_floor: residual floor of the
@@ -200,7 +200,7 @@ class DMRG:
     def __init__(self, ctx, mpo, nup: int, ndown: int, max_bond_dimension: int, init_bond_dimension: int | None = None,
                  truncation_cutoff: float = 1e-16, jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0,
                  heev: dict | None = None, precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite",
-                 mixed_floor: float = 0.0, mixed_refine: int = 1):
+                 mixed_floor: float = 0.0, mixed_refine: int = 0):
         self.ctx, self.mpo = ctx, mpo
         p = _params(max_bond_dimension, init_bond_dimension or max_bond_dimension, truncation_cutoff, jcd_tol,
                     jcd_maxiter, ecore, heev, precision, jcd_gmres, optimization, mixed_floor, mixed_refine)
@@ -214,7 +214,7 @@ class DMRG:
     def from_mps(cls, ctx, mpo, sites, max_bond_dimension: int, truncation_cutoff: float = 1e-16,
                  jcd_tol: float = 1e-10, jcd_maxiter: int = 8, ecore: float = 0.0, heev: dict | None = None,
                  precision="fp64", jcd_gmres: int = 0, optimization: str = "twosite", initial_site: int = 0,
-                 mixed_floor: float = 0.0, mixed_refine: int = 1):
+                 mixed_floor: float = 0.0, mixed_refine: int = 0):
         """Restart from a given MPS: sites = [dict(phys, left, right, blocks)] with right-paired blocks
         (one per left sector, in sector order), sites 1 .. L-1 right-normalised.  initial_site > 0 resumes
         the sweep at that site (boundaries built from the given MPS, qcm_dmrg_create_from_mps_at)."""
