@@ -243,6 +243,37 @@ int qcm_heff_profile(qcm_heff* h, const double* x_dev, double* y_dev, float* ms)
 int qcm_heff_profile_mode(qcm_heff* h, const double* x_dev, double* y_dev, float* ms, int precision);
 void qcm_heff_free(qcm_heff* h);
 
+/* Groups of independent plans (the batching form; no counterpart in the reference, which runs one
+ * schedule per solve and splits a schedule's ket sectors over devices and threads,
+ * solver/tasks.cpp:884-977).  A group merges the work lists of n plans of one context into one plan:
+ * one apply of the group runs every member's H_eff in one launch sequence (T-GEMM, S build and
+ * split-K L.S per tile shape), each member's arithmetic unchanged, so member i's result equals
+ * qcm_heff_apply on that plan bit for bit.  The members' vectors live in one arena of arena_len
+ * doubles: member i's vector (its vec_len doubles, the qcm_heff_apply layout) at offsets[i]; the
+ * gaps between them are ignored on input and zero on output.  The members must outlive the group;
+ * FP64 only.  Typical use: many small independent site problems (for example one step of each of many
+ * independent DMRG solves), whose separate applies would be bound by launch latency. */
+typedef struct qcm_heff_group qcm_heff_group;
+int qcm_heff_group_create(qcm_ctx* ctx, qcm_heff* const* plans, int n, qcm_heff_group** out);
+/* *arena_len, and offsets[n] / lengths[n] of the members (any may be NULL). */
+int qcm_heff_group_layout(const qcm_heff_group* g, uint64_t* arena_len, uint64_t* offsets, uint64_t* lengths);
+/* vec_len (the arena length), buffer sizes, flop counts (summed over the members) and launches. */
+int qcm_heff_group_get_info(const qcm_heff_group* g, qcm_heff_info* info);
+/* y = H_eff x for every member; host arenas (synchronous) or device arenas (enqueued on the context
+ * stream). */
+int qcm_heff_group_apply(qcm_heff_group* g, const double* x, double* y);
+int qcm_heff_group_apply_device(qcm_heff_group* g, const double* x_dev, double* y_dev);
+/* Lowest eigenpair of every member by Jacobi-Davidson in lockstep (host arenas x0 -> out; evals[n],
+ * iters[n]; *applies: group applies run).  Each iteration applies all members at once and runs the
+ * rest of the iteration (classical Gram-Schmidt twice, Rayleigh-Ritz on the device, residuals,
+ * convergence |r| <= tol |theta| or |r| < tol, next direction -r + (r.u)/(u.u) u as in
+ * ietl/jacobi.h:386-474) for all members in single launches; with use_graphs each iteration is
+ * captured once as a CUDA graph and replayed.  A converged member keeps its eigenpair; the group
+ * stops when every member has converged or after maxiter (1..16) iterations. */
+int qcm_jd_solve_batched(qcm_heff_group* g, const double* x0, double tol, int maxiter, int use_graphs, double* out,
+                         double* evals, int* iters, int* applies);
+void qcm_heff_group_free(qcm_heff_group* g);
+
 /* No counterpart in the reference.  For callers that cannot allocate device memory
  * when they need H.psi -- a host code whose HBM is owned by its own caching
  * allocator (a cudaMalloc here may fail or fragment it) or a solver loop that

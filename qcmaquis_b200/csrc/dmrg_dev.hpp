@@ -228,6 +228,16 @@ constexpr int JD_MAX_GMRES = 64;
 double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, int& iters, int precision = 0,
                        const JDOptions* opt = nullptr, int* applies = nullptr);
 
+// Jacobi-Davidson for many independent site problems in lockstep on a merged plan group (the batching
+// form): X (device, the group's vector arena) holds the start vectors and receives the eigenvectors;
+// solve i's entries are X[xo[i] .. xo[i] + xn[i]).  Every iteration applies all H_eff in one launch
+// sequence and runs the rest (classical Gram-Schmidt twice, device Rayleigh-Ritz, residuals,
+// convergence, next direction) for all solves at once; with use_graphs each iteration is captured as a
+// CUDA graph and replayed.  maxiter <= 16; ev / iters per solve; *applies: group applies run.
+void jacobi_davidson_batched(HeffPlan& g, const std::vector<uint64_t>& xo, const std::vector<uint64_t>& xn, double* X,
+                             double tol, int maxiter, std::vector<double>& ev, std::vector<int>& iters, bool use_graphs,
+                             int* applies);
+
 // Boundary steps (contractions/boundary_ops/move_boundary.hpp:147-404): new left boundary
 // from L[site] and mps[site]; new right boundary from R[site+1] and mps[site].
 std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& L, const DMPS& ket_rp, const DMPS& bra_lp,

@@ -257,6 +257,15 @@ struct HeffPlan {
 
     const DevBoundary* L = nullptr;
     const DevBoundary* R = nullptr;
+    // a merged plan (merge_plans): the boundaries and coefficient blocks of its member plans are
+    // addressed from these bases (its job offsets are relative to them); FP64 applies only
+    bool merged = false;
+    const double* base_L = nullptr;
+    const double* base_R = nullptr;
+    const double* base_W = nullptr;
+    const double* l_data() const { return merged ? base_L : L->data.get(); }
+    const double* r_data() const { return merged ? base_R : R->data.get(); }
+    const double* w_data() const { return merged ? base_W : d_W.get(); }
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     const double* graph_x = nullptr;
@@ -299,6 +308,13 @@ void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<T
 void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const uint32_t* line_b1,
                const uint64_t* slice_off, const uint16_t* klist, const double* W, const double* T, double* S,
                cudaStream_t s);
+// Many plans as one (the batching form): the work lists of `plans` concatenated into one merged
+// plan whose vector is the arena of the plans' vectors (plan i's at xo[i], each rounded up to 32
+// doubles); T, S and the split-K partials get merged buffers, the boundaries and coefficient blocks
+// stay in the plans' buffers (which must outlive the merged plan).  heff_apply_device on the merged
+// plan applies every member's H_eff in one launch sequence, with each member's arithmetic unchanged.
+std::unique_ptr<HeffPlan> merge_plans(const std::vector<HeffPlan*>& plans, std::vector<uint64_t>& xo, cudaStream_t s);
+void upload_merged(HeffPlan& g);
 // Same apply with caller-provided scratch: Tb (t_len), Sb (s_len) and Pb (p_len) doubles.
 void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* Tb, double* Sb, double* Pb);
 

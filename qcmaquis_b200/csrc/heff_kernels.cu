@@ -446,21 +446,21 @@ void launch_t(HeffPlan& p, int sh, const double* x, double* Tb, cudaStream_t s, 
               float* Tlo = nullptr) {
     if (!p.ttiles[sh].empty())
         k_tgemm<S><<<unsigned(p.ttiles[sh].size()), NTHR, 0, s>>>(p.d_tjobs.get(), p.d_ttiles[sh].get(), x,
-                                                                  p.R->data.get(), Tb, Thi, Tlo);
+                                                                  p.r_data(), Tb, Thi, Tlo);
 }
 
 template <class S>
 void launch_s(HeffPlan& p, int sh, const double* Tb, double* Sb, cudaStream_t s) {
     if (!p.utiles[sh].empty())
         k_sgemm<S><<<unsigned(p.utiles[sh].size()), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get(), p.d_line_b1.get(),
-                                                                  p.d_slice_off.get(), p.d_klist.get(), p.d_W.get(), Tb, Sb);
+                                                                  p.d_slice_off.get(), p.d_klist.get(), p.w_data(), Tb, Sb);
 }
 
 template <class S>
 void launch_ls(HeffPlan& p, int sh, const double* Sb, double* Pb, double* y, cudaStream_t s) {
     if (p.kitems[sh].empty()) return;
     k_lspart<S><<<unsigned(p.kitems[sh].size()), NTHR, 0, s>>>(p.d_kitems[sh].get(), p.d_otiles[sh].get(), p.d_outs.get(),
-                                                               p.d_segs.get(), p.L->data.get(), Sb, Pb);
+                                                               p.d_segs.get(), p.l_data(), Sb, Pb);
     const dim3 rg(unsigned(p.otiles[sh].size()), unsigned((S::BM * S::BN + 255) / 256));
     k_lsreduce<S><<<rg, 256, 0, s>>>(p.d_otiles[sh].get(), p.d_outs.get(), Pb, y);
 }
@@ -530,6 +530,7 @@ void heff_tgemm_device(HeffPlan& p, const double* x, double* T) {
 }
 
 void prepare_mixed(HeffPlan& p, bool tc) {
+    if (p.merged) throw std::runtime_error("a merged plan group applies in FP64 only");
     AllocStream scope(p.stream);
     if (!p.d_merr.size()) {
         p.d_merr.alloc(1);
@@ -595,6 +596,45 @@ int heff_launches_per_apply(const HeffPlan& p) {
         n += p.kitems[sh].empty() ? 0 : 2;
     }
     return n;
+}
+
+// The merged plan's work lists (member plans validated each against their own buffers when staged;
+// here the merged T, S and k-step lists are checked again) and its own T, S and partial buffers.
+void upload_merged(HeffPlan& p) {
+    cudaStream_t s = p.stream;
+    for (const TJobD& j : p.tjobs)
+        if (j.brs == 0 || j.N % j.brs || j.sst < j.brs * j.M || j.sst % 4 || j.c_off % 4 ||
+            j.c_off + uint64_t(j.N / j.brs) * j.sst > p.t_len || j.a_off + uint64_t(j.K ? j.K - 1 : 0) * j.lda + j.M > p.x_len)
+            throw std::runtime_error("plan group: T job outside the merged buffers");
+    for (const UnitD& u : p.units)
+        if (u.nk && u.slice0 + u.nk > p.slice_off.size()) throw std::runtime_error("plan group: unit outside its slices");
+    for (std::size_t k = 0; k < p.slice_off.size(); ++k)
+        if (p.slice_off[k] % 4 || p.slice_off[k] > p.t_len) throw std::runtime_error("plan group: T slice misplaced");
+    for (int sh = 0; sh < N_SHAPES; ++sh)
+        for (const TileD& t : p.utiles[sh])
+            if (t.item >= p.units.size() || std::size_t(t.pad) >= p.klist.size() ||
+                std::size_t(t.pad) + 1 + p.klist[t.pad] > p.klist.size())
+                throw std::runtime_error("plan group: S tile outside its work lists");
+    for (const OutD& o : p.outs)
+        if (o.y_off + uint64_t(o.M) * o.N > p.x_len || o.seg_start + o.seg_count > p.segs.size())
+            throw std::runtime_error("plan group: output block outside the arena");
+    p.d_tjobs.upload(p.tjobs, s);
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        p.d_ttiles[sh].upload(p.ttiles[sh], s);
+        p.d_utiles[sh].upload(p.utiles[sh], s);
+        p.d_otiles[sh].upload(p.otiles[sh], s);
+        p.d_kitems[sh].upload(p.kitems[sh], s);
+    }
+    p.d_units.upload(p.units, s);
+    p.d_line_b1.upload(p.line_b1, s);
+    p.d_slice_off.upload(p.slice_off, s);
+    p.d_klist.upload(p.klist, s);
+    p.d_segs.upload(p.segs, s);
+    p.d_outs.upload(p.outs, s);
+    p.d_T.alloc(p.t_len);
+    p.d_S.alloc(p.s_len);
+    p.d_P.alloc(p.p_len);
+    QCM_CUDA(cudaStreamSynchronize(s));
 }
 
 void upload_plan(HeffPlan& p) {

@@ -91,6 +91,14 @@ def precision_mode(precision) -> int:
     return m[precision]
 NOALLOC_SCRATCH_DOUBLES = 8 * 1024 * 1024
 _lib._sig("qcm_heff_free", None, c_void_p)
+_lib._sig("qcm_heff_group_create", c_int, c_void_p, P(c_void_p), c_int, P(c_void_p))
+_lib._sig("qcm_heff_group_layout", c_int, c_void_p, P(c_uint64), P(c_uint64), P(c_uint64))
+_lib._sig("qcm_heff_group_get_info", c_int, c_void_p, P(HeffInfo))
+_lib._sig("qcm_heff_group_apply", c_int, c_void_p, P(c_double), P(c_double))
+_lib._sig("qcm_heff_group_apply_device", c_int, c_void_p, c_void_p, c_void_p)
+_lib._sig("qcm_jd_solve_batched", c_int, c_void_p, P(c_double), c_double, c_int, c_int, P(c_double), P(c_double),
+          P(ctypes.c_int), P(ctypes.c_int))
+_lib._sig("qcm_heff_group_free", None, c_void_p)
 _lib._sig("qcm_probe_fp64_peaks", c_int, P(c_double), P(c_double))
 
 
@@ -400,3 +408,63 @@ def plan_from_problem(ctx: Context, problem: dict, ts_mpo, site: int, bookkeepin
     L = Boundary(ctx, problem["L"])
     R = Boundary(ctx, problem["R"])
     return HeffPlan(ctx, L, R, ts_mpo, site, problem["phys"], problem["left"], problem["right"], bookkeeping)
+
+
+class HeffGroup:
+    """Independent plans of one context merged into one (qcm_heff_group): one apply or one lockstep
+    Jacobi-Davidson for all of them.  Vectors are arenas of n doubles, member i's at offsets[i]."""
+
+    def __init__(self, ctx, plans):
+        self.ctx, self.plans = ctx, list(plans)
+        arr = (c_void_p * len(self.plans))(*[p.h.value if isinstance(p.h, c_void_p) else p.h for p in self.plans])
+        h = c_void_p()
+        check(lib.qcm_heff_group_create(ctx.h, arr, len(self.plans), ctypes.byref(h)), "qcm_heff_group_create")
+        self.h = h
+        n = c_uint64()
+        self.offsets = np.zeros(len(self.plans), np.uint64)
+        self.lengths = np.zeros(len(self.plans), np.uint64)
+        u64 = lambda a: a.ctypes.data_as(P(c_uint64))
+        check(lib.qcm_heff_group_layout(h, ctypes.byref(n), u64(self.offsets), u64(self.lengths)), "qcm_heff_group_layout")
+        self.n = int(n.value)
+        info = HeffInfo()
+        check(lib.qcm_heff_group_get_info(h, ctypes.byref(info)), "qcm_heff_group_get_info")
+        self.info = {f: getattr(info, f) for f, _ in HeffInfo._fields_}
+
+    def pack(self, xs) -> np.ndarray:
+        out = np.zeros(self.n)
+        for x, o, l in zip(xs, self.offsets, self.lengths):
+            assert x.size == l
+            out[int(o):int(o) + int(l)] = x
+        return out
+
+    def unpack(self, arena):
+        return [arena[int(o):int(o) + int(l)].copy() for o, l in zip(self.offsets, self.lengths)]
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert x.size == self.n
+        y = np.empty_like(x)
+        check(lib.qcm_heff_group_apply(self.h, _lib.dptr(x), _lib.dptr(y)), "qcm_heff_group_apply")
+        return y
+
+    def apply_device(self, x_ptr: int, y_ptr: int):
+        check(lib.qcm_heff_group_apply_device(self.h, c_void_p(x_ptr), c_void_p(y_ptr)), "qcm_heff_group_apply_device")
+
+    def jd_solve(self, x0: np.ndarray, tol: float = 1e-10, maxiter: int = 8, graphs: bool = True):
+        """Lockstep Jacobi-Davidson of every member: (eigenvalues, eigenvector arena, iterations, group applies)."""
+        x0 = np.ascontiguousarray(x0, dtype=np.float64)
+        assert x0.size == self.n
+        out = np.empty_like(x0)
+        k = len(self.plans)
+        ev = np.zeros(k)
+        it = np.zeros(k, dtype=np.int32)
+        na = ctypes.c_int()
+        check(lib.qcm_jd_solve_batched(self.h, _lib.dptr(x0), tol, maxiter, 1 if graphs else 0, _lib.dptr(out),
+                                       _lib.dptr(ev), it.ctypes.data_as(P(ctypes.c_int)), ctypes.byref(na)),
+              "qcm_jd_solve_batched")
+        return ev, out, it, na.value
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            lib.qcm_heff_group_free(self.h)
+            self.h = c_void_p()
