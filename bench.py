@@ -27,7 +27,9 @@ Reported beside the metric (not part of it): the mixed-precision forms of the
 same step; the adjoint; `--sweeps` full two-site sweeps of the configuration
 from the const initial state in the FP64 form and in the mixed form (per-sweep
 time, energy, truncated weight and the mixed form's deviations); one
-single-site sweep; the boundary storage with and without the Hermitian pairs.
+single-site sweep; the boundary storage with and without the Hermitian pairs;
+the batching form (128 independent L=12, M=128 problems as one plan group:
+grouped apply and lockstep Jacobi-Davidson against separate ones).
 
 The reference arm (--impl reference) times the CPU restatement of the same
 H.psi (the oracle: OpenMP over ket sectors, OpenBLAS dgemm, all host threads)
@@ -66,6 +68,7 @@ def parse():
     ap.add_argument("--no-mixed-sweep", action="store_true", help="skip the mixed-precision sweeps")
     ap.add_argument("--no-single-site-sweep", action="store_true", help="skip the single-site sweep")
     ap.add_argument("--no-extras", action="store_true", help="the metric only (no sweeps, forms, adjoint)")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-solve form")
     return ap.parse_args()
 
 
@@ -412,6 +415,67 @@ def single_site_sweep(a, ctx, m, d, e_ts):
         return {"error": f"{type(ex).__name__}: {ex}"}
 
 
+def batched_solves(a, ctx, n=128, L=12, M=128):
+    """The batching form on the batched-solve configuration: n independent problems (synthetic Hamiltonians
+    of L orbitals, N = L, seeds 1 .. n; MPS over the bond sectors of a converged M state, seeded entries), the
+    two-site problem at the middle bond of each.  Their plans merged into one group: one apply of all against
+    n separate applies, and one lockstep Jacobi-Davidson (each iteration a CUDA graph) against n separate
+    solves (tol 1e-10, maxiter 8), with the largest eigenvalue difference."""
+    import torch
+    from qcmaquis_b200 import heff
+    from qcmaquis_b200.dmrg import jd_solve
+    fd = _fcidump()
+    phys, bonds, fixture = bond_sectors(argparse.Namespace(L=L, M=M))
+    site1 = L // 2 - 1
+    t0 = time.perf_counter()
+    dmrgs, plans, xs = [], [], []
+    for seed in range(1, n + 1):
+        h, V, _ = fd.synthetic_integrals(L, seed)
+        d, plan, x, _ = device_problem(ctx, h, V, synthetic_mps(phys, bonds, seed), site1, M)
+        dmrgs.append(d); plans.append(plan); xs.append(x)
+    g = heff.HeffGroup(ctx, plans)
+    setup = time.perf_counter() - t0
+    dev = torch.device("cuda", torch.cuda.current_device())
+    X = torch.from_numpy(g.pack(xs)).to(dev)
+    Y = torch.empty_like(X)
+    xd = [torch.from_numpy(x).to(dev) for x in xs]
+    yd = [torch.empty_like(x) for x in xd]
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps):
+        for _ in range(3):
+            fn()
+        ctx.synchronize()
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        ctx.synchronize()
+        return (time.perf_counter() - t) / reps
+
+    t_group = timed(lambda: g.apply_device(X.data_ptr(), Y.data_ptr()), 20)
+    t_sep = timed(lambda: [p.apply_device(x.data_ptr(), y.data_ptr()) for p, x, y in zip(plans, xd, yd)], 5)
+    x0 = g.pack(xs)
+    t = time.perf_counter()
+    evb, _, itb, napply = g.jd_solve(x0, 1e-10, 8, graphs=True)
+    t_jd_group = time.perf_counter() - t
+    t = time.perf_counter()
+    ev_sep = [jd_solve(p, x, 1e-10, 8)[0] for p, x in zip(plans, xs)]
+    t_jd_sep = time.perf_counter() - t
+    flops = g.info["flops"]
+    out = {"workload": (f"{n} independent two-site problems at the middle bond: synthetic Hamiltonians L={L} N={L} "
+                        f"TwoU1 Sz=0 seeds 1..{n}, MPS over the bond sectors of a converged M={M} state ({fixture}), "
+                        f"seeded entries"),
+           "setup_s": setup, "flops_per_group_apply": flops, "launches_per_group_apply": int(g.info["launches"]),
+           "group_apply_ms": t_group * 1e3, "separate_applies_ms": t_sep * 1e3,
+           "group_apply_gflops": flops / t_group / 1e9, "separate_applies_gflops": flops / t_sep / 1e9,
+           "group_jd_s": t_jd_group, "separate_jd_s": t_jd_sep, "group_jd_applies": napply,
+           "jd_max_abs_eigenvalue_diff": float(np.max(np.abs(np.array(ev_sep) - evb))),
+           "note": "wall times with host synchronisation; the group JD replays one CUDA graph per iteration"}
+    del g, plans, dmrgs
+    return out
+
+
 def sweep_comparison(a, ctx, h, V):
     """FP64 and mixed-form sweeps from the same const state: per-sweep time, energy, truncated weight, and
     the mixed form's deviations from the FP64 sweeps (the FP64 device sweeps match the oracle's to 1e-10 Eh
@@ -539,6 +603,11 @@ def run_b200(a, world, rank, local, pg):
         del pn, dn
         if a.sweeps > 0:
             extras["sweep"] = sweep_comparison(a, ctx, h, V)
+        if not a.no_batched:
+            try:
+                extras["batched"] = batched_solves(a, ctx)
+            except FileNotFoundError as ex:  # the sector fixture of the batched configuration is missing
+                extras["batched"] = {"error": str(ex)}
     cpu = None
     if want_oracle and world == 1:
         cpu = cpu_baseline(snap, blob, site1, x_host, info["flops"])

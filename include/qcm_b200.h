@@ -390,9 +390,11 @@ typedef struct {
                                      the density-matrix prediction with noise alpha_*; twosite_truncation
                                      does not apply) */
     double mixed_residual_floor;  /* QCM_PRECISION_MIXED*: the mixed iterations of a step's JD stop as the
-                                     FP64 ones do (|r| <= jcd_tol |theta| or jcd_maxiter), and also once
-                                     |r| <= this |theta| and |r| no longer halves: below the mixed H.psi's
-                                     relative error the residual is noise (<= 0: 1e-7) */
+                                     FP64 ones do (|r| <= jcd_tol |theta| or jcd_maxiter), so that the sweep
+                                     follows the FP64 sweep's path; > 0: they also stop once |r| <= this
+                                     |theta| and |r| no longer halves (below the mixed H.psi's relative
+                                     error, ~1e-7, the residual is noise): fewer applies in converged
+                                     sweeps, a path that can leave the FP64 one by ~1e-5 Eh early on */
     int32_t mixed_fp64_refine;    /* QCM_PRECISION_MIXED*: FP64 residual-correction steps after them (0: only
                                      the FP64 Rayleigh quotient of the final vector); each is one FP64
                                      H.psi and one Jacobi-Davidson step while |r| > jcd_tol |theta| */

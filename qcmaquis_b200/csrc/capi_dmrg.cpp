@@ -257,7 +257,7 @@ const char* to_params(const qcm_dmrg_params& prm, qcm::DMRGParams& p) {
     p.precision = prm.hpsi_precision;
     p.single_site = prm.optimization == QCM_OPTIMIZATION_SINGLESITE;
     if (prm.mixed_fp64_refine < 0 || prm.mixed_fp64_refine > 64) return "qcm_dmrg: mixed_fp64_refine must be in 0..64";
-    p.mixed_floor = prm.mixed_residual_floor > 0 ? prm.mixed_residual_floor : qcm::MIXED_RESIDUAL_FLOOR;
+    p.mixed_floor = prm.mixed_residual_floor > 0 ? prm.mixed_residual_floor : 0.0;
     p.mixed_refine = prm.mixed_fp64_refine;
     return nullptr;
 }

@@ -200,13 +200,13 @@ TruncResults grow_r2l(Ctx& c, DMPS& a, DMPS& b, const DevBoundary& R, const MPOT
 // Jacobi-Davidson for the lowest eigenpair (solve_ietl_jcd, solver/ietl_jacobi_davidson.h:35-76;
 // ietl/jacobi.h:386-474): x (device, plan vector layout) holds the start vector and receives the
 // eigenvector.
-// mixed: every H.psi in the mixed form (heff_apply_device_mixed), stopping by the FP64 rule or once
-// the residual is below mixed_floor |theta| and no longer halves; then the FP64 residual correction:
-// one FP64 H.psi gives the
+// mixed: every H.psi in the mixed form (heff_apply_device_mixed), stopping by the FP64 rule (and, with
+// mixed_floor > 0, once the residual is below mixed_floor |theta| and no longer halves); then the FP64
+// residual correction: one FP64 H.psi gives the
 // Rayleigh quotient and the FP64 residual of the final vector, and up to mixed_refine Jacobi-Davidson
 // steps in FP64 (the correction t = -r + (r.u)/(u.u) u, Rayleigh-Ritz on span{u, t}, one FP64 H.psi
 // each) improve it while its FP64 residual is above tol |theta|.  The returned eigenvalue is FP64.
-constexpr double MIXED_RESIDUAL_FLOOR = 1e-7;
+constexpr double MIXED_RESIDUAL_FLOOR = 1e-7;  // the mixed H.psi's relative error: a floor worth setting
 // Beyond the plain solve: the correction equation (I - uu*)(A - theta)(I - uu*) t = -r solved by
 // GMRES with `gmres` iterations from t0 = -r + (r.u)/(u.u) u (jcd_gmres_solver, ietl/jacobi.h:126-164;
 // ietl_gmres, ietl/gmres.h:78-146; 0 = t0 itself), and the search space kept orthogonal to n_ortho
@@ -217,8 +217,8 @@ struct JDOptions {
     const double* ortho = nullptr;
     int n_ortho = 0;
     uint64_t ortho_ld = 0;
-    double mixed_floor = MIXED_RESIDUAL_FLOOR;  // mixed form: residual floor of its own iterations
-    int mixed_refine = 0;                       // mixed form: FP64 correction steps after them
+    double mixed_floor = 0.0;  // mixed form: residual floor of its own iterations (0: none)
+    int mixed_refine = 0;      // mixed form: FP64 correction steps after them
     int fp64_applies = 0;                       // out: FP64 applies of a mixed solve
 };
 constexpr int JD_MAX_GMRES = 64;
@@ -276,8 +276,8 @@ struct DMRGParams {
     double alpha_initial = 1e-2, alpha_main = 1e-4, alpha_final = 1e-8;
     int ngrowsweeps = 0, nmainsweeps = 0;
     int precision = 0;  // H.psi form of the JD (QCM_PRECISION_*); mixed: FP64 Rayleigh quotient per step
-    double mixed_floor = MIXED_RESIDUAL_FLOOR;  // mixed JD: residual floor of its mixed iterations
-    int mixed_refine = 0;                       // mixed JD: FP64 correction steps at most
+    double mixed_floor = 0.0;  // mixed JD: residual floor of its mixed iterations (0: none)
+    int mixed_refine = 0;      // mixed JD: FP64 correction steps at most
     // optimization = singlesite (ss_optimize.hpp:59-186): 2L steps per sweep over sites 0 .. L-1, L-1 .. 0,
     // each solved with the single-site MPO tensor and grown with the alphas above (heev does not apply)
     bool single_site = false;

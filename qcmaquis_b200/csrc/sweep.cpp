@@ -119,7 +119,7 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
     // and steps remain, one Jacobi-Davidson step in FP64: t = -r + (r.u)/(u.u) u projected and made
     // orthogonal to u, Rayleigh-Ritz on span{u, t} (2 x 2, FP64 H.psi of t).  Returns the FP64
     // eigenvalue, u normalised.
-    const double mixed_floor = opt ? opt->mixed_floor : MIXED_RESIDUAL_FLOOR;
+    const double mixed_floor = opt ? opt->mixed_floor : 0.0;
     const int mixed_refine = opt ? opt->mixed_refine : 0;
     int fp64_applies = 0;
     double rn_prev = std::numeric_limits<double>::infinity();
@@ -286,10 +286,11 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
         download(c, sc + 160, h3, 3);
         ++it;
         const double rn = std::sqrt(h3[0]);
-        // The mixed H.psi carries ~1e-7 relative error, so its residual is noise below that level:
-        // the mixed iterations follow the FP64 stopping rule, and also stop once the residual is
-        // below mixed_floor |theta| and no longer halves (the FP64 solve would converge there)
-        const bool stalled = mixed && rn <= mixed_floor * std::fabs(theta) && rn > 0.5 * rn_prev;
+        // The mixed iterations follow the FP64 stopping rule, so that a sweep in the mixed form takes
+        // the FP64 sweep's path; with a floor (mixed_floor > 0) they also stop once the residual is
+        // below mixed_floor |theta| and no longer halves: below the mixed H.psi's relative error
+        // (~1e-7) the residual is noise, and a converged step then costs fewer applies
+        const bool stalled = mixed && mixed_floor > 0.0 && rn <= mixed_floor * std::fabs(theta) && rn > 0.5 * rn_prev;
         rn_prev = rn;
         if (rn <= tol * std::fabs(theta) || rn < tol || it >= maxiter || stalled) {
             if (mixed) {

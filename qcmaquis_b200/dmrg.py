@@ -32,8 +32,9 @@ def _params(M, init_bd, cutoff, tol, maxiter, ecore, heev, precision="fp64", gmr
             mixed_floor=0.0, mixed_refine=0):
     """heev: None (svd truncation) or dict(alpha_initial, alpha_main, alpha_final, ngrowsweeps, nmainsweeps);
     precision: "fp64" or "mixed" (JD with the mixed H.psi, then the FP64 residual correction: the FP64
-    Rayleigh quotient and up to mixed_refine FP64 correction steps; mixed_floor: residual floor of the
-    mixed iterations, 0 for the default 1e-7);
+    Rayleigh quotient and up to mixed_refine FP64 correction steps; mixed_floor: 0 (the default) stops the
+    mixed iterations by the FP64 rule, so the sweep follows the FP64 sweep's path; > 0 also stops them once
+    the residual stalls below mixed_floor |theta|);
     gmres: ietl_jcd_gmres, GMRES iterations per JD correction;
     optimization: "twosite" (ts_optimize) or "singlesite" (ss_optimize: the alphas of heev, or its defaults,
     are the noise of every step's growth)."""
