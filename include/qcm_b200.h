@@ -410,8 +410,13 @@ typedef struct {
     uint64_t hpsi_count;
     double hpsi_flops; /* reference flop count (ScheduleNew::total_flops) summed over the applies */
     double plan_s, jd_s, trunc_s, boundary_s, total_s; /* wall time per phase, summed over sweeps */
-    uint64_t hpsi_count_fp64;  /* mixed form: the FP64 Rayleigh-quotient applies (not in hpsi_count) */
+    uint64_t hpsi_count_fp64;  /* mixed form: the FP64 applies of the residual correction (not in hpsi_count) */
     double hpsi_flops_fp64;
+    /* step plans built from scratch, and re-staged from the previous sweep's plan of the same step
+     * (whose boundaries and site indices had the same structure: sectors, cohorts, block offsets,
+     * conjugate scales), which skips the host schedule construction
+     * (create_contraction_schedule, site_hamil_schedule.hpp:42-93) */
+    uint64_t plans_built, plans_reused;
 } qcm_dmrg_stats;
 
 /* mpo: single-site QC MPO; nup/ndown: u1_total_charge1/2.  Builds the const

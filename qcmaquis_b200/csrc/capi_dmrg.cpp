@@ -557,6 +557,8 @@ int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* s) {
     s->trunc_s = t.trunc_s;
     s->boundary_s = t.boundary_s;
     s->total_s = t.total_s;
+    s->plans_built = t.plans_built;
+    s->plans_reused = t.plans_reused;
     return QCM_OK;
 }
 

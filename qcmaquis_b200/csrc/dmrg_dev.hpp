@@ -284,6 +284,7 @@ struct DMRGParams {
 };
 
 struct DMRGStats {
+    uint64_t plans_built = 0, plans_reused = 0;  // step plans built from scratch / re-staged from the cache
     uint64_t hpsi_count = 0;
     uint64_t hpsi_count64 = 0;   // mixed form: the extra FP64 applies (Rayleigh quotients)
     double hpsi_flops64 = 0;
@@ -331,6 +332,18 @@ struct DevDMRG {
     void step_sites(int step, int& lr, int& site1, int& site2) const;
 
   private:
+    // H_eff plans of the previous sweep's steps, kept on the host with their device buffers released:
+    // a step whose boundaries and site indices have the same structure (the same sectors, cohorts,
+    // block offsets and conjugate scales) as its cached plan's re-stages that plan (work lists
+    // uploaded, coefficient blocks regenerated on the device) instead of rebuilding the schedule.
+    struct CachedPlan {
+        std::unique_ptr<HeffPlan> plan;
+        uint64_t key = 0;
+    };
+    std::vector<CachedPlan> plan_cache_;
+    std::unique_ptr<HeffPlan> plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
+                                       const Index& phys, const Index& left, const Index& right, uint64_t& key);
+    void keep_plan(int step, std::unique_ptr<HeffPlan> plan, uint64_t key);
     void init_boundaries(int site = 0);
     void step(int step, double& energy, TruncResults& tr);
     void step_single(int step, double& energy, TruncResults& tr);

@@ -276,6 +276,14 @@ struct HeffPlan {
 std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& L, const DevBoundary& R, const MPOTensor& W,
                                           const Index& phys, const Index& left, const Index& right, bool bookkeeping);
 void upload_plan(HeffPlan& p);
+// Frees a plan's device buffers (work lists, coefficient blocks, scratch) and keeps its host work lists:
+// upload_plan stages it again, against boundaries of the same structure (rebind_plan).
+void release_plan_device(HeffPlan& p);
+void rebind_plan(HeffPlan& p, const DevBoundary& L, const DevBoundary& R);
+// 64-bit fingerprint of what a plan's work lists depend on besides the MPO tensor: the two boundaries'
+// sectors, cohorts, block offsets, conjugate scales and transposition flags, and the site indices.
+uint64_t plan_structure_key(const BoundaryIndexH& L, const BoundaryIndexH& R, const Index& phys, const Index& left,
+                            const Index& right);
 
 // y = H_eff x on device (x, y device pointers of length x_len), launched on p.stream.
 // ev (optional, 4 events) is recorded before the T-GEMM, after it, after the S

@@ -598,6 +598,27 @@ int heff_launches_per_apply(const HeffPlan& p) {
     return n;
 }
 
+void release_plan_device(HeffPlan& p) {
+    p.d_tjobs.reset();
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        p.d_ttiles[sh].reset(); p.d_utiles[sh].reset(); p.d_otiles[sh].reset(); p.d_kitems[sh].reset();
+    }
+    p.d_P.reset(); p.d_units.reset(); p.d_line_b1.reset(); p.d_slice_off.reset(); p.d_W.reset(); p.d_klist.reset();
+    p.d_segs.reset(); p.d_outs.reset(); p.d_T.reset(); p.d_S.reset(); p.d_W32.reset(); p.d_W32s.reset();
+    p.d_merr.reset(); p.d_x.reset(); p.d_y.reset();
+    p.adj.reset();
+    CoefGen& g = p.cg;
+    g.d_units.reset(); g.d_gin.reset(); g.d_line_major.reset(); g.d_smap_id.reset(); g.d_smap_slot.reset();
+    g.d_m_ptr.reset(); g.d_m_other.reset(); g.d_m_op.reset(); g.d_o_ptr.reset(); g.d_o_in.reset(); g.d_err.reset();
+    g.d_line_scale.reset(); g.d_m_scale.reset(); g.d_o_val.reset(); g.d_b_cs.reset(); g.d_b_pos.reset();
+}
+
+void rebind_plan(HeffPlan& p, const DevBoundary& L, const DevBoundary& R) {
+    p.L = &L;
+    p.R = &R;
+    p.cg.b_cs = &R.idx.cscale;  // the coefficient generation reads the right boundary's conjugate scales
+}
+
 // The merged plan's work lists (member plans validated each against their own buffers when staged;
 // here the merged T, S and k-step lists are checked again) and its own T, S and partial buffers.
 void upload_merged(HeffPlan& p) {

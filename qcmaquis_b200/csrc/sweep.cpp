@@ -533,6 +533,32 @@ double DevDMRG::expectation(const std::vector<MPOTensor>& W) {
     return v / n2;
 }
 
+std::unique_ptr<HeffPlan> DevDMRG::plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
+                                            const Index& phys, const Index& left, const Index& right, uint64_t& key) {
+    key = plan_structure_key(Lb.idx, Rb.idx, phys, left, right);
+    if (plan_cache_.size() != std::size_t(steps_per_sweep())) plan_cache_.resize(std::size_t(steps_per_sweep()));
+    CachedPlan& e = plan_cache_[std::size_t(step)];
+    if (e.plan && e.key == key) {
+        std::unique_ptr<HeffPlan> p = std::move(e.plan);
+        rebind_plan(*p, Lb, Rb);
+        ++st.plans_reused;
+        return p;
+    }
+    e.plan.reset();
+    ++st.plans_built;
+    return build_heff_plan(Lb, Rb, W, phys, left, right, false);
+}
+
+void DevDMRG::keep_plan(int step, std::unique_ptr<HeffPlan> plan, uint64_t key) {
+    release_plan_device(*plan);
+    plan->L = nullptr;
+    plan->R = nullptr;
+    plan->cg.b_cs = nullptr;
+    CachedPlan& e = plan_cache_[std::size_t(step)];
+    e.plan = std::move(plan);
+    e.key = key;
+}
+
 void DevDMRG::step_sites(int _site, int& lr, int& site1, int& site2) const {
     const int site = (_site < L - 1) ? _site : 2 * L - 2 - _site;
     if (_site < L - 1) { lr = 1; site1 = site; site2 = site + 1; }
@@ -587,7 +613,8 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     DTwoSite tst;
     tst.build(c, mps[site1], mps[site2]);
     mark(1);
-    auto plan = build_heff_plan(*left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, false);
+    uint64_t key = 0;
+    auto plan = plan_for(_site, *left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, key);
     mark(2);
     plan->stream = c.s;
     upload_plan(*plan);
@@ -600,7 +627,7 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         ortho_vector(c, tst.twin, tso.twin, ortho_left_[o][site1], ortho_right_[o][site2 + 1], v);
     });
     const double t2 = now_s();
-    plan.reset();
+    keep_plan(_site, std::move(plan), key);
     tst.twin_to_both(c);
     mark(3);
     energy = E + p.ecore;
@@ -656,7 +683,8 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
     make_right_paired(c, mps[site]);
     DMPS x = packed_right(c, mps[site]);
     // solve_site_problem with the single-site MPO tensor (ss_optimize.hpp:120)
-    auto plan = build_heff_plan(*left_[site], *right_[site + 1], mpo[site], x.phys, x.left, x.right, false);
+    uint64_t key = 0;
+    auto plan = plan_for(_site, *left_[site], *right_[site + 1], mpo[site], x.phys, x.left, x.right, key);
     plan->stream = c.s;
     if (plan->x_len != x.b.total) throw std::runtime_error("DMRG: site tensor layout differs from the plan");
     upload_plan(*plan);
@@ -665,7 +693,7 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
     const double E = solve(*plan, x, [&](std::size_t o, double* v) {
         ortho_vector(c, x, ortho_rp[o][site], ortho_left_[o][site], ortho_right_[o][site + 1], v);
     });
-    plan.reset();
+    keep_plan(_site, std::move(plan), key);
     mps[site] = std::move(x);
     energy = E + p.ecore;
     // alpha, cutoff and Mmax of this sweep (ss_optimize.hpp:143-155)

@@ -229,3 +229,26 @@ def test_open_shell_and_odd_sweeps_match_fci(gpu_ctx, nup, ndown):
     dev = DMRG(gpu_ctx, m, nup, ndown, 64)
     Es = [float(dev.sweep()[0].min()) for _ in range(4)]
     assert abs(Es[-1] - E_fci) < 1e-8, (Es, E_fci)
+
+
+def test_plan_cache_reuses_converged_steps(gpu_ctx):
+    """Once the bond sectors stop changing, every step re-stages its plan from the previous sweep (no host
+    schedule construction) and the energies still match the oracle step by step."""
+    from oracle.oracle import OracleDMRG
+    from qcmaquis_b200.dmrg import DMRG
+    from qcmaquis_b200.heff import parse_mps_tensor
+    L, M = 6, 16
+    h, V, e, m, ts, blob = qc_system(L)
+    ref = OracleDMRG(blob, L, L // 2, L // 2, M)
+    sites = [parse_mps_tensor(ref.mps_export(i)) for i in range(L)]
+    dev = DMRG.from_mps(gpu_ctx, m, sites, M)
+    reused = []
+    for s in range(4):
+        E_ref = ref.sweep(s)[0]
+        st0 = dev.stats()
+        E, _ = dev.sweep()
+        st1 = dev.stats()
+        assert np.abs(E - E_ref).max() < E_TOL, (s, E - E_ref)
+        reused.append(st1["plans_reused"] - st0["plans_reused"])
+        assert st1["plans_reused"] + st1["plans_built"] == (s + 1) * (2 * L - 2)
+    assert reused[0] == 0 and reused[-1] == 2 * L - 2, reused
