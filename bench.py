@@ -221,6 +221,17 @@ def dist_setup(a):
     return world, rank, local, pg
 
 
+def measured_traffic(a):
+    """DRAM bytes (read + written) of the S-GEMM phase per apply, from the ncu capture of this workload
+    summarised in profiles/ (dram__bytes_read.sum + dram__bytes_write.sum), or (None, None)."""
+    import re
+    path = os.path.join(ROOT, "profiles", f"heff_launches_traffic_L{a.L}_M{a.M}.md")
+    if a.seed != 0 or not os.path.exists(path):
+        return None, None
+    m = re.search(r"S-GEMM phase[^*]*\*\*([0-9.]+) GB\*\* per apply", open(path).read())
+    return (float(m.group(1)) * 1e9, os.path.relpath(path, ROOT)) if m else (None, None)
+
+
 def cpu_baseline(snap, blob, site, x, flops, budget_s=20.0):
     from oracle.oracle import heff_apply, lib as olib
     olib()
@@ -581,8 +592,10 @@ def run_b200(a, world, rank, local, pg):
     work = [info["flops_t"], info["flops_s"], info["flops_ls"]]
     dom = int(np.argmax(ph))
     ach = work[dom] / (ph[dom] * 1e-3) / 1e12
+    traffic, tsrc = measured_traffic(a)
     roof = {"kernel": names[dom], "bound": "tensor", "achieved": ach, "peak": dmma_peak, "unit": "TFLOP/s",
-            "frac": ach / dmma_peak, "traffic": None,
+            "frac": ach / dmma_peak, "traffic": traffic if dom == 1 else None, "traffic_source": tsrc,
+            "traffic_min_bytes": 8.0 * (info["w_len"] + info["t_len"] + info["s_len"]),
             "algorithmic": "reference flop count of the phase (ScheduleNew::total_flops terms)",
             "peak_source": "FP64 DMMA probe qcm_probe_fp64_peaks (of measured)"}
     if dom == 1:

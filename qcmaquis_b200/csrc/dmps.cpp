@@ -198,6 +198,7 @@ DBlocks normalize_left(Ctx& c, DMPS& t) {
     }
     Q.allocate(c.s, true);
     R.allocate(c.s, true);
+    if (!c.sv) c.sv = std::make_unique<Solver>();
     for (std::size_t k = 0; k < t.b.n(); ++k)
         qr_thin(*c.sv, c.s, t.b.d.get() + t.b.off[k], int(t.b.rows[k]), int(t.b.cols[k]), Q.d.get() + Q.off[k],
                 R.d.get() + R.off[k]);
@@ -217,6 +218,7 @@ DBlocks normalize_right(Ctx& c, DMPS& t) {
     }
     Lm.allocate(c.s, true);
     Q.allocate(c.s, true);
+    if (!c.sv) c.sv = std::make_unique<Solver>();
     for (std::size_t k = 0; k < t.b.n(); ++k)
         lq_thin(*c.sv, c.s, t.b.d.get() + t.b.off[k], int(t.b.rows[k]), int(t.b.cols[k]), Lm.d.get() + Lm.off[k],
                 Q.d.get() + Q.off[k]);

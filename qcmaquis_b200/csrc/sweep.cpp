@@ -419,7 +419,6 @@ DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTens
     : mpo(single), ts_mpo(twosite), p(prm) {
     c.s = s;
     QCM_CUDA(cudaGetDevice(&c.device));
-    c.sv = std::make_unique<Solver>();
     L = int(mpo.size());
     if (L < 2 || int(ts_mpo.size()) != L - 1) throw std::runtime_error("DMRG: need L >= 2 site tensors and L - 1 two-site tensors");
     const Index& phys = mpo[0].phys;
@@ -448,7 +447,6 @@ DevDMRG::DevDMRG(const std::vector<MPOTensor>& single, const std::vector<MPOTens
     : mpo(single), ts_mpo(twosite), mps(std::move(sites)), p(prm) {
     c.s = s;
     QCM_CUDA(cudaGetDevice(&c.device));
-    c.sv = std::make_unique<Solver>();
     L = int(mpo.size());
     if (L < 2 || int(ts_mpo.size()) != L - 1 || int(mps.size()) != L)
         throw std::runtime_error("DMRG: need L site tensors, L MPO tensors and L - 1 two-site tensors");
