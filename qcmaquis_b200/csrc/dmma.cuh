@@ -79,9 +79,7 @@ static __device__ __forceinline__ void mma_stage(const double (*A)[S::BM + PAD],
     }
 }
 
-// Same, skipping the 4-slice k groups whose bit in mask is clear (all-zero coefficients), and within
-// a group every warp's 8 x 4 A fragment that is all zero: the warp's lanes hold its 32 entries, one
-// vote decides, and the fragment's FN products (each exactly zero) are not issued
+// Same, skipping the 4-slice k groups whose bit in mask is clear (all-zero coefficients)
 template <class S>
 static __device__ __forceinline__ void mma_stage_masked(const double (*A)[S::BM + PAD], const double (*B)[S::BN + PAD],
                                                  Acc<S>& acc, int warp, int lane, uint32_t mask) {
@@ -96,11 +94,9 @@ static __device__ __forceinline__ void mma_stage_masked(const double (*A)[S::BM 
 #pragma unroll
         for (int j = 0; j < S::FN; ++j) b[j] = B[kk + q][wn * S::FN * 8 + j * 8 + r];
 #pragma unroll
-        for (int i = 0; i < S::FM; ++i) {
-            if (!__any_sync(0xffffffffu, a[i] != 0.0)) continue;
+        for (int i = 0; i < S::FM; ++i)
 #pragma unroll
             for (int j = 0; j < S::FN; ++j) dmma(acc.c[i][j], a[i], b[j]);
-        }
     }
 }
 

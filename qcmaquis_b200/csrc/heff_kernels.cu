@@ -37,7 +37,7 @@ using namespace dm;
 // ---------------------------------------------------------------------------
 // T-GEMM: one CTA per (job, tile)
 template <class S>
-__global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, const TileD* __restrict__ tiles,
+__global__ void __launch_bounds__(NTHR, 5) k_tgemm(const TJobD* __restrict__ jobs, const TileD* __restrict__ tiles,
                                                 const double* __restrict__ x, const double* __restrict__ R,
                                                 double* __restrict__ T, float* __restrict__ Thi, float* __restrict__ Tlo) {
     __shared__ Stage<S> st[2];
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(NTHR) k_tgemm(const TJobD* __restrict__ jobs, 
 // ---------------------------------------------------------------------------
 // S build: one CTA per (unit, line tile, element tile)
 template <class S>
-__global__ void __launch_bounds__(NTHR) k_sgemm(const UnitD* __restrict__ units, const TileD* __restrict__ tiles,
+__global__ void __launch_bounds__(NTHR, 5) k_sgemm(const UnitD* __restrict__ units, const TileD* __restrict__ tiles,
                                                 const uint32_t* __restrict__ line_b1, const uint64_t* __restrict__ slice_off,
                                                 const uint16_t* __restrict__ klist, const double* __restrict__ W,
                                                 const double* __restrict__ T, double* __restrict__ Sm) {
