@@ -506,6 +506,14 @@ void qcm_dmrg_free(qcm_dmrg* d);
 int qcm_truncate_svd(qcm_ctx* ctx, uint32_t n_blocks, const uint32_t* rows, const uint32_t* cols, const double* blocks,
                      uint64_t max_bond_dimension, double cutoff, uint32_t* keep, double* U, double* S, double* Vt,
                      qcm_trunc_result* result);
+/* Thin QR (lq = 0) or LQ (lq = 1) of every block, all blocks in one launch (one CTA each, Householder
+ * reflectors as geqrf / orgqr and gelqf / orglq define them): replaces qr / lq of
+ * framework/alps/matrix/algorithms.hpp:260-325, which MPSTensor::normalize_left / normalize_right
+ * (mp_tensors/mpstensor.hpp:242-300) call per block.  With k = min(rows, cols), outputs packed in block
+ * order: QR -- Q_k (rows x k) in Q, R_k (k x cols, upper triangular) in R; LQ -- Q_k (k x cols) in Q,
+ * L_k (rows x k, lower triangular) in R; all column-major. */
+int qcm_qr_blocks(qcm_ctx* ctx, uint32_t n_blocks, const uint32_t* rows, const uint32_t* cols, const double* blocks,
+                  int lq, double* Q, double* R);
 /* qcm_truncate_heev: symmetric blocks (density matrices, dims[k] x dims[k]); the cut is on
  * sqrt of the positive eigenvalues and the truncated fraction is reported in both
  * truncated_weight and truncated_fraction (as heev_truncate does).  Outputs per block:

@@ -105,3 +105,35 @@ int qcm_truncate_heev(qcm_ctx* ctx, uint32_t n_blocks, const uint32_t* dims, con
     return QCM_OK;
     QCM_CATCH
 }
+
+extern "C" int qcm_qr_blocks(qcm_ctx* ctx, uint32_t n_blocks, const uint32_t* rows, const uint32_t* cols,
+                             const double* blocks, int lq, double* Q, double* R) {
+    QCM_TRY
+    if (!ctx || !n_blocks || !rows || !cols || !blocks || !Q || !R) return qcm::fail(QCM_ERR_ARG, "qcm_qr_blocks: NULL argument");
+    QCM_CUDA(cudaSetDevice(ctx->device));
+    qcm::AllocStream scope(ctx->stream);
+    qcm::Ctx c;
+    c.s = ctx->stream;
+    c.device = ctx->device;
+    qcm::DBlocks M = upload_blocks(c, n_blocks, rows, cols, blocks);
+    // outputs packed like the inputs: per block Q (m x k or k x n) then R / L, k = min(m, n)
+    std::vector<uint64_t> qo(n_blocks), ro(n_blocks);
+    uint64_t ql = 0, rl = 0, wl = 0;
+    std::vector<qcm::QrJob> jobs;
+    for (uint32_t k = 0; k < n_blocks; ++k) {
+        const uint64_t m = rows[k], n = cols[k], kk = std::min(m, n);
+        qo[k] = ql; ro[k] = rl;
+        ql += kk * (lq ? n : m);
+        rl += kk * (lq ? m : n);
+        if (!m || !n) continue;
+        jobs.push_back(qcm::QrJob{M.off[k], qo[k], ro[k], wl, uint32_t(m), uint32_t(n), uint32_t(lq != 0), 0});
+        wl += (qcm::qr_scratch(uint32_t(m), uint32_t(n), lq != 0) + 31) / 32 * 32;
+    }
+    qcm::DBuf<double> dq(std::max<uint64_t>(ql, 1)), dr(std::max<uint64_t>(rl, 1)), dw(std::max<uint64_t>(wl, 1));
+    qcm::batched_qr(jobs, M.d.get(), M.total, dq.get(), ql, dr.get(), rl, dw.get(), wl ? wl : 1, c.qjobs, c.s);
+    download(c, dq.get(), Q, ql);
+    download(c, dr.get(), R, rl);
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    return QCM_OK;
+    QCM_CATCH
+}

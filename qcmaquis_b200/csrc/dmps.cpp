@@ -198,11 +198,16 @@ DBlocks normalize_left(Ctx& c, DMPS& t) {
     }
     Q.allocate(c.s, true);
     R.allocate(c.s, true);
-    if (!c.sv) c.sv = std::make_unique<Solver>();
-    for (std::size_t k = 0; k < t.b.n(); ++k)
-        qr_thin(*c.sv, c.s, t.b.d.get() + t.b.off[k], int(t.b.rows[k]), int(t.b.cols[k]), Q.d.get() + Q.off[k],
-                R.d.get() + R.off[k]);
-    c.sv->check(c.s);
+    // every block's thin QR in one launch (qr, alps/matrix/algorithms.hpp:260-291)
+    std::vector<QrJob> jobs;
+    uint64_t wl = 0;
+    for (std::size_t k = 0; k < t.b.n(); ++k) {
+        if (!t.b.rows[k] || !t.b.cols[k]) continue;
+        jobs.push_back(QrJob{t.b.off[k], Q.off[k], R.off[k], wl, t.b.rows[k], t.b.cols[k], 0, 0});
+        wl += (qr_scratch(t.b.rows[k], t.b.cols[k], false) + 31) / 32 * 32;
+    }
+    Ctx::ensure(c.qrw, std::max<uint64_t>(wl, 1));
+    batched_qr(jobs, t.b.d.get(), t.b.total, Q.d.get(), Q.total, R.d.get(), R.total, c.qrw.get(), c.qrw.size(), c.qjobs, c.s);
     t.b = std::move(Q);
     t.right = t.b.right_basis();
     return R;
@@ -218,11 +223,16 @@ DBlocks normalize_right(Ctx& c, DMPS& t) {
     }
     Lm.allocate(c.s, true);
     Q.allocate(c.s, true);
-    if (!c.sv) c.sv = std::make_unique<Solver>();
-    for (std::size_t k = 0; k < t.b.n(); ++k)
-        lq_thin(*c.sv, c.s, t.b.d.get() + t.b.off[k], int(t.b.rows[k]), int(t.b.cols[k]), Lm.d.get() + Lm.off[k],
-                Q.d.get() + Q.off[k]);
-    c.sv->check(c.s);
+    // every block's thin LQ in one launch (lq, alps/matrix/algorithms.hpp:293-325)
+    std::vector<QrJob> jobs;
+    uint64_t wl = 0;
+    for (std::size_t k = 0; k < t.b.n(); ++k) {
+        if (!t.b.rows[k] || !t.b.cols[k]) continue;
+        jobs.push_back(QrJob{t.b.off[k], Q.off[k], Lm.off[k], wl, t.b.rows[k], t.b.cols[k], 1, 0});
+        wl += (qr_scratch(t.b.rows[k], t.b.cols[k], true) + 31) / 32 * 32;
+    }
+    Ctx::ensure(c.qrw, std::max<uint64_t>(wl, 1));
+    batched_qr(jobs, t.b.d.get(), t.b.total, Q.d.get(), Q.total, Lm.d.get(), Lm.total, c.qrw.get(), c.qrw.size(), c.qjobs, c.s);
     t.b = std::move(Q);
     t.left = t.b.left_basis();
     return Lm;

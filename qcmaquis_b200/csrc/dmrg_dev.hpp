@@ -106,6 +106,8 @@ struct Ctx {
     DBuf<uint32_t> gtiles;
     DBuf<CopyJob> cjobs;
     DBuf<SvdJob> sjobs;
+    DBuf<QrJob> qjobs;
+    DBuf<double> qrw;  // QR / LQ scratch
     DBuf<TJobD> tjobs;
     DBuf<TileD> ttiles[N_SHAPES];
     DBuf<int> info;

@@ -70,6 +70,17 @@ uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n);
 void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
                         uint64_t s_len, double* V, uint64_t v_len, double* W, uint64_t w_len, int* zero_count,
                         DBuf<SvdJob>& jobbuf, cudaStream_t s, int* sweeps_used = nullptr);
+// Thin QR / LQ of many blocks in one launch (Householder, one CTA per block; qr_batched.cu):
+//   lq = 0: A_j (m x n, ld m) = Q_j R_j, Q_j (m x k, ld m), R_j (k x n, ld k);
+//   lq = 1: A_j = L_j Q_j, L_j (m x k, ld m) at r_off, Q_j (k x n, ld k) at q_off;
+// k = min(m, n); W: scratch of qr_scratch(m, n, lq) doubles per block at w_off.
+struct QrJob {
+    uint64_t a_off, q_off, r_off, w_off;
+    uint32_t m, n, lq, pad;
+};
+uint64_t qr_scratch(uint32_t m, uint32_t n, bool lq);
+void batched_qr(const std::vector<QrJob>& jobs, const double* A, uint64_t a_len, double* Q, uint64_t q_len, double* R,
+                uint64_t r_len, double* W, uint64_t w_len, DBuf<QrJob>& jobbuf, cudaStream_t s);
 // Symmetric eigendecomposition (divide and conquer, lower triangle) on lane `l`: A (n x n, ld n)
 // is overwritten by the eigenvectors, W receives the eigenvalues in ascending order.
 // Replaces heevd('V') of alps/matrix/algorithms.hpp:374-396 (which then reverses the order).

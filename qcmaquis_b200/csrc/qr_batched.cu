@@ -1,0 +1,161 @@
+// Thin QR and LQ of many blocks in one launch (the canonisation steps of the sweep).
+//
+// The reference canonises a site tensor block by block with LAPACK: qr / lq
+// (framework/alps/matrix/algorithms.hpp:260-325, geqrf + orgqr, gelqf + orglq), called by
+// MPSTensor::normalize_left / normalize_right (mp_tensors/mpstensor.hpp:242-300).  Here every
+// block of a site tensor is factorised by one CTA of the same launch, with the unblocked Householder
+// method LAPACK's geqr2 / org2r define (a published algorithm; Golub & Van Loan, Algorithm 5.2.1):
+//   for j < k = min(m, n): alpha = A(j, j), xnorm = |A(j+1:m, j)|;
+//     xnorm = 0: tau_j = 0 (H_j = I);
+//     else beta = -sign(alpha) hypot(alpha, xnorm), tau_j = (beta - alpha) / beta,
+//          v_j = (1, A(j+1:m, j) / (alpha - beta)), A(j, j) = beta;
+//     A(j:m, j+1:n) -= tau_j v_j (v_j^T A(j:m, j+1:n));
+//   R = the upper triangle (k x n); Q = H_0 ... H_{k-1} applied to the first k columns of I (m x k).
+// LQ is the QR of the transpose (the same reflectors as gelqf): L = R'^T, Q = Q'^T.
+// The work matrix and the reflectors live in global scratch (L2-resident at these sizes); a warp
+// updates one trailing column at a time (its dot product reduced within the warp).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+#include <vector>
+
+#include "linalg.hpp"
+
+namespace qcm {
+
+namespace {
+
+constexpr int QR_THR = 256;
+constexpr int QR_WARPS = QR_THR / 32;
+
+__device__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(QR_THR) k_qr(const QrJob* __restrict__ jobs, const double* __restrict__ A,
+                                               double* __restrict__ Q, double* __restrict__ R, double* __restrict__ W) {
+    __shared__ double red[QR_WARPS];
+    __shared__ double sh_tau, sh_scale;
+    const QrJob J = jobs[blockIdx.x];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // the matrix factorised: F (mm x nn) = A_j, or A_j^T for an LQ
+    const uint32_t mm = J.lq ? J.n : J.m, nn = J.lq ? J.m : J.n, k = mm < nn ? mm : nn;
+    double* w = W + J.w_off;              // F, then R above and the reflectors below the diagonal
+    double* taus = w + uint64_t(mm) * nn;  // k reflector scales
+    double* qf = taus + k;                 // Q' (mm x k) for an LQ; the QR writes Q directly
+    const double* a = A + J.a_off;
+    for (uint64_t e = tid; e < uint64_t(mm) * nn; e += QR_THR) {
+        const uint32_t i = uint32_t(e % mm), c = uint32_t(e / mm);
+        w[e] = J.lq ? a[c + uint64_t(i) * J.m] : a[i + uint64_t(c) * J.m];
+    }
+    __syncthreads();
+    for (uint32_t j = 0; j < k; ++j) {
+        double* vj = w + uint64_t(j) * mm;
+        double s = 0.0;
+        for (uint32_t i = j + 1 + tid; i < mm; i += QR_THR) s = fma(vj[i], vj[i], s);
+        s = warp_sum(s);
+        if (lane == 0) red[warp] = s;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int q = 0; q < QR_WARPS; ++q) t += red[q];
+            const double alpha = vj[j], xnorm = sqrt(t);
+            double tau = 0.0, scale = 1.0;
+            if (xnorm != 0.0) {
+                const double beta = -copysign(hypot(alpha, xnorm), alpha);
+                tau = (beta - alpha) / beta;
+                scale = 1.0 / (alpha - beta);
+                vj[j] = beta;
+            }
+            sh_tau = tau;
+            sh_scale = scale;
+            taus[j] = tau;
+        }
+        __syncthreads();
+        const double tau = sh_tau;
+        if (tau != 0.0) {
+            const double scale = sh_scale;
+            for (uint32_t i = j + 1 + tid; i < mm; i += QR_THR) vj[i] *= scale;
+            __syncthreads();
+            // trailing columns, one warp each: F(j:mm, c) -= tau v (v^T F(j:mm, c)), v_j = 1
+            for (uint32_t c = j + 1 + warp; c < nn; c += QR_WARPS) {
+                double* fc = w + uint64_t(c) * mm;
+                const double fj = fc[j];  // read by every lane before lane 0 writes it
+                double d = 0.0;
+                for (uint32_t i = j + 1 + lane; i < mm; i += 32) d = fma(vj[i], fc[i], d);
+                d = warp_sum(d) + fj;
+                d *= tau;
+                if (lane == 0) fc[j] -= d;
+                for (uint32_t i = j + 1 + lane; i < mm; i += 32) fc[i] = fma(-d, vj[i], fc[i]);
+            }
+        }
+        __syncthreads();
+    }
+    // R (k x nn, ld k) from the upper triangle; for an LQ, L = R'^T (m x k, ld m)
+    double* r = R + J.r_off;
+    for (uint64_t e = tid; e < uint64_t(k) * nn; e += QR_THR) {
+        const uint32_t i = uint32_t(e % k), c = uint32_t(e / k);
+        const double v = i <= c ? w[i + uint64_t(c) * mm] : 0.0;
+        if (J.lq) r[c + uint64_t(i) * J.m] = v;
+        else r[e] = v;
+    }
+    // Q' = H_0 ... H_{k-1} I(:, 0:k), the reflectors applied from the last to the first
+    double* qo = J.lq ? qf : Q + J.q_off;
+    for (uint64_t e = tid; e < uint64_t(mm) * k; e += QR_THR) {
+        const uint32_t i = uint32_t(e % mm), c = uint32_t(e / mm);
+        qo[e] = i == c ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    for (int jj = int(k) - 1; jj >= 0; --jj) {
+        const uint32_t j = uint32_t(jj);
+        const double tau = taus[j];
+        if (tau != 0.0) {
+            const double* vj = w + uint64_t(j) * mm;
+            for (uint32_t c = j + warp; c < k; c += QR_WARPS) {
+                double* qc = qo + uint64_t(c) * mm;
+                const double qj = qc[j];
+                double d = 0.0;
+                for (uint32_t i = j + 1 + lane; i < mm; i += 32) d = fma(vj[i], qc[i], d);
+                d = warp_sum(d) + qj;
+                d *= tau;
+                if (lane == 0) qc[j] -= d;
+                for (uint32_t i = j + 1 + lane; i < mm; i += 32) qc[i] = fma(-d, vj[i], qc[i]);
+            }
+        }
+        __syncthreads();
+    }
+    if (J.lq) {
+        // Q = Q'^T (k x n, ld k)
+        double* q = Q + J.q_off;
+        for (uint64_t e = tid; e < uint64_t(mm) * k; e += QR_THR) {
+            const uint32_t i = uint32_t(e % mm), c = uint32_t(e / mm);
+            q[c + uint64_t(i) * k] = qf[e];
+        }
+    }
+}
+
+}  // namespace
+
+uint64_t qr_scratch(uint32_t m, uint32_t n, bool lq) {
+    const uint64_t k = std::min(m, n);
+    return uint64_t(m) * n + k + (lq ? uint64_t(m) * n : 0) + 1;
+}
+
+void batched_qr(const std::vector<QrJob>& jobs, const double* A, uint64_t a_len, double* Q, uint64_t q_len, double* R,
+                uint64_t r_len, double* W, uint64_t w_len, DBuf<QrJob>& jobbuf, cudaStream_t s) {
+    if (jobs.empty()) return;
+    for (const QrJob& j : jobs) {
+        const uint64_t k = std::min(j.m, j.n);
+        if (!j.m || !j.n || j.a_off + uint64_t(j.m) * j.n > a_len || j.w_off + qr_scratch(j.m, j.n, j.lq != 0) > w_len ||
+            j.q_off + k * (j.lq ? j.n : j.m) > q_len || j.r_off + k * (j.lq ? j.m : j.n) > r_len)
+            throw std::runtime_error("batched QR: a block outside its buffers");
+    }
+    jobbuf.upload(jobs, s);
+    k_qr<<<unsigned(jobs.size()), QR_THR, 0, s>>>(jobbuf.get(), A, Q, R, W);
+    QCM_CUDA(cudaGetLastError());
+}
+
+}  // namespace qcm

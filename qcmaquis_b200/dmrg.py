@@ -120,6 +120,35 @@ def truncate_svd(ctx, blocks, max_bond_dimension: int, cutoff: float = 1e-16):
     return out, {f: getattr(r, f) for f, _ in TruncResult._fields_}
 
 
+_lib._sig("qcm_qr_blocks", c_int, c_void_p, ctypes.c_uint32, _U32, _U32, P(c_double), c_int, P(c_double), P(c_double))
+
+
+def qr_blocks(ctx, blocks, lq: bool = False):
+    """Thin QR (or LQ) of every block on the device, one launch: [(Q, R) per block] (LQ: [(L, Q)])."""
+    bl = [np.asarray(b, dtype=np.float64) for b in blocks]
+    rows = np.array([b.shape[0] for b in bl], dtype=np.uint32)
+    cols = np.array([b.shape[1] for b in bl], dtype=np.uint32)
+    k = np.minimum(rows, cols).astype(np.int64)
+    data = np.ascontiguousarray(np.concatenate([b.ravel(order="F") for b in bl]))
+    nq = int((k * (cols if lq else rows)).sum())
+    nr = int((k * (rows if lq else cols)).sum())
+    Q, R = np.zeros(max(1, nq)), np.zeros(max(1, nr))
+    check(lib.qcm_qr_blocks(ctx.h, len(bl), _u32(rows), _u32(cols), _lib.dptr(data), 1 if lq else 0, _lib.dptr(Q),
+                            _lib.dptr(R)), "qcm_qr_blocks")
+    out, pq, pr = [], 0, 0
+    for m, n, kk in zip(rows.tolist(), cols.tolist(), k.tolist()):
+        if lq:
+            Qb = Q[pq:pq + kk * n].reshape(n, kk).T.copy()
+            Lb = R[pr:pr + m * kk].reshape(kk, m).T.copy()
+            out.append((Lb, Qb))
+        else:
+            Qb = Q[pq:pq + m * kk].reshape(kk, m).T.copy()
+            Rb = R[pr:pr + kk * n].reshape(n, kk).T.copy()
+            out.append((Qb, Rb))
+        pq += kk * (n if lq else m); pr += kk * (m if lq else n)
+    return out
+
+
 def truncate_heev(ctx, blocks, max_bond_dimension: int, cutoff: float = 1e-16):
     """heev_truncate of symmetric blocks on the device: ([(U, evals) per block, kept eigenpairs in
     descending order], truncation result dict; truncated_weight = truncated_fraction)."""

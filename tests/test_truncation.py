@@ -157,3 +157,37 @@ def test_device_heev_truncate_matches_oracle(gpu_ctx):
         if ev.size:
             assert np.abs(b @ U - U * ev).max() < 1e-9 * abs(ev[0])
             assert np.abs(np.abs(np.diag(U.T @ Ur)) - 1).max() < 1e-8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("lq", [False, True])
+def test_qr_blocks_householder(gpu_ctx, lq):
+    """Batched thin QR / LQ (one launch for all blocks): tall, wide, square, 1 x n, n x 1, rank-deficient and
+    zero blocks; A = QR (LQ), orthonormal Q, triangular R (L), and R's diagonal equal to LAPACK's (numpy's
+    Householder QR: the same reflector convention beta = -sign(alpha) |x|) up to rounding."""
+    from qcmaquis_b200.dmrg import qr_blocks
+    rng = np.random.default_rng(3)
+    shapes = [(40, 12), (12, 40), (33, 33), (1, 7), (7, 1), (300, 90), (64, 200)]
+    blocks = [rng.standard_normal(s) for s in shapes]
+    blocks.append(np.outer(rng.standard_normal(20), rng.standard_normal(9)))  # rank 1
+    blocks.append(np.ones((6, 4)))                                             # the const state's blocks
+    out = qr_blocks(gpu_ctx, blocks, lq=lq)
+    for A, (X, Y) in zip(blocks, out):
+        m, n = A.shape
+        k = min(m, n)
+        if lq:
+            L, Q = X, Y
+            assert L.shape == (m, k) and Q.shape == (k, n)
+            assert np.abs(L @ Q - A).max() <= 1e-13 * max(1.0, np.abs(A).max())
+            assert np.abs(Q @ Q.T - np.eye(k)).max() < 1e-13
+            assert np.abs(np.triu(L[:k, :k], 1)).max() == 0.0
+            ref = np.linalg.qr(A.T, mode="r")
+            assert np.allclose(np.diag(L[:k, :k]), np.diag(ref[:k, :k]), rtol=1e-10, atol=1e-12)
+        else:
+            Q, R = X, Y
+            assert Q.shape == (m, k) and R.shape == (k, n)
+            assert np.abs(Q @ R - A).max() <= 1e-13 * max(1.0, np.abs(A).max())
+            assert np.abs(Q.T @ Q - np.eye(k)).max() < 1e-13
+            assert np.abs(np.tril(R[:, :k], -1)).max() == 0.0
+            ref = np.linalg.qr(A, mode="r")
+            assert np.allclose(np.diag(R[:, :k]), np.diag(ref[:k, :k]), rtol=1e-10, atol=1e-12)
