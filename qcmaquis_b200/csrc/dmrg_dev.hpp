@@ -338,13 +338,18 @@ struct DevDMRG {
     // a step whose boundaries and site indices have the same structure (the same sectors, cohorts,
     // block offsets and conjugate scales) as its cached plan's re-stages that plan (work lists
     // uploaded, coefficient blocks regenerated on the device) instead of rebuilding the schedule.
+    // Plans whose work lists and coefficient blocks fit in the device budget keep them on the device (a
+    // reuse then only re-binds the boundaries); the others keep their host lists only.
     struct CachedPlan {
         std::unique_ptr<HeffPlan> plan;
         uint64_t key = 0;
+        uint64_t resident = 0;  // device bytes kept with the plan
     };
     std::vector<CachedPlan> plan_cache_;
+    uint64_t plan_cache_budget_ = 0, plan_cache_bytes_ = 0;
     std::unique_ptr<HeffPlan> plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
-                                       const Index& phys, const Index& left, const Index& right, uint64_t& key);
+                                       const Index& phys, const Index& left, const Index& right, uint64_t& key,
+                                       bool& resident);
     void keep_plan(int step, std::unique_ptr<HeffPlan> plan, uint64_t key);
     void init_boundaries(int site = 0);
     void step(int step, double& energy, TruncResults& tr);

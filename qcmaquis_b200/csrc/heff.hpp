@@ -279,6 +279,12 @@ void upload_plan(HeffPlan& p);
 // Frees a plan's device buffers (work lists, coefficient blocks, scratch) and keeps its host work lists:
 // upload_plan stages it again, against boundaries of the same structure (rebind_plan).
 void release_plan_device(HeffPlan& p);
+// Frees only the scratch (T, S, partials, staging, mixed-form copies, coefficient-generation tables):
+// the work lists and coefficient blocks stay on the device (plan_resident_bytes of them), and
+// restage_plan makes the plan applicable again, against boundaries of the same structure.
+void release_plan_scratch(HeffPlan& p);
+uint64_t plan_resident_bytes(const HeffPlan& p);
+void restage_plan(HeffPlan& p);
 void rebind_plan(HeffPlan& p, const DevBoundary& L, const DevBoundary& R);
 // 64-bit fingerprint of what a plan's work lists depend on besides the MPO tensor: the two boundaries'
 // sectors, cohorts, block offsets, conjugate scales and transposition flags, and the site indices.

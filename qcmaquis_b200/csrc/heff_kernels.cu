@@ -613,6 +613,33 @@ void release_plan_device(HeffPlan& p) {
     g.d_line_scale.reset(); g.d_m_scale.reset(); g.d_o_val.reset(); g.d_b_cs.reset(); g.d_b_pos.reset();
 }
 
+void release_plan_scratch(HeffPlan& p) {
+    p.d_T.reset(); p.d_S.reset(); p.d_P.reset(); p.d_x.reset(); p.d_y.reset();
+    p.d_W32.reset(); p.d_W32s.reset(); p.d_merr.reset();
+    p.adj.reset();
+    CoefGen& g = p.cg;
+    g.d_units.reset(); g.d_gin.reset(); g.d_line_major.reset(); g.d_smap_id.reset(); g.d_smap_slot.reset();
+    g.d_m_ptr.reset(); g.d_m_other.reset(); g.d_m_op.reset(); g.d_o_ptr.reset(); g.d_o_in.reset(); g.d_err.reset();
+    g.d_line_scale.reset(); g.d_m_scale.reset(); g.d_o_val.reset(); g.d_b_cs.reset(); g.d_b_pos.reset();
+}
+
+uint64_t plan_resident_bytes(const HeffPlan& p) {
+    uint64_t b = p.d_W.size() * sizeof(double) + p.d_tjobs.size() * sizeof(TJobD) + p.d_units.size() * sizeof(UnitD) +
+                 p.d_line_b1.size() * 4 + p.d_slice_off.size() * 8 + p.d_klist.size() * 2 + p.d_segs.size() * sizeof(SegD) +
+                 p.d_outs.size() * sizeof(OutD);
+    for (int sh = 0; sh < N_SHAPES; ++sh)
+        b += (p.d_ttiles[sh].size() + p.d_utiles[sh].size()) * sizeof(TileD) + p.d_otiles[sh].size() * sizeof(OTileD) +
+             p.d_kitems[sh].size() * sizeof(KItemD);
+    return b;
+}
+
+void restage_plan(HeffPlan& p) {
+    AllocStream scope(p.stream);
+    p.d_T.alloc(p.t_len);
+    p.d_S.alloc(p.s_len);
+    p.d_P.alloc(p.p_len);
+}
+
 void rebind_plan(HeffPlan& p, const DevBoundary& L, const DevBoundary& R) {
     p.L = &L;
     p.R = &R;

@@ -49,15 +49,9 @@ namespace {
 constexpr uint32_t NONE = 0xffffffffu;
 // K rows per split-K item of the L.S GEMM (measured at L=24 M=512: 512 -> 1.06 ms, 1024 -> 0.77 ms,
 // 2048 -> 0.84 ms, 4096 -> 1.28 ms: more partial tiles to reduce below, fewer concurrent items above)
-constexpr uint32_t KCHUNK_DEFAULT = 1024;
-uint32_t ls_kchunk() {
-    static const uint32_t v = [] {
-        const char* e = std::getenv("QCM_LS_KCHUNK");
-        const long x = e ? std::atol(e) : 0;
-        return (x >= 64 && x % 16 == 0) ? uint32_t(x) : KCHUNK_DEFAULT;
-    }();
-    return v;
-}
+// split-K chunk of the L.S GEMM (rows of K per work item): 512 gives about twice the CTAs of 1024 at the
+// L=24, M=512 middle bond and took the L.S phase from 0.47 to 0.41 ms; 256 was no faster
+constexpr uint32_t KCHUNK = 512;
 
 void add_tiles(std::vector<TileD>* tiles, uint32_t item, uint32_t M, uint32_t N) {
     int sh = shape_for_rows(M);
@@ -789,8 +783,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     t.part0 = uint32_t(p->kitems[sh].size());
                     for (uint32_t sg = o.seg_start; sg < o.seg_start + o.seg_count; ++sg) {
                         uint32_t Kc = p->segs[sg].nS * p->segs[sg].ls_in;
-                        for (uint32_t k0 = 0; k0 < Kc; k0 += ls_kchunk())
-                            p->kitems[sh].push_back(KItemD{uint32_t(p->otiles[sh].size()), sg, k0, std::min(Kc, k0 + ls_kchunk())});
+                        for (uint32_t k0 = 0; k0 < Kc; k0 += KCHUNK)
+                            p->kitems[sh].push_back(KItemD{uint32_t(p->otiles[sh].size()), sg, k0, std::min(Kc, k0 + KCHUNK)});
                     }
                     t.nparts = uint32_t(p->kitems[sh].size()) - t.part0;
                     p->otiles[sh].push_back(t);

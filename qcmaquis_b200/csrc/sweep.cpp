@@ -532,27 +532,48 @@ double DevDMRG::expectation(const std::vector<MPOTensor>& W) {
 }
 
 std::unique_ptr<HeffPlan> DevDMRG::plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
-                                            const Index& phys, const Index& left, const Index& right, uint64_t& key) {
+                                            const Index& phys, const Index& left, const Index& right, uint64_t& key,
+                                            bool& resident) {
     key = plan_structure_key(Lb.idx, Rb.idx, phys, left, right);
     if (plan_cache_.size() != std::size_t(steps_per_sweep())) plan_cache_.resize(std::size_t(steps_per_sweep()));
     CachedPlan& e = plan_cache_[std::size_t(step)];
+    resident = false;
     if (e.plan && e.key == key) {
         std::unique_ptr<HeffPlan> p = std::move(e.plan);
         rebind_plan(*p, Lb, Rb);
+        resident = e.resident > 0;
+        plan_cache_bytes_ -= e.resident;
+        e.resident = 0;
         ++st.plans_reused;
         return p;
     }
     e.plan.reset();
+    plan_cache_bytes_ -= e.resident;
+    e.resident = 0;
     ++st.plans_built;
     return build_heff_plan(Lb, Rb, W, phys, left, right, false);
 }
 
 void DevDMRG::keep_plan(int step, std::unique_ptr<HeffPlan> plan, uint64_t key) {
-    release_plan_device(*plan);
+    if (!plan_cache_budget_) {
+        // a quarter of the device's memory for the work lists and coefficient blocks kept between sweeps
+        size_t free_b = 0, total_b = 0;
+        QCM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        plan_cache_budget_ = uint64_t(total_b) / 4;
+    }
+    CachedPlan& e = plan_cache_[std::size_t(step)];
+    const uint64_t rb = plan_resident_bytes(*plan);
+    if (plan_cache_bytes_ + rb <= plan_cache_budget_) {
+        release_plan_scratch(*plan);
+        e.resident = rb;
+        plan_cache_bytes_ += rb;
+    } else {
+        release_plan_device(*plan);
+        e.resident = 0;
+    }
     plan->L = nullptr;
     plan->R = nullptr;
     plan->cg.b_cs = nullptr;
-    CachedPlan& e = plan_cache_[std::size_t(step)];
     e.plan = std::move(plan);
     e.key = key;
 }
@@ -612,10 +633,13 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
     tst.build(c, mps[site1], mps[site2]);
     mark(1);
     uint64_t key = 0;
-    auto plan = plan_for(_site, *left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, key);
+    bool resident = false;
+    auto plan = plan_for(_site, *left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, key,
+                         resident);
     mark(2);
     plan->stream = c.s;
-    upload_plan(*plan);
+    if (resident) restage_plan(*plan);
+    else upload_plan(*plan);
     QCM_CUDA(cudaStreamSynchronize(c.s));
     const double t1 = now_s();
     st.plan_s += t1 - t0;
@@ -682,10 +706,12 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
     DMPS x = packed_right(c, mps[site]);
     // solve_site_problem with the single-site MPO tensor (ss_optimize.hpp:120)
     uint64_t key = 0;
-    auto plan = plan_for(_site, *left_[site], *right_[site + 1], mpo[site], x.phys, x.left, x.right, key);
+    bool resident = false;
+    auto plan = plan_for(_site, *left_[site], *right_[site + 1], mpo[site], x.phys, x.left, x.right, key, resident);
     plan->stream = c.s;
     if (plan->x_len != x.b.total) throw std::runtime_error("DMRG: site tensor layout differs from the plan");
-    upload_plan(*plan);
+    if (resident) restage_plan(*plan);
+    else upload_plan(*plan);
     QCM_CUDA(cudaStreamSynchronize(c.s));
     st.plan_s += now_s() - t0;
     const double E = solve(*plan, x, [&](std::size_t o, double* v) {
