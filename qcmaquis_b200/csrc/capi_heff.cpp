@@ -161,13 +161,18 @@ int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info) {
     info->t_len = p.t_len;
     info->s_len = p.s_len;
     info->n_tjobs = p.tjobs.size();
-    info->n_ttiles = p.ttiles[0].size() + p.ttiles[1].size() + p.ttiles[2].size();
+    info->n_ttiles = 0;
+    info->n_otiles = 0;
+    info->n_kitems = 0;
+    for (int sh = 0; sh < qcm::N_SHAPES; ++sh) {
+        info->n_ttiles += p.ttiles[sh].size();
+        info->n_otiles += p.otiles[sh].size();
+        info->n_kitems += p.kitems[sh].size();
+    }
     info->n_gtasks = p.units.size();
     info->n_alpha = p.n_alpha;
     info->n_segs = p.segs.size();
     info->n_outs = p.outs.size();
-    info->n_otiles = p.otiles[0].size() + p.otiles[1].size() + p.otiles[2].size();
-    info->n_kitems = p.kitems[0].size() + p.kitems[1].size() + p.kitems[2].size();
     info->launches = uint64_t(qcm::heff_launches_per_apply(p));
     info->w_len = p.w_len;
     info->flops_sexec = p.flops_sexec;

@@ -652,7 +652,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     }
                 P.line_b1.insert(P.line_b1.end(), u.lines.begin(), u.lines.end());
                 // S-GEMM tiles of the unit and the tensor work they execute
-                const std::size_t tb[4] = {P.utiles[0].size(), P.utiles[1].size(), P.utiles[2].size(), P.utiles[3].size()};
+                std::size_t tb[N_SHAPES];
+                for (int sh = 0; sh < N_SHAPES; ++sh) tb[sh] = P.utiles[sh].size();
                 emit_tiles(ud, uint32_t(P.units.size()), tch, P.utiles, P.klist);
                 for (int sh = 0; sh < N_SHAPES; ++sh)
                     for (std::size_t t = tb[sh]; t < P.utiles[sh].size(); ++t) {
