@@ -271,8 +271,6 @@ typedef void (*dgemm_t)(const char*, const char*, const int*, const int*, const 
                         const int*, const double*, const int*, const double*, double*, const int*);
 typedef void (*dgesvd_t)(const char*, const char*, const int*, const int*, double*, const int*, double*, double*,
                          const int*, double*, const int*, double*, const int*, int*);
-typedef void (*dgeqrf_t)(const int*, const int*, double*, const int*, double*, double*, const int*, int*);
-typedef void (*dorgqr_t)(const int*, const int*, const int*, double*, const int*, const double*, double*, const int*, int*);
 typedef void (*dsyevx_t)(const char*, const char*, const char*, const int*, double*, const int*, const double*,
                          const double*, const int*, const int*, const double*, int*, double*, double*, const int*,
                          double*, const int*, int*, int*, int*);
@@ -281,8 +279,6 @@ typedef void (*dsyevd_t)(const char*, const char*, const int*, double*, const in
 typedef void (*setthreads_t)(int);
 dgemm_t p_dgemm = nullptr;
 dgesvd_t p_dgesvd = nullptr;
-dgeqrf_t p_dgeqrf = nullptr, p_dgelqf = nullptr;
-dorgqr_t p_dorgqr = nullptr, p_dorglq = nullptr;
 dsyevx_t p_dsyevx = nullptr;
 dsyevd_t p_dsyevd = nullptr;
 }  // namespace
@@ -295,14 +291,10 @@ bool blas_init(const char* path, std::string& err) {
     if (!h) { err = dlerror(); return false; }
     p_dgemm = (dgemm_t)dlsym(h, "scipy_dgemm_");
     p_dgesvd = (dgesvd_t)dlsym(h, "scipy_dgesvd_");
-    p_dgeqrf = (dgeqrf_t)dlsym(h, "scipy_dgeqrf_");
-    p_dgelqf = (dgeqrf_t)dlsym(h, "scipy_dgelqf_");
-    p_dorgqr = (dorgqr_t)dlsym(h, "scipy_dorgqr_");
-    p_dorglq = (dorgqr_t)dlsym(h, "scipy_dorglq_");
     p_dsyevx = (dsyevx_t)dlsym(h, "scipy_dsyevx_");
     p_dsyevd = (dsyevd_t)dlsym(h, "scipy_dsyevd_");
     auto st = (setthreads_t)dlsym(h, "scipy_openblas_set_num_threads");
-    if (!p_dgemm || !p_dgesvd || !p_dgeqrf || !p_dgelqf || !p_dorgqr || !p_dorglq || !p_dsyevx || !p_dsyevd) {
+    if (!p_dgemm || !p_dgesvd || !p_dsyevx || !p_dsyevd) {
         err = "missing LAPACK symbol";
         p_dgemm = nullptr;
         return false;
@@ -342,53 +334,88 @@ void dgesvd_thin(const Mat& A0, Mat& U, std::vector<double>& S, Mat& VT) {
     if (info != 0) throw std::runtime_error("oracle dgesvd failed");
 }
 
-// alps/matrix/algorithms.hpp:259-289 (geqrf + orgqr)
+// qr / lq (alps/matrix/algorithms.hpp:259-325: geqrf + orgqr, gelqf + orglq) restated as the
+// unblocked Householder method of geqr2 / org2r, with one rule added on both the oracle's and the
+// device's side: a column whose remaining part is below 64 eps |A|_F (rounding noise, e.g. every
+// column after the first of a rank-1 block) is set to exactly zero and gets no reflector.  The
+// orthonormal completion of Q is then H_0 ... H_{k-1} applied to unit vectors, fixed by the
+// arithmetic instead of by rounding noise (LAPACK's completion of a rank-deficient block differs
+// between implementations, so the reference itself is not reproducible there).
+namespace {
+// Householder QR of F (m x n, column-major, in place): R above, reflectors below the diagonal, tau
+void householder(Mat& F, std::vector<double>& tau) {
+    const std::size_t m = F.r, n = F.c, k = std::min(m, n);
+    double fro = 0.0;
+    for (double x : F.d) fro += x * x;
+    const double thr = 64.0 * 2.220446049250313e-16 * std::sqrt(fro);
+    tau.assign(k, 0.0);
+    for (std::size_t j = 0; j < k; ++j) {
+        double s = 0.0;
+        for (std::size_t i = j + 1; i < m; ++i) s += F(i, j) * F(i, j);
+        const double alpha = F(j, j), xnorm = std::sqrt(s);
+        if (std::hypot(alpha, xnorm) <= thr) {
+            for (std::size_t i = j; i < m; ++i) F(i, j) = 0.0;
+            continue;
+        }
+        if (xnorm == 0.0) continue;
+        const double beta = -std::copysign(std::hypot(alpha, xnorm), alpha);
+        const double t = (beta - alpha) / beta, sc = 1.0 / (alpha - beta);
+        for (std::size_t i = j + 1; i < m; ++i) F(i, j) *= sc;
+        F(j, j) = beta;
+        tau[j] = t;
+        for (std::size_t c = j + 1; c < n; ++c) {
+            double d = F(j, c);
+            for (std::size_t i = j + 1; i < m; ++i) d += F(i, j) * F(i, c);
+            d *= t;
+            F(j, c) -= d;
+            for (std::size_t i = j + 1; i < m; ++i) F(i, c) -= d * F(i, j);
+        }
+    }
+}
+// Q (m x k) = H_0 ... H_{k-1} I(:, 0:k)
+Mat householder_q(const Mat& F, const std::vector<double>& tau) {
+    const std::size_t m = F.r, k = tau.size();
+    Mat Q(m, k);
+    for (std::size_t c = 0; c < k; ++c) Q(c, c) = 1.0;
+    for (std::size_t jj = k; jj-- > 0;) {
+        if (tau[jj] == 0.0) continue;
+        for (std::size_t c = jj; c < k; ++c) {
+            double d = Q(jj, c);
+            for (std::size_t i = jj + 1; i < m; ++i) d += F(i, jj) * Q(i, c);
+            d *= tau[jj];
+            Q(jj, c) -= d;
+            for (std::size_t i = jj + 1; i < m; ++i) Q(i, c) -= d * F(i, jj);
+        }
+    }
+    return Q;
+}
+}  // namespace
+
 void qr(const Mat& A0, Mat& Qm, Mat& R) {
-    int m = int(A0.r), n = int(A0.c), k = std::min(m, n);
-    Mat A = A0;
-    std::vector<double> tau(std::max(k, 1));
-    int lwork = -1, info = 0;
-    double wq;
-    p_dgeqrf(&m, &n, A.d.data(), &m, tau.data(), &wq, &lwork, &info);
-    lwork = std::max(1, int(wq));
-    std::vector<double> work(lwork);
-    p_dgeqrf(&m, &n, A.d.data(), &m, tau.data(), work.data(), &lwork, &info);
+    const std::size_t m = A0.r, n = A0.c, k = std::min(m, n);
+    Mat F = A0;
+    std::vector<double> tau;
+    householder(F, tau);
     R = Mat(k, n);
-    for (int j = 0; j < n; ++j)
-        for (int i = 0; i <= std::min(j, k - 1); ++i) R(i, j) = A(i, j);
-    Qm = Mat(m, k);
-    for (int j = 0; j < k; ++j)
-        for (int i = 0; i < m; ++i) Qm(i, j) = A(i, j);
-    lwork = -1;
-    p_dorgqr(&m, &k, &k, Qm.d.data(), &m, tau.data(), &wq, &lwork, &info);
-    lwork = std::max(1, int(wq));
-    work.resize(lwork);
-    p_dorgqr(&m, &k, &k, Qm.d.data(), &m, tau.data(), work.data(), &lwork, &info);
-    if (info != 0) throw std::runtime_error("oracle QR failed");
+    for (std::size_t j = 0; j < n; ++j)
+        for (std::size_t i = 0; i <= std::min(j, k - 1); ++i) R(i, j) = F(i, j);
+    Qm = householder_q(F, tau);
 }
 
 void lq(const Mat& A0, Mat& Lm, Mat& Qm) {
-    int m = int(A0.r), n = int(A0.c), k = std::min(m, n);
-    Mat A = A0;
-    std::vector<double> tau(std::max(k, 1));
-    int lwork = -1, info = 0;
-    double wq;
-    p_dgelqf(&m, &n, A.d.data(), &m, tau.data(), &wq, &lwork, &info);
-    lwork = std::max(1, int(wq));
-    std::vector<double> work(lwork);
-    p_dgelqf(&m, &n, A.d.data(), &m, tau.data(), work.data(), &lwork, &info);
+    const std::size_t m = A0.r, n = A0.c, k = std::min(m, n);
+    Mat F(n, m);
+    for (std::size_t j = 0; j < n; ++j)
+        for (std::size_t i = 0; i < m; ++i) F(j, i) = A0(i, j);
+    std::vector<double> tau;
+    householder(F, tau);
     Lm = Mat(m, k);
-    for (int j = 0; j < k; ++j)
-        for (int i = j; i < m; ++i) Lm(i, j) = A(i, j);
+    for (std::size_t j = 0; j < k; ++j)
+        for (std::size_t i = j; i < m; ++i) Lm(i, j) = F(j, i);
+    const Mat Qt = householder_q(F, tau);  // n x k
     Qm = Mat(k, n);
-    for (int j = 0; j < n; ++j)
-        for (int i = 0; i < k; ++i) Qm(i, j) = A(i, j);
-    lwork = -1;
-    p_dorglq(&k, &n, &k, Qm.d.data(), &k, tau.data(), &wq, &lwork, &info);
-    lwork = std::max(1, int(wq));
-    work.resize(lwork);
-    p_dorglq(&k, &n, &k, Qm.d.data(), &k, tau.data(), work.data(), &lwork, &info);
-    if (info != 0) throw std::runtime_error("oracle LQ failed");
+    for (std::size_t j = 0; j < n; ++j)
+        for (std::size_t i = 0; i < k; ++i) Qm(i, j) = Qt(j, i);
 }
 
 // ietl/jacobi.h:476-516

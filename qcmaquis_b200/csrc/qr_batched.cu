@@ -11,6 +11,11 @@
 //          v_j = (1, A(j+1:m, j) / (alpha - beta)), A(j, j) = beta;
 //     A(j:m, j+1:n) -= tau_j v_j (v_j^T A(j:m, j+1:n));
 //   R = the upper triangle (k x n); Q = H_0 ... H_{k-1} applied to the first k columns of I (m x k).
+// One rule is added (the oracle's restatement has it too): a column whose remaining part
+// |A(j:m, j)| is at most 64 eps |A|_F -- rounding noise, as in every column after the first of a
+// rank-1 block -- is set to exactly zero and gets no reflector, so that the orthonormal completion
+// of Q is fixed by the arithmetic rather than by that noise (which LAPACK implementations resolve
+// differently).
 // LQ is the QR of the transpose (the same reflectors as gelqf): L = R'^T, Q = Q'^T.
 // The work matrix and the reflectors live in global scratch (L2-resident at these sizes); a warp
 // updates one trailing column at a time (its dot product reduced within the warp).
@@ -38,7 +43,8 @@ __device__ double warp_sum(double v) {
 __global__ void __launch_bounds__(QR_THR) k_qr(const QrJob* __restrict__ jobs, const double* __restrict__ A,
                                                double* __restrict__ Q, double* __restrict__ R, double* __restrict__ W) {
     __shared__ double red[QR_WARPS];
-    __shared__ double sh_tau, sh_scale;
+    __shared__ double sh_tau, sh_scale, sh_thr;
+    __shared__ int sh_zero;
     const QrJob J = jobs[blockIdx.x];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // the matrix factorised: F (mm x nn) = A_j, or A_j^T for an LQ
@@ -50,6 +56,19 @@ __global__ void __launch_bounds__(QR_THR) k_qr(const QrJob* __restrict__ jobs, c
     for (uint64_t e = tid; e < uint64_t(mm) * nn; e += QR_THR) {
         const uint32_t i = uint32_t(e % mm), c = uint32_t(e / mm);
         w[e] = J.lq ? a[c + uint64_t(i) * J.m] : a[i + uint64_t(c) * J.m];
+    }
+    {
+        // the negligible-column threshold 64 eps |A|_F
+        double f = 0.0;
+        for (uint64_t e = tid; e < uint64_t(J.m) * J.n; e += QR_THR) f = fma(a[e], a[e], f);
+        f = warp_sum(f);
+        if (lane == 0) red[warp] = f;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int q = 0; q < QR_WARPS; ++q) t += red[q];
+            sh_thr = 64.0 * 2.220446049250313e-16 * sqrt(t);
+        }
     }
     __syncthreads();
     for (uint32_t j = 0; j < k; ++j) {
@@ -64,7 +83,8 @@ __global__ void __launch_bounds__(QR_THR) k_qr(const QrJob* __restrict__ jobs, c
             for (int q = 0; q < QR_WARPS; ++q) t += red[q];
             const double alpha = vj[j], xnorm = sqrt(t);
             double tau = 0.0, scale = 1.0;
-            if (xnorm != 0.0) {
+            const int zero = hypot(alpha, xnorm) <= sh_thr;
+            if (!zero && xnorm != 0.0) {
                 const double beta = -copysign(hypot(alpha, xnorm), alpha);
                 tau = (beta - alpha) / beta;
                 scale = 1.0 / (alpha - beta);
@@ -72,9 +92,16 @@ __global__ void __launch_bounds__(QR_THR) k_qr(const QrJob* __restrict__ jobs, c
             }
             sh_tau = tau;
             sh_scale = scale;
+            sh_zero = zero;
             taus[j] = tau;
         }
         __syncthreads();
+        if (sh_zero) {
+            // a negligible column: exactly zero in R, no reflector
+            for (uint32_t i = j + tid; i < mm; i += QR_THR) vj[i] = 0.0;
+            __syncthreads();
+            continue;
+        }
         const double tau = sh_tau;
         if (tau != 0.0) {
             const double scale = sh_scale;

@@ -123,10 +123,10 @@ def test_sweep_energies_match_oracle(gpu_ctx, L, M, sweeps, gauge):
 
 
 def test_config1_sweeps_match_golden(gpu_ctx):
-    """L=8, N=8, M=64, 4 sweeps from the device's own const initial state: per-sweep minimum
-    energies vs the committed oracle values once converged (sweeps 3, 4: 1e-10 Eh), and vs FCI.
-    Sweeps 1 and 2 start from a different rounding-fixed completion of the const state
-    (see test_sweep_energies_match_oracle) and agree to 1e-4 / 1e-7 Eh."""
+    """L=8, N=8, M=64, 4 sweeps from the device's own const initial state: every sweep's minimum energy
+    vs the committed oracle values to 1e-10 Eh, and vs FCI.  The const state's rank-1 blocks are
+    canonised by the same Householder rule on both sides (negligible columns get no reflector), so the
+    orthonormal completion, and with it the first sweeps' path, no longer depends on rounding noise."""
     import json
     import os
     from qcmaquis_b200.dmrg import DMRG
@@ -136,7 +136,7 @@ def test_config1_sweeps_match_golden(gpu_ctx):
     mins = [float(dev.sweep()[0].min()) for _ in range(4)]
     ref = golden["config1_oracle_sweep_energies"]
     d = np.abs(np.array(mins) - np.array(ref))
-    assert d[0] < 1e-4 and d[1] < 1e-7 and d[2:].max() < E_TOL, (mins, ref)
+    assert d.max() < E_TOL, (mins, ref, d)
     assert abs(mins[-1] - golden["config1_fci"]) < 1e-8
 
 
