@@ -38,7 +38,6 @@ struct Shape {
     static constexpr int A_PER = BM * BK / NTHR, B_PER = BN * BK / NTHR;
     static_assert(WM * WN * 32 == NTHR, "4 warps per CTA");
 };
-using Sh8 = Shape<1, 4, 1, 4>;   // 8 x 128
 using Sh16 = Shape<1, 4, 2, 4>;  // 16 x 128
 using Sh32 = Shape<1, 4, 4, 4>;  // 32 x 128
 using Sh64 = Shape<2, 2, 4, 4>;  // 64 x 64

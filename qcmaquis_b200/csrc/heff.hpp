@@ -106,11 +106,9 @@ struct OTileD {       // output tile of the L.S GEMM and its contiguous range of
 // count (16 x 128, 32 x 128, 64 x 64); S-build units also use 128 x 32 (see add_unit_tiles).
 // (An 8 x 128 shape for GEMM jobs of at most 8 rows measured slower at L=24, M=512: T-GEMM +7 us,
 // L.S +36 us; the 16-row tile's padding rows cost less than the extra B traffic of half-height tiles.)
-enum { SHAPE_16 = 0, SHAPE_32 = 1, SHAPE_64 = 2, SHAPE_128 = 3, SHAPE_8 = 4, N_SHAPES = 5 };
+enum { SHAPE_16 = 0, SHAPE_32 = 1, SHAPE_64 = 2, SHAPE_128 = 3, N_SHAPES = 4 };
 inline int shape_for_rows(uint32_t M) { return M <= 16 ? SHAPE_16 : (M <= 32 ? SHAPE_32 : SHAPE_64); }
-inline uint32_t shape_bm(int s) {
-    return s == SHAPE_8 ? 8 : (s == SHAPE_16 ? 16 : (s == SHAPE_32 ? 32 : (s == SHAPE_64 ? 64 : 128)));
-}
+inline uint32_t shape_bm(int s) { return s == SHAPE_16 ? 16 : (s == SHAPE_32 ? 32 : (s == SHAPE_64 ? 64 : 128)); }
 inline uint32_t shape_bn(int s) { return s == SHAPE_64 ? 64 : (s == SHAPE_128 ? 32 : 128); }
 
 struct LKD { uint32_t line, k; };  // (line, slice) position of one coefficient term

@@ -474,7 +474,6 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
     cudaStream_t s = p.stream;
     if (ev) QCM_CUDA(cudaEventRecord(ev[0], s));
     QCM_CUDA(cudaMemsetAsync(y, 0, p.x_len * sizeof(double), s));
-    launch_t<Sh8>(p, SHAPE_8, x, Tb, s);
     launch_t<Sh16>(p, SHAPE_16, x, Tb, s);
     launch_t<Sh32>(p, SHAPE_32, x, Tb, s);
     launch_t<Sh64>(p, SHAPE_64, x, Tb, s);
@@ -485,7 +484,6 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
     launch_s<Sh64>(p, SHAPE_64, Tb, Sb, s);
     launch_s<Sh128>(p, SHAPE_128, Tb, Sb, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
-    launch_ls<Sh8>(p, SHAPE_8, Sb, Pb, y, s);
     launch_ls<Sh16>(p, SHAPE_16, Sb, Pb, y, s);
     launch_ls<Sh32>(p, SHAPE_32, Sb, Pb, y, s);
     launch_ls<Sh64>(p, SHAPE_64, Sb, Pb, y, s);
@@ -503,7 +501,6 @@ void apply_mixed_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, 
     double* Tb = p.d_T.get();
     float* Thi = reinterpret_cast<float*>(Tb);
     float* Tlo = tc ? Thi + p.t_len : nullptr;
-    launch_t<Sh8>(p, SHAPE_8, x, Tb, s, Thi, Tlo);
     launch_t<Sh16>(p, SHAPE_16, x, Tb, s, Thi, Tlo);
     launch_t<Sh32>(p, SHAPE_32, x, Tb, s, Thi, Tlo);
     launch_t<Sh64>(p, SHAPE_64, x, Tb, s, Thi, Tlo);
@@ -513,7 +510,6 @@ void apply_mixed_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, 
     if (tc) run_sgemm_mixed(p, true, p.d_W32s.get(), p.d_W32s.get() + p.w_len, Thi, Tlo, Sb, p.d_merr.get(), s);
     else run_sgemm_mixed(p, false, p.d_W32.get(), nullptr, Thi, nullptr, Sb, p.d_merr.get(), s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
-    launch_ls<Sh8>(p, SHAPE_8, Sb, p.d_P.get(), y, s);
     launch_ls<Sh16>(p, SHAPE_16, Sb, p.d_P.get(), y, s);
     launch_ls<Sh32>(p, SHAPE_32, Sb, p.d_P.get(), y, s);
     launch_ls<Sh64>(p, SHAPE_64, Sb, p.d_P.get(), y, s);
@@ -527,7 +523,6 @@ void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev)
 }
 
 void heff_tgemm_device(HeffPlan& p, const double* x, double* T) {
-    launch_t<Sh8>(p, SHAPE_8, x, T, p.stream);
     launch_t<Sh16>(p, SHAPE_16, x, T, p.stream);
     launch_t<Sh32>(p, SHAPE_32, x, T, p.stream);
     launch_t<Sh64>(p, SHAPE_64, x, T, p.stream);
@@ -569,8 +564,6 @@ void heff_apply_device_scratch(HeffPlan& p, const double* x, double* y, double* 
 
 void run_tgemm(const TJobD* jobs, const DBuf<TileD>* dtiles, const std::vector<TileD>* htiles, const double* x,
                const double* R, double* T, cudaStream_t s) {
-    if (!htiles[SHAPE_8].empty())
-        k_tgemm<Sh8><<<unsigned(htiles[SHAPE_8].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_8].get(), x, R, T, nullptr, nullptr);
     if (!htiles[SHAPE_16].empty())
         k_tgemm<Sh16><<<unsigned(htiles[SHAPE_16].size()), NTHR, 0, s>>>(jobs, dtiles[SHAPE_16].get(), x, R, T, nullptr, nullptr);
     if (!htiles[SHAPE_32].empty())
