@@ -44,6 +44,15 @@ typedef struct qcm_mpo qcm_mpo;
  * (framework/dmrg/models/chem/2u1/model.hpp:184, models/generate_mpo.hpp:37). */
 int qcm_mpo_build_qc(int L, const double* h, const double* V, double cutoff, qcm_mpo** out);
 
+/* The same Hamiltonian with its integral provenance (the differentiation form): every term the spin
+ * structure allows is kept whatever its value (no cutoff), and for every entry the builder records which
+ * integrals its scale sums.  qcm_mpo_provenance: site tensor `site`'s records, scale of entry e =
+ * sum_{j in [ptr[e], ptr[e+1])} val[j] * x[id[j]] with x = (h[0 .. L^2), V[0 .. L^4)) as passed; ptr has
+ * entries + 1 elements, *n = the record count (every array NULL: only *n); pass-through entries have no
+ * records (scale 1).  Chain rule for host codes: dE/dx[id] = sum val * dE/d scale (qcm_dmrg_mpo_gradient). */
+int qcm_mpo_build_qc_tracked(int L, const double* h, const double* V, qcm_mpo** out);
+int qcm_mpo_provenance(const qcm_mpo* m, int site, uint64_t* ptr, uint64_t* id, double* val, uint64_t cap, uint64_t* n);
+
 /* Two-site MPO W_ts[p] = W[p] (x) W[p+1] contracted over the shared bond.
  * Replaces make_ts_cache_mpo / make_twosite_mpo
  * (framework/dmrg/mp_tensors/ts_ops.hpp:97-185). */
@@ -463,6 +472,25 @@ int qcm_dmrg_measure_1rdm(qcm_dmrg* d, double* gamma);
  * symmetrised over the 8 index permutations.  One expectation value per unique integral (the QC MPO of
  * the integral's orbit): about L^4 / 8 contractions, for small and moderate L. */
 int qcm_dmrg_measure_2rdm_grad(qcm_dmrg* d, double* G);
+/* Differentiation form: the energy's gradient through the adjoint of the apply (heff_adjoint; the
+ * reference has no counterpart, its oneptdm / twoptdm measurements, lib/interface/cpp_maquis.cpp:235-366,
+ * are what the gradients are checked against).  E = <Psi|W|Psi> / <Psi|Psi> of the current MPS is linear
+ * in each site tensor of W, so dE/d scale_e for an entry of site k is the adjoint of the single-site
+ * H_eff of site k (boundaries of W) with x = ybar = the orthogonality centre at k; the centre moves
+ * through a copy of the MPS by QR, with one left boundary step of W per site (the boundaries of W are
+ * recomputed for the gradient, not kept from the sweep).  Between sweeps.
+ * qcm_dmrg_mpo_gradient: W any single-site MPO of the state's physical basis and length; grad[k] receives
+ * qcm_mpo_tensor_terms(W, k) doubles, dE/d scale in W[k]'s entry order. */
+int qcm_dmrg_mpo_gradient(qcm_dmrg* d, const qcm_mpo* W, double* const* grad);
+/* qcm_dmrg_integral_gradient: dE/dh and dE/dV of the QC Hamiltonian of qcm_mpo_build_qc(L, h, V) (the
+ * integrals of the state's own Hamiltonian, or any others) through the MPO's integral provenance: the
+ * builder keeps every term the spin structure allows, whatever its value, and records which integrals
+ * each entry's scale sums; the entry gradients of qcm_dmrg_mpo_gradient are then summed per integral.
+ * dh[p*L + q] = dE/dh[p*L + q] and dV[((p*L + q)*L + r)*L + s] = dE/dV[((p*L + q)*L + r)*L + s], every
+ * array element as its own variable (dV may be NULL): dh is the spin-summed 1-RDM <a+_p a_q>, and
+ * averaging dV over the 8 index permutations of real (pq|rs) gives qcm_dmrg_measure_2rdm_grad.
+ * E - ecore = sum h dh + sum V dV (E is linear in the integrals). */
+int qcm_dmrg_integral_gradient(qcm_dmrg* d, const double* h, const double* V, double* dh, double* dV);
 /* One sweep (qcm_dmrg_steps_per_sweep steps: 2L - 2 two-site, 2L single-site): energies[steps],
  * trunc[steps] (may be NULL); only between sweeps (see qcm_dmrg_run).  Single-site steps that end a
  * half-sweep (site L-1 left to right, site 0 right to left) canonise without truncation and report

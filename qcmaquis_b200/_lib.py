@@ -43,6 +43,9 @@ def _sig(name, restype, *argtypes):
 _sig("qcm_last_error", ctypes.c_char_p)
 _sig("qcm_version", ctypes.c_char_p)
 _sig("qcm_mpo_build_qc", c_int, c_int, P(c_double), P(c_double), c_double, P(c_void_p))
+_sig("qcm_mpo_build_qc_tracked", c_int, c_int, P(c_double), P(c_double), P(c_void_p))
+_sig("qcm_mpo_provenance", c_int, c_void_p, c_int, P(ctypes.c_uint64), P(ctypes.c_uint64), P(c_double), c_uint64,
+     P(c_uint64))
 _sig("qcm_mpo_make_twosite", c_int, c_void_p, P(c_void_p))
 _sig("qcm_mpo_length", c_int, c_void_p)
 _sig("qcm_mpo_serialize", c_int, c_void_p, c_void_p, c_size_t, P(c_size_t))

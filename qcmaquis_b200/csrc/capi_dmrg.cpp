@@ -346,6 +346,43 @@ int qcm_dmrg_measure_1rdm(qcm_dmrg* d, double* gamma) {
     QCM_CATCH
 }
 
+int qcm_dmrg_mpo_gradient(qcm_dmrg* d, const qcm_mpo* W, double* const* grad) {
+    QCM_TRY
+    if (!d || !W || !grad) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_mpo_gradient: NULL argument");
+    const qcm::MPO& m = qcm::mpo_of(W);
+    qcm::DevDMRG& e = *d->e;
+    if (m.twosite || int(m.t.size()) != e.L)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_mpo_gradient: expected a single-site MPO of the state's length");
+    for (int k = 0; k < e.L; ++k)
+        if (!grad[k] && !m.t[std::size_t(k)].b1.empty()) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_mpo_gradient: NULL gradient buffer");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
+    const auto g = e.mpo_gradient(m.t);
+    for (int k = 0; k < e.L; ++k)
+        if (!g[std::size_t(k)].empty()) std::memcpy(grad[k], g[std::size_t(k)].data(), g[std::size_t(k)].size() * sizeof(double));
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_dmrg_integral_gradient(qcm_dmrg* d, const double* h, const double* V, double* dh, double* dV) {
+    QCM_TRY
+    if (!d || !h || !V || !dh) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_integral_gradient: NULL argument");
+    qcm::DevDMRG& e = *d->e;
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
+    const int L = e.L;
+    const uint64_t L2 = uint64_t(L) * L, n = L2 + L2 * L2;
+    qcm::IntegralProvenance prov;
+    const qcm::MPO W = qcm::build_qc_mpo(L, h, V, 0.0, &prov);
+    const auto g = e.mpo_gradient(W.t);
+    std::vector<double> dx(n, 0.0);
+    qcm::integral_gradient(prov, g, dx.data(), n);
+    std::memcpy(dh, dx.data(), L2 * sizeof(double));
+    if (dV) std::memcpy(dV, dx.data() + L2, L2 * L2 * sizeof(double));
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_dmrg_measure_2rdm_grad(qcm_dmrg* d, double* G) {
     QCM_TRY
     if (!d || !G) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_measure_2rdm_grad: NULL argument");

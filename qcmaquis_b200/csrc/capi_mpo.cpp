@@ -15,6 +15,7 @@
 struct qcm_mpo {
     qcm::MPO m;
     std::vector<char> unset;  // tensors qcm_mpo_create left for qcm_mpo_set_tensor
+    std::shared_ptr<qcm::IntegralProvenance> prov;  // qcm_mpo_build_qc_tracked
 };
 
 namespace {
@@ -52,6 +53,34 @@ int qcm_mpo_build_qc(int L, const double* h, const double* V, double cutoff, qcm
     auto* p = new qcm_mpo;
     p->m = qcm::build_qc_mpo(L, h, V, cutoff);
     *out = p;
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_mpo_build_qc_tracked(int L, const double* h, const double* V, qcm_mpo** out) {
+    QCM_TRY
+    if (!h || !V || !out || L < 2) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_build_qc_tracked: bad arguments");
+    auto p = std::make_unique<qcm_mpo>();
+    p->prov = std::make_shared<qcm::IntegralProvenance>();
+    p->m = qcm::build_qc_mpo(L, h, V, 0.0, p->prov.get());
+    *out = p.release();
+    return QCM_OK;
+    QCM_CATCH
+}
+
+int qcm_mpo_provenance(const qcm_mpo* m, int site, uint64_t* ptr, uint64_t* id, double* val, uint64_t cap, uint64_t* n) {
+    QCM_TRY
+    if (!m || !n) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_provenance: bad arguments");
+    if (!m->prov) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_provenance: MPO built without provenance (qcm_mpo_build_qc_tracked)");
+    if (site < 0 || std::size_t(site) >= m->prov->ptr.size()) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_provenance: site out of range");
+    const auto& pp = m->prov->ptr[std::size_t(site)];
+    const uint64_t nr = pp.back();
+    *n = nr;
+    if (!ptr && !id && !val) return QCM_OK;
+    if (!ptr || !id || !val || cap < nr) return qcm::fail(QCM_ERR_ARG, "qcm_mpo_provenance: buffers too small");
+    std::copy(pp.begin(), pp.end(), ptr);
+    std::copy(m->prov->id[std::size_t(site)].begin(), m->prov->id[std::size_t(site)].end(), id);
+    std::copy(m->prov->val[std::size_t(site)].begin(), m->prov->val[std::size_t(site)].end(), val);
     return QCM_OK;
     QCM_CATCH
 }

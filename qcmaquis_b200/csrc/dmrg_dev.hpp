@@ -320,6 +320,10 @@ struct DevDMRG {
     // <Psi|W|Psi> / <Psi|Psi> of the current MPS between sweeps (the MPS canonised to site 0) for an MPO W
     // of the same physical basis: left boundary steps through every site
     double expectation(const std::vector<MPOTensor>& W);
+    // dE/d scale_e, E = <Psi|W|Psi> / <Psi|Psi>, for every entry e of every site tensor of a single-site
+    // MPO W of the same physical basis (grad[k] in the entry order of W[k]), between sweeps: the adjoint
+    // of the single-site H_eff apply at each site, the orthogonality centre moved through a copy of the MPS
+    std::vector<std::vector<double>> mpo_gradient(const std::vector<MPOTensor>& W);
     int next_step = 0;  // step index (0 .. steps_per_sweep() - 1) the sweep continues with
     int steps_per_sweep() const { return p.single_site ? 2 * L : 2 * L - 2; }
     int sweep_count = 0;  // completed sweeps

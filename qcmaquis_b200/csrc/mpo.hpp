@@ -53,9 +53,26 @@ struct MPO {
     bool twosite = false;
 };
 
+// Integral provenance of a QC MPO: the scale of entry e of site tensor k is
+//   sum_{j in [ptr[k][e], ptr[k][e + 1])} val[k][j] * x[id[k][j]],
+// x = (h[0 .. L^2), V[0 .. L^4)) as passed to build_qc_mpo, every array element a variable of its
+// own (pass-through entries have no provenance: their scale is 1).
+struct IntegralProvenance {
+    std::vector<std::vector<uint64_t>> ptr, id;
+    std::vector<std::vector<double>> val;
+};
+
 // Builds the exact QC Hamiltonian MPO (TwoU1) from integrals h (L x L) and
 // V (L^4, chemist notation (pq|rs)).  The core energy is not part of the MPO.
-MPO build_qc_mpo(int L, const double* h, const double* V, double cutoff);
+// With prov, every term the spin structure allows is kept whatever its value (cutoff is not
+// applied) and the provenance of every entry is recorded: the MPO then holds an entry for every
+// integral the energy depends on, zero-valued ones included.
+MPO build_qc_mpo(int L, const double* h, const double* V, double cutoff, IntegralProvenance* prov = nullptr);
+
+// dE/dx over the integrals from dE/d scale of every entry (grad[k][e], entry order of site k):
+// dx[id] += val * grad for every provenance record; dx has L^2 + L^4 elements (h, then V).
+void integral_gradient(const IntegralProvenance& prov, const std::vector<std::vector<double>>& grad, double* dx,
+                       uint64_t n);
 
 // Two-site MPO: W_ts[p](b1,b3) = sum_b2 kron(W[p](b1,b2), W[p+1](b2,b3))
 // (mp_tensors/ts_ops.hpp:97-168).

@@ -134,8 +134,12 @@ struct Builder {
     std::unordered_map<uint64_t, KeyInfo> Lkeys, Rkeys;
     std::vector<uint64_t> Lkey_of, Rkey_of;  // id -> packed key
     std::vector<std::unordered_map<TKey, double, TKeyHash>> trans;  // per site
+    // integral provenance of the coefficient transitions (track): (integral id, factor) records
+    bool track = false;
+    using Prov = std::vector<std::pair<uint64_t, double>>;
+    std::vector<std::unordered_map<TKey, Prov, TKeyHash>> ptrans;
 
-    explicit Builder(int L_) : L(L_), trans(L_) {
+    explicit Builder(int L_, bool track_ = false) : L(L_), trans(L_), track(track_), ptrans(track_ ? L_ : 0) {
         id_I = ops.raw(lo.I);
         id_F = ops.raw(lo.F);
     }
@@ -163,8 +167,10 @@ struct Builder {
         return it->second.id;
     }
 
-    // One term: product (left to right) of n fermion operators.
-    void add_term(int n, const int* mode, const bool* dag, double coeff) {
+    // One term: product (left to right) of n fermion operators; its coefficient is
+    // sum_j pv[j].second * x[pv[j].first] (npv records, recorded when tracking).
+    void add_term(int n, const int* mode, const bool* dag, double coeff, const std::pair<uint64_t, double>* pv = nullptr,
+                  int npv = 0) {
         int sites[4], ns = 0;
         for (int k = 0; k < n; ++k) {
             int s = mode[k] >> 1;
@@ -175,6 +181,7 @@ struct Builder {
         std::sort(sites, sites + ns);
         uint32_t opid[4];
         int par[4];
+        double sgn = 1.0;
         for (int j = 0; j < ns; ++j) {
             int x = sites[j];
             Mat4 M = lo.I;
@@ -187,6 +194,7 @@ struct Builder {
             double sign;
             if (!ops.intern(M, opid[j], sign)) return;  // operator string vanishes
             coeff *= sign;
+            sgn *= sign;
             par[j] = cnt & 1;
         }
         const int mid = (L - 2) / 2;  // ties: L state for bonds p <= mid, R state after
@@ -243,8 +251,13 @@ struct Builder {
             uint32_t tin = sin >> 28, tout = sout >> 28;
             bool sw = (tin == T_V || tin == T_L) && (tout == T_R || tout == T_D);
             TKey key{sin, sout, op};
-            if (sw) trans[y][key] += coeff;
-            else trans[y].emplace(key, 1.0);
+            if (sw) {
+                trans[y][key] += coeff;
+                if (track) {
+                    Prov& pr = ptrans[y][key];
+                    for (int k = 0; k < npv; ++k) pr.push_back({pv[k].first, pv[k].second * sgn});
+                }
+            } else trans[y].emplace(key, 1.0);
         }
     }
 
@@ -286,7 +299,7 @@ struct Builder {
         return true;
     }
 
-    MPO finish(double cutoff) {
+    MPO finish(double cutoff, IntegralProvenance* prov = nullptr) {
         // pass-through transitions of L and R keys over their extents
         for (auto& kv : Lkeys) {
             const KeyInfo& k = kv.second;
@@ -360,21 +373,31 @@ struct Builder {
 
         MPO mpo;
         mpo.t.resize(L);
+        if (prov) {
+            prov->ptr.assign(L, {});
+            prov->id.assign(L, {});
+            prov->val.assign(L, {});
+        }
         for (int y = 0; y < L; ++y) {
             MPOTensor& T = mpo.t[y];
             T.rows = bdim[y];
             T.cols = bdim[y + 1];
             T.ops = sops;
             T.phys = qc_site_index();
-            struct E { uint32_t b1, b2, op; double v; };
+            struct E { uint32_t b1, b2, op; double v; const Prov* pv; };
             std::vector<E> es;
             for (auto& kv : trans[y]) {
-                if (std::fabs(kv.second) <= cutoff) continue;
+                if (!track && std::fabs(kv.second) <= cutoff) continue;
                 auto ib = bond[y].find(kv.first.in);
                 auto ob = bond[y + 1].find(kv.first.out);
                 if (ib == bond[y].end() || ob == bond[y + 1].end())
                     throw std::runtime_error("qc mpo: dangling automaton state");
-                es.push_back({ib->second, ob->second, kv.first.op, kv.second});
+                const Prov* pv = nullptr;
+                if (track) {
+                    auto it = ptrans[y].find(kv.first);
+                    if (it != ptrans[y].end()) pv = &it->second;
+                }
+                es.push_back({ib->second, ob->second, kv.first.op, kv.second, pv});
             }
             std::sort(es.begin(), es.end(), [](const E& a, const E& b) {
                 if (a.b1 != b.b1) return a.b1 < b.b1;
@@ -382,6 +405,26 @@ struct Builder {
                 return a.op < b.op;
             });
             for (auto& e : es) { T.b1.push_back(e.b1); T.b2.push_back(e.b2); T.op.push_back(e.op); T.scale.push_back(e.v); }
+            if (prov) {
+                // per entry its records by integral id, duplicates summed
+                auto& pp = prov->ptr[y];
+                auto& pi = prov->id[y];
+                auto& pw = prov->val[y];
+                pp.assign(1, 0);
+                Prov r;
+                for (auto& e : es) {
+                    r.clear();
+                    if (e.pv) r = *e.pv;
+                    std::sort(r.begin(), r.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+                    for (std::size_t k = 0; k < r.size();) {
+                        const uint64_t id = r[k].first;
+                        double f = 0.0;
+                        for (; k < r.size() && r[k].first == id; ++k) f += r[k].second;
+                        if (f != 0.0) { pi.push_back(id); pw.push_back(f); }
+                    }
+                    pp.push_back(pi.size());
+                }
+            }
             T.herm_left = bherm[y]; T.phase_left = bphase[y];
             T.herm_right = bherm[y + 1]; T.phase_right = bphase[y + 1];
             T.finalize();
@@ -392,26 +435,34 @@ struct Builder {
 
 }  // namespace
 
-MPO build_qc_mpo(int L, const double* h, const double* V, double cutoff) {
+MPO build_qc_mpo(int L, const double* h, const double* V, double cutoff, IntegralProvenance* prov) {
     if (L < 2) throw std::runtime_error("qc mpo: need at least two orbitals");
-    Builder B(L);
+    Builder B(L, prov != nullptr);
+    const uint64_t L2 = uint64_t(L) * L;
     const int M = 2 * L;
     auto Vat = [&](int p, int q, int r, int s) { return V[((std::size_t(p) * L + q) * L + r) * L + s]; };
     // one-electron part
     for (int p = 0; p < L; ++p)
         for (int q = 0; q < L; ++q) {
             double v = h[p * L + q];
-            if (std::fabs(v) <= cutoff) continue;
+            if (!prov && std::fabs(v) <= cutoff) continue;
+            const std::pair<uint64_t, double> pv{uint64_t(p) * L + q, 1.0};
             for (int s = 0; s < 2; ++s) {
                 int mode[2] = {2 * p + s, 2 * q + s};
                 bool dag[2] = {true, false};
-                B.add_term(2, mode, dag, v);
+                B.add_term(2, mode, dag, v, &pv, 1);
             }
         }
     // two-electron part, one canonical string a+_A a+_B a_C a_D per A<B, C<D
     auto W = [&](int i, int j, int k, int l) -> double {
         if ((i & 1) != (l & 1) || (j & 1) != (k & 1)) return 0.0;
         return 0.5 * Vat(i >> 1, l >> 1, j >> 1, k >> 1);
+    };
+    // the provenance record of W(i, j, k, l) with sign f (none where the spins forbid it)
+    auto Wp = [&](int i, int j, int k, int l, double f, std::pair<uint64_t, double>* pv, int& n) {
+        if ((i & 1) != (l & 1) || (j & 1) != (k & 1)) return;
+        const uint64_t p = uint64_t(i >> 1), q = uint64_t(l >> 1), r = uint64_t(j >> 1), t = uint64_t(k >> 1);
+        pv[n++] = {L2 + ((p * L + q) * L + r) * L + t, 0.5 * f};
     };
     for (int A = 0; A < M; ++A)
         for (int Bm = A + 1; Bm < M; ++Bm)
@@ -420,12 +471,35 @@ MPO build_qc_mpo(int L, const double* h, const double* V, double cutoff) {
                     // spin conservation: spins of {A,B} equal spins of {C,D}
                     if (((A & 1) + (Bm & 1)) != ((C & 1) + (D & 1))) continue;
                     double g = W(A, Bm, C, D) - W(Bm, A, C, D) - W(A, Bm, D, C) + W(Bm, A, D, C);
-                    if (std::fabs(g) <= cutoff) continue;
+                    std::pair<uint64_t, double> pv[4];
+                    int npv = 0;
+                    if (prov) {
+                        Wp(A, Bm, C, D, 1.0, pv, npv);
+                        Wp(Bm, A, C, D, -1.0, pv, npv);
+                        Wp(A, Bm, D, C, -1.0, pv, npv);
+                        Wp(Bm, A, D, C, 1.0, pv, npv);
+                        if (!npv) continue;
+                    } else if (std::fabs(g) <= cutoff) continue;
                     int mode[4] = {A, Bm, C, D};
                     bool dag[4] = {true, true, false, false};
-                    B.add_term(4, mode, dag, g);
+                    B.add_term(4, mode, dag, g, pv, npv);
                 }
-    return B.finish(cutoff);
+    return B.finish(cutoff, prov);
+}
+
+void integral_gradient(const IntegralProvenance& prov, const std::vector<std::vector<double>>& grad, double* dx,
+                       uint64_t n) {
+    if (grad.size() != prov.ptr.size()) throw std::runtime_error("integral gradient: one gradient per site tensor");
+    for (std::size_t k = 0; k < grad.size(); ++k) {
+        const auto& pp = prov.ptr[k];
+        if (grad[k].size() + 1 != pp.size()) throw std::runtime_error("integral gradient: entry count differs from the MPO's");
+        for (std::size_t e = 0; e < grad[k].size(); ++e)
+            for (uint64_t j = pp[e]; j < pp[e + 1]; ++j) {
+                const uint64_t id = prov.id[k][j];
+                if (id >= n) throw std::runtime_error("integral gradient: integral id out of range");
+                dx[id] += prov.val[k][j] * grad[k][e];
+            }
+    }
 }
 
 // ---------------------------------------------------------------------------

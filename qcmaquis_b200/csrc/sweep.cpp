@@ -531,6 +531,61 @@ double DevDMRG::expectation(const std::vector<MPOTensor>& W) {
     return v / n2;
 }
 
+std::vector<std::vector<double>> DevDMRG::mpo_gradient(const std::vector<MPOTensor>& W) {
+    if (next_step != 0) throw std::runtime_error("DMRG: gradients are taken between sweeps");
+    if (int(W.size()) != L) throw std::runtime_error("DMRG: gradient MPO of the wrong length");
+    for (int k = 0; k < L; ++k)
+        if (!(W[k].phys == mps[k].phys)) throw std::runtime_error("DMRG: gradient MPO with another physical basis");
+    // E = <Psi|W|Psi> / <Psi|Psi> is linear in each site tensor of W, so dE/d scale_e for an entry of
+    // site k is the single-site H_eff of site k differentiated in that scale, x . (dH_eff/ds_e) x / x.x,
+    // with x the orthogonality centre at site k (the other sites orthonormal).  The centre moves
+    // through a copy of the MPS (right-normalised on sites 1 .. L-1 between sweeps): QR of site k,
+    // R into site k + 1, one left boundary step of W; the right boundaries of W are built first.
+    std::vector<DMPS> m;
+    m.reserve(std::size_t(L));
+    for (int k = 0; k < L; ++k) {
+        make_right_paired(c, mps[k]);
+        m.push_back(right_paired_copy(c, mps[k]));
+    }
+    std::vector<std::unique_ptr<DevBoundary>> R(std::size_t(L) + 1);
+    R[std::size_t(L)] = trivial_boundary(m[std::size_t(L) - 1].right, W[std::size_t(L) - 1].cols, c.s);
+    for (int k = L - 1; k >= 1; --k) R[std::size_t(k)] = boundary_step_right(c, *R[std::size_t(k) + 1], m[std::size_t(k)], W[std::size_t(k)], true);
+    std::unique_ptr<DevBoundary> Lb = trivial_boundary(m[0].left, W[0].rows, c.s);
+    std::vector<std::vector<double>> grad(static_cast<std::size_t>(L));
+    for (int k = 0; k < L; ++k) {
+        DMPS& a = m[std::size_t(k)];
+        make_right_paired(c, a);
+        DMPS x = packed_right(c, a);
+        {
+            auto plan = build_heff_plan(*Lb, *R[std::size_t(k) + 1], W[std::size_t(k)], x.phys, x.left, x.right, false);
+            plan->stream = c.s;
+            if (plan->x_len != x.b.total) throw std::runtime_error("DMRG: site tensor layout differs from the gradient plan");
+            const uint64_t nt = heff_adjoint_terms(*plan);
+            if (nt != W[std::size_t(k)].b1.size()) throw std::runtime_error("DMRG: gradient plan without every MPO entry");
+            upload_plan(*plan);
+            const double n2 = norm2(c, x.b);
+            if (!(n2 > 0.0)) throw std::runtime_error("DMRG: zero state");
+            DBuf<double> cb(nt + 1);
+            heff_adjoint_device(*plan, x.b.d.get(), x.b.d.get(), nullptr, cb.get());
+            std::vector<double>& g = grad[std::size_t(k)];
+            g.resize(nt);
+            if (nt) QCM_CUDA(cudaMemcpyAsync(g.data(), cb.get(), nt * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+            QCM_CUDA(cudaStreamSynchronize(c.s));
+            for (double& v : g) v /= n2;
+        }
+        R[std::size_t(k) + 1].reset();
+        if (k + 1 < L) {
+            DBlocks Rm = normalize_left(c, a);
+            multiply_from_left(c, m[std::size_t(k) + 1], Rm);
+            make_left_paired(c, a);
+            DMPS ket = right_paired_copy(c, a);
+            Lb = boundary_step_left(c, *Lb, ket, a, W[std::size_t(k)], true);
+        }
+    }
+    QCM_CUDA(cudaStreamSynchronize(c.s));
+    return grad;
+}
+
 std::unique_ptr<HeffPlan> DevDMRG::plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
                                             const Index& phys, const Index& left, const Index& right, uint64_t& key,
                                             bool& resident) {

@@ -78,6 +78,8 @@ _lib._sig("qcm_dmrg_set_ortho", c_int, c_void_p, c_int, P(MPSDesc), P(P(c_double
 _lib._sig("qcm_dmrg_export_site", c_int, c_void_p, c_int, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
 _lib._sig("qcm_dmrg_measure_1rdm", c_int, c_void_p, P(c_double))
 _lib._sig("qcm_dmrg_measure_2rdm_grad", c_int, c_void_p, P(c_double))
+_lib._sig("qcm_dmrg_mpo_gradient", c_int, c_void_p, c_void_p, P(P(c_double)))
+_lib._sig("qcm_dmrg_integral_gradient", c_int, c_void_p, P(c_double), P(c_double), P(c_double), P(c_double))
 _lib._sig("qcm_dmrg_run", c_int, c_void_p, c_int, P(c_double), P(TruncResult), P(c_int))
 _lib._sig("qcm_dmrg_next_step", c_int, c_void_p)
 _lib._sig("qcm_dmrg_pending_plan", c_int, c_void_p, P(c_double), c_uint64, P(c_void_p))
@@ -326,6 +328,28 @@ class DMRG:
         G = np.zeros(self.L ** 4)
         check(lib.qcm_dmrg_measure_2rdm_grad(self.h, _lib.dptr(G)), "qcm_dmrg_measure_2rdm_grad")
         return G.reshape((self.L,) * 4, order="F")
+
+    def mpo_gradient(self, W) -> list:
+        """dE/d scale of every entry of every site tensor of the single-site MPO W (an MPO object of the
+        state's physical basis), E = <Psi|W|Psi> / <Psi|Psi>, through the adjoint of the single-site
+        apply at each site; one array per site in W's entry order.  Between sweeps."""
+        grads = [np.zeros(W.terms(k)["scale"].size) for k in range(self.L)]
+        ptrs = (P(c_double) * self.L)(*[_lib.dptr(g) for g in grads])
+        check(lib.qcm_dmrg_mpo_gradient(self.h, W.handle, ptrs), "qcm_dmrg_mpo_gradient")
+        return grads
+
+    def integral_gradient(self, h, V, with_V: bool = True):
+        """(dE/dh [p, q], dE/dV [p, q, r, s] or None) for the QC Hamiltonian of the integrals h (L x L) and V
+        (L^4, chemist notation, row-major as for MPO.qc), every array element its own variable: dh is the
+        spin-summed 1-RDM; dV averaged over the 8 permutations of real (pq|rs) is measure_2rdm_grad."""
+        L = self.L
+        h = np.ascontiguousarray(h, dtype=np.float64).reshape(L, L)
+        V = np.ascontiguousarray(V, dtype=np.float64).reshape(L, L, L, L)
+        dh = np.zeros((L, L))
+        dV = np.zeros((L, L, L, L)) if with_V else None
+        check(lib.qcm_dmrg_integral_gradient(self.h, _lib.dptr(h), _lib.dptr(V), _lib.dptr(dh),
+                                             _lib.dptr(dV) if with_V else None), "qcm_dmrg_integral_gradient")
+        return dh, dV
 
     def set_ortho(self, states):
         """Excited states: states = [[site dicts of an ortho state, as for from_mps]]; every step's solution

@@ -90,6 +90,30 @@ class MPO:
         check(lib.qcm_mpo_make_twosite(self._h, ctypes.byref(out)), "qcm_mpo_make_twosite")
         return MPO(out)
 
+    @classmethod
+    def qc_tracked(cls, h, V) -> "MPO":
+        """The QC MPO with every term the spin structure allows and its integral provenance (provenance())."""
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        L = h.shape[0]
+        out = ctypes.c_void_p()
+        check(lib.qcm_mpo_build_qc_tracked(L, _lib.dptr(h), _lib.dptr(V), ctypes.byref(out)), "qcm_mpo_build_qc_tracked")
+        return cls(out)
+
+    def provenance(self, site: int):
+        """(ptr, id, val) of tensor `site`: scale[e] = sum(val[ptr[e]:ptr[e+1]] * x[id[ptr[e]:ptr[e+1]]]), x = (h, V)
+        flattened row-major."""
+        n = ctypes.c_uint64()
+        check(lib.qcm_mpo_provenance(self._h, site, None, None, None, 0, ctypes.byref(n)), "qcm_mpo_provenance")
+        ne = self.terms(site)["scale"].size
+        ptr = np.zeros(ne + 1, dtype=np.uint64)
+        ids = np.zeros(n.value, dtype=np.uint64)
+        val = np.zeros(n.value)
+        u64 = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+        check(lib.qcm_mpo_provenance(self._h, site, u64(ptr), u64(ids), _lib.dptr(val), n.value, ctypes.byref(n)),
+              "qcm_mpo_provenance")
+        return ptr, ids, val
+
     def __len__(self):
         return lib.qcm_mpo_length(self._h)
 

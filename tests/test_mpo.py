@@ -201,3 +201,66 @@ def test_mpo_from_terms_rejects_bad_input():
     nb[2]["herm_left"] = None
     with pytest.raises(QcmError, match="disagree"):
         MPO.from_tensors(nb).blob()
+
+
+def test_tracked_mpo_provenance_and_dense_gradient():
+    """The QC MPO with integral provenance: the records reproduce every entry's scale, zero integrals keep
+    their entries, the Hamiltonian is the plain MPO's, and the entry gradients of the FCI ground state (dense
+    contraction, c^T dH/d scale_e c) summed through the records give dE/dh = the FCI one-particle density
+    matrix and sum h dh + sum V dV = E - ecore."""
+    L = 4
+    h, V, e = synthetic_integrals(L, 3)
+    h[0, 3] = h[3, 0] = 0.0
+    for (p, q, r, s) in ((0, 1, 2, 3), (1, 0, 2, 3), (0, 1, 3, 2), (1, 0, 3, 2),
+                         (2, 3, 0, 1), (3, 2, 0, 1), (2, 3, 1, 0), (3, 2, 1, 0)):
+        V[p, q, r, s] = 0.0
+    m = MPO.qc_tracked(h, V)
+    x = np.concatenate([h.ravel(), V.ravel()])
+    ts = m.tensors()
+    prov = [m.provenance(k) for k in range(L)]
+    ids_seen = set()
+    for k in range(L):
+        ptr, ids, val = prov[k]
+        sc = ts[k]["scale"]
+        assert ptr.size == sc.size + 1 and ptr[0] == 0 and ptr[-1] == ids.size
+        for j in range(sc.size):
+            a, b = int(ptr[j]), int(ptr[j + 1])
+            if a == b:
+                assert sc[j] == 1.0  # pass-through entry
+            else:
+                assert abs(np.dot(val[a:b], x[ids[a:b]]) - sc[j]) < 1e-14
+        ids_seen.update(int(i) for i in ids)
+    assert 0 * L + 3 in ids_seen and L * L + ((0 * L + 1) * L + 2) * L + 3 in ids_seen
+    H, ch = dense_mpo(ts)
+    H0, ch0 = dense_mpo(MPO.qc(h, V).tensors())
+    assert np.abs(H - H0).max() < 1e-12 and np.array_equal(ch, ch0)
+    nu = nd = L // 2
+    sel = np.where((ch[:, 0] == nu) & (ch[:, 1] == nd))[0]
+    w, Z = np.linalg.eigh(H[np.ix_(sel, sel)])
+    c = Z[:, 0]
+    grads = []
+    for k in range(L):
+        g = np.zeros(ts[k]["scale"].size)
+        for j in range(g.size):
+            unit = [dict(t) for t in ts]
+            s = np.zeros(g.size)
+            s[j] = 1.0
+            unit[k]["scale"] = s
+            Hj, _ = dense_mpo(unit)
+            g[j] = c @ Hj[np.ix_(sel, sel)] @ c
+        grads.append(g)
+    dx = np.zeros(x.size)
+    for k in range(L):
+        ptr, ids, val = prov[k]
+        for j in range(grads[k].size):
+            a, b = int(ptr[j]), int(ptr[j + 1])
+            np.add.at(dx, ids[a:b].astype(np.int64), val[a:b] * grads[k][j])
+    dh = dx[:L * L].reshape(L, L)
+    dV = dx[L * L:].reshape((L,) * 4)
+    f = FCI(h, V, e, nu, nd)
+    wf, Zf = np.linalg.eigh(f.dense())
+    cf = Zf[:, 0]
+    g1 = np.array([[cf @ (f.E[p][q] @ cf) for q in range(L)] for p in range(L)])
+    assert abs(w[0] + e - wf[0]) < 1e-11
+    assert np.abs(dh - g1).max() < 1e-10, np.abs(dh - g1).max()
+    assert abs(np.sum(h * dh) + np.sum(V * dV) - w[0]) < 1e-10
