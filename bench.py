@@ -380,6 +380,7 @@ def sweep_record(d, E, tr, dt, st0, st1, s):
             "hpsi_fp64_rayleigh": int(st1["hpsi_count_fp64"] - st0["hpsi_count_fp64"]),
             "hpsi_gflop": (st1["hpsi_flops"] - st0["hpsi_flops"]) / 1e9,
             "plans_reused": int(st1["plans_reused"] - st0["plans_reused"]),
+            "boundary_schedules_reused": int(st1["bsteps_reused"] - st0["bsteps_reused"]),
             "phase_s": {k: st1[k] - st0[k] for k in ("plan_s", "jd_s", "trunc_s", "boundary_s")}}
 
 

@@ -426,6 +426,9 @@ typedef struct {
      * conjugate scales), which skips the host schedule construction
      * (create_contraction_schedule, site_hamil_schedule.hpp:42-93) */
     uint64_t plans_built, plans_reused;
+    /* boundary steps whose schedule was built, and those that ran the previous sweep's schedule of the
+     * same step again (same structure: old boundary, site tensor sectors and block layouts) */
+    uint64_t bsteps_built, bsteps_reused;
 } qcm_dmrg_stats;
 
 /* mpo: single-site QC MPO; nup/ndown: u1_total_charge1/2.  Builds the const

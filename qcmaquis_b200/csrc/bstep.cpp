@@ -380,6 +380,106 @@ std::unique_ptr<DevBoundary> finish_boundary(BoundaryIndexH& idx, cudaStream_t s
     return B;
 }
 
+// a new boundary of a finished index (copied), zeroed
+std::unique_ptr<DevBoundary> alloc_boundary(const BoundaryIndexH& idx, cudaStream_t s) {
+    auto B = std::make_unique<DevBoundary>();
+    B->idx = idx;
+    B->data.alloc(B->idx.total ? B->idx.total : 1);
+    QCM_CUDA(cudaMemsetAsync(B->data.get(), 0, (B->idx.total ? B->idx.total : 1) * sizeof(double), s));
+    return B;
+}
+
+template <class T> uint64_t dbytes(const DBuf<T>& b) { return uint64_t(b.size()) * sizeof(T); }
+
+void hash_blocks(KeyHash& k, const DBlocks& b) {
+    k.word(b.n());
+    k.word(b.total);
+    for (std::size_t i = 0; i < b.n(); ++i) {
+        k.word(uint64_t(uint32_t(b.lc[i].a)) | (uint64_t(uint32_t(b.lc[i].b)) << 32));
+        k.word(uint64_t(uint32_t(b.rc[i].a)) | (uint64_t(uint32_t(b.rc[i].b)) << 32));
+        k.word(uint64_t(b.rows[i]) | (uint64_t(b.cols[i]) << 32));
+        k.word(b.off[i]);
+    }
+}
+
+// structure of a boundary step: side, old boundary, site tensors (indices and block layouts), MPO tensor
+uint64_t step_key(int side, const DevBoundary& B, const DMPS& ket, const DMPS* bra, const MPOTensor& W, bool symmetric) {
+    KeyHash k;
+    k.word(uint64_t(side));
+    k.word(boundary_key(B));
+    k.index(ket.phys);
+    k.index(ket.left);
+    k.index(ket.right);
+    hash_blocks(k, ket.b);
+    if (bra) {
+        k.index(bra->left);
+        k.index(bra->right);
+        hash_blocks(k, bra->b);
+    }
+    k.word(uint64_t(reinterpret_cast<uintptr_t>(&W)));
+    k.word(W.b1.size());
+    k.word(symmetric ? 1 : 0);
+    return k.h;
+}
+
+}  // namespace
+
+// One boundary step's schedule, built once and run again while the structure stays the same.
+struct BStepPlan {
+    std::vector<GemmJob> tj_gemm;  // left step: T_b jobs (A = old boundary, B = ket)
+    std::vector<TJobD> tjobs;      // right step: T-GEMM jobs and tiles (A = ket, B = old boundary)
+    std::vector<TileD> ttiles[N_SHAPES];
+    DBuf<TJobD> d_tjobs;
+    DBuf<TileD> d_ttiles[N_SHAPES];
+    SBuild sb;                     // units and coefficient tables, on the device
+    BoundaryIndexH nidx;           // the new boundary's index (finished)
+    std::vector<GemmJob> prop;     // new boundary from S and the bra / ket
+    uint64_t t_len = 0, s_len = 0;
+    uint64_t device_bytes() const {
+        uint64_t b = dbytes(d_tjobs) + dbytes(sb.d_units) + dbytes(sb.d_klist) + dbytes(sb.d_line_b1) + dbytes(sb.d_slice_off);
+        for (int k = 0; k < N_SHAPES; ++k) b += dbytes(d_ttiles[k]) + dbytes(sb.d_utiles[k]);
+        const CoefGen& g = sb.cg;
+        b += dbytes(g.d_units) + dbytes(g.d_gin) + dbytes(g.d_line_major) + dbytes(g.d_smap_id) + dbytes(g.d_smap_slot) +
+             dbytes(g.d_m_ptr) + dbytes(g.d_m_other) + dbytes(g.d_m_op) + dbytes(g.d_o_ptr) + dbytes(g.d_o_in) +
+             dbytes(g.d_line_scale) + dbytes(g.d_m_scale) + dbytes(g.d_o_val) + dbytes(g.d_b_cs) + dbytes(g.d_b_pos);
+        return b;
+    }
+};
+
+namespace {
+
+// T, S and the projections of a left step's schedule
+std::unique_ptr<DevBoundary> run_left(Ctx& c, BStepPlan& P, const DevBoundary& Lold, const DMPS& ket, const DMPS& bra) {
+    auto Ln = alloc_boundary(P.nidx, c.s);
+    Ctx::ensure(c.T, P.t_len ? P.t_len : 1);
+    Ctx::ensure(c.S, P.s_len ? P.s_len : 1);
+    batched_gemm(P.tj_gemm, Lold.data.get(), Lold.idx.total, ket.b.d.get(), ket.b.total, c.T.get(), P.t_len, c.gjobs, c.gtiles,
+                 c.s);
+    if (P.s_len) QCM_CUDA(cudaMemsetAsync(c.S.get(), 0, P.s_len * sizeof(double), c.s));
+    Ctx::ensure(c.W, P.sb.w_len ? P.sb.w_len : 1);
+    P.sb.cg.generate(c.W.get(), c.s);
+    run_sgemm(P.sb.d_units.get(), P.sb.d_utiles, P.sb.utiles, P.sb.d_line_b1.get(), P.sb.d_slice_off.get(), P.sb.d_klist.get(),
+              c.W.get(), c.T.get(), c.S.get(), c.s);
+    batched_gemm(P.prop, bra.b.d.get(), bra.b.total, c.S.get(), P.s_len, Ln->data.get(), Ln->idx.total, c.gjobs, c.gtiles, c.s);
+    return Ln;
+}
+
+// the same for a right step
+std::unique_ptr<DevBoundary> run_right(Ctx& c, BStepPlan& P, const DevBoundary& Rold, const DMPS& ket) {
+    auto Rn = alloc_boundary(P.nidx, c.s);
+    Ctx::ensure(c.T, P.t_len ? P.t_len : 1);
+    Ctx::ensure(c.S, P.s_len ? P.s_len : 1);
+    run_tgemm(P.d_tjobs.get(), P.d_ttiles, P.ttiles, ket.b.d.get(), Rold.data.get(), c.T.get(), c.s);
+    if (P.s_len) QCM_CUDA(cudaMemsetAsync(c.S.get(), 0, P.s_len * sizeof(double), c.s));
+    Ctx::ensure(c.W, P.sb.w_len ? P.sb.w_len : 1);
+    P.sb.cg.generate(c.W.get(), c.s);
+    run_sgemm(P.sb.d_units.get(), P.sb.d_utiles, P.sb.utiles, P.sb.d_line_b1.get(), P.sb.d_slice_off.get(), P.sb.d_klist.get(),
+              c.W.get(), c.T.get(), c.S.get(), c.s);
+    // A = S scratch, B = ket data, C = new boundary: three different base pointers
+    batched_gemm(P.prop, c.S.get(), P.s_len, ket.b.d.get(), ket.b.total, Rn->data.get(), Rn->idx.total, c.gjobs, c.gtiles, c.s);
+    return Rn;
+}
+
 }  // namespace
 
 namespace {
@@ -400,9 +500,22 @@ void run_accumulating(const std::vector<GemmJob>& jobs, const std::vector<std::s
 
 // ---------------------------------------------------------------------------
 static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, const DMPS& ket, const MPOTensor& W,
-                                               bool symmetric, DensityNoise* dn) {
+                                               bool symmetric, DensityNoise* dn, BStepCache* cache) {
     if (!ket.right_paired) throw std::runtime_error("boundary_step_right: ket must be right-paired");
     const double tb0 = step_now();
+    uint64_t key = 0;
+    if (cache && !dn) {
+        key = step_key(1, Rold, ket, nullptr, W, symmetric);
+        if (cache->plan && cache->key == key) {
+            auto Rn = run_right(c, *cache->plan, Rold, ket);
+            cache->hit = true;
+            step_report("right (cached)", tb0, tb0, tb0, c.s);
+            return Rn;
+        }
+        cache->plan.reset();
+        cache->bytes = 0;
+        cache->hit = false;
+    }
     const BoundaryIndexH& R = Rold.idx;
     const Index& phys = ket.phys;
     const Index& left = ket.left;
@@ -595,11 +708,10 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
         s_len += P.s_len;
         P = BPart();
     }
-    std::unique_ptr<DevBoundary> Rn;
-    std::vector<GemmJob> prop;
     if (!dn) {
+        auto P = std::make_shared<BStepPlan>();
         if (symmetric) complement_transpose(nidx, W.herm_left, W.phase_left, false);
-        Rn = finish_boundary(nidx, c.s);
+        nidx.finish();
         // prop_r: new_R[b] (ls_ket x ls_bra) = S_b * bra^T for all b of a cohort in one job
         // (rows b-major in S; C row blocks = the cohort's MPO-index blocks)
         for (const Pend& pd : pend) {
@@ -607,10 +719,31 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
             GemmJob g{};
             g.a_off = pd.s_off; g.lda = pd.nS * ls;
             g.b_off = koff[pd.lb_bra]; g.ldb = lsb; g.tb = 1;
-            g.c_off = Rn->idx.data_off[pd.ci_new]; g.ldc = ls; g.crb = ls; g.c_bs = uint64_t(ls) * lsb;
+            g.c_off = nidx.data_off[pd.ci_new]; g.ldc = ls; g.crb = ls; g.c_bs = uint64_t(ls) * lsb;
             g.M = pd.nS * ls; g.N = lsb; g.K = kcols[pd.lb_bra]; g.alpha = 1.0; g.beta = 0.0;
-            prop.push_back(g);
+            P->prop.push_back(g);
         }
+        validate_tjobs(tjobs, ket.b.total, Rold.idx.total, t_len);
+        sb.validate(t_len, s_len);
+        P->tjobs = std::move(tjobs);
+        for (int k = 0; k < N_SHAPES; ++k) P->ttiles[k] = std::move(ttiles[k]);
+        P->d_tjobs.upload(P->tjobs, c.s);
+        for (int k = 0; k < N_SHAPES; ++k) P->d_ttiles[k].upload(P->ttiles[k], c.s);
+        P->sb = std::move(sb);
+        P->sb.upload(c.s);
+        P->sb.cg.b_cs = nullptr;  // uploaded; the old boundary's scales are not read again
+        P->nidx = std::move(nidx);
+        P->t_len = t_len;
+        P->s_len = s_len;
+        const double tb1 = step_now();
+        auto Rn = run_right(c, *P, Rold, ket);
+        if (cache) {
+            cache->key = key;
+            cache->bytes = P->device_bytes();
+            cache->plan = std::move(P);
+        }
+        step_report("right", tb0, tbp, tb1, c.s);
+        return Rn;
     }
     const double tb1 = step_now();
     // execute
@@ -627,10 +760,7 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
     sb.cg.generate(c.W.get(), c.s);
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
               c.T.get(), c.S.get(), c.s);
-    if (!dn) {
-        // A = S scratch, B = ket data, C = new boundary: three different base pointers
-        batched_gemm(prop, c.S.get(), s_len, ket.b.d.get(), ket.b.total, Rn->data.get(), Rn->idx.total, c.gjobs, c.gtiles, c.s);
-    } else {
+    {
         // rbtm (tasks.cpp:364-380): dm[lb_bra] += alpha S^T S, S = (nS*ls_ket) x stripe
         std::vector<GemmJob> acc;
         std::vector<std::size_t> tgt;
@@ -649,25 +779,38 @@ static std::unique_ptr<DevBoundary> step_right(Ctx& c, const DevBoundary& Rold, 
         }
         run_accumulating(acc, tgt, c.S.get(), s_len, c.S.get(), s_len, dn->dm->d.get(), dn->dm->total, c);
     }
-    step_report("right", tb0, tbp, tb1, c.s);
-    return Rn;
+    step_report("right (noise)", tb0, tbp, tb1, c.s);
+    return nullptr;
 }
 
 std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& Rold, const DMPS& ket, const MPOTensor& W,
-                                                 bool symmetric) {
-    return step_right(c, Rold, ket, W, symmetric, nullptr);
+                                                 bool symmetric, BStepCache* cache) {
+    return step_right(c, Rold, ket, W, symmetric, nullptr, cache);
 }
 
 void rbtm_accumulate(Ctx& c, const DevBoundary& R, const DMPS& ket_rp, const MPOTensor& W, DBlocks& dm, double alpha) {
     DensityNoise dn{&dm, alpha};
-    step_right(c, R, ket_rp, W, false, &dn);
+    step_right(c, R, ket_rp, W, false, &dn, nullptr);
 }
 
 // ---------------------------------------------------------------------------
 static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, const DMPS& ket, const DMPS& bra,
-                                              const MPOTensor& W, bool symmetric, DensityNoise* dn) {
+                                              const MPOTensor& W, bool symmetric, DensityNoise* dn, BStepCache* cache) {
     if (!ket.right_paired || bra.right_paired) throw std::runtime_error("boundary_step_left: ket right-paired, bra left-paired");
     const double tb0 = step_now();
+    uint64_t key = 0;
+    if (cache && !dn) {
+        key = step_key(0, Lold, ket, &bra, W, symmetric);
+        if (cache->plan && cache->key == key) {
+            auto Ln = run_left(c, *cache->plan, Lold, ket, bra);
+            cache->hit = true;
+            step_report("left (cached)", tb0, tb0, tb0, c.s);
+            return Ln;
+        }
+        cache->plan.reset();
+        cache->bytes = 0;
+        cache->hit = false;
+    }
     const BoundaryIndexH& L = Lold.idx;
     const Index& phys = ket.phys;
     const Index& left = ket.left;
@@ -863,21 +1006,37 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
         s_len += P.s_len;
         P = BPart();
     }
-    std::unique_ptr<DevBoundary> Ln;
-    std::vector<GemmJob> prop;
     if (!dn) {
+        auto P = std::make_shared<BStepPlan>();
         if (symmetric) complement_transpose(nidx, W.herm_right, W.phase_right, true);
-        Ln = finish_boundary(nidx, c.s);
+        nidx.finish();
         // prop_l: L_new (rs_bra x nS*rs_ket) = bra^T * S
         for (const Pend& pd : pend) {
             GemmJob g{};
             g.a_off = boff[pd.rb_bra]; g.ta = 1; g.lda = brows[pd.rb_bra];
             g.b_off = pd.s_off; g.ldb = brows[pd.rb_bra];
-            g.c_off = Ln->idx.data_off[pd.ci_new]; g.ldc = uint32_t(right[pd.rb_bra].second);
+            g.c_off = nidx.data_off[pd.ci_new]; g.ldc = uint32_t(right[pd.rb_bra].second);
             g.M = uint32_t(right[pd.rb_bra].second); g.N = pd.nS * pd.rs_ket; g.K = brows[pd.rb_bra];
             g.alpha = 1.0; g.beta = 0.0;
-            prop.push_back(g);
+            P->prop.push_back(g);
         }
+        sb.validate(t_len, s_len);
+        P->tj_gemm = std::move(tj_gemm);
+        P->sb = std::move(sb);
+        P->sb.upload(c.s);
+        P->sb.cg.b_cs = nullptr;  // uploaded; the old boundary's scales are not read again
+        P->nidx = std::move(nidx);
+        P->t_len = t_len;
+        P->s_len = s_len;
+        const double tb1 = step_now();
+        auto Ln = run_left(c, *P, Lold, ket, bra);
+        if (cache) {
+            cache->key = key;
+            cache->bytes = P->device_bytes();
+            cache->plan = std::move(P);
+        }
+        step_report("left", tb0, tbp, tb1, c.s);
+        return Ln;
     }
     const double tb1 = step_now();
     Ctx::ensure(c.T, t_len ? t_len : 1);
@@ -890,9 +1049,7 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
     sb.cg.generate(c.W.get(), c.s);
     run_sgemm(sb.d_units.get(), sb.d_utiles, sb.utiles, sb.d_line_b1.get(), sb.d_slice_off.get(), sb.d_klist.get(), c.W.get(),
               c.T.get(), c.S.get(), c.s);
-    if (!dn) {
-        batched_gemm(prop, bra.b.d.get(), bra.b.total, c.S.get(), s_len, Ln->data.get(), Ln->idx.total, c.gjobs, c.gtiles, c.s);
-    } else {
+    {
         // lbtm (tasks.cpp:346-362): dm[rb_bra] += alpha S S^T, S = stripe x (nS*rs_ket)
         std::vector<GemmJob> acc;
         std::vector<std::size_t> tgt;
@@ -911,19 +1068,19 @@ static std::unique_ptr<DevBoundary> step_left(Ctx& c, const DevBoundary& Lold, c
         }
         run_accumulating(acc, tgt, c.S.get(), s_len, c.S.get(), s_len, dn->dm->d.get(), dn->dm->total, c);
     }
-    step_report("left", tb0, tbp, tb1, c.s);
-    return Ln;
+    step_report("left (noise)", tb0, tbp, tb1, c.s);
+    return nullptr;
 }
 
 std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& Lold, const DMPS& ket, const DMPS& bra,
-                                                const MPOTensor& W, bool symmetric) {
-    return step_left(c, Lold, ket, bra, W, symmetric, nullptr);
+                                                const MPOTensor& W, bool symmetric, BStepCache* cache) {
+    return step_left(c, Lold, ket, bra, W, symmetric, nullptr, cache);
 }
 
 void lbtm_accumulate(Ctx& c, const DevBoundary& L, const DMPS& ket_rp, const DMPS& bra_lp, const MPOTensor& W, DBlocks& dm,
                      double alpha) {
     DensityNoise dn{&dm, alpha};
-    step_left(c, L, ket_rp, bra_lp, W, false, &dn);
+    step_left(c, L, ket_rp, bra_lp, W, false, &dn, nullptr);
 }
 
 }  // namespace qcm

@@ -596,6 +596,8 @@ int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* s) {
     s->total_s = t.total_s;
     s->plans_built = t.plans_built;
     s->plans_reused = t.plans_reused;
+    s->bsteps_built = t.bsteps_built;
+    s->bsteps_reused = t.bsteps_reused;
     return QCM_OK;
 }
 

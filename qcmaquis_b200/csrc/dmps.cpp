@@ -8,6 +8,7 @@
 // svd_truncate / estimate_truncation (block_matrix_algorithms.h:136-240) with
 // the per-block SVDs on the device and the global cut on the host.
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
@@ -17,6 +18,12 @@
 #include "dmrg_dev.hpp"
 
 namespace qcm {
+
+namespace {
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
 
 namespace {
 
@@ -434,9 +441,18 @@ BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff)
         if (nb) QCM_CUDA(cudaMemcpyAsync(hsw.data(), swp.get(), nb * sizeof(int), cudaMemcpyDeviceToHost, c.s));
         QCM_CUDA(cudaStreamSynchronize(c.s));
         uint32_t mr = 0, mc = 0;
-        for (std::size_t k = 0; k < nb; ++k) { mr = std::max(mr, both.rows[k]); mc = std::max(mc, both.cols[k]); }
-        std::fprintf(stderr, "[svd] %zu blocks (max %u x %u): %.3f ms, sweeps max %d\n", nb, mr, mc, ms,
-                     hsw.empty() ? 0 : *std::max_element(hsw.begin(), hsw.end()));
+        std::size_t kbig = 0;
+        int modes[3] = {0, 0, 0};  // work matrix and rotations in shared memory / work matrix only / neither
+        for (std::size_t k = 0; k < nb; ++k) {
+            mr = std::max(mr, both.rows[k]);
+            mc = std::max(mc, both.cols[k]);
+            const uint64_t rr = std::max(both.rows[k], both.cols[k]), cc = std::min(both.rows[k], both.cols[k]);
+            if (rr * cc > uint64_t(both.rows[kbig]) * both.cols[kbig]) kbig = k;
+            modes[rr * cc + cc * cc <= jacobi_svd_smem_doubles() ? 0 : (rr * cc <= jacobi_svd_smem_doubles() ? 1 : 2)]++;
+        }
+        std::fprintf(stderr, "[svd] %zu blocks (max %u x %u): %.3f ms, sweeps max %d; largest %u x %u: %d sweeps; modes %d/%d/%d\n",
+                     nb, mr, mc, ms, hsw.empty() ? 0 : *std::max_element(hsw.begin(), hsw.end()), both.rows[kbig],
+                     both.cols[kbig], nb ? hsw[kbig] : 0, modes[0], modes[1], modes[2]);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
     }
@@ -529,37 +545,51 @@ BlockHeev heev_truncate(Ctx& c, DBlocks& dm, uint64_t Mmax, double cutoff) {
     const std::size_t nb = dm.n();
     for (std::size_t k = 0; k < nb; ++k)
         if (dm.rows[k] != dm.cols[k]) throw std::runtime_error("heev_truncate: density-matrix block is not square");
-    if (!c.sv) c.sv = std::make_unique<Solver>();
-    // heev per block (lanes, one host thread each), eigenvalues ascending on the device
-    std::vector<uint64_t> wo(nb);
-    uint64_t wl = 0;
-    for (std::size_t k = 0; k < nb; ++k) { wo[k] = wl; wl += dm.rows[k]; }
-    DBuf<double> Wv(std::max<uint64_t>(wl, 1));
-    int* info = c.sv->reserve_info(uint32_t(nb), c.s);
-    std::vector<std::size_t> order(nb);
-    for (std::size_t k = 0; k < nb; ++k) order[k] = k;
-    std::stable_sort(order.begin(), order.end(), [&](std::size_t x, std::size_t y) { return dm.rows[x] > dm.rows[y]; });
-    c.sv->fork(c.s);
-    std::string err;
-#pragma omp parallel for num_threads(Solver::LANES) schedule(static, 1)
-    for (int lane = 0; lane < Solver::LANES; ++lane) {
-        try {
-            QCM_CUDA(cudaSetDevice(c.device));
-            for (std::size_t i = std::size_t(lane); i < nb; i += Solver::LANES) {
-                const std::size_t k = order[i];
-                syevd_lane(*c.sv, lane, dm.d.get() + dm.off[k], int(dm.rows[k]), Wv.get() + wo[k], info + k);
-            }
-        } catch (const std::exception& e) {
-#pragma omp critical
-            err = e.what();
-        }
+    // Every block in one launch of the one-sided Jacobi SVD: a density-matrix block (the reduced density
+    // matrix plus alpha S S^T) is symmetric positive semi-definite, so its singular values are its
+    // eigenvalues and its right singular vectors -- the accumulated rotations, orthonormal and complete
+    // on the null space too -- its eigenvectors.
+    std::vector<uint64_t> wo(nb), uo(nb), vo(nb);
+    uint64_t wl = 0, ul = 0, vl = 0, jl = 0;
+    std::vector<SvdJob> sj;
+    for (std::size_t k = 0; k < nb; ++k) {
+        const uint32_t n = dm.rows[k];
+        wo[k] = wl; wl += n;
+        uo[k] = ul; ul += (uint64_t(n) * n + 31) / 32 * 32;
+        vo[k] = vl; vl += (uint64_t(n) * n + 31) / 32 * 32;
+        if (!n) continue;
+        sj.push_back(SvdJob{dm.off[k], uo[k], wo[k], vo[k], jl, n, n, uint32_t(k), 0});
+        jl += jacobi_svd_scratch(n, n);
     }
-    if (!err.empty()) throw std::runtime_error(err);
-    c.sv->join(c.s);
-    c.sv->check(c.s);
-    std::vector<double> hw(wl);
-    if (wl) QCM_CUDA(cudaMemcpyAsync(hw.data(), Wv.get(), wl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    DBuf<double> Ub(std::max<uint64_t>(ul, 1)), Sb(std::max<uint64_t>(wl, 1)), Vb(std::max<uint64_t>(vl, 1)),
+        Wj(std::max<uint64_t>(jl, 1));
+    DBuf<int> zc(std::max<std::size_t>(nb, 1));
+    double t_heev = 0.0;
+    static const bool stats = std::getenv("QCM_SVD_STATS") != nullptr;
+    if (stats) {
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        t_heev = now_ms();
+    }
+    batched_jacobi_svd(sj, dm.d.get(), dm.total, Ub.get(), std::max<uint64_t>(ul, 1), Sb.get(), std::max<uint64_t>(wl, 1),
+                       Vb.get(), std::max<uint64_t>(vl, 1), Wj.get(), std::max<uint64_t>(jl, 1), zc.get(), c.sjobs, c.s, nullptr);
+    // eigenvectors back into dm in ascending eigenvalue order (the SVD's descending order reversed)
+    std::vector<CopyJob> cj;
+    for (std::size_t k = 0; k < nb; ++k)
+        if (dm.rows[k]) cj.push_back(CopyJob{vo[k], dm.off[k], dm.rows[k], dm.rows[k], dm.rows[k], dm.rows[k], 0, 1});
+    if (!cj.empty()) batched_copy(cj, Vb.get(), std::max<uint64_t>(vl, 1), dm.d.get(), dm.total, c.cjobs, c.s);
+    std::vector<double> hs(wl);
+    if (wl) QCM_CUDA(cudaMemcpyAsync(hs.data(), Sb.get(), wl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
     QCM_CUDA(cudaStreamSynchronize(c.s));
+    if (stats) {
+        uint32_t mn = 0;
+        uint64_t n3 = 0;
+        for (std::size_t k = 0; k < nb; ++k) { mn = std::max(mn, dm.rows[k]); n3 += uint64_t(dm.rows[k]) * dm.rows[k] * dm.rows[k]; }
+        std::fprintf(stderr, "[heev] %zu blocks (max %u, sum n^3 %.3g): %.3f ms\n", nb, mn, double(n3), now_ms() - t_heev);
+    }
+    // ascending eigenvalues per block, as the eigenvectors
+    std::vector<double> hw(wl);
+    for (std::size_t k = 0; k < nb; ++k)
+        for (uint32_t i = 0; i < dm.rows[k]; ++i) hw[wo[k] + i] = hs[wo[k] + dm.rows[k] - 1 - i];
     // descending order; the cut is on sqrt of the positive eigenvalues (others kept as they are)
     std::vector<std::vector<double>> vals(nb);
     for (std::size_t k = 0; k < nb; ++k) {

@@ -242,10 +242,21 @@ void jacobi_davidson_batched(HeffPlan& g, const std::vector<uint64_t>& xo, const
 
 // Boundary steps (contractions/boundary_ops/move_boundary.hpp:147-404): new left boundary
 // from L[site] and mps[site]; new right boundary from R[site+1] and mps[site].
+// A step's schedule (T jobs, S-build units and their coefficient tables, the new boundary's index,
+// the projection GEMMs) depends only on structure: the old boundary's index, the site tensors' sectors
+// and block layouts, the MPO tensor.  With a cache, a step whose structure matches the cached
+// schedule's runs that schedule again (its device lists stay on the device) instead of building it.
+struct BStepPlan;
+struct BStepCache {
+    uint64_t key = 0;
+    std::shared_ptr<BStepPlan> plan;
+    uint64_t bytes = 0;  // device bytes the cached schedule holds
+    bool hit = false;    // the last step ran the cached schedule
+};
 std::unique_ptr<DevBoundary> boundary_step_left(Ctx& c, const DevBoundary& L, const DMPS& ket_rp, const DMPS& bra_lp,
-                                                const MPOTensor& W, bool symmetric);
+                                                const MPOTensor& W, bool symmetric, BStepCache* cache = nullptr);
 std::unique_ptr<DevBoundary> boundary_step_right(Ctx& c, const DevBoundary& R, const DMPS& ket, const MPOTensor& W,
-                                                 bool symmetric);
+                                                 bool symmetric, BStepCache* cache = nullptr);
 
 // trivial boundary: one cohort per sector, aux_dim blocks of ones (boundary.h / optimize.h:158-195)
 std::unique_ptr<DevBoundary> trivial_boundary(const Index& idx, uint32_t aux_dim, cudaStream_t s);
@@ -287,6 +298,7 @@ struct DMRGParams {
 
 struct DMRGStats {
     uint64_t plans_built = 0, plans_reused = 0;  // step plans built from scratch / re-staged from the cache
+    uint64_t bsteps_built = 0, bsteps_reused = 0;  // boundary-step schedules built / run again from the cache
     uint64_t hpsi_count = 0;
     uint64_t hpsi_count64 = 0;   // mixed form: the extra FP64 applies (Rayleigh quotients)
     double hpsi_flops64 = 0;
@@ -351,6 +363,12 @@ struct DevDMRG {
     };
     std::vector<CachedPlan> plan_cache_;
     uint64_t plan_cache_budget_ = 0, plan_cache_bytes_ = 0;
+    // boundary-step schedules of the previous sweep's steps (one per step), their device lists within
+    // a budget of a sixteenth of the device's memory
+    std::vector<BStepCache> bstep_cache_;
+    uint64_t bstep_cache_bytes_ = 0, bstep_cache_budget_ = 0;
+    BStepCache* bstep_cache_for(int step);
+    void bstep_cache_done(int step);
     std::unique_ptr<HeffPlan> plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
                                        const Index& phys, const Index& left, const Index& right, uint64_t& key,
                                        bool& resident);

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <memory>
 #include <unordered_map>
 #include <vector>
@@ -58,7 +59,38 @@ struct BoundaryIndexH {
 struct DevBoundary {
     BoundaryIndexH idx;
     DBuf<double> data;
+    // structure hash of idx (boundary_key), computed on first use: the index of a boundary is not
+    // changed after the boundary is made
+    mutable uint64_t key = 0;
 };
+
+// Hash of structure (sectors, cohorts, block offsets, conjugate scales) for the plan caches
+struct KeyHash {
+    uint64_t h = 0x243F6A8885A308D3ull;
+    void word(uint64_t v) {
+        h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
+        h *= 0xBF58476D1CE4E5B9ull;
+        h ^= h >> 31;
+    }
+    template <class T> void vec(const std::vector<T>& v) {
+        word(v.size());
+        for (const T& x : v) {
+            uint64_t u = 0;
+            std::memcpy(&u, &x, sizeof(T) < 8 ? sizeof(T) : 8);
+            word(u);
+        }
+    }
+    void index(const Index& I) {
+        word(I.size());
+        for (auto& e : I.d) { word(uint64_t(uint32_t(e.first.a))); word(uint64_t(uint32_t(e.first.b))); word(e.second); }
+    }
+    void boundary(const BoundaryIndexH& B) {
+        index(B.bra); index(B.ket); word(B.aux);
+        vec(B.cbra); vec(B.cket); vec(B.lsz); vec(B.rsz); vec(B.nb); vec(B.tr); vec(B.offsets); vec(B.cscale);
+    }
+};
+// B's structure hash, cached in B
+uint64_t boundary_key(const DevBoundary& B);
 
 // Flattened plan.  All offsets are element offsets into the device buffers.
 struct TJobD {        // T[c_off] (M x N) = psi[a_off] (M x K, lda) * Rop (K x N)
@@ -291,6 +323,9 @@ void rebind_plan(HeffPlan& p, const DevBoundary& L, const DevBoundary& R);
 // 64-bit fingerprint of what a plan's work lists depend on besides the MPO tensor: the two boundaries'
 // sectors, cohorts, block offsets, conjugate scales and transposition flags, and the site indices.
 uint64_t plan_structure_key(const BoundaryIndexH& L, const BoundaryIndexH& R, const Index& phys, const Index& left,
+                            const Index& right);
+// the same from the boundaries' cached hashes
+uint64_t plan_structure_key(const DevBoundary& L, const DevBoundary& R, const Index& phys, const Index& left,
                             const Index& right);
 
 // y = H_eff x on device (x, y device pointers of length x_len), launched on p.stream.

@@ -227,38 +227,32 @@ void add_unit_tiles(const UnitD& u, uint32_t item, const LKD* ents, std::size_t 
     emit_tiles(u, item, c, utiles, klist);
 }
 
-namespace {
-struct KeyHash {
-    uint64_t h = 0x243F6A8885A308D3ull;
-    void word(uint64_t v) {
-        h ^= v + 0x9E3779B97F4A7C15ull + (h << 6) + (h >> 2);
-        h *= 0xBF58476D1CE4E5B9ull;
-        h ^= h >> 31;
-    }
-    template <class T> void vec(const std::vector<T>& v) {
-        word(v.size());
-        for (const T& x : v) {
-            uint64_t u = 0;
-            std::memcpy(&u, &x, sizeof(T) < 8 ? sizeof(T) : 8);
-            word(u);
-        }
-    }
-    void index(const Index& I) {
-        word(I.size());
-        for (auto& e : I.d) { word(uint64_t(uint32_t(e.first.a))); word(uint64_t(uint32_t(e.first.b))); word(e.second); }
-    }
-    void boundary(const BoundaryIndexH& B) {
-        index(B.bra); index(B.ket); word(B.aux);
-        vec(B.cbra); vec(B.cket); vec(B.lsz); vec(B.rsz); vec(B.nb); vec(B.tr); vec(B.offsets); vec(B.cscale);
-    }
-};
-}  // namespace
 
 uint64_t plan_structure_key(const BoundaryIndexH& L, const BoundaryIndexH& R, const Index& phys, const Index& left,
                             const Index& right) {
     KeyHash k;
     k.boundary(L);
     k.boundary(R);
+    k.index(phys);
+    k.index(left);
+    k.index(right);
+    return k.h;
+}
+
+uint64_t boundary_key(const DevBoundary& B) {
+    if (!B.key) {
+        KeyHash k;
+        k.boundary(B.idx);
+        B.key = k.h | 1;
+    }
+    return B.key;
+}
+
+uint64_t plan_structure_key(const DevBoundary& L, const DevBoundary& R, const Index& phys, const Index& left,
+                            const Index& right) {
+    KeyHash k;
+    k.word(boundary_key(L));
+    k.word(boundary_key(R));
     k.index(phys);
     k.index(left);
     k.index(right);

@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <stdexcept>
 #include <string>
 
@@ -20,58 +21,6 @@ namespace {
 
 constexpr uint32_t INFO_CAP = 4096;
 
-// 32 x 32 tiled transpose: dst(j, i) = src(i, j), src m x n (ld lds), dst n x m (ld ldd)
-__global__ void k_transpose(const double* __restrict__ src, uint32_t m, uint32_t n, uint32_t lds, double* __restrict__ dst,
-                            uint32_t ldd) {
-    __shared__ double t[32][33];
-    const uint32_t i0 = blockIdx.x * 32, j0 = blockIdx.y * 32;
-    for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
-        uint32_t i = i0 + threadIdx.x, j = j0 + r;
-        if (i < m && j < n) t[r][threadIdx.x] = src[i + uint64_t(j) * lds];
-    }
-    __syncthreads();
-    for (uint32_t r = threadIdx.y; r < 32; r += blockDim.y) {
-        uint32_t j = j0 + threadIdx.x, i = i0 + r;
-        if (i < m && j < n) dst[j + uint64_t(i) * ldd] = t[threadIdx.x][r];
-    }
-}
-
-// mode 0: dst(i, j) = i <= j ? src(i, j) : 0   (R factor)
-// mode 1: dst(i, j) = j <= i ? src(j, i) : 0   (L factor = transposed R factor)
-__global__ void k_tri(const double* __restrict__ src, uint32_t lds, double* __restrict__ dst, uint32_t ldd, uint32_t rows,
-                      uint32_t cols, int mode) {
-    const uint64_t n = uint64_t(rows) * cols;
-    for (uint64_t e = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; e < n; e += uint64_t(gridDim.x) * blockDim.x) {
-        uint32_t j = uint32_t(e / rows), i = uint32_t(e - uint64_t(j) * rows);
-        double v = 0.0;
-        if (mode == 0) { if (i <= j) v = src[i + uint64_t(j) * lds]; }
-        else { if (j <= i) v = src[j + uint64_t(i) * lds]; }
-        dst[i + uint64_t(j) * ldd] = v;
-    }
-}
-
-void transpose(const double* src, uint32_t m, uint32_t n, uint32_t lds, double* dst, uint32_t ldd, cudaStream_t s) {
-    if (!m || !n) return;
-    dim3 g((m + 31) / 32, (n + 31) / 32), b(32, 8);
-    k_transpose<<<g, b, 0, s>>>(src, m, n, lds, dst, ldd);
-    QCM_CUDA(cudaGetLastError());
-}
-
-void tri(const double* src, uint32_t lds, double* dst, uint32_t ldd, uint32_t rows, uint32_t cols, int mode, cudaStream_t s) {
-    if (!rows || !cols) return;
-    uint64_t n = uint64_t(rows) * cols;
-    unsigned g = unsigned(std::min<uint64_t>((n + 255) / 256, 148 * 8));
-    k_tri<<<g, 256, 0, s>>>(src, lds, dst, ldd, rows, cols, mode);
-    QCM_CUDA(cudaGetLastError());
-}
-
-void ensure(DBuf<double>& b, std::size_t n) { if (b.size() < n) b.alloc(std::max<std::size_t>(n, 1)); }
-
-int* next_info(Solver& sv, cudaStream_t s) {
-    if (sv.n_info >= INFO_CAP) sv.check(s);
-    return sv.info.get() + sv.n_info++;
-}
-
 }  // namespace
 
 Solver::Solver() {
@@ -80,7 +29,6 @@ Solver::Solver() {
     QCM_SOLVER(cusolverDnXgesvdjSetMaxSweeps(svdp, 100));
     QCM_SOLVER(cusolverDnXgesvdjSetSortEig(svdp, 1));
     info.alloc(INFO_CAP);
-    tau.alloc(1024);
     QCM_CUDA(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
     for (Lane& L : lane) {
         QCM_CUDA(cudaStreamCreateWithFlags(&L.s, cudaStreamNonBlocking));
@@ -145,19 +93,6 @@ void Solver::check(cudaStream_t s) {
         if (v != 0) throw std::runtime_error("device factorization failed (info " + std::to_string(v) + ")");
 }
 
-void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* U, double* S, double* V) {
-    if (m == 0 || n == 0) return;
-    sv.bind(s);
-    ensure(sv.a, std::size_t(m) * n);
-    QCM_CUDA(cudaMemcpyAsync(sv.a.get(), A, std::size_t(m) * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    int lwork = 0;
-    QCM_SOLVER(cusolverDnDgesvdj_bufferSize(sv.h, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, sv.a.get(), m, S, U, m, V, n, &lwork,
-                                            sv.svdp));
-    ensure(sv.work, std::size_t(lwork));
-    QCM_SOLVER(cusolverDnDgesvdj(sv.h, CUSOLVER_EIG_MODE_VECTOR, 1, m, n, sv.a.get(), m, S, U, m, V, n, sv.work.get(), lwork,
-                                 next_info(sv, s), sv.svdp));
-}
-
 void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, double* S, double* V, int* info) {
     if (m == 0 || n == 0) return;
     Solver::Lane& L = sv.lane[l];
@@ -204,9 +139,11 @@ __device__ __forceinline__ double half_sum(double v) {
 __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ jobs, const double* __restrict__ A,
                                                      double* __restrict__ U, double* __restrict__ S, double* __restrict__ V,
                                                      double* __restrict__ Wg, uint32_t smem_doubles,
-                                                     int* __restrict__ zero_count, int* __restrict__ sweeps_used) {
+                                                     int* __restrict__ zero_count, int* __restrict__ sweeps_used,
+                                                     int deflate) {
     extern __shared__ double smem[];
     __shared__ int rotated;
+    __shared__ double thr2;
     __shared__ uint32_t rank_of[1024];
     __shared__ double nrm[1024];
     const SvdJob J = jobs[blockIdx.x];
@@ -228,6 +165,19 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         G[i] = tall ? a[row + uint64_t(col) * J.m] : a[col + uint64_t(row) * J.m];
     }
     for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
+    {
+        // the negligible-column level (64 eps |A|_F)^2; rotations keep |A|_F
+        double f = 0.0;
+        for (uint64_t i = tid; i < uint64_t(r) * c; i += JTHR) f = fma(a[i], a[i], f);
+        f = warp_sum(f);
+        if (lane == 0) nrm[warp] = f;
+        __syncthreads();
+        if (tid == 0) {
+            double t = 0.0;
+            for (int w = 0; w < nwarp; ++w) t += nrm[w];
+            thr2 = deflate ? (64.0 * JEPS) * (64.0 * JEPS) * t : 0.0;
+        }
+    }
     __syncthreads();
     const uint32_t cp = c + (c & 1u);  // players, padded to even
     const double tol2 = (JEPS * double(r)) * (JEPS * double(r));
@@ -235,10 +185,17 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
     for (int sweep = 0; sweep < JMAX_SWEEPS && c > 1; ++sweep) {
         if (tid == 0) rotated = 0;
         for (uint32_t j = warp; j < c; j += nwarp) {
-            const double* g = G + uint64_t(j) * r;
+            double* g = G + uint64_t(j) * r;
             double x = 0.0;
             for (uint32_t i = lane; i < r; i += 32) x = fma(g[i], g[i], x);
             x = warp_sum(x);
+            // a column at the rounding level of A is set to exactly zero and takes no further
+            // rotation (gamma = 0): rotating rounding noise against the other columns would only
+            // feed it back into them
+            if (x <= thr2 && x > 0.0) {
+                for (uint32_t i = lane; i < r; i += 32) g[i] = 0.0;
+                x = 0.0;
+            }
             if (lane == 0) nrm[j] = x;
         }
         __syncthreads();
@@ -339,6 +296,8 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
 }
 }  // namespace
 
+uint64_t jacobi_svd_smem_doubles() { return JSMEM_DOUBLES; }
+
 uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n) {
     const uint64_t r = std::max(m, n), c = std::min(m, n);
     return r * c + c * c;
@@ -350,7 +309,6 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
     // one launch for the blocks whose work matrix G fits in shared memory (their rotations Q too where
     // they fit), one with both in the global scratch for the rest
     std::vector<SvdJob> small, large;
-    uint64_t smax = 0;
     for (const SvdJob& j : jobs) {
         const uint64_t k = std::min(j.m, j.n);
         if (!j.m || !j.n) continue;
@@ -358,77 +316,25 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
         if (j.a_off + uint64_t(j.m) * j.n > a_len || j.u_off + uint64_t(j.m) * k > u_len || j.s_off + k > s_len ||
             j.v_off + uint64_t(j.n) * k > v_len || j.w_off + jacobi_svd_scratch(j.m, j.n) > w_len)
             throw std::runtime_error("batched_jacobi_svd: block outside its buffers");
-        // shared memory for G (r x c) and, where it fits too, Q (c x c)
-        const uint64_t need = jacobi_svd_scratch(j.m, j.n), rc = std::max(j.m, j.n) * uint64_t(k);
-        if (rc <= JSMEM_DOUBLES) { small.push_back(j); smax = std::max(smax, need <= JSMEM_DOUBLES ? need : rc); }
+        // the blocks working in global memory first: they take longest
+        if (std::max(j.m, j.n) * uint64_t(k) <= JSMEM_DOUBLES) small.push_back(j);
         else large.push_back(j);
     }
     uint32_t nid = 0;
     for (const SvdJob& j : jobs) nid = std::max(nid, j.id + 1);
     if (nid) QCM_CUDA(cudaMemsetAsync(zero_count, 0, nid * sizeof(int), s));
-    std::vector<SvdJob> all(small);
-    all.insert(all.end(), large.begin(), large.end());
+    std::vector<SvdJob> all(large);
+    all.insert(all.end(), small.begin(), small.end());
     if (all.empty()) return;
     jobbuf.upload(all, s);
-    if (!small.empty()) {
-        const std::size_t bytes = smax * sizeof(double);
-        QCM_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
-        k_jacobi_svd<<<unsigned(small.size()), JTHR, bytes, s>>>(jobbuf.get(), A, U, S, V, W, uint32_t(smax), zero_count,
-                                                                 sweeps_used);
-        QCM_CUDA(cudaGetLastError());
-    }
-    if (!large.empty()) {
-        k_jacobi_svd<<<unsigned(large.size()), JTHR, 0, s>>>(jobbuf.get() + small.size(), A, U, S, V, W, 0u, zero_count,
-                                                              sweeps_used);
-        QCM_CUDA(cudaGetLastError());
-    }
-}
-
-void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info) {
-    if (n == 0) return;
-    Solver::Lane& L = sv.lane[l];
-    AllocStream scope(L.s);
-    int lwork = 0;
-    QCM_SOLVER(cusolverDnDsyevd_bufferSize(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, W, &lwork));
-    if (L.work.size() < std::size_t(lwork)) L.work.alloc(std::size_t(lwork));
-    QCM_SOLVER(cusolverDnDsyevd(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, W, L.work.get(), lwork, info));
-}
-
-namespace {
-// Householder QR of a (m x n, ld m) in place; leaves R in the upper triangle and Q's reflectors below
-void geqrf_orgqr(Solver& sv, cudaStream_t s, int m, int n, double* Rout, uint32_t ldr, int rmode, uint32_t rrows,
-                 uint32_t rcols) {
-    const int k = std::min(m, n);
-    ensure(sv.tau, std::size_t(k));
-    int lw1 = 0, lw2 = 0;
-    QCM_SOLVER(cusolverDnDgeqrf_bufferSize(sv.h, m, n, sv.a.get(), m, &lw1));
-    QCM_SOLVER(cusolverDnDorgqr_bufferSize(sv.h, m, k, k, sv.a.get(), m, sv.tau.get(), &lw2));
-    ensure(sv.work, std::size_t(std::max(lw1, lw2)));
-    QCM_SOLVER(cusolverDnDgeqrf(sv.h, m, n, sv.a.get(), m, sv.tau.get(), sv.work.get(), std::max(lw1, lw2), next_info(sv, s)));
-    tri(sv.a.get(), uint32_t(m), Rout, ldr, rrows, rcols, rmode, s);
-    QCM_SOLVER(cusolverDnDorgqr(sv.h, m, k, k, sv.a.get(), m, sv.tau.get(), sv.work.get(), std::max(lw1, lw2),
-                                next_info(sv, s)));
-}
-}  // namespace
-
-void qr_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* Q, double* R) {
-    if (m == 0 || n == 0) return;
-    sv.bind(s);
-    const int k = std::min(m, n);
-    ensure(sv.a, std::size_t(m) * n);
-    QCM_CUDA(cudaMemcpyAsync(sv.a.get(), A, std::size_t(m) * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    geqrf_orgqr(sv, s, m, n, R, uint32_t(k), 0, uint32_t(k), uint32_t(n));
-    QCM_CUDA(cudaMemcpyAsync(Q, sv.a.get(), std::size_t(m) * k * sizeof(double), cudaMemcpyDeviceToDevice, s));
-}
-
-void lq_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* L, double* Q) {
-    if (m == 0 || n == 0) return;
-    sv.bind(s);
-    const int k = std::min(m, n);
-    ensure(sv.a, std::size_t(m) * n);
-    transpose(A, uint32_t(m), uint32_t(n), uint32_t(m), sv.a.get(), uint32_t(n), s);  // a = A^T (n x m)
-    geqrf_orgqr(sv, s, n, m, L, uint32_t(m), 1, uint32_t(m), uint32_t(k));             // L = R'^T (m x k)
-    transpose(sv.a.get(), uint32_t(n), uint32_t(k), uint32_t(n), Q, uint32_t(k), s);   // Q = Q'^T (k x n)
+    // one launch: each CTA places its work matrix and rotations by its own size (one CTA per SM
+    // in either case, at 1024 threads)
+    static const int deflate = std::getenv("QCM_JACOBI_DEFLATE") ? 1 : 0;
+    const std::size_t bytes = std::size_t(JSMEM_DOUBLES) * sizeof(double);
+    QCM_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    k_jacobi_svd<<<unsigned(all.size()), JTHR, bytes, s>>>(jobbuf.get(), A, U, S, V, W, JSMEM_DOUBLES, zero_count,
+                                                           sweeps_used, deflate);
+    QCM_CUDA(cudaGetLastError());
 }
 
 void sym_lowest_eigenpair(const double* M, int ldm, int n, double& w, std::vector<double>& z) {

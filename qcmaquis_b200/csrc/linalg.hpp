@@ -1,10 +1,12 @@
 // Dense per-block factorizations on the device, used by the truncation and
-// canonisation steps of the sweep:
-//   thin SVD   (framework/alps/matrix/algorithms.hpp:243-257, gesvd 'S','S')
-//   thin QR    (algorithms.hpp:260-291, geqrf + orgqr)
-//   thin LQ    (algorithms.hpp:293-325, gelqf + orglq; here QR of the transpose,
-//               which applies the same Householder reflectors)
-// plus the Rayleigh-Ritz eigenproblem of the Jacobi-Davidson solver (host, <= 64 x 64).
+// canonisation steps of the sweep, each a batched kernel of this project (one CTA per block):
+//   thin SVD   (framework/alps/matrix/algorithms.hpp:243-257, gesvd 'S','S'): one-sided Jacobi
+//   symmetric eigendecomposition of a density-matrix block (algorithms.hpp:374-396, heevd): the
+//              same Jacobi, the block being positive semi-definite
+//   thin QR    (algorithms.hpp:260-291, geqrf + orgqr) and thin LQ (algorithms.hpp:293-325, gelqf
+//              + orglq, here QR of the transpose): Householder
+// plus the Rayleigh-Ritz eigenproblem of the Jacobi-Davidson solver (host, <= 64 x 64).  cuSOLVER's
+// gesvdj remains only as the completion of a block whose kept singular values include exact zeros.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -20,11 +22,10 @@ namespace qcm {
 struct Solver {
     cusolverDnHandle_t h = nullptr;
     gesvdjInfo_t svdp = nullptr;
-    DBuf<double> work, a, b, tau;
     DBuf<int> info;  // one status word per factorization since the last check
     uint32_t n_info = 0;
-    // side streams for independent per-block factorizations (fork from / join to a stream)
-    static constexpr int LANES = 8;
+    // a side stream for the per-block completions (fork from / join to a stream)
+    static constexpr int LANES = 1;
     struct Lane {
         cudaStream_t s = nullptr;
         cusolverDnHandle_t h = nullptr;
@@ -49,10 +50,8 @@ struct Solver {
 };
 
 // A (m x n, lda = m) is read only.  k = min(m, n).
-// U (m x k, ld m), S (k, descending), V (n x k, ld n): A = U diag(S) V^T
-void svd_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* U, double* S, double* V);
-// the same on side lane `l` (between fork and join), status to *info; lanes may be driven
-// from different host threads (one thread per lane: the Jacobi SVD blocks its caller)
+// U (m x k, ld m), S (k, descending), V (n x k, ld n): A = U diag(S) V^T, by cuSOLVER's gesvdj on side
+// lane `l` (between fork and join), status to *info
 void svd_thin_lane(Solver& sv, int l, const double* A, int m, int n, double* U, double* S, double* V, int* info);
 // Thin SVDs of many small blocks in one launch (one-sided Jacobi, one CTA per block):
 // A_j (m x n, ld m) = U_j diag(S_j) V_j^T with U_j (m x k, ld m), S_j descending (k), V_j
@@ -66,6 +65,8 @@ struct SvdJob {
     uint32_t id, pad;  // zero_count[id] receives the block's number of zero singular values
 };
 uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n);
+// doubles of the Jacobi kernel's shared-memory work space (blocks larger than it work in L2)
+uint64_t jacobi_svd_smem_doubles();
 // A, U, S, V, W: base pointers of the offsets in jobs (host list, validated against the lengths)
 void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
                         uint64_t s_len, double* V, uint64_t v_len, double* W, uint64_t w_len, int* zero_count,
@@ -81,14 +82,6 @@ struct QrJob {
 uint64_t qr_scratch(uint32_t m, uint32_t n, bool lq);
 void batched_qr(const std::vector<QrJob>& jobs, const double* A, uint64_t a_len, double* Q, uint64_t q_len, double* R,
                 uint64_t r_len, double* W, uint64_t w_len, DBuf<QrJob>& jobbuf, cudaStream_t s);
-// Symmetric eigendecomposition (divide and conquer, lower triangle) on lane `l`: A (n x n, ld n)
-// is overwritten by the eigenvectors, W receives the eigenvalues in ascending order.
-// Replaces heevd('V') of alps/matrix/algorithms.hpp:374-396 (which then reverses the order).
-void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info);
-// Q (m x k, ld m), R (k x n, ld k, upper trapezoidal): A = Q R
-void qr_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* Q, double* R);
-// L (m x k, ld m, lower trapezoidal), Q (k x n, ld k): A = L Q
-void lq_thin(Solver& sv, cudaStream_t s, const double* A, int m, int n, double* L, double* Q);
 
 // Lowest eigenpair of the symmetric n x n matrix held in the upper triangle of
 // M (column-major, leading dimension ldm); cyclic Jacobi rotations, FP64.

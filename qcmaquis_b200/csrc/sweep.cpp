@@ -586,10 +586,37 @@ std::vector<std::vector<double>> DevDMRG::mpo_gradient(const std::vector<MPOTens
     return grad;
 }
 
+BStepCache* DevDMRG::bstep_cache_for(int step) {
+    if (bstep_cache_.size() != std::size_t(steps_per_sweep())) {
+        bstep_cache_.clear();
+        bstep_cache_.resize(std::size_t(steps_per_sweep()));
+        bstep_cache_bytes_ = 0;
+    }
+    if (!bstep_cache_budget_) {
+        size_t free_b = 0, total_b = 0;
+        QCM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        bstep_cache_budget_ = uint64_t(total_b) / 16;
+    }
+    BStepCache& e = bstep_cache_[std::size_t(step)];
+    bstep_cache_bytes_ -= e.bytes;
+    return &e;
+}
+
+void DevDMRG::bstep_cache_done(int step) {
+    BStepCache& e = bstep_cache_[std::size_t(step)];
+    ++(e.hit ? st.bsteps_reused : st.bsteps_built);
+    if (bstep_cache_bytes_ + e.bytes > bstep_cache_budget_) {
+        e.plan.reset();
+        e.key = 0;
+        e.bytes = 0;
+    }
+    bstep_cache_bytes_ += e.bytes;
+}
+
 std::unique_ptr<HeffPlan> DevDMRG::plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
                                             const Index& phys, const Index& left, const Index& right, uint64_t& key,
                                             bool& resident) {
-    key = plan_structure_key(Lb.idx, Rb.idx, phys, left, right);
+    key = plan_structure_key(Lb, Rb, phys, left, right);
     if (plan_cache_.size() != std::size_t(steps_per_sweep())) plan_cache_.resize(std::size_t(steps_per_sweep()));
     CachedPlan& e = plan_cache_[std::size_t(step)];
     resident = false;
@@ -722,7 +749,8 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         t3_last = t3;
         st.trunc_s += t3 - t2;
         DMPS ket = right_paired_copy(c, mps[site1]);
-        left_[site2] = boundary_step_left(c, *left_[site1], ket, mps[site1], mpo[site1], true);
+        left_[site2] = boundary_step_left(c, *left_[site1], ket, mps[site1], mpo[site1], true, bstep_cache_for(_site));
+        bstep_cache_done(_site);
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_left_[o][site2] = ortho_left_step(c, mps[site1], ortho_rp[o][site1], ortho_left_[o][site1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
@@ -737,7 +765,8 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         const double t3 = now_s();
         t3_last = t3;
         st.trunc_s += t3 - t2;
-        right_[site2] = boundary_step_right(c, *right_[site2 + 1], mps[site2], mpo[site2], true);
+        right_[site2] = boundary_step_right(c, *right_[site2 + 1], mps[site2], mpo[site2], true, bstep_cache_for(_site));
+        bstep_cache_done(_site);
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_right_[o][site2] = ortho_right_step(c, mps[site2], ortho_lp[o][site2], ortho_right_[o][site2 + 1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
@@ -788,7 +817,8 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
         const double t3 = now_s();
         st.trunc_s += t3 - t2;
         DMPS ket = right_paired_copy(c, mps[site]);
-        left_[site + 1] = boundary_step_left(c, *left_[site], ket, mps[site], mpo[site], true);
+        left_[site + 1] = boundary_step_left(c, *left_[site], ket, mps[site], mpo[site], true, bstep_cache_for(_site));
+        bstep_cache_done(_site);
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_left_[o][site + 1] = ortho_left_step(c, mps[site], ortho_rp[o][site], ortho_left_[o][site]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
@@ -800,7 +830,8 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
         QCM_CUDA(cudaStreamSynchronize(c.s));
         const double t3 = now_s();
         st.trunc_s += t3 - t2;
-        right_[site] = boundary_step_right(c, *right_[site + 1], mps[site], mpo[site], true);
+        right_[site] = boundary_step_right(c, *right_[site + 1], mps[site], mpo[site], true, bstep_cache_for(_site));
+        bstep_cache_done(_site);
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_right_[o][site] = ortho_right_step(c, mps[site], ortho_lp[o][site], ortho_right_[o][site + 1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));

@@ -56,7 +56,7 @@ class DMRGStats(ctypes.Structure):
     _fields_ = [("hpsi_count", c_uint64), ("hpsi_flops", c_double), ("plan_s", c_double), ("jd_s", c_double),
                 ("trunc_s", c_double), ("boundary_s", c_double), ("total_s", c_double),
                 ("hpsi_count_fp64", c_uint64), ("hpsi_flops_fp64", c_double), ("plans_built", c_uint64),
-                ("plans_reused", c_uint64)]
+                ("plans_reused", c_uint64), ("bsteps_built", c_uint64), ("bsteps_reused", c_uint64)]
 
 
 _lib._sig("qcm_jd_solve", c_int, c_void_p, P(c_double), c_double, c_int, P(c_double), P(c_double), P(c_int))

@@ -249,6 +249,8 @@ def test_plan_cache_reuses_converged_steps(gpu_ctx):
         E, _ = dev.sweep()
         st1 = dev.stats()
         assert np.abs(E - E_ref).max() < E_TOL, (s, E - E_ref)
-        reused.append(st1["plans_reused"] - st0["plans_reused"])
+        reused.append((st1["plans_reused"] - st0["plans_reused"], st1["bsteps_reused"] - st0["bsteps_reused"]))
         assert st1["plans_reused"] + st1["plans_built"] == (s + 1) * (2 * L - 2)
-    assert reused[0] == 0 and reused[-1] == 2 * L - 2, reused
+        assert st1["bsteps_reused"] + st1["bsteps_built"] == (s + 1) * (2 * L - 2)
+    # the boundary steps' schedules are cached with the plans: both are reused once the sectors settle
+    assert reused[0] == (0, 0) and reused[-1] == (2 * L - 2, 2 * L - 2), reused
