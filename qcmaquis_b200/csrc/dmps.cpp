@@ -545,51 +545,50 @@ BlockHeev heev_truncate(Ctx& c, DBlocks& dm, uint64_t Mmax, double cutoff) {
     const std::size_t nb = dm.n();
     for (std::size_t k = 0; k < nb; ++k)
         if (dm.rows[k] != dm.cols[k]) throw std::runtime_error("heev_truncate: density-matrix block is not square");
-    // Every block in one launch of the one-sided Jacobi SVD: a density-matrix block (the reduced density
-    // matrix plus alpha S S^T) is symmetric positive semi-definite, so its singular values are its
-    // eigenvalues and its right singular vectors -- the accumulated rotations, orthonormal and complete
-    // on the null space too -- its eigenvectors.
-    std::vector<uint64_t> wo(nb), uo(nb), vo(nb);
-    uint64_t wl = 0, ul = 0, vl = 0, jl = 0;
-    std::vector<SvdJob> sj;
-    for (std::size_t k = 0; k < nb; ++k) {
-        const uint32_t n = dm.rows[k];
-        wo[k] = wl; wl += n;
-        uo[k] = ul; ul += (uint64_t(n) * n + 31) / 32 * 32;
-        vo[k] = vl; vl += (uint64_t(n) * n + 31) / 32 * 32;
-        if (!n) continue;
-        sj.push_back(SvdJob{dm.off[k], uo[k], wo[k], vo[k], jl, n, n, uint32_t(k), 0});
-        jl += jacobi_svd_scratch(n, n);
-    }
-    DBuf<double> Ub(std::max<uint64_t>(ul, 1)), Sb(std::max<uint64_t>(wl, 1)), Vb(std::max<uint64_t>(vl, 1)),
-        Wj(std::max<uint64_t>(jl, 1));
-    DBuf<int> zc(std::max<std::size_t>(nb, 1));
+    if (!c.sv) c.sv = std::make_unique<Solver>();
+    // heev per block (lanes, one host thread each), eigenvalues ascending on the device
+    std::vector<uint64_t> wo(nb);
+    uint64_t wl = 0;
+    for (std::size_t k = 0; k < nb; ++k) { wo[k] = wl; wl += dm.rows[k]; }
+    DBuf<double> Wv(std::max<uint64_t>(wl, 1));
+    int* info = c.sv->reserve_info(uint32_t(nb), c.s);
+    std::vector<std::size_t> order(nb);
+    for (std::size_t k = 0; k < nb; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](std::size_t x, std::size_t y) { return dm.rows[x] > dm.rows[y]; });
     double t_heev = 0.0;
     static const bool stats = std::getenv("QCM_SVD_STATS") != nullptr;
     if (stats) {
         QCM_CUDA(cudaStreamSynchronize(c.s));
         t_heev = now_ms();
     }
-    batched_jacobi_svd(sj, dm.d.get(), dm.total, Ub.get(), std::max<uint64_t>(ul, 1), Sb.get(), std::max<uint64_t>(wl, 1),
-                       Vb.get(), std::max<uint64_t>(vl, 1), Wj.get(), std::max<uint64_t>(jl, 1), zc.get(), c.sjobs, c.s, nullptr);
-    // eigenvectors back into dm in ascending eigenvalue order (the SVD's descending order reversed)
-    std::vector<CopyJob> cj;
-    for (std::size_t k = 0; k < nb; ++k)
-        if (dm.rows[k]) cj.push_back(CopyJob{vo[k], dm.off[k], dm.rows[k], dm.rows[k], dm.rows[k], dm.rows[k], 0, 1});
-    if (!cj.empty()) batched_copy(cj, Vb.get(), std::max<uint64_t>(vl, 1), dm.d.get(), dm.total, c.cjobs, c.s);
-    std::vector<double> hs(wl);
-    if (wl) QCM_CUDA(cudaMemcpyAsync(hs.data(), Sb.get(), wl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
-    QCM_CUDA(cudaStreamSynchronize(c.s));
+    c.sv->fork(c.s);
+    std::string err;
+#pragma omp parallel for num_threads(Solver::LANES) schedule(static, 1)
+    for (int lane = 0; lane < Solver::LANES; ++lane) {
+        try {
+            QCM_CUDA(cudaSetDevice(c.device));
+            for (std::size_t i = std::size_t(lane); i < nb; i += Solver::LANES) {
+                const std::size_t k = order[i];
+                syevd_lane(*c.sv, lane, dm.d.get() + dm.off[k], int(dm.rows[k]), Wv.get() + wo[k], info + k);
+            }
+        } catch (const std::exception& e) {
+#pragma omp critical
+            err = e.what();
+        }
+    }
+    if (!err.empty()) throw std::runtime_error(err);
+    c.sv->join(c.s);
+    c.sv->check(c.s);
     if (stats) {
+        QCM_CUDA(cudaStreamSynchronize(c.s));
         uint32_t mn = 0;
         uint64_t n3 = 0;
         for (std::size_t k = 0; k < nb; ++k) { mn = std::max(mn, dm.rows[k]); n3 += uint64_t(dm.rows[k]) * dm.rows[k] * dm.rows[k]; }
         std::fprintf(stderr, "[heev] %zu blocks (max %u, sum n^3 %.3g): %.3f ms\n", nb, mn, double(n3), now_ms() - t_heev);
     }
-    // ascending eigenvalues per block, as the eigenvectors
     std::vector<double> hw(wl);
-    for (std::size_t k = 0; k < nb; ++k)
-        for (uint32_t i = 0; i < dm.rows[k]; ++i) hw[wo[k] + i] = hs[wo[k] + dm.rows[k] - 1 - i];
+    if (wl) QCM_CUDA(cudaMemcpyAsync(hw.data(), Wv.get(), wl * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+    QCM_CUDA(cudaStreamSynchronize(c.s));
     // descending order; the cut is on sqrt of the positive eigenvalues (others kept as they are)
     std::vector<std::vector<double>> vals(nb);
     for (std::size_t k = 0; k < nb; ++k) {

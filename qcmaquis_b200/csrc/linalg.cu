@@ -139,11 +139,9 @@ __device__ __forceinline__ double half_sum(double v) {
 __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ jobs, const double* __restrict__ A,
                                                      double* __restrict__ U, double* __restrict__ S, double* __restrict__ V,
                                                      double* __restrict__ Wg, uint32_t smem_doubles,
-                                                     int* __restrict__ zero_count, int* __restrict__ sweeps_used,
-                                                     int deflate) {
+                                                     int* __restrict__ zero_count, int* __restrict__ sweeps_used) {
     extern __shared__ double smem[];
     __shared__ int rotated;
-    __shared__ double thr2;
     __shared__ uint32_t rank_of[1024];
     __shared__ double nrm[1024];
     const SvdJob J = jobs[blockIdx.x];
@@ -165,19 +163,6 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         G[i] = tall ? a[row + uint64_t(col) * J.m] : a[col + uint64_t(row) * J.m];
     }
     for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
-    {
-        // the negligible-column level (64 eps |A|_F)^2; rotations keep |A|_F
-        double f = 0.0;
-        for (uint64_t i = tid; i < uint64_t(r) * c; i += JTHR) f = fma(a[i], a[i], f);
-        f = warp_sum(f);
-        if (lane == 0) nrm[warp] = f;
-        __syncthreads();
-        if (tid == 0) {
-            double t = 0.0;
-            for (int w = 0; w < nwarp; ++w) t += nrm[w];
-            thr2 = deflate ? (64.0 * JEPS) * (64.0 * JEPS) * t : 0.0;
-        }
-    }
     __syncthreads();
     const uint32_t cp = c + (c & 1u);  // players, padded to even
     const double tol2 = (JEPS * double(r)) * (JEPS * double(r));
@@ -185,17 +170,10 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
     for (int sweep = 0; sweep < JMAX_SWEEPS && c > 1; ++sweep) {
         if (tid == 0) rotated = 0;
         for (uint32_t j = warp; j < c; j += nwarp) {
-            double* g = G + uint64_t(j) * r;
+            const double* g = G + uint64_t(j) * r;
             double x = 0.0;
             for (uint32_t i = lane; i < r; i += 32) x = fma(g[i], g[i], x);
             x = warp_sum(x);
-            // a column at the rounding level of A is set to exactly zero and takes no further
-            // rotation (gamma = 0): rotating rounding noise against the other columns would only
-            // feed it back into them
-            if (x <= thr2 && x > 0.0) {
-                for (uint32_t i = lane; i < r; i += 32) g[i] = 0.0;
-                x = 0.0;
-            }
             if (lane == 0) nrm[j] = x;
         }
         __syncthreads();
@@ -296,6 +274,16 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
 }
 }  // namespace
 
+void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info) {
+    if (n == 0) return;
+    Solver::Lane& L = sv.lane[l];
+    AllocStream scope(L.s);
+    int lwork = 0;
+    QCM_SOLVER(cusolverDnDsyevd_bufferSize(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, W, &lwork));
+    if (L.work.size() < std::size_t(lwork)) L.work.alloc(std::size_t(lwork));
+    QCM_SOLVER(cusolverDnDsyevd(L.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, A, n, W, L.work.get(), lwork, info));
+}
+
 uint64_t jacobi_svd_smem_doubles() { return JSMEM_DOUBLES; }
 
 uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n) {
@@ -329,11 +317,10 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
     jobbuf.upload(all, s);
     // one launch: each CTA places its work matrix and rotations by its own size (one CTA per SM
     // in either case, at 1024 threads)
-    static const int deflate = std::getenv("QCM_JACOBI_DEFLATE") ? 1 : 0;
     const std::size_t bytes = std::size_t(JSMEM_DOUBLES) * sizeof(double);
     QCM_CUDA(cudaFuncSetAttribute(k_jacobi_svd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
     k_jacobi_svd<<<unsigned(all.size()), JTHR, bytes, s>>>(jobbuf.get(), A, U, S, V, W, JSMEM_DOUBLES, zero_count,
-                                                           sweeps_used, deflate);
+                                                           sweeps_used);
     QCM_CUDA(cudaGetLastError());
 }
 

@@ -1,12 +1,13 @@
 // Dense per-block factorizations on the device, used by the truncation and
-// canonisation steps of the sweep, each a batched kernel of this project (one CTA per block):
-//   thin SVD   (framework/alps/matrix/algorithms.hpp:243-257, gesvd 'S','S'): one-sided Jacobi
-//   symmetric eigendecomposition of a density-matrix block (algorithms.hpp:374-396, heevd): the
-//              same Jacobi, the block being positive semi-definite
+// canonisation steps of the sweep:
+//   thin SVD   (framework/alps/matrix/algorithms.hpp:243-257, gesvd 'S','S'): one-sided Jacobi,
+//              all blocks in one launch (cuSOLVER gesvdj completes a block whose kept singular
+//              values include exact zeros)
 //   thin QR    (algorithms.hpp:260-291, geqrf + orgqr) and thin LQ (algorithms.hpp:293-325, gelqf
-//              + orglq, here QR of the transpose): Householder
-// plus the Rayleigh-Ritz eigenproblem of the Jacobi-Davidson solver (host, <= 64 x 64).  cuSOLVER's
-// gesvdj remains only as the completion of a block whose kept singular values include exact zeros.
+//              + orglq, here QR of the transpose): Householder, all blocks in one launch
+//   symmetric eigendecomposition of the density-matrix blocks (algorithms.hpp:374-396, heevd):
+//              cuSOLVER syevd on side lanes
+// plus the Rayleigh-Ritz eigenproblem of the Jacobi-Davidson solver (host, <= 64 x 64).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -24,8 +25,8 @@ struct Solver {
     gesvdjInfo_t svdp = nullptr;
     DBuf<int> info;  // one status word per factorization since the last check
     uint32_t n_info = 0;
-    // a side stream for the per-block completions (fork from / join to a stream)
-    static constexpr int LANES = 1;
+    // side streams for independent per-block factorizations (fork from / join to a stream)
+    static constexpr int LANES = 8;
     struct Lane {
         cudaStream_t s = nullptr;
         cusolverDnHandle_t h = nullptr;
@@ -67,6 +68,10 @@ struct SvdJob {
 uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n);
 // doubles of the Jacobi kernel's shared-memory work space (blocks larger than it work in L2)
 uint64_t jacobi_svd_smem_doubles();
+// Symmetric eigendecomposition (divide and conquer, lower triangle) on lane `l`: A (n x n, ld n)
+// is overwritten by the eigenvectors, W receives the eigenvalues in ascending order.
+// Replaces heevd('V') of alps/matrix/algorithms.hpp:374-396 (which then reverses the order).
+void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info);
 // A, U, S, V, W: base pointers of the offsets in jobs (host list, validated against the lengths)
 void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
                         uint64_t s_len, double* V, uint64_t v_len, double* W, uint64_t w_len, int* zero_count,
