@@ -396,6 +396,65 @@ void DTwoSite::twin_to_both(Ctx& c) {
     batched_copy(cj, twin.b.d.get(), twin.b.total, both.d.get(), both.total, c.cjobs, c.s);
 }
 
+namespace {
+
+uint64_t round32(uint64_t n) { return (n + 31) / 32 * 32; }
+
+// Thin SVDs of the blocks of `both` into r.U, r.S, r.V (the BlockSVD layout), by the preconditioned
+// one-sided Jacobi method (Drmac and Veselic, SIAM J. Matrix Anal. Appl. 29, 2008): F = A (rows >= cols)
+// or A^T, a Householder QR with column pivoting F P = Q R, the one-sided Jacobi SVD of X = R^T
+// (k x k, k = min(rows, cols)), X = Ux S Vx^T; then F = (Q Vx) S (P Ux)^T.  The pivoted R's rows are
+// graded, so the Jacobi sweeps converge in a few sweeps over k-long columns.  F's left factor is one
+// GEMM per block, its right factor the rows of Ux scattered by the permutation.  Zero singular values
+// leave zero columns in the scattered factor (V for rows >= cols, U otherwise).
+void preconditioned_svd(Ctx& c, const DBlocks& both, BlockSVD& r, int* zero_count, int* sweeps) {
+    const std::size_t nb = both.n();
+    std::vector<QrJob> qj;
+    std::vector<SvdJob> sj;
+    std::vector<GemmJob> gu, gv;
+    std::vector<PermJob> pu, pv;
+    uint64_t ql = 0, xl = 0, pl = 0, wq = 0, wj = 0;
+    for (std::size_t k = 0; k < nb; ++k) {
+        const uint32_t kk = r.kk[k], m = both.rows[k], n = both.cols[k];
+        if (!kk) continue;
+        const bool tall = m >= n;
+        const uint64_t qo = ql, xo = xl, po = pl;
+        ql += round32(uint64_t(m) * n);  // Q: m x k (QR of A) or k x n (LQ of A)
+        xl += round32(uint64_t(kk) * kk);  // X, Ux and Vx at the same offsets of three buffers
+        pl += kk;
+        qj.push_back(QrJob{both.off[k], qo, xo, wq, m, n, tall ? 0u : 1u, QR_PIVOT | (tall ? QR_RT : 0u), po});
+        wq += qr_scratch(m, n, !tall);
+        sj.push_back(SvdJob{xo, xo, r.so[k], xo, wj, kk, kk, uint32_t(k), 0});
+        wj += jacobi_svd_scratch(kk, kk);
+        GemmJob g{};
+        g.alpha = 1.0; g.beta = 0.0;
+        g.b_off = xo; g.ldb = kk; g.tb = 0; g.N = kk; g.K = kk;
+        if (tall) {
+            // U (m x k) = Q (m x k) Vx; V = P Ux
+            g.a_off = qo; g.lda = m; g.ta = 0; g.c_off = r.uo[k]; g.ldc = m; g.M = m;
+            gu.push_back(g);
+            pv.push_back(PermJob{xo, r.vo[k], po, kk, n});
+        } else {
+            // V (n x k) = (Q (k x n))^T Vx; U = P Ux
+            g.a_off = qo; g.lda = kk; g.ta = 1; g.c_off = r.vo[k]; g.ldc = n; g.M = n;
+            gv.push_back(g);
+            pu.push_back(PermJob{xo, r.uo[k], po, kk, m});
+        }
+    }
+    if (qj.empty()) return;
+    DBuf<double> Qb(ql), Xb(xl), Uxb(xl), Vxb(xl), Wq(wq), Wjb(wj);
+    DBuf<uint32_t> Pb(pl);
+    batched_qr(qj, both.d.get(), both.total, Qb.get(), ql, Xb.get(), xl, Wq.get(), wq, c.qjobs, c.s, Pb.get(), pl);
+    batched_jacobi_svd(sj, Xb.get(), xl, Uxb.get(), xl, r.S.get(), r.s_len, Vxb.get(), xl, Wjb.get(), wj, zero_count, c.sjobs,
+                       c.s, sweeps);
+    if (!gu.empty()) batched_gemm(gu, Qb.get(), ql, Vxb.get(), xl, r.U.get(), r.u_len, c.gjobs, c.gtiles, c.s);
+    if (!gv.empty()) batched_gemm(gv, Qb.get(), ql, Vxb.get(), xl, r.V.get(), r.v_len, c.gjobs, c.gtiles, c.s);
+    batched_permute_rows(pv, Uxb.get(), xl, r.V.get(), r.v_len, Pb.get(), pl, c.pjobs, c.s);
+    batched_permute_rows(pu, Uxb.get(), xl, r.U.get(), r.u_len, Pb.get(), pl, c.pjobs, c.s);
+}
+
+}  // namespace
+
 BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff) {
     const std::size_t nb = both.n();
     BlockSVD r;
@@ -409,15 +468,7 @@ BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff)
     }
     r.u_len = std::max<uint64_t>(ul, 1); r.s_len = std::max<uint64_t>(sl, 1); r.v_len = std::max<uint64_t>(vl, 1);
     r.U.alloc(r.u_len); r.S.alloc(r.s_len); r.V.alloc(r.v_len);
-    // all block SVDs in one launch (one-sided Jacobi, one CTA per block)
-    std::vector<SvdJob> sj;
-    uint64_t wl = 0;
-    for (std::size_t k = 0; k < nb; ++k) {
-        if (!r.kk[k]) continue;
-        sj.push_back(SvdJob{both.off[k], r.uo[k], r.so[k], r.vo[k], wl, both.rows[k], both.cols[k], uint32_t(k), 0});
-        wl += jacobi_svd_scratch(both.rows[k], both.cols[k]);
-    }
-    DBuf<double> Wj(std::max<uint64_t>(wl, 1));
+    // all blocks at once: pivoted QR, one-sided Jacobi on R^T, assembly (preconditioned_svd)
     DBuf<int> zc(std::max<std::size_t>(nb, 1));
     // QCM_SVD_STATS=1 prints the kernel time and the Jacobi sweeps of every batch
     static const bool stats = std::getenv("QCM_SVD_STATS") != nullptr;
@@ -430,8 +481,7 @@ BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff)
         QCM_CUDA(cudaEventCreate(&e1));
         QCM_CUDA(cudaEventRecord(e0, c.s));
     }
-    batched_jacobi_svd(sj, both.d.get(), both.total, r.U.get(), r.u_len, r.S.get(), r.s_len, r.V.get(), r.v_len, Wj.get(),
-                       std::max<uint64_t>(wl, 1), zc.get(), c.sjobs, c.s, stats ? swp.get() : nullptr);
+    preconditioned_svd(c, both, r, zc.get(), stats ? swp.get() : nullptr);
     if (stats) {
         QCM_CUDA(cudaEventRecord(e1, c.s));
         QCM_CUDA(cudaEventSynchronize(e1));
@@ -446,11 +496,12 @@ BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff)
         for (std::size_t k = 0; k < nb; ++k) {
             mr = std::max(mr, both.rows[k]);
             mc = std::max(mc, both.cols[k]);
-            const uint64_t rr = std::max(both.rows[k], both.cols[k]), cc = std::min(both.rows[k], both.cols[k]);
-            if (rr * cc > uint64_t(both.rows[kbig]) * both.cols[kbig]) kbig = k;
-            modes[rr * cc + cc * cc <= jacobi_svd_smem_doubles() ? 0 : (rr * cc <= jacobi_svd_smem_doubles() ? 1 : 2)]++;
+            // the Jacobi runs on the k x k factor R^T
+            const uint64_t cc = std::min(both.rows[k], both.cols[k]);
+            if (uint64_t(both.rows[k]) * both.cols[k] > uint64_t(both.rows[kbig]) * both.cols[kbig]) kbig = k;
+            modes[2 * cc * cc <= jacobi_svd_smem_doubles() ? 0 : (cc * cc <= jacobi_svd_smem_doubles() ? 1 : 2)]++;
         }
-        std::fprintf(stderr, "[svd] %zu blocks (max %u x %u): %.3f ms, sweeps max %d; largest %u x %u: %d sweeps; modes %d/%d/%d\n",
+        std::fprintf(stderr, "[svd] %zu blocks (max %u x %u): %.3f ms, Jacobi sweeps max %d; largest %u x %u: %d sweeps; modes %d/%d/%d\n",
                      nb, mr, mc, ms, hsw.empty() ? 0 : *std::max_element(hsw.begin(), hsw.end()), both.rows[kbig],
                      both.cols[kbig], nb ? hsw[kbig] : 0, modes[0], modes[1], modes[2]);
         cudaEventDestroy(e0);

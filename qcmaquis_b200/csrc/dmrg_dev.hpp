@@ -107,6 +107,7 @@ struct Ctx {
     DBuf<CopyJob> cjobs;
     DBuf<SvdJob> sjobs;
     DBuf<QrJob> qjobs;
+    DBuf<PermJob> pjobs;
     DBuf<double> qrw;  // QR / LQ scratch
     DBuf<TJobD> tjobs;
     DBuf<TileD> ttiles[N_SHAPES];

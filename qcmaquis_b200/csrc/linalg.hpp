@@ -80,13 +80,28 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
 //   lq = 0: A_j (m x n, ld m) = Q_j R_j, Q_j (m x k, ld m), R_j (k x n, ld k);
 //   lq = 1: A_j = L_j Q_j, L_j (m x k, ld m) at r_off, Q_j (k x n, ld k) at q_off;
 // k = min(m, n); W: scratch of qr_scratch(m, n, lq) doubles per block at w_off.
+// flags QR_PIVOT: column pivoting of the factorised matrix F (A, or A^T for an LQ): F P = Q' R' with
+//   the column of largest remaining norm taken at every step (ties: the lowest index); perm (at p_off,
+//   min(m, n) = the columns of F, which must then be at most 1024) receives column i of F P as perm[i].
+// flags QR_RT (lq = 0): R is written transposed, R^T (n x k, ld n).
+constexpr uint32_t QR_PIVOT = 1, QR_RT = 2;
+// dst[dst_off + perm[p_off + i] + j * ldd] = src[src_off + i + j * n] for i, j < n (rows of an n x n
+// block scattered by a permutation), one CTA per job
+struct PermJob {
+    uint64_t src_off, dst_off, p_off;
+    uint32_t n, ldd;
+};
+void batched_permute_rows(const std::vector<PermJob>& jobs, const double* src, uint64_t src_len, double* dst, uint64_t dst_len,
+                          const uint32_t* perm, uint64_t p_len, DBuf<PermJob>& jobbuf, cudaStream_t s);
 struct QrJob {
     uint64_t a_off, q_off, r_off, w_off;
-    uint32_t m, n, lq, pad;
+    uint32_t m, n, lq, flags;
+    uint64_t p_off;
 };
 uint64_t qr_scratch(uint32_t m, uint32_t n, bool lq);
 void batched_qr(const std::vector<QrJob>& jobs, const double* A, uint64_t a_len, double* Q, uint64_t q_len, double* R,
-                uint64_t r_len, double* W, uint64_t w_len, DBuf<QrJob>& jobbuf, cudaStream_t s);
+                uint64_t r_len, double* W, uint64_t w_len, DBuf<QrJob>& jobbuf, cudaStream_t s, uint32_t* P = nullptr,
+                uint64_t p_len = 0);
 
 // Lowest eigenpair of the symmetric n x n matrix held in the upper triangle of
 // M (column-major, leading dimension ldm); cyclic Jacobi rotations, FP64.
