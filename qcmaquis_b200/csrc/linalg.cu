@@ -130,6 +130,12 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// placement of the work matrix (r x c) and the rotations (c x c): 0 both in shared memory, 1 the work
+// matrix there and the rotations logged (then replayed in shared memory), 2 both in global scratch
+__host__ __device__ __forceinline__ int jacobi_mode(uint32_t r, uint32_t c, uint64_t smem_doubles) {
+    const uint64_t rc = uint64_t(r) * c, cc = uint64_t(c) * c;
+    return rc + cc <= smem_doubles ? 0 : (rc <= smem_doubles ? 1 : 2);
+}
 // sum over the 16 lanes of each half-warp (all 32 lanes call it)
 __device__ __forceinline__ double half_sum(double v) {
     for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -141,19 +147,23 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                                                      double* __restrict__ Wg, uint32_t smem_doubles,
                                                      int* __restrict__ zero_count, int* __restrict__ sweeps_used) {
     extern __shared__ double smem[];
-    __shared__ int rotated;
+    __shared__ int rotated, sweeps_done;
     __shared__ uint32_t rank_of[1024];
     __shared__ double nrm[1024];
     const SvdJob J = jobs[blockIdx.x];
     const bool tall = J.m >= J.n;
     const uint32_t r = tall ? J.m : J.n, c = tall ? J.n : J.m;
-    // work matrix G (r x c) and rotations Q (c x c): both in the launch's shared memory when they fit,
-    // else G there and Q in the block's global scratch (L2-resident), else both in the scratch
+    const uint32_t cp = c + (c & 1u);  // players, padded to even
+    // work matrix G (r x c) and rotations Q (c x c): both in the launch's shared memory when they fit;
+    // else G there, every round's rotations logged to the block's global scratch and Q built from the
+    // log in shared memory once G is done; else both in the scratch (L2-resident)
+    const int mode = jacobi_mode(r, c, smem_doubles);
     const uint64_t rc = uint64_t(r) * c;
     double* G;
-    double* Q;
-    if (rc + uint64_t(c) * c <= smem_doubles) { G = smem; Q = smem + rc; }
-    else if (rc <= smem_doubles) { G = smem; Q = Wg + J.w_off + rc; }
+    double* Q = nullptr;
+    double2* rlog = nullptr;  // mode 1: (cos, sin) per (round, pair), (1, 0) for no rotation
+    if (mode == 0) { G = smem; Q = smem + rc; }
+    else if (mode == 1) { G = smem; rlog = reinterpret_cast<double2*>(Wg + J.w_off); }
     else { G = Wg + J.w_off; Q = G + rc; }
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = JTHR / 32;
     // G = A or A^T, Q = I
@@ -162,9 +172,10 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         const uint32_t row = uint32_t(i % r), col = uint32_t(i / r);
         G[i] = tall ? a[row + uint64_t(col) * J.m] : a[col + uint64_t(row) * J.m];
     }
-    for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
+    if (Q)
+        for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
+    if (tid == 0) sweeps_done = 0;
     __syncthreads();
-    const uint32_t cp = c + (c & 1u);  // players, padded to even
     const double tol2 = (JEPS * double(r)) * (JEPS * double(r));
     const uint32_t grp = uint32_t(tid) >> 4, hl = uint32_t(tid) & 15u, ngrp = JTHR / 16;
     for (int sweep = 0; sweep < JMAX_SWEEPS && c > 1; ++sweep) {
@@ -198,6 +209,8 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                 ga = half_sum(ga);
                 const double al = act ? nrm[p] : 0.0, be = act ? nrm[q] : 0.0;
                 const bool rot = act && ga * ga > tol2 * (al * be);
+                if (rlog && act && !rot && hl == 0)
+                    rlog[(uint64_t(sweep) * (cp - 1) + k) * (cp / 2) + t] = make_double2(1.0, 0.0);
                 if (rot) {
                     const double zeta = (be - al) / (2.0 * ga);
                     const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
@@ -207,12 +220,16 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                         gp[i] = cs * x - sn * y;
                         gq[i] = sn * x + cs * y;
                     }
-                    double* qp = Q + uint64_t(p) * c;
-                    double* qq = Q + uint64_t(q) * c;
-                    for (uint32_t i = hl; i < c; i += 16) {
-                        const double x = qp[i], y = qq[i];
-                        qp[i] = cs * x - sn * y;
-                        qq[i] = sn * x + cs * y;
+                    if (Q) {
+                        double* qp = Q + uint64_t(p) * c;
+                        double* qq = Q + uint64_t(q) * c;
+                        for (uint32_t i = hl; i < c; i += 16) {
+                            const double x = qp[i], y = qq[i];
+                            qp[i] = cs * x - sn * y;
+                            qq[i] = sn * x + cs * y;
+                        }
+                    } else if (hl == 0) {
+                        rlog[(uint64_t(sweep) * (cp - 1) + k) * (cp / 2) + t] = make_double2(cs, sn);
                     }
                     if (hl == 0) {
                         nrm[p] = al - tt * ga;
@@ -226,6 +243,7 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         }
         const int any = rotated;
         __syncthreads();
+        if (tid == 0) sweeps_done = sweep + 1;
         if (sweeps_used && tid == 0) sweeps_used[J.id] = sweep + 1;
         if (!any) break;
     }
@@ -257,18 +275,47 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         const double sg = sv[col];
         Gout[row + uint64_t(rank_of[col]) * r] = sg > 0.0 ? G[i] / sg : 0.0;
     }
+    if (mode == 1) {
+        // Q = the logged rotations applied to I, in shared memory (G is written out): thread (row i,
+        // group g) applies the rotations of pairs t = g, g + ng, ... of each round to row i of Q; the
+        // pairs of a round are disjoint, the rounds follow each other
+        __syncthreads();
+        Q = smem;
+        for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
+        __syncthreads();
+        const uint32_t ng = JTHR / c, row = uint32_t(tid) % c, g = uint32_t(tid) / c;
+        const bool part = g < ng;
+        const uint64_t rounds = uint64_t(sweeps_done) * (cp - 1);
+        for (uint64_t rr = 0; rr < rounds; ++rr) {
+            if (part) {
+                const uint32_t k = uint32_t(rr % (cp - 1));
+                for (uint32_t t = g; t < cp / 2; t += ng) {
+                    const uint32_t i0 = t, i1 = cp - 1 - t;
+                    const uint32_t p = i0 == 0 ? 0 : (i0 - 1 + k) % (cp - 1) + 1;
+                    const uint32_t q = i1 == 0 ? 0 : (i1 - 1 + k) % (cp - 1) + 1;
+                    if (p >= c || q >= c) continue;
+                    const double2 cs = rlog[rr * (cp / 2) + t];
+                    if (cs.y == 0.0) continue;
+                    const double x = Q[row + uint64_t(p) * c], y = Q[row + uint64_t(q) * c];
+                    Q[row + uint64_t(p) * c] = cs.x * x - cs.y * y;
+                    Q[row + uint64_t(q) * c] = cs.y * x + cs.x * y;
+                }
+            }
+            __syncthreads();
+        }
+    }
     for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) {
         const uint32_t row = uint32_t(i % c), col = uint32_t(i / c);
         Qout[row + uint64_t(rank_of[col]) * c] = Q[i];
     }
     __syncthreads();
-    // sigma in sorted order (through the scratch column space, G is no longer needed)
-    for (uint32_t j = tid; j < c; j += JTHR) G[rank_of[j]] = sv[j];
+    // sigma in sorted order (through nrm, free after the sweeps)
+    for (uint32_t j = tid; j < c; j += JTHR) nrm[rank_of[j]] = sv[j];
     __syncthreads();
     int zeros = 0;
     for (uint32_t j = tid; j < c; j += JTHR) {
-        sv[j] = G[j];
-        zeros += G[j] == 0.0 ? 1 : 0;
+        sv[j] = nrm[j];
+        zeros += nrm[j] == 0.0 ? 1 : 0;
     }
     if (zeros) atomicAdd(zero_count + J.id, zeros);
 }
@@ -287,8 +334,14 @@ void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info) {
 uint64_t jacobi_svd_smem_doubles() { return JSMEM_DOUBLES; }
 
 uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n) {
-    const uint64_t r = std::max(m, n), c = std::min(m, n);
-    return r * c + c * c;
+    const uint64_t r = std::max(m, n), c = std::min(m, n), cp = c + (c & 1u);
+    uint64_t d = 0;
+    switch (jacobi_mode(uint32_t(r), uint32_t(c), JSMEM_DOUBLES)) {
+    case 0: d = 0; break;
+    case 1: d = uint64_t(JMAX_SWEEPS) * (cp - 1) * (cp / 2) * 2; break;  // the rotation log
+    default: d = r * c + c * c;
+    }
+    return (d + 31) / 32 * 32;  // whole multiples of 32 doubles: consecutive blocks stay 16-byte aligned
 }
 
 void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
@@ -304,6 +357,7 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
         if (j.a_off + uint64_t(j.m) * j.n > a_len || j.u_off + uint64_t(j.m) * k > u_len || j.s_off + k > s_len ||
             j.v_off + uint64_t(j.n) * k > v_len || j.w_off + jacobi_svd_scratch(j.m, j.n) > w_len)
             throw std::runtime_error("batched_jacobi_svd: block outside its buffers");
+        if (j.w_off % 2) throw std::runtime_error("batched_jacobi_svd: scratch offset not 16-byte aligned");
         // the blocks working in global memory first: they take longest
         if (std::max(j.m, j.n) * uint64_t(k) <= JSMEM_DOUBLES) small.push_back(j);
         else large.push_back(j);

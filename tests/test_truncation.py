@@ -116,6 +116,38 @@ def test_device_svd_truncate_matches_oracle(gpu_ctx, case):
             assert np.abs(Vt[j] - sg * Vtr[j]).max() < 1e-8
 
 
+def middle_bond_blocks(seed=1):
+    """44 blocks shaped like the two-site tensor's at the L=24, M=512 middle bond (up to 178 x 114), each with
+    its own exponentially decaying spectrum and scale (no ties across blocks)."""
+    rng = np.random.default_rng(seed)
+    shapes = [(178, 114), (160, 120), (150, 100), (114, 140)] + [(int(rng.integers(20, 140)), int(rng.integers(16, 110)))
+                                                                 for _ in range(40)]
+    blocks = []
+    for (m, n) in shapes:
+        k = min(m, n)
+        U, _ = np.linalg.qr(rng.standard_normal((m, k)))
+        V, _ = np.linalg.qr(rng.standard_normal((n, k)))
+        s = rng.uniform(0.5, 2.0) * np.exp(-np.arange(k) * rng.uniform(0.15, 0.4))
+        blocks.append((U * s) @ V.T)
+    return blocks
+
+
+@pytest.mark.gpu
+def test_device_svd_truncate_middle_bond_blocks(gpu_ctx):
+    """The truncation SVD (pivoted QR, Jacobi on R^T) on blocks of the bench bond's sizes and graded spectra,
+    against the oracle (LAPACK): kept dimensions, singular values, kept singular vectors up to sign."""
+    from qcmaquis_b200.dmrg import truncate_svd
+    blocks = middle_bond_blocks()
+    ref, res_ref = orc_svd(blocks, 512, 1e-16)
+    out, res = truncate_svd(gpu_ctx, blocks, 512, 1e-16)
+    check_svd(out, res, blocks, [o[1].size for o in ref], [o[1] for o in ref], res_ref, 1e-12)
+    for (U, S, Vt), (Ur, Sr, Vtr) in zip(out, ref):
+        for j in range(S.size):
+            sg = np.sign(U[:, j] @ Ur[:, j])
+            assert np.abs(U[:, j] - sg * Ur[:, j]).max() < 1e-8
+            assert np.abs(Vt[j] - sg * Vtr[j]).max() < 1e-8
+
+
 @pytest.mark.gpu
 def test_device_svd_truncate_degenerate(gpu_ctx):
     """Orthogonal blocks (all singular values 1) and a scaled copy: the cut falls in the gap."""
