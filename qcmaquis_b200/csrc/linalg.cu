@@ -212,8 +212,10 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                 if (rlog && act && !rot && hl == 0)
                     rlog[(uint64_t(sweep) * (cp - 1) + k) * (cp / 2) + t] = make_double2(1.0, 0.0);
                 if (rot) {
-                    const double zeta = (be - al) / (2.0 * ga);
-                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)) with zeta = d / h, d = beta - alpha,
+                    // h = 2 gamma, multiplied through by |h|: one hypot and one division
+                    const double d = be - al, h = 2.0 * ga;
+                    const double tt = (d >= 0.0 ? h : -h) / (fabs(d) + hypot(d, h));
                     const double cs = rsqrt(1.0 + tt * tt), sn = cs * tt;
                     for (uint32_t i = hl; i < r; i += 16) {
                         const double x = gp[i], y = gq[i];
