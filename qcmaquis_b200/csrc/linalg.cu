@@ -130,15 +130,9 @@ __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
-// placement of the work matrix (r x c) and the rotations (c x c): 0 both in shared memory, 1 the work
-// matrix there and the rotations logged (then replayed in shared memory), 2 both in global scratch
-__host__ __device__ __forceinline__ int jacobi_mode(uint32_t r, uint32_t c, uint64_t smem_doubles) {
-    const uint64_t rc = uint64_t(r) * c, cc = uint64_t(c) * c;
-    return rc + cc <= smem_doubles ? 0 : (rc <= smem_doubles ? 1 : 2);
-}
-// sum over the 16 lanes of each half-warp (all 32 lanes call it)
-__device__ __forceinline__ double half_sum(double v) {
-    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+// sum over each aligned group of gs lanes (gs = 8 or 16; all 32 lanes call it)
+__device__ __forceinline__ double group_sum(double v, uint32_t gs) {
+    for (uint32_t o = gs >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, int(o));
     return v;
 }
 
@@ -147,23 +141,19 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                                                      double* __restrict__ Wg, uint32_t smem_doubles,
                                                      int* __restrict__ zero_count, int* __restrict__ sweeps_used) {
     extern __shared__ double smem[];
-    __shared__ int rotated, sweeps_done;
+    __shared__ int rotated;
     __shared__ uint32_t rank_of[1024];
     __shared__ double nrm[1024];
     const SvdJob J = jobs[blockIdx.x];
     const bool tall = J.m >= J.n;
     const uint32_t r = tall ? J.m : J.n, c = tall ? J.n : J.m;
-    const uint32_t cp = c + (c & 1u);  // players, padded to even
-    // work matrix G (r x c) and rotations Q (c x c): both in the launch's shared memory when they fit;
-    // else G there, every round's rotations logged to the block's global scratch and Q built from the
-    // log in shared memory once G is done; else both in the scratch (L2-resident)
-    const int mode = jacobi_mode(r, c, smem_doubles);
+    // work matrix G (r x c) and rotations Q (c x c): both in the launch's shared memory when they fit,
+    // else G there and Q in the block's global scratch (L2-resident), else both in the scratch
     const uint64_t rc = uint64_t(r) * c;
     double* G;
-    double* Q = nullptr;
-    double2* rlog = nullptr;  // mode 1: (cos, sin) per (round, pair), (1, 0) for no rotation
-    if (mode == 0) { G = smem; Q = smem + rc; }
-    else if (mode == 1) { G = smem; rlog = reinterpret_cast<double2*>(Wg + J.w_off); }
+    double* Q;
+    if (rc + uint64_t(c) * c <= smem_doubles) { G = smem; Q = smem + rc; }
+    else if (rc <= smem_doubles) { G = smem; Q = Wg + J.w_off + rc; }
     else { G = Wg + J.w_off; Q = G + rc; }
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = JTHR / 32;
     // G = A or A^T, Q = I
@@ -172,12 +162,14 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         const uint32_t row = uint32_t(i % r), col = uint32_t(i / r);
         G[i] = tall ? a[row + uint64_t(col) * J.m] : a[col + uint64_t(row) * J.m];
     }
-    if (Q)
-        for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
-    if (tid == 0) sweeps_done = 0;
+    for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
     __syncthreads();
+    const uint32_t cp = c + (c & 1u);  // players, padded to even
     const double tol2 = (JEPS * double(r)) * (JEPS * double(r));
-    const uint32_t grp = uint32_t(tid) >> 4, hl = uint32_t(tid) & 15u, ngrp = JTHR / 16;
+    // lanes per pair: 16, or 8 when the pairs of a round outnumber the half-warps, so that a round
+    // is one pass of the CTA (its latency chain is the round's cost)
+    const uint32_t gs = cp / 2 > uint32_t(JTHR / 16) ? 8u : 16u;
+    const uint32_t grp = uint32_t(tid) / gs, hl = uint32_t(tid) % gs, ngrp = JTHR / gs;
     for (int sweep = 0; sweep < JMAX_SWEEPS && c > 1; ++sweep) {
         if (tid == 0) rotated = 0;
         for (uint32_t j = warp; j < c; j += nwarp) {
@@ -189,7 +181,7 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         }
         __syncthreads();
         for (uint32_t k = 0; k + 1 < cp; ++k) {
-            // one pair per half-warp; every lane runs the same number of passes so the half-warp
+            // one pair per lane group; every lane runs the same number of passes so the group
             // shuffles never diverge
             for (uint32_t pass = 0; pass * ngrp < cp / 2; ++pass) {
                 const uint32_t t = pass * ngrp + grp;
@@ -205,33 +197,25 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                 double* gq = G + uint64_t(q) * r;
                 double ga = 0.0;
                 if (act)
-                    for (uint32_t i = hl; i < r; i += 16) ga = fma(gp[i], gq[i], ga);
-                ga = half_sum(ga);
+                    for (uint32_t i = hl; i < r; i += gs) ga = fma(gp[i], gq[i], ga);
+                ga = group_sum(ga, gs);
                 const double al = act ? nrm[p] : 0.0, be = act ? nrm[q] : 0.0;
                 const bool rot = act && ga * ga > tol2 * (al * be);
-                if (rlog && act && !rot && hl == 0)
-                    rlog[(uint64_t(sweep) * (cp - 1) + k) * (cp / 2) + t] = make_double2(1.0, 0.0);
                 if (rot) {
-                    // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)) with zeta = d / h, d = beta - alpha,
-                    // h = 2 gamma, multiplied through by |h|: one hypot and one division
-                    const double d = be - al, h = 2.0 * ga;
-                    const double tt = (d >= 0.0 ? h : -h) / (fabs(d) + hypot(d, h));
+                    const double zeta = (be - al) / (2.0 * ga);
+                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                     const double cs = rsqrt(1.0 + tt * tt), sn = cs * tt;
-                    for (uint32_t i = hl; i < r; i += 16) {
+                    for (uint32_t i = hl; i < r; i += gs) {
                         const double x = gp[i], y = gq[i];
                         gp[i] = cs * x - sn * y;
                         gq[i] = sn * x + cs * y;
                     }
-                    if (Q) {
-                        double* qp = Q + uint64_t(p) * c;
-                        double* qq = Q + uint64_t(q) * c;
-                        for (uint32_t i = hl; i < c; i += 16) {
-                            const double x = qp[i], y = qq[i];
-                            qp[i] = cs * x - sn * y;
-                            qq[i] = sn * x + cs * y;
-                        }
-                    } else if (hl == 0) {
-                        rlog[(uint64_t(sweep) * (cp - 1) + k) * (cp / 2) + t] = make_double2(cs, sn);
+                    double* qp = Q + uint64_t(p) * c;
+                    double* qq = Q + uint64_t(q) * c;
+                    for (uint32_t i = hl; i < c; i += gs) {
+                        const double x = qp[i], y = qq[i];
+                        qp[i] = cs * x - sn * y;
+                        qq[i] = sn * x + cs * y;
                     }
                     if (hl == 0) {
                         nrm[p] = al - tt * ga;
@@ -245,7 +229,6 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         }
         const int any = rotated;
         __syncthreads();
-        if (tid == 0) sweeps_done = sweep + 1;
         if (sweeps_used && tid == 0) sweeps_used[J.id] = sweep + 1;
         if (!any) break;
     }
@@ -277,47 +260,18 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
         const double sg = sv[col];
         Gout[row + uint64_t(rank_of[col]) * r] = sg > 0.0 ? G[i] / sg : 0.0;
     }
-    if (mode == 1) {
-        // Q = the logged rotations applied to I, in shared memory (G is written out): thread (row i,
-        // group g) applies the rotations of pairs t = g, g + ng, ... of each round to row i of Q; the
-        // pairs of a round are disjoint, the rounds follow each other
-        __syncthreads();
-        Q = smem;
-        for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
-        __syncthreads();
-        const uint32_t ng = JTHR / c, row = uint32_t(tid) % c, g = uint32_t(tid) / c;
-        const bool part = g < ng;
-        const uint64_t rounds = uint64_t(sweeps_done) * (cp - 1);
-        for (uint64_t rr = 0; rr < rounds; ++rr) {
-            if (part) {
-                const uint32_t k = uint32_t(rr % (cp - 1));
-                for (uint32_t t = g; t < cp / 2; t += ng) {
-                    const uint32_t i0 = t, i1 = cp - 1 - t;
-                    const uint32_t p = i0 == 0 ? 0 : (i0 - 1 + k) % (cp - 1) + 1;
-                    const uint32_t q = i1 == 0 ? 0 : (i1 - 1 + k) % (cp - 1) + 1;
-                    if (p >= c || q >= c) continue;
-                    const double2 cs = rlog[rr * (cp / 2) + t];
-                    if (cs.y == 0.0) continue;
-                    const double x = Q[row + uint64_t(p) * c], y = Q[row + uint64_t(q) * c];
-                    Q[row + uint64_t(p) * c] = cs.x * x - cs.y * y;
-                    Q[row + uint64_t(q) * c] = cs.y * x + cs.x * y;
-                }
-            }
-            __syncthreads();
-        }
-    }
     for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) {
         const uint32_t row = uint32_t(i % c), col = uint32_t(i / c);
         Qout[row + uint64_t(rank_of[col]) * c] = Q[i];
     }
     __syncthreads();
-    // sigma in sorted order (through nrm, free after the sweeps)
-    for (uint32_t j = tid; j < c; j += JTHR) nrm[rank_of[j]] = sv[j];
+    // sigma in sorted order (through the scratch column space, G is no longer needed)
+    for (uint32_t j = tid; j < c; j += JTHR) G[rank_of[j]] = sv[j];
     __syncthreads();
     int zeros = 0;
     for (uint32_t j = tid; j < c; j += JTHR) {
-        sv[j] = nrm[j];
-        zeros += nrm[j] == 0.0 ? 1 : 0;
+        sv[j] = G[j];
+        zeros += G[j] == 0.0 ? 1 : 0;
     }
     if (zeros) atomicAdd(zero_count + J.id, zeros);
 }
@@ -336,14 +290,8 @@ void syevd_lane(Solver& sv, int l, double* A, int n, double* W, int* info) {
 uint64_t jacobi_svd_smem_doubles() { return JSMEM_DOUBLES; }
 
 uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n) {
-    const uint64_t r = std::max(m, n), c = std::min(m, n), cp = c + (c & 1u);
-    uint64_t d = 0;
-    switch (jacobi_mode(uint32_t(r), uint32_t(c), JSMEM_DOUBLES)) {
-    case 0: d = 0; break;
-    case 1: d = uint64_t(JMAX_SWEEPS) * (cp - 1) * (cp / 2) * 2; break;  // the rotation log
-    default: d = r * c + c * c;
-    }
-    return (d + 31) / 32 * 32;  // whole multiples of 32 doubles: consecutive blocks stay 16-byte aligned
+    const uint64_t r = std::max(m, n), c = std::min(m, n);
+    return r * c + c * c;
 }
 
 void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
@@ -359,7 +307,6 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
         if (j.a_off + uint64_t(j.m) * j.n > a_len || j.u_off + uint64_t(j.m) * k > u_len || j.s_off + k > s_len ||
             j.v_off + uint64_t(j.n) * k > v_len || j.w_off + jacobi_svd_scratch(j.m, j.n) > w_len)
             throw std::runtime_error("batched_jacobi_svd: block outside its buffers");
-        if (j.w_off % 2) throw std::runtime_error("batched_jacobi_svd: scratch offset not 16-byte aligned");
         // the blocks working in global memory first: they take longest
         if (std::max(j.m, j.n) * uint64_t(k) <= JSMEM_DOUBLES) small.push_back(j);
         else large.push_back(j);
