@@ -444,13 +444,28 @@ void preconditioned_svd(Ctx& c, const DBlocks& both, BlockSVD& r, int* zero_coun
     if (qj.empty()) return;
     DBuf<double> Qb(ql), Xb(xl), Uxb(xl), Vxb(xl), Wq(wq), Wjb(wj);
     DBuf<uint32_t> Pb(pl);
+    // QCM_SVD_STATS=1: the time of each part
+    cudaEvent_t ev[4] = {};
+    if (sweeps)
+        for (auto& e : ev) QCM_CUDA(cudaEventCreate(&e));
+    if (sweeps) QCM_CUDA(cudaEventRecord(ev[0], c.s));
     batched_qr(qj, both.d.get(), both.total, Qb.get(), ql, Xb.get(), xl, Wq.get(), wq, c.qjobs, c.s, Pb.get(), pl);
+    if (sweeps) QCM_CUDA(cudaEventRecord(ev[1], c.s));
     batched_jacobi_svd(sj, Xb.get(), xl, Uxb.get(), xl, r.S.get(), r.s_len, Vxb.get(), xl, Wjb.get(), wj, zero_count, c.sjobs,
                        c.s, sweeps);
+    if (sweeps) QCM_CUDA(cudaEventRecord(ev[2], c.s));
     if (!gu.empty()) batched_gemm(gu, Qb.get(), ql, Vxb.get(), xl, r.U.get(), r.u_len, c.gjobs, c.gtiles, c.s);
     if (!gv.empty()) batched_gemm(gv, Qb.get(), ql, Vxb.get(), xl, r.V.get(), r.v_len, c.gjobs, c.gtiles, c.s);
     batched_permute_rows(pv, Uxb.get(), xl, r.V.get(), r.v_len, Pb.get(), pl, c.pjobs, c.s);
     batched_permute_rows(pu, Uxb.get(), xl, r.U.get(), r.u_len, Pb.get(), pl, c.pjobs, c.s);
+    if (sweeps) {
+        QCM_CUDA(cudaEventRecord(ev[3], c.s));
+        QCM_CUDA(cudaEventSynchronize(ev[3]));
+        float t[3];
+        for (int i = 0; i < 3; ++i) QCM_CUDA(cudaEventElapsedTime(&t[i], ev[i], ev[i + 1]));
+        std::fprintf(stderr, "[svd parts] qr %.3f ms, jacobi %.3f ms, assembly %.3f ms\n", t[0], t[1], t[2]);
+        for (auto& e : ev) cudaEventDestroy(e);
+    }
 }
 
 }  // namespace
@@ -497,9 +512,9 @@ BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff)
             mr = std::max(mr, both.rows[k]);
             mc = std::max(mc, both.cols[k]);
             // the Jacobi runs on the k x k factor R^T
-            const uint64_t cc = std::min(both.rows[k], both.cols[k]);
+            const uint64_t cc = std::min(both.rows[k], both.cols[k]), cpd = (cc + (cc & 1)) * cc;
             if (uint64_t(both.rows[k]) * both.cols[k] > uint64_t(both.rows[kbig]) * both.cols[kbig]) kbig = k;
-            modes[2 * cc * cc <= jacobi_svd_smem_doubles() ? 0 : (cc * cc <= jacobi_svd_smem_doubles() ? 1 : 2)]++;
+            modes[2 * cpd <= jacobi_svd_smem_doubles() ? 0 : (cpd <= jacobi_svd_smem_doubles() ? 1 : 2)]++;
         }
         std::fprintf(stderr, "[svd] %zu blocks (max %u x %u): %.3f ms, Jacobi sweeps max %d; largest %u x %u: %d sweeps; modes %d/%d/%d\n",
                      nb, mr, mc, ms, hsw.empty() ? 0 : *std::max_element(hsw.begin(), hsw.end()), both.rows[kbig],

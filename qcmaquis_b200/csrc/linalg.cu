@@ -140,29 +140,32 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                                                      double* __restrict__ U, double* __restrict__ S, double* __restrict__ V,
                                                      double* __restrict__ Wg, uint32_t smem_doubles,
                                                      int* __restrict__ zero_count, int* __restrict__ sweeps_used) {
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) double smem[];
     __shared__ int rotated;
     __shared__ uint32_t rank_of[1024];
     __shared__ double nrm[1024];
     const SvdJob J = jobs[blockIdx.x];
     const bool tall = J.m >= J.n;
     const uint32_t r = tall ? J.m : J.n, c = tall ? J.n : J.m;
-    // work matrix G (r x c) and rotations Q (c x c): both in the launch's shared memory when they fit,
-    // else G there and Q in the block's global scratch (L2-resident), else both in the scratch
-    const uint64_t rc = uint64_t(r) * c;
+    // work matrix G (r x c) and rotations Q (c x c), columns padded to an even length (a zero row, which
+    // rotations keep zero) so that every column starts on 16 bytes and is read and written two
+    // elements at a time: both in the launch's shared memory when they fit, else G there and Q in the
+    // block's global scratch (L2-resident), else both in the scratch
+    const uint32_t rp = r + (r & 1u), cq = c + (c & 1u);
+    const uint64_t rc = uint64_t(rp) * c;
     double* G;
     double* Q;
-    if (rc + uint64_t(c) * c <= smem_doubles) { G = smem; Q = smem + rc; }
+    if (rc + uint64_t(cq) * c <= smem_doubles) { G = smem; Q = smem + rc; }
     else if (rc <= smem_doubles) { G = smem; Q = Wg + J.w_off + rc; }
     else { G = Wg + J.w_off; Q = G + rc; }
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = JTHR / 32;
     // G = A or A^T, Q = I
     const double* a = A + J.a_off;
-    for (uint64_t i = tid; i < uint64_t(r) * c; i += JTHR) {
-        const uint32_t row = uint32_t(i % r), col = uint32_t(i / r);
-        G[i] = tall ? a[row + uint64_t(col) * J.m] : a[col + uint64_t(row) * J.m];
+    for (uint64_t i = tid; i < uint64_t(rp) * c; i += JTHR) {
+        const uint32_t row = uint32_t(i % rp), col = uint32_t(i / rp);
+        G[i] = row >= r ? 0.0 : (tall ? a[row + uint64_t(col) * J.m] : a[col + uint64_t(row) * J.m]);
     }
-    for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) Q[i] = (i % c == i / c) ? 1.0 : 0.0;
+    for (uint64_t i = tid; i < uint64_t(cq) * c; i += JTHR) Q[i] = (i % cq == i / cq) ? 1.0 : 0.0;
     __syncthreads();
     const uint32_t cp = c + (c & 1u);  // players, padded to even
     const double tol2 = (JEPS * double(r)) * (JEPS * double(r));
@@ -173,13 +176,14 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
     for (int sweep = 0; sweep < JMAX_SWEEPS && c > 1; ++sweep) {
         if (tid == 0) rotated = 0;
         for (uint32_t j = warp; j < c; j += nwarp) {
-            const double* g = G + uint64_t(j) * r;
+            const double* g = G + uint64_t(j) * rp;
             double x = 0.0;
             for (uint32_t i = lane; i < r; i += 32) x = fma(g[i], g[i], x);
             x = warp_sum(x);
             if (lane == 0) nrm[j] = x;
         }
         __syncthreads();
+        const uint32_t rh = rp / 2, ch = cq / 2;  // column lengths in element pairs
         for (uint32_t k = 0; k + 1 < cp; ++k) {
             // one pair per lane group; every lane runs the same number of passes so the group
             // shuffles never diverge
@@ -193,29 +197,42 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                     q = i1 == 0 ? 0 : (i1 - 1 + k) % (cp - 1) + 1;
                     act = p < c && q < c;
                 }
-                double* gp = G + uint64_t(p) * r;
-                double* gq = G + uint64_t(q) * r;
+                double2* gp = reinterpret_cast<double2*>(G + uint64_t(p) * rp);
+                double2* gq = reinterpret_cast<double2*>(G + uint64_t(q) * rp);
                 double ga = 0.0;
                 if (act)
-                    for (uint32_t i = hl; i < r; i += gs) ga = fma(gp[i], gq[i], ga);
+                    for (uint32_t i = hl; i < rh; i += gs) {
+                        const double2 x = gp[i], y = gq[i];
+                        ga = fma(x.x, y.x, ga);
+                        ga = fma(x.y, y.y, ga);
+                    }
                 ga = group_sum(ga, gs);
                 const double al = act ? nrm[p] : 0.0, be = act ? nrm[q] : 0.0;
                 const bool rot = act && ga * ga > tol2 * (al * be);
                 if (rot) {
-                    const double zeta = (be - al) / (2.0 * ga);
-                    const double tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
-                    const double cs = rsqrt(1.0 + tt * tt), sn = cs * tt;
-                    for (uint32_t i = hl; i < r; i += gs) {
-                        const double x = gp[i], y = gq[i];
-                        gp[i] = cs * x - sn * y;
-                        gq[i] = sn * x + cs * y;
+                    // t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), zeta = d / h, d = beta - alpha, h = 2 gamma,
+                    // multiplied through by |h| (one square root and one division) unless d^2 + h^2 could
+                    // overflow
+                    const double d = be - al, h = 2.0 * ga;
+                    double tt;
+                    if (fabs(d) < 1e150 && fabs(h) < 1e150) {
+                        tt = (d >= 0.0 ? h : -h) / (fabs(d) + sqrt(fma(d, d, h * h)));
+                    } else {
+                        const double zeta = d / h;
+                        tt = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
                     }
-                    double* qp = Q + uint64_t(p) * c;
-                    double* qq = Q + uint64_t(q) * c;
-                    for (uint32_t i = hl; i < c; i += gs) {
-                        const double x = qp[i], y = qq[i];
-                        qp[i] = cs * x - sn * y;
-                        qq[i] = sn * x + cs * y;
+                    const double cs = rsqrt(1.0 + tt * tt), sn = cs * tt;
+                    for (uint32_t i = hl; i < rh; i += gs) {
+                        const double2 x = gp[i], y = gq[i];
+                        gp[i] = make_double2(cs * x.x - sn * y.x, cs * x.y - sn * y.y);
+                        gq[i] = make_double2(sn * x.x + cs * y.x, sn * x.y + cs * y.y);
+                    }
+                    double2* qp = reinterpret_cast<double2*>(Q + uint64_t(p) * cq);
+                    double2* qq = reinterpret_cast<double2*>(Q + uint64_t(q) * cq);
+                    for (uint32_t i = hl; i < ch; i += gs) {
+                        const double2 x = qp[i], y = qq[i];
+                        qp[i] = make_double2(cs * x.x - sn * y.x, cs * x.y - sn * y.y);
+                        qq[i] = make_double2(sn * x.x + cs * y.x, sn * x.y + cs * y.y);
                     }
                     if (hl == 0) {
                         nrm[p] = al - tt * ga;
@@ -235,7 +252,7 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
     // sigma_j = |G_j| into S (unsorted, temporarily), then ranks by descending sigma (ties by index)
     double* sv = S + J.s_off;
     for (uint32_t j = warp; j < c; j += nwarp) {
-        const double* g = G + uint64_t(j) * r;
+        const double* g = G + uint64_t(j) * rp;
         double x = 0.0;
         for (uint32_t i = lane; i < r; i += 32) x = fma(g[i], g[i], x);
         x = warp_sum(x);
@@ -258,11 +275,11 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
     for (uint64_t i = tid; i < uint64_t(r) * c; i += JTHR) {
         const uint32_t row = uint32_t(i % r), col = uint32_t(i / r);
         const double sg = sv[col];
-        Gout[row + uint64_t(rank_of[col]) * r] = sg > 0.0 ? G[i] / sg : 0.0;
+        Gout[row + uint64_t(rank_of[col]) * r] = sg > 0.0 ? G[row + uint64_t(col) * rp] / sg : 0.0;
     }
     for (uint64_t i = tid; i < uint64_t(c) * c; i += JTHR) {
         const uint32_t row = uint32_t(i % c), col = uint32_t(i / c);
-        Qout[row + uint64_t(rank_of[col]) * c] = Q[i];
+        Qout[row + uint64_t(rank_of[col]) * c] = Q[row + uint64_t(col) * cq];
     }
     __syncthreads();
     // sigma in sorted order (through the scratch column space, G is no longer needed)
@@ -291,7 +308,8 @@ uint64_t jacobi_svd_smem_doubles() { return JSMEM_DOUBLES; }
 
 uint64_t jacobi_svd_scratch(uint32_t m, uint32_t n) {
     const uint64_t r = std::max(m, n), c = std::min(m, n);
-    return r * c + c * c;
+    const uint64_t d = (r + (r & 1)) * c + (c + (c & 1)) * c;  // the padded columns
+    return (d + 31) / 32 * 32;  // whole multiples of 32 doubles: the next block's scratch stays 16-byte aligned
 }
 
 void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64_t a_len, double* U, uint64_t u_len, double* S,
@@ -307,6 +325,7 @@ void batched_jacobi_svd(const std::vector<SvdJob>& jobs, const double* A, uint64
         if (j.a_off + uint64_t(j.m) * j.n > a_len || j.u_off + uint64_t(j.m) * k > u_len || j.s_off + k > s_len ||
             j.v_off + uint64_t(j.n) * k > v_len || j.w_off + jacobi_svd_scratch(j.m, j.n) > w_len)
             throw std::runtime_error("batched_jacobi_svd: block outside its buffers");
+        if (j.w_off % 2) throw std::runtime_error("batched_jacobi_svd: scratch offset not 16-byte aligned");
         // the blocks working in global memory first: they take longest
         if (std::max(j.m, j.n) * uint64_t(k) <= JSMEM_DOUBLES) small.push_back(j);
         else large.push_back(j);

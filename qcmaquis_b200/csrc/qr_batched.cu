@@ -32,9 +32,10 @@ namespace qcm {
 
 namespace {
 
-constexpr int QR_THR = 256;
+constexpr int QR_THR = 1024;
 constexpr int QR_WARPS = QR_THR / 32;
 constexpr uint32_t QR_PIV_MAX = 1024;  // columns of a pivoted factorisation
+constexpr uint64_t QR_SMEM_DOUBLES = 26000;  // dynamic shared memory (with the 12.4 KB static part, under 227 KB)
 
 __device__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -43,7 +44,8 @@ __device__ double warp_sum(double v) {
 
 __global__ void __launch_bounds__(QR_THR) k_qr(const QrJob* __restrict__ jobs, const double* __restrict__ A,
                                                double* __restrict__ Q, double* __restrict__ R, double* __restrict__ W,
-                                               uint32_t* __restrict__ P) {
+                                               uint32_t* __restrict__ P, uint32_t smem_doubles) {
+    extern __shared__ double qsm[];
     __shared__ double red[QR_WARPS];
     __shared__ uint32_t redi[QR_WARPS];
     __shared__ double sh_tau, sh_scale, sh_thr;
@@ -56,9 +58,12 @@ __global__ void __launch_bounds__(QR_THR) k_qr(const QrJob* __restrict__ jobs, c
     // the matrix factorised: F (mm x nn) = A_j, or A_j^T for an LQ
     const uint32_t mm = J.lq ? J.n : J.m, nn = J.lq ? J.m : J.n, k = mm < nn ? mm : nn;
     const bool pivot = (J.flags & QR_PIVOT) != 0;
-    double* w = W + J.w_off;              // F, then R above and the reflectors below the diagonal
-    double* taus = w + uint64_t(mm) * nn;  // k reflector scales
-    double* qf = taus + k;                 // Q' (mm x k) for an LQ; the QR writes Q directly
+    // F, then R above and the reflectors below the diagonal, with the k reflector scales after it: in the
+    // launch's shared memory when they fit, else in the block's global scratch (L2-resident)
+    const uint64_t fsz = uint64_t(mm) * nn + k;
+    double* w = fsz <= smem_doubles ? qsm : W + J.w_off;
+    double* taus = w + uint64_t(mm) * nn;
+    double* qf = W + J.w_off + fsz;  // Q' (mm x k) for an LQ; the QR writes Q directly
     const double* a = A + J.a_off;
     for (uint64_t e = tid; e < uint64_t(mm) * nn; e += QR_THR) {
         const uint32_t i = uint32_t(e % mm), c = uint32_t(e / mm);
@@ -269,8 +274,16 @@ void batched_qr(const std::vector<QrJob>& jobs, const double* A, uint64_t a_len,
         if ((j.flags & QR_PIVOT) && (!P || nn > QR_PIV_MAX || j.p_off + nn > p_len))
             throw std::runtime_error("batched QR: pivoting needs a permutation buffer and at most 1024 columns");
     }
+    // shared memory for the largest work matrix that fits (one CTA per SM in either case)
+    uint64_t sm = 0;
+    for (const QrJob& j : jobs) {
+        const uint64_t f = uint64_t(j.m) * j.n + std::min(j.m, j.n);
+        if (f <= QR_SMEM_DOUBLES) sm = std::max(sm, f);
+    }
+    const std::size_t bytes = std::size_t(sm) * sizeof(double);
+    if (bytes) QCM_CUDA(cudaFuncSetAttribute(k_qr, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
     jobbuf.upload(jobs, s);
-    k_qr<<<unsigned(jobs.size()), QR_THR, 0, s>>>(jobbuf.get(), A, Q, R, W, P);
+    k_qr<<<unsigned(jobs.size()), QR_THR, bytes, s>>>(jobbuf.get(), A, Q, R, W, P, uint32_t(sm));
     QCM_CUDA(cudaGetLastError());
 }
 
