@@ -448,6 +448,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     }
     const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
     std::vector<double> part_s(tdbg ? nl : 0);
+    double sum_terms = 0, sum_tiles = 0;  // QCM_PLAN_TIMING: thread time in the term enumeration / tile planning
     auto tnow = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
     const double t_a = tnow();
     std::string err;
@@ -556,6 +557,7 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
             // each unit's terms in (b1, MPO entry, operator term) order: slots numbered at first use, the
             // 16-line groups of every slot's lines recorded, lines appended once they have a term
             std::size_t n_alpha = 0;
+            const double tt0 = tdbg ? tnow() : 0.0;
             for (std::size_t ui = 0; ui < nu; ++ui) {
                 U& un = units[ui];
                 un.nw = nw16;
@@ -599,6 +601,10 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 for (uint32_t id : un.sl) slot[id] = NONE;
                 n_alpha += un.nterms;
             }
+            if (tdbg) {
+#pragma omp atomic
+                sum_terms += tnow() - tt0;
+            }
             if (n_alpha == 0) continue;
             P.n_alpha += n_alpha;
             const uint64_t s_off = P.s_len;
@@ -612,7 +618,12 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                 UnitD ud{};
                 ud.nl = uint32_t(u.lines.size()); ud.nk = uint32_t(slices.size()); ud.ne = ls_in * u.ms;
                 TileChoice tch;
+                const double tt1 = tdbg ? tnow() : 0.0;
                 plan_unit_tiles(ud, u.sig.data(), u.nw, corder, tch);
+                if (tdbg) {
+#pragma omp atomic
+                    sum_tiles += tnow() - tt1;
+                }
                 ctmp.assign(slices.begin(), slices.end());
                 for (std::size_t i = 0; i < slices.size(); ++i) slices[i] = ctmp[corder[i]];
                 if (bookkeeping) {
@@ -790,8 +801,9 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     if (tdbg) {
         double psum = 0, pmax = 0;
         for (double t : part_s) { psum += t; pmax = std::max(pmax, t); }
-        std::fprintf(stderr, "plan: tables %.4f s, parts %.4f s (sum %.4f s, largest %.4f s), merge %.4f s; %zu units, %llu "
-                     "coefficient terms, %zu S tiles, %.3e dense coefficients\n", t_a - t_0, t_b - t_a, psum, pmax, tnow() - t_b,
+        std::fprintf(stderr, "plan: tables %.4f s, parts %.4f s (sum %.4f s: terms %.4f, tiles %.4f; largest %.4f s), merge %.4f s; "
+                     "%zu units, %llu coefficient terms, %zu S tiles, %.3e dense coefficients\n", t_a - t_0, t_b - t_a, psum,
+                     sum_terms, sum_tiles, pmax, tnow() - t_b,
                      p->units.size(), (unsigned long long)p->n_alpha,
                      p->utiles[0].size() + p->utiles[1].size() + p->utiles[2].size() + p->utiles[3].size(), double(p->w_len));
     }
