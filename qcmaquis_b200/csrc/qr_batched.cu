@@ -35,7 +35,7 @@ namespace {
 constexpr int QR_THR = 1024;
 constexpr int QR_WARPS = QR_THR / 32;
 constexpr uint32_t QR_PIV_MAX = 1024;  // columns of a pivoted factorisation
-constexpr uint64_t QR_SMEM_DOUBLES = 26000;  // dynamic shared memory (with the 12.4 KB static part, under 227 KB)
+constexpr uint64_t QR_SMEM_DOUBLES = 27400;  // dynamic shared memory (with the 12.4 KB static part, under 227 KB)
 
 __device__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
