@@ -47,10 +47,9 @@ HeffPlan::~HeffPlan() {
 namespace {
 
 constexpr uint32_t NONE = 0xffffffffu;
-// K rows per split-K item of the L.S GEMM (measured at L=24 M=512: 512 -> 1.06 ms, 1024 -> 0.77 ms,
-// 2048 -> 0.84 ms, 4096 -> 1.28 ms: more partial tiles to reduce below, fewer concurrent items above)
 // split-K chunk of the L.S GEMM (rows of K per work item): 512 gives about twice the CTAs of 1024 at the
-// L=24, M=512 middle bond and took the L.S phase from 0.47 to 0.41 ms; 256 was no faster
+// L=24, M=512 middle bond and took the L.S phase from 0.47 to 0.41 ms (with the per-element reduction of
+// the partials); 256 was no faster
 constexpr uint32_t KCHUNK = 512;
 
 void add_tiles(std::vector<TileD>* tiles, uint32_t item, uint32_t M, uint32_t N) {
