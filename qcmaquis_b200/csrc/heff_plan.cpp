@@ -162,10 +162,10 @@ uint32_t checked_ksteps(const UnitD& u) {
 }
 
 // Slot order and tiling of an H_eff unit from its slot signatures: sig[slot * nw + w] bit r set where a
-// line of 16-line group 64 w + r uses the slot.  For each tile height (16, 32, 64, 128 lines) the slots
-// are sorted by the line tiles that use them (then by the 16-line groups; first-use order among
-// equal sets), so that slots used by the same line tiles share 4-slot k-groups; the ordering and shape
-// of least tensor work are kept.  order[new slot] = old slot.
+// line of 16-line group 64 w + r uses the slot.  For line tiles of 16, 64 and 128 lines the slots are
+// sorted by the line tiles that use them (then by the 16-line groups; first-use order among equal
+// sets), so that slots used by the same line tiles share 4-slot k-groups; the ordering and shape of
+// least tensor work (over all four shapes) are kept.  order[new slot] = old slot.
 void plan_unit_tiles(const UnitD& u, const uint64_t* sig, uint32_t nw, std::vector<uint32_t>& order, TileChoice& best) {
     const uint32_t nk = u.nk;
     order.resize(nk);
@@ -175,7 +175,9 @@ void plan_unit_tiles(const UnitD& u, const uint64_t* sig, uint32_t nw, std::vect
     std::vector<uint64_t> key;
     std::vector<uint32_t> ord(nk);
     std::vector<uint8_t> occ16, scratch;
-    for (uint32_t f : {1u, 2u, 4u, 8u}) {
+    // line-tile coarseness of the ordering key: 16, 64 and 128 lines (32 won in 13 of 4,878 units at the
+    // L=24, M=512 middle bond without changing the executed work; leaving it out saves 40 % of this step)
+    for (uint32_t f : {1u, 4u, 8u}) {
         if (f > 1 && (n16 + f / 2 - 1) / (f / 2) <= 1) break;  // one coarse tile: the same order as before
         const uint32_t nc = (n16 + f - 1) / f, ncw = (nc + 63) / 64;
         key.assign(std::size_t(nk) * ncw, 0);
