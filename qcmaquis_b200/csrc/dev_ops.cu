@@ -59,15 +59,31 @@ __global__ void __launch_bounds__(NTHR) k_bgemm(const GemmJob* __restrict__ jobs
         if (kc + 1 < nk) issue((kc + 1) & 1, (kc + 1) * BK);
         mma_stage<S>(st[kc & 1].A, st[kc & 1].B, acc, warp, lane);
     }
-    for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
-        uint32_t gm = tile.m0 + m, gn = tile.n0 + n;
-        if (gm < J.M && gn < J.N) {
-            uint64_t base = J.c_off;
-            if (J.crb) { const uint32_t blk = gm / J.crb; base += uint64_t(blk) * J.c_bs; gm -= blk * J.crb; }
-            double* c = C + base + gm + uint64_t(gn) * J.ldc;
-            *c = (J.beta == 0.0) ? J.alpha * v : J.alpha * v + J.beta * *c;
+    // the thread's FM rows (row-blocked C: block gm / crb) and FN x 2 columns, each offset once
+    const int r = lane >> 2, q = lane & 3;
+    const int wm = warp % S::WM, wn = warp / S::WM;
+#pragma unroll
+    for (int i = 0; i < S::FM; ++i) {
+        uint32_t gm = tile.m0 + wm * S::FM * 8 + i * 8 + r;
+        if (gm >= J.M) continue;
+        uint64_t base = J.c_off;
+        if (J.crb) {
+            const uint32_t blk = gm / J.crb;
+            base += uint64_t(blk) * J.c_bs;
+            gm -= blk * J.crb;
         }
-    });
+        double* crow = C + base + gm;
+#pragma unroll
+        for (int j = 0; j < S::FN; ++j)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc) {
+                const uint32_t gn = tile.n0 + wn * S::FN * 8 + j * 8 + q * 2 + cc;
+                if (gn >= J.N) continue;
+                double* c = crow + uint64_t(gn) * J.ldc;
+                const double v = acc.c[i][j][cc];
+                *c = (J.beta == 0.0) ? J.alpha * v : J.alpha * v + J.beta * *c;
+            }
+    }
 }
 
 __global__ void k_bcopy(const CopyJob* __restrict__ jobs, uint32_t njobs, const double* __restrict__ src,

@@ -214,14 +214,30 @@ __global__ void __launch_bounds__(NTHR, 5) k_sgemm(const UnitD* __restrict__ uni
         }
         mma_stage_masked<S>(st[i & 1].A, st[i & 1].B, acc, warp, lane, mask);
     }
-    for_acc<S>(acc, warp, lane, [&](int m, int n, double v) {
-        uint32_t gl = tile.m0 + m, gn = tile.n0 + n;
-        if (gl < U.nl && gn < U.ne) {
-            uint32_t b1 = line_b1[U.line0 + gl];
-            uint32_t c = gn / U.erows, r = gn - c * U.erows;
-            Sm[U.s_off + uint64_t(b1) * U.line_stride + r + uint64_t(c) * U.col_stride] = v;
+    // the thread's outputs: its FN x 2 columns (element gn % erows of column block gn / erows) and FM
+    // lines (S row block of line_b1), each offset computed once
+    const int r = lane >> 2, q = lane & 3;
+    const int wm = warp % S::WM, wn = warp / S::WM;
+    uint32_t cof[S::FN][2];
+#pragma unroll
+    for (int j = 0; j < S::FN; ++j)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const uint32_t gn = tile.n0 + wn * S::FN * 8 + j * 8 + q * 2 + c;
+            const uint32_t cb = gn / U.erows;
+            cof[j][c] = gn < U.ne ? (gn - cb * U.erows) + cb * U.col_stride : 0xffffffffu;
         }
-    });
+#pragma unroll
+    for (int i = 0; i < S::FM; ++i) {
+        const uint32_t gl = tile.m0 + wm * S::FM * 8 + i * 8 + r;
+        if (gl >= U.nl) continue;
+        double* srow = Sm + U.s_off + uint64_t(line_b1[U.line0 + gl]) * U.line_stride;
+#pragma unroll
+        for (int j = 0; j < S::FN; ++j)
+#pragma unroll
+            for (int c = 0; c < 2; ++c)
+                if (cof[j][c] != 0xffffffffu) srow[cof[j][c]] = acc.c[i][j][c];
+    }
 }
 
 // One CTA per unit, one thread per line: the line's coefficient terms (CoefGen), in MPO-entry

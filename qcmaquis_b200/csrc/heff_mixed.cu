@@ -215,20 +215,30 @@ __global__ void __launch_bounds__(XTHR) k_sgemm_x3(const UnitD* __restrict__ uni
                 }
         }
     }
+    // the thread's outputs: FN x 2 columns (element gn % erows of column block gn / erows) and FM x 2 lines,
+    // each offset computed once
+    uint32_t cof[S::FN][2];
+#pragma unroll
+    for (int j = 0; j < S::FN; ++j)
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const uint32_t gn = tile.n0 + wn * S::FN * 8 + j * 8 + 2 * t + c;
+            const uint32_t cb = gn / U.erows;
+            cof[j][c] = gn < U.ne ? (gn - cb * U.erows) + cb * U.col_stride : 0xffffffffu;
+        }
 #pragma unroll
     for (int i = 0; i < S::FM; ++i)
 #pragma unroll
-        for (int j = 0; j < S::FN; ++j)
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t gl = tile.m0 + wm * S::FM * 16 + i * 16 + g + h * 8;
+            if (gl >= U.nl) continue;
+            double* srow = Sm + U.s_off + uint64_t(line_b1[U.line0 + gl]) * U.line_stride;
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const uint32_t gl = tile.m0 + wm * S::FM * 16 + i * 16 + g + (c >> 1) * 8;
-                const uint32_t gn = tile.n0 + wn * S::FN * 8 + j * 8 + 2 * t + (c & 1);
-                if (gl < U.nl && gn < U.ne) {
-                    const uint32_t b1 = line_b1[U.line0 + gl];
-                    const uint32_t col = gn / U.erows, row = gn - col * U.erows;
-                    Sm[U.s_off + uint64_t(b1) * U.line_stride + row + uint64_t(col) * U.col_stride] = double(acc[i][j][c]);
-                }
-            }
+            for (int j = 0; j < S::FN; ++j)
+#pragma unroll
+                for (int c = 0; c < 2; ++c)
+                    if (cof[j][c] != 0xffffffffu) srow[cof[j][c]] = double(acc[i][j][2 * h + c]);
+        }
 }
 
 // ---------------------------------------------------------------------------
