@@ -381,7 +381,9 @@ __global__ void __launch_bounds__(NTHR) k_lspart(const KItemD* __restrict__ item
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t M = O.M, Kc = sg.nS * sg.ls_in;
     const uint64_t blk = uint64_t(M) * sg.ls_in;
-    auto issue = [&](int sidx, uint32_t k0) {
+    // L column bases of a stage's 16 k rows, written two stages ahead so that the loop's barrier
+    // publishes them before their stage is issued
+    auto bases = [&](int sidx, uint32_t k0) {
         if (tid < BK) {
             uint32_t kk = k0 + tid;
             uint64_t kb = sg.l_off;
@@ -391,7 +393,8 @@ __global__ void __launch_bounds__(NTHR) k_lspart(const KItemD* __restrict__ item
             }
             kbase[sidx][tid] = kb;
         }
-        __syncthreads();
+    };
+    auto issue = [&](int sidx, uint32_t k0) {
         Stage<S>& s = st[sidx];
         if (!sg.tr) {
 #pragma unroll
@@ -425,11 +428,16 @@ __global__ void __launch_bounds__(NTHR) k_lspart(const KItemD* __restrict__ item
     Acc<S> acc;
     acc.zero();
     const uint32_t nk = (it.k1 - it.k0 + BK - 1) / BK;
+    bases(0, it.k0);
+    bases(1, it.k0 + BK);
+    __syncthreads();
     issue(0, it.k0);
     for (uint32_t kc = 0; kc < nk; ++kc) {
         cp_wait_all();
         __syncthreads();
         if (kc + 1 < nk) issue((kc + 1) & 1, it.k0 + (kc + 1) * BK);
+        // stage kc's bases were consumed when it was issued: the buffer takes stage kc + 2's
+        if (kc + 2 < nk) bases(kc & 1, it.k0 + (kc + 2) * BK);
         mma_stage<S>(st[kc & 1].A, st[kc & 1].B, acc, warp, lane);
     }
     double* Pt = P + uint64_t(blockIdx.x) * S::BM * S::BN;
