@@ -182,6 +182,11 @@ struct MPOTables {
     // the same grouped by (operator, output state), in their order within the operator
     std::vector<uint32_t> o_ptr, o_in;
     std::vector<double> o_val;
+    // per (operator, output state): the input state of its only term, O_NONE without a term, O_MANY with
+    // several; and per entry in row order (op * nst) << 32 | b2, the entry's two lookups in one word
+    static constexpr uint32_t O_NONE = 0xfffffffeu, O_MANY = 0xffffffffu;
+    std::vector<uint32_t> o_one;
+    std::vector<uint64_t> row_qb;
     // MPO entries by row b1 (other index b2) and by column b2 (other index b1, increasing b1)
     std::vector<uint32_t> row_ptr, row_other, row_op, col_ptr, col_other, col_op;
     std::vector<double> row_scale, col_scale;

@@ -303,6 +303,14 @@ std::shared_ptr<const MPOTables> build_mpo_tables(const MPOTensor& W) {
             t->o_in[d] = t->oin[k];
             t->o_val[d] = t->oval[k];
         }
+    t->o_one.assign(nops * nst, MPOTables::O_NONE);
+    for (std::size_t i = 0; i < nops * nst; ++i) {
+        const uint32_t n = t->o_ptr[i + 1] - t->o_ptr[i];
+        if (n == 1) t->o_one[i] = t->o_in[t->o_ptr[i]];
+        else if (n > 1) t->o_one[i] = MPOTables::O_MANY;
+    }
+    t->row_qb.resize(nent);
+    for (std::size_t e = 0; e < nent; ++e) t->row_qb[e] = (uint64_t(W.op[e]) * nst << 32) | W.b2[e];
     // entries by row and by column
     t->row_ptr = W.row_ptr;
     t->row_other = W.b2; t->row_op = W.op; t->row_scale = W.scale;
@@ -425,6 +433,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
     // the same grouped by (operator, output state), in their order within the operator
     const std::vector<uint32_t>& og_ptr = mt->o_ptr;
     const std::vector<uint32_t>& og_in = mt->o_in;
+    const uint32_t* o_one = mt->o_one.data();
+    const uint64_t* row_qb = mt->row_qb.data();
     const std::vector<double>& og_val = mt->o_val;
     // coefficient generation: lines iterate MPO rows b1, slices come from R cohorts
     p->cg.set_mpo(W, true);
@@ -568,34 +578,38 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     const uint64_t before = un.nterms;
                     const uint32_t gw = (line >> 4) >> 6;
                     const uint64_t gbit = 1ull << ((line >> 4) & 63);
-                    for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
-                        const uint32_t b2 = W.b2[e];
-                        const std::size_t q = std::size_t(W.op[e]) * nst + un.st;
-                        for (uint32_t k = og_ptr[q]; k < og_ptr[q + 1]; ++k) {
-                            const uint32_t sti = og_in[k];
-                            const GRef g = gu[sti];
-                            if (!g.rp) continue;
-                            const int32_t pos = g.rp[b2];
-                            if (pos < 0) continue;
-                            const uint32_t id = g.jbase + uint32_t(pos);
-                            uint32_t& sl = slot[id];
-                            if (sl == NONE) {
-                                sl = uint32_t(un.sl.size());
-                                un.sl.push_back(id);
-                                un.sig.resize(un.sig.size() + nw16, 0);
-                            }
-                            un.sig[std::size_t(sl) * nw16 + gw] |= gbit;
-                            ++un.nterms;
-                            if (bookkeeping) {
-                                un.em.push_back(LKD{line, sl});
-                                const uint32_t c = gin[ui * nst + sti].c;
-                                const uint32_t col = uint32_t(R.offset(c, b2) / rsin_t[sti]);
-                                const uint32_t job = tj[std::size_t(sti) * nr + un.rb_out];
-                                const uint32_t row[3] = {P.tjob_mps[job], c, col};
-                                un.bk.insert(un.bk.end(), row, row + 3);
-                                un.bk_a.push_back(og_val[k] * R.conj_scale(c, b2) * (W.scale[e] * L.conj_scale(ci, b1)));
-                            }
+                    // one term: input state sti of the entry's operator (term k), MPO column b2
+                    auto term = [&](uint32_t sti, uint32_t k, uint32_t b2, uint32_t e) {
+                        const GRef g = gu[sti];
+                        if (!g.rp) return;
+                        const int32_t pos = g.rp[b2];
+                        if (pos < 0) return;
+                        const uint32_t id = g.jbase + uint32_t(pos);
+                        uint32_t& sl = slot[id];
+                        if (sl == NONE) {
+                            sl = uint32_t(un.sl.size());
+                            un.sl.push_back(id);
+                            un.sig.resize(un.sig.size() + nw16, 0);
                         }
+                        un.sig[std::size_t(sl) * nw16 + gw] |= gbit;
+                        ++un.nterms;
+                        if (bookkeeping) {
+                            un.em.push_back(LKD{line, sl});
+                            const uint32_t c = gin[ui * nst + sti].c;
+                            const uint32_t col = uint32_t(R.offset(c, b2) / rsin_t[sti]);
+                            const uint32_t job = tj[std::size_t(sti) * nr + un.rb_out];
+                            const uint32_t row[3] = {P.tjob_mps[job], c, col};
+                            un.bk.insert(un.bk.end(), row, row + 3);
+                            un.bk_a.push_back(og_val[k] * R.conj_scale(c, b2) * (W.scale[e] * L.conj_scale(ci, b1)));
+                        }
+                    };
+                    for (uint32_t e = W.row_ptr[b1]; e < W.row_ptr[b1 + 1]; ++e) {
+                        const uint64_t x = row_qb[e];
+                        const uint32_t b2 = uint32_t(x), q = uint32_t(x >> 32) + un.st;
+                        const uint32_t one = o_one[q];
+                        if (one < MPOTables::O_NONE) term(one, og_ptr[q], b2, e);
+                        else if (one == MPOTables::O_MANY)
+                            for (uint32_t k = og_ptr[q]; k < og_ptr[q + 1]; ++k) term(og_in[k], k, b2, e);
                     }
                     if (un.nterms != before) { un.lines.push_back(lr.second); un.rows.push_back(b1); }
                 }
