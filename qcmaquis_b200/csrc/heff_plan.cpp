@@ -180,25 +180,33 @@ void plan_unit_tiles(const UnitD& u, const uint64_t* sig, uint32_t nw, std::vect
     for (uint32_t f : {1u, 4u, 8u}) {
         if (f > 1 && (n16 + f / 2 - 1) / (f / 2) <= 1) break;  // one coarse tile: the same order as before
         const uint32_t nc = (n16 + f - 1) / f, ncw = (nc + 63) / 64;
-        key.assign(std::size_t(nk) * ncw, 0);
-        for (uint32_t sl = 0; sl < nk; ++sl)
-            for (uint32_t w = 0; w < nw; ++w)
-                for (uint64_t bits = sig[std::size_t(sl) * nw + w]; bits; bits &= bits - 1) {
-                    const uint32_t c = (64 * w + uint32_t(__builtin_ctzll(bits))) / f;
-                    key[std::size_t(sl) * ncw + c / 64] |= 1ull << (c % 64);
-                }
-        for (uint32_t i = 0; i < nk; ++i) ord[i] = i;
-        std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
-            for (uint32_t w = ncw; w-- > 0;) {
-                const uint64_t x = key[std::size_t(a) * ncw + w], y = key[std::size_t(b) * ncw + w];
-                if (x != y) return x < y;
-            }
+        auto by_sig = [&](uint32_t a, uint32_t b) {
             for (uint32_t w = nw; w-- > 0;) {
                 const uint64_t x = sig[std::size_t(a) * nw + w], y = sig[std::size_t(b) * nw + w];
                 if (x != y) return x < y;
             }
             return false;
-        });
+        };
+        for (uint32_t i = 0; i < nk; ++i) ord[i] = i;
+        if (f == 1) {
+            // 16-line tiles: the key is the signature itself
+            std::stable_sort(ord.begin(), ord.end(), by_sig);
+        } else {
+            key.assign(std::size_t(nk) * ncw, 0);
+            for (uint32_t sl = 0; sl < nk; ++sl)
+                for (uint32_t w = 0; w < nw; ++w)
+                    for (uint64_t bits = sig[std::size_t(sl) * nw + w]; bits; bits &= bits - 1) {
+                        const uint32_t c = (64 * w + uint32_t(__builtin_ctzll(bits))) / f;
+                        key[std::size_t(sl) * ncw + c / 64] |= 1ull << (c % 64);
+                    }
+            std::stable_sort(ord.begin(), ord.end(), [&](uint32_t a, uint32_t b) {
+                for (uint32_t w = ncw; w-- > 0;) {
+                    const uint64_t x = key[std::size_t(a) * ncw + w], y = key[std::size_t(b) * ncw + w];
+                    if (x != y) return x < y;
+                }
+                return by_sig(a, b);
+            });
+        }
         occ16.assign(std::size_t(n16) * nks, 0);
         for (uint32_t i = 0; i < nk; ++i) {
             const uint32_t sl = ord[i];
