@@ -489,6 +489,41 @@ def batched_solves(a, ctx, n=128, L=12, M=128):
     return out
 
 
+def group_sweeps(a, ctx, n=16, L=12, M=128, sweeps=3):
+    """Whole DMRG runs in lockstep: n independent two-site FP64 runs (synthetic Hamiltonians of L orbitals,
+    N = L, seeds 1 .. n, const initial state with bond dimension 16, Mmax M) swept together by
+    qcm_dmrg_group_sweep (one merged plan group and one lockstep JD per step) against the same runs swept one
+    after the other; per-sweep wall times of both and the largest step-energy difference between them."""
+    from qcmaquis_b200.dmrg import DMRG
+    from qcmaquis_b200.mpo import MPO
+    fd = _fcidump()
+    mpos = []
+    for seed in range(1, n + 1):
+        h, V, _ = fd.synthetic_integrals(L, seed)
+        mpos.append(MPO.qc(h, V))
+    grp = [DMRG(ctx, m, L // 2, L // 2, M, 16) for m in mpos]
+    sep = [DMRG(ctx, m, L // 2, L // 2, M, 16) for m in mpos]
+    t_grp, t_sep, dE = [], [], []
+    for s in range(sweeps):
+        t = time.perf_counter()
+        Eg, _ = DMRG.group_sweep(grp)
+        t_grp.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        Es = np.array([d.sweep()[0] for d in sep])
+        t_sep.append(time.perf_counter() - t)
+        dE.append(float(np.abs(Eg - Es).max()))
+    st = [d.stats() for d in grp]
+    out = {"workload": (f"{n} independent two-site DMRG runs: synthetic Hamiltonians L={L} N={L} TwoU1 Sz=0 seeds "
+                        f"1..{n}, Mmax {M}, const initial state (bond dimension 16), jcd_tol 1e-10, maxiter 8"),
+           "group_sweep_s": t_grp, "separate_sweeps_s": t_sep,
+           "group_jd_s": sum(x["jd_s"] for x in st), "group_plan_s": sum(x["plan_s"] for x in st),
+           "group_trunc_s": sum(x["trunc_s"] for x in st), "group_boundary_s": sum(x["boundary_s"] for x in st),
+           "max_abs_step_energy_diff": dE,
+           "note": "wall times; the group form batches the JD of every step, truncation and boundary steps run per run"}
+    del grp, sep
+    return out
+
+
 def sweep_comparison(a, ctx, h, V):
     """FP64 and mixed-form sweeps from the same const state: per-sweep time, energy, truncated weight, and
     the mixed form's deviations from the FP64 sweeps (the FP64 device sweeps match the oracle's to 1e-10 Eh
@@ -623,6 +658,7 @@ def run_b200(a, world, rank, local, pg):
                 extras["batched"] = batched_solves(a, ctx)
             except FileNotFoundError as ex:  # the sector fixture of the batched configuration is missing
                 extras["batched"] = {"error": str(ex)}
+            extras["group_sweeps"] = group_sweeps(a, ctx)
     cpu = None
     if want_oracle and world == 1:
         cpu = cpu_baseline(snap, blob, site1, x_host, info["flops"])

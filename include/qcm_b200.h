@@ -499,6 +499,16 @@ int qcm_dmrg_integral_gradient(qcm_dmrg* d, const double* h, const double* V, do
  * half-sweep (site L-1 left to right, site 0 right to left) canonise without truncation and report
  * zero truncation results. */
 int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);
+/* One sweep of n independent runs in lockstep (the batching form for whole DMRG solves; the reference
+ * runs one solve per process, sim.h / dmrg_sim.cpp): at every step each run builds (or re-binds) its
+ * H_eff plan and two-site tensor, the n plans are merged into one plan group and one lockstep
+ * Jacobi-Davidson (as qcm_jd_solve_batched, CUDA graphs) finds every run's ground state, then each run
+ * truncates and moves its boundary as qcm_dmrg_sweep does.  Every run: two-site, FP64, no GMRES
+ * corrections, no ortho states, jcd_maxiter <= 16, the same length, jcd_tol, jcd_maxiter and context,
+ * between sweeps.  energies[n * steps] and trunc[n * steps] (may be NULL) run-major.  Each run's
+ * energies agree with its own qcm_dmrg_sweep to the JD tolerance (the lockstep JD orthogonalises its
+ * subspace by classical Gram-Schmidt twice instead of the single solve's modified Gram-Schmidt). */
+int qcm_dmrg_group_sweep(qcm_dmrg* const* runs, int n, double* energies, qcm_trunc_result* trunc);
 int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* stats);
 /* Run the current sweep up to (not including) step stop_step (steps_per_sweep
  * completes it); energies / trunc receive one entry per step run (may be NULL),

@@ -582,6 +582,35 @@ int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc) {
     QCM_CATCH
 }
 
+int qcm_dmrg_group_sweep(qcm_dmrg* const* runs, int n, double* energies, qcm_trunc_result* trunc) {
+    QCM_TRY
+    if (!runs || n <= 0 || !energies) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_group_sweep: NULL argument");
+    std::vector<qcm::DevDMRG*> e(n);
+    for (int i = 0; i < n; ++i) {
+        if (!runs[i]) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_group_sweep: NULL run");
+        if (runs[i]->ctx != runs[0]->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_group_sweep: the runs use different contexts");
+        for (int j = 0; j < i; ++j)
+            if (runs[j] == runs[i]) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_group_sweep: a run appears twice");
+        e[i] = runs[i]->e.get();
+    }
+    QCM_CUDA(cudaSetDevice(runs[0]->ctx->device));
+    qcm::AllocStream scope(runs[0]->ctx->stream);
+    std::vector<std::vector<double>> E;
+    std::vector<std::vector<qcm::TruncResults>> T;
+    qcm::dmrg_group_sweep(e, E, T);
+    const std::size_t steps = E[0].size();
+    for (int i = 0; i < n; ++i) {
+        std::memcpy(energies + i * steps, E[i].data(), steps * sizeof(double));
+        if (trunc)
+            for (std::size_t k = 0; k < steps; ++k) {
+                const qcm::TruncResults& t = T[i][k];
+                trunc[i * steps + k] = qcm_trunc_result{t.bond_dimension, t.truncated_weight, t.truncated_fraction, t.smallest_ev};
+            }
+    }
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* s) {
     if (!d || !s) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_get_stats: NULL argument");
     const qcm::DMRGStats& t = d->e->st;

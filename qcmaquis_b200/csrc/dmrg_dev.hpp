@@ -307,6 +307,17 @@ struct DMRGStats {
     double plan_s = 0, jd_s = 0, trunc_s = 0, boundary_s = 0, total_s = 0;
 };
 
+// One two-site step between its phases: the two-site tensor and its staged plan (step_prepare), then
+// the eigenvector in tst.twin and the eigenvalue (the JD), then truncation and boundary step (step_finish)
+struct StepState {
+    int step = 0, lr = 0, site1 = 0, site2 = 0;
+    DTwoSite tst;
+    std::unique_ptr<HeffPlan> plan;
+    uint64_t key = 0;
+    bool timing = false;
+    double t0 = 0, t1 = 0, tt[8] = {};
+};
+
 struct DevDMRG {
     int L = 0;
     std::vector<MPOTensor> mpo, ts_mpo;
@@ -350,6 +361,11 @@ struct DevDMRG {
     void pending_twin(std::vector<double>& twin);
     void step_sites(int step, int& lr, int& site1, int& site2) const;
 
+    // the phases of a two-site step (step = prepare, the JD on the plan and twin, finish)
+    void step_prepare(StepState& S, int step);
+    void step_finish(StepState& S, double eigenvalue, double& energy, TruncResults& tr);
+    int last_iters = 0;  // JD iterations of the last step
+
   private:
     // H_eff plans of the previous sweep's steps, kept on the host with their device buffers released:
     // a step whose boundaries and site indices have the same structure (the same sectors, cohorts,
@@ -377,9 +393,16 @@ struct DevDMRG {
     void init_boundaries(int site = 0);
     void step(int step, double& energy, TruncResults& tr);
     void step_single(int step, double& energy, TruncResults& tr);
-    int last_iters = 0;  // JD iterations of the last step
     // JD of one step's plan with this object's ortho vectors (built by make_ortho) and its statistics
     double solve(HeffPlan& plan, DMPS& x, const std::function<void(std::size_t, double*)>& make_ortho);
 };
+
+// Many independent two-site FP64 runs (same length and JD settings, one stream, at the start of a sweep)
+// swept in lockstep, the batching form for whole solves: at every step each run builds or re-binds its
+// plan, the plans are merged into one group (merge_plans) and one lockstep Jacobi-Davidson
+// (jacobi_davidson_batched, a CUDA graph per iteration) solves every run's two-site problem, then each
+// run truncates and moves its boundary.  energies[run][step], trunc[run][step].
+void dmrg_group_sweep(const std::vector<DevDMRG*>& runs, std::vector<std::vector<double>>& energies,
+                      std::vector<std::vector<TruncResults>>& trunc);
 
 }  // namespace qcm

@@ -696,49 +696,52 @@ double DevDMRG::solve(HeffPlan& plan, DMPS& x, const std::function<void(std::siz
     return E;
 }
 
-void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
-    int lr, site1, site2;
-    step_sites(_site, lr, site1, site2);
-    // QCM_SWEEP_TIMING=1 prints the wall time of each phase of every step
-    static const bool timing = std::getenv("QCM_SWEEP_TIMING") != nullptr;
-    double tt[8];
+void DevDMRG::step_prepare(StepState& S, int _site) {
+    S.step = _site;
+    step_sites(_site, S.lr, S.site1, S.site2);
+    const int site1 = S.site1, site2 = S.site2;
+    S.timing = std::getenv("QCM_SWEEP_TIMING") != nullptr;
     auto mark = [&](int i) {
-        if (!timing) return;
+        if (!S.timing) return;
         QCM_CUDA(cudaStreamSynchronize(c.s));
-        tt[i] = now_s();
+        S.tt[i] = now_s();
     };
-    const double t0 = now_s();
-    tt[0] = t0;
+    S.t0 = now_s();
+    S.tt[0] = S.t0;
     make_left_paired(c, mps[site1]);
     make_right_paired(c, mps[site2]);
-    DTwoSite tst;
-    tst.build(c, mps[site1], mps[site2]);
+    S.tst = DTwoSite();
+    S.tst.build(c, mps[site1], mps[site2]);
     mark(1);
-    uint64_t key = 0;
     bool resident = false;
-    auto plan = plan_for(_site, *left_[site1], *right_[site2 + 1], ts_mpo[site1], tst.phys, tst.twin.left, tst.right, key,
-                         resident);
+    S.plan = plan_for(_site, *left_[site1], *right_[site2 + 1], ts_mpo[site1], S.tst.phys, S.tst.twin.left, S.tst.right,
+                      S.key, resident);
     mark(2);
-    plan->stream = c.s;
-    if (resident) restage_plan(*plan);
-    else upload_plan(*plan);
+    S.plan->stream = c.s;
+    if (resident) restage_plan(*S.plan);
+    else upload_plan(*S.plan);
     QCM_CUDA(cudaStreamSynchronize(c.s));
-    const double t1 = now_s();
-    st.plan_s += t1 - t0;
-    const double E = solve(*plan, tst.twin, [&](std::size_t o, double* v) {
-        DTwoSite tso;
-        tso.build(c, ortho_lp[o][site1], ortho_rp[o][site2]);
-        ortho_vector(c, tst.twin, tso.twin, ortho_left_[o][site1], ortho_right_[o][site2 + 1], v);
-    });
+    S.t1 = now_s();
+    st.plan_s += S.t1 - S.t0;
+}
+
+void DevDMRG::step_finish(StepState& S, double E, double& energy, TruncResults& tr) {
+    const int _site = S.step, site1 = S.site1, site2 = S.site2;
+    DTwoSite& tst = S.tst;
+    auto mark = [&](int i) {
+        if (!S.timing) return;
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        S.tt[i] = now_s();
+    };
     const double t2 = now_s();
-    keep_plan(_site, std::move(plan), key);
+    keep_plan(_site, std::move(S.plan), S.key);
     tst.twin_to_both(c);
     mark(3);
     energy = E + p.ecore;
     double t3_last = 0;
     const double alpha = sweep_count < p.ngrowsweeps ? p.alpha_initial
                          : (sweep_count < p.ngrowsweeps + p.nmainsweeps ? p.alpha_main : p.alpha_final);
-    if (lr == 1) {
+    if (S.lr == 1) {
         tr = p.heev ? tst.predict_split(c, true, p.Mmax, p.cutoff, alpha, *left_[site1], mpo[site1], mps[site1], mps[site2])
                     : tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
         mark(4);
@@ -772,12 +775,101 @@ void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
         QCM_CUDA(cudaStreamSynchronize(c.s));
         st.boundary_s += now_s() - t3;
     }
-    if (timing) {
+    if (S.timing) {
         const double tend = now_s();
         std::fprintf(stderr,
                      "[step %d] twosite %.4f plan %.4f upload %.4f jd %.4f (%d) t2b %.4f svd %.4f qr %.4f bstep %.4f total %.4f\n",
-                     _site, tt[1] - tt[0], tt[2] - tt[1], t1 - tt[2], t2 - t1, last_iters, tt[3] - t2, tt[4] - tt[3],
-                     t3_last - tt[4], tend - t3_last, tend - tt[0]);
+                     _site, S.tt[1] - S.tt[0], S.tt[2] - S.tt[1], S.t1 - S.tt[2], t2 - S.t1, last_iters, S.tt[3] - t2,
+                     S.tt[4] - S.tt[3], t3_last - S.tt[4], tend - t3_last, tend - S.tt[0]);
+    }
+}
+
+void DevDMRG::step(int _site, double& energy, TruncResults& tr) {
+    StepState S;
+    step_prepare(S, _site);
+    const int site1 = S.site1, site2 = S.site2;
+    const double E = solve(*S.plan, S.tst.twin, [&](std::size_t o, double* v) {
+        DTwoSite tso;
+        tso.build(c, ortho_lp[o][site1], ortho_rp[o][site2]);
+        ortho_vector(c, S.tst.twin, tso.twin, ortho_left_[o][site1], ortho_right_[o][site2 + 1], v);
+    });
+    step_finish(S, E, energy, tr);
+}
+
+void dmrg_group_sweep(const std::vector<DevDMRG*>& runs, std::vector<std::vector<double>>& energies,
+                      std::vector<std::vector<TruncResults>>& trunc) {
+    if (runs.empty()) throw std::runtime_error("DMRG group: no runs");
+    DevDMRG& r0 = *runs[0];
+    const int n = r0.steps_per_sweep();
+    for (const DevDMRG* d : runs) {
+        if (d->p.single_site || d->p.precision != 0 || d->p.jcd_gmres != 0 || !d->ortho_rp.empty())
+            throw std::runtime_error("DMRG group: two-site FP64 runs without GMRES or ortho states only");
+        if (d->steps_per_sweep() != n || d->next_step != 0 || d->c.s != r0.c.s)
+            throw std::runtime_error("DMRG group: the runs differ in length, position or stream");
+        if (d->p.jcd_tol != r0.p.jcd_tol || d->p.jcd_maxiter != r0.p.jcd_maxiter || d->p.jcd_maxiter > 16)
+            throw std::runtime_error("DMRG group: the runs differ in the JD tolerance or iteration limit (at most 16)");
+    }
+    const std::size_t nr = runs.size();
+    energies.assign(nr, {});
+    trunc.assign(nr, {});
+    const double t_start = now_s();
+    std::vector<StepState> S(nr);
+    const bool timing = std::getenv("QCM_SWEEP_TIMING") != nullptr;
+    for (int step = 0; step < n; ++step) {
+        const double tp = now_s();
+        for (std::size_t i = 0; i < nr; ++i) runs[i]->step_prepare(S[i], step);
+        double tm = 0, tjd = 0;
+        // one plan group, one lockstep Jacobi-Davidson over every run's two-site problem
+        const double tj = now_s();
+        std::vector<HeffPlan*> plans(nr);
+        for (std::size_t i = 0; i < nr; ++i) plans[i] = S[i].plan.get();
+        std::vector<uint64_t> xo, xn(nr);
+        std::vector<double> ev;
+        std::vector<int> iters;
+        int applies = 0;
+        {
+            AllocStream scope(r0.c.s);
+            auto g = merge_plans(plans, xo, r0.c.s);
+            if (timing) { QCM_CUDA(cudaStreamSynchronize(r0.c.s)); tm = now_s(); }
+            DBuf<double> X(g->x_len ? g->x_len : 1);
+            QCM_CUDA(cudaMemsetAsync(X.get(), 0, (g->x_len ? g->x_len : 1) * sizeof(double), r0.c.s));
+            for (std::size_t i = 0; i < nr; ++i) {
+                xn[i] = S[i].plan->x_len;
+                if (xn[i] != S[i].tst.twin.b.total) throw std::runtime_error("DMRG group: twin layout differs from its plan");
+                if (xn[i])
+                    QCM_CUDA(cudaMemcpyAsync(X.get() + xo[i], S[i].tst.twin.b.d.get(), xn[i] * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, r0.c.s));
+            }
+            jacobi_davidson_batched(*g, xo, xn, X.get(), r0.p.jcd_tol, r0.p.jcd_maxiter, ev, iters, true, &applies);
+            if (timing) { QCM_CUDA(cudaStreamSynchronize(r0.c.s)); tjd = now_s(); }
+            for (std::size_t i = 0; i < nr; ++i)
+                if (xn[i])
+                    QCM_CUDA(cudaMemcpyAsync(S[i].tst.twin.b.d.get(), X.get() + xo[i], xn[i] * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, r0.c.s));
+            QCM_CUDA(cudaStreamSynchronize(r0.c.s));
+        }
+        const double dt = (now_s() - tj) / double(nr);
+        for (std::size_t i = 0; i < nr; ++i) {
+            DevDMRG& d = *runs[i];
+            d.st.jd_s += dt;
+            d.st.hpsi_count += uint64_t(applies);
+            d.st.hpsi_flops += double(applies) * S[i].plan->flops;
+            d.last_iters = iters[i];
+            double E = 0;
+            TruncResults tr;
+            d.step_finish(S[i], ev[i], E, tr);
+            energies[i].push_back(E);
+            trunc[i].push_back(tr);
+        }
+        if (timing)
+            std::fprintf(stderr, "[group step %d] prepare %.4f merge %.4f jd %.4f (%d applies) finish %.4f\n", step, tj - tp,
+                         tm - tj, tjd - tm, applies, now_s() - tjd);
+    }
+    const double dt = (now_s() - t_start) / double(nr);
+    for (DevDMRG* d : runs) {
+        d->next_step = 0;
+        ++d->sweep_count;
+        d->st.total_s += dt;
     }
 }
 

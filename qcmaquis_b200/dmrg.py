@@ -87,6 +87,7 @@ _lib._sig("qcm_dmrg_pending_twin", c_int, c_void_p, P(c_double), c_uint64, P(c_u
 _lib._sig("qcm_dmrg_pending_export", c_int, c_void_p, c_int, c_void_p, ctypes.c_size_t, P(ctypes.c_size_t))
 _lib._sig("qcm_dmrg_sweep", c_int, c_void_p, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
+_lib._sig("qcm_dmrg_group_sweep", c_int, P(c_void_p), c_int, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_bond_dimensions", c_int, c_void_p, P(c_uint64))
 _lib._sig("qcm_dmrg_free", None, c_void_p)
 _U32 = P(ctypes.c_uint32)
@@ -271,6 +272,19 @@ class DMRG:
         tr = (TruncResult * n)()
         check(lib.qcm_dmrg_sweep(self.h, _lib.dptr(E), tr), "qcm_dmrg_sweep")
         return E, [{f: getattr(t, f) for f, _ in TruncResult._fields_} for t in tr]
+
+    @staticmethod
+    def group_sweep(runs):
+        """One sweep of independent two-site FP64 runs in lockstep (one merged plan group and one lockstep
+        Jacobi-Davidson per step): (energies[len(runs), steps], per run a list of truncation dicts)."""
+        runs = list(runs)
+        n, steps = len(runs), runs[0].steps
+        E = np.zeros((n, steps))
+        tr = (TruncResult * (n * steps))()
+        hs = (c_void_p * n)(*[r.h.value for r in runs])
+        check(lib.qcm_dmrg_group_sweep(hs, n, _lib.dptr(E), tr), "qcm_dmrg_group_sweep")
+        T = [{f: getattr(t, f) for f, _ in TruncResult._fields_} for t in tr]
+        return E, [T[i * steps:(i + 1) * steps] for i in range(n)]
 
     def run(self, stop_step: int):
         """Run the current sweep up to (not including) step stop_step: (energies, truncation dicts)."""
