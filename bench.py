@@ -489,7 +489,7 @@ def batched_solves(a, ctx, n=128, L=12, M=128):
     return out
 
 
-def group_sweeps(a, ctx, n=16, L=12, M=128, sweeps=3):
+def group_sweeps(a, ctx, n=16, L=12, M=128, sweeps=6):
     """Whole DMRG runs in lockstep: n independent two-site FP64 runs (synthetic Hamiltonians of L orbitals,
     N = L, seeds 1 .. n, const initial state with bond dimension 16, Mmax M) swept together by
     qcm_dmrg_group_sweep (one merged plan group and one lockstep JD per step) against the same runs swept one

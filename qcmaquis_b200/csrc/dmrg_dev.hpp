@@ -314,6 +314,7 @@ struct StepState {
     DTwoSite tst;
     std::unique_ptr<HeffPlan> plan;
     uint64_t key = 0;
+    bool resident = false;  // the plan's device buffers were kept from the previous sweep
     bool timing = false;
     double t0 = 0, t1 = 0, tt[8] = {};
 };
@@ -363,6 +364,12 @@ struct DevDMRG {
 
     // the phases of a two-site step (step = prepare, the JD on the plan and twin, finish)
     void step_prepare(StepState& S, int step);
+    // step_prepare in parts: the two-site tensor (device), the plan (host only: built, or re-bound from
+    // the previous sweep; runs of a group build theirs concurrently), the plan staged on the device (a
+    // group member's coefficient blocks only)
+    void step_prepare_site(StepState& S, int step);
+    void step_prepare_plan(StepState& S);
+    void step_prepare_stage(StepState& S, bool group);
     void step_finish(StepState& S, double eigenvalue, double& energy, TruncResults& tr);
     int last_iters = 0;  // JD iterations of the last step
 

@@ -299,6 +299,7 @@ struct HeffPlan {
     // a merged plan (merge_plans): the boundaries and coefficient blocks of its member plans are
     // addressed from these bases (its job offsets are relative to them); FP64 applies only
     bool merged = false;
+    bool lists_staged = false;  // the work lists are on the device (upload_plan with lists, restage_plan)
     const double* base_L = nullptr;
     const double* base_R = nullptr;
     const double* base_W = nullptr;
@@ -314,13 +315,17 @@ struct HeffPlan {
 
 std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& L, const DevBoundary& R, const MPOTensor& W,
                                           const Index& phys, const Index& left, const Index& right, bool bookkeeping);
-void upload_plan(HeffPlan& p);
+// Stages a plan on the device: its coefficient blocks (generated on the device) and, with lists, its
+// work lists and scratch.  A plan staged without lists is applied only inside a merged plan group
+// (merge_plans, which stages the group's own lists); restage_plan adds the lists when it is reused alone.
+void upload_plan(HeffPlan& p, bool lists = true);
 // Frees a plan's device buffers (work lists, coefficient blocks, scratch) and keeps its host work lists:
 // upload_plan stages it again, against boundaries of the same structure (rebind_plan).
 void release_plan_device(HeffPlan& p);
 // Frees only the scratch (T, S, partials, staging, mixed-form copies, coefficient-generation tables):
 // the work lists and coefficient blocks stay on the device (plan_resident_bytes of them), and
-// restage_plan makes the plan applicable again, against boundaries of the same structure.
+// restage_plan makes the plan applicable again, against boundaries of the same structure (staging the
+// work lists first when the plan was staged without them).
 void release_plan_scratch(HeffPlan& p);
 uint64_t plan_resident_bytes(const HeffPlan& p);
 void restage_plan(HeffPlan& p);

@@ -10,6 +10,9 @@
 // addressed from a common base (the lowest of the plans' buffer addresses), each job's
 // offset shifted by its plan's distance from that base.
 #include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cstdint>
 #include <stdexcept>
 #include <vector>
@@ -39,7 +42,7 @@ std::unique_ptr<HeffPlan> merge_plans(const std::vector<HeffPlan*>& plans, std::
     const double *bL = nullptr, *bR = nullptr, *bW = nullptr;
     for (const HeffPlan* p : plans) {
         if (!p || !p->L || !p->R || p->merged) throw std::runtime_error("plan group: a plan without boundaries, or a group");
-        if (!p->d_W.get() || p->d_units.size() < p->units.size()) throw std::runtime_error("plan group: a plan not staged on the device");
+        if (!p->d_W.get()) throw std::runtime_error("plan group: a plan without its coefficient blocks on the device");
         const double* l = p->L->data.get();
         const double* r = p->R->data.get();
         const double* w = p->d_W.get();
@@ -50,6 +53,24 @@ std::unique_ptr<HeffPlan> merge_plans(const std::vector<HeffPlan*>& plans, std::
     g->base_L = bL;
     g->base_R = bR;
     g->base_W = bW;
+    {
+        std::size_t nt = 0, nu = 0, nl = 0, ns = 0, nk = 0, ng = 0, no = 0;
+        std::size_t ntt[N_SHAPES] = {}, nut[N_SHAPES] = {},not_[N_SHAPES] = {}, nki[N_SHAPES] = {};
+        for (const HeffPlan* p : plans) {
+            nt += p->tjobs.size(); nu += p->units.size(); nl += p->line_b1.size(); ns += p->slice_off.size();
+            nk += p->klist.size(); ng += p->segs.size(); no += p->outs.size();
+            for (int sh = 0; sh < N_SHAPES; ++sh) {
+                ntt[sh] += p->ttiles[sh].size(); nut[sh] += p->utiles[sh].size();
+                not_[sh] += p->otiles[sh].size(); nki[sh] += p->kitems[sh].size();
+            }
+        }
+        g->tjobs.reserve(nt); g->units.reserve(nu); g->line_b1.reserve(nl); g->slice_off.reserve(ns);
+        g->klist.reserve(nk); g->segs.reserve(ng); g->outs.reserve(no);
+        for (int sh = 0; sh < N_SHAPES; ++sh) {
+            g->ttiles[sh].reserve(ntt[sh]); g->utiles[sh].reserve(nut[sh]);
+            g->otiles[sh].reserve(not_[sh]); g->kitems[sh].reserve(nki[sh]);
+        }
+    }
     xo.assign(plans.size(), 0);
     uint64_t xl = 0, tl = 0, sl = 0;
     uint64_t kl_items[N_SHAPES] = {};
@@ -102,7 +123,14 @@ std::unique_ptr<HeffPlan> merge_plans(const std::vector<HeffPlan*>& plans, std::
     uint64_t pl = 0;
     for (int sh = 0; sh < N_SHAPES; ++sh) pl = std::max<uint64_t>(pl, kl_items[sh] * shape_bm(sh) * shape_bn(sh));
     g->p_len = pl;
+    static const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
+    const auto t0 = std::chrono::steady_clock::now();
     upload_merged(*g);
+    if (tdbg) {
+        const auto t1 = std::chrono::steady_clock::now();
+        std::fprintf(stderr, "plan group: %zu plans, %zu T jobs, %zu units, %zu k-list words, upload %.4f s\n", plans.size(),
+                     g->tjobs.size(), g->units.size(), g->klist.size(), std::chrono::duration<double>(t1 - t0).count());
+    }
     return g;
 }
 

@@ -496,6 +496,7 @@ namespace {
 // explicitly (the plan's own buffers, or caller-provided memory of the same sizes).
 void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double* Tb, double* Sb, double* Pb) {
     cudaStream_t s = p.stream;
+    if (!p.lists_staged) throw std::runtime_error("heff apply: the plan's work lists are not on the device");
     if (ev) QCM_CUDA(cudaEventRecord(ev[0], s));
     QCM_CUDA(cudaMemsetAsync(y, 0, p.x_len * sizeof(double), s));
     launch_t<Sh16>(p, SHAPE_16, x, Tb, s);
@@ -518,6 +519,7 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
 // cores from the FP32 coefficient blocks, the L.S GEMM stays FP64.
 void apply_mixed_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, bool tc) {
     cudaStream_t s = p.stream;
+    if (!p.lists_staged) throw std::runtime_error("heff apply: the plan's work lists are not on the device");
     prepare_mixed(p, tc);
     if (ev) QCM_CUDA(cudaEventRecord(ev[0], s));
     QCM_CUDA(cudaMemsetAsync(y, 0, p.x_len * sizeof(double), s));
@@ -547,6 +549,7 @@ void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev)
 }
 
 void heff_tgemm_device(HeffPlan& p, const double* x, double* T) {
+    if (!p.lists_staged) throw std::runtime_error("heff T-GEMM: the plan's work lists are not on the device");
     launch_t<Sh16>(p, SHAPE_16, x, T, p.stream);
     launch_t<Sh32>(p, SHAPE_32, x, T, p.stream);
     launch_t<Sh64>(p, SHAPE_64, x, T, p.stream);
@@ -635,6 +638,7 @@ void release_plan_device(HeffPlan& p) {
     g.d_units.reset(); g.d_gin.reset(); g.d_line_major.reset(); g.d_smap_id.reset(); g.d_smap_slot.reset();
     g.d_m_ptr.reset(); g.d_m_other.reset(); g.d_m_op.reset(); g.d_o_ptr.reset(); g.d_o_in.reset(); g.d_err.reset();
     g.d_line_scale.reset(); g.d_m_scale.reset(); g.d_o_val.reset(); g.d_b_cs.reset(); g.d_b_pos.reset();
+    p.lists_staged = false;
 }
 
 void release_plan_scratch(HeffPlan& p) {
@@ -657,8 +661,17 @@ uint64_t plan_resident_bytes(const HeffPlan& p) {
     return b;
 }
 
+namespace {
+void stage_lists(HeffPlan& p);
+}
+
 void restage_plan(HeffPlan& p) {
     AllocStream scope(p.stream);
+    if (!p.lists_staged) {
+        stage_lists(p);
+        QCM_CUDA(cudaStreamSynchronize(p.stream));
+        return;
+    }
     p.d_T.alloc(p.t_len);
     p.d_S.alloc(p.s_len);
     p.d_P.alloc(p.p_len);
@@ -706,10 +719,37 @@ void upload_merged(HeffPlan& p) {
     p.d_T.alloc(p.t_len);
     p.d_S.alloc(p.s_len);
     p.d_P.alloc(p.p_len);
+    p.lists_staged = true;
     QCM_CUDA(cudaStreamSynchronize(s));
 }
 
-void upload_plan(HeffPlan& p) {
+namespace {
+
+// the work lists and the scratch of one plan on the device
+void stage_lists(HeffPlan& p) {
+    cudaStream_t s = p.stream;
+    p.d_tjobs.upload(p.tjobs, s);
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        p.d_ttiles[sh].upload(p.ttiles[sh], s);
+        p.d_utiles[sh].upload(p.utiles[sh], s);
+        p.d_otiles[sh].upload(p.otiles[sh], s);
+        p.d_kitems[sh].upload(p.kitems[sh], s);
+    }
+    p.d_units.upload(p.units, s);
+    p.d_line_b1.upload(p.line_b1, s);
+    p.d_slice_off.upload(p.slice_off, s);
+    p.d_klist.upload(p.klist, s);
+    p.d_segs.upload(p.segs, s);
+    p.d_outs.upload(p.outs, s);
+    p.d_T.alloc(p.t_len);
+    p.d_S.alloc(p.s_len);
+    p.d_P.alloc(p.p_len);
+    p.lists_staged = true;
+}
+
+}  // namespace
+
+void upload_plan(HeffPlan& p, bool lists) {
     cudaStream_t s = p.stream;
     for (const UnitD& u : p.units)
         if (u.wld < u.nl || u.wld % 4 || u.w_off % 4 || u.w_off + uint64_t(u.wld) * u.nk > p.w_len ||
@@ -729,23 +769,8 @@ void upload_plan(HeffPlan& p) {
             for (uint32_t i = 0; i < p.klist[t.pad]; ++i)
                 if (uint32_t(p.klist[t.pad + 1 + i] >> 4) * BK >= p.units[t.item].nk) throw std::runtime_error("heff plan: S tile k-step out of range");
         }
-    p.d_tjobs.upload(p.tjobs, s);
-    for (int sh = 0; sh < N_SHAPES; ++sh) {
-        p.d_ttiles[sh].upload(p.ttiles[sh], s);
-        p.d_utiles[sh].upload(p.utiles[sh], s);
-        p.d_otiles[sh].upload(p.otiles[sh], s);
-        p.d_kitems[sh].upload(p.kitems[sh], s);
-    }
-    p.d_units.upload(p.units, s);
-    p.d_line_b1.upload(p.line_b1, s);
-    p.d_slice_off.upload(p.slice_off, s);
+    if (lists) stage_lists(p);
     p.cg.upload(s);
-    p.d_klist.upload(p.klist, s);
-    p.d_segs.upload(p.segs, s);
-    p.d_outs.upload(p.outs, s);
-    p.d_T.alloc(p.t_len);
-    p.d_S.alloc(p.s_len);
-    p.d_P.alloc(p.p_len);
     // dense coefficient blocks, built once per plan and reused by every apply
     p.d_W.alloc(p.w_len ? p.w_len : 1);
     static const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;

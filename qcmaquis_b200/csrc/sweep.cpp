@@ -19,6 +19,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <stdexcept>
+#include <string>
 
 #include "dmrg_dev.hpp"
 
@@ -696,32 +697,47 @@ double DevDMRG::solve(HeffPlan& plan, DMPS& x, const std::function<void(std::siz
     return E;
 }
 
-void DevDMRG::step_prepare(StepState& S, int _site) {
+void DevDMRG::step_prepare_site(StepState& S, int _site) {
     S.step = _site;
     step_sites(_site, S.lr, S.site1, S.site2);
-    const int site1 = S.site1, site2 = S.site2;
     S.timing = std::getenv("QCM_SWEEP_TIMING") != nullptr;
-    auto mark = [&](int i) {
-        if (!S.timing) return;
-        QCM_CUDA(cudaStreamSynchronize(c.s));
-        S.tt[i] = now_s();
-    };
     S.t0 = now_s();
     S.tt[0] = S.t0;
-    make_left_paired(c, mps[site1]);
-    make_right_paired(c, mps[site2]);
+    make_left_paired(c, mps[S.site1]);
+    make_right_paired(c, mps[S.site2]);
     S.tst = DTwoSite();
-    S.tst.build(c, mps[site1], mps[site2]);
-    mark(1);
-    bool resident = false;
-    S.plan = plan_for(_site, *left_[site1], *right_[site2 + 1], ts_mpo[site1], S.tst.phys, S.tst.twin.left, S.tst.right,
-                      S.key, resident);
-    mark(2);
+    S.tst.build(c, mps[S.site1], mps[S.site2]);
+    if (S.timing) {
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        S.tt[1] = now_s();
+    }
+}
+
+void DevDMRG::step_prepare_plan(StepState& S) {
+    S.resident = false;
+    S.plan = plan_for(S.step, *left_[S.site1], *right_[S.site2 + 1], ts_mpo[S.site1], S.tst.phys, S.tst.twin.left,
+                      S.tst.right, S.key, S.resident);
     S.plan->stream = c.s;
-    if (resident) restage_plan(*S.plan);
-    else upload_plan(*S.plan);
+    S.tt[2] = now_s();
+}
+
+void DevDMRG::step_prepare_stage(StepState& S, bool group) {
+    if (group) {
+        // applied only inside the step's plan group: its coefficient blocks, not its work lists
+        if (!S.resident) upload_plan(*S.plan, false);
+    } else if (S.resident) {
+        restage_plan(*S.plan);
+    } else {
+        upload_plan(*S.plan);
+    }
     QCM_CUDA(cudaStreamSynchronize(c.s));
     S.t1 = now_s();
+}
+
+void DevDMRG::step_prepare(StepState& S, int _site) {
+    step_prepare_site(S, _site);
+    step_prepare_plan(S);
+    step_prepare_stage(S, false);
     st.plan_s += S.t1 - S.t0;
 }
 
@@ -816,11 +832,26 @@ void dmrg_group_sweep(const std::vector<DevDMRG*>& runs, std::vector<std::vector
     std::vector<StepState> S(nr);
     const bool timing = std::getenv("QCM_SWEEP_TIMING") != nullptr;
     for (int step = 0; step < n; ++step) {
+        // the runs' two-site tensors, then their plans (host schedules, built or re-bound from the previous
+        // sweep, one run per thread), then their coefficient blocks
         const double tp = now_s();
-        for (std::size_t i = 0; i < nr; ++i) runs[i]->step_prepare(S[i], step);
+        for (std::size_t i = 0; i < nr; ++i) runs[i]->step_prepare_site(S[i], step);
+        std::vector<std::string> err(nr);
+#pragma omp parallel for schedule(dynamic, 1)
+        for (long i = 0; i < long(nr); ++i) {
+            try {
+                runs[std::size_t(i)]->step_prepare_plan(S[std::size_t(i)]);
+            } catch (const std::exception& e) {
+                err[std::size_t(i)] = e.what();
+            }
+        }
+        for (const std::string& e : err)
+            if (!e.empty()) throw std::runtime_error(e);
+        for (std::size_t i = 0; i < nr; ++i) runs[i]->step_prepare_stage(S[i], true);
         double tm = 0, tjd = 0;
         // one plan group, one lockstep Jacobi-Davidson over every run's two-site problem
         const double tj = now_s();
+        for (DevDMRG* d : runs) d->st.plan_s += (tj - tp) / double(nr);
         std::vector<HeffPlan*> plans(nr);
         for (std::size_t i = 0; i < nr; ++i) plans[i] = S[i].plan.get();
         std::vector<uint64_t> xo, xn(nr);
