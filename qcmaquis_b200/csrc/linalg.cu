@@ -169,8 +169,12 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
     __syncthreads();
     const uint32_t cp = c + (c & 1u);  // players, padded to even
     const double tol2 = (JEPS * double(r)) * (JEPS * double(r));
-    // lanes per pair: 16, or 8 when the pairs of a round outnumber the half-warps, so that a round
-    // is one pass of the CTA (its latency chain is the round's cost)
+    // lanes per pair: a round costs about the larger of the CTA's instructions over its four
+    // schedulers and one lane group's dependent chain; each active warp pays the fixed part of a pair
+    // (indices, reduction, rotation angle: about JFIX instructions) once per pair it holds, and every
+    // lane JELEM instructions per element pair of its share of the two columns (dot product, G and Q
+    // rotations).  Fewer lanes per pair spread the fixed part over more pairs per warp; more lanes
+    // shorten the chain when the columns are long or the pairs few.
     const uint32_t gs = cp / 2 > uint32_t(JTHR / 16) ? 8u : 16u;
     const uint32_t grp = uint32_t(tid) / gs, hl = uint32_t(tid) % gs, ngrp = JTHR / gs;
     for (int sweep = 0; sweep < JMAX_SWEEPS && c > 1; ++sweep) {
@@ -193,8 +197,12 @@ __global__ void __launch_bounds__(JTHR) k_jacobi_svd(const SvdJob* __restrict__ 
                 uint32_t p = 0, q = 0;
                 bool act = t < cp / 2;
                 if (act) {
-                    p = i0 == 0 ? 0 : (i0 - 1 + k) % (cp - 1) + 1;
-                    q = i1 == 0 ? 0 : (i1 - 1 + k) % (cp - 1) + 1;
+                    // (i - 1 + k) mod (cp - 1) + 1 with i - 1 + k < 2 (cp - 1)
+                    uint32_t xp = i0 - 1 + k, xq = i1 - 1 + k;
+                    xp -= xp >= cp - 1 ? cp - 1 : 0u;
+                    xq -= xq >= cp - 1 ? cp - 1 : 0u;
+                    p = i0 == 0 ? 0 : xp + 1;
+                    q = i1 == 0 ? 0 : xq + 1;
                     act = p < c && q < c;
                 }
                 double2* gp = reinterpret_cast<double2*>(G + uint64_t(p) * rp);
