@@ -429,6 +429,10 @@ typedef struct {
     /* boundary steps whose schedule was built, and those that ran the previous sweep's schedule of the
      * same step again (same structure: old boundary, site tensor sectors and block layouts) */
     uint64_t bsteps_built, bsteps_reused;
+    /* device bytes of the sweep's boundaries after a step (the largest since the run was created or
+     * its boundary budget last set), and the boundaries moved to pinned host memory and back under
+     * qcm_dmrg_set_boundary_budget */
+    uint64_t boundary_bytes_peak, boundaries_offloaded, boundaries_fetched;
 } qcm_dmrg_stats;
 
 /* mpo: single-site QC MPO; nup/ndown: u1_total_charge1/2.  Builds the const
@@ -510,6 +514,14 @@ int qcm_dmrg_sweep(qcm_dmrg* d, double* energies, qcm_trunc_result* trunc);
  * subspace by classical Gram-Schmidt twice instead of the single solve's modified Gram-Schmidt). */
 int qcm_dmrg_group_sweep(qcm_dmrg* const* runs, int n, double* energies, qcm_trunc_result* trunc);
 int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* stats);
+/* Boundary residency (the reference keeps only the active boundaries in memory and moves the others
+ * to its storage directory, utils/storage.h:88-330, ts_optimize.hpp:151-182): after every step the
+ * boundaries no later step reads before the next half-sweep rebuilds them are released, and with
+ * bytes > 0 the device copies of the others, farthest from the next step's two first, move to pinned
+ * host memory until the device holds at most bytes of boundaries (the next step's two always stay);
+ * a step brings its two back before it runs.  bytes = 0: no limit (the default).  Energies and
+ * truncations do not depend on the budget. */
+int qcm_dmrg_set_boundary_budget(qcm_dmrg* d, uint64_t bytes);
 /* Run the current sweep up to (not including) step stop_step (steps_per_sweep
  * completes it); energies / trunc receive one entry per step run (may be NULL),
  * *n_steps their count. */

@@ -627,7 +627,23 @@ int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* s) {
     s->plans_reused = t.plans_reused;
     s->bsteps_built = t.bsteps_built;
     s->bsteps_reused = t.bsteps_reused;
+    s->boundary_bytes_peak = t.boundary_bytes_peak;
+    s->boundaries_offloaded = t.boundaries_offloaded;
+    s->boundaries_fetched = t.boundaries_fetched;
     return QCM_OK;
+}
+
+int qcm_dmrg_set_boundary_budget(qcm_dmrg* d, uint64_t bytes) {
+    QCM_TRY
+    if (!d) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_set_boundary_budget: NULL argument");
+    QCM_CUDA(cudaSetDevice(d->ctx->device));
+    qcm::AllocStream scope(d->ctx->stream);
+    d->e->boundary_budget = bytes;
+    d->e->st.boundary_bytes_peak = 0;  // the peak counts from here
+    d->e->bnd_trim(d->e->next_step);
+    QCM_CUDA(cudaStreamSynchronize(d->ctx->stream));
+    return QCM_OK;
+    QCM_CATCH
 }
 
 int qcm_dmrg_bond_dimensions(const qcm_dmrg* d, uint64_t* dims) {

@@ -305,6 +305,8 @@ struct DMRGStats {
     double hpsi_flops64 = 0;
     double hpsi_flops = 0, hpsi_ms = 0;  // reference flop count and device time of the H.psi applies
     double plan_s = 0, jd_s = 0, trunc_s = 0, boundary_s = 0, total_s = 0;
+    uint64_t boundary_bytes_peak = 0;  // device bytes of the sweep's boundaries, largest after a step
+    uint64_t boundaries_offloaded = 0, boundaries_fetched = 0;  // moves to and from pinned host memory
 };
 
 // One two-site step between its phases: the two-site tensor and its staged plan (step_prepare), then
@@ -363,6 +365,15 @@ struct DevDMRG {
     void step_sites(int step, int& lr, int& site1, int& site2) const;
 
     // the phases of a two-site step (step = prepare, the JD on the plan and twin, finish)
+    // device bytes allowed for the sweep's boundaries (0: no limit); over it, boundaries move to pinned
+    // host memory and back (the reference's boundary storage, storage.h, as host offload)
+    uint64_t boundary_budget = 0;
+    // boundary residency: the boundaries a step uses are brought to the device (bnd_use); after a step,
+    // those no later step reads before the next half-sweep rebuilds them are released, and over the
+    // budget the device copies farthest from the next step's two are moved to pinned host memory
+    // (bnd_trim, with the step that comes next)
+    void bnd_use(DevBoundary* b);
+    void bnd_trim(int next_step);
     void step_prepare(StepState& S, int step);
     // step_prepare in parts: the two-site tensor (device), the plan (host only: built, or re-bound from
     // the previous sweep; runs of a group build theirs concurrently), the plan staged on the device (a
@@ -393,6 +404,7 @@ struct DevDMRG {
     uint64_t bstep_cache_bytes_ = 0, bstep_cache_budget_ = 0;
     BStepCache* bstep_cache_for(int step);
     void bstep_cache_done(int step);
+
     std::unique_ptr<HeffPlan> plan_for(int step, const DevBoundary& Lb, const DevBoundary& Rb, const MPOTensor& W,
                                        const Index& phys, const Index& left, const Index& right, uint64_t& key,
                                        bool& resident);

@@ -62,6 +62,12 @@ struct DevBoundary {
     // structure hash of idx (boundary_key), computed on first use: the index of a boundary is not
     // changed after the boundary is made
     mutable uint64_t key = 0;
+    // a copy in pinned host memory (host_len doubles), made when the boundary is moved out of device
+    // memory (its data released until it is fetched back); a boundary's values never change, so the
+    // copy stays valid and a later eviction only releases the device data
+    std::shared_ptr<double> host;
+    uint64_t host_len = 0;
+    bool on_device() const { return data.get() != nullptr || !host; }
 };
 
 // Hash of structure (sectors, cohorts, block offsets, conjugate scales) for the plan caches

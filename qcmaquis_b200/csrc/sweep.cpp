@@ -474,6 +474,7 @@ void DevDMRG::init_boundaries(int site) {
     }
     next_step = site;
     QCM_CUDA(cudaStreamSynchronize(c.s));
+    bnd_trim(site);
 }
 
 void DevDMRG::set_ortho(std::vector<std::vector<DMPS>> states_rp) {
@@ -603,6 +604,54 @@ BStepCache* DevDMRG::bstep_cache_for(int step) {
     return &e;
 }
 
+void DevDMRG::bnd_use(DevBoundary* b) {
+    if (!b || b->data.get() || !b->host) return;
+    b->data.alloc(b->host_len);
+    QCM_CUDA(cudaMemcpyAsync(b->data.get(), b->host.get(), b->host_len * sizeof(double), cudaMemcpyHostToDevice, c.s));
+    ++st.boundaries_fetched;
+}
+
+void DevDMRG::bnd_trim(int next) {
+    const int n = steps_per_sweep();
+    next = ((next % n) + n) % n;
+    int lb = 0, rb = 0;  // the boundaries the next step reads
+    if (p.single_site) {
+        const int site = next < L ? next : 2 * L - 1 - next;
+        lb = site; rb = site + 1;
+    } else {
+        int lr = 0, s1 = 0, s2 = 0;
+        step_sites(next, lr, s1, s2);
+        lb = s1; rb = s2 + 1;
+    }
+    auto bytes = [](const DevBoundary* b) { return b && b->data.get() ? uint64_t(b->data.size()) * sizeof(double) : 0; };
+    uint64_t tot = 0;
+    for (const auto& b : left_) tot += bytes(b.get());
+    for (const auto& b : right_) tot += bytes(b.get());
+    while (boundary_budget && tot > boundary_budget) {
+        // the device-resident boundary farthest from the next step's two
+        DevBoundary* far = nullptr;
+        int fd = -1;
+        for (int i = 0; i < int(left_.size()); ++i)
+            if (i != lb && bytes(left_[std::size_t(i)].get()) && std::abs(i - lb) > fd) { fd = std::abs(i - lb); far = left_[std::size_t(i)].get(); }
+        for (int j = 0; j < int(right_.size()); ++j)
+            if (j != rb && bytes(right_[std::size_t(j)].get()) && std::abs(j - rb) > fd) { fd = std::abs(j - rb); far = right_[std::size_t(j)].get(); }
+        if (!far) break;
+        tot -= bytes(far);
+        if (!far->host) {
+            double* h = nullptr;
+            const uint64_t len = far->data.size();
+            QCM_CUDA(cudaMallocHost(&h, len * sizeof(double)));
+            far->host = std::shared_ptr<double>(h, [](double* q) { cudaFreeHost(q); });
+            far->host_len = len;
+            QCM_CUDA(cudaMemcpyAsync(h, far->data.get(), len * sizeof(double), cudaMemcpyDeviceToHost, c.s));
+            QCM_CUDA(cudaStreamSynchronize(c.s));
+        }
+        far->data.reset();
+        ++st.boundaries_offloaded;
+    }
+    st.boundary_bytes_peak = std::max(st.boundary_bytes_peak, tot);
+}
+
 void DevDMRG::bstep_cache_done(int step) {
     BStepCache& e = bstep_cache_[std::size_t(step)];
     ++(e.hit ? st.bsteps_reused : st.bsteps_built);
@@ -703,6 +752,8 @@ void DevDMRG::step_prepare_site(StepState& S, int _site) {
     S.timing = std::getenv("QCM_SWEEP_TIMING") != nullptr;
     S.t0 = now_s();
     S.tt[0] = S.t0;
+    bnd_use(left_[S.site1].get());
+    bnd_use(right_[S.site2 + 1].get());
     make_left_paired(c, mps[S.site1]);
     make_right_paired(c, mps[S.site2]);
     S.tst = DTwoSite();
@@ -773,6 +824,9 @@ void DevDMRG::step_finish(StepState& S, double E, double& energy, TruncResults& 
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_left_[o][site2] = ortho_left_step(c, mps[site1], ortho_rp[o][site1], ortho_left_[o][site1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
+        // the right-to-left half-sweep rebuilds every right boundary but the last: this one is done
+        if (site2 + 1 < L) right_[site2 + 1].reset();
+        if (site2 == L - 1) left_[site2].reset();  // no two-site step reads the last left boundary
         st.boundary_s += now_s() - t3;
     } else {
         tr = p.heev ? tst.predict_split(c, false, p.Mmax, p.cutoff, alpha, *right_[site2 + 1], mpo[site2], mps[site1], mps[site2])
@@ -789,8 +843,12 @@ void DevDMRG::step_finish(StepState& S, double E, double& energy, TruncResults& 
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_right_[o][site2] = ortho_right_step(c, mps[site2], ortho_lp[o][site2], ortho_right_[o][site2 + 1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
+        // the next left-to-right half-sweep rebuilds every left boundary but the first
+        if (site1 > 0) left_[site1].reset();
+        if (site2 == 1) right_[site2].reset();  // no two-site step reads the first right boundary
         st.boundary_s += now_s() - t3;
     }
+    bnd_trim(_site + 1);
     if (S.timing) {
         const double tend = now_s();
         std::fprintf(stderr,
@@ -909,6 +967,8 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
     const int lr = _site < L ? 1 : -1;
     const int site = _site < L ? _site : 2 * L - 1 - _site;
     const double t0 = now_s();
+    bnd_use(left_[site].get());
+    bnd_use(right_[site + 1].get());
     make_right_paired(c, mps[site]);
     DMPS x = packed_right(c, mps[site]);
     // solve_site_problem with the single-site MPO tensor (ss_optimize.hpp:120)
@@ -945,6 +1005,9 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_left_[o][site + 1] = ortho_left_step(c, mps[site], ortho_rp[o][site], ortho_left_[o][site]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
+        // the right-to-left half-sweep rebuilds every right boundary but the last; none reads left_[L]
+        if (site + 1 < L) right_[site + 1].reset();
+        else left_[site + 1].reset();
         st.boundary_s += now_s() - t3;
     } else {
         // ss_optimize.hpp:174-186
@@ -958,8 +1021,12 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
         for (std::size_t o = 0; o < ortho_rp.size(); ++o)
             ortho_right_[o][site] = ortho_right_step(c, mps[site], ortho_lp[o][site], ortho_right_[o][site + 1]);
         QCM_CUDA(cudaStreamSynchronize(c.s));
+        // the next left-to-right half-sweep rebuilds every left boundary but the first; none reads right_[0]
+        if (site > 0) left_[site].reset();
+        else right_[site].reset();
         st.boundary_s += now_s() - t3;
     }
+    bnd_trim(_site + 1);
 }
 
 void DevDMRG::run_until(int stop, std::vector<double>& energies, std::vector<TruncResults>& trunc) {
@@ -988,6 +1055,8 @@ void DevDMRG::pending_twin(std::vector<double>& twin) {
     if (p.single_site) throw std::runtime_error("DMRG: pending site problems of two-site sweeps only");
     int lr, site1, site2;
     step_sites(next_step, lr, site1, site2);
+    bnd_use(left_[site1].get());
+    bnd_use(right_[site2 + 1].get());
     make_left_paired(c, mps[site1]);
     make_right_paired(c, mps[site2]);
     DTwoSite tst;
@@ -1003,6 +1072,8 @@ std::unique_ptr<HeffPlan> DevDMRG::pending_plan(std::vector<double>* twin, Index
     if (p.single_site) throw std::runtime_error("DMRG: pending site problems of two-site sweeps only");
     int lr, site1, site2;
     step_sites(next_step, lr, site1, site2);
+    bnd_use(left_[site1].get());
+    bnd_use(right_[site2 + 1].get());
     make_left_paired(c, mps[site1]);
     make_right_paired(c, mps[site2]);
     DTwoSite tst;

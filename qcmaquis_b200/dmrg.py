@@ -56,7 +56,8 @@ class DMRGStats(ctypes.Structure):
     _fields_ = [("hpsi_count", c_uint64), ("hpsi_flops", c_double), ("plan_s", c_double), ("jd_s", c_double),
                 ("trunc_s", c_double), ("boundary_s", c_double), ("total_s", c_double),
                 ("hpsi_count_fp64", c_uint64), ("hpsi_flops_fp64", c_double), ("plans_built", c_uint64),
-                ("plans_reused", c_uint64), ("bsteps_built", c_uint64), ("bsteps_reused", c_uint64)]
+                ("plans_reused", c_uint64), ("bsteps_built", c_uint64), ("bsteps_reused", c_uint64),
+                ("boundary_bytes_peak", c_uint64), ("boundaries_offloaded", c_uint64), ("boundaries_fetched", c_uint64)]
 
 
 _lib._sig("qcm_jd_solve", c_int, c_void_p, P(c_double), c_double, c_int, P(c_double), P(c_double), P(c_int))
@@ -88,6 +89,7 @@ _lib._sig("qcm_dmrg_pending_export", c_int, c_void_p, c_int, c_void_p, ctypes.c_
 _lib._sig("qcm_dmrg_sweep", c_int, c_void_p, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
 _lib._sig("qcm_dmrg_group_sweep", c_int, P(c_void_p), c_int, P(c_double), P(TruncResult))
+_lib._sig("qcm_dmrg_set_boundary_budget", c_int, c_void_p, c_uint64)
 _lib._sig("qcm_dmrg_bond_dimensions", c_int, c_void_p, P(c_uint64))
 _lib._sig("qcm_dmrg_free", None, c_void_p)
 _U32 = P(ctypes.c_uint32)
@@ -371,6 +373,11 @@ class DMRG:
         sites = [st for state in states for st in state]
         descs, ptrs, keep = _pack_sites(sites)
         check(lib.qcm_dmrg_set_ortho(self.h, len(states), descs, ptrs), "qcm_dmrg_set_ortho")
+
+    def set_boundary_budget(self, nbytes: int):
+        """Device bytes allowed for the sweep's boundaries (0: no limit); over it, boundaries move to
+        pinned host memory and back (qcm_dmrg_set_boundary_budget)."""
+        check(lib.qcm_dmrg_set_boundary_budget(self.h, int(nbytes)), "qcm_dmrg_set_boundary_budget")
 
     def stats(self) -> dict:
         s = DMRGStats()

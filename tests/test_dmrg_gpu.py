@@ -99,7 +99,8 @@ def test_jd_matches_oracle_step_energy(gpu_ctx, L, M, sw, step):
     assert abs(np.dot(vec, hv) - ev) < 1e-9
 
 
-@pytest.mark.parametrize("L,M,sweeps,gauge", [(6, 16, 3, None), (8, 32, 3, None), (8, 32, 2, 3)])
+@pytest.mark.parametrize("L,M,sweeps,gauge", [(6, 16, 3, None), (8, 32, 3, None), (8, 32, 2, 3), (8, 24, 8, None),
+                                              (12, 128, 4, None)])
 def test_sweep_energies_match_oracle(gpu_ctx, L, M, sweeps, gauge):
     """Both engines start from the oracle's initial MPS.  (The const initial state itself is
     not reproducible across LAPACK implementations: normalize_left QR-factorises rank-1
