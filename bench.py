@@ -371,6 +371,38 @@ def measure_adjoint(a, plan, x_host, mpo, site):
                     "in the scales) is the consistency check"}
 
 
+def measure_streamed(a, plan, xd, yd, flush, info):
+    """The same H.psi with its coefficient blocks streamed through a bounded scratch (generated chunk by
+    chunk in every apply instead of kept, the form for problems whose blocks do not fit): per chunk size the
+    time per apply and of its S phase (CUDA events, L2 flushed), and whether the result equals the kept
+    form's to the bit."""
+    import torch
+    plan.apply_device(xd.data_ptr(), yd.data_ptr())
+    torch.cuda.synchronize()
+    y_kept = yd.clone()
+    out = {"coefficient_block_bytes": 8 * int(info["w_len"]), "chunks": []}
+    try:
+        for mib in (512, 128):
+            plan.stream_coefficients(mib * 2**20)
+            for _ in range(3):
+                plan.apply_device(xd.data_ptr(), yd.data_ptr())
+            tot, sph = [], []
+            for _ in range(10):
+                flush.zero_()
+                torch.cuda.synchronize()
+                ms = plan.profile(xd.data_ptr(), yd.data_ptr())
+                tot.append(ms[3])
+                sph.append(ms[1])
+            torch.cuda.synchronize()
+            out["chunks"].append({"chunk_bytes": mib * 2**20, "launches_per_apply": int(plan.info["launches"]),
+                                  "ms_per_apply": float(np.mean(tot)), "s_phase_ms": float(np.mean(sph)),
+                                  "gflops": info["flops"] / (np.mean(tot) * 1e-3) / 1e9,
+                                  "bitwise_equal_to_kept": bool(torch.equal(yd, y_kept))})
+    finally:
+        plan.stream_coefficients(0)
+    return out
+
+
 def sweep_record(d, E, tr, dt, st0, st1, s):
     tw = np.array([t["truncated_weight"] for t in tr])
     return {"sweep": s, "seconds": dt, "energy_min": float(E.min()), "truncated_weight_max": float(tw.max()),
@@ -646,6 +678,7 @@ def run_b200(a, world, rank, local, pg):
                                                     blob, site1, x_host, form="mixed_tc")
         extras["mixed"] = mixed
         extras["adjoint"] = measure_adjoint(a, plan, x_host, mpo, site1)
+        extras["streamed_coefficients"] = measure_streamed(a, plan, xd, yd, flush, info)
         herm = boundary_storage(d, plan)
         del plan, d
         dn, pn, _, _ = device_problem(ctx, h, V, sites, site1, a.M, hermitian=False)

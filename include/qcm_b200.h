@@ -220,6 +220,13 @@ int qcm_heff_get_info(const qcm_heff* h, qcm_heff_info* info);
  * synchronous.  Replaces ietl::mult -> super_hamil_mv
  * (solver/ietl_interface_dv.h:112-118, solver/super_hamil_mv.hpp:100-155). */
 int qcm_heff_apply(qcm_heff* h, const double* x, double* y);
+/* Bounds the plan's coefficient blocks (the dense S-build operands, qcm_heff_info.w_len doubles) to
+ * max_bytes of device memory: every FP64 apply then generates them chunk by chunk (consecutive S-build
+ * units, at most max_bytes each unless one unit is larger) and runs each chunk's S-GEMM tiles from one
+ * scratch, with the same result to the bit; the plan is staged again.  max_bytes = 0 keeps them
+ * whole.  For problems whose blocks do not fit (they grow with the MPO bond dimension times the
+ * squared sector sizes).  Mixed-form applies and plan groups need them whole (QCM_ERR_ARG). */
+int qcm_heff_stream_coefficients(qcm_heff* h, uint64_t max_bytes);
 /* Same with device pointers, enqueued on the context stream (asynchronous). */
 int qcm_heff_apply_device(qcm_heff* h, const double* x_dev, double* y_dev);
 
@@ -522,6 +529,10 @@ int qcm_dmrg_get_stats(const qcm_dmrg* d, qcm_dmrg_stats* stats);
  * a step brings its two back before it runs.  bytes = 0: no limit (the default).  Energies and
  * truncations do not depend on the budget. */
 int qcm_dmrg_set_boundary_budget(qcm_dmrg* d, uint64_t bytes);
+/* Coefficient blocks of the H_eff plans the run builds from here on bounded to max_bytes each
+ * (qcm_heff_stream_coefficients); 0 keeps them whole (the default).  FP64 runs only, not in
+ * qcm_dmrg_group_sweep.  Energies and truncations do not depend on it. */
+int qcm_dmrg_set_coefficient_budget(qcm_dmrg* d, uint64_t max_bytes);
 /* Run the current sweep up to (not including) step stop_step (steps_per_sweep
  * completes it); energies / trunc receive one entry per step run (may be NULL),
  * *n_steps their count. */

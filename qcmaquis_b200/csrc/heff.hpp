@@ -235,6 +235,10 @@ struct CoefGen {
     void upload(cudaStream_t s);
     // W (w_len doubles) = coefficient blocks; waits for the stream and throws if a term had no slot
     void generate(double* W, cudaStream_t s);
+    // the blocks of units [u0, u1) (elements [w0, w1) of the whole, written from W on), without the
+    // check of generate; check_generated reads and clears the error flag of the generations so far
+    void generate_range(double* W, uint32_t u0, uint32_t u1, uint64_t w0, uint64_t w1, cudaStream_t s);
+    void check_generated(cudaStream_t s);
 };
 
 struct HeffAdjointWork;  // work lists and buffers of the adjoint, made on its first call
@@ -286,7 +290,17 @@ struct HeffPlan {
     DBuf<TileD> d_utiles[N_SHAPES];
     DBuf<uint32_t> d_line_b1;
     DBuf<uint64_t> d_slice_off;
-    DBuf<double> d_W;
+    DBuf<double> d_W;  // the coefficient blocks (w_len doubles), or one chunk of them when streamed
+    // coefficient blocks generated chunk by chunk inside every apply instead of kept
+    // (stream_coefficients): units [u0, u1) with their blocks [w0, w1) and, per tile shape, their
+    // S-GEMM tiles [t0, t1)
+    struct WChunk {
+        uint32_t u0 = 0, u1 = 0;
+        uint64_t w0 = 0, w1 = 0;
+        uint32_t t0[N_SHAPES] = {}, t1[N_SHAPES] = {};
+    };
+    std::vector<WChunk> wchunks;
+    bool streamed() const { return !wchunks.empty(); }
     DBuf<uint16_t> d_klist;
     DBuf<SegD> d_segs;
     DBuf<OutD> d_outs;
@@ -325,6 +339,13 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& L, const DevBoundar
 // work lists and scratch.  A plan staged without lists is applied only inside a merged plan group
 // (merge_plans, which stages the group's own lists); restage_plan adds the lists when it is reused alone.
 void upload_plan(HeffPlan& p, bool lists = true);
+// Bounds a plan's coefficient blocks to max_doubles on the device (0 or w_len <= max_doubles: kept
+// whole): the units are cut into consecutive chunks of at most max_doubles of blocks (a larger unit
+// is a chunk of its own) and every FP64 apply generates each chunk into one scratch and runs its
+// S-GEMM tiles from it, in the same order and with the same arithmetic as the kept blocks (the apply's
+// result is the same to the bit).  Set before upload_plan; the mixed forms and plan groups need the
+// blocks kept.
+void stream_coefficients(HeffPlan& p, uint64_t max_doubles);
 // Frees a plan's device buffers (work lists, coefficient blocks, scratch) and keeps its host work lists:
 // upload_plan stages it again, against boundaries of the same structure (rebind_plan).
 void release_plan_device(HeffPlan& p);

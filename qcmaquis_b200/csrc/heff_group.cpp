@@ -43,6 +43,7 @@ std::unique_ptr<HeffPlan> merge_plans(const std::vector<HeffPlan*>& plans, std::
     for (const HeffPlan* p : plans) {
         if (!p || !p->L || !p->R || p->merged) throw std::runtime_error("plan group: a plan without boundaries, or a group");
         if (!p->d_W.get()) throw std::runtime_error("plan group: a plan without its coefficient blocks on the device");
+        if (p->streamed()) throw std::runtime_error("plan group: a plan with streamed coefficient blocks");
         const double* l = p->L->data.get();
         const double* r = p->R->data.get();
         const double* w = p->d_W.get();

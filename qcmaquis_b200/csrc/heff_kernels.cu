@@ -145,7 +145,7 @@ template <class S>
 __global__ void __launch_bounds__(NTHR, 5) k_sgemm(const UnitD* __restrict__ units, const TileD* __restrict__ tiles,
                                                 const uint32_t* __restrict__ line_b1, const uint64_t* __restrict__ slice_off,
                                                 const uint16_t* __restrict__ klist, const double* __restrict__ W,
-                                                const double* __restrict__ T, double* __restrict__ Sm) {
+                                                const double* __restrict__ T, double* __restrict__ Sm, uint64_t w0) {
     __shared__ Stage<S> st[2];
     const TileD tile = tiles[blockIdx.x];
     const UnitD U = units[tile.item];
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(NTHR, 5) k_sgemm(const UnitD* __restrict__ uni
     // only the k-steps whose coefficient block (this tile's lines x 16 slices) holds an entry
     const uint16_t* ks = klist + tile.pad;
     const uint32_t nsteps = ks[0];
-    const double* Wu = W + U.w_off;
+    const double* Wu = W + (U.w_off - w0);  // W holds the coefficient blocks from element w0 on
     // 16-byte chunks (2 doubles): W_u columns (ld wld, rows nl .. wld - 1 zero) and T slices (sst
     // apart, 16-byte aligned) are read 16 bytes at a time; a chunk past the slice's ne elements
     // is not read, one that straddles ne reads the slice's padding into columns the epilogue drops
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ u
                                                  const uint32_t* __restrict__ o_ptr, const uint32_t* __restrict__ o_in,
                                                  const double* __restrict__ o_val, const int32_t* __restrict__ b_pos,
                                                  const double* __restrict__ b_cs, uint32_t b_aux, double* __restrict__ W,
-                                                 uint32_t* __restrict__ err) {
+                                                 uint64_t w0, uint32_t* __restrict__ err) {
     __shared__ uint32_t sid[WG_SMAP], sslot[WG_SMAP];
     __shared__ WGenInD sin[WG_NST];
     const WGenUnitD U = units[blockIdx.x];
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ u
     for (uint32_t line = threadIdx.x; line < U.nl; line += blockDim.x) {
         const uint32_t m = line_major[U.line0 + line];
         const double lsc = line_scale[U.line0 + line];
-        double* Wl = W + U.w_off + line;
+        double* Wl = W + (U.w_off - w0) + line;
         for (uint32_t e = m_ptr[m]; e < m_ptr[m + 1]; ++e) {
             const uint32_t x = m_other[e], op = m_op[e];
             const double wsc = __dmul_rn(m_scale[e], lsc);
@@ -347,19 +347,32 @@ void CoefGen::upload(cudaStream_t s) {
 }
 
 void CoefGen::generate(double* W, cudaStream_t s) {
-    if (w_len) QCM_CUDA(cudaMemsetAsync(W, 0, w_len * sizeof(double), s));
-    if (units.empty()) return;
+    generate_range(W, 0, uint32_t(units.size()), 0, w_len, s);
+    check_generated(s);
+}
+
+void CoefGen::generate_range(double* W, uint32_t u0, uint32_t u1, uint64_t w0, uint64_t w1, cudaStream_t s) {
+    if (w1 > w0) QCM_CUDA(cudaMemsetAsync(W, 0, (w1 - w0) * sizeof(double), s));
+    if (u1 <= u0) return;
     if (d_units.size() < units.size()) throw std::runtime_error("coefficient tables: not uploaded");
-    d_err.alloc(1);
-    QCM_CUDA(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
-    k_wgen<<<unsigned(units.size()), WG_THR, 0, s>>>(d_units.get(), d_gin.get(), nst, d_line_major.get(), d_line_scale.get(),
-                                                     d_smap_id.get(), d_smap_slot.get(), d_m_ptr.get(), d_m_other.get(),
-                                                     d_m_op.get(), d_m_scale.get(), d_o_ptr.get(), d_o_in.get(), d_o_val.get(),
-                                                     d_b_pos.get(), d_b_cs.get(), b_aux, W, d_err.get());
+    if (u1 > units.size()) throw std::runtime_error("coefficient tables: unit range outside the plan");
+    if (d_err.size() < 1) {
+        d_err.alloc(1);
+        QCM_CUDA(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
+    }
+    k_wgen<<<unsigned(u1 - u0), WG_THR, 0, s>>>(d_units.get() + u0, d_gin.get() + std::size_t(u0) * nst, nst, d_line_major.get(),
+                                                d_line_scale.get(), d_smap_id.get(), d_smap_slot.get(), d_m_ptr.get(),
+                                                d_m_other.get(), d_m_op.get(), d_m_scale.get(), d_o_ptr.get(), d_o_in.get(),
+                                                d_o_val.get(), d_b_pos.get(), d_b_cs.get(), b_aux, W, w0, d_err.get());
     QCM_CUDA(cudaGetLastError());
+}
+
+void CoefGen::check_generated(cudaStream_t s) {
+    if (units.empty() || d_err.size() < 1) return;
     uint32_t h = 0;
     QCM_CUDA(cudaMemcpyAsync(&h, d_err.get(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     QCM_CUDA(cudaStreamSynchronize(s));
+    QCM_CUDA(cudaMemsetAsync(d_err.get(), 0, sizeof(uint32_t), s));
     if (h) throw std::runtime_error("coefficient tables: a term has no slice slot");
 }
 
@@ -477,7 +490,16 @@ template <class S>
 void launch_s(HeffPlan& p, int sh, const double* Tb, double* Sb, cudaStream_t s) {
     if (!p.utiles[sh].empty())
         k_sgemm<S><<<unsigned(p.utiles[sh].size()), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get(), p.d_line_b1.get(),
-                                                                  p.d_slice_off.get(), p.d_klist.get(), p.w_data(), Tb, Sb);
+                                                                  p.d_slice_off.get(), p.d_klist.get(), p.w_data(), Tb, Sb, 0);
+}
+
+// the S-GEMM tiles of one coefficient chunk, reading the chunk's blocks from the plan's scratch
+template <class S>
+void launch_s_range(HeffPlan& p, int sh, const HeffPlan::WChunk& ch, const double* Tb, double* Sb, cudaStream_t s) {
+    if (ch.t1[sh] > ch.t0[sh])
+        k_sgemm<S><<<unsigned(ch.t1[sh] - ch.t0[sh]), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get() + ch.t0[sh],
+                                                                    p.d_line_b1.get(), p.d_slice_off.get(), p.d_klist.get(),
+                                                                    p.d_W.get(), Tb, Sb, ch.w0);
 }
 
 template <class S>
@@ -504,10 +526,20 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
     launch_t<Sh64>(p, SHAPE_64, x, Tb, s);
     if (ev) QCM_CUDA(cudaEventRecord(ev[1], s));
     if (p.s_len) QCM_CUDA(cudaMemsetAsync(Sb, 0, p.s_len * sizeof(double), s));  // rows without lines stay 0
-    launch_s<Sh16>(p, SHAPE_16, Tb, Sb, s);
-    launch_s<Sh32>(p, SHAPE_32, Tb, Sb, s);
-    launch_s<Sh64>(p, SHAPE_64, Tb, Sb, s);
-    launch_s<Sh128>(p, SHAPE_128, Tb, Sb, s);
+    if (p.streamed()) {
+        for (const HeffPlan::WChunk& ch : p.wchunks) {
+            p.cg.generate_range(p.d_W.get(), ch.u0, ch.u1, ch.w0, ch.w1, s);
+            launch_s_range<Sh16>(p, SHAPE_16, ch, Tb, Sb, s);
+            launch_s_range<Sh32>(p, SHAPE_32, ch, Tb, Sb, s);
+            launch_s_range<Sh64>(p, SHAPE_64, ch, Tb, Sb, s);
+            launch_s_range<Sh128>(p, SHAPE_128, ch, Tb, Sb, s);
+        }
+    } else {
+        launch_s<Sh16>(p, SHAPE_16, Tb, Sb, s);
+        launch_s<Sh32>(p, SHAPE_32, Tb, Sb, s);
+        launch_s<Sh64>(p, SHAPE_64, Tb, Sb, s);
+        launch_s<Sh128>(p, SHAPE_128, Tb, Sb, s);
+    }
     if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
     launch_ls<Sh16>(p, SHAPE_16, Sb, Pb, y, s);
     launch_ls<Sh32>(p, SHAPE_32, Sb, Pb, y, s);
@@ -558,6 +590,7 @@ void heff_tgemm_device(HeffPlan& p, const double* x, double* T) {
 
 void prepare_mixed(HeffPlan& p, bool tc) {
     if (p.merged) throw std::runtime_error("a merged plan group applies in FP64 only");
+    if (p.streamed()) throw std::runtime_error("a plan with streamed coefficient blocks applies in FP64 only");
     AllocStream scope(p.stream);
     if (!p.d_merr.size()) {
         p.d_merr.alloc(1);
@@ -604,13 +637,13 @@ void run_sgemm(const UnitD* units, const DBuf<TileD>* dtiles, const std::vector<
                const uint64_t* slice_off, const uint16_t* klist, const double* W, const double* T, double* S,
                cudaStream_t s) {
     if (!htiles[SHAPE_16].empty())
-        k_sgemm<Sh16><<<unsigned(htiles[SHAPE_16].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_16].get(), line_b1, slice_off, klist, W, T, S);
+        k_sgemm<Sh16><<<unsigned(htiles[SHAPE_16].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_16].get(), line_b1, slice_off, klist, W, T, S, 0);
     if (!htiles[SHAPE_32].empty())
-        k_sgemm<Sh32><<<unsigned(htiles[SHAPE_32].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_32].get(), line_b1, slice_off, klist, W, T, S);
+        k_sgemm<Sh32><<<unsigned(htiles[SHAPE_32].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_32].get(), line_b1, slice_off, klist, W, T, S, 0);
     if (!htiles[SHAPE_64].empty())
-        k_sgemm<Sh64><<<unsigned(htiles[SHAPE_64].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_64].get(), line_b1, slice_off, klist, W, T, S);
+        k_sgemm<Sh64><<<unsigned(htiles[SHAPE_64].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_64].get(), line_b1, slice_off, klist, W, T, S, 0);
     if (!htiles[SHAPE_128].empty())
-        k_sgemm<Sh128><<<unsigned(htiles[SHAPE_128].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_128].get(), line_b1, slice_off, klist, W, T, S);
+        k_sgemm<Sh128><<<unsigned(htiles[SHAPE_128].size()), NTHR, 0, s>>>(units, dtiles[SHAPE_128].get(), line_b1, slice_off, klist, W, T, S, 0);
     QCM_CUDA(cudaGetLastError());
 }
 
@@ -619,8 +652,12 @@ int heff_launches_per_apply(const HeffPlan& p) {
     int n = 0;
     for (int sh = 0; sh < N_SHAPES; ++sh) {
         n += !p.ttiles[sh].empty();
-        n += !p.utiles[sh].empty();
+        if (!p.streamed()) n += !p.utiles[sh].empty();
         n += p.kitems[sh].empty() ? 0 : 2;
+    }
+    for (const HeffPlan::WChunk& ch : p.wchunks) {
+        n += ch.u1 > ch.u0;  // the chunk's coefficient generation
+        for (int sh = 0; sh < N_SHAPES; ++sh) n += ch.t1[sh] > ch.t0[sh];
     }
     return n;
 }
@@ -667,6 +704,7 @@ void stage_lists(HeffPlan& p);
 
 void restage_plan(HeffPlan& p) {
     AllocStream scope(p.stream);
+    if (p.streamed()) p.cg.upload(p.stream);  // the generation tables of every apply
     if (!p.lists_staged) {
         stage_lists(p);
         QCM_CUDA(cudaStreamSynchronize(p.stream));
@@ -772,6 +810,16 @@ void upload_plan(HeffPlan& p, bool lists) {
     if (lists) stage_lists(p);
     p.cg.upload(s);
     // dense coefficient blocks, built once per plan and reused by every apply
+    if (p.streamed()) {
+        // one chunk's scratch; every chunk generated once here so that a term without a slot is found
+        // when the plan is staged (each apply generates them again, unchecked)
+        uint64_t mx = 1;
+        for (const HeffPlan::WChunk& ch : p.wchunks) mx = std::max(mx, ch.w1 - ch.w0);
+        p.d_W.alloc(mx);
+        for (const HeffPlan::WChunk& ch : p.wchunks) p.cg.generate_range(p.d_W.get(), ch.u0, ch.u1, ch.w0, ch.w1, s);
+        p.cg.check_generated(s);
+        return;
+    }
     p.d_W.alloc(p.w_len ? p.w_len : 1);
     static const bool tdbg = std::getenv("QCM_PLAN_TIMING") != nullptr;
     auto now = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
@@ -785,6 +833,44 @@ void upload_plan(HeffPlan& p, bool lists) {
     if (tdbg)
         std::fprintf(stderr, "plan upload: coefficient generation %.4f s (%llu terms, %llu coefficients)\n", now() - t0,
                      (unsigned long long)p.n_alpha, (unsigned long long)p.w_len);
+}
+
+}  // namespace qcm
+
+namespace qcm {
+
+void stream_coefficients(HeffPlan& p, uint64_t max_doubles) {
+    p.wchunks.clear();
+    if (p.merged) throw std::runtime_error("stream_coefficients: a merged plan group keeps its members' blocks");
+    if (!max_doubles || p.w_len <= max_doubles || p.units.empty()) return;
+    if (p.cg.units.size() != p.units.size()) throw std::runtime_error("stream_coefficients: generation units differ from the plan's");
+    for (std::size_t i = 0; i < p.units.size(); ++i)
+        if (p.cg.units[i].w_off != p.units[i].w_off || (i && p.units[i].w_off < p.units[i - 1].w_off))
+            throw std::runtime_error("stream_coefficients: coefficient blocks out of unit order");
+    auto wend = [&](std::size_t i) { return p.units[i].w_off + uint64_t(p.units[i].wld) * p.units[i].nk; };
+    HeffPlan::WChunk ch;
+    ch.u0 = 0;
+    ch.w0 = p.units[0].w_off;
+    for (std::size_t i = 1; i <= p.units.size(); ++i) {
+        if (i < p.units.size() && wend(i) - ch.w0 <= max_doubles) continue;
+        ch.u1 = uint32_t(i);
+        ch.w1 = i < p.units.size() ? p.units[i].w_off : p.w_len;
+        p.wchunks.push_back(ch);
+        if (i < p.units.size()) { ch = HeffPlan::WChunk(); ch.u0 = uint32_t(i); ch.w0 = p.units[i].w_off; }
+    }
+    // each shape's tiles are in unit order: a chunk's are one range
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        const std::vector<TileD>& t = p.utiles[sh];
+        for (std::size_t k = 1; k < t.size(); ++k)
+            if (t[k].item < t[k - 1].item) throw std::runtime_error("stream_coefficients: S tiles out of unit order");
+        std::size_t k = 0;
+        for (HeffPlan::WChunk& c : p.wchunks) {
+            while (k < t.size() && t[k].item < c.u0) ++k;
+            c.t0[sh] = uint32_t(k);
+            while (k < t.size() && t[k].item < c.u1) ++k;
+            c.t1[sh] = uint32_t(k);
+        }
+    }
 }
 
 }  // namespace qcm

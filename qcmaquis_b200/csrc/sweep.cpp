@@ -773,6 +773,7 @@ void DevDMRG::step_prepare_plan(StepState& S) {
 }
 
 void DevDMRG::step_prepare_stage(StepState& S, bool group) {
+    if (!S.resident && !group) stream_coefficients(*S.plan, coefficient_budget);
     if (group) {
         // applied only inside the step's plan group: its coefficient blocks, not its work lists
         if (!S.resident) upload_plan(*S.plan, false);
@@ -882,6 +883,7 @@ void dmrg_group_sweep(const std::vector<DevDMRG*>& runs, std::vector<std::vector
             throw std::runtime_error("DMRG group: the runs differ in length, position or stream");
         if (d->p.jcd_tol != r0.p.jcd_tol || d->p.jcd_maxiter != r0.p.jcd_maxiter || d->p.jcd_maxiter > 16)
             throw std::runtime_error("DMRG group: the runs differ in the JD tolerance or iteration limit (at most 16)");
+        if (d->coefficient_budget) throw std::runtime_error("DMRG group: a run with streamed coefficient blocks");
     }
     const std::size_t nr = runs.size();
     energies.assign(nr, {});
@@ -977,8 +979,12 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
     auto plan = plan_for(_site, *left_[site], *right_[site + 1], mpo[site], x.phys, x.left, x.right, key, resident);
     plan->stream = c.s;
     if (plan->x_len != x.b.total) throw std::runtime_error("DMRG: site tensor layout differs from the plan");
-    if (resident) restage_plan(*plan);
-    else upload_plan(*plan);
+    if (resident) {
+        restage_plan(*plan);
+    } else {
+        stream_coefficients(*plan, coefficient_budget);
+        upload_plan(*plan);
+    }
     QCM_CUDA(cudaStreamSynchronize(c.s));
     st.plan_s += now_s() - t0;
     const double E = solve(*plan, x, [&](std::size_t o, double* v) {

@@ -69,6 +69,7 @@ _lib._sig("qcm_boundary_download", c_int, c_void_p, P(Sector), P(Sector), P(c_ui
 _lib._sig("qcm_heff_plan_create", c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, P(MPSDesc), c_int, P(c_void_p))
 _lib._sig("qcm_heff_get_info", c_int, c_void_p, P(HeffInfo))
 _lib._sig("qcm_heff_apply", c_int, c_void_p, P(c_double), P(c_double))
+_lib._sig("qcm_heff_stream_coefficients", c_int, c_void_p, c_uint64)
 _lib._sig("qcm_heff_adjoint", c_int, c_void_p, P(c_double), P(c_double), P(c_double), P(c_double))
 _lib._sig("qcm_heff_adjoint_terms", c_int, c_void_p, P(c_uint64))
 _lib._sig("qcm_heff_apply_device", c_int, c_void_p, c_void_p, c_void_p)
@@ -342,6 +343,14 @@ class HeffPlan:
         self.info = {f: getattr(info, f) for f, _ in HeffInfo._fields_}
         self.n = int(info.vec_len)
         return self
+
+    def stream_coefficients(self, nbytes: int):
+        """Keep at most nbytes of coefficient blocks on the device, generated chunk by chunk in every FP64
+        apply (0: whole); the plan is staged again and its info refreshed."""
+        check(lib.qcm_heff_stream_coefficients(self.h, int(nbytes)), "qcm_heff_stream_coefficients")
+        info = HeffInfo()
+        check(lib.qcm_heff_get_info(self.h, ctypes.byref(info)), "qcm_heff_get_info")
+        self.info = {f: getattr(info, f) for f, _ in HeffInfo._fields_}
 
     def apply(self, x: np.ndarray, precision="fp64") -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)
