@@ -704,7 +704,14 @@ void stage_lists(HeffPlan& p);
 
 void restage_plan(HeffPlan& p) {
     AllocStream scope(p.stream);
-    if (p.streamed()) p.cg.upload(p.stream);  // the generation tables of every apply
+    if (p.streamed()) {
+        // the generation tables of every apply, and its error word (applies allocate nothing)
+        p.cg.upload(p.stream);
+        if (!p.cg.d_err.size()) {
+            p.cg.d_err.alloc(1);
+            QCM_CUDA(cudaMemsetAsync(p.cg.d_err.get(), 0, sizeof(uint32_t), p.stream));
+        }
+    }
     if (!p.lists_staged) {
         stage_lists(p);
         QCM_CUDA(cudaStreamSynchronize(p.stream));
