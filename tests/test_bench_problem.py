@@ -74,6 +74,30 @@ def test_bench_synthetic_mps_and_problem():
     assert all(np.array_equal(x[1], y[1]) for s1, s2 in zip(sites, again) for x, y in zip(s1["blocks"], s2["blocks"]))
 
 
+def test_bench_sector_fixtures_well_formed():
+    """Every committed bond-sector fixture: L + 1 bonds from the vacuum to (N/2, N/2), bond dimensions at most
+    M (plus the one degenerate state the truncation may keep), each bond's sectors reachable from the
+    previous or the next bond's through one site's physical states (TwoU1 charges; a sector the truncation
+    of the neighbouring bond cut off on one side may stay on the other), and the recorded sweep energies
+    decreasing."""
+    import glob
+    import json
+    files = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "bench_sectors_L*_M*.json")))
+    assert len(files) >= 4
+    for f in files:
+        d = json.load(open(f))
+        L, M, bonds, phys = d["L"], d["M"], d["bonds"], [tuple(p[:2]) for p in d["phys"]]
+        assert len(bonds) == L + 1, f
+        assert [tuple(s[:2]) for s in bonds[0]] == [(0, 0)] and [tuple(s[:2]) for s in bonds[-1]] == [(L // 2, L // 2)]
+        for i in range(1, L):
+            assert sum(s[2] for s in bonds[i]) <= M + 1, f
+            fwd = {(a[0] + p[0], a[1] + p[1]) for a in bonds[i - 1] for p in phys}
+            bwd = {(a[0] - p[0], a[1] - p[1]) for a in bonds[i + 1] for p in phys}
+            assert all(tuple(s[:2]) in fwd or tuple(s[:2]) in bwd for s in bonds[i]), (f, i)
+        E = d["energies_min_per_sweep"]
+        assert all(e1 <= e0 + 1e-9 for e0, e1 in zip(E, E[1:])), f
+
+
 @pytest.mark.gpu
 def test_device_problem_from_mps_matches_oracle(gpu_ctx):
     """qcm_dmrg_create_from_mps_at on the bench's synthetic MPS (boundaries built on the device from the given
