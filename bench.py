@@ -398,7 +398,25 @@ def measure_streamed(a, plan, xd, yd, flush, info):
                                   "ms_per_apply": float(np.mean(tot)), "s_phase_ms": float(np.mean(sph)),
                                   "gflops": info["flops"] / (np.mean(tot) * 1e-3) / 1e9,
                                   "bitwise_equal_to_kept": bool(torch.equal(yd, y_kept))})
+        # the apply cut by ket sector: T, coefficient blocks, S and split-K partials chunk by chunk
+        out["sector_chunks"] = []
+        whole = 8 * (int(info["t_len"]) + int(info["s_len"]) + int(info["w_len"]))
+        for parts in (4, 16):
+            plan.chunk_apply(whole // parts)
+            for _ in range(3):
+                plan.apply_device(xd.data_ptr(), yd.data_ptr())
+            tot = []
+            for _ in range(10):
+                flush.zero_()
+                torch.cuda.synchronize()
+                tot.append(plan.profile(xd.data_ptr(), yd.data_ptr())[3])
+            torch.cuda.synchronize()
+            out["sector_chunks"].append({"budget_bytes": whole // parts, "launches_per_apply": int(plan.info["launches"]),
+                                         "ms_per_apply": float(np.mean(tot)),
+                                         "gflops": info["flops"] / (np.mean(tot) * 1e-3) / 1e9,
+                                         "bitwise_equal_to_kept": bool(torch.equal(yd, y_kept))})
     finally:
+        plan.chunk_apply(0)
         plan.stream_coefficients(0)
     return out
 

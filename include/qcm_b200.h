@@ -227,6 +227,15 @@ int qcm_heff_apply(qcm_heff* h, const double* x, double* y);
  * whole.  For problems whose blocks do not fit (they grow with the MPO bond dimension times the
  * squared sector sizes).  Mixed-form applies and plan groups need them whole (QCM_ERR_ARG). */
 int qcm_heff_stream_coefficients(qcm_heff* h, uint64_t max_bytes);
+/* Bounds the device memory of the plan's applies to about max_bytes of T slices, S rows and coefficient
+ * blocks: the ket sectors are cut into consecutive chunks (a larger sector is a chunk of its own) and
+ * every FP64 apply runs them in turn (T-GEMM, coefficient generation, S-GEMM and split-K L.S of the
+ * chunk, in scratch buffers the size of the largest chunk), with the split-K partials of all chunks
+ * summed at the end in the fixed order: the result equals the whole apply's to the bit.  The plan is
+ * staged again.  max_bytes = 0 undoes it.  For problems whose T and S buffers (which grow with the MPO
+ * bond dimension and the squared bond dimension) do not fit.  Supersedes qcm_heff_stream_coefficients;
+ * mixed-form applies, the adjoint and plan groups need the whole apply (QCM_ERR_ARG). */
+int qcm_heff_chunk_apply(qcm_heff* h, uint64_t max_bytes);
 /* Same with device pointers, enqueued on the context stream (asynchronous). */
 int qcm_heff_apply_device(qcm_heff* h, const double* x_dev, double* y_dev);
 
@@ -533,6 +542,11 @@ int qcm_dmrg_set_boundary_budget(qcm_dmrg* d, uint64_t bytes);
  * (qcm_heff_stream_coefficients); 0 keeps them whole (the default).  FP64 runs only, not in
  * qcm_dmrg_group_sweep.  Energies and truncations do not depend on it. */
 int qcm_dmrg_set_coefficient_budget(qcm_dmrg* d, uint64_t max_bytes);
+/* The H_eff plans the run builds from here on apply in ket-sector chunks of at most max_bytes of T, S and
+ * coefficient blocks each (qcm_heff_chunk_apply; it supersedes the coefficient budget); 0 for whole
+ * applies (the default).  FP64 runs only, not in qcm_dmrg_group_sweep.  Energies and truncations do not
+ * depend on it. */
+int qcm_dmrg_set_apply_budget(qcm_dmrg* d, uint64_t max_bytes);
 /* Run the current sweep up to (not including) step stop_step (steps_per_sweep
  * completes it); energies / trunc receive one entry per step run (may be NULL),
  * *n_steps their count. */

@@ -641,6 +641,14 @@ int qcm_dmrg_set_coefficient_budget(qcm_dmrg* d, uint64_t max_bytes) {
     return QCM_OK;
 }
 
+int qcm_dmrg_set_apply_budget(qcm_dmrg* d, uint64_t max_bytes) {
+    if (!d) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_set_apply_budget: NULL argument");
+    if (max_bytes && d->e->p.precision != 0)
+        return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_set_apply_budget: chunked applies are for FP64 runs");
+    d->e->apply_budget = max_bytes / sizeof(double);
+    return QCM_OK;
+}
+
 int qcm_dmrg_set_boundary_budget(qcm_dmrg* d, uint64_t bytes) {
     QCM_TRY
     if (!d) return qcm::fail(QCM_ERR_ARG, "qcm_dmrg_set_boundary_budget: NULL argument");

@@ -213,6 +213,21 @@ int qcm_heff_stream_coefficients(qcm_heff* h, uint64_t max_bytes) {
     QCM_CATCH
 }
 
+int qcm_heff_chunk_apply(qcm_heff* h, uint64_t max_bytes) {
+    QCM_TRY
+    if (!h) return qcm::fail(QCM_ERR_ARG, "qcm_heff_chunk_apply: NULL argument");
+    if (!h->ctx || !h->p->stream) return qcm::fail(QCM_ERR_ARG, "qcm_heff_chunk_apply: a plan built for the host only");
+    QCM_CUDA(cudaSetDevice(h->ctx->device));
+    qcm::AllocStream scope(h->ctx->stream);
+    qcm::HeffPlan& p = *h->p;
+    qcm::release_plan_device(p);
+    qcm::chunk_sectors(p, max_bytes / sizeof(double));
+    p.stream = h->ctx->stream;
+    qcm::upload_plan(p);
+    return QCM_OK;
+    QCM_CATCH
+}
+
 int qcm_heff_apply(qcm_heff* h, const double* x, double* y) {
     QCM_TRY
     if (!h || !x || !y) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply: NULL argument");

@@ -370,6 +370,8 @@ struct DevDMRG {
     uint64_t boundary_budget = 0;
     // doubles of coefficient blocks a plan keeps on the device (0: no limit); larger plans stream them
     uint64_t coefficient_budget = 0;
+    // doubles of T, S and coefficient blocks one apply chunk may hold (0: whole applies)
+    uint64_t apply_budget = 0;
     // boundary residency: the boundaries a step uses are brought to the device (bnd_use); after a step,
     // those no later step reads before the next half-sweep rebuilds them are released, and over the
     // budget the device copies farthest from the next step's two are moved to pinned host memory

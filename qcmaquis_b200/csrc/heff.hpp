@@ -133,8 +133,8 @@ struct OutD {
     uint32_t M, N, seg_start, seg_count;
 };
 struct TileD { uint32_t item, m0, n0, pad; };
-struct KItemD {       // split-K work item of the L.S GEMM: output tile, one segment, K range
-    uint32_t tile, seg, k0, k1;
+struct KItemD {       // split-K work item of the L.S GEMM: output tile, one segment, K range, partial slot
+    uint32_t tile, seg, k0, k1, slot;
 };
 struct OTileD {       // output tile of the L.S GEMM and its contiguous range of split-K partials
     uint32_t out, m0, n0, part0, nparts, pad0, pad1, pad2;
@@ -301,6 +301,28 @@ struct HeffPlan {
     };
     std::vector<WChunk> wchunks;
     bool streamed() const { return !wchunks.empty(); }
+    // where each ket sector's share starts in the plan's lists (prefixes over the ket sectors: T jobs,
+    // S units, T and S elements, coefficient elements), for the ket-sector chunks
+    std::vector<uint32_t> part_job, part_unit;
+    std::vector<uint64_t> part_t, part_s, part_w;
+    // the apply cut by ket sector (chunk_sectors): chunk c covers ket sectors [p0, p1), whose T slices
+    // [t0, t1), S rows [s0, s1) and coefficient blocks [w0, w1) (units [u0, u1)) are made and used by
+    // the chunk alone; per tile shape, its T-GEMM tiles, S-GEMM tiles and L.S items (the lists are
+    // ordered by chunk) are the ranges [a, b)
+    struct SChunk {
+        uint32_t p0 = 0, p1 = 0, u0 = 0, u1 = 0;
+        uint64_t t0 = 0, t1 = 0, s0 = 0, s1 = 0, w0 = 0, w1 = 0;
+        uint32_t tt[2][N_SHAPES] = {}, ut[2][N_SHAPES] = {}, kt[2][N_SHAPES] = {};
+    };
+    std::vector<SChunk> schunks;
+    bool sector_chunked() const { return !schunks.empty(); }
+    // a chunked apply sums every shape's partials at the end, so each shape has its own partial region
+    // (from pc_off[sh] on; pc_len in all) instead of the one region the shapes take in turn
+    uint64_t pc_off[N_SHAPES] = {}, pc_len = 0;
+    // in a chunked plan the T offsets of its T jobs and slices and the S offsets of its units and L.S
+    // segments count from their chunk's t0 and s0 (the kernels address one chunk's scratch); seg_chunk
+    // is each segment's chunk, for undoing it
+    std::vector<uint32_t> seg_chunk;
     DBuf<uint16_t> d_klist;
     DBuf<SegD> d_segs;
     DBuf<OutD> d_outs;
@@ -346,6 +368,14 @@ void upload_plan(HeffPlan& p, bool lists = true);
 // result is the same to the bit).  Set before upload_plan; the mixed forms and plan groups need the
 // blocks kept.
 void stream_coefficients(HeffPlan& p, uint64_t max_doubles);
+// Bounds the device memory of an apply: the ket sectors are cut into consecutive chunks whose T slices,
+// S rows and coefficient blocks together take at most max_doubles (a larger sector is a chunk of its
+// own), and every FP64 apply runs chunk by chunk: the chunk's T-GEMM into one T scratch, its coefficient
+// blocks generated into one scratch, its S-GEMM into one S scratch and its split-K L.S partials; the
+// partials of all chunks are summed at the end in the fixed order, so the result is the whole apply's
+// to the bit.  0 (or a plan that fits) undoes it.  Set before upload_plan; supersedes
+// stream_coefficients; the mixed forms, the adjoint and plan groups need the whole apply.
+void chunk_sectors(HeffPlan& p, uint64_t max_doubles);
 // Frees a plan's device buffers (work lists, coefficient blocks, scratch) and keeps its host work lists:
 // upload_plan stages it again, against boundaries of the same structure (rebind_plan).
 void release_plan_device(HeffPlan& p);

@@ -268,6 +268,7 @@ uint64_t heff_adjoint_terms(const HeffPlan& p) { return p.cg.mt ? p.cg.mt->row_o
 
 void heff_adjoint_device(HeffPlan& p, const double* x, const double* ybar, double* psi_bar, double* coeff_bar) {
     cudaStream_t s = p.stream;
+    if (p.sector_chunked()) throw std::runtime_error("heff adjoint: the plan's apply is chunked by ket sector");
     if (psi_bar) heff_apply_device(p, ybar, psi_bar);
     if (!coeff_bar) return;
     HeffAdjointWork& w = adjoint_work(p);

@@ -108,7 +108,7 @@ std::unique_ptr<HeffPlan> merge_plans(const std::vector<HeffPlan*>& plans, std::
         for (int sh = 0; sh < N_SHAPES; ++sh) {
             const uint32_t ot0 = uint32_t(g->otiles[sh].size());
             for (OTileD t : p.otiles[sh]) { t.out += o0; t.part0 += uint32_t(kl_items[sh]); g->otiles[sh].push_back(t); }
-            for (KItemD k : p.kitems[sh]) { k.tile += ot0; k.seg += sg0; g->kitems[sh].push_back(k); }
+            for (KItemD k : p.kitems[sh]) { k.tile += ot0; k.seg += sg0; k.slot += uint32_t(kl_items[sh]); g->kitems[sh].push_back(k); }
             kl_items[sh] += p.kitems[sh].size();
         }
         g->flops += p.flops; g->flops_t += p.flops_t; g->flops_s += p.flops_s; g->flops_ls += p.flops_ls;

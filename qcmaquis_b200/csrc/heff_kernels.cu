@@ -453,7 +453,7 @@ __global__ void __launch_bounds__(NTHR) k_lspart(const KItemD* __restrict__ item
         if (kc + 2 < nk) bases(kc & 1, it.k0 + (kc + 2) * BK);
         mma_stage<S>(st[kc & 1].A, st[kc & 1].B, acc, warp, lane);
     }
-    double* Pt = P + uint64_t(blockIdx.x) * S::BM * S::BN;
+    double* Pt = P + uint64_t(it.slot) * S::BM * S::BN;
     for_acc<S>(acc, warp, lane, [&](int m, int n, double v) { Pt[m + n * S::BM] = v; });
 }
 
@@ -493,6 +493,39 @@ void launch_s(HeffPlan& p, int sh, const double* Tb, double* Sb, cudaStream_t s)
                                                                   p.d_slice_off.get(), p.d_klist.get(), p.w_data(), Tb, Sb, 0);
 }
 
+// one ket-sector chunk's T-GEMM tiles, S-GEMM tiles and L.S items (T, S and the coefficient blocks from
+// their chunk bases on)
+template <class S>
+void launch_t_chunk(HeffPlan& p, int sh, const HeffPlan::SChunk& c, const double* x, double* Tb, cudaStream_t s) {
+    const uint32_t a = c.tt[0][sh], b = c.tt[1][sh];
+    if (b > a)
+        k_tgemm<S><<<unsigned(b - a), NTHR, 0, s>>>(p.d_tjobs.get(), p.d_ttiles[sh].get() + a, x, p.r_data(), Tb, nullptr,
+                                                    nullptr);
+}
+
+template <class S>
+void launch_s_chunk(HeffPlan& p, int sh, const HeffPlan::SChunk& c, const double* Tb, double* Sb, cudaStream_t s) {
+    const uint32_t a = c.ut[0][sh], b = c.ut[1][sh];
+    if (b > a)
+        k_sgemm<S><<<unsigned(b - a), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get() + a, p.d_line_b1.get(),
+                                                    p.d_slice_off.get(), p.d_klist.get(), p.d_W.get(), Tb, Sb, c.w0);
+}
+
+template <class S>
+void launch_ls_chunk(HeffPlan& p, int sh, const HeffPlan::SChunk& c, const double* Sb, double* Pb, cudaStream_t s) {
+    const uint32_t a = c.kt[0][sh], b = c.kt[1][sh];
+    if (b > a)
+        k_lspart<S><<<unsigned(b - a), NTHR, 0, s>>>(p.d_kitems[sh].get() + a, p.d_otiles[sh].get(), p.d_outs.get(),
+                                                     p.d_segs.get(), p.l_data(), Sb, Pb + p.pc_off[sh]);
+}
+
+template <class S>
+void launch_lsreduce(HeffPlan& p, int sh, const double* Pb, double* y, cudaStream_t s) {
+    if (p.kitems[sh].empty()) return;
+    const dim3 rg(unsigned(p.otiles[sh].size()), unsigned((S::BM * S::BN + 255) / 256));
+    k_lsreduce<S><<<rg, 256, 0, s>>>(p.d_otiles[sh].get(), p.d_outs.get(), Pb + p.pc_off[sh], y);
+}
+
 // the S-GEMM tiles of one coefficient chunk, reading the chunk's blocks from the plan's scratch
 template <class S>
 void launch_s_range(HeffPlan& p, int sh, const HeffPlan::WChunk& ch, const double* Tb, double* Sb, cudaStream_t s) {
@@ -521,6 +554,32 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
     if (!p.lists_staged) throw std::runtime_error("heff apply: the plan's work lists are not on the device");
     if (ev) QCM_CUDA(cudaEventRecord(ev[0], s));
     QCM_CUDA(cudaMemsetAsync(y, 0, p.x_len * sizeof(double), s));
+    if (p.sector_chunked()) {
+        // chunk by chunk: T, coefficient blocks, S and the L.S partials of its ket sectors; the partials
+        // of all chunks summed at the end (the phase events mark the chunk loop and the sum)
+        for (const HeffPlan::SChunk& c : p.schunks) {
+            launch_t_chunk<Sh16>(p, SHAPE_16, c, x, Tb, s);
+            launch_t_chunk<Sh32>(p, SHAPE_32, c, x, Tb, s);
+            launch_t_chunk<Sh64>(p, SHAPE_64, c, x, Tb, s);
+            if (c.s1 > c.s0) QCM_CUDA(cudaMemsetAsync(Sb, 0, (c.s1 - c.s0) * sizeof(double), s));
+            p.cg.generate_range(p.d_W.get(), c.u0, c.u1, c.w0, c.w1, s);
+            launch_s_chunk<Sh16>(p, SHAPE_16, c, Tb, Sb, s);
+            launch_s_chunk<Sh32>(p, SHAPE_32, c, Tb, Sb, s);
+            launch_s_chunk<Sh64>(p, SHAPE_64, c, Tb, Sb, s);
+            launch_s_chunk<Sh128>(p, SHAPE_128, c, Tb, Sb, s);
+            launch_ls_chunk<Sh16>(p, SHAPE_16, c, Sb, Pb, s);
+            launch_ls_chunk<Sh32>(p, SHAPE_32, c, Sb, Pb, s);
+            launch_ls_chunk<Sh64>(p, SHAPE_64, c, Sb, Pb, s);
+        }
+        if (ev) QCM_CUDA(cudaEventRecord(ev[1], s));
+        if (ev) QCM_CUDA(cudaEventRecord(ev[2], s));
+        launch_lsreduce<Sh16>(p, SHAPE_16, Pb, y, s);
+        launch_lsreduce<Sh32>(p, SHAPE_32, Pb, y, s);
+        launch_lsreduce<Sh64>(p, SHAPE_64, Pb, y, s);
+        if (ev) QCM_CUDA(cudaEventRecord(ev[3], s));
+        QCM_CUDA(cudaGetLastError());
+        return;
+    }
     launch_t<Sh16>(p, SHAPE_16, x, Tb, s);
     launch_t<Sh32>(p, SHAPE_32, x, Tb, s);
     launch_t<Sh64>(p, SHAPE_64, x, Tb, s);
@@ -582,6 +641,7 @@ void heff_apply_device(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev)
 
 void heff_tgemm_device(HeffPlan& p, const double* x, double* T) {
     if (!p.lists_staged) throw std::runtime_error("heff T-GEMM: the plan's work lists are not on the device");
+    if (p.sector_chunked()) throw std::runtime_error("heff T-GEMM: the plan's apply is chunked by ket sector");
     launch_t<Sh16>(p, SHAPE_16, x, T, p.stream);
     launch_t<Sh32>(p, SHAPE_32, x, T, p.stream);
     launch_t<Sh64>(p, SHAPE_64, x, T, p.stream);
@@ -590,7 +650,8 @@ void heff_tgemm_device(HeffPlan& p, const double* x, double* T) {
 
 void prepare_mixed(HeffPlan& p, bool tc) {
     if (p.merged) throw std::runtime_error("a merged plan group applies in FP64 only");
-    if (p.streamed()) throw std::runtime_error("a plan with streamed coefficient blocks applies in FP64 only");
+    if (p.streamed() || p.sector_chunked())
+        throw std::runtime_error("a plan with streamed coefficient blocks or a chunked apply applies in FP64 only");
     AllocStream scope(p.stream);
     if (!p.d_merr.size()) {
         p.d_merr.alloc(1);
@@ -659,6 +720,15 @@ int heff_launches_per_apply(const HeffPlan& p) {
         n += ch.u1 > ch.u0;  // the chunk's coefficient generation
         for (int sh = 0; sh < N_SHAPES; ++sh) n += ch.t1[sh] > ch.t0[sh];
     }
+    if (p.sector_chunked()) {
+        n = 0;
+        for (const HeffPlan::SChunk& c : p.schunks) {
+            n += c.u1 > c.u0;
+            for (int sh = 0; sh < N_SHAPES; ++sh)
+                n += (c.tt[1][sh] > c.tt[0][sh]) + (c.ut[1][sh] > c.ut[0][sh]) + (c.kt[1][sh] > c.kt[0][sh]);
+        }
+        for (int sh = 0; sh < N_SHAPES; ++sh) n += !p.kitems[sh].empty();  // the partial sums
+    }
     return n;
 }
 
@@ -700,11 +770,13 @@ uint64_t plan_resident_bytes(const HeffPlan& p) {
 
 namespace {
 void stage_lists(HeffPlan& p);
+uint64_t chunk_t_len(const HeffPlan& p);
+uint64_t chunk_s_len(const HeffPlan& p);
 }
 
 void restage_plan(HeffPlan& p) {
     AllocStream scope(p.stream);
-    if (p.streamed()) {
+    if (p.streamed() || p.sector_chunked()) {
         // the generation tables of every apply, and its error word (applies allocate nothing)
         p.cg.upload(p.stream);
         if (!p.cg.d_err.size()) {
@@ -717,9 +789,9 @@ void restage_plan(HeffPlan& p) {
         QCM_CUDA(cudaStreamSynchronize(p.stream));
         return;
     }
-    p.d_T.alloc(p.t_len);
-    p.d_S.alloc(p.s_len);
-    p.d_P.alloc(p.p_len);
+    p.d_T.alloc(chunk_t_len(p));
+    p.d_S.alloc(chunk_s_len(p));
+    p.d_P.alloc(p.sector_chunked() ? p.pc_len : p.p_len);
 }
 
 void rebind_plan(HeffPlan& p, const DevBoundary& L, const DevBoundary& R) {
@@ -770,6 +842,20 @@ void upload_merged(HeffPlan& p) {
 
 namespace {
 
+// T and S scratch of one apply: the whole buffers, or the largest ket-sector chunk's
+uint64_t chunk_t_len(const HeffPlan& p) {
+    if (!p.sector_chunked()) return p.t_len;
+    uint64_t m = 1;
+    for (const HeffPlan::SChunk& c : p.schunks) m = std::max(m, c.t1 - c.t0);
+    return m;
+}
+uint64_t chunk_s_len(const HeffPlan& p) {
+    if (!p.sector_chunked()) return p.s_len;
+    uint64_t m = 1;
+    for (const HeffPlan::SChunk& c : p.schunks) m = std::max(m, c.s1 - c.s0);
+    return m;
+}
+
 // the work lists and the scratch of one plan on the device
 void stage_lists(HeffPlan& p) {
     cudaStream_t s = p.stream;
@@ -786,9 +872,9 @@ void stage_lists(HeffPlan& p) {
     p.d_klist.upload(p.klist, s);
     p.d_segs.upload(p.segs, s);
     p.d_outs.upload(p.outs, s);
-    p.d_T.alloc(p.t_len);
-    p.d_S.alloc(p.s_len);
-    p.d_P.alloc(p.p_len);
+    p.d_T.alloc(chunk_t_len(p));
+    p.d_S.alloc(chunk_s_len(p));
+    p.d_P.alloc(p.sector_chunked() ? p.pc_len : p.p_len);
     p.lists_staged = true;
 }
 
@@ -817,13 +903,15 @@ void upload_plan(HeffPlan& p, bool lists) {
     if (lists) stage_lists(p);
     p.cg.upload(s);
     // dense coefficient blocks, built once per plan and reused by every apply
-    if (p.streamed()) {
+    if (p.streamed() || p.sector_chunked()) {
         // one chunk's scratch; every chunk generated once here so that a term without a slot is found
         // when the plan is staged (each apply generates them again, unchecked)
         uint64_t mx = 1;
         for (const HeffPlan::WChunk& ch : p.wchunks) mx = std::max(mx, ch.w1 - ch.w0);
+        for (const HeffPlan::SChunk& c : p.schunks) mx = std::max(mx, c.w1 - c.w0);
         p.d_W.alloc(mx);
         for (const HeffPlan::WChunk& ch : p.wchunks) p.cg.generate_range(p.d_W.get(), ch.u0, ch.u1, ch.w0, ch.w1, s);
+        for (const HeffPlan::SChunk& c : p.schunks) p.cg.generate_range(p.d_W.get(), c.u0, c.u1, c.w0, c.w1, s);
         p.cg.check_generated(s);
         return;
     }
@@ -878,6 +966,121 @@ void stream_coefficients(HeffPlan& p, uint64_t max_doubles) {
             c.t1[sh] = uint32_t(k);
         }
     }
+}
+
+}  // namespace qcm
+
+namespace qcm {
+
+namespace {
+
+// adds (sign +1) or removes (-1) the chunk bases of a chunked plan's T and S offsets
+void rebase_chunks(HeffPlan& p, int sign) {
+    for (std::size_t c = 0; c < p.schunks.size(); ++c) {
+        const HeffPlan::SChunk& ch = p.schunks[c];
+        const uint64_t t0 = ch.t0, s0 = ch.s0;
+        auto shift = [sign](uint64_t& v, uint64_t b) { v = sign > 0 ? v + b : v - b; };
+        for (uint32_t j = p.part_job[ch.p0]; j < p.part_job[ch.p1]; ++j) shift(p.tjobs[j].c_off, t0);
+        for (uint32_t u = ch.u0; u < ch.u1; ++u) {
+            UnitD& U = p.units[u];
+            shift(U.s_off, s0);
+            for (uint32_t k = 0; k < U.nk; ++k) shift(p.slice_off[U.slice0 + k], t0);
+        }
+        for (std::size_t g = 0; g < p.segs.size(); ++g)
+            if (p.seg_chunk[g] == c) shift(p.segs[g].s_off, s0);
+    }
+}
+
+}  // namespace
+
+void chunk_sectors(HeffPlan& p, uint64_t max_doubles) {
+    if (p.sector_chunked()) rebase_chunks(p, +1);  // back to whole-buffer offsets first
+    p.schunks.clear();
+    p.seg_chunk.clear();
+    if (p.merged) throw std::runtime_error("chunk_sectors: a merged plan group");
+    if (!max_doubles || p.t_len + p.s_len + p.w_len <= max_doubles) return;
+    if (p.part_t.size() < 2) throw std::runtime_error("chunk_sectors: the plan has no ket-sector prefixes");
+    p.wchunks.clear();  // the chunks below generate their own coefficient blocks
+    const std::size_t np = p.part_t.size() - 1;
+    auto size = [&](std::size_t a, std::size_t b) {
+        return (p.part_t[b] - p.part_t[a]) + (p.part_s[b] - p.part_s[a]) + (p.part_w[b] - p.part_w[a]);
+    };
+    std::vector<uint32_t> chunk_of(np);
+    std::size_t a = 0;
+    for (std::size_t i = 1; i <= np; ++i) {
+        if (i < np && size(a, i + 1) <= max_doubles) continue;
+        HeffPlan::SChunk c;
+        c.p0 = uint32_t(a); c.p1 = uint32_t(i);
+        c.u0 = p.part_unit[a]; c.u1 = p.part_unit[i];
+        c.t0 = p.part_t[a]; c.t1 = p.part_t[i];
+        c.s0 = p.part_s[a]; c.s1 = p.part_s[i];
+        c.w0 = p.part_w[a]; c.w1 = p.part_w[i];
+        for (std::size_t k = a; k < i; ++k) chunk_of[k] = uint32_t(p.schunks.size());
+        p.schunks.push_back(c);
+        a = i;
+    }
+    const std::size_t nc = p.schunks.size();
+    // the ket sector of a T job, an S unit and an L.S segment (by its S rows)
+    auto part_of = [](const auto& pre, uint64_t v) {
+        return std::size_t(std::upper_bound(pre.begin(), pre.end(), v) - pre.begin()) - 1;
+    };
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        // each list grouped by chunk, in its order within a chunk (the tiles write disjoint parts of T and
+        // S, and an L.S item its own partial slot, so the order of the launches does not matter)
+        // returns the chunk boundaries in the regrouped list
+        auto regroup = [&](auto& list, auto chunk_fn) {
+            std::vector<std::size_t> cnt(nc + 1, 0);
+            for (const auto& e : list) ++cnt[chunk_fn(e) + 1];
+            for (std::size_t c = 0; c < nc; ++c) cnt[c + 1] += cnt[c];
+            std::remove_reference_t<decltype(list)> out(list.size());
+            std::vector<std::size_t> pos(cnt.begin(), cnt.end() - 1);
+            for (const auto& e : list) out[pos[chunk_fn(e)]++] = e;
+            list.swap(out);
+            return cnt;
+        };
+        auto tcnt = regroup(p.ttiles[sh], [&](const TileD& t) { return chunk_of[part_of(p.part_job, t.item)]; });
+        auto ucnt = regroup(p.utiles[sh], [&](const TileD& t) { return chunk_of[part_of(p.part_unit, t.item)]; });
+        auto kcnt = regroup(p.kitems[sh], [&](const KItemD& k) { return chunk_of[part_of(p.part_s, p.segs[k.seg].s_off)]; });
+        for (std::size_t c = 0; c < nc; ++c) {
+            HeffPlan::SChunk& ch = p.schunks[c];
+            ch.tt[0][sh] = uint32_t(tcnt[c]); ch.tt[1][sh] = uint32_t(tcnt[c + 1]);
+            ch.ut[0][sh] = uint32_t(ucnt[c]); ch.ut[1][sh] = uint32_t(ucnt[c + 1]);
+            ch.kt[0][sh] = uint32_t(kcnt[c]); ch.kt[1][sh] = uint32_t(kcnt[c + 1]);
+        }
+    }
+    p.seg_chunk.resize(p.segs.size());
+    for (std::size_t g = 0; g < p.segs.size(); ++g) p.seg_chunk[g] = chunk_of[part_of(p.part_s, p.segs[g].s_off)];
+    // each shape's partials in a region of its own
+    p.pc_len = 0;
+    for (int sh = 0; sh < N_SHAPES; ++sh) {
+        p.pc_off[sh] = p.pc_len;
+        p.pc_len += uint64_t(p.kitems[sh].size()) * shape_bm(sh) * shape_bn(sh);
+    }
+    p.pc_len = std::max<uint64_t>(p.pc_len, 1);
+    // every chunk's T slices, S rows and coefficient blocks lie in its ranges
+    for (std::size_t c = 0; c < nc; ++c) {
+        const HeffPlan::SChunk& ch = p.schunks[c];
+        for (int sh = 0; sh < N_SHAPES; ++sh) {
+            for (uint32_t i = ch.tt[0][sh]; i < ch.tt[1][sh]; ++i) {
+                const TJobD& j = p.tjobs[p.ttiles[sh][i].item];
+                if (j.c_off < ch.t0 || j.c_off + uint64_t(j.N / j.brs) * j.sst > ch.t1)
+                    throw std::runtime_error("chunk_sectors: T job outside its chunk");
+            }
+            for (uint32_t i = ch.ut[0][sh]; i < ch.ut[1][sh]; ++i) {
+                const UnitD& u = p.units[p.utiles[sh][i].item];
+                if (u.s_off < ch.s0 || u.s_off > ch.s1 || u.w_off < ch.w0 || u.w_off + uint64_t(u.wld) * u.nk > ch.w1)
+                    throw std::runtime_error("chunk_sectors: S unit outside its chunk");
+                for (uint32_t k = 0; k < u.nk; ++k)
+                    if (p.slice_off[u.slice0 + k] < ch.t0 || p.slice_off[u.slice0 + k] >= ch.t1)
+                        throw std::runtime_error("chunk_sectors: T slice outside its chunk");
+            }
+            for (uint32_t i = ch.kt[0][sh]; i < ch.kt[1][sh]; ++i) {
+                const SegD& g = p.segs[p.kitems[sh][i].seg];
+                if (g.s_off < ch.s0 || g.s_off > ch.s1) throw std::runtime_error("chunk_sectors: L.S segment outside its chunk");
+            }
+        }
+    }
+    rebase_chunks(p, -1);
 }
 
 }  // namespace qcm

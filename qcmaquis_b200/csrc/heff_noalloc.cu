@@ -64,6 +64,8 @@ extern "C" int qcm_heff_apply_device_noalloc(qcm_heff* h, const double* x_dev, d
     if (!h || !x_dev || !y_dev) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device_noalloc: NULL argument");
     if (!h->ctx) return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device_noalloc: host-only plan");
     qcm::HeffPlan& p = *h->p;
+    if (p.sector_chunked())
+        return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device_noalloc: a chunked plan applies through qcm_heff_apply_device");
     const uint64_t need = round32(p.t_len) + round32(p.s_len) + round32(p.p_len);
     if (need > QCM_NOALLOC_SCRATCH_DOUBLES)
         return qcm::fail(QCM_ERR_ARG, "qcm_heff_apply_device_noalloc: plan needs " + std::to_string(need) +

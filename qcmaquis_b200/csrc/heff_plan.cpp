@@ -727,6 +727,12 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
         p->flops_sexec += P.flops_sexec;
     }
     const Base& tot = base[nl];
+    p->part_job.resize(nl + 1); p->part_unit.resize(nl + 1);
+    p->part_t.resize(nl + 1); p->part_s.resize(nl + 1); p->part_w.resize(nl + 1);
+    for (uint32_t i = 0; i <= nl; ++i) {
+        p->part_job[i] = base[i].job; p->part_unit[i] = base[i].unit;
+        p->part_t[i] = base[i].t; p->part_s[i] = base[i].s; p->part_w[i] = base[i].w;
+    }
     p->tjobs.resize(tot.job);
     p->units.resize(tot.unit);
     CoefGen& cg = p->cg;
@@ -813,7 +819,8 @@ std::unique_ptr<HeffPlan> build_heff_plan(const DevBoundary& Lb, const DevBounda
                     for (uint32_t sg = o.seg_start; sg < o.seg_start + o.seg_count; ++sg) {
                         uint32_t Kc = p->segs[sg].nS * p->segs[sg].ls_in;
                         for (uint32_t k0 = 0; k0 < Kc; k0 += KCHUNK)
-                            p->kitems[sh].push_back(KItemD{uint32_t(p->otiles[sh].size()), sg, k0, std::min(Kc, k0 + KCHUNK)});
+                            p->kitems[sh].push_back(KItemD{uint32_t(p->otiles[sh].size()), sg, k0, std::min(Kc, k0 + KCHUNK),
+                                                           uint32_t(p->kitems[sh].size())});
                     }
                     t.nparts = uint32_t(p->kitems[sh].size()) - t.part0;
                     p->otiles[sh].push_back(t);

@@ -773,7 +773,10 @@ void DevDMRG::step_prepare_plan(StepState& S) {
 }
 
 void DevDMRG::step_prepare_stage(StepState& S, bool group) {
-    if (!S.resident && !group) stream_coefficients(*S.plan, coefficient_budget);
+    if (!S.resident && !group) {
+        stream_coefficients(*S.plan, coefficient_budget);
+        chunk_sectors(*S.plan, apply_budget);
+    }
     if (group) {
         // applied only inside the step's plan group: its coefficient blocks, not its work lists
         if (!S.resident) upload_plan(*S.plan, false);
@@ -883,7 +886,8 @@ void dmrg_group_sweep(const std::vector<DevDMRG*>& runs, std::vector<std::vector
             throw std::runtime_error("DMRG group: the runs differ in length, position or stream");
         if (d->p.jcd_tol != r0.p.jcd_tol || d->p.jcd_maxiter != r0.p.jcd_maxiter || d->p.jcd_maxiter > 16)
             throw std::runtime_error("DMRG group: the runs differ in the JD tolerance or iteration limit (at most 16)");
-        if (d->coefficient_budget) throw std::runtime_error("DMRG group: a run with streamed coefficient blocks");
+        if (d->coefficient_budget || d->apply_budget)
+            throw std::runtime_error("DMRG group: a run with streamed coefficient blocks or chunked applies");
     }
     const std::size_t nr = runs.size();
     energies.assign(nr, {});
@@ -983,6 +987,7 @@ void DevDMRG::step_single(int _site, double& energy, TruncResults& tr) {
         restage_plan(*plan);
     } else {
         stream_coefficients(*plan, coefficient_budget);
+        chunk_sectors(*plan, apply_budget);
         upload_plan(*plan);
     }
     QCM_CUDA(cudaStreamSynchronize(c.s));

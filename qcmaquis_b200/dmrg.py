@@ -91,6 +91,7 @@ _lib._sig("qcm_dmrg_get_stats", c_int, c_void_p, P(DMRGStats))
 _lib._sig("qcm_dmrg_group_sweep", c_int, P(c_void_p), c_int, P(c_double), P(TruncResult))
 _lib._sig("qcm_dmrg_set_boundary_budget", c_int, c_void_p, c_uint64)
 _lib._sig("qcm_dmrg_set_coefficient_budget", c_int, c_void_p, c_uint64)
+_lib._sig("qcm_dmrg_set_apply_budget", c_int, c_void_p, c_uint64)
 _lib._sig("qcm_dmrg_bond_dimensions", c_int, c_void_p, P(c_uint64))
 _lib._sig("qcm_dmrg_free", None, c_void_p)
 _U32 = P(ctypes.c_uint32)
@@ -384,6 +385,11 @@ class DMRG:
         """Device bytes of coefficient blocks each H_eff plan built from here on keeps (0: no limit); larger
         plans generate them chunk by chunk in every apply (qcm_dmrg_set_coefficient_budget)."""
         check(lib.qcm_dmrg_set_coefficient_budget(self.h, int(nbytes)), "qcm_dmrg_set_coefficient_budget")
+
+    def set_apply_budget(self, nbytes: int):
+        """Device bytes of T, S and coefficient blocks one apply chunk of the plans built from here on may
+        hold (0: whole applies; qcm_dmrg_set_apply_budget)."""
+        check(lib.qcm_dmrg_set_apply_budget(self.h, int(nbytes)), "qcm_dmrg_set_apply_budget")
 
     def stats(self) -> dict:
         s = DMRGStats()

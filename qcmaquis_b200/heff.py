@@ -70,6 +70,7 @@ _lib._sig("qcm_heff_plan_create", c_int, c_void_p, c_void_p, c_void_p, c_void_p,
 _lib._sig("qcm_heff_get_info", c_int, c_void_p, P(HeffInfo))
 _lib._sig("qcm_heff_apply", c_int, c_void_p, P(c_double), P(c_double))
 _lib._sig("qcm_heff_stream_coefficients", c_int, c_void_p, c_uint64)
+_lib._sig("qcm_heff_chunk_apply", c_int, c_void_p, c_uint64)
 _lib._sig("qcm_heff_adjoint", c_int, c_void_p, P(c_double), P(c_double), P(c_double), P(c_double))
 _lib._sig("qcm_heff_adjoint_terms", c_int, c_void_p, P(c_uint64))
 _lib._sig("qcm_heff_apply_device", c_int, c_void_p, c_void_p, c_void_p)
@@ -348,6 +349,14 @@ class HeffPlan:
         """Keep at most nbytes of coefficient blocks on the device, generated chunk by chunk in every FP64
         apply (0: whole); the plan is staged again and its info refreshed."""
         check(lib.qcm_heff_stream_coefficients(self.h, int(nbytes)), "qcm_heff_stream_coefficients")
+        info = HeffInfo()
+        check(lib.qcm_heff_get_info(self.h, ctypes.byref(info)), "qcm_heff_get_info")
+        self.info = {f: getattr(info, f) for f, _ in HeffInfo._fields_}
+
+    def chunk_apply(self, nbytes: int):
+        """Apply in ket-sector chunks of at most nbytes of T, S and coefficient blocks (0: whole); the plan
+        is staged again and its info refreshed."""
+        check(lib.qcm_heff_chunk_apply(self.h, int(nbytes)), "qcm_heff_chunk_apply")
         info = HeffInfo()
         check(lib.qcm_heff_get_info(self.h, ctypes.byref(info)), "qcm_heff_get_info")
         self.info = {f: getattr(info, f) for f, _ in HeffInfo._fields_}
