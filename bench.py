@@ -401,8 +401,11 @@ def measure_streamed(a, plan, xd, yd, flush, info):
         # the apply cut by ket sector: T, coefficient blocks, S and split-K partials chunk by chunk
         out["sector_chunks"] = []
         whole = 8 * (int(info["t_len"]) + int(info["s_len"]) + int(info["w_len"]))
-        for parts in (4, 16):
-            plan.chunk_apply(whole // parts)
+        ts_bytes, w_bytes = 8 * (int(info["t_len"]) + int(info["s_len"])), 8 * int(info["w_len"])
+        # two budgets below the coefficient blocks' share (each chunk generates its own), and one that
+        # keeps them whole (generated once) while T and S run in four chunks
+        for budget in (whole // 4, whole // 16, max(2 * w_bytes, w_bytes + ts_bytes // 4)):
+            plan.chunk_apply(budget)
             for _ in range(3):
                 plan.apply_device(xd.data_ptr(), yd.data_ptr())
             tot = []
@@ -411,7 +414,7 @@ def measure_streamed(a, plan, xd, yd, flush, info):
                 torch.cuda.synchronize()
                 tot.append(plan.profile(xd.data_ptr(), yd.data_ptr())[3])
             torch.cuda.synchronize()
-            out["sector_chunks"].append({"budget_bytes": whole // parts, "launches_per_apply": int(plan.info["launches"]),
+            out["sector_chunks"].append({"budget_bytes": budget, "launches_per_apply": int(plan.info["launches"]),
                                          "ms_per_apply": float(np.mean(tot)),
                                          "gflops": info["flops"] / (np.mean(tot) * 1e-3) / 1e9,
                                          "bitwise_equal_to_kept": bool(torch.equal(yd, y_kept))})

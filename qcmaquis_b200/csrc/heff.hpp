@@ -323,6 +323,9 @@ struct HeffPlan {
     // segments count from their chunk's t0 and s0 (the kernels address one chunk's scratch); seg_chunk
     // is each segment's chunk, for undoing it
     std::vector<uint32_t> seg_chunk;
+    // the chunks share the whole coefficient blocks, generated once (they take at most half the budget),
+    // instead of generating their own in every apply
+    bool chunk_keeps_w = false;
     DBuf<uint16_t> d_klist;
     DBuf<SegD> d_segs;
     DBuf<OutD> d_outs;
@@ -370,8 +373,10 @@ void upload_plan(HeffPlan& p, bool lists = true);
 void stream_coefficients(HeffPlan& p, uint64_t max_doubles);
 // Bounds the device memory of an apply: the ket sectors are cut into consecutive chunks whose T slices,
 // S rows and coefficient blocks together take at most max_doubles (a larger sector is a chunk of its
-// own), and every FP64 apply runs chunk by chunk: the chunk's T-GEMM into one T scratch, its coefficient
-// blocks generated into one scratch, its S-GEMM into one S scratch and its split-K L.S partials; the
+// own; when the whole coefficient blocks take at most half of max_doubles they are kept, generated once,
+// and the chunks' T and S share the rest), and every FP64 apply runs chunk by chunk: the chunk's T-GEMM
+// into one T scratch, its coefficient blocks (unless kept) generated into one scratch, its S-GEMM into
+// one S scratch and its split-K L.S partials; the
 // partials of all chunks are summed at the end in the fixed order, so the result is the whole apply's
 // to the bit.  0 (or a plan that fits) undoes it.  Set before upload_plan; supersedes
 // stream_coefficients; the mixed forms, the adjoint and plan groups need the whole apply.

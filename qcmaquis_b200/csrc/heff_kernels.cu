@@ -504,11 +504,12 @@ void launch_t_chunk(HeffPlan& p, int sh, const HeffPlan::SChunk& c, const double
 }
 
 template <class S>
-void launch_s_chunk(HeffPlan& p, int sh, const HeffPlan::SChunk& c, const double* Tb, double* Sb, cudaStream_t s) {
+void launch_s_chunk(HeffPlan& p, int sh, const HeffPlan::SChunk& c, uint64_t w0, const double* Tb, double* Sb,
+                    cudaStream_t s) {
     const uint32_t a = c.ut[0][sh], b = c.ut[1][sh];
     if (b > a)
         k_sgemm<S><<<unsigned(b - a), NTHR, 0, s>>>(p.d_units.get(), p.d_utiles[sh].get() + a, p.d_line_b1.get(),
-                                                    p.d_slice_off.get(), p.d_klist.get(), p.d_W.get(), Tb, Sb, c.w0);
+                                                    p.d_slice_off.get(), p.d_klist.get(), p.d_W.get(), Tb, Sb, w0);
 }
 
 template <class S>
@@ -562,11 +563,12 @@ void apply_impl(HeffPlan& p, const double* x, double* y, cudaEvent_t* ev, double
             launch_t_chunk<Sh32>(p, SHAPE_32, c, x, Tb, s);
             launch_t_chunk<Sh64>(p, SHAPE_64, c, x, Tb, s);
             if (c.s1 > c.s0) QCM_CUDA(cudaMemsetAsync(Sb, 0, (c.s1 - c.s0) * sizeof(double), s));
-            p.cg.generate_range(p.d_W.get(), c.u0, c.u1, c.w0, c.w1, s);
-            launch_s_chunk<Sh16>(p, SHAPE_16, c, Tb, Sb, s);
-            launch_s_chunk<Sh32>(p, SHAPE_32, c, Tb, Sb, s);
-            launch_s_chunk<Sh64>(p, SHAPE_64, c, Tb, Sb, s);
-            launch_s_chunk<Sh128>(p, SHAPE_128, c, Tb, Sb, s);
+            const uint64_t w0 = p.chunk_keeps_w ? 0 : c.w0;  // kept blocks: the whole, from element 0
+            if (!p.chunk_keeps_w) p.cg.generate_range(p.d_W.get(), c.u0, c.u1, c.w0, c.w1, s);
+            launch_s_chunk<Sh16>(p, SHAPE_16, c, w0, Tb, Sb, s);
+            launch_s_chunk<Sh32>(p, SHAPE_32, c, w0, Tb, Sb, s);
+            launch_s_chunk<Sh64>(p, SHAPE_64, c, w0, Tb, Sb, s);
+            launch_s_chunk<Sh128>(p, SHAPE_128, c, w0, Tb, Sb, s);
             launch_ls_chunk<Sh16>(p, SHAPE_16, c, Sb, Pb, s);
             launch_ls_chunk<Sh32>(p, SHAPE_32, c, Sb, Pb, s);
             launch_ls_chunk<Sh64>(p, SHAPE_64, c, Sb, Pb, s);
@@ -723,7 +725,7 @@ int heff_launches_per_apply(const HeffPlan& p) {
     if (p.sector_chunked()) {
         n = 0;
         for (const HeffPlan::SChunk& c : p.schunks) {
-            n += c.u1 > c.u0;
+            n += !p.chunk_keeps_w && c.u1 > c.u0;
             for (int sh = 0; sh < N_SHAPES; ++sh)
                 n += (c.tt[1][sh] > c.tt[0][sh]) + (c.ut[1][sh] > c.ut[0][sh]) + (c.kt[1][sh] > c.kt[0][sh]);
         }
@@ -903,7 +905,7 @@ void upload_plan(HeffPlan& p, bool lists) {
     if (lists) stage_lists(p);
     p.cg.upload(s);
     // dense coefficient blocks, built once per plan and reused by every apply
-    if (p.streamed() || p.sector_chunked()) {
+    if (p.streamed() || (p.sector_chunked() && !p.chunk_keeps_w)) {
         // one chunk's scratch; every chunk generated once here so that a term without a slot is found
         // when the plan is staged (each apply generates them again, unchecked)
         uint64_t mx = 1;
@@ -1002,13 +1004,16 @@ void chunk_sectors(HeffPlan& p, uint64_t max_doubles) {
     if (p.part_t.size() < 2) throw std::runtime_error("chunk_sectors: the plan has no ket-sector prefixes");
     p.wchunks.clear();  // the chunks below generate their own coefficient blocks
     const std::size_t np = p.part_t.size() - 1;
+    p.chunk_keeps_w = p.w_len <= max_doubles / 2;
+    const uint64_t room = p.chunk_keeps_w ? max_doubles - p.w_len : max_doubles;
     auto size = [&](std::size_t a, std::size_t b) {
-        return (p.part_t[b] - p.part_t[a]) + (p.part_s[b] - p.part_s[a]) + (p.part_w[b] - p.part_w[a]);
+        return (p.part_t[b] - p.part_t[a]) + (p.part_s[b] - p.part_s[a]) +
+               (p.chunk_keeps_w ? 0 : p.part_w[b] - p.part_w[a]);
     };
     std::vector<uint32_t> chunk_of(np);
     std::size_t a = 0;
     for (std::size_t i = 1; i <= np; ++i) {
-        if (i < np && size(a, i + 1) <= max_doubles) continue;
+        if (i < np && size(a, i + 1) <= room) continue;
         HeffPlan::SChunk c;
         c.p0 = uint32_t(a); c.p1 = uint32_t(i);
         c.u0 = p.part_unit[a]; c.u1 = p.part_unit[i];

@@ -121,3 +121,20 @@ def test_chunked_apply_at_the_bench_bond_shapes(gpu_ctx):
     assert np.array_equal(plan.apply(x), y)
     plan.stream_coefficients(0)
     assert np.array_equal(plan.apply(x), y)
+
+
+def test_chunked_apply_keeping_the_coefficient_blocks(gpu_ctx):
+    """A budget of at least twice the coefficient blocks keeps them whole (generated once, no generation
+    launches in the apply) while T and S still run in chunks: the same apply to the bit."""
+    from qcmaquis_b200.heff import parse_site_problem, plan_from_problem
+    L, M, sw, step = 10, 48, 1, 4
+    h, V, e, m, ts, blob = qc_system(L)
+    prob = parse_site_problem(snapshot(L, M, sw, step))
+    plan = plan_from_problem(gpu_ctx, prob, ts, site_of_step(L, step))
+    x = np.random.default_rng(5).standard_normal(plan.n)
+    y = plan.apply(x)
+    i = plan.info
+    w, tsb = 8 * int(i["w_len"]), 8 * (int(i["t_len"]) + int(i["s_len"]))
+    plan.chunk_apply(w + tsb // 3 if w + tsb // 3 >= 2 * w else 2 * w + tsb // 3)
+    assert np.array_equal(plan.apply(x), y)
+    plan.chunk_apply(0)
