@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(NTHR, 5) k_sgemm(const UnitD* __restrict__ uni
 // One CTA per unit, one thread per line: the line's coefficient terms (CoefGen), in MPO-entry
 // then operator-term order, summed into W_u.  Products and sums are rounded separately (no
 // contraction), so W_u holds the same values as a host evaluation of the same terms.
-constexpr int WG_THR = 128;
+constexpr int WG_THR = 256;  // 256 against 128: streamed applies 3-11 % faster
 constexpr uint32_t WG_SMAP = 4096;  // (slice id, slot) pairs staged in shared memory
 constexpr uint32_t WG_NST = 64;     // physical states of the basis
 __global__ void __launch_bounds__(WG_THR) k_wgen(const WGenUnitD* __restrict__ units, const WGenInD* __restrict__ gin,
