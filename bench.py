@@ -221,6 +221,16 @@ def dist_setup(a):
     return world, rank, local, pg
 
 
+def max_over_ranks(v, pg, dev):
+    """The largest of every rank's v (a time): all ranks take part; with no process group, v."""
+    if pg is None:
+        return float(v)
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_traffic(a):
     """DRAM bytes (read + written) of the S-GEMM phase per apply, from the ncu capture of this workload
     summarised in profiles/ (dram__bytes_read.sum + dram__bytes_write.sum), or (None, None)."""
@@ -325,11 +335,8 @@ def measure_mixed(a, plan, xd, yd, xp, yp, hb, flush, info, world, pg, dev, snap
         t0 = time.perf_counter()
         check(lib.qcm_heff_apply_mode(plan.h, xp, yp, mode), "qcm_heff_apply_mode")
         e2e_t.append(time.perf_counter() - t0)
-    e2e_s = float(sum(e2e_t))
-    if pg is not None:
-        t = torch.tensor([total_ms, e2e_s], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms, e2e_s = float(t[0].item()), float(t[1].item())
+    total_ms = max_over_ranks(total_ms, pg, dev)
+    e2e_s = max_over_ranks(sum(e2e_t), pg, dev)
     ph = np.mean(np.array(phases), axis=0)
     y_mixed = hb["y"].numpy().copy()
     out = {"value": info["flops"] * a.steps * world / (total_ms * 1e-3) / 1e9, "unit": "GFLOP/s",
@@ -634,11 +641,8 @@ def run_b200(a, world, rank, local, pg):
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     ck = clocks.stop()
-    total_ms = float(sum(times))
+    total_ms = max_over_ranks(sum(times), pg, dev)
     if pg is not None:
-        t = torch.tensor([total_ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
         pg.barrier()
     value = info["flops"] * a.steps * world / (total_ms * 1e-3) / 1e9
     # e2e through the C-ABI with pinned host buffers
@@ -655,11 +659,7 @@ def run_b200(a, world, rank, local, pg):
         t0 = time.perf_counter()
         check(lib.qcm_heff_apply(plan.h, xp, yp), "qcm_heff_apply")
         e2e_t.append(time.perf_counter() - t0)
-    e2e_s = float(sum(e2e_t))
-    if pg is not None:
-        t = torch.tensor([e2e_s], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(sum(e2e_t), pg, dev)
     e2e_val = info["flops"] * a.steps * world / e2e_s / 1e9
     y_dev = yh.numpy().copy()
     # the checker: the oracle builds the same problem itself; the device result against it, and the
