@@ -22,7 +22,7 @@
 // staged K-major (the element-wise copies transpose them on the way) in the canonical
 // no-swizzle layout: 8 MN rows x 4 consecutive slices = one 128-byte core matrix, groups of 8
 // MN rows 128 B apart (SBO), 4-slice chunks MN/8 * 128 B apart (LBO), two chunks per K = 8
-// MMA.  (This build's probe of the MN-major encoding of these descriptors on B200 returned
+// MMA.  (A standalone probe of the MN-major encoding of these descriptors on B200 returned
 // zeros, the K-major one the exact product, so the K-major form is the one used.)  One
 // thread issues the MMAs of a stage and commits them to the stage's mbarrier; a stage buffer
 // is refilled only after that mbarrier completes.
@@ -393,7 +393,7 @@ __global__ void __launch_bounds__(XTHR) k_sgemm_tc(const UnitD* __restrict__ uni
         if (it + 1 < nsteps) {
             mcur = ks[2 + it] & 15u;
             // the other buffer was read by the MMAs of step it - 1: wait for them before refilling it
-            // (the verdict is made uniform, so every thread leaves the loop at the same barrier)
+            // (the outcome is made uniform, so every thread leaves the loop at the same barrier)
             if (it >= 1) {
                 const bool w = mbar_wait(saddr(&mbar[(it + 1) & 1]), ((it - 1) >> 1) & 1u);
                 if (!__syncthreads_and(w)) { ok = false; break; }

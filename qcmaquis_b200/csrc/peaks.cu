@@ -1,5 +1,5 @@
-// FP64 throughput probes (the FP64 peaks are not part of the driver-measured
-// MEASURED_PEAKS.json): a DMMA (mma.sync m8n8k4 .f64) loop and a DFMA loop,
+// FP64 throughput probes (the measured copy and bf16 peaks have no FP64 counterpart): a DMMA
+// (mma.sync m8n8k4 .f64) loop and a DFMA loop,
 // register-resident, one CTA per SM x occupancy.  Used as roofline denominators
 // for the plain FP64 form.
 #include <cuda_runtime.h>

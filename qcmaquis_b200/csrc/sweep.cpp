@@ -115,7 +115,7 @@ double jacobi_davidson(Ctx& c, HeffPlan& p, double* x, double tol, int maxiter, 
             dev_axpy_dscalar(sc + 243, -inv_oo[a], Oi(a), t, n, c.s);
         }
     };
-    // The mixed form's FP64 residual correction (north star form 1): u (the mixed solve's vector) gets an
+    // The mixed form's FP64 residual correction (the precision form): u (the mixed solve's vector) gets an
     // FP64 apply for its Rayleigh quotient and residual; then, while that residual is above tol |theta|
     // and steps remain, one Jacobi-Davidson step in FP64: t = -r + (r.u)/(u.u) u projected and made
     // orthogonal to u, Rayleigh-Ritz on span{u, t} (2 x 2, FP64 H.psi of t).  Returns the FP64
