@@ -471,7 +471,24 @@ void preconditioned_svd(Ctx& c, const DBlocks& both, BlockSVD& r, int* zero_coun
 }  // namespace
 
 BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff) {
-    const std::size_t nb = both.n();
+    BlockSVD r = svd_truncate_groups(c, both, {0, both.n()}, {Mmax}, {cutoff});
+    r.tr = r.gtr[0];
+    return r;
+}
+
+BlockSVD svd_truncate_groups(Ctx& c, const DBlocks& both, const std::vector<std::size_t>& g0,
+                             const std::vector<uint64_t>& Mmax, const std::vector<double>& cutoff) {
+    const std::size_t nb = both.n(), ng = Mmax.size();
+    if (g0.size() != ng + 1 || cutoff.size() != ng || g0.front() != 0 || g0.back() != nb)
+        throw std::runtime_error("svd_truncate_groups: group ranges do not cover the blocks");
+    // the cut of group g over its blocks' singular values: keep[k] for its blocks
+    auto cut = [&](std::size_t g, const std::vector<std::vector<double>>& vals, std::vector<uint32_t>& keep) {
+        std::vector<std::vector<double>> gv(vals.begin() + long(g0[g]), vals.begin() + long(g0[g + 1]));
+        std::vector<uint32_t> gk;
+        const TruncResults t = estimate_cut(gv, Mmax[g], cutoff[g], gk);
+        std::copy(gk.begin(), gk.end(), keep.begin() + long(g0[g]));
+        return t;
+    };
     BlockSVD r;
     r.uo.resize(nb); r.so.resize(nb); r.vo.resize(nb); r.kk.resize(nb);
     uint64_t ul = 0, sl = 0, vl = 0;
@@ -532,8 +549,8 @@ BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff)
     {
         // a kept singular value of exactly zero needs an orthonormal completion of its singular
         // vectors: such blocks are recomputed by cuSOLVER's gesvdj
-        std::vector<uint32_t> keep0;
-        estimate_cut(r.vals, Mmax, cutoff, keep0);
+        std::vector<uint32_t> keep0(nb, 0);
+        for (std::size_t g = 0; g < ng; ++g) cut(g, r.vals, keep0);
         std::vector<std::size_t> redo;
         for (std::size_t k = 0; k < nb; ++k)
             if (hz[k] && keep0[k] + uint32_t(hz[k]) > r.kk[k]) redo.push_back(k);
@@ -555,21 +572,28 @@ BlockSVD svd_truncate(Ctx& c, const DBlocks& both, uint64_t Mmax, double cutoff)
             for (std::size_t k : redo) r.vals[k].assign(hs.begin() + r.so[k], hs.begin() + r.so[k] + r.kk[k]);
         }
     }
-    r.tr = estimate_cut(r.vals, Mmax, cutoff, r.keep);
+    r.keep.assign(nb, 0);
+    r.gtr.resize(ng);
+    for (std::size_t g = 0; g < ng; ++g) r.gtr[g] = cut(g, r.vals, r.keep);
     return r;
 }
 
 TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMPS& m1, DMPS& m2) {
-    const std::size_t nb = both.n();
     BlockSVD sv = svd_truncate(c, both, Mmax, cutoff);
-    const std::vector<uint32_t>& keep = sv.keep;
-    const TruncResults tr = sv.tr;
-    const std::vector<uint64_t>& uo = sv.uo;
-    const std::vector<uint64_t>& so = sv.so;
-    const std::vector<uint64_t>& vo = sv.vo;
-    DBuf<double>& U = sv.U;
-    DBuf<double>& S = sv.S;
-    DBuf<double>& V = sv.V;
+    return split_from(c, l2r, sv, 0, 0, m1, m2);
+}
+
+TruncResults DTwoSite::split_from(Ctx& c, bool l2r, const BlockSVD& sv, std::size_t b0, std::size_t g, DMPS& m1, DMPS& m2) {
+    const std::size_t nb = both.n();
+    if (b0 + nb > sv.keep.size() || g >= sv.gtr.size()) throw std::runtime_error("split: blocks outside the decomposition");
+    const std::vector<uint32_t> keep(sv.keep.begin() + long(b0), sv.keep.begin() + long(b0 + nb));
+    const TruncResults tr = sv.gtr[g];
+    const std::vector<uint64_t> uo(sv.uo.begin() + long(b0), sv.uo.begin() + long(b0 + nb));
+    const std::vector<uint64_t> so(sv.so.begin() + long(b0), sv.so.begin() + long(b0 + nb));
+    const std::vector<uint64_t> vo(sv.vo.begin() + long(b0), sv.vo.begin() + long(b0 + nb));
+    const DBuf<double>& U = sv.U;
+    const DBuf<double>& S = sv.S;
+    const DBuf<double>& V = sv.V;
     const uint64_t ul = sv.u_len, vl = sv.v_len;
     // U[:, :keep] and V^T[:keep, :], with S multiplied into V^T (l2r) or U (r2l)
     m1 = DMPS(); m2 = DMPS();
@@ -603,7 +627,7 @@ TruncResults DTwoSite::split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMP
         else dev_scale_cols(m1.b.d.get() + m1.b.off[i], both.rows[k], keep[k], both.rows[k], S.get() + so[k], c.s);
         ++i;
     }
-    QCM_CUDA(cudaStreamSynchronize(c.s));  // U, S, V are released on return
+    QCM_CUDA(cudaStreamSynchronize(c.s));  // the decomposition's buffers may be released on return
     return tr;
 }
 

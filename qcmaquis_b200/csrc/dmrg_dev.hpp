@@ -159,8 +159,14 @@ struct BlockSVD {
     DBuf<double> U, S, V;
     uint64_t u_len = 0, s_len = 0, v_len = 0;
     TruncResults tr;
+    std::vector<TruncResults> gtr;  // per group (svd_truncate_groups)
 };
 BlockSVD svd_truncate(Ctx& c, const DBlocks& M, uint64_t Mmax, double cutoff);
+// The blocks of several independent matrices in one decomposition (one QR, one Jacobi and one assembly
+// launch for all), each group of blocks [g0[g], g0[g+1]) cut by its own Mmax and cutoff: keep[] per
+// block, gtr[] per group.
+BlockSVD svd_truncate_groups(Ctx& c, const DBlocks& M, const std::vector<std::size_t>& g0,
+                             const std::vector<uint64_t>& Mmax, const std::vector<double>& cutoff);
 // heev_truncate (block_matrix_algorithms.h:299-355) of device symmetric blocks: dm is
 // overwritten by its eigenvectors (ascending eigenvalue order, so the kept ones are the last
 // keep[k] columns read backwards); the cut is on sqrt of the positive eigenvalues and the
@@ -182,6 +188,9 @@ struct DTwoSite {
     void twin_to_both(Ctx& c);  // reshape_right_to_both
     // split_mps_l2r / split_mps_r2l with svd_truncate (block_matrix_algorithms.h:136-240)
     TruncResults split(Ctx& c, bool l2r, uint64_t Mmax, double cutoff, DMPS& m1, DMPS& m2);
+    // the same from a decomposition already made: this tensor's blocks are sv's blocks b0 .. b0 + n,
+    // cut as sv's group g
+    TruncResults split_from(Ctx& c, bool l2r, const BlockSVD& sv, std::size_t b0, std::size_t g, DMPS& m1, DMPS& m2);
     // predict_split_l2r / _r2l (contractions/boundary_ops/prediction.hpp:152-236): reduced density
     // matrix plus alpha times the boundary noise (B = L[site1] with W = mpo[site1] for l2r,
     // R[site2+1] with mpo[site2] for r2l), truncated by heev; alpha = 0 is the SVD split
@@ -318,7 +327,8 @@ struct StepState {
     uint64_t key = 0;
     bool resident = false;  // the plan's device buffers were kept from the previous sweep
     bool timing = false;
-    double t0 = 0, t1 = 0, tt[8] = {};
+    bool pre_done = false;  // step_finish_pre ran
+    double t0 = 0, t1 = 0, t2 = 0, tt[8] = {};
 };
 
 struct DevDMRG {
@@ -385,7 +395,12 @@ struct DevDMRG {
     void step_prepare_site(StepState& S, int step);
     void step_prepare_plan(StepState& S);
     void step_prepare_stage(StepState& S, bool group);
-    void step_finish(StepState& S, double eigenvalue, double& energy, TruncResults& tr);
+    // step_finish_pre: the plan kept for the next sweep and the eigenvector reshaped to the two-site
+    // blocks (the first part of step_finish); step_finish with sv: the truncation from a decomposition
+    // made for many runs at once, this run's blocks from b0 on, cut as its group g
+    void step_finish_pre(StepState& S);
+    void step_finish(StepState& S, double eigenvalue, double& energy, TruncResults& tr, const BlockSVD* sv = nullptr,
+                     std::size_t b0 = 0, std::size_t g = 0);
     int last_iters = 0;  // JD iterations of the last step
 
   private:

@@ -757,6 +757,7 @@ void DevDMRG::step_prepare_site(StepState& S, int _site) {
     make_left_paired(c, mps[S.site1]);
     make_right_paired(c, mps[S.site2]);
     S.tst = DTwoSite();
+    S.pre_done = false;
     S.tst.build(c, mps[S.site1], mps[S.site2]);
     if (S.timing) {
         QCM_CUDA(cudaStreamSynchronize(c.s));
@@ -796,7 +797,20 @@ void DevDMRG::step_prepare(StepState& S, int _site) {
     st.plan_s += S.t1 - S.t0;
 }
 
-void DevDMRG::step_finish(StepState& S, double E, double& energy, TruncResults& tr) {
+void DevDMRG::step_finish_pre(StepState& S) {
+    if (S.pre_done) return;
+    S.t2 = now_s();
+    keep_plan(S.step, std::move(S.plan), S.key);
+    S.tst.twin_to_both(c);
+    if (S.timing) {
+        QCM_CUDA(cudaStreamSynchronize(c.s));
+        S.tt[3] = now_s();
+    }
+    S.pre_done = true;
+}
+
+void DevDMRG::step_finish(StepState& S, double E, double& energy, TruncResults& tr, const BlockSVD* sv, std::size_t b0,
+                          std::size_t g) {
     const int _site = S.step, site1 = S.site1, site2 = S.site2;
     DTwoSite& tst = S.tst;
     auto mark = [&](int i) {
@@ -804,16 +818,15 @@ void DevDMRG::step_finish(StepState& S, double E, double& energy, TruncResults& 
         QCM_CUDA(cudaStreamSynchronize(c.s));
         S.tt[i] = now_s();
     };
-    const double t2 = now_s();
-    keep_plan(_site, std::move(S.plan), S.key);
-    tst.twin_to_both(c);
-    mark(3);
+    step_finish_pre(S);
+    const double t2 = S.t2;
     energy = E + p.ecore;
     double t3_last = 0;
     const double alpha = sweep_count < p.ngrowsweeps ? p.alpha_initial
                          : (sweep_count < p.ngrowsweeps + p.nmainsweeps ? p.alpha_main : p.alpha_final);
     if (S.lr == 1) {
         tr = p.heev ? tst.predict_split(c, true, p.Mmax, p.cutoff, alpha, *left_[site1], mpo[site1], mps[site1], mps[site2])
+             : sv   ? tst.split_from(c, true, *sv, b0, g, mps[site1], mps[site2])
                     : tst.split(c, true, p.Mmax, p.cutoff, mps[site1], mps[site2]);
         mark(4);
         DBlocks t = normalize_left(c, mps[site2]);
@@ -834,6 +847,7 @@ void DevDMRG::step_finish(StepState& S, double E, double& energy, TruncResults& 
         st.boundary_s += now_s() - t3;
     } else {
         tr = p.heev ? tst.predict_split(c, false, p.Mmax, p.cutoff, alpha, *right_[site2 + 1], mpo[site2], mps[site1], mps[site2])
+             : sv   ? tst.split_from(c, false, *sv, b0, g, mps[site1], mps[site2])
                     : tst.split(c, false, p.Mmax, p.cutoff, mps[site1], mps[site2]);
         mark(4);
         DBlocks t = normalize_right(c, mps[site1]);
@@ -950,9 +964,56 @@ void dmrg_group_sweep(const std::vector<DevDMRG*>& runs, std::vector<std::vector
             d.st.hpsi_count += uint64_t(applies);
             d.st.hpsi_flops += double(applies) * S[i].plan->flops;
             d.last_iters = iters[i];
+        }
+        // the truncations: every run's two-site blocks in one decomposition (one QR, one Jacobi and one
+        // assembly launch), each run cut by its own bond dimension and cutoff (runs truncating by the
+        // density matrix run their own)
+        for (std::size_t i = 0; i < nr; ++i) runs[i]->step_finish_pre(S[i]);
+        std::vector<std::size_t> svd_run;
+        for (std::size_t i = 0; i < nr; ++i)
+            if (!runs[i]->p.heev) svd_run.push_back(i);
+        BlockSVD sv;
+        std::vector<std::size_t> b0(nr, 0), gi(nr, 0);
+        if (!svd_run.empty()) {
+            const double ts = now_s();
+            DBlocks all;
+            std::vector<std::size_t> g0{0};
+            std::vector<uint64_t> mm;
+            std::vector<double> co;
+            std::vector<uint64_t> base;
+            for (std::size_t q = 0; q < svd_run.size(); ++q) {
+                const DBlocks& b = S[svd_run[q]].tst.both;
+                b0[svd_run[q]] = all.n();
+                gi[svd_run[q]] = q;
+                base.push_back(all.total);
+                for (std::size_t k = 0; k < b.n(); ++k) {
+                    all.lc.push_back(b.lc[k]); all.rc.push_back(b.rc[k]);
+                    all.rows.push_back(b.rows[k]); all.cols.push_back(b.cols[k]);
+                    all.off.push_back(all.total + b.off[k]);
+                }
+                all.total += (b.total + 31) / 32 * 32;
+                g0.push_back(all.n());
+                mm.push_back(runs[svd_run[q]]->p.Mmax);
+                co.push_back(runs[svd_run[q]]->p.cutoff);
+            }
+            all.allocate(r0.c.s, false);
+            for (std::size_t q = 0; q < svd_run.size(); ++q) {
+                const DBlocks& b = S[svd_run[q]].tst.both;
+                if (b.total)
+                    QCM_CUDA(cudaMemcpyAsync(all.d.get() + base[q], b.d.get(), b.total * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, r0.c.s));
+            }
+            sv = svd_truncate_groups(r0.c, all, g0, mm, co);
+            const double dts = (now_s() - ts) / double(svd_run.size());
+            for (std::size_t i : svd_run) runs[i]->st.trunc_s += dts;
+        }
+        for (std::size_t i = 0; i < nr; ++i) {
+            DevDMRG& d = *runs[i];
             double E = 0;
             TruncResults tr;
-            d.step_finish(S[i], ev[i], E, tr);
+            S[i].t2 = now_s();  // the shared decomposition is counted above
+            if (d.p.heev) d.step_finish(S[i], ev[i], E, tr);
+            else d.step_finish(S[i], ev[i], E, tr, &sv, b0[i], gi[i]);
             energies[i].push_back(E);
             trunc[i].push_back(tr);
         }
